@@ -1,0 +1,262 @@
+/*
+ * ostc.h — C ABI of the B200-native right-hand-side and time-advance path of
+ * the OpenSTC-dev structured-grid compressible reacting-flow solver.
+ *
+ * The ABI keeps the reference's device data model so that the path is a
+ * drop-in for the per-stage calls made by RK3_bv (src/RK.cuh:301-355):
+ *
+ *   - every field array is a ColMajor ggxl::VectorField3D / Array3D
+ *     (src/gxl_lib/Array.hpp:128-194): one plane per variable, i fastest,
+ *     element (i,j,k,l) at  k*disp1 + j*disp2 + i + dispt + l*sz  with
+ *     disp2 = mx+2g, disp1 = (my+2g)*disp2, dispt = (disp1+disp2+1)*g,
+ *     sz = (mx+2g)(my+2g)(mz+2g), g = the array's own ghost count;
+ *   - the metric is the reference's gxl::Matrix<double,3,3,1> per point
+ *     (src/gxl_lib/Matrix.hpp:214-233): an int bias, 4 bytes of padding and
+ *     9 doubles, 80 bytes per point; row d (0 = xi, 1 = eta, 2 = zeta) holds
+ *     (d_x, d_y, d_z);
+ *   - scheme selection uses the reference's setup-file tags
+ *     (input_files/setup/2_scheme.txt, decoded in src/Parameter.cpp:165-218).
+ *
+ * All pointers in ostc_zone are DEVICE pointers owned by the caller (the
+ * reference's Field::h_ptr members, src/Field.cu:133-251). Species and
+ * reaction tables in ostc_param are HOST pointers copied at ostc_create.
+ *
+ * Every entry point returns an ostc_status; none aborts. Work is enqueued on
+ * the stream passed in; no entry point below synchronises the host unless
+ * its comment says so.
+ */
+#ifndef OSTC_H
+#define OSTC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------------- */
+/* status codes                                                            */
+/* ----------------------------------------------------------------------- */
+typedef enum ostc_status {
+  OSTC_OK = 0,
+  OSTC_ERR_INVALID_ARG = 1,   /* bad pointer, size, tag or combination      */
+  OSTC_ERR_CUDA = 2,          /* a CUDA runtime call failed                 */
+  OSTC_ERR_TIMEOUT = 3,       /* a bounded device wait gave up              */
+  OSTC_ERR_NONPHYSICAL = 4,   /* NaN / non-positive density or pressure     */
+  OSTC_ERR_UNSUPPORTED = 5,   /* scheme combination not built               */
+  OSTC_ERR_NO_DEVICE = 6      /* no CUDA device visible                     */
+} ostc_status;
+
+/* Mixture model, same meaning as cfd::MixtureModel (src/Define.h:19-25).  */
+enum { OSTC_MIX_AIR = 0, OSTC_MIX_MIXTURE = 1, OSTC_MIX_FR = 2 };
+
+/* Boundary labels, same numbers as the reference (src/BoundCond.h:4-11).
+ * OSTC_BC_PERIODIC has no counterpart in the reference (quirk A13): it
+ * wraps ghost layers from the opposite face of the same block.            */
+enum {
+  OSTC_BC_WALL = 2, OSTC_BC_SYMMETRY = 3, OSTC_BC_FARFIELD = 4,
+  OSTC_BC_INFLOW = 5, OSTC_BC_OUTFLOW = 6, OSTC_BC_SUBSONIC_INFLOW = 7,
+  OSTC_BC_BACK_PRESSURE = 9, OSTC_BC_PERIODIC = 100
+};
+
+#define OSTC_MAX_SPEC 20   /* MAX_SPEC_NUMBER of the reference build      */
+#define OSTC_MAX_REAC 50   /* MAX_REAC_NUMBER of the reference build      */
+
+/* ----------------------------------------------------------------------- */
+/* data model                                                              */
+/* ----------------------------------------------------------------------- */
+
+/* One grid block: the device arrays of cfd::DZone (src/Field.h:13-71).
+ * Arrays with "g=ngg" carry the block's ghost layers, "g=0" none,
+ * "g=dq_ngg" the dq ghost count (0 for RK3, 1 for DPLUR, src/Field.cu:203-212).
+ * Unused arrays may be NULL (see ostc_zone_required()).                    */
+typedef struct ostc_zone {
+  int mx, my, mz, ngg;       /* interior extents and ghost count           */
+  int dq_ngg;                /* ghosts of dq/dq0/dqk/spectral radii: 0 or 1 */
+  int reserved_;
+  const double *x, *y, *z;   /* g=ngg; only read by ostc_metric_from_grid   */
+  const double *jac;         /* g=ngg                                        */
+  const void *metric;        /* g=ngg, 80-byte gxl::Matrix<real,3,3,1>      */
+  double *wall_distance;     /* g=ngg (SST)                                  */
+  double *cv;                /* g=ngg, n_var planes                          */
+  double *bv;                /* g=ngg, 6 planes: rho,u,v,w,p,T               */
+  double *sv;                /* g=ngg, n_scalar planes: Y_k, k, omega        */
+  double *bv_last;           /* g=0, 4 planes (residual)                     */
+  double *vel, *acoustic_speed, *mach, *mul, *thermal_conductivity; /* g=ngg */
+  double *rho_D;             /* g=ngg, n_spec planes                         */
+  double *gamma, *cp;        /* g=ngg (mixtures)                             */
+  double *chem_src_jac;      /* g=0, n_spec^2 (EPI) or n_spec (DA) planes    */
+  double *mut, *turb_therm_cond; /* g=ngg (SST)                              */
+  double *turb_src_jac;      /* g=0, 2 planes (SST implicit)                 */
+  double *dq, *dq0, *dqk;    /* g=dq_ngg, n_var planes                       */
+  double *inv_spectr_rad;    /* g=dq_ngg, 3 interleaved doubles per point    */
+  double *visc_spectr_rad;   /* g=dq_ngg                                     */
+  double *dt_local;          /* g=0                                          */
+  double *entropy_fix_delta; /* g=1 (Roe)                                    */
+  double *qn;                /* g=ngg, n_var planes (RK3)                    */
+} ostc_zone;
+
+/* Scheme tags and physical tables: the fields of cfd::DParameter
+ * (src/DParameter.cuh:13-92) plus the derived tags of
+ * Parameter::deduce_known_info (src/Parameter.cpp:165-218).
+ * Table pointers are HOST pointers, row-major, copied by ostc_create.      */
+typedef struct ostc_param {
+  int mix_model;             /* OSTC_MIX_*                                   */
+  int turbulence;            /* 0 laminar, 1 RANS (SST when rans_model==2)   */
+  int n_var, n_scalar, n_spec, n_reac, i_turb_cv;
+  int inviscid_scheme;       /* 1 LF, 2 Roe, 3 AUSM+, 4 HLLC                 */
+  int reconstruction;        /* 1 first order, 2 MUSCL, 3 NND2, 4 WENO5      */
+  int limiter;               /* 0 minmod                                     */
+  int inviscid_type;         /* derived: 0 pv, 1 AWENO, 2 Roe (Parameter.cpp:193-198) */
+  int viscous_scheme;        /* viscous_order: 0 inviscid, 2 central         */
+  int rans_model, turb_implicit, compressibility_correction;
+  int chemSrcMethod;         /* 0 explicit, 1 EPI, 2 DA                      */
+  int gradPInDiffusionFlux;
+  int dimension;             /* 2 or 3                                       */
+  double entropy_fix_factor, Pr, Prt, Sct, Sc, cfl;
+  /* species tables */
+  const double *mw;          /* [n_spec]                                     */
+  const double *high_temp_coeff, *low_temp_coeff; /* [n_spec][7]           */
+  const double *t_low, *t_mid, *t_high;           /* [n_spec]              */
+  const double *LJ_potent_inv, *vis_coeff;        /* [n_spec]              */
+  const double *WjDivWi_to_One4th, *sqrt_WiDivWjPl1Mul8; /* [n_spec][n_spec] */
+  const double *binary_diffusivity_coeff, *kb_over_eps_jk; /* [n_spec][n_spec] */
+  /* reaction tables */
+  const int *reac_type;                 /* [n_reac] labels 0..7             */
+  const int *stoi_f, *stoi_b;           /* [n_reac][n_spec]                 */
+  const int *reac_order;                /* [n_reac]                         */
+  const double *A, *b, *Ea, *A2, *b2, *Ea2; /* [n_reac]                     */
+  const double *third_body_coeff;       /* [n_reac][n_spec]                 */
+  const double *troe_alpha, *troe_t3, *troe_t1, *troe_t2; /* [n_reac]       */
+} ostc_param;
+
+/* One boundary face of one block: cfd::Boundary (src/Mesh.h:9-31) after
+ * register_boundary (ranges already widened by ngg on tangential axes),
+ * with the state of the boundary condition attached (src/BoundCond.h).    */
+typedef struct ostc_bc_face {
+  int block;                 /* zone index                                   */
+  int type_label;            /* OSTC_BC_*                                    */
+  int face;                  /* 0 i, 1 j, 2 k                                */
+  int direction;             /* -1 on the min face, +1 on the max face       */
+  int range_start[3], range_end[3]; /* inclusive                            */
+  /* inflow / farfield state (cfd::Inflow, src/BoundCond.h:23-44)           */
+  double density, u, v, w, pressure, temperature, velocity, mut;
+  double sv[OSTC_MAX_SPEC + 4];
+  /* wall (cfd::Wall): isothermal flag and temperature                       */
+  int wall_isothermal;
+  double wall_temperature;
+} ostc_bc_face;
+
+/* Options of the time-advance path (the relevant keys of 2_scheme.txt). */
+typedef struct ostc_config {
+  int steady;                /* 0 unsteady (RK3), 1 steady                   */
+  int temporal_scheme;       /* 3 SSPRK3                                     */
+  int implicit_method;       /* 0 explicit, 1 DPLUR                          */
+  int DPLUR_inner_step;
+  int fixed_time_step;       /* 1: dt given; 0: CFL dt each stage (quirk A12) */
+  double dt;
+  int output_screen;         /* residual cadence, RK.cuh:289                 */
+  int compat;                /* 1: replicate reference quirks (Appendix A)   */
+} ostc_config;
+
+typedef struct ostc_ctx ostc_ctx;
+
+/* ----------------------------------------------------------------------- */
+/* lifecycle                                                               */
+/* ----------------------------------------------------------------------- */
+
+/* Build a context over n_zones caller-owned blocks. Replaces the setup half
+ * of Driver<mix,turb> (src/Driver.cu:10-35): copies the DParameter tables
+ * and BC data to the device and repacks the 80-byte metric into SoA planes
+ * (immutable input). Synchronises the device once.                        */
+ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param,
+                        const ostc_zone *zones, int n_zones,
+                        const ostc_bc_face *faces, int n_faces,
+                        ostc_ctx **out);
+ostc_status ostc_destroy(ostc_ctx *ctx);
+
+/* Which optional ostc_zone arrays the given param/config needs (bit mask in
+ * the order of ostc_zone's pointer members starting at bit 0 = x).         */
+uint64_t ostc_zone_required(const ostc_config *cfg, const ostc_param *param);
+
+/* Last error recorded on the context: status, CUDA error code, and the
+ * first failing block/cell when the status is OSTC_ERR_NONPHYSICAL.        */
+ostc_status ostc_get_error(const ostc_ctx *ctx, int *cuda_error, int *block,
+                           int *i, int *j, int *k);
+
+/* ----------------------------------------------------------------------- */
+/* operator API: one call per reference operator of the RK3 stage         */
+/* ----------------------------------------------------------------------- */
+
+/* compute_cv_from_bv<mix,turb> over [-ngg, m+ngg) (src/FieldOperation.cuh:43-79). */
+ostc_status ostc_compute_cv_from_bv(ostc_ctx *ctx, void *stream);
+
+/* cudaMemset(dq) + compute_source + compute_inviscid_flux +
+ * compute_viscous_flux (src/RK.cuh:303-311): the right-hand side of every
+ * block into dq, in fused sm_100a kernels.                                 */
+ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream);
+
+/* local_time_step (src/TimeAdvanceFunc.cuh:50-100) + global_time_step
+ * (src/TimeAdvanceFunc.cu:155-201) as one fused kernel with an on-device
+ * min; the result stays in device memory (ostc_dt_device) unless dt_host is
+ * non-NULL, in which case this call synchronises the stream.              */
+ostc_status ostc_global_time_step(ostc_ctx *ctx, double *dt_host, void *stream);
+const double *ostc_dt_device(const ostc_ctx *ctx);
+
+/* update_cv_and_bv_rk (src/RK.cuh:392-448) for SSPRK3 stage rk in {0,1,2}.
+ * dt < 0 reads the device dt written by ostc_global_time_step.            */
+ostc_status ostc_update_cv_and_bv_rk(ostc_ctx *ctx, double dt, int rk, void *stream);
+
+/* DBoundCond::apply_boundary_conditions<mix,turb,with_cv> in the reference's
+ * priority order (src/BoundCond.cuh:673-822), plus periodic faces.        */
+ostc_status ostc_apply_boundary_conditions(ostc_ctx *ctx, int with_cv, void *stream);
+
+/* data_communication<mix,turb,with_cv> for same-device 1-to-1 interfaces
+ * (src/DataCommunication.cuh:27-110). A no-op without interfaces.          */
+ostc_status ostc_data_communication(ostc_ctx *ctx, int with_cv, void *stream);
+
+/* update_physical_properties<mix> over [-1, m] (src/FieldOperation.cuh:112-146). */
+ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream);
+
+/* ----------------------------------------------------------------------- */
+/* fused drivers                                                           */
+/* ----------------------------------------------------------------------- */
+
+/* Driver::initialize_computation (src/Driver.cu:39-98) followed by the
+ * pre-loop of RK3_bv (src/RK.cuh:235-244).                                */
+ostc_status ostc_initialize(ostc_ctx *ctx, void *stream);
+
+/* One SSPRK3 stage: RHS, dt (if CFL), update, BCs, interfaces, properties. */
+ostc_status ostc_rk3_stage(ostc_ctx *ctx, int rk, void *stream);
+
+/* n_steps full RK3 steps (the body of the while loop in RK3_bv,
+ * src/RK.cuh:284-357), captured once as a CUDA graph and replayed.
+ * If res_hist is non-NULL it receives 4 doubles per step (the RMS change of
+ * rho, |V|, p, T, src/Residual.cuh:57-161, unnormalised) and dt_hist one dt
+ * per step; both synchronise the stream at the end.                        */
+ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist,
+                           double *dt_hist, void *stream);
+
+/* Metric and Jacobian from grid coordinates that carry ngg+1 ghost layers
+ * (x,y,z as host arrays with ghost count ngg+1), as Block::compute_jac_metric
+ * (src/Mesh.cpp:259-521). Host-only helper: fills host jac (g=ngg) and host
+ * metric (80-byte records, g=ngg). Returns OSTC_ERR_NONPHYSICAL on a
+ * non-positive interior Jacobian.                                           */
+ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg,
+                                  const double *x, const double *y, const double *z,
+                                  double *jac_out, void *metric_out);
+
+/* Tile shape of the flux kernel of direction dir (0 x, 1 y, 2 z): rows of
+ * 32 threads per CTA (1, 2, 4 or 8) and chunks marched per CTA. Set by the
+ * autotuner (openstc-dev_b200/ostc.py: autotune) or by hand; resets graphs. */
+ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks);
+ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks);
+
+/* Library version string. */
+const char *ostc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OSTC_H */

@@ -1,0 +1,613 @@
+// api.cu — the C ABI of include/ostc.h: context, operator entry points,
+// fused RK3 stage and the CUDA-graph step driver.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <type_traits>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace ostc;
+
+#define OSTC_VERSION_STRING "openstc-b200 0.1 (sm_100a)"
+
+struct GraphEntry {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+struct ostc_ctx {
+  ostc_config cfg{};
+  ostc_param prm{};
+  DevParam dp{};
+  int ns = 0;  // compile-time species count selecting the kernel instantiation
+  bool has_source = false;
+  std::vector<ostc_zone> zones;
+  std::vector<DevZone> dz;
+  std::vector<double *> met_soa;
+  std::vector<BcFace> faces;
+  std::vector<int> face_zone;
+  TileShape tile[3] = {{4, 4}, {8, 2}, {8, 2}};
+  unsigned long long *dt_bits = nullptr;  // device dt (as bits)
+  double *res_partial = nullptr;          // [n_part_total][4]
+  int n_part_per_zone = 0;
+  double *hist_res = nullptr, *hist_dt = nullptr;  // device history buffers
+  int *hist_counter = nullptr;
+  int hist_cap = 0;
+  double n_total = 0;
+  std::map<int, GraphEntry> graphs;  // key: with_residual
+  ostc_status last = OSTC_OK;
+  int last_cuda = 0;
+  int err_block = -1, err_i = 0, err_j = 0, err_k = 0;
+};
+
+namespace {
+
+const ostc_ctx *g_uploaded = nullptr;
+
+ostc_status fail(ostc_ctx *c, ostc_status s, cudaError_t e = cudaSuccess) {
+  if (c) {
+    c->last = s;
+    c->last_cuda = (int)e;
+  }
+  return s;
+}
+
+#define CK(expr)                                         \
+  do {                                                   \
+    cudaError_t e_ = (expr);                             \
+    if (e_ != cudaSuccess) return fail(ctx, OSTC_ERR_CUDA, e_); \
+  } while (0)
+
+ostc_status ensure_param(ostc_ctx *ctx, cudaStream_t s) {
+  if (g_uploaded != ctx) {
+    CK(upload_param(ctx->dp, s));
+    g_uploaded = ctx;
+  }
+  return OSTC_OK;
+}
+
+template <typename F>
+cudaError_t dispatch_ns(int ns, F &&f) {
+  switch (ns) {
+    case 0: return f(std::integral_constant<int, 0>{});
+    case 9: return f(std::integral_constant<int, 9>{});
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// repack the reference's 80-byte gxl::Matrix<real,3,3,1> records into 9 planes
+__global__ void repack_metric_kernel(const unsigned char *src, double *dst, long long n) {
+  const long long q = blockIdx.x * 256ll + threadIdx.x;
+  if (q >= n) return;
+  const double *m = (const double *)(src + 80 * q + 8);
+#pragma unroll
+  for (int c = 0; c < 9; ++c) dst[c * n + q] = m[c];
+}
+
+__global__ void step_end_kernel(const double *partial, int n_part, double n_total, const double *dt_dev,
+                                double dt_fixed, double *hist_res, double *hist_dt, int *counter, int cap) {
+  if (threadIdx.x != 0) return;
+  const int s = *counter;
+  if (s < cap) {
+    if (hist_res && partial) {
+      for (int l = 0; l < 4; ++l) {
+        double acc = 0;
+        for (int p = 0; p < n_part; ++p) acc += partial[p * 4 + l];
+        hist_res[s * 4 + l] = sqrt(acc / n_total);
+      }
+    }
+    if (hist_dt) hist_dt[s] = dt_dev ? *dt_dev : dt_fixed;
+  }
+  *counter = s + 1;
+}
+
+void fill_devzone(const ostc_zone &z, DevZone &d) {
+  d.mx = z.mx;
+  d.my = z.my;
+  d.mz = z.mz;
+  d.ngg = z.ngg;
+  auto strides = [&](int g, int &s2, int &s1, int &st, long long &sz) {
+    s2 = z.mx + 2 * g;
+    s1 = (z.my + 2 * g) * s2;
+    st = (s1 + s2 + 1) * g;
+    sz = (long long)(z.mx + 2 * g) * (z.my + 2 * g) * (z.mz + 2 * g);
+  };
+  strides(z.ngg, d.d2, d.d1, d.dt_, d.sz);
+  strides(z.dq_ngg, d.q2, d.q1, d.qt, d.qsz);
+  int dummy;
+  strides(0, d.n2, d.n1, dummy, d.nsz);
+  d.bv = z.bv;
+  d.sv = z.sv;
+  d.cv = z.cv;
+  d.qn = z.qn;
+  d.dq = z.dq;
+  d.vel = z.vel;
+  d.a = z.acoustic_speed;
+  d.mach = z.mach;
+  d.mul = z.mul;
+  d.kappa = z.thermal_conductivity;
+  d.rhoD = z.rho_D;
+  d.gam = z.gamma;
+  d.cp = z.cp;
+  d.mut = z.mut;
+  d.ttc = z.turb_therm_cond;
+  d.wall = z.wall_distance;
+  d.dt_local = z.dt_local;
+  d.bv_last = z.bv_last;
+  d.jac = z.jac;
+}
+
+ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zone *zones, int n_zones,
+                     const ostc_bc_face *faces, int n_faces) {
+  if (!cfg || !p || !zones || n_zones <= 0 || (n_faces > 0 && !faces)) return OSTC_ERR_INVALID_ARG;
+  if (p->mix_model == OSTC_MIX_AIR) {
+    if (p->n_spec != 0 || p->n_var != 5 || p->n_scalar != 0) return OSTC_ERR_INVALID_ARG;
+  } else if (p->mix_model == OSTC_MIX_MIXTURE || p->mix_model == OSTC_MIX_FR) {
+    if (p->n_spec != 9) return OSTC_ERR_UNSUPPORTED;
+    if (p->n_var != 5 + p->n_spec || p->n_scalar != p->n_spec) return OSTC_ERR_INVALID_ARG;
+    if (p->mix_model == OSTC_MIX_FR && (p->n_reac < 0 || p->n_reac > OSTC_MAX_REAC)) return OSTC_ERR_INVALID_ARG;
+  } else {
+    return OSTC_ERR_UNSUPPORTED;
+  }
+  if (p->turbulence) return OSTC_ERR_UNSUPPORTED;
+  if (p->inviscid_type == 2) return OSTC_ERR_UNSUPPORTED;  // Roe
+  if (p->inviscid_type == 1 && p->mix_model != OSTC_MIX_AIR) return OSTC_ERR_UNSUPPORTED;  // quirk A2
+  if (p->inviscid_type == 1 && p->reconstruction != 4) return OSTC_ERR_INVALID_ARG;
+  if (p->inviscid_scheme == 1 && p->mix_model != OSTC_MIX_AIR) return OSTC_ERR_UNSUPPORTED;
+  if (p->inviscid_scheme < 1 || p->inviscid_scheme > 4) return OSTC_ERR_INVALID_ARG;
+  if (p->limiter != 0) return OSTC_ERR_INVALID_ARG;
+  if (cfg->steady || cfg->temporal_scheme != 3) return OSTC_ERR_UNSUPPORTED;
+  if (!(p->cfl > 0) && !cfg->fixed_time_step) return OSTC_ERR_INVALID_ARG;
+  const int need_ngg = p->inviscid_type == 1 ? 3 : 2;
+  for (int b = 0; b < n_zones; ++b) {
+    const ostc_zone &z = zones[b];
+    if (z.mx < 2 || z.my < 2 || z.mz < 1 || z.ngg < need_ngg || z.dq_ngg < 0 || z.dq_ngg > 1)
+      return OSTC_ERR_INVALID_ARG;
+    if (z.mz == 1) return OSTC_ERR_UNSUPPORTED;  // 2-D path not built
+    if (!z.bv || !z.cv || !z.qn || !z.dq || !z.jac || !z.metric || !z.vel || !z.acoustic_speed || !z.mach ||
+        !z.mul || !z.thermal_conductivity)
+      return OSTC_ERR_INVALID_ARG;
+    if (p->n_spec > 0 && (!z.sv || !z.rho_D || !z.gamma || !z.cp)) return OSTC_ERR_INVALID_ARG;
+    // int32 ghosted index space
+    const double np = (double)(z.mx + 2 * z.ngg) * (z.my + 2 * z.ngg) * (z.mz + 2 * z.ngg);
+    if (np * std::max(p->n_var, 6) >= 2147483647.0) return OSTC_ERR_INVALID_ARG;
+  }
+  for (int q = 0; q < n_faces; ++q) {
+    const ostc_bc_face &f = faces[q];
+    if (f.block < 0 || f.block >= n_zones || f.face < 0 || f.face > 2 || (f.direction != 1 && f.direction != -1))
+      return OSTC_ERR_INVALID_ARG;
+    const ostc_zone &z = zones[f.block];
+    const int ext[3] = {z.mx, z.my, z.mz};
+    for (int d = 0; d < 3; ++d) {
+      if (f.range_start[d] > f.range_end[d]) return OSTC_ERR_INVALID_ARG;
+      if (d == f.face) {
+        const int want = f.direction < 0 ? 0 : ext[d] - 1;
+        if (f.range_start[d] != want || f.range_end[d] != want) return OSTC_ERR_INVALID_ARG;
+      } else if (f.range_start[d] < -z.ngg || f.range_end[d] > ext[d] - 1 + z.ngg) {
+        return OSTC_ERR_INVALID_ARG;
+      }
+    }
+    switch (f.type_label) {
+      case OSTC_BC_INFLOW:
+      case OSTC_BC_OUTFLOW:
+      case OSTC_BC_SYMMETRY: break;
+      case OSTC_BC_PERIODIC:
+        if (ext[f.face] < z.ngg) return OSTC_ERR_INVALID_ARG;
+        break;
+      default: return OSTC_ERR_UNSUPPORTED;
+    }
+  }
+  return OSTC_OK;
+}
+
+void build_devparam(const ostc_param *p, DevParam &d) {
+  std::memset(&d, 0, sizeof(d));
+  d.n_var = p->n_var;
+  d.n_scalar = p->n_scalar;
+  d.n_spec = p->n_spec;
+  d.n_reac = p->mix_model == OSTC_MIX_FR ? p->n_reac : 0;
+  d.mix = p->mix_model;
+  d.inviscid_scheme = p->inviscid_scheme;
+  d.reconstruction = p->reconstruction;
+  d.limiter = p->limiter;
+  d.inviscid_type = p->inviscid_type;
+  d.viscous_scheme = p->viscous_scheme;
+  d.chemSrcMethod = p->chemSrcMethod;
+  d.gradP = p->gradPInDiffusionFlux;
+  d.dimension = p->dimension;
+  d.turbulence = p->turbulence;
+  d.Pr = p->Pr;
+  d.Prt = p->Prt;
+  d.Sct = p->Sct;
+  d.Sc = p->Sc;
+  d.cfl = p->cfl;
+  d.entropy_fix_factor = p->entropy_fix_factor;
+  const int ns = p->n_spec;
+  for (int i = 0; i < ns; ++i) {
+    d.mw[i] = p->mw[i];
+    d.imw[i] = 1.0 / p->mw[i];
+    d.Rmw[i] = R_u / p->mw[i];
+    for (int c = 0; c < 7; ++c) {
+      d.lo[i][c] = p->low_temp_coeff[i * 7 + c];
+      d.hi[i][c] = p->high_temp_coeff[i * 7 + c];
+    }
+    d.t_low[i] = p->t_low[i];
+    d.t_mid[i] = p->t_mid[i];
+    d.LJ_inv[i] = p->LJ_potent_inv[i];
+    d.vis_coeff[i] = p->vis_coeff[i];
+    for (int j = 0; j < ns; ++j) {
+      d.WjWi4[i][j] = p->WjDivWi_to_One4th[i * ns + j];
+      d.sqWW8[i][j] = p->sqrt_WiDivWjPl1Mul8[i * ns + j];
+      d.bdc[i][j] = p->binary_diffusivity_coeff[i * ns + j];
+      d.kbe[i][j] = p->kb_over_eps_jk[i * ns + j];
+    }
+  }
+  for (int r = 0; r < d.n_reac; ++r) {
+    d.reac_type[r] = p->reac_type[r];
+    d.reac_order[r] = p->reac_order[r];
+    d.A[r] = p->A[r];
+    d.b[r] = p->b[r];
+    d.Ea[r] = p->Ea[r];
+    d.A2[r] = p->A2[r];
+    d.b2[r] = p->b2[r];
+    d.Ea2[r] = p->Ea2[r];
+    d.troe_alpha[r] = p->troe_alpha[r];
+    d.troe_t3[r] = p->troe_t3[r];
+    d.troe_t1[r] = p->troe_t1[r];
+    d.troe_t2[r] = p->troe_t2[r];
+    for (int l = 0; l < ns; ++l) {
+      d.nuf[r][l] = (signed char)p->stoi_f[r * ns + l];
+      d.nub[r][l] = (signed char)p->stoi_b[r * ns + l];
+      d.tb[r][l] = p->third_body_coeff[r * ns + l];
+    }
+    if (d.reac_type[r] != 0 && d.reac_type[r] != 2) d.need_gibbs = 1;
+  }
+}
+
+// default tile shapes: enough CTAs for ~4 per SM, as few re-computed faces as possible
+void default_tiles(ostc_ctx *c) {
+  const DevZone &z = c->dz[0];
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long target = 4ll * sms;
+  // x: rows 4, chunks so a segment spans the line, unless that leaves too few CTAs
+  {
+    int R = 4, C = (z.mx + 1 + 31) / 32;
+    while (C > 1 && (long long)((z.mx + 32 * C - 2) / (32 * C - 1)) * ((z.my + R - 1) / R) * z.mz < target) --C;
+    c->tile[0] = {R, std::max(C, 1)};
+  }
+  for (int d = 1; d < 3; ++d) {
+    const int n = d == 1 ? z.my : z.mz;
+    const int other = d == 1 ? z.mz : z.my;
+    int R = 8, C = (n + 1 + R - 1) / R;
+    while (C > 1 && (long long)((z.mx + 31) / 32) * other * ((n + R * C - 2) / (R * C - 1)) < target) --C;
+    c->tile[d] = {R, std::max(C, 1)};
+  }
+}
+
+cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char *ostc_version(void) { return OSTC_VERSION_STRING; }
+
+uint64_t ostc_zone_required(const ostc_config *cfg, const ostc_param *p) {
+  // bit order = pointer members of ostc_zone starting at x
+  enum { X, Y, Z_, JAC, MET, WALL, CV, BV, SV, BVL, VEL, A, MACH, MUL, KAP, RHOD, GAM, CP, CHEM, MUT, TTC, TSJ,
+         DQ, DQ0, DQK, ISR, VSR, DTL, EFD, QN };
+  uint64_t m = (1ull << JAC) | (1ull << MET) | (1ull << CV) | (1ull << BV) | (1ull << VEL) | (1ull << A) |
+               (1ull << MACH) | (1ull << MUL) | (1ull << KAP) | (1ull << DQ) | (1ull << QN);
+  if (p && p->n_spec > 0) m |= (1ull << SV) | (1ull << RHOD) | (1ull << GAM) | (1ull << CP);
+  if (cfg && cfg->output_screen > 0) m |= (1ull << BVL);
+  return m;
+}
+
+ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const ostc_zone *zones, int n_zones,
+                        const ostc_bc_face *faces, int n_faces, ostc_ctx **out) {
+  if (!out) return OSTC_ERR_INVALID_ARG;
+  *out = nullptr;
+  ostc_status st = validate(cfg, param, zones, n_zones, faces, n_faces);
+  if (st != OSTC_OK) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return OSTC_ERR_NO_DEVICE;
+  std::unique_ptr<ostc_ctx> c(new ostc_ctx);
+  ostc_ctx *ctx = c.get();
+  c->cfg = *cfg;
+  c->prm = *param;
+  build_devparam(param, c->dp);
+  c->ns = param->n_spec;
+  c->has_source = param->mix_model == OSTC_MIX_FR && c->dp.n_reac > 0;
+  c->zones.assign(zones, zones + n_zones);
+  c->dz.resize(n_zones);
+  for (int b = 0; b < n_zones; ++b) {
+    fill_devzone(zones[b], c->dz[b]);
+    c->dz[b].block_id = b;
+    double *soa = nullptr;
+    CK(cudaMalloc(&soa, sizeof(double) * 9 * c->dz[b].sz));
+    c->met_soa.push_back(soa);
+    const long long n = c->dz[b].sz;
+    repack_metric_kernel<<<(unsigned)((n + 255) / 256), 256>>>((const unsigned char *)zones[b].metric, soa, n);
+    CK(cudaGetLastError());
+    c->dz[b].met = soa;
+    c->n_total += (double)zones[b].mx * zones[b].my * zones[b].mz;
+  }
+  for (int q = 0; q < n_faces; ++q) {
+    const ostc_bc_face &f = faces[q];
+    const DevZone &z = c->dz[f.block];
+    BcFace b{};
+    b.type = f.type_label;
+    b.face = f.face;
+    b.direction = f.direction;
+    for (int d = 0; d < 3; ++d) {
+      b.rs[d] = f.range_start[d];
+      b.re[d] = f.range_end[d];
+    }
+    const int unit = f.face == 0 ? 1 : (f.face == 1 ? z.d2 : z.d1);
+    b.dir_stride = f.direction * unit;
+    const int ext[3] = {z.mx, z.my, z.mz};
+    b.period_stride = f.direction * unit * ext[f.face];
+    b.density = f.density;
+    b.u = f.u;
+    b.v = f.v;
+    b.w = f.w;
+    b.pressure = f.pressure;
+    b.temperature = f.temperature;
+    b.velocity = f.velocity;
+    b.mut = f.mut;
+    for (int l = 0; l < OSTC_MAX_SPEC + 4; ++l) b.sv[l] = f.sv[l];
+    c->faces.push_back(b);
+    c->face_zone.push_back(f.block);
+  }
+  CK(cudaMalloc(&c->dt_bits, sizeof(unsigned long long)));
+  c->n_part_per_zone = 148 * 2;
+  CK(cudaMalloc(&c->res_partial, sizeof(double) * 4 * c->n_part_per_zone * n_zones));
+  CK(cudaMalloc(&c->hist_counter, sizeof(int)));
+  CK(cudaDeviceSynchronize());
+  default_tiles(ctx);
+  *out = c.release();
+  return OSTC_OK;
+}
+
+ostc_status ostc_destroy(ostc_ctx *ctx) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  cudaDeviceSynchronize();
+  for (auto &kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  for (double *p : ctx->met_soa) cudaFree(p);
+  cudaFree(ctx->dt_bits);
+  cudaFree(ctx->res_partial);
+  cudaFree(ctx->hist_counter);
+  cudaFree(ctx->hist_res);
+  cudaFree(ctx->hist_dt);
+  if (g_uploaded == ctx) g_uploaded = nullptr;
+  delete ctx;
+  return OSTC_OK;
+}
+
+ostc_status ostc_get_error(const ostc_ctx *ctx, int *cuda_error, int *block, int *i, int *j, int *k) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  if (cuda_error) *cuda_error = ctx->last_cuda;
+  if (block) *block = ctx->err_block;
+  if (i) *i = ctx->err_i;
+  if (j) *j = ctx->err_j;
+  if (k) *k = ctx->err_k;
+  return ctx->last;
+}
+
+const double *ostc_dt_device(const ostc_ctx *ctx) { return ctx ? (const double *)ctx->dt_bits : nullptr; }
+
+ostc_status ostc_compute_cv_from_bv(ostc_ctx *ctx, void *stream) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  for (auto &z : ctx->dz)
+    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::CvFromBv, z, {}, S(stream)); }));
+  return OSTC_OK;
+}
+
+ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  const int inv = ctx->prm.inviscid_type;
+  const int vis = ctx->prm.viscous_scheme != 0;
+  for (auto &z : ctx->dz) {
+    if (z.qt != 0) CK(cudaMemsetAsync(z.dq, 0, sizeof(double) * z.qsz * ctx->prm.n_var, S(stream)));
+    bool acc = z.qt != 0;
+    if (ctx->has_source) {
+      CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, {}, S(stream)); }));
+      acc = true;
+    }
+    for (int d = 0; d < (z.mz > 1 ? 3 : 2); ++d) {
+      CK(dispatch_ns(ctx->ns, [&](auto n) {
+        return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], (acc || d > 0) ? 1 : 0, vis, S(stream));
+      }));
+    }
+  }
+  return OSTC_OK;
+}
+
+ostc_status ostc_global_time_step(ostc_ctx *ctx, double *dt_host, void *stream) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  CellArgs a;
+  a.dt_bits = ctx->dt_bits;
+  CK(launch_cells<0>(CellOp::DtReset, ctx->dz[0], a, S(stream)));
+  for (auto &z : ctx->dz)
+    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Dt, z, a, S(stream)); }));
+  if (dt_host) {
+    CK(cudaMemcpyAsync(dt_host, ctx->dt_bits, sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
+    CK(cudaStreamSynchronize(S(stream)));
+  }
+  return OSTC_OK;
+}
+
+ostc_status ostc_update_cv_and_bv_rk(ostc_ctx *ctx, double dt, int rk, void *stream) {
+  if (!ctx || rk < 0 || rk > 2) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  CellArgs a;
+  a.dt = dt;
+  a.dt_dev = dt < 0 ? (const double *)ctx->dt_bits : nullptr;
+  a.rk = rk;
+  for (auto &z : ctx->dz)
+    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::UpdateRK, z, a, S(stream)); }));
+  return OSTC_OK;
+}
+
+ostc_status ostc_apply_boundary_conditions(ostc_ctx *ctx, int with_cv, void *stream) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  // priority order of BoundCond.cuh:673-822; periodic wraps after all others
+  static const int order[] = {OSTC_BC_FARFIELD, OSTC_BC_OUTFLOW, OSTC_BC_BACK_PRESSURE, OSTC_BC_INFLOW,
+                              OSTC_BC_SUBSONIC_INFLOW, OSTC_BC_SYMMETRY, OSTC_BC_WALL, OSTC_BC_PERIODIC};
+  for (int t : order) {
+    for (size_t q = 0; q < ctx->faces.size(); ++q) {
+      if (ctx->faces[q].type != t) continue;
+      const DevZone &z = ctx->dz[ctx->face_zone[q]];
+      CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_bc<decltype(n)::value>(z, ctx->faces[q], with_cv, S(stream)); }));
+    }
+  }
+  return OSTC_OK;
+}
+
+ostc_status ostc_data_communication(ostc_ctx *ctx, int with_cv, void *stream) {
+  (void)with_cv;
+  (void)stream;
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  return OSTC_OK;  // no 1-to-1 interfaces in a context built from single blocks
+}
+
+ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  for (auto &z : ctx->dz)
+    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Properties, z, {}, S(stream)); }));
+  return OSTC_OK;
+}
+
+ostc_status ostc_initialize(ostc_ctx *ctx, void *stream) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  ostc_status st;
+  if ((st = ostc_apply_boundary_conditions(ctx, 0, stream))) return st;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  for (auto &z : ctx->dz)
+    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Velocity, z, {}, S(stream)); }));
+  if ((st = ostc_data_communication(ctx, 0, stream))) return st;
+  if ((st = ostc_update_physical_properties(ctx, stream))) return st;
+  return ostc_compute_cv_from_bv(ctx, stream);
+}
+
+ostc_status ostc_rk3_stage(ostc_ctx *ctx, int rk, void *stream) {
+  if (!ctx || rk < 0 || rk > 2) return OSTC_ERR_INVALID_ARG;
+  ostc_status st;
+  if ((st = ostc_compute_rhs(ctx, stream))) return st;
+  double dt = ctx->cfg.dt;
+  if (!ctx->cfg.fixed_time_step) {
+    if ((st = ostc_global_time_step(ctx, nullptr, stream))) return st;
+    dt = -1;
+  }
+  if ((st = ostc_update_cv_and_bv_rk(ctx, dt, rk, stream))) return st;
+  if ((st = ostc_apply_boundary_conditions(ctx, 1, stream))) return st;
+  if ((st = ostc_data_communication(ctx, 1, stream))) return st;
+  return ostc_update_physical_properties(ctx, stream);
+}
+
+// one full step as enqueued work (captured into a graph by ostc_rk3_steps)
+static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
+  ostc_status st;
+  if (with_hist)
+    for (auto &z : ctx->dz) CK(launch_cells<0>(CellOp::StoreLast, z, {}, s));
+  for (auto &z : ctx->dz)
+    CK(cudaMemcpyAsync(z.qn, z.cv, sizeof(double) * z.sz * ctx->prm.n_var, cudaMemcpyDeviceToDevice, s));
+  for (int rk = 0; rk < 3; ++rk)
+    if ((st = ostc_rk3_stage(ctx, rk, s))) return st;
+  if (with_hist) {
+    CellArgs a;
+    a.n_part = ctx->n_part_per_zone;
+    for (size_t b = 0; b < ctx->dz.size(); ++b) {
+      a.partial = ctx->res_partial + 4 * ctx->n_part_per_zone * b;
+      CK(launch_cells<0>(CellOp::ResidualPartial, ctx->dz[b], a, s));
+    }
+    step_end_kernel<<<1, 32, 0, s>>>(ctx->res_partial, ctx->n_part_per_zone * (int)ctx->dz.size(), ctx->n_total,
+                                     ctx->cfg.fixed_time_step ? nullptr : (const double *)ctx->dt_bits, ctx->cfg.dt,
+                                     ctx->hist_res, ctx->hist_dt, ctx->hist_counter, ctx->hist_cap);
+    CK(cudaGetLastError());
+  }
+  return OSTC_OK;
+}
+
+ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist, double *dt_hist, void *stream) {
+  if (!ctx || n_steps < 0) return OSTC_ERR_INVALID_ARG;
+  cudaStream_t s = S(stream);
+  const bool hist = res_hist || dt_hist;
+  if (hist && n_steps > ctx->hist_cap) {
+    cudaFree(ctx->hist_res);
+    cudaFree(ctx->hist_dt);
+    ctx->hist_res = ctx->hist_dt = nullptr;
+    CK(cudaMalloc(&ctx->hist_res, sizeof(double) * 4 * n_steps));
+    CK(cudaMalloc(&ctx->hist_dt, sizeof(double) * n_steps));
+    ctx->hist_cap = n_steps;
+    // cached graphs captured the old buffers
+    for (auto &kv : ctx->graphs) {
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+      if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    ctx->graphs.clear();
+  }
+  if (ensure_param(ctx, s)) return ctx->last;
+  if (hist) CK(cudaMemsetAsync(ctx->hist_counter, 0, sizeof(int), s));
+  GraphEntry &ge = ctx->graphs[hist ? 1 : 0];
+  if (!ge.exec) {
+    // a legacy default stream cannot be captured: capture on a private stream
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    ostc_status st = enqueue_step(ctx, hist, cs);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (st) return st;
+    CK(e);
+    CK(cudaGraphInstantiate(&ge.exec, g, 0));
+    ge.graph = g;
+  }
+  for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(ge.exec, s));
+  if (hist) {
+    if (res_hist) CK(cudaMemcpyAsync(res_hist, ctx->hist_res, sizeof(double) * 4 * n_steps, cudaMemcpyDeviceToHost, s));
+    if (dt_hist) CK(cudaMemcpyAsync(dt_hist, ctx->hist_dt, sizeof(double) * n_steps, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  return OSTC_OK;
+}
+
+// tile-shape control for the autotuner: dir 0..2
+ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
+  if (!ctx || dir < 0 || dir > 2 || chunks < 1 || chunks > 64) return OSTC_ERR_INVALID_ARG;
+  if (!(rows == 1 || rows == 2 || rows == 4 || rows == 8)) return OSTC_ERR_INVALID_ARG;
+  ctx->tile[dir] = {rows, chunks};
+  for (auto &kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  ctx->graphs.clear();
+  return OSTC_OK;
+}
+
+ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks) {
+  if (!ctx || dir < 0 || dir > 2 || !rows || !chunks) return OSTC_ERR_INVALID_ARG;
+  *rows = ctx->tile[dir].rows;
+  *chunks = ctx->tile[dir].chunks;
+  return OSTC_OK;
+}
+
+}  // extern "C"

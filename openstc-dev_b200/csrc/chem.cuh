@@ -1,0 +1,171 @@
+// chem.cuh — finite-rate chemistry source and mixture transport properties.
+//
+// Chemistry follows src/FiniteRateChem.cu:7-194 (forward rates with
+// duplicate / third-body / Lindemann / Troe forms, backward rates from the
+// Gibbs energy, rates of progress, species source). Stoichiometric
+// coefficients sit in __constant__ memory; zero coefficients are skipped
+// (multiplying by pow(c,0) = 1 or adding 0 is exact) and c^nu uses exact
+// small-integer powers. Transport follows
+// src/Transport.cu:40-109 (Wilke viscosity, the 1.065/0.065 conductivity
+// rule, mixture-averaged rho*D_k).
+#pragma once
+#include "common.cuh"
+#include "thermo.cuh"
+
+namespace ostc {
+
+__device__ __forceinline__ double ipow(double c, int n) {
+  switch (n) {
+    case 0: return 1.0;
+    case 1: return c;
+    case 2: return c * c;
+    case 3: return c * c * c;
+    default: return pow(c, (double)n);
+  }
+}
+
+__device__ __forceinline__ double arrhenius(double t, double A, double b, double Ea) {
+  return A * pow(t, b) * exp(-Ea / t);
+}
+
+// omega[NS] in kg/(m^3 s) at density rho, temperature t, mass fractions Y
+template <int NS>
+__device__ __forceinline__ void chemistry_omega(double rho, double t, const double *Y, double *omega) {
+  double c[NS];
+#pragma unroll
+  for (int l = 0; l < NS; ++l) c[l] = rho * Y[l] / c_p.mw[l] * 1e-3;
+  double g[NS];
+  if (c_p.need_gibbs) gibbs_div_rt<NS>(t, g);
+  constexpr double temp_p = p_atm / R_u * 1e-3;
+  const double temp_t = temp_p / t;
+  double cre[NS], des[NS];
+#pragma unroll
+  for (int l = 0; l < NS; ++l) {
+    cre[l] = 0;
+    des[l] = 0;
+  }
+  const int nr = c_p.n_reac;
+  for (int r = 0; r < nr; ++r) {
+    const int type = c_p.reac_type[r];
+    double kf = arrhenius(t, c_p.A[r], c_p.b[r], c_p.Ea[r]);
+    if (type == 3) kf += arrhenius(t, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
+    if (type > 3) {
+      double cc = 0;
+#pragma unroll
+      for (int l = 0; l < NS; ++l) cc += c[l] * c_p.tb[r][l];
+      if (type == 4) {
+        kf *= cc;
+      } else {
+        const double kf_low = arrhenius(t, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
+        const double kf_high = kf;
+        const double pr = kf_low * cc / kf_high;
+        double F = 1.0;
+        if (type > 5) {
+          double f_cent = (1 - c_p.troe_alpha[r]) * exp(-t / c_p.troe_t3[r]) + c_p.troe_alpha[r] * exp(-t / c_p.troe_t1[r]);
+          if (type == 7) f_cent += exp(-c_p.troe_t2[r] / t);
+          const double logFc = log10(f_cent);
+          const double cc2 = -0.4 - 0.67 * logFc;
+          const double nn = 0.75 - 1.27 * logFc;
+          const double logPr = log10(pr);
+          const double tempo = (logPr + cc2) / (nn - 0.14 * (logPr + cc2));
+          const double pp = logFc / (1.0 + tempo * tempo);
+          F = pow(10.0, pp);
+        }
+        kf = kf_high * pr / (1.0 + pr) * F;
+      }
+    }
+    double kb = 0;
+    if (type == 2) {
+      kb = arrhenius(t, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
+    } else if (type != 0) {
+      double dg = 0;
+#pragma unroll
+      for (int l = 0; l < NS; ++l) dg += g[l] * (c_p.nub[r][l] - c_p.nuf[r][l]);
+      const double kc = pow(temp_t, (double)c_p.reac_order[r]) * exp(-dg);
+      kb = kf / kc;
+    }
+    // rates of progress: species in increasing order, as the reference's loop
+    double q1 = 1.0, q2 = 1.0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      const int nf = c_p.nuf[r][l], nb = c_p.nub[r][l];
+      if (nf) q1 *= ipow(c[l], nf);
+      if (nb && type != 0) q2 *= ipow(c[l], nb);
+    }
+    q1 *= kf;
+    if (type != 0) q2 *= kb; else q2 = 0.0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      const int nf = c_p.nuf[r][l], nb = c_p.nub[r][l];
+      if (nf | nb) {
+        cre[l] += q2 * nf + q1 * nb;
+        des[l] += q1 * nf + q2 * nb;
+      }
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < NS; ++l) omega[l] = cre[l] * (c_p.mw[l] * 1e+3) - des[l] * (c_p.mw[l] * 1e+3);
+}
+
+// mixture transport at one state (Transport.cu:40-109)
+template <int NS>
+__device__ __forceinline__ void mixture_transport(double T, double mw_total, const double *Y, const double *cp,
+                                                  double rho, double p, double &mu, double &kappa, double *rhoD) {
+  double X[NS], vis[NS];
+  const double sqT = sqrt(T);
+#pragma unroll
+  for (int l = 0; l < NS; ++l) {
+    X[l] = Y[l] * mw_total / c_p.mw[l];
+    const double t_dl = T * c_p.LJ_inv[l];
+    const double ci = 1.147 * pow(t_dl, -0.145) + pow(t_dl + 0.5, -2.0);
+    vis[l] = c_p.vis_coeff[l] * sqT / ci;
+  }
+  double viscosity = 0, conductivity = 0;
+#pragma unroll
+  for (int m = 0; m < NS; ++m) {
+    double vt = 0;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      double pf = 1.0;
+      if (m != n) {
+        const double num = 1 + sqrt(vis[m] / vis[n]) * c_p.WjWi4[m][n];
+        pf = num * num * c_p.sqWW8[m][n];
+      }
+      vt += pf * X[n];
+    }
+    const double ct = 1.065 * vt - 0.065 * X[m];
+    viscosity += vis[m] * X[m] / vt;
+    const double lambda = vis[m] * (cp[m] + 1.25 * c_p.Rmw[m]);
+    conductivity += lambda * X[m] / ct;
+  }
+  mu = viscosity;
+  kappa = conductivity;
+  const double t32p = T * sqT / p;
+  double dinv[NS][NS];
+#pragma unroll
+  for (int m = 0; m < NS; ++m) {
+#pragma unroll
+    for (int n = m + 1; n < NS; ++n) {
+      const double t_red = T * c_p.kbe[m][n];
+      const double od = 1.0 / pow(t_red, 0.145) + 1.0 / ((t_red + 0.5) * (t_red + 0.5));
+      const double d = c_p.bdc[m][n] * t32p / od;
+      dinv[m][n] = d;
+      dinv[n][m] = d;
+    }
+  }
+  constexpr double eps = 1e-12;
+#pragma unroll
+  for (int l = 0; l < NS; ++l) {
+    double num = 0, den = 0;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      if (l != n) {
+        num += (X[n] + eps) * c_p.mw[n];
+        den += (X[n] + eps) / dinv[l][n];
+      }
+    }
+    rhoD[l] = rho * num / (den * mw_total);
+  }
+}
+
+}  // namespace ostc

@@ -1,0 +1,557 @@
+// face.cuh — per-face inviscid and viscous fluxes and the per-cell AWENO
+// central correction, as device functions of one thread.
+//
+// A face of direction DIR lies between the cell at ghosted index gi and the
+// cell at gi + sd (sd = the stride along DIR). All inputs are read straight
+// from the ColMajor planes through the read-only path; threads of a warp
+// always differ in i, so every load is a coalesced 32-wide row.
+#pragma once
+#include "common.cuh"
+#include "thermo.cuh"
+
+namespace ostc {
+
+template <int DIR>
+__device__ __forceinline__ int dir_stride(const DevZone &z) {
+  return DIR == 0 ? 1 : (DIR == 1 ? z.d2 : z.d1);
+}
+
+__device__ __forceinline__ double bvl(const DevZone &z, int g, int l) { return ld(z.bv + l * z.sz + g); }
+__device__ __forceinline__ double svl(const DevZone &z, int g, int l) { return ld(z.sv + l * z.sz + g); }
+__device__ __forceinline__ double cvl(const DevZone &z, int g, int l) { return ld(z.cv + l * z.sz + g); }
+__device__ __forceinline__ double met(const DevZone &z, int g, int c) { return ld(z.met + c * z.sz + g); }
+
+__device__ __forceinline__ int sgn(double a) { return a < 0 ? -1 : 1; }
+__device__ __forceinline__ double minmod(double a, double b) {  // Limiter.cuh:13-16
+  return 0.5 * (sgn(a) + sgn(b)) * fmin(fabs(a), fabs(b));
+}
+
+// ---------------------------------------------------------------------------
+// Riemann solvers on reconstructed states (pl/pr: NV primitive values, then
+// total energy at NV and gamma at NV+1). Output: NV face fluxes.
+// ---------------------------------------------------------------------------
+// AUSM+ (AusmP.cu:6-94); k1..k3: jac-weighted face metric
+template <int NV, bool MIXG>
+__device__ __forceinline__ void ausm_plus(const double *pl, const double *pr, double k1, double k2, double k3,
+                                          double *F) {
+  const double gk = sqrt(k1 * k1 + k2 * k2 + k3 * k3);
+  const double ul = (k1 * pl[1] + k2 * pl[2] + k3 * pl[3]) / gk;
+  const double ur = (k1 * pr[1] + k2 * pr[2] + k3 * pr[3]) / gk;
+  const double gl = MIXG ? pl[NV + 1] : gamma_air, gr = MIXG ? pr[NV + 1] : gamma_air;
+  const double c = 0.5 * (sqrt(gl * pl[4] / pl[0]) + sqrt(gr * pr[4] / pr[0]));
+  const double mlm = ul / c, mrm = ur / c;
+  double mlp, mrn, plp, prn;
+  constexpr double alpha = 3 / 16.0;
+  if (fabs(mlm) > 1) {
+    mlp = 0.5 * (mlm + fabs(mlm));
+    plp = mlp / mlm;
+  } else {
+    const double a = (mlm + 1) * (mlm + 1) * 0.25;
+    const double b = (mlm * mlm - 1) * (mlm * mlm - 1);
+    mlp = a + 0.125 * b;
+    plp = a * (2 - mlm) + alpha * mlm * b;
+  }
+  if (fabs(mrm) > 1) {
+    mrn = 0.5 * (mrm - fabs(mrm));
+    prn = mrn / mrm;
+  } else {
+    const double a = (mrm - 1) * (mrm - 1) * 0.25;
+    const double b = (mrm * mrm - 1) * (mrm * mrm - 1);
+    mrn = -a - 0.125 * b;
+    prn = a * (2 + mrm) - alpha * mrm * b;
+  }
+  const double pc = plp * pl[4] + prn * pr[4];
+  const double mh = mlp + mrn;
+  const double mass = c * (pl[0] * 0.5 * (mh + fabs(mh)) + pr[0] * 0.5 * (mh - fabs(mh)));
+  const double co = mass * gk;
+  const bool left = mass >= 0;
+  const double q0 = left ? pl[0] : pr[0], q1 = left ? pl[1] : pr[1], q2 = left ? pl[2] : pr[2];
+  const double q3 = left ? pl[3] : pr[3], q4 = left ? pl[4] : pr[4], qe = left ? pl[NV] : pr[NV];
+  F[0] = co;
+  F[1] = co * q1 + pc * k1;
+  F[2] = co * q2 + pc * k2;
+  F[3] = co * q3 + pc * k3;
+  F[4] = co * (qe + q4) / q0;
+#pragma unroll
+  for (int l = 5; l < NV; ++l) F[l] = co * (left ? pl[l] : pr[l]);
+}
+
+// HLLC (HLLC.cu:10-143); kx..kz: face-averaged metric, jac_ave: face Jacobian
+template <int NV, int NS>
+__device__ __forceinline__ void hllc(const double *pl, const double *pr, double kx, double ky, double kz,
+                                     double jac_ave, double *F) {
+  const double sl0 = sqrt(pl[0]), sr0 = sqrt(pr[0]);
+  const double rlc = sl0 / (sl0 + sr0), rrc = sr0 / (sl0 + sr0);
+  const double ut = pl[1] * rlc + pr[1] * rrc;
+  const double vt = pl[2] * rlc + pr[2] * rrc;
+  const double wt = pl[3] * rlc + pr[3] * rrc;
+  const double hl = (pl[NV] + pl[4]) / pl[0], hr = (pr[NV] + pr[4]) / pr[0];
+  const double ht = hl * rlc + hr * rrc;
+  const double ekt = 0.5 * (ut * ut + vt * vt + wt * wt);
+  double c_tilde;
+  if constexpr (NS == 0) {
+    c_tilde = sqrt((gamma_air - 1) * (ht - ekt));
+  } else {
+    double svm[NS], mw_inv = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      svm[l] = rlc * pl[l + 5] + rrc * pr[l + 5];
+      mw_inv += svm[l] / c_p.mw[l];
+    }
+    const double t = (rlc * (pl[4] / pl[0]) + rrc * (pr[4] / pr[0])) / (R_u * mw_inv);
+    double h_i[NS], cp_i[NS];
+    enthalpy_cp<NS>(t, h_i, cp_i);
+    double cvv = 0, cpp = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      cpp += cp_i[l] * svm[l];
+      cvv += svm[l] * (cp_i[l] - c_p.Rmw[l]);
+    }
+    c_tilde = sqrt(cpp / cvv * R_u * mw_inv * t);
+  }
+  const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
+  const double Ub = (kx * ut + ky * vt + kz * wt) / gradK;
+  const double gl = NS > 0 ? pl[NV + 1] : gamma_air, gr = NS > 0 ? pr[NV + 1] : gamma_air;
+  const double Ul = kx * pl[1] + ky * pl[2] + kz * pl[3];
+  const double cl = sqrt(gl * pl[4] / pl[0]);
+  const double sl = fmin(Ul / gradK - cl, Ub - c_tilde);
+  const double Ur = kx * pr[1] + ky * pr[2] + kz * pr[3];
+  const double cr = sqrt(gr * pr[4] / pr[0]);
+  const double sr = fmax(Ur / gradK + cr, Ub + c_tilde);
+  if (sl >= 0 || sr < 0) {
+    const double *q = sl >= 0 ? pl : pr;
+    const double U = sl >= 0 ? Ul : Ur;
+    const double rhoUk = q[0] * U;
+    F[0] = jac_ave * rhoUk;
+    F[1] = jac_ave * (rhoUk * q[1] + q[4] * kx);
+    F[2] = jac_ave * (rhoUk * q[2] + q[4] * ky);
+    F[3] = jac_ave * (rhoUk * q[3] + q[4] * kz);
+    F[4] = jac_ave * ((q[NV] + q[4]) * U);
+#pragma unroll
+    for (int l = 5; l < NV; ++l) F[l] = jac_ave * rhoUk * q[l];
+    return;
+  }
+  const double sm = ((pr[0] * Ur * (sr - Ur / gradK) - pl[0] * Ul * (sl - Ul / gradK)) / gradK + pl[4] - pr[4]) /
+                    (pr[0] * (sr - Ur / gradK) - pl[0] * (sl - Ul / gradK));
+  const double pm = pl[0] * (sl - Ul / gradK) * (sm - Ul / gradK) + pl[4];
+  const bool lft = sm >= 0;
+  const double *q = lft ? pl : pr;
+  const double s = lft ? sl : sr, U = lft ? Ul : Ur;
+  const double pC = 1.0 / (s - sm);
+  const double Q = jac_ave * pC * sm * (s * gradK - U) * q[0];
+  F[0] = Q;
+  const double dP = (s * pm - sm * q[4]) * pC * jac_ave;
+  F[1] = Q * q[1] + dP * kx;
+  F[2] = Q * q[2] + dP * ky;
+  F[3] = Q * q[3] + dP * kz;
+  F[4] = Q * q[NV] / q[0] + pC * jac_ave * (s * pm * sm * gradK - sm * q[4] * U);
+#pragma unroll
+  for (int l = 5; l < NV; ++l) F[l] = Q * q[l];
+}
+
+// Lax-Friedrichs, air only (LaxFriedrichs.cu:13-49)
+template <int NV>
+__device__ __forceinline__ void lax_friedrichs(const double *pl, const double *pr, double kx, double ky, double kz,
+                                               double jac_ave, double *F) {
+  const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
+  const double Ukl = pl[1] * kx + pl[2] * ky + pl[3] * kz;
+  const double Ukr = pr[1] * kx + pr[2] * ky + pr[3] * kz;
+  const double cl = sqrt(gamma_air * pl[4] / pl[0]), cr = sqrt(gamma_air * pr[4] / pr[0]);
+  const double sr = fmax(fabs(Ukl) + cl * gradK, fabs(Ukr) + cr * gradK);
+  const double hj = 0.5 * jac_ave;
+  const double rUl = pl[0] * Ukl, rUr = pr[0] * Ukr;
+  F[0] = (rUl + rUr - sr * (pr[0] - pl[0])) * hj;
+  F[1] = (rUl * pl[1] + rUr * pr[1] + kx * (pl[4] + pr[4]) - sr * (pr[1] * pr[0] - pl[1] * pl[0])) * hj;
+  F[2] = (rUl * pl[2] + rUr * pr[2] + ky * (pl[4] + pr[4]) - sr * (pr[2] * pr[0] - pl[2] * pl[0])) * hj;
+  F[3] = (rUl * pl[3] + rUr * pr[3] + kz * (pl[4] + pr[4]) - sr * (pr[3] * pr[0] - pl[3] * pl[0])) * hj;
+  F[4] = ((pl[NV] + pl[4]) * Ukl + (pr[NV] + pr[4]) * Ukr - sr * (pr[NV] - pl[NV])) * hj;
+}
+
+// dispatch on the inviscid_scheme tag (InviscidScheme.cu:137-150; Roe -> AUSM+, quirk A1)
+template <int NV, int NS>
+__device__ __forceinline__ void riemann(const double *pl, const double *pr, const DevZone &z, int g0, int g1,
+                                        int DIR, double *F) {
+  const double j0 = ld(z.jac + g0), j1 = ld(z.jac + g1);
+  const double m0x = met(z, g0, 3 * DIR), m0y = met(z, g0, 3 * DIR + 1), m0z = met(z, g0, 3 * DIR + 2);
+  const double m1x = met(z, g1, 3 * DIR), m1y = met(z, g1, 3 * DIR + 1), m1z = met(z, g1, 3 * DIR + 2);
+  const int sch = c_p.inviscid_scheme;
+  if (sch == 4) {
+    hllc<NV, NS>(pl, pr, 0.5 * (m0x + m1x), 0.5 * (m0y + m1y), 0.5 * (m0z + m1z), 0.5 * (j0 + j1), F);
+  } else if (sch == 1 && NS == 0) {
+    lax_friedrichs<NV>(pl, pr, 0.5 * (m0x + m1x), 0.5 * (m0y + m1y), 0.5 * (m0z + m1z), 0.5 * (j0 + j1), F);
+  } else {
+    ausm_plus<NV, (NS > 0)>(pl, pr, 0.5 * (j0 * m0x + j1 * m1x), 0.5 * (j0 * m0y + j1 * m1y),
+                            0.5 * (j0 * m0z + j1 * m1z), F);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// primitive-variable reconstruction face (InviscidScheme.cu:48-158 +
+// Reconstruction.cu:5-46 + Reconstruction.cuh:20-72)
+// ---------------------------------------------------------------------------
+template <int NS, int DIR>
+__device__ __forceinline__ void inviscid_face_pv(const DevZone &z, int g0, double *F) {
+  constexpr int NV = 5 + NS;
+  const int sd = dir_stride<DIR>(z);
+  double pl[NV + 2], pr[NV + 2];
+  const int rec = c_p.reconstruction;
+#pragma unroll
+  for (int l = 0; l < NV; ++l) {
+    const double *base = l < 5 ? z.bv + l * z.sz : z.sv + (l - 5) * z.sz;
+    const double v0 = ld(base + g0), v1 = ld(base + g0 + sd);
+    if (rec == 2 || rec == 3) {
+      const double vm = ld(base + g0 - sd), v2 = ld(base + g0 + 2 * sd);
+      const double di = v0 - vm, di1 = v1 - v0, di2 = v2 - v1;
+      if (rec == 2) {
+        constexpr double kappa = 1.0 / 3.0;
+        pl[l] = v0 + 0.25 * ((1 - kappa) * minmod(di, di1) + (1 + kappa) * minmod(di1, di));
+        pr[l] = v1 - 0.25 * ((1 - kappa) * minmod(di2, di1) + (1 + kappa) * minmod(di1, di2));
+      } else {
+        pl[l] = v0 + 0.5 * minmod(di, di1);
+        pr[l] = v1 - 0.5 * minmod(di1, di2);
+      }
+    } else {
+      pl[l] = v0;
+      pr[l] = v1;
+    }
+  }
+  if constexpr (NS > 0) {
+    double el = 0.5 * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]);
+    double er = 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]);
+    double mwl = 0, mwr = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      mwl += pl[5 + l] / c_p.mw[l];
+      mwr += pr[5 + l] / c_p.mw[l];
+    }
+    const double tl = pl[4] / (pl[0] * R_u * mwl), tr = pr[4] / (pr[0] * R_u * mwr);
+    double cpl = 0, cpr = 0, cvl = 0, cvr = 0;
+    {
+      double h[NS], cp[NS];
+      enthalpy_cp<NS>(tl, h, cp);
+#pragma unroll
+      for (int l = 0; l < NS; ++l) {
+        cpl += cp[l] * pl[l + 5];
+        cvl += pl[l + 5] * (cp[l] - c_p.Rmw[l]);
+        el += h[l] * pl[l + 5];
+      }
+    }
+    {
+      double h[NS], cp[NS];
+      enthalpy_cp<NS>(tr, h, cp);
+#pragma unroll
+      for (int l = 0; l < NS; ++l) {
+        cpr += cp[l] * pr[l + 5];
+        cvr += pr[l + 5] * (cp[l] - c_p.Rmw[l]);
+        er += h[l] * pr[l + 5];
+      }
+    }
+    pl[NV] = pl[0] * el - pl[4];
+    pr[NV] = pr[0] * er - pr[4];
+    pl[NV + 1] = cpl / cvl;
+    pr[NV + 1] = cpr / cvr;
+  } else {
+    pl[NV] = 0.5 * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]) * pl[0] + pl[4] / (gamma_air - 1);
+    pr[NV] = 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]) * pr[0] + pr[4] / (gamma_air - 1);
+    pl[NV + 1] = gamma_air;
+    pr[NV + 1] = gamma_air;
+  }
+  riemann<NV, NS>(pl, pr, z, g0, g0 + sd, DIR, F);
+}
+
+// ---------------------------------------------------------------------------
+// AWENO-5 characteristic face, air only (AWENO.cu:17-206). The characteristic
+// rows are processed one at a time so that only one row of the left
+// eigenvector matrix is live.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void weno5_pair(const double v[6], double &vminus, double &vplus) {
+  constexpr double t13 = 13.0 / 12, eps = 1e-6, d0 = 1.0 / 16, d1 = 5.0 / 8, d2 = 5.0 / 16;
+  double v0 = 0.125 * (3 * v[0] - 10 * v[1] + 15 * v[2]);
+  double v1 = 0.125 * (-v[1] + 6 * v[2] + 3 * v[3]);
+  double v2 = 0.125 * (3 * v[2] + 6 * v[3] - v[4]);
+  double b0 = t13 * (v[0] + v[2] - 2 * v[1]) * (v[0] + v[2] - 2 * v[1]) +
+              0.25 * (v[0] + 3 * v[2] - 4 * v[1]) * (v[0] + 3 * v[2] - 4 * v[1]);
+  double b1 = t13 * (v[1] + v[3] - 2 * v[2]) * (v[1] + v[3] - 2 * v[2]) + 0.25 * (v[3] - v[1]) * (v[3] - v[1]);
+  double b2 = t13 * (v[2] + v[4] - 2 * v[3]) * (v[2] + v[4] - 2 * v[3]) +
+              0.25 * (3 * v[2] + v[4] - 4 * v[3]) * (3 * v[2] + v[4] - 4 * v[3]);
+  double tau = (b0 - b2) * (b0 - b2);
+  double a0 = d0 + d0 * tau / ((eps + b0) * (eps + b0));
+  double a1 = d1 + d1 * tau / ((eps + b1) * (eps + b1));
+  double a2 = d2 + d2 * tau / ((eps + b2) * (eps + b2));
+  vminus = (a0 * v0 + a1 * v1 + a2 * v2) / (a0 + a1 + a2);
+  v0 = v1;
+  v1 = v2;
+  v2 = 0.125 * (15 * v[3] - 10 * v[4] + 3 * v[5]);
+  b0 = t13 * (v[1] + v[3] - 2 * v[2]) * (v[1] + v[3] - 2 * v[2]) +
+       0.25 * (v[1] + 3 * v[3] - 4 * v[2]) * (v[1] + 3 * v[3] - 4 * v[2]);
+  b1 = t13 * (v[2] + v[4] - 2 * v[3]) * (v[2] + v[4] - 2 * v[3]) + 0.25 * (v[4] - v[2]) * (v[4] - v[2]);
+  b2 = t13 * (v[3] + v[5] - 2 * v[4]) * (v[3] + v[5] - 2 * v[4]) +
+       0.25 * (3 * v[3] + v[5] - 4 * v[4]) * (3 * v[3] + v[5] - 4 * v[4]);
+  tau = (b0 - b2) * (b0 - b2);
+  a0 = d2 + d2 * tau / ((eps + b0) * (eps + b0));
+  a1 = d1 + d1 * tau / ((eps + b1) * (eps + b1));
+  a2 = d0 + d0 * tau / ((eps + b2) * (eps + b2));
+  vplus = (a0 * v0 + a1 * v1 + a2 * v2) / (a0 + a1 + a2);
+}
+
+template <int DIR>
+__device__ __forceinline__ void inviscid_face_aweno(const DevZone &z, int g0, double *F) {
+  constexpr double gm1 = gamma_air - 1;
+  const int sd = dir_stride<DIR>(z);
+  double U[6][5];
+#pragma unroll
+  for (int s = 0; s < 6; ++s)
+#pragma unroll
+    for (int l = 0; l < 5; ++l) U[s][l] = cvl(z, g0 + (s - 2) * sd, l);
+  const double pL = bvl(z, g0, 4), pR = bvl(z, g0 + sd, 4);
+  const double *cl = U[2], *cr = U[3];
+  const double sl0 = sqrt(cl[0]), sr0 = sqrt(cr[0]);
+  const double rlc = sl0 / (sl0 + sr0), rrc = sr0 / (sl0 + sr0);
+  const double um = rlc * cl[1] / cl[0] + rrc * cr[1] / cr[0];
+  const double vm = rlc * cl[2] / cl[0] + rrc * cr[2] / cr[0];
+  const double wm = rlc * cl[3] / cl[0] + rrc * cr[3] / cr[0];
+  const double ekm = 0.5 * (um * um + vm * vm + wm * wm);
+  const double hm = rlc * ((cl[4] + pL) / cl[0]) + rrc * ((cr[4] + pR) / cr[0]);
+  const double cm2 = gm1 * (hm - ekm);
+  const double cm = sqrt(cm2);
+  const int g1 = g0 + sd;
+  double kx = 0.5 * (met(z, g0, 3 * DIR) + met(z, g1, 3 * DIR));
+  double ky = 0.5 * (met(z, g0, 3 * DIR + 1) + met(z, g1, 3 * DIR + 1));
+  double kz = 0.5 * (met(z, g0, 3 * DIR + 2) + met(z, g1, 3 * DIR + 2));
+  const double gK = sqrt(kx * kx + ky * ky + kz * kz);
+  kx /= gK;
+  ky /= gK;
+  kz /= gK;
+  const double Uk = kx * um + ky * vm + kz * wm;
+  const double alpha = gm1 * ekm;
+  double ql[5] = {0, 0, 0, 0, 0}, qr[5] = {0, 0, 0, 0, 0};
+  if (c_p.reconstruction == 4) {
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double L[5];
+      switch (r) {
+        case 0:
+          L[0] = (alpha + Uk * cm) / cm2 * 0.5;
+          L[1] = -(gm1 * um + kx * cm) / cm2 * 0.5;
+          L[2] = -(gm1 * vm + ky * cm) / cm2 * 0.5;
+          L[3] = -(gm1 * wm + kz * cm) / cm2 * 0.5;
+          L[4] = gm1 / cm2 * 0.5;
+          break;
+        case 1:
+          L[0] = kx * (1 - alpha / cm2) - (kz * vm - ky * wm) / cm;
+          L[1] = kx * gm1 * um / cm2;
+          L[2] = (kx * gm1 * vm + kz * cm) / cm2;
+          L[3] = (kx * gm1 * wm - ky * cm) / cm2;
+          L[4] = -kx * gm1 / cm2;
+          break;
+        case 2:
+          L[0] = ky * (1 - alpha / cm2) - (kx * wm - kz * um) / cm;
+          L[1] = (ky * gm1 * um - kz * cm) / cm2;
+          L[2] = ky * gm1 * vm / cm2;
+          L[3] = (ky * gm1 * wm + kx * cm) / cm2;
+          L[4] = -ky * gm1 / cm2;
+          break;
+        case 3:
+          L[0] = kz * (1 - alpha / cm2) - (ky * um - kx * vm) / cm;
+          L[1] = (kz * gm1 * um + ky * cm) / cm2;
+          L[2] = (kz * gm1 * vm - kx * cm) / cm2;
+          L[3] = kz * gm1 * wm / cm2;
+          L[4] = -kz * gm1 / cm2;
+          break;
+        default:
+          L[0] = (alpha - Uk * cm) / cm2 * 0.5;
+          L[1] = -(gm1 * um - kx * cm) / cm2 * 0.5;
+          L[2] = -(gm1 * vm - ky * cm) / cm2 * 0.5;
+          L[3] = -(gm1 * wm - kz * cm) / cm2 * 0.5;
+          L[4] = gm1 / cm2 * 0.5;
+      }
+      double v[6];
+#pragma unroll
+      for (int s = 0; s < 6; ++s) {
+        double acc = 0;
+#pragma unroll
+        for (int j = 0; j < 5; ++j) acc += L[j] * U[s][j];
+        v[s] = acc;
+      }
+      double vmn, vpl;
+      weno5_pair(v, vmn, vpl);
+      // column r of the right eigenvector matrix (AWENO.cu:98-122)
+      double Rc[5];
+      switch (r) {
+        case 0: Rc[0] = 1.0; Rc[1] = um - kx * cm; Rc[2] = vm - ky * cm; Rc[3] = wm - kz * cm; Rc[4] = hm - Uk * cm; break;
+        case 1: Rc[0] = kx; Rc[1] = kx * um; Rc[2] = kx * vm + kz * cm; Rc[3] = kx * wm - ky * cm;
+                Rc[4] = kx * alpha / gm1 + (kz * vm - ky * wm) * cm; break;
+        case 2: Rc[0] = ky; Rc[1] = ky * um - kz * cm; Rc[2] = ky * vm; Rc[3] = ky * wm + kx * cm;
+                Rc[4] = ky * alpha / gm1 + (kx * wm - kz * um) * cm; break;
+        case 3: Rc[0] = kz; Rc[1] = kz * um + ky * cm; Rc[2] = kz * vm - kx * cm; Rc[3] = kz * wm;
+                Rc[4] = kz * alpha / gm1 + (ky * um - kx * vm) * cm; break;
+        default: Rc[0] = 1.0; Rc[1] = um + kx * cm; Rc[2] = vm + ky * cm; Rc[3] = wm + kz * cm; Rc[4] = hm + Uk * cm;
+      }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        ql[m] += Rc[m] * vmn;
+        qr[m] += Rc[m] * vpl;
+      }
+    }
+  }
+  double pl[7], pr[7];
+  pl[0] = ql[0];
+  pl[1] = ql[1] / ql[0];
+  pl[2] = ql[2] / ql[0];
+  pl[3] = ql[3] / ql[0];
+  pl[4] = gm1 * (ql[4] - 0.5 * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]) * ql[0]);
+  pl[5] = ql[4];
+  pl[6] = gamma_air;
+  pr[0] = qr[0];
+  pr[1] = qr[1] / qr[0];
+  pr[2] = qr[2] / qr[0];
+  pr[3] = qr[3] / qr[0];
+  pr[4] = gm1 * (qr[4] - 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]) * qr[0]);
+  pr[5] = qr[4];
+  pr[6] = gamma_air;
+  riemann<5, 0>(pl, pr, z, g0, g1, DIR, F);
+}
+
+// physical flux of the AWENO central correction at one point (AWENO.cu:236-249)
+template <int DIR>
+__device__ __forceinline__ void cds_point_flux(const DevZone &z, int g, double *f) {
+  const double kx = met(z, g, 3 * DIR), ky = met(z, g, 3 * DIR + 1), kz = met(z, g, 3 * DIR + 2);
+  const double jac = ld(z.jac + g);
+  const double u = bvl(z, g, 1), v = bvl(z, g, 2), w = bvl(z, g, 3);
+  const double Uk = kx * u + ky * v + kz * w;
+  const double rUk = bvl(z, g, 0) * Uk;
+  const double p = bvl(z, g, 4);
+  f[0] = rUk * jac;
+  f[1] = jac * (rUk * u + kx * p);
+  f[2] = jac * (rUk * v + ky * p);
+  f[3] = jac * (rUk * w + kz * p);
+  f[4] = jac * Uk * (cvl(z, g, 4) + p);
+}
+
+// sum_m c_m (f(c+m) - f(c-m)), m = 3, 2, 1 (AWENO.cu:257-263)
+template <int DIR>
+__device__ __forceinline__ void cds_correction(const DevZone &z, int g, double *corr) {
+  const int sd = dir_stride<DIR>(z);
+  constexpr double c1 = 19.0 / 3840, c2 = -13.0 / 320, c3 = 17.0 / 256;
+  double fp[5], fm[5], d3[5], d2[5];
+  cds_point_flux<DIR>(z, g + 3 * sd, fp);
+  cds_point_flux<DIR>(z, g - 3 * sd, fm);
+#pragma unroll
+  for (int l = 0; l < 5; ++l) d3[l] = fp[l] - fm[l];
+  cds_point_flux<DIR>(z, g + 2 * sd, fp);
+  cds_point_flux<DIR>(z, g - 2 * sd, fm);
+#pragma unroll
+  for (int l = 0; l < 5; ++l) d2[l] = fp[l] - fm[l];
+  cds_point_flux<DIR>(z, g + sd, fp);
+  cds_point_flux<DIR>(z, g - sd, fm);
+#pragma unroll
+  for (int l = 0; l < 5; ++l) corr[l] = c1 * d3[l] + c2 * d2[l] + c3 * (fp[l] - fm[l]);
+}
+
+// ---------------------------------------------------------------------------
+// laminar viscous face flux (ViscousScheme.cuh:22-821, compute_{f,g,h}v_2nd_order)
+// ---------------------------------------------------------------------------
+template <int NS, int DIR>
+__device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F) {
+  constexpr int NV = 5 + NS;
+  const int sd = dir_stride<DIR>(z);
+  const int g1 = g0 + sd;
+  // tangential strides
+  constexpr int TA = DIR == 0 ? 1 : 0, TB = DIR == 2 ? 1 : 2;
+  const int sa = TA == 0 ? 1 : (TA == 1 ? z.d2 : z.d1);
+  const int sb = TB == 1 ? z.d2 : z.d1;
+  double mm[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) mm[c] = 0.5 * (met(z, g0, c) + met(z, g1, c));
+  // derivative along (normal, ta, tb) ordered as (xi, eta, zeta)
+  auto der = [&](const double *base, double out[3]) {
+    const double dn = ld(base + g1) - ld(base + g0);
+    const double da = 0.25 * (ld(base + g0 + sa) - ld(base + g0 - sa) + ld(base + g1 + sa) - ld(base + g1 - sa));
+    const double db = 0.25 * (ld(base + g0 + sb) - ld(base + g0 - sb) + ld(base + g1 + sb) - ld(base + g1 - sb));
+    out[DIR] = dn;
+    out[TA] = da;
+    out[TB] = db;
+  };
+  double du[3], dv[3], dw[3], dt[3];
+  der(z.bv + 1 * z.sz, du);
+  der(z.bv + 2 * z.sz, dv);
+  der(z.bv + 3 * z.sz, dw);
+  der(z.bv + 5 * z.sz, dt);
+  const double u_x = du[0] * mm[0] + du[1] * mm[3] + du[2] * mm[6];
+  const double u_y = du[0] * mm[1] + du[1] * mm[4] + du[2] * mm[7];
+  const double u_z = du[0] * mm[2] + du[1] * mm[5] + du[2] * mm[8];
+  const double v_x = dv[0] * mm[0] + dv[1] * mm[3] + dv[2] * mm[6];
+  const double v_y = dv[0] * mm[1] + dv[1] * mm[4] + dv[2] * mm[7];
+  const double v_z = dv[0] * mm[2] + dv[1] * mm[5] + dv[2] * mm[8];
+  const double w_x = dw[0] * mm[0] + dw[1] * mm[3] + dw[2] * mm[6];
+  const double w_y = dw[0] * mm[1] + dw[1] * mm[4] + dw[2] * mm[7];
+  const double w_z = dw[0] * mm[2] + dw[1] * mm[5] + dw[2] * mm[8];
+  const double mu = 0.5 * (ld(z.mul + g0) + ld(z.mul + g1));
+  const double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
+  const double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
+  const double tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  const double txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
+  const double j0 = ld(z.jac + g0), j1 = ld(z.jac + g1);
+  const double kxj = 0.5 * (met(z, g0, 3 * DIR) * j0 + met(z, g1, 3 * DIR) * j1);
+  const double kyj = 0.5 * (met(z, g0, 3 * DIR + 1) * j0 + met(z, g1, 3 * DIR + 1) * j1);
+  const double kzj = 0.5 * (met(z, g0, 3 * DIR + 2) * j0 + met(z, g1, 3 * DIR + 2) * j1);
+  F[0] = 0;
+  F[1] = kxj * txx + kyj * txy + kzj * txz;
+  F[2] = kxj * txy + kyj * tyy + kzj * tyz;
+  F[3] = kxj * txz + kyj * tyz + kzj * tzz;
+  const double um = 0.5 * (bvl(z, g0, 1) + bvl(z, g1, 1));
+  const double vm = 0.5 * (bvl(z, g0, 2) + bvl(z, g1, 2));
+  const double wm = 0.5 * (bvl(z, g0, 3) + bvl(z, g1, 3));
+  const double t_x = dt[0] * mm[0] + dt[1] * mm[3] + dt[2] * mm[6];
+  const double t_y = dt[0] * mm[1] + dt[1] * mm[4] + dt[2] * mm[7];
+  const double t_z = dt[0] * mm[2] + dt[1] * mm[5] + dt[2] * mm[8];
+  const double cond = 0.5 * (ld(z.kappa + g0) + ld(z.kappa + g1));
+  F[4] = um * F[1] + vm * F[2] + wm * F[3] + cond * (kxj * t_x + kyj * t_y + kzj * t_z);
+  if constexpr (NS > 0) {
+    double yk[NS], diff[NS], ddf[NS];
+    double sgw = 0, srdy = 0, corr = 0, mwt = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      const double *ys = z.sv + l * z.sz;
+      yk[l] = 0.5 * (ld(ys + g0) + ld(ys + g1));
+      diff[l] = 0.5 * (ld(z.rhoD + l * z.sz + g0) + ld(z.rhoD + l * z.sz + g1));
+      double dy[3];
+      der(ys, dy);
+      const double y_x = dy[0] * mm[0] + dy[1] * mm[3] + dy[2] * mm[6];
+      const double y_y = dy[0] * mm[1] + dy[1] * mm[4] + dy[2] * mm[7];
+      const double y_z = dy[0] * mm[2] + dy[1] * mm[5] + dy[2] * mm[8];
+      const double g = kxj * y_x + kyj * y_y + kzj * y_z;
+      ddf[l] = g;
+      corr += diff[l] * g;
+      sgw += g / c_p.mw[l];
+      mwt += yk[l] / c_p.mw[l];
+      srdy += diff[l] * yk[l];
+    }
+    mwt = 1.0 / mwt;
+    corr -= mwt * srdy * sgw;
+    if (c_p.gradP) {
+      double dp[3];
+      der(z.bv + 4 * z.sz, dp);
+      const double p_x = dp[0] * mm[0] + dp[1] * mm[3] + dp[2] * mm[6];
+      const double p_y = dp[0] * mm[1] + dp[1] * mm[4] + dp[2] * mm[7];
+      const double p_z = dp[0] * mm[2] + dp[1] * mm[5] + dp[2] * mm[8];
+      const double gp = (kxj * p_x + kyj * p_y + kzj * p_z) / (0.5 * (bvl(z, g1, 4) + bvl(z, g0, 4)));
+#pragma unroll
+      for (int l = 0; l < NS; ++l) {
+        ddf[l] += (mwt / c_p.mw[l] - 1) * yk[l] * gp;
+        corr += (mwt / c_p.mw[l] - 1) * yk[l] * gp * diff[l];
+      }
+    }
+    double h[NS];
+    enthalpy<NS>(0.5 * (bvl(z, g0, 5) + bvl(z, g1, 5)), h);
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      const double flux = diff[l] * (ddf[l] - mwt * yk[l] * sgw) - yk[l] * corr;
+      F[5 + l] = flux;
+      F[4] += h[l] * flux;
+    }
+  }
+  (void)NV;
+}
+
+}  // namespace ostc

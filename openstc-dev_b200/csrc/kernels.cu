@@ -1,0 +1,676 @@
+// kernels.cu — sm_100a kernels of the RHS / RK3 stage.
+//
+//  flux_dir<NS,INV,DIR>   fused inviscid + viscous flux difference along one
+//                         direction (InviscidScheme.cu, AWENO.cu, ViscousScheme.cuh)
+//  source_kernel<NS>      finite-rate chemistry source, starts dq (SourceTerm.cuh:11-37)
+//  update_rk_kernel<NS>   SSPRK3 stage update, cv -> bv/sv, T and p (RK.cuh:392-448)
+//  properties_kernel<NS>  cp, gamma, a, mu, kappa, rho*D, Mach over [-1, m] (FieldOperation.cuh:112-146)
+//  cv_from_bv_kernel<NS>  conservative from primitive, ghosts included (FieldOperation.cuh:43-79)
+//  dt_kernel<NS>          local time step + block min + atomic min (TimeAdvanceFunc.cuh:50-100, .cu:155-201)
+//  bc_*_kernel            boundary conditions (BoundCond.cuh:52-210) and periodic wrap
+//  residual kernels       store_last_step / square of d(bv) / deterministic sums (Residual.cuh:57-161)
+//
+// Flux kernels march along the sweep direction: a CTA owns a segment of
+// S = R*C - 1 cells of 32 (or R) lines, computes the R*C faces that bound
+// them chunk by chunk, and carries the last face flux of each chunk into the
+// next, so every face is evaluated once and dq is touched once per direction.
+#include <cstdio>
+
+#include "common.cuh"
+
+namespace ostc {
+__constant__ DevParam c_p;
+}
+
+#include "chem.cuh"
+#include "face.cuh"
+#include "kernels.cuh"
+#include "thermo.cuh"
+
+namespace ostc {
+
+// ---------------------------------------------------------------------------
+// flux kernels
+// ---------------------------------------------------------------------------
+template <int NS, int INV, int DIR>
+__device__ __forceinline__ void face_total(const DevZone &z, int g0, bool viscous, double *G) {
+  constexpr int NV = 5 + NS;
+  double Fi[NV];
+  if constexpr (INV == 1)
+    inviscid_face_aweno<DIR>(z, g0, Fi);
+  else
+    inviscid_face_pv<NS, DIR>(z, g0, Fi);
+  if (viscous) {
+    double Fv[NV];
+    viscous_face<NS, DIR>(z, g0, Fv);
+#pragma unroll
+    for (int l = 0; l < NV; ++l) G[l] = Fv[l] - Fi[l];
+  } else {
+#pragma unroll
+    for (int l = 0; l < NV; ++l) G[l] = -Fi[l];
+  }
+}
+
+template <int NS, int INV, int DIR>
+__global__ void __launch_bounds__(256) flux_dir(DevZone z, int nchunk, int accumulate, int viscous) {
+  constexpr int NV = 5 + NS;
+  const int lane = threadIdx.x, row = threadIdx.y, R = blockDim.y;
+  const int n = DIR == 0 ? z.mx : (DIR == 1 ? z.my : z.mz);
+  const int cds_limit = n - 2 * z.ngg;  // quirk A4: no central correction on the last 2*ngg cells
+  const bool vis = viscous != 0;
+  if constexpr (DIR == 0) {
+    const int S = 32 * nchunk - 1;
+    const int c0 = blockIdx.x * S;
+    const int j = blockIdx.y * R + row, k = blockIdx.z;
+    const bool line_ok = j < z.my;
+    double carry[NV];
+#pragma unroll
+    for (int l = 0; l < NV; ++l) carry[l] = 0;
+    for (int ch = 0; ch < nchunk; ++ch) {
+      const int f = c0 - 1 + 32 * ch + lane;
+      const bool active = line_ok && f <= n - 1;
+      double G[NV];
+      if (active) {
+        face_total<NS, INV, DIR>(z, gidx(z, f, j, k), vis, G);
+      } else {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) G[l] = 0;
+      }
+      double Gm[NV];
+#pragma unroll
+      for (int l = 0; l < NV; ++l) {
+        const double up = __shfl_up_sync(0xffffffffu, G[l], 1);
+        Gm[l] = lane == 0 ? carry[l] : up;
+        carry[l] = __shfl_sync(0xffffffffu, G[l], 31);
+      }
+      if (active && f >= c0 && f >= 0) {
+        double corr[5] = {0, 0, 0, 0, 0};
+        if constexpr (INV == 1) {
+          if (f < cds_limit) cds_correction<DIR>(z, gidx(z, f, j, k), corr);
+        }
+        double *dq = z.dq + qidx(z, f, j, k);
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          double d = G[l] - Gm[l];
+          if (INV == 1 && l < 5) d -= corr[l];
+          if (accumulate)
+            dq[l * z.qsz] += d;
+          else
+            dq[l * z.qsz] = d;
+        }
+      }
+    }
+  } else {
+    extern __shared__ double sG[];  // [R+1][NV][32]
+    const int S = R * nchunk - 1;
+    const int i = blockIdx.x * 32 + lane;
+    const int c0 = (DIR == 1 ? blockIdx.y : blockIdx.z) * S;
+    const int j_fixed = blockIdx.y, k_fixed = blockIdx.z;
+    const bool col_ok = i < z.mx;
+    for (int ch = 0; ch < nchunk; ++ch) {
+      const int f = c0 - 1 + R * ch + row;
+      const bool active = col_ok && f <= n - 1;
+      const int ci = i, cj = DIR == 1 ? f : j_fixed, ck = DIR == 2 ? f : k_fixed;
+      double G[NV];
+      if (active) {
+        face_total<NS, INV, DIR>(z, gidx(z, ci, cj, ck), vis, G);
+      } else {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) G[l] = 0;
+      }
+#pragma unroll
+      for (int l = 0; l < NV; ++l) sG[((row + 1) * NV + l) * 32 + lane] = G[l];
+      __syncthreads();
+      if (active && f >= c0 && f >= 0 && !(ch == 0 && row == 0)) {
+        double corr[5] = {0, 0, 0, 0, 0};
+        if constexpr (INV == 1) {
+          if (f < cds_limit) cds_correction<DIR>(z, gidx(z, ci, cj, ck), corr);
+        }
+        double *dq = z.dq + qidx(z, ci, cj, ck);
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          double d = G[l] - sG[(row * NV + l) * 32 + lane];
+          if (INV == 1 && l < 5) d -= corr[l];
+          if (accumulate)
+            dq[l * z.qsz] += d;
+          else
+            dq[l * z.qsz] = d;
+        }
+      }
+      __syncthreads();
+      if (row == 0) {
+#pragma unroll
+        for (int l = 0; l < NV; ++l) sG[l * 32 + lane] = sG[(R * NV + l) * 32 + lane];
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// per-cell kernels
+// ---------------------------------------------------------------------------
+template <int NS>
+__global__ void __launch_bounds__(256) source_kernel(DevZone z) {
+  constexpr int NV = 5 + NS;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
+  const int g = gidx(z, i, j, k);
+  double *dq = z.dq + qidx(z, i, j, k);
+#pragma unroll
+  for (int l = 0; l < 5; ++l) dq[l * z.qsz] = 0;
+  if constexpr (NS > 0) {
+    double Y[NS], om[NS];
+#pragma unroll
+    for (int l = 0; l < NS; ++l) Y[l] = svl(z, g, l);
+    chemistry_omega<NS>(bvl(z, g, 0), bvl(z, g, 5), Y, om);
+    const double jc = ld(z.jac + g);
+#pragma unroll
+    for (int l = 0; l < NS; ++l) dq[(5 + l) * z.qsz] = jc * om[l];
+  }
+  (void)NV;
+}
+
+__constant__ double c_rk_a[3] = {1.0, 0.75, 1.0 / 3.0};
+__constant__ double c_rk_b[3] = {0.0, 0.25, 2.0 / 3.0};
+__constant__ double c_rk_c[3] = {1.0, 0.25, 2.0 / 3.0};
+
+template <int NS>
+__global__ void __launch_bounds__(256) update_rk_kernel(DevZone z, double dt_in, const double *dt_dev, int rk) {
+  constexpr int NV = 5 + NS;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
+  const double dt = dt_dev ? *dt_dev : dt_in;
+  const int g = gidx(z, i, j, k);
+  const int q = qidx(z, i, j, k);
+  const double a = c_rk_a[rk], b = c_rk_b[rk], c = c_rk_c[rk];
+  const double dtj = dt / z.jac[g];
+  double cv[NV];
+#pragma unroll
+  for (int l = 0; l < NV; ++l) {
+    cv[l] = a * z.qn[l * z.sz + g] + b * z.cv[l * z.sz + g] + c * dtj * z.dq[l * z.qsz + q];
+  }
+  if (z.mz == 1) cv[3] = 0;
+#pragma unroll
+  for (int l = 0; l < NV; ++l) z.cv[l * z.sz + g] = cv[l];
+  const double rho = cv[0];
+  const double ri = 1.0 / rho;
+  const double u = cv[1] * ri, v = cv[2] * ri, w = cv[3] * ri;
+  z.bv[g] = rho;
+  z.bv[z.sz + g] = u;
+  z.bv[2 * z.sz + g] = v;
+  z.bv[3 * z.sz + g] = w;
+  const double V2 = u * u + v * v + w * w;
+  if constexpr (NS == 0) {
+    const double p = (gamma_air - 1) * (cv[4] - 0.5 * rho * V2);
+    z.bv[4 * z.sz + g] = p;
+    z.bv[5 * z.sz + g] = p * mw_air * ri / R_u;
+  } else {
+    double Y[NS];
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      Y[l] = cv[5 + l] * ri;
+      z.sv[l * z.sz + g] = Y[l];
+    }
+    // compute_temperature_and_pressure (FieldOperation.cu:3-39)
+    double mw = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) mw += Y[l] / c_p.mw[l];
+    mw = 1 / mw;
+    const double R = R_u / mw;
+    const double e = cv[4] / rho - 0.5 * V2;
+    double err = 1, t = z.bv[5 * z.sz + g];
+    int iter = 0;
+    while (err > 1e-3 && iter++ < 1000) {
+      double h[NS], cp[NS];
+      enthalpy_cp<NS>(t, h, cp);
+      double cpt = 0, hh = 0;
+#pragma unroll
+      for (int l = 0; l < NS; ++l) {
+        cpt += cp[l] * Y[l];
+        hh += h[l] * Y[l];
+      }
+      const double t1 = t - (hh - R * t - e) / (cpt - R);
+      err = fabs(1 - t1 / t);
+      t = t1;
+    }
+    z.bv[5 * z.sz + g] = t;
+    z.bv[4 * z.sz + g] = rho * t * R;
+  }
+  z.vel[g] = sqrt(V2);
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256) properties_kernel(DevZone z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
+  const int k = blockIdx.z - 1;
+  if (i > z.mx || j > z.my) return;
+  const int g = gidx(z, i, j, k);
+  const double T = z.bv[5 * z.sz + g];
+  double a;
+  if constexpr (NS == 0) {
+    constexpr double c_temp = gamma_air * R_u / mw_air;
+    constexpr double cpa = gamma_air * R_u / mw_air / (gamma_air - 1);
+    a = sqrt(c_temp * T);
+    const double mu = sutherland(T);
+    z.mul[g] = mu;
+    z.kappa[g] = mu * cpa / c_p.Pr;
+  } else {
+    double Y[NS], cp[NS], rD[NS];
+    cp_only<NS>(T, cp);
+    double mw = 0, cpt = 0, cvv = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      Y[l] = z.sv[l * z.sz + g];
+      mw += Y[l] / c_p.mw[l];
+      cpt += Y[l] * cp[l];
+      cvv += Y[l] * (cp[l] - c_p.Rmw[l]);
+    }
+    mw = 1 / mw;
+    const double gam = cpt / cvv;
+    z.cp[g] = cpt;
+    z.gam[g] = gam;
+    a = sqrt(gam * R_u * T / mw);
+    double mu, kap;
+    mixture_transport<NS>(T, mw, Y, cp, z.bv[g], z.bv[4 * z.sz + g], mu, kap, rD);
+    z.mul[g] = mu;
+    z.kappa[g] = kap;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) z.rhoD[l * z.sz + g] = rD[l];
+  }
+  z.a[g] = a;
+  z.mach[g] = z.vel[g] / a;
+}
+
+template <int NS>
+__device__ __forceinline__ void cv_from_bv_point(const DevZone &z, int g) {
+  const double rho = z.bv[g], u = z.bv[z.sz + g], v = z.bv[2 * z.sz + g], w = z.bv[3 * z.sz + g];
+  const double p = z.bv[4 * z.sz + g];
+  z.cv[g] = rho;
+  z.cv[z.sz + g] = rho * u;
+  z.cv[2 * z.sz + g] = rho * v;
+  z.cv[3 * z.sz + g] = rho * w;
+  const double V2 = u * u + v * v + w * w;
+  double E = 0.5 * V2;
+  if constexpr (NS == 0) {
+    E *= rho;
+    E += p / (gamma_air - 1);
+  } else {
+    double h[NS];
+    enthalpy<NS>(z.bv[5 * z.sz + g], h);
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      const double Y = z.sv[l * z.sz + g];
+      z.cv[(5 + l) * z.sz + g] = rho * Y;
+      E += h[l] * Y;
+    }
+    E *= rho;
+    E -= p;
+  }
+  z.cv[4 * z.sz + g] = E;
+  z.vel[g] = sqrt(V2);
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256) cv_from_bv_kernel(DevZone z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - z.ngg;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - z.ngg;
+  const int k = blockIdx.z - z.ngg;
+  if (i >= z.mx + z.ngg || j >= z.my + z.ngg) return;
+  cv_from_bv_point<NS>(z, gidx(z, i, j, k));
+}
+
+__global__ void __launch_bounds__(256) velocity_kernel(DevZone z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - z.ngg;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - z.ngg;
+  const int k = blockIdx.z - z.ngg;
+  if (i >= z.mx + z.ngg || j >= z.my + z.ngg) return;
+  const int g = gidx(z, i, j, k);
+  const double u = z.bv[z.sz + g], v = z.bv[2 * z.sz + g], w = z.bv[3 * z.sz + g];
+  z.vel[g] = sqrt(u * u + v * v + w * w);
+}
+
+// local time step and global minimum; dt_bits holds the IEEE bits of a
+// positive double, whose unsigned order equals the numeric order
+template <int NS>
+__global__ void __launch_bounds__(256) dt_kernel(DevZone z, unsigned long long *dt_bits) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  double dtl = 1e6;
+  if (i < z.mx && j < z.my) {
+    const int g = gidx(z, i, j, k);
+    double m[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) m[c] = met(z, g, c);
+    const double gx = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    const double ge = sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
+    const double gz = sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
+    const double u = bvl(z, g, 1), v = bvl(z, g, 2), w = bvl(z, g, 3);
+    const double U = u * m[0] + v * m[1] + w * m[2];
+    const double V = u * m[3] + v * m[4] + w * m[5];
+    const double W = u * m[6] + v * m[7] + w * m[8];
+    const double a = ld(z.a + g);
+    const bool d3 = z.mz > 1;
+    const double sri = (fabs(U) + a * gx) + (fabs(V) + a * ge) + (d3 ? fabs(W) + a * gz : 0.0);
+    const double gamma = NS == 0 ? gamma_air : ld(z.gam + g);
+    const double c1 = fmax(gamma, 4.0 / 3.0) / bvl(z, g, 0);
+    const double c2 = ld(z.mul + g) / c_p.Pr;
+    double srv = gx * gx + ge * ge;
+    if (d3) srv += gz * gz;
+    srv *= c1 * c2;
+    dtl = c_p.cfl / (sri + srv);
+    if (z.dt_local) z.dt_local[nidx(z, i, j, k)] = dtl;
+  }
+  // warp then block min
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dtl = fmin(dtl, __shfl_xor_sync(0xffffffffu, dtl, o));
+  __shared__ double wmin[32];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  if ((tid & 31) == 0) wmin[tid >> 5] = dtl;
+  __syncthreads();
+  if (tid < 32) {
+    const int nw = (blockDim.x * blockDim.y + 31) / 32;
+    double v = tid < nw ? wmin[tid] : 1e6;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (tid == 0) atomicMin(dt_bits, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+__global__ void dt_reset_kernel(unsigned long long *dt_bits) {
+  *dt_bits = (unsigned long long)__double_as_longlong(1e6);
+}
+
+// ---------------------------------------------------------------------------
+// boundary conditions. One thread per boundary point of the face range.
+// ---------------------------------------------------------------------------
+template <int NS>
+__global__ void bc_outflow_kernel(DevZone z, BcFace b, int with_cv) {  // BoundCond.cuh:120-150
+  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = b.rs[2] + blockIdx.z;
+  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+  const int g = gidx(z, i, j, k);
+  const int step = b.dir_stride;
+  for (int gg = 1; gg <= z.ngg; ++gg) {
+    const int gi = g + gg * step;
+    for (int l = 0; l < 6; ++l) z.bv[l * z.sz + gi] = z.bv[l * z.sz + g];
+    for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + gi] = z.sv[l * z.sz + g];
+    if (with_cv) cv_from_bv_point<NS>(z, gi);
+  }
+}
+
+template <int NS>
+__global__ void bc_inflow_kernel(DevZone z, BcFace b, int with_cv) {  // BoundCond.cuh:152-210
+  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = b.rs[2] + blockIdx.z;
+  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+  const int g = gidx(z, i, j, k);
+  const int step = b.dir_stride;
+  for (int gg = 0; gg <= z.ngg; ++gg) {
+    const int gi = g + gg * step;
+    z.bv[gi] = b.density;
+    z.bv[z.sz + gi] = b.u;
+    z.bv[2 * z.sz + gi] = b.v;
+    z.bv[3 * z.sz + gi] = b.w;
+    z.bv[4 * z.sz + gi] = b.pressure;
+    z.bv[5 * z.sz + gi] = b.temperature;
+    for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + gi] = b.sv[l];
+    if (gg == 0) z.vel[gi] = b.velocity;
+    if (with_cv) {
+      // compute_cv_from_bv_1_point also rewrites vel from bv (FieldOperation.cuh:40)
+      cv_from_bv_point<NS>(z, gi);
+    }
+  }
+}
+
+__global__ void bc_symmetry_kernel(DevZone z, BcFace b) {  // BoundCond.cuh:52-118
+  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = b.rs[2] + blockIdx.z;
+  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+  const int g = gidx(z, i, j, k);
+  const int step = b.dir_stride;
+  const int gin = g - step;
+  double kx = z.met[(3 * b.face) * z.sz + g], ky = z.met[(3 * b.face + 1) * z.sz + g];
+  double kz = z.met[(3 * b.face + 2) * z.sz + g];
+  const double km = sqrt(kx * kx + ky * ky + kz * kz);
+  kx /= km;
+  ky /= km;
+  kz /= km;
+  const double u1 = z.bv[z.sz + gin], v1 = z.bv[2 * z.sz + gin], w1 = z.bv[3 * z.sz + gin];
+  double uk = kx * u1 + ky * v1 + kz * w1;
+  const double ut = u1 - kx * uk, vt = v1 - ky * uk, wt = w1 - kz * uk;
+  z.bv[z.sz + g] = ut;
+  z.bv[2 * z.sz + g] = vt;
+  z.bv[3 * z.sz + g] = wt;
+  z.vel[g] = sqrt(ut * ut + vt * vt + wt * wt);
+  z.bv[g] = z.bv[gin];
+  z.bv[4 * z.sz + g] = z.bv[4 * z.sz + gin];
+  z.bv[5 * z.sz + g] = z.bv[5 * z.sz + gin];
+  for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + g] = z.sv[l * z.sz + gin];
+  for (int gg = 1; gg <= z.ngg; ++gg) {
+    const int go = g + gg * step, gi = g - gg * step;
+    z.bv[go] = z.bv[gi];
+    const double u = z.bv[z.sz + gi], v = z.bv[2 * z.sz + gi], w = z.bv[3 * z.sz + gi];
+    uk = kx * u + ky * v + kz * w;
+    const double uo = u - 2 * uk * kx, vo = v - 2 * uk * ky, wo = w - 2 * uk * kz;
+    z.bv[z.sz + go] = uo;
+    z.bv[2 * z.sz + go] = vo;
+    z.bv[3 * z.sz + go] = wo;
+    z.vel[go] = sqrt(uo * uo + vo * vo + wo * wo);
+    z.bv[4 * z.sz + go] = z.bv[4 * z.sz + gi];
+    z.bv[5 * z.sz + go] = z.bv[5 * z.sz + gi];
+    for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = z.sv[l * z.sz + gi];
+  }
+}
+
+// periodic wrap (no reference counterpart): ghost layer gg of this face takes
+// the point n cells back along the face normal
+__global__ void bc_periodic_kernel(DevZone z, BcFace b, int with_cv) {
+  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = b.rs[2] + blockIdx.z;
+  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+  const int g = gidx(z, i, j, k);
+  for (int gg = 1; gg <= z.ngg; ++gg) {
+    const int go = g + gg * b.dir_stride;
+    const int gs = go - b.period_stride;
+    for (int l = 0; l < 6; ++l) z.bv[l * z.sz + go] = z.bv[l * z.sz + gs];
+    for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = z.sv[l * z.sz + gs];
+    z.vel[go] = z.vel[gs];
+    if (with_cv)
+      for (int l = 0; l < c_p.n_var; ++l) z.cv[l * z.sz + go] = z.cv[l * z.sz + gs];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// residual: store_last_step (TimeAdvanceFunc.cu:6-17), square of the change
+// and deterministic two-level sums (Residual.cuh:57-111, Residual.cu:49-89)
+// ---------------------------------------------------------------------------
+__global__ void store_last_kernel(DevZone z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
+  const int g = gidx(z, i, j, k), n = nidx(z, i, j, k);
+  z.bv_last[n] = z.bv[g];
+  z.bv_last[z.nsz + n] = z.vel[g];
+  z.bv_last[2 * z.nsz + n] = z.bv[4 * z.sz + g];
+  z.bv_last[3 * z.nsz + n] = z.bv[5 * z.sz + g];
+}
+
+// one partial sum of the 4 squared changes per CTA (256 threads, grid-stride)
+__global__ void __launch_bounds__(256) residual_partial_kernel(DevZone z, double *partial) {
+  const long long n = (long long)z.mx * z.my * z.mz;
+  double s[4] = {0, 0, 0, 0};
+  for (long long q = blockIdx.x * 256ll + threadIdx.x; q < n; q += 256ll * gridDim.x) {
+    const int i = (int)(q % z.mx);
+    const int j = (int)((q / z.mx) % z.my);
+    const int k = (int)(q / ((long long)z.mx * z.my));
+    const int g = gidx(z, i, j, k);
+    const double d0 = z.bv[g] - z.bv_last[q];
+    const double d1 = z.vel[g] - z.bv_last[z.nsz + q];
+    const double d2 = z.bv[4 * z.sz + g] - z.bv_last[2 * z.nsz + q];
+    const double d3 = z.bv[5 * z.sz + g] - z.bv_last[3 * z.nsz + q];
+    s[0] += d0 * d0;
+    s[1] += d1 * d1;
+    s[2] += d2 * d2;
+    s[3] += d3 * d3;
+  }
+  __shared__ double red[4][256];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) red[l][threadIdx.x] = s[l];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) red[l][threadIdx.x] += red[l][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int l = 0; l < 4; ++l) partial[blockIdx.x * 4 + l] = red[l][0];
+}
+
+// sums n_part partials (fixed order) of every zone and writes sqrt(sum / n_total)
+__global__ void residual_final_kernel(const double *partial, int n_part, double n_total, double *out) {
+  const int l = threadIdx.x;
+  if (l >= 4) return;
+  double s = 0;
+  for (int p = 0; p < n_part; ++p) s += partial[p * 4 + l];
+  out[l] = sqrt(s / n_total);
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers (kernels.cuh)
+// ---------------------------------------------------------------------------
+namespace {
+dim3 plane_grid(int nx, int ny, int nz, dim3 blk) {
+  return dim3((nx + blk.x - 1) / blk.x, (ny + blk.y - 1) / blk.y, nz);
+}
+}  // namespace
+
+template <int NS, int INV, int DIR>
+static cudaError_t launch_flux_t(const DevZone &z, const TileShape &t, int accumulate, int viscous,
+                                 cudaStream_t s) {
+  constexpr int NV = 5 + NS;
+  const int R = t.rows, C = t.chunks;
+  dim3 blk(32, R);
+  dim3 grid;
+  size_t smem = 0;
+  if (DIR == 0) {
+    const int S = 32 * C - 1;
+    grid = dim3((z.mx + S - 1) / S, (z.my + R - 1) / R, z.mz);
+  } else {
+    const int S = R * C - 1;
+    smem = sizeof(double) * (R + 1) * NV * 32;
+    if (DIR == 1)
+      grid = dim3((z.mx + 31) / 32, (z.my + S - 1) / S, z.mz);
+    else
+      grid = dim3((z.mx + 31) / 32, z.my, (z.mz + S - 1) / S);
+  }
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(flux_dir<NS, INV, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  flux_dir<NS, INV, DIR><<<grid, blk, smem, s>>>(z, C, accumulate, viscous);
+  return cudaGetLastError();
+}
+
+template <int NS>
+cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, int accumulate, int viscous,
+                        cudaStream_t s) {
+  if constexpr (NS == 0) {
+    if (inv == 1) {
+      switch (dir) {
+        case 0: return launch_flux_t<0, 1, 0>(z, t, accumulate, viscous, s);
+        case 1: return launch_flux_t<0, 1, 1>(z, t, accumulate, viscous, s);
+        default: return launch_flux_t<0, 1, 2>(z, t, accumulate, viscous, s);
+      }
+    }
+  }
+  switch (dir) {
+    case 0: return launch_flux_t<NS, 0, 0>(z, t, accumulate, viscous, s);
+    case 1: return launch_flux_t<NS, 0, 1>(z, t, accumulate, viscous, s);
+    default: return launch_flux_t<NS, 0, 2>(z, t, accumulate, viscous, s);
+  }
+}
+
+template <int NS>
+cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStream_t s) {
+  const dim3 blk(32, 8);
+  switch (op) {
+    case CellOp::Source:
+      source_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z);
+      break;
+    case CellOp::UpdateRK:
+      update_rk_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z, a.dt, a.dt_dev, a.rk);
+      break;
+    case CellOp::Properties:
+      properties_kernel<NS><<<plane_grid(z.mx + 2, z.my + 2, z.mz + 2, blk), blk, 0, s>>>(z);
+      break;
+    case CellOp::CvFromBv:
+      cv_from_bv_kernel<NS>
+          <<<plane_grid(z.mx + 2 * z.ngg, z.my + 2 * z.ngg, z.mz + 2 * z.ngg, blk), blk, 0, s>>>(z);
+      break;
+    case CellOp::Velocity:
+      velocity_kernel<<<plane_grid(z.mx + 2 * z.ngg, z.my + 2 * z.ngg, z.mz + 2 * z.ngg, blk), blk, 0, s>>>(z);
+      break;
+    case CellOp::Dt:
+      dt_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z, a.dt_bits);
+      break;
+    case CellOp::DtReset:
+      dt_reset_kernel<<<1, 1, 0, s>>>(a.dt_bits);
+      break;
+    case CellOp::StoreLast:
+      store_last_kernel<<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z);
+      break;
+    case CellOp::ResidualPartial:
+      residual_partial_kernel<<<a.n_part, 256, 0, s>>>(z, a.partial);
+      break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s) {
+  residual_final_kernel<<<1, 32, 0, s>>>(partial, n_part, n_total, out);
+  return cudaGetLastError();
+}
+
+template <int NS>
+cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s) {
+  const int n0 = b.re[0] - b.rs[0] + 1, n1 = b.re[1] - b.rs[1] + 1, n2 = b.re[2] - b.rs[2] + 1;
+  const dim3 blk(n0 >= 32 ? 32 : (n0 >= 8 ? 8 : 1), n1 >= 8 ? 8 : 1);
+  const dim3 grid((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, n2);
+  switch (b.type) {
+    case OSTC_BC_OUTFLOW: bc_outflow_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
+    case OSTC_BC_INFLOW: bc_inflow_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
+    case OSTC_BC_SYMMETRY: bc_symmetry_kernel<<<grid, blk, 0, s>>>(z, b); break;
+    case OSTC_BC_PERIODIC: bc_periodic_kernel<<<grid, blk, 0, s>>>(z, b, with_cv); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
+  return cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
+}
+
+#define OSTC_INSTANTIATE(NS)                                                                                  \
+  template cudaError_t launch_flux<NS>(const DevZone &, int, int, const TileShape &, int, int, cudaStream_t); \
+  template cudaError_t launch_cells<NS>(CellOp, const DevZone &, const CellArgs &, cudaStream_t);            \
+  template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);
+
+OSTC_INSTANTIATE(0)
+OSTC_INSTANTIATE(9)
+
+}  // namespace ostc

@@ -1,0 +1,46 @@
+// kernels.cuh — host-side launch interface of kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace ostc {
+
+// launch shape of one flux-direction kernel: R rows of 32 threads, C chunks per segment
+struct TileShape {
+  int rows;
+  int chunks;
+};
+
+// one boundary face as the kernels see it
+struct BcFace {
+  int type, face, direction;
+  int rs[3], re[3];
+  int dir_stride;     // ghosted-index stride of one step along the outward normal
+  int period_stride;  // periodic: ghosted-index stride of n cells along the normal
+  double density, u, v, w, pressure, temperature, velocity, mut;
+  double sv[OSTC_MAX_SPEC + 4];
+};
+
+enum class CellOp { Source, UpdateRK, Properties, CvFromBv, Velocity, Dt, DtReset, StoreLast, ResidualPartial };
+
+struct CellArgs {
+  double dt = 0;
+  const double *dt_dev = nullptr;
+  int rk = 0;
+  unsigned long long *dt_bits = nullptr;
+  double *partial = nullptr;
+  int n_part = 0;
+};
+
+template <int NS>
+cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, int accumulate, int viscous,
+                        cudaStream_t s);
+template <int NS>
+cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStream_t s);
+template <int NS>
+cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s);
+cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
+cudaError_t upload_param(const DevParam &p, cudaStream_t s);
+
+}  // namespace ostc

@@ -1,0 +1,573 @@
+"""Python host side of the B200 RHS / RK3 path: ctypes binding of the C ABI
+in include/ostc.h, block storage in the reference's DZone layout, and the
+synthetic workloads.
+
+The binding mirrors the reference's operator API (src/RK.cuh:301-355):
+``Solver.compute_rhs`` is compute_source + compute_inviscid_flux +
+compute_viscous_flux, ``Solver.rk3_stage`` one SSPRK3 stage, and so on. All
+arithmetic runs in libostc.so (sm_100a); torch only owns device memory.
+Loading fails loudly when libostc.so is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Dict, List, Optional
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libostc.so"
+MAX_SPEC = 20
+MAX_REAC = 50
+
+# status codes (include/ostc.h)
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_TIMEOUT, ERR_NONPHYSICAL, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(7)
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "CUDA", 3: "TIMEOUT", 4: "NONPHYSICAL", 5: "UNSUPPORTED",
+                6: "NO_DEVICE"}
+MIX_AIR, MIX_MIXTURE, MIX_FR = 0, 1, 2
+BC_WALL, BC_SYMMETRY, BC_FARFIELD, BC_INFLOW, BC_OUTFLOW = 2, 3, 4, 5, 6
+BC_SUBSONIC_INFLOW, BC_BACK_PRESSURE, BC_PERIODIC = 7, 9, 100
+
+R_U = 8314.462618
+MW_AIR = 28.9647
+GAMMA_AIR = 1.4
+
+
+class OstcError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__("%s failed: %s" % (what, STATUS_NAMES.get(status, status)))
+
+
+# ---------------------------------------------------------------------------
+# C structures (include/ostc.h)
+# ---------------------------------------------------------------------------
+_ZONE_PTRS = ["x", "y", "z", "jac", "metric", "wall_distance", "cv", "bv", "sv", "bv_last", "vel",
+              "acoustic_speed", "mach", "mul", "thermal_conductivity", "rho_D", "gamma", "cp", "chem_src_jac",
+              "mut", "turb_therm_cond", "turb_src_jac", "dq", "dq0", "dqk", "inv_spectr_rad", "visc_spectr_rad",
+              "dt_local", "entropy_fix_delta", "qn"]
+
+
+class Zone(C.Structure):
+    _fields_ = [("mx", C.c_int), ("my", C.c_int), ("mz", C.c_int), ("ngg", C.c_int), ("dq_ngg", C.c_int),
+                ("reserved_", C.c_int)] + [(n, C.c_void_p) for n in _ZONE_PTRS]
+
+
+_PARAM_INTS = ["mix_model", "turbulence", "n_var", "n_scalar", "n_spec", "n_reac", "i_turb_cv", "inviscid_scheme",
+               "reconstruction", "limiter", "inviscid_type", "viscous_scheme", "rans_model", "turb_implicit",
+               "compressibility_correction", "chemSrcMethod", "gradPInDiffusionFlux", "dimension"]
+_PARAM_DBLS = ["entropy_fix_factor", "Pr", "Prt", "Sct", "Sc", "cfl"]
+_PARAM_TABS = ["mw", "high_temp_coeff", "low_temp_coeff", "t_low", "t_mid", "t_high", "LJ_potent_inv", "vis_coeff",
+               "WjDivWi_to_One4th", "sqrt_WiDivWjPl1Mul8", "binary_diffusivity_coeff", "kb_over_eps_jk",
+               "reac_type", "stoi_f", "stoi_b", "reac_order", "A", "b", "Ea", "A2", "b2", "Ea2", "third_body_coeff",
+               "troe_alpha", "troe_t3", "troe_t1", "troe_t2"]
+_INT_TABS = {"reac_type", "stoi_f", "stoi_b", "reac_order"}
+
+
+class Param(C.Structure):
+    _fields_ = [(n, C.c_int) for n in _PARAM_INTS] + [(n, C.c_double) for n in _PARAM_DBLS] + \
+               [(n, C.c_void_p) for n in _PARAM_TABS]
+
+
+class BcFaceC(C.Structure):
+    _fields_ = [("block", C.c_int), ("type_label", C.c_int), ("face", C.c_int), ("direction", C.c_int),
+                ("range_start", C.c_int * 3), ("range_end", C.c_int * 3),
+                ("density", C.c_double), ("u", C.c_double), ("v", C.c_double), ("w", C.c_double),
+                ("pressure", C.c_double), ("temperature", C.c_double), ("velocity", C.c_double),
+                ("mut", C.c_double), ("sv", C.c_double * (MAX_SPEC + 4)),
+                ("wall_isothermal", C.c_int), ("wall_temperature", C.c_double)]
+
+
+class Config(C.Structure):
+    _fields_ = [("steady", C.c_int), ("temporal_scheme", C.c_int), ("implicit_method", C.c_int),
+                ("DPLUR_inner_step", C.c_int), ("fixed_time_step", C.c_int), ("dt", C.c_double),
+                ("output_screen", C.c_int), ("compat", C.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """The product library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError("libostc.so is missing at %s: run __graft_entry__.build() (no CPU fallback)" % LIB_PATH)
+        L = C.CDLL(str(LIB_PATH))
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        sig = {
+            "ostc_create": [C.POINTER(Config), C.POINTER(Param), C.POINTER(Zone), i, C.POINTER(BcFaceC), i,
+                            C.POINTER(vp)],
+            "ostc_destroy": [vp],
+            "ostc_compute_cv_from_bv": [vp, vp],
+            "ostc_compute_rhs": [vp, vp],
+            "ostc_global_time_step": [vp, C.POINTER(d), vp],
+            "ostc_update_cv_and_bv_rk": [vp, d, i, vp],
+            "ostc_apply_boundary_conditions": [vp, i, vp],
+            "ostc_data_communication": [vp, i, vp],
+            "ostc_update_physical_properties": [vp, vp],
+            "ostc_initialize": [vp, vp],
+            "ostc_rk3_stage": [vp, i, vp],
+            "ostc_rk3_steps": [vp, i, C.POINTER(d), C.POINTER(d), vp],
+            "ostc_metric_from_grid": [i, i, i, i, vp, vp, vp, vp, vp],
+            "ostc_get_error": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)],
+            "ostc_set_tile": [vp, i, i, i],
+            "ostc_get_tile": [vp, i, C.POINTER(i), C.POINTER(i)],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.ostc_version.restype = C.c_char_p
+        L.ostc_dt_device.restype = C.c_void_p
+        L.ostc_dt_device.argtypes = [vp]
+        L.ostc_zone_required.restype = C.c_uint64
+        L.ostc_zone_required.argtypes = [C.POINTER(Config), C.POINTER(Param)]
+        _lib = L
+    return _lib
+
+
+def check(status: int, what: str):
+    if status != OK:
+        raise OstcError(status, what)
+
+
+# ---------------------------------------------------------------------------
+# layout helpers (ggxl ColMajor, src/gxl_lib/Array.hpp:128-194)
+# ---------------------------------------------------------------------------
+def plane_shape(mx, my, mz, g):
+    """numpy shape of one plane: element (i,j,k) is arr[k+g, j+g, i+g]."""
+    return (mz + 2 * g, my + 2 * g, mx + 2 * g)
+
+
+def plane_size(mx, my, mz, g):
+    return (mx + 2 * g) * (my + 2 * g) * (mz + 2 * g)
+
+
+METRIC_DTYPE = np.dtype([("bias", "<i4"), ("pad", "<i4"), ("m", "<f8", (9,))])  # gxl::Matrix<real,3,3,1>
+
+
+# ---------------------------------------------------------------------------
+# physical tables (DParameter)
+# ---------------------------------------------------------------------------
+@dataclass
+class Mechanism:
+    """Species / reaction tables of cfd::Species and cfd::Reaction (src/ChemData.h)."""
+    names: List[str]
+    tables: Dict[str, np.ndarray]
+    n_reac: int = 0
+
+    @property
+    def n_spec(self):
+        return len(self.names)
+
+
+@dataclass
+class Scheme:
+    mix_model: int = MIX_AIR
+    inviscid_scheme: int = 3
+    reconstruction: int = 2
+    limiter: int = 0
+    viscous_order: int = 2
+    chemSrcMethod: int = 0
+    gradPInDiffusionFlux: int = 0
+    Pr: float = 0.72
+    Prt: float = 0.9
+    Sct: float = 0.9
+    Sc: float = 0.9
+    cfl: float = 0.5
+    entropy_fix_factor: float = 0.125
+    fixed_time_step: int = 0
+    dt: float = 1e-6
+
+    @property
+    def inviscid_type(self):
+        # Parameter::deduce_known_info (src/Parameter.cpp:193-198): Roe -> 2, WENO5 overrides to 1
+        t = 2 if self.inviscid_scheme == 2 else 0
+        if self.reconstruction in (4, 5):
+            t = 1
+        return t
+
+    @property
+    def ngg(self):
+        return 3 if self.reconstruction == 4 else 2  # Parameter.cpp:170-180
+
+
+def make_param(s: Scheme, mech: Optional[Mechanism]):
+    """Returns (Param, keepalive) with host tables packed as the ABI expects."""
+    p = Param()
+    ns = mech.n_spec if (mech is not None and s.mix_model != MIX_AIR) else 0
+    p.mix_model = s.mix_model
+    p.turbulence = 0
+    p.n_spec = ns
+    p.n_scalar = ns
+    p.n_var = 5 + ns
+    p.n_reac = mech.n_reac if (mech is not None and s.mix_model == MIX_FR) else 0
+    p.i_turb_cv = 5 + ns
+    p.inviscid_scheme = s.inviscid_scheme
+    p.reconstruction = s.reconstruction
+    p.limiter = s.limiter
+    p.inviscid_type = s.inviscid_type
+    p.viscous_scheme = s.viscous_order
+    p.rans_model = 0
+    p.turb_implicit = 0
+    p.compressibility_correction = 0
+    p.chemSrcMethod = s.chemSrcMethod
+    p.gradPInDiffusionFlux = s.gradPInDiffusionFlux
+    p.dimension = 3
+    for n in _PARAM_DBLS:
+        setattr(p, n, getattr(s, n))
+    keep = []
+    if ns:
+        for n in _PARAM_TABS:
+            if n not in mech.tables:
+                continue
+            arr = np.ascontiguousarray(mech.tables[n], dtype=np.int32 if n in _INT_TABS else np.float64)
+            keep.append(arr)
+            setattr(p, n, arr.ctypes.data)
+    return p, keep
+
+
+def make_config(s: Scheme, output_screen: int = 1) -> Config:
+    c = Config()
+    c.steady = 0
+    c.temporal_scheme = 3
+    c.implicit_method = 0
+    c.DPLUR_inner_step = 3
+    c.fixed_time_step = s.fixed_time_step
+    c.dt = s.dt
+    c.output_screen = output_screen
+    c.compat = 1
+    return c
+
+
+# ---------------------------------------------------------------------------
+# block storage
+# ---------------------------------------------------------------------------
+@dataclass
+class HostBlock:
+    """One block in the reference layout, host (numpy) side."""
+    mx: int
+    my: int
+    mz: int
+    ngg: int
+    n_var: int
+    n_spec: int
+    arrays: Dict[str, np.ndarray] = field(default_factory=dict)
+
+    def plane(self, g=None):
+        return plane_shape(self.mx, self.my, self.mz, self.ngg if g is None else g)
+
+    @staticmethod
+    def allocate(mx, my, mz, ngg, n_var, n_spec) -> "HostBlock":
+        b = HostBlock(mx, my, mz, ngg, n_var, n_spec)
+        P = plane_shape(mx, my, mz, ngg)
+        I = plane_shape(mx, my, mz, 0)
+        ns = n_spec
+        a = b.arrays
+        a["bv"] = np.zeros((6,) + P)
+        a["sv"] = np.zeros((max(ns, 0),) + P)
+        a["cv"] = np.zeros((n_var,) + P)
+        a["qn"] = np.zeros((n_var,) + P)
+        a["dq"] = np.zeros((n_var,) + I)
+        a["jac"] = np.zeros(P)
+        a["metric"] = np.zeros(P, dtype=METRIC_DTYPE)
+        for n in ("vel", "acoustic_speed", "mach", "mul", "thermal_conductivity"):
+            a[n] = np.zeros(P)
+        if ns:
+            a["rho_D"] = np.zeros((ns,) + P)
+            a["gamma"] = np.zeros(P)
+            a["cp"] = np.zeros(P)
+        a["dt_local"] = np.zeros(I)
+        a["bv_last"] = np.zeros((4,) + I)
+        return b
+
+    def copy(self) -> "HostBlock":
+        b = HostBlock(self.mx, self.my, self.mz, self.ngg, self.n_var, self.n_spec)
+        b.arrays = {k: v.copy() for k, v in self.arrays.items()}
+        return b
+
+    def zone(self) -> Zone:
+        z = Zone()
+        z.mx, z.my, z.mz, z.ngg, z.dq_ngg = self.mx, self.my, self.mz, self.ngg, 0
+        for n, v in self.arrays.items():
+            if v.size:
+                setattr(z, n, v.ctypes.data)
+        return z
+
+
+class DeviceBlock:
+    """One block on the GPU (torch-owned memory), same layout as HostBlock."""
+
+    def __init__(self, host: HostBlock, device="cuda"):
+        import torch
+
+        self.host_shape = host
+        self.mx, self.my, self.mz, self.ngg = host.mx, host.my, host.mz, host.ngg
+        self.t = {}
+        for n, v in host.arrays.items():
+            if n == "metric":
+                raw = np.ascontiguousarray(v).view(np.uint8)
+                self.t[n] = torch.from_numpy(raw.copy()).to(device)
+            else:
+                self.t[n] = torch.from_numpy(np.ascontiguousarray(v)).to(device)
+
+    def zone(self) -> Zone:
+        z = Zone()
+        z.mx, z.my, z.mz, z.ngg, z.dq_ngg = self.mx, self.my, self.mz, self.ngg, 0
+        for n, v in self.t.items():
+            if v.numel():
+                setattr(z, n, v.data_ptr())
+        return z
+
+    def download(self, name) -> np.ndarray:
+        v = self.t[name].cpu().numpy()
+        if name == "metric":
+            return v.view(METRIC_DTYPE).reshape(self.host_shape.arrays["metric"].shape)
+        return v
+
+    def upload(self, name, arr: np.ndarray):
+        import torch
+
+        self.t[name].copy_(torch.from_numpy(np.ascontiguousarray(arr)))
+
+
+# ---------------------------------------------------------------------------
+# boundary faces
+# ---------------------------------------------------------------------------
+def bc_face(block: int, label: int, face: int, direction: int, ext, ngg, state: Optional[dict] = None) -> BcFaceC:
+    """A face of one block after Boundary::register_boundary (src/Mesh.cpp:14-32):
+    the tangential ranges are widened by ngg."""
+    f = BcFaceC()
+    f.block, f.type_label, f.face, f.direction = block, label, face, direction
+    for d in range(3):
+        if d == face:
+            v = 0 if direction < 0 else ext[d] - 1
+            f.range_start[d] = v
+            f.range_end[d] = v
+        else:
+            f.range_start[d] = -ngg
+            f.range_end[d] = ext[d] - 1 + ngg
+    if state:
+        for k in ("density", "u", "v", "w", "pressure", "temperature", "velocity", "mut"):
+            setattr(f, k, float(state.get(k, 0.0)))
+        for l, y in enumerate(state.get("sv", [])):
+            f.sv[l] = float(y)
+    return f
+
+
+# ---------------------------------------------------------------------------
+# the solver (one ostc_ctx)
+# ---------------------------------------------------------------------------
+class Solver:
+    def __init__(self, scheme: Scheme, mech: Optional[Mechanism], blocks: List[DeviceBlock], faces: List[BcFaceC],
+                 output_screen: int = 1):
+        import torch
+
+        self.scheme = scheme
+        self.blocks = blocks
+        self.param, self._keep = make_param(scheme, mech)
+        self.config = make_config(scheme, output_screen)
+        zones = (Zone * len(blocks))(*[b.zone() for b in blocks])
+        self._zones = zones
+        fa = (BcFaceC * max(len(faces), 1))(*faces)
+        self._faces = fa
+        ctx = C.c_void_p()
+        check(lib().ostc_create(C.byref(self.config), C.byref(self.param), zones, len(blocks), fa, len(faces),
+                                C.byref(ctx)), "ostc_create")
+        self.ctx = ctx
+        self.stream = torch.cuda.current_stream().cuda_stream
+
+    def close(self):
+        if self.ctx:
+            lib().ostc_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _s(self):
+        import torch
+
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def initialize(self):
+        check(lib().ostc_initialize(self.ctx, self._s()), "ostc_initialize")
+
+    def compute_rhs(self):
+        check(lib().ostc_compute_rhs(self.ctx, self._s()), "ostc_compute_rhs")
+
+    def compute_cv_from_bv(self):
+        check(lib().ostc_compute_cv_from_bv(self.ctx, self._s()), "ostc_compute_cv_from_bv")
+
+    def global_time_step(self) -> float:
+        dt = C.c_double()
+        check(lib().ostc_global_time_step(self.ctx, C.byref(dt), self._s()), "ostc_global_time_step")
+        return dt.value
+
+    def update_cv_and_bv_rk(self, dt: float, rk: int):
+        check(lib().ostc_update_cv_and_bv_rk(self.ctx, dt, rk, self._s()), "ostc_update_cv_and_bv_rk")
+
+    def apply_boundary_conditions(self, with_cv: bool):
+        check(lib().ostc_apply_boundary_conditions(self.ctx, int(with_cv), self._s()), "ostc_apply_bc")
+
+    def update_physical_properties(self):
+        check(lib().ostc_update_physical_properties(self.ctx, self._s()), "ostc_update_physical_properties")
+
+    def rk3_stage(self, rk: int):
+        check(lib().ostc_rk3_stage(self.ctx, rk, self._s()), "ostc_rk3_stage")
+
+    def rk3_steps(self, n: int, history: bool = False):
+        if history:
+            res = (C.c_double * (4 * n))()
+            dts = (C.c_double * n)()
+            check(lib().ostc_rk3_steps(self.ctx, n, res, dts, self._s()), "ostc_rk3_steps")
+            return np.array(res).reshape(n, 4), np.array(dts)
+        check(lib().ostc_rk3_steps(self.ctx, n, None, None, self._s()), "ostc_rk3_steps")
+        return None
+
+    def set_tile(self, d, rows, chunks):
+        check(lib().ostc_set_tile(self.ctx, d, rows, chunks), "ostc_set_tile")
+
+    def get_tile(self, d):
+        r, c = C.c_int(), C.c_int()
+        check(lib().ostc_get_tile(self.ctx, d, C.byref(r), C.byref(c)), "ostc_get_tile")
+        return r.value, c.value
+
+    def autotune(self, warmup: int = 1, reps: int = 3, verbose: bool = False):
+        """Pick per-direction flux tile shapes (rows, chunks) by timing one RHS
+        evaluation with CUDA events on the launching stream. Leaves the state
+        as it found it (the RHS only writes dq)."""
+        import torch
+
+        blk = self.blocks[0]
+        ext = (blk.mx, blk.my, blk.mz)
+        best = {}
+        for d in range(3):
+            n = ext[d]
+            cands = []
+            rows_list = (2, 4, 8) if d == 0 else (4, 8)
+            for R in rows_list:
+                span = 32 if d == 0 else R
+                cmax = max(1, (n + 1 + span - 1) // span)
+                c = 1
+                while True:
+                    cands.append((R, min(c, cmax)))
+                    if c >= cmax:
+                        break
+                    c *= 2
+            cands = sorted(set(cands))
+            times = []
+            for R, Cc in cands:
+                self.set_tile(d, R, Cc)
+                for _ in range(warmup):
+                    self.compute_rhs()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    self.compute_rhs()
+                e1.record()
+                torch.cuda.synchronize()
+                times.append((e0.elapsed_time(e1) / reps, R, Cc))
+            times.sort()
+            best[d] = times[0]
+            self.set_tile(d, times[0][1], times[0][2])
+            if verbose:
+                print("dir", d, "best", times[0], "of", len(times))
+        return best
+
+
+# ---------------------------------------------------------------------------
+# synthetic workloads
+# ---------------------------------------------------------------------------
+def grid_coordinates(mx, my, mz, ng, dx, warp=0.02, periodic_k=True):
+    """Node coordinates with ng ghost layers: x = i dx plus a 2% sinusoidal
+    curvilinear warp, periodic in k with period mz*dx (nodes k = 0..mz-1
+    are distinct), analytic in the ghost layers."""
+    i = np.arange(-ng, mx + ng, dtype=np.float64)
+    j = np.arange(-ng, my + ng, dtype=np.float64)
+    k = np.arange(-ng, mz + ng, dtype=np.float64)
+    K, J, I = np.meshgrid(k, j, i, indexing="ij")
+    Lx, Ly, Lz = (mx - 1) * dx, (my - 1) * dx, mz * dx
+    x0, y0, z0 = I * dx, J * dx, K * dx
+    sx, sy, sz = np.sin(2 * np.pi * x0 / Lx), np.sin(2 * np.pi * y0 / Ly), np.sin(2 * np.pi * z0 / Lz)
+    x = x0 + warp * dx * sy * sz
+    y = y0 + warp * dx * sx * sz
+    z = z0 + warp * dx * sx * sy
+    return x, y, z
+
+
+def fill_metric(block: HostBlock, x, y, z):
+    check(lib().ostc_metric_from_grid(block.mx, block.my, block.mz, block.ngg, x.ctypes.data, y.ctypes.data,
+                                      z.ctypes.data, block.arrays["jac"].ctypes.data,
+                                      block.arrays["metric"].ctypes.data), "ostc_metric_from_grid")
+
+
+@dataclass
+class Case:
+    name: str
+    scheme: Scheme
+    mech: Optional[Mechanism]
+    blocks: List[HostBlock]
+    faces: List[BcFaceC]
+    steps: int
+
+    @property
+    def cells(self):
+        return sum(b.mx * b.my * b.mz for b in self.blocks)
+
+
+def air_state(mach, T, p):
+    a = math.sqrt(GAMMA_AIR * R_U / MW_AIR * T)
+    rho = p * MW_AIR / (R_U * T)
+    return dict(density=rho, u=mach * a, v=0.0, w=0.0, pressure=p, temperature=T, velocity=mach * a, mut=0.0)
+
+
+def case_vortex(mx=128, my=128, mz=8, dx=1e-3, k_bc="periodic", steps=100, fixed_dt=None) -> Case:
+    """The single-species air workload: a Mach 2 stream (T = 300 K,
+    p = 101325 Pa) along +x with an isentropic vortex (strength 0.3 U_inf,
+    radius 5 dx) at the domain centre; AWENO-5 with the Roe tag (which runs
+    AUSM+ in the reference, quirk A1), laminar Sutherland viscosity, RK3 at
+    CFL 0.5. Supersonic inlet at i-min, supersonic outlet at i-max, symmetry
+    on the j faces, periodic in k (k_bc="periodic") or symmetry in k
+    (k_bc="symmetry", a configuration the reference itself can run)."""
+    s = Scheme(mix_model=MIX_AIR, inviscid_scheme=2, reconstruction=4, viscous_order=2, cfl=0.5)
+    if fixed_dt:
+        s.fixed_time_step, s.dt = 1, fixed_dt
+    ng = s.ngg
+    b = HostBlock.allocate(mx, my, mz, ng, 5, 0)
+    x, y, z = grid_coordinates(mx, my, mz, ng + 1, dx, periodic_k=True)
+    fill_metric(b, x, y, z)
+    inf = air_state(2.0, 300.0, 101325.0)
+    # state on all points incl. ghosts (coordinates with ng layers)
+    xs, ys = x[1:-1, 1:-1, 1:-1], y[1:-1, 1:-1, 1:-1]
+    xc, yc = (mx // 2) * dx, (my // 2) * dx
+    R, beta = 5 * dx, 0.3
+    U = inf["u"]
+    r2 = ((xs - xc) ** 2 + (ys - yc) ** 2) / R ** 2
+    ex = np.exp(0.5 * (1 - r2))
+    Rg = R_U / MW_AIR
+    T = 300.0 - (GAMMA_AIR - 1) / (2 * GAMMA_AIR) * (beta * U) ** 2 / Rg * ex ** 2
+    rho = inf["density"] * (T / 300.0) ** (1 / (GAMMA_AIR - 1))
+    bv = b.arrays["bv"]
+    bv[0] = rho
+    bv[1] = U - beta * U * (ys - yc) / R * ex
+    bv[2] = beta * U * (xs - xc) / R * ex
+    bv[3] = 0.0
+    bv[4] = rho * Rg * T
+    bv[5] = T
+    ext = (mx, my, mz)
+    faces = [bc_face(0, BC_INFLOW, 0, -1, ext, ng, inf), bc_face(0, BC_OUTFLOW, 0, 1, ext, ng),
+             bc_face(0, BC_SYMMETRY, 1, -1, ext, ng), bc_face(0, BC_SYMMETRY, 1, 1, ext, ng)]
+    if k_bc == "periodic":
+        faces += [bc_face(0, BC_PERIODIC, 2, -1, ext, ng), bc_face(0, BC_PERIODIC, 2, 1, ext, ng)]
+    else:
+        faces += [bc_face(0, BC_SYMMETRY, 2, -1, ext, ng), bc_face(0, BC_SYMMETRY, 2, 1, ext, ng)]
+    return Case("vortex_air_%dx%dx%d" % (mx, my, mz), s, None, [b], faces, steps)
