@@ -1,0 +1,388 @@
+"""Throughput of the RHS / RK3 time-advance path on B200.
+
+One step = one full SSPRK3 step (three RHS evaluations, CFL time step,
+stage updates, boundary conditions, properties) of the reacting mixing-layer
+workload at 256^3 cells (9 species, 19 reactions, MUSCL + AUSM+, laminar,
+finite-rate chemistry), FP64. Metric: Mcell-updates/s = cells x steps / s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs (torchrun) are independent replicas, one per rank: the
+single-GPU path has no exchange step of its own (replicas only); value is
+the sum of cell updates over all ranks divided by the max time over ranks.
+
+--impl reference times the reference's own physics as FP64 host code
+(oracle/_ref, the reference sources compiled by oracle/build_ref.sh) with
+OpenMP on all host cores, or the oracle port when that library is absent,
+on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "openstc-dev_b200"))
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixing256", choices=["mixing256", "vortex128"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def _peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def _make_case(name, full_host=False):
+    import ostc
+
+    if name == "mixing256":
+        return ostc.case_mixing_layer(256, 256, 256, full_host=full_host)
+    return ostc.case_vortex(128, 128, 8)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        if not self.rows:
+            return None
+        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
+        mx = max(float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in self.rows for q in range(4) if len(r) > 5 + q and r[5 + q] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# per-kernel timing and the roofline of the dominant kernel
+# ---------------------------------------------------------------------------
+def kernel_table(solver, case, reps=3):
+    """Average device time of each kernel family (CUDA events on the launching
+    stream, state left in a valid post-stage condition)."""
+    import torch
+
+    ops = [("flux_x", solver.OP_FLUX, 0, 3), ("flux_y", solver.OP_FLUX, 1, 3), ("flux_z", solver.OP_FLUX, 2, 3),
+           ("properties", solver.OP_PROPERTIES, 0, 3), ("update_rk", solver.OP_UPDATE, 1, 3),
+           ("dt", solver.OP_DT, 0, 3), ("bc", solver.OP_BC, 1, 3)]
+    if case.scheme.mix_model == 2:
+        ops.insert(3, ("source", solver.OP_SOURCE, 0, 3))
+    out = {}
+    for name, op, arg, per_step in ops:
+        solver.launch_op(op, arg)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            solver.launch_op(op, arg)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = {"ms": e0.elapsed_time(e1) / reps, "per_step": per_step}
+    return out
+
+
+def algorithmic_bytes(name, case):
+    """Minimum HBM bytes of one launch of a kernel family on this workload
+    (each input plane read once, each output plane written once)."""
+    b = case.blocks[0]
+    ns = case.mech.n_spec if case.mech else 0
+    nv = 5 + ns
+    cells = b.mx * b.my * b.mz
+    props = 2 + (ns + 2 if ns else 0)  # mu, kappa (+ rho*D_k, cp, gamma)
+    per_cell = {
+        # state (bv 6, sv), geometry (9 metric + jac), properties read; dq read+written
+        "flux_x": 6 + ns + 10 + props + 2 * nv,
+        "flux_y": 6 + ns + 10 + props + 2 * nv,
+        "flux_z": 6 + ns + 10 + props + 2 * nv,
+        "source": 2 + ns + 1 + nv,
+        "properties": 6 + ns + 1 + props + 3,
+        "update_rk": 3 * nv + 1 + nv + 6 + ns + 1,
+        "dt": 9 + 6 + 3,
+        "bc": 0,
+    }[name]
+    return 8.0 * per_cell * cells
+
+
+# ---------------------------------------------------------------------------
+# the timed run
+# ---------------------------------------------------------------------------
+def run_ours(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import ostc
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    case = _make_case(a.workload)
+    blocks = [ostc.DeviceBlock(b) for b in case.blocks]
+    solver = ostc.Solver(case.scheme, case.mech, blocks, case.faces)
+    solver.initialize()
+    solver.autotune(warmup=1, reps=2)
+    solver.initialize()  # autotuning ran RHS evaluations only; re-derive the same start state
+    torch.cuda.synchronize()
+    solver.rk3_steps(max(a.warmup, 3))
+    torch.cuda.synchronize()
+    launches_per_step = solver.step_kernel_count(False)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    solver.rk3_steps(a.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    ck = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = case.cells
+    value = cells * a.steps * world / (ms * 1e-3) / 1e6
+
+    # per-kernel table and roofline of the dominant kernel (HBM-bound stencils)
+    ktab = kernel_table(solver, case)
+    dom = max(ktab, key=lambda k: ktab[k]["ms"] * ktab[k]["per_step"])
+    hbm, src = _peaks()
+    alg = algorithmic_bytes(dom, case)
+    achieved = alg / (ktab[dom]["ms"] * 1e-3) / 1e9
+    traffic = None
+    tf = REPO / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            tt = json.loads(tf.read_text()).get(a.workload, {}).get(dom)
+            traffic = float(tt) if tt is not None else None
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_source": src, "traffic": traffic,
+                "alg_bytes_per_launch": alg, "launch_ms": round(ktab[dom]["ms"], 4)}
+
+    # end to end through the public API from host buffers
+    tiles = [solver.get_tile(d) for d in range(3)]
+    solver.close()
+    del blocks
+    torch.cuda.empty_cache()
+    e2e = None
+    if not a.no_e2e:
+        e2e = run_e2e(a, case, tiles)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cpu = cpu_baseline(a)
+
+    if rank == 0:
+        line = {"metric": "Mcell-updates/s per RK3 step (plain FP64 chemistry)", "value": round(value, 2),
+                "unit": "Mcell-updates/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": case.name, "cells_per_gpu": cells,
+                           "n_spec": case.mech.n_spec if case.mech else 0,
+                           "n_reac": case.mech.n_reac if case.mech else 0,
+                           "scheme": "MUSCL(minmod)+AUSM+, laminar, finite-rate chemistry, SSPRK3 CFL %.1f"
+                                     % case.scheme.cfl if case.mech else "AWENO5+AUSM+, laminar, SSPRK3",
+                           "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "inputs larger than L2 (%.1f GB state), no flush" % (state_bytes(case) / 1e9)},
+                "gpu_launches": launches_per_step * a.steps, "launches_per_step": launches_per_step,
+                "tiles": tiles,
+                "clocks": ck, "roofline": roofline, "kernels_ms": {k: round(v["ms"], 4) for k, v in ktab.items()},
+                "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def state_bytes(case):
+    b = case.blocks[0]
+    ns = case.mech.n_spec if case.mech else 0
+    return 8.0 * (6 + ns + 10 + 2 * (5 + ns)) * (b.mx + 2 * b.ngg) * (b.my + 2 * b.ngg) * (b.mz + 2 * b.ngg)
+
+
+def run_e2e(a, case, tiles=None):
+    """Whole job through the public API from pinned host buffers: upload of the
+    initial state and geometry, initialisation, the steps, download of the
+    final primitive state and the residual history; timed with CUDA events."""
+    import numpy as np
+    import torch
+
+    import ostc
+
+    host = case.blocks[0]
+    pinned = {n: torch.from_numpy(v.view(np.uint8).reshape(-1) if n == "metric" else v).pin_memory()
+              for n, v in host.arrays.items()}
+    blocks = [ostc.DeviceBlock(ostc.HostBlock(host.mx, host.my, host.mz, host.ngg, host.n_var, host.n_spec))]
+    out_bv = torch.empty_like(blocks[0].t["bv"], device="cpu").pin_memory()
+    out_sv = torch.empty_like(blocks[0].t["sv"], device="cpu").pin_memory()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    h2d = 0
+    for n, t in pinned.items():
+        blocks[0].t[n].copy_(t.view(blocks[0].t[n].dtype).reshape(blocks[0].t[n].shape), non_blocking=True)
+        h2d += t.numel() * t.element_size()
+    solver = ostc.Solver(case.scheme, case.mech, blocks, case.faces)
+    for d, (r, c) in enumerate(tiles or []):
+        solver.set_tile(d, r, c)
+    solver.initialize()
+    res, dts = solver.rk3_steps(a.steps, history=True)
+    out_bv.copy_(blocks[0].t["bv"], non_blocking=True)
+    out_sv.copy_(blocks[0].t["sv"], non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    d2h = out_bv.numel() * 8 + out_sv.numel() * 8 + res.size * 8 + dts.size * 8
+    solver.close()
+    assert np.all(np.isfinite(res)), "non-finite residual in the e2e run"
+    return {"value": round(case.cells * a.steps / (ms * 1e-3) / 1e6, 2), "unit": "Mcell-updates/s",
+            "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(d2h / a.steps),
+            "ms_total": round(ms, 2), "includes": "H2D state+geometry, initialize, steps, D2H bv/sv/residuals"}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (oracle port / reference host build)
+# ---------------------------------------------------------------------------
+def _cpu_engine():
+    sys.path.insert(0, str(REPO / "tests"))
+    ref = REPO / "oracle" / "_ref" / "libostc_ref.so"
+    if ref.exists():
+        import ref_bind
+
+        return "reference", ref_bind.RefRun
+    from oracle_bind import OracleRun
+
+    return "port", OracleRun
+
+
+def cpu_sample(a, budget_s=15.0):
+    """Time the CPU implementation on a bounded sample of the workload: the
+    same case at 64^3 (or the full air case), stepping until ~budget_s."""
+    import ostc
+
+    kind, Run = _cpu_engine()
+    if a.workload == "mixing256":
+        case = ostc.case_mixing_layer(64, 64, 64, full_host=True)
+    else:
+        case = ostc.case_vortex(128, 128, 8)
+    r = Run(case)
+    r.initialize()
+    threads = r.threads() if hasattr(r, "threads") else 1
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        r.rk3_steps(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or steps >= 50:
+            break
+    value = case.cells * steps / el / 1e6
+    return {"value": round(value, 4), "unit": "Mcell-updates/s", "cores": threads, "kind": kind,
+            "sample": "%s, %d RK3 steps, %.1f s" % (case.name, steps, el)}
+
+
+def cpu_baseline(a):
+    return cpu_sample(a)
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    samples = []
+    vals = []
+    for _ in range(max(1, min(a.steps, 3))):
+        c = cpu_sample(a, budget_s=20.0)
+        vals.append(c["value"])
+        samples.append(c)
+    value = sorted(vals)[len(vals) // 2]
+    c = samples[0]
+    line = {"impl": "reference", "metric": "Mcell-updates/s per RK3 step (plain FP64 chemistry)", "value": value,
+            "unit": "Mcell-updates/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": a.steps,
+            "warmup": a.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": _make_case_name(a.workload), "sample": c["sample"]},
+            "cpu_baseline": {"value": value, "unit": c["unit"], "cores": c["cores"], "kind": c["kind"],
+                             "sample": c["sample"]},
+            "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def _make_case_name(w):
+    return "mixing_layer_h2air_256x256x256" if w == "mixing256" else "vortex_air_128x128x8"
+
+
+if __name__ == "__main__":
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)

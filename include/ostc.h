@@ -224,7 +224,8 @@ ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream);
 /* ----------------------------------------------------------------------- */
 
 /* Driver::initialize_computation (src/Driver.cu:39-98) followed by the
- * pre-loop of RK3_bv (src/RK.cuh:235-244).                                */
+ * pre-loop of RK3_bv (src/RK.cuh:235-244). Also re-reads the metric records
+ * (so they may be written after ostc_create).                             */
 ostc_status ostc_initialize(ostc_ctx *ctx, void *stream);
 
 /* One SSPRK3 stage: RHS, dt (if CFL), update, BCs, interfaces, properties. */
@@ -252,6 +253,19 @@ ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg,
  * autotuner (openstc-dev_b200/ostc.py: autotune) or by hand; resets graphs. */
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks);
 ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks);
+
+/* Launch one kernel family on every block (timing and autotuning aid):
+ * OSTC_OP_FLUX (arg = direction, accumulates into dq), OSTC_OP_SOURCE,
+ * OSTC_OP_PROPERTIES, OSTC_OP_UPDATE (arg = rk stage), OSTC_OP_DT,
+ * OSTC_OP_BC (arg = with_cv). No reference counterpart: the reference
+ * launches these only from its stage loop (src/RK.cuh:301-355).            */
+enum { OSTC_OP_FLUX = 0, OSTC_OP_SOURCE = 1, OSTC_OP_PROPERTIES = 2, OSTC_OP_UPDATE = 3, OSTC_OP_DT = 4,
+       OSTC_OP_BC = 5 };
+ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream);
+
+/* Number of kernel nodes in the CUDA graph of one RK3 step (with or without
+ * the residual epilogue); captures the graph if it does not exist yet.     */
+ostc_status ostc_step_kernel_count(ostc_ctx *ctx, int with_hist, int *count);
 
 /* Library version string. */
 const char *ostc_version(void);

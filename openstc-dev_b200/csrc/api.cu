@@ -294,6 +294,18 @@ void default_tiles(ostc_ctx *c) {
 
 cudaStream_t S(void *s) { return (cudaStream_t)s; }
 
+// the metric is immutable input: its SoA copy is refreshed at create and at
+// every initialize, so callers may fill the 80-byte records after ostc_create
+ostc_status repack_metrics(ostc_ctx *ctx, cudaStream_t s) {
+  for (size_t b = 0; b < ctx->dz.size(); ++b) {
+    const long long n = ctx->dz[b].sz;
+    repack_metric_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+        (const unsigned char *)ctx->zones[b].metric, ctx->met_soa[b], n);
+    CK(cudaGetLastError());
+  }
+  return OSTC_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -335,9 +347,6 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
     double *soa = nullptr;
     CK(cudaMalloc(&soa, sizeof(double) * 9 * c->dz[b].sz));
     c->met_soa.push_back(soa);
-    const long long n = c->dz[b].sz;
-    repack_metric_kernel<<<(unsigned)((n + 255) / 256), 256>>>((const unsigned char *)zones[b].metric, soa, n);
-    CK(cudaGetLastError());
     c->dz[b].met = soa;
     c->n_total += (double)zones[b].mx * zones[b].my * zones[b].mz;
   }
@@ -368,6 +377,7 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
     c->faces.push_back(b);
     c->face_zone.push_back(f.block);
   }
+  if ((st = repack_metrics(ctx, nullptr))) return st;
   CK(cudaMalloc(&c->dt_bits, sizeof(unsigned long long)));
   c->n_part_per_zone = 148 * 2;
   CK(cudaMalloc(&c->res_partial, sizeof(double) * 4 * c->n_part_per_zone * n_zones));
@@ -498,6 +508,7 @@ ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream) {
 ostc_status ostc_initialize(ostc_ctx *ctx, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;
   ostc_status st;
+  if ((st = repack_metrics(ctx, S(stream)))) return st;
   if ((st = ostc_apply_boundary_conditions(ctx, 0, stream))) return st;
   if (ensure_param(ctx, S(stream))) return ctx->last;
   for (auto &z : ctx->dz)
@@ -546,26 +557,24 @@ static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
   return OSTC_OK;
 }
 
-ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist, double *dt_hist, void *stream) {
-  if (!ctx || n_steps < 0) return OSTC_ERR_INVALID_ARG;
-  cudaStream_t s = S(stream);
-  const bool hist = res_hist || dt_hist;
-  if (hist && n_steps > ctx->hist_cap) {
-    cudaFree(ctx->hist_res);
-    cudaFree(ctx->hist_dt);
-    ctx->hist_res = ctx->hist_dt = nullptr;
-    CK(cudaMalloc(&ctx->hist_res, sizeof(double) * 4 * n_steps));
-    CK(cudaMalloc(&ctx->hist_dt, sizeof(double) * n_steps));
-    ctx->hist_cap = n_steps;
-    // cached graphs captured the old buffers
-    for (auto &kv : ctx->graphs) {
-      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-      if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
-    }
-    ctx->graphs.clear();
+static ostc_status ensure_hist(ostc_ctx *ctx, int n_steps) {
+  if (n_steps <= ctx->hist_cap) return OSTC_OK;
+  cudaFree(ctx->hist_res);
+  cudaFree(ctx->hist_dt);
+  ctx->hist_res = ctx->hist_dt = nullptr;
+  CK(cudaMalloc(&ctx->hist_res, sizeof(double) * 4 * n_steps));
+  CK(cudaMalloc(&ctx->hist_dt, sizeof(double) * n_steps));
+  ctx->hist_cap = n_steps;
+  // cached graphs captured the old buffers
+  for (auto &kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
-  if (ensure_param(ctx, s)) return ctx->last;
-  if (hist) CK(cudaMemsetAsync(ctx->hist_counter, 0, sizeof(int), s));
+  ctx->graphs.clear();
+  return OSTC_OK;
+}
+
+static ostc_status ensure_graph(ostc_ctx *ctx, bool hist, GraphEntry **out) {
   GraphEntry &ge = ctx->graphs[hist ? 1 : 0];
   if (!ge.exec) {
     // a legacy default stream cannot be captured: capture on a private stream
@@ -581,7 +590,21 @@ ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist, double 
     CK(cudaGraphInstantiate(&ge.exec, g, 0));
     ge.graph = g;
   }
-  for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(ge.exec, s));
+  *out = &ge;
+  return OSTC_OK;
+}
+
+ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist, double *dt_hist, void *stream) {
+  if (!ctx || n_steps < 0) return OSTC_ERR_INVALID_ARG;
+  cudaStream_t s = S(stream);
+  const bool hist = res_hist || dt_hist;
+  ostc_status st;
+  if (hist && (st = ensure_hist(ctx, n_steps))) return st;
+  if (ensure_param(ctx, s)) return ctx->last;
+  if (hist) CK(cudaMemsetAsync(ctx->hist_counter, 0, sizeof(int), s));
+  GraphEntry *ge = nullptr;
+  if ((st = ensure_graph(ctx, hist, &ge))) return st;
+  for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(ge->exec, s));
   if (hist) {
     if (res_hist) CK(cudaMemcpyAsync(res_hist, ctx->hist_res, sizeof(double) * 4 * n_steps, cudaMemcpyDeviceToHost, s));
     if (dt_hist) CK(cudaMemcpyAsync(dt_hist, ctx->hist_dt, sizeof(double) * n_steps, cudaMemcpyDeviceToHost, s));
@@ -590,9 +613,56 @@ ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist, double 
   return OSTC_OK;
 }
 
+// one kernel family on every block, for per-kernel timing and the autotuner
+ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  const int inv = ctx->prm.inviscid_type;
+  const int vis = ctx->prm.viscous_scheme != 0;
+  switch (op) {
+    case OSTC_OP_FLUX:
+      if (arg < 0 || arg > 2) return OSTC_ERR_INVALID_ARG;
+      for (auto &z : ctx->dz)
+        CK(dispatch_ns(ctx->ns, [&](auto n) {
+          return launch_flux<decltype(n)::value>(z, inv, arg, ctx->tile[arg], 1, vis, S(stream));
+        }));
+      return OSTC_OK;
+    case OSTC_OP_SOURCE:
+      for (auto &z : ctx->dz)
+        CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, {}, S(stream)); }));
+      return OSTC_OK;
+    case OSTC_OP_PROPERTIES: return ostc_update_physical_properties(ctx, stream);
+    case OSTC_OP_UPDATE: return ostc_update_cv_and_bv_rk(ctx, ctx->cfg.fixed_time_step ? ctx->cfg.dt : -1, arg, stream);
+    case OSTC_OP_DT: return ostc_global_time_step(ctx, nullptr, stream);
+    case OSTC_OP_BC: return ostc_apply_boundary_conditions(ctx, arg, stream);
+    default: return OSTC_ERR_INVALID_ARG;
+  }
+}
+
+// kernel launches in one captured step (captures the graph if needed)
+ostc_status ostc_step_kernel_count(ostc_ctx *ctx, int with_hist, int *count) {
+  if (!ctx || !count) return OSTC_ERR_INVALID_ARG;
+  ostc_status st;
+  if (with_hist && (st = ensure_hist(ctx, 1))) return st;
+  GraphEntry *ge = nullptr;
+  if ((st = ensure_graph(ctx, with_hist != 0, &ge))) return st;
+  size_t n = 0;
+  CK(cudaGraphGetNodes(ge->graph, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  CK(cudaGraphGetNodes(ge->graph, nodes.data(), &n));
+  int k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    CK(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) ++k;
+  }
+  *count = k;
+  return OSTC_OK;
+}
+
 // tile-shape control for the autotuner: dir 0..2
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
-  if (!ctx || dir < 0 || dir > 2 || chunks < 1 || chunks > 64) return OSTC_ERR_INVALID_ARG;
+  if (!ctx || dir < 0 || dir > 2 || chunks < 1 || chunks > 4096) return OSTC_ERR_INVALID_ARG;
   if (!(rows == 1 || rows == 2 || rows == 4 || rows == 8)) return OSTC_ERR_INVALID_ARG;
   ctx->tile[dir] = {rows, chunks};
   for (auto &kv : ctx->graphs) {

@@ -1,0 +1,18 @@
+"""Regenerates h2_air_9sp.json: the species/reaction tables of the 9-species,
+19-reaction H2-air CHEMKIN mechanism (combustion_mechanism.inp + therm.dat +
+tran.dat of the reference's input_files/chemistry), parsed by chemdata.py.
+
+usage: python make_mechanism.py <dir holding the three CHEMKIN files>
+"""
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent))
+
+import chemdata  # noqa: E402
+
+src = Path(sys.argv[1])
+mech = chemdata.load_chemkin(src / "combustion_mechanism.inp", src / "therm.dat", src / "tran.dat")
+chemdata.save_json(mech, HERE / "h2_air_9sp.json")
+print(mech.names, mech.n_reac)

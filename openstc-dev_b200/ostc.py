@@ -116,6 +116,8 @@ def lib():
             "ostc_get_error": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)],
             "ostc_set_tile": [vp, i, i, i],
             "ostc_get_tile": [vp, i, C.POINTER(i), C.POINTER(i)],
+            "ostc_launch_op": [vp, i, i, vp],
+            "ostc_step_kernel_count": [vp, i, C.POINTER(i)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -262,33 +264,44 @@ class HostBlock:
         return plane_shape(self.mx, self.my, self.mz, self.ngg if g is None else g)
 
     @staticmethod
-    def allocate(mx, my, mz, ngg, n_var, n_spec) -> "HostBlock":
-        b = HostBlock(mx, my, mz, ngg, n_var, n_spec)
+    def specs(mx, my, mz, ngg, n_var, n_spec):
+        """name -> (shape, dtype) of every array of a block (Field::setup_device_memory)."""
         P = plane_shape(mx, my, mz, ngg)
         I = plane_shape(mx, my, mz, 0)
-        ns = n_spec
-        a = b.arrays
-        a["bv"] = np.zeros((6,) + P)
-        a["sv"] = np.zeros((max(ns, 0),) + P)
-        a["cv"] = np.zeros((n_var,) + P)
-        a["qn"] = np.zeros((n_var,) + P)
-        a["dq"] = np.zeros((n_var,) + I)
-        a["jac"] = np.zeros(P)
-        a["metric"] = np.zeros(P, dtype=METRIC_DTYPE)
+        f8 = np.float64
+        sp = {"bv": ((6,) + P, f8), "sv": ((n_spec,) + P, f8), "cv": ((n_var,) + P, f8),
+              "qn": ((n_var,) + P, f8), "dq": ((n_var,) + I, f8), "jac": (P, f8), "metric": (P, METRIC_DTYPE)}
         for n in ("vel", "acoustic_speed", "mach", "mul", "thermal_conductivity"):
-            a[n] = np.zeros(P)
-        if ns:
-            a["rho_D"] = np.zeros((ns,) + P)
-            a["gamma"] = np.zeros(P)
-            a["cp"] = np.zeros(P)
-        a["dt_local"] = np.zeros(I)
-        a["bv_last"] = np.zeros((4,) + I)
+            sp[n] = (P, f8)
+        if n_spec:
+            sp["rho_D"] = ((n_spec,) + P, f8)
+            sp["gamma"] = (P, f8)
+            sp["cp"] = (P, f8)
+        sp["dt_local"] = (I, f8)
+        sp["bv_last"] = ((4,) + I, f8)
+        return sp
+
+    INPUTS = ("bv", "sv", "jac", "metric")
+
+    @staticmethod
+    def allocate(mx, my, mz, ngg, n_var, n_spec, full=True) -> "HostBlock":
+        """full=False holds only the inputs (bv, sv, jac, metric); the device
+        block creates the rest zero-filled."""
+        b = HostBlock(mx, my, mz, ngg, n_var, n_spec)
+        for n, (shape, dt) in HostBlock.specs(mx, my, mz, ngg, n_var, n_spec).items():
+            if full or n in HostBlock.INPUTS:
+                b.arrays[n] = np.zeros(shape, dtype=dt)
+        return b
+
+    def complete(self) -> "HostBlock":
+        """a full copy (all arrays) for the oracle"""
+        b = HostBlock.allocate(self.mx, self.my, self.mz, self.ngg, self.n_var, self.n_spec, full=True)
+        for n, v in self.arrays.items():
+            b.arrays[n][...] = v
         return b
 
     def copy(self) -> "HostBlock":
-        b = HostBlock(self.mx, self.my, self.mz, self.ngg, self.n_var, self.n_spec)
-        b.arrays = {k: v.copy() for k, v in self.arrays.items()}
-        return b
+        return self.complete()
 
     def zone(self) -> Zone:
         z = Zone()
@@ -307,13 +320,25 @@ class DeviceBlock:
 
         self.host_shape = host
         self.mx, self.my, self.mz, self.ngg = host.mx, host.my, host.mz, host.ngg
+        self.specs = HostBlock.specs(host.mx, host.my, host.mz, host.ngg, host.n_var, host.n_spec)
         self.t = {}
-        for n, v in host.arrays.items():
+        for n, (shape, dt) in self.specs.items():
             if n == "metric":
-                raw = np.ascontiguousarray(v).view(np.uint8)
-                self.t[n] = torch.from_numpy(raw.copy()).to(device)
+                nbytes = int(np.prod(shape)) * METRIC_DTYPE.itemsize
+                self.t[n] = torch.zeros(nbytes, dtype=torch.uint8, device=device)
             else:
-                self.t[n] = torch.from_numpy(np.ascontiguousarray(v)).to(device)
+                self.t[n] = torch.zeros(shape, dtype=torch.float64, device=device)
+        self.upload_inputs(host)
+
+    def upload_inputs(self, host: HostBlock, names=None):
+        import torch
+
+        for n in names or host.arrays.keys():
+            v = host.arrays[n]
+            if n == "metric":
+                self.t[n].copy_(torch.from_numpy(np.ascontiguousarray(v).view(np.uint8).reshape(-1)))
+            else:
+                self.t[n].copy_(torch.from_numpy(np.ascontiguousarray(v)))
 
     def zone(self) -> Zone:
         z = Zone()
@@ -326,7 +351,7 @@ class DeviceBlock:
     def download(self, name) -> np.ndarray:
         v = self.t[name].cpu().numpy()
         if name == "metric":
-            return v.view(METRIC_DTYPE).reshape(self.host_shape.arrays["metric"].shape)
+            return v.view(METRIC_DTYPE).reshape(self.specs["metric"][0])
         return v
 
     def upload(self, name, arr: np.ndarray):
@@ -432,6 +457,16 @@ class Solver:
         check(lib().ostc_rk3_steps(self.ctx, n, None, None, self._s()), "ostc_rk3_steps")
         return None
 
+    OP_FLUX, OP_SOURCE, OP_PROPERTIES, OP_UPDATE, OP_DT, OP_BC = range(6)
+
+    def launch_op(self, op, arg=0):
+        check(lib().ostc_launch_op(self.ctx, op, arg, self._s()), "ostc_launch_op")
+
+    def step_kernel_count(self, with_hist=False):
+        n = C.c_int()
+        check(lib().ostc_step_kernel_count(self.ctx, int(with_hist), C.byref(n)), "ostc_step_kernel_count")
+        return n.value
+
     def set_tile(self, d, rows, chunks):
         check(lib().ostc_set_tile(self.ctx, d, rows, chunks), "ostc_set_tile")
 
@@ -455,7 +490,7 @@ class Solver:
             rows_list = (2, 4, 8) if d == 0 else (4, 8)
             for R in rows_list:
                 span = 32 if d == 0 else R
-                cmax = max(1, (n + 1 + span - 1) // span)
+                cmax = min(64, max(1, (n + 1 + span - 1) // span))
                 c = 1
                 while True:
                     cands.append((R, min(c, cmax)))
@@ -571,3 +606,80 @@ def case_vortex(mx=128, my=128, mz=8, dx=1e-3, k_bc="periodic", steps=100, fixed
     else:
         faces += [bc_face(0, BC_SYMMETRY, 2, -1, ext, ng), bc_face(0, BC_SYMMETRY, 2, 1, ext, ng)]
     return Case("vortex_air_%dx%dx%d" % (mx, my, mz), s, None, [b], faces, steps)
+
+
+# ---------------------------------------------------------------------------
+# the reacting mixing layer (9-species H2-air)
+# ---------------------------------------------------------------------------
+def mixture_state(mech: Mechanism, Y, T, p, mach):
+    """rho, sound speed and velocity of a mixture stream (cfd::Inflow, src/BoundCond.cpp:7-80)."""
+    t = mech.tables
+    mw_inv = float(np.sum(Y / t["mw"]))
+    W = 1.0 / mw_inv
+    cp_i = np.empty(len(Y))
+    for i in range(len(Y)):
+        c = t["low_temp_coeff"][i] if T < t["t_mid"][i] else t["high_temp_coeff"][i]
+        cp_i[i] = (c[0] + c[1] * T + c[2] * T ** 2 + c[3] * T ** 3 + c[4] * T ** 4) * R_U / t["mw"][i]
+    cp = float(np.sum(Y * cp_i))
+    cv = float(np.sum(Y * (cp_i - R_U / t["mw"])))
+    gamma = cp / cv
+    a = math.sqrt(gamma * R_U / W * T)
+    rho = p * W / (R_U * T)
+    return rho, a, mach * a
+
+
+def case_mixing_layer(mx=256, my=256, mz=256, dx=1e-4, seed=2024, steps=200, full_host=False, mech=None,
+                      cfl=0.4) -> Case:
+    """The reacting mixing layer: upper stream (y > 0) air (O2/N2 mass
+    0.233/0.767) at 1500 K, Mach 2; lower stream H2/N2 (mole 0.3/0.7) at
+    300 K, Mach 1.2; p = 1 atm; profiles blended by 0.5(1 + tanh(y / 8dy));
+    seeded 1 % white-noise velocity perturbation (numpy PCG64). 9-species,
+    19-reaction H2-air mechanism, MUSCL (minmod) + AUSM+, laminar viscous
+    flux, point-implicit chemistry tag (explicit under RK3, quirk A8), RK3 at
+    CFL 0.4. Uniform Cartesian grid dx = dy = dz. Extrapolation (outflow)
+    faces in x and y, periodic in z."""
+    import chemdata
+
+    mech = mech or chemdata.h2_air_9sp()
+    s = Scheme(mix_model=MIX_FR, inviscid_scheme=3, reconstruction=2, limiter=0, viscous_order=2, chemSrcMethod=1,
+               cfl=cfl)
+    ng = s.ngg
+    ns = mech.n_spec
+    b = HostBlock.allocate(mx, my, mz, ng, 5 + ns, ns, full=full_host)
+    x, y, z = grid_coordinates(mx, my, mz, ng + 1, dx, warp=0.0)
+    fill_metric(b, x, y, z)
+    names = mech.names
+    Y_air = np.zeros(ns)
+    Y_air[names.index("O2")], Y_air[names.index("N2")] = 0.233, 0.767
+    W = mech.tables["mw"]
+    X_f = np.zeros(ns)
+    X_f[names.index("H2")], X_f[names.index("N2")] = 0.3, 0.7
+    Y_fuel = X_f * W / np.sum(X_f * W)
+    p0 = 101325.0
+    _, _, U_air = mixture_state(mech, Y_air, 1500.0, p0, 2.0)
+    _, _, U_fuel = mixture_state(mech, Y_fuel, 300.0, p0, 1.2)
+    P = b.plane()
+    jj = (np.arange(-ng, my + ng) - my // 2) * dx
+    f = 0.5 * (1 + np.tanh(jj / (8 * dx)))[None, :, None]
+    f = np.broadcast_to(f, P)
+    T = f * 1500.0 + (1 - f) * 300.0
+    sv = b.arrays["sv"]
+    for l in range(ns):
+        sv[l] = f * Y_air[l] + (1 - f) * Y_fuel[l]
+    mw_inv = np.zeros(P)
+    for l in range(ns):
+        mw_inv += sv[l] / W[l]
+    U = f * U_air + (1 - f) * U_fuel
+    rng = np.random.default_rng(seed)
+    bv = b.arrays["bv"]
+    bv[0] = p0 / (R_U * mw_inv * T)
+    bv[1] = U * (1 + 0.01 * rng.uniform(-1, 1, P))
+    bv[2] = 0.01 * U * rng.uniform(-1, 1, P)
+    bv[3] = 0.01 * U * rng.uniform(-1, 1, P)
+    bv[4] = p0
+    bv[5] = T
+    ext = (mx, my, mz)
+    faces = [bc_face(0, BC_OUTFLOW, 0, -1, ext, ng), bc_face(0, BC_OUTFLOW, 0, 1, ext, ng),
+             bc_face(0, BC_OUTFLOW, 1, -1, ext, ng), bc_face(0, BC_OUTFLOW, 1, 1, ext, ng),
+             bc_face(0, BC_PERIODIC, 2, -1, ext, ng), bc_face(0, BC_PERIODIC, 2, 1, ext, ng)]
+    return Case("mixing_layer_h2air_%dx%dx%d" % (mx, my, mz), s, mech, [b], faces, steps)

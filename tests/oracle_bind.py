@@ -57,6 +57,9 @@ class OracleRun:
         self.faces = (ostc.BcFaceC * max(len(case.faces), 1))(*case.faces)
         self.nf = len(case.faces)
 
+    def threads(self):
+        return oracle().oracle_get_threads()
+
     def _ck(self, st, what):
         if st != 0:
             raise RuntimeError("%s -> %d" % (what, st))

@@ -1,0 +1,83 @@
+"""GPU parity of the 9-species H2-air path (MUSCL/NND2/first-order
+reconstruction + AUSM+/HLLC, mixture thermodynamics and transport,
+finite-rate chemistry source, Newton temperature solve) against the CPU
+oracle, through the C ABI.
+
+Tolerances as for air: 1e-11 per RHS evaluation in the conditioning-aware
+normwise measure of tests/oracle_bind.py (rhs_errors); properties 1e-12
+relative; 1e-9 on multi-step histories.
+"""
+import numpy as np
+import pytest
+
+import ostc
+from oracle_bind import OracleRun, normwise, rhs_errors
+
+pytestmark = pytest.mark.gpu
+RHS_TOL = 1e-11
+
+
+def _case(shape, **kw):
+    return ostc.case_mixing_layer(*shape, full_host=True, **kw)
+
+
+def _gpu(case):
+    blocks = [ostc.DeviceBlock(b) for b in case.blocks]
+    return ostc.Solver(case.scheme, case.mech, blocks, case.faces), blocks
+
+
+def test_properties_match():
+    case = _case((24, 20, 8))
+    ref = OracleRun(case)
+    ref.initialize()
+    s, blocks = _gpu(case)
+    s.initialize()
+    hb = ref.blocks[0].arrays
+    for name in ("cv", "mul", "thermal_conductivity", "rho_D", "gamma", "cp", "acoustic_speed"):
+        got = blocks[0].download(name)
+        den = np.max(np.abs(hb[name]))
+        assert np.max(np.abs(got - hb[name])) <= 1e-12 * den, name
+
+
+@pytest.mark.parametrize("rec,flux", [(2, 3), (3, 3), (1, 3), (2, 4), (3, 4)])
+@pytest.mark.parametrize("shape", [(24, 20, 8), (33, 17, 10)])
+def test_rhs_matches_oracle(shape, rec, flux):
+    case = _case(shape)
+    case.scheme.reconstruction = rec
+    case.scheme.inviscid_scheme = flux
+    ref = OracleRun(case)
+    ref.initialize()
+    scale = ref.flux_scale()
+    s, blocks = _gpu(case)
+    s.initialize()
+    s.compute_rhs()
+    err = rhs_errors(blocks[0].download("dq"), ref.blocks[0].arrays["dq"], scale)
+    assert max(err) <= RHS_TOL, err
+
+
+def test_rk3_history_matches_oracle():
+    case = _case((24, 20, 8))
+    n = 6
+    ref = OracleRun(case)
+    ref.initialize()
+    res_o, dt_o = ref.rk3_steps(n)
+    s, blocks = _gpu(case)
+    s.initialize()
+    res_g, dt_g = s.rk3_steps(n, history=True)
+    assert np.max(np.abs(dt_g - dt_o) / dt_o) <= 1e-9
+    assert np.max(np.abs(res_g - res_o) / res_o) <= 1e-9
+    for name in ("bv", "sv"):
+        err = normwise(blocks[0].download(name), ref.blocks[0].arrays[name])
+        assert max(err) <= 1e-9, (name, err)
+
+
+def test_inviscid_only_and_no_reactions():
+    case = _case((20, 16, 8))
+    case.scheme.viscous_order = 0
+    ref = OracleRun(case)
+    ref.initialize()
+    scale = ref.flux_scale()
+    s, blocks = _gpu(case)
+    s.initialize()
+    s.compute_rhs()
+    assert max(rhs_errors(blocks[0].download("dq"), ref.blocks[0].arrays["dq"], scale)) <= RHS_TOL
