@@ -42,6 +42,7 @@ def _args():
     ap.add_argument("--workload", default="mixing256", choices=["mixing256", "vortex128"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-refcuda", action="store_true")
     return ap.parse_args()
 
 
@@ -241,6 +242,9 @@ def run_ours(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_baseline(a)
+    refcuda = None
+    if rank == 0 and world == 1 and not a.no_refcuda:
+        refcuda = reference_cuda_build(a, value)
 
     if rank == 0:
         line = {"metric": "Mcell-updates/s per RK3 step (plain FP64 chemistry)", "value": round(value, 2),
@@ -257,7 +261,7 @@ def run_ours(a):
                 "gpu_launches": launches_per_step * a.steps, "launches_per_step": launches_per_step,
                 "tiles": tiles,
                 "clocks": ck, "roofline": roofline, "kernels_ms": {k: round(v["ms"], 4) for k, v in ktab.items()},
-                "e2e": e2e, "cpu_baseline": cpu}
+                "e2e": e2e, "cpu_baseline": cpu, "reference_cuda_build": refcuda}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
@@ -351,6 +355,33 @@ def cpu_sample(a, budget_s=15.0):
 
 def cpu_baseline(a):
     return cpu_sample(a)
+
+
+def reference_cuda_build(a, ours_value):
+    """The reference's own kernels (sources compiled for sm_100a, driven by
+    oracle/ref_cuda_harness.cu through RK3_bv's per-step sequence) on the same
+    workload, timed with CUDA events; periodic faces become extrapolation
+    faces since the reference has no periodic boundary."""
+    sys.path.insert(0, str(REPO / "tests"))
+    import ref_bind
+
+    if not ref_bind.available():
+        return {"unavailable": "oracle/_ref/libostc_ref_cuda.so not built (needs the reference sources)"}
+    import ostc
+
+    case = _make_case(a.workload)
+    for f in case.faces:
+        if f.type_label == ostc.BC_PERIODIC:
+            f.type_label = ostc.BC_OUTFLOW
+    r = ref_bind.RefCudaRun(case)
+    r.initialize()
+    r.time_steps(1)
+    n = 3
+    ms = r.time_steps(n)
+    v = case.cells * n / (ms * 1e-3) / 1e6
+    return {"value": round(v, 2), "unit": "Mcell-updates/s", "steps": n, "ms_per_step": round(ms / n, 3),
+            "speedup_ours_over_reference_build": round(ours_value / v, 2),
+            "note": "reference sources compiled for sm_100a, same workload, extrapolation faces instead of periodic"}
 
 
 def run_reference(a):

@@ -1,0 +1,428 @@
+// ref_cuda_harness.cu — drives the REFERENCE's own CUDA kernels (compiled
+// for sm_100a from the reference sources by oracle/build_ref.sh) on the same
+// inputs as the B200 path. Test and measurement infrastructure: the tight
+// GPU oracle of the parity tests and the "reference CUDA build" timing.
+//
+// It rebuilds what Driver<mix,turb> sets up (src/Driver.cu:10-35,
+// src/Field.cu:133-251, src/DParameter.cu:7-159) from ostc_param /
+// ostc_zone host data, and repeats the per-step sequence of RK3_bv
+// (src/RK.cuh:284-357) calling the reference's launchers and kernels:
+// compute_source, compute_inviscid_flux, compute_viscous_flux,
+// local_time_step + min_of_arr, update_cv_and_bv_rk, the apply_* boundary
+// kernels in the priority order of DBoundCond::apply_boundary_conditions
+// (src/BoundCond.cuh:673-822) with its launch shapes, and
+// update_physical_properties. Everything runs on the legacy default stream
+// with the reference's implicit synchronisations (the per-stage dt D2H copy).
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+// include order of the reference's own translation units (RK.cuh needs the
+// I/O managers and the time-advance helpers declared first)
+#include "Define.h"
+#include "DParameter.cuh"
+#include "Field.h"
+#include "Mesh.h"
+#include "Parameter.h"
+#include "BoundCond.cuh"
+#include "FieldOperation.cuh"
+#include "TimeAdvanceFunc.cuh"
+#include "IOManager.h"
+#include "RK.cuh"
+#include "Residual.cuh"
+#include "SchemeSelector.cuh"
+#include "SourceTerm.cuh"
+#include "../include/ostc.h"
+
+using namespace cfd;
+
+namespace {
+
+struct RefCtx {
+  ostc_config cfg{};
+  int mix = 0, n_var = 5, n_scalar = 0, n_spec = 0, ngg = 2, mx = 0, my = 0, mz = 0;
+  Parameter *parameter = nullptr;
+  Block *block = nullptr;
+  DZone h{};
+  DZone *d_zone = nullptr;
+  DParameter h_param{};
+  DParameter *d_param = nullptr;
+  std::vector<Boundary> faces;
+  std::vector<int> face_inflow;  // index into inflows, or -1
+  std::vector<Inflow *> d_inflows;
+  std::vector<double *> d_inflow_sv;
+};
+
+template <typename T>
+T *dcopy(const T *src, size_t n) {
+  T *d = nullptr;
+  cudaMalloc(&d, n * sizeof(T));
+  cudaMemcpy(d, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  return d;
+}
+
+template <typename M, typename T>
+void fill_matrix(M &m, const T *src, int r, int c) {
+  m.init_with_size(r, c);
+  cudaMemcpy(m.data(), src, sizeof(T) * r * c, cudaMemcpyHostToDevice);
+}
+
+size_t plane(int mx, int my, int mz, int g) { return (size_t)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g); }
+
+void build_param(RefCtx &c, const ostc_param *p) {
+  DParameter &d = c.h_param;
+  d.dim = 3;
+  d.n_var = p->n_var;
+  d.n_scalar = p->n_scalar;
+  d.n_scalar_transported = p->n_scalar;
+  d.n_spec = p->n_spec;
+  d.i_turb_cv = 5 + p->n_spec;
+  d.inviscid_scheme = p->inviscid_scheme;
+  d.reconstruction = p->reconstruction;
+  d.limiter = p->limiter;
+  d.entropy_fix_factor = p->entropy_fix_factor;
+  d.viscous_scheme = p->viscous_scheme;
+  d.rans_model = 0;
+  d.turb_implicit = 0;
+  d.compressibility_correction = 0;
+  d.chemSrcMethod = p->chemSrcMethod;
+  d.n_reac = p->mix_model == OSTC_MIX_FR ? p->n_reac : 0;
+  d.Pr = p->Pr;
+  d.cfl = p->cfl;
+  d.gradPInDiffusionFlux = p->gradPInDiffusionFlux != 0;
+  d.Sc = p->Sc;
+  d.Prt = p->Prt;
+  d.Sct = p->Sct;
+  const int ns = p->n_spec;
+  if (ns > 0) {
+    d.mw = dcopy(p->mw, ns);
+    fill_matrix(d.high_temp_coeff, p->high_temp_coeff, ns, 7);
+    fill_matrix(d.low_temp_coeff, p->low_temp_coeff, ns, 7);
+    d.t_low = dcopy(p->t_low, ns);
+    d.t_mid = dcopy(p->t_mid, ns);
+    d.t_high = dcopy(p->t_high ? p->t_high : p->t_mid, ns);
+    d.LJ_potent_inv = dcopy(p->LJ_potent_inv, ns);
+    d.vis_coeff = dcopy(p->vis_coeff, ns);
+    fill_matrix(d.WjDivWi_to_One4th, p->WjDivWi_to_One4th, ns, ns);
+    fill_matrix(d.sqrt_WiDivWjPl1Mul8, p->sqrt_WiDivWjPl1Mul8, ns, ns);
+    fill_matrix(d.binary_diffusivity_coeff, p->binary_diffusivity_coeff, ns, ns);
+    fill_matrix(d.kb_over_eps_jk, p->kb_over_eps_jk, ns, ns);
+  }
+  const int nr = d.n_reac;
+  if (nr > 0) {
+    d.reac_type = dcopy(p->reac_type, nr);
+    fill_matrix(d.stoi_f, p->stoi_f, nr, ns);
+    fill_matrix(d.stoi_b, p->stoi_b, nr, ns);
+    d.reac_order = dcopy(p->reac_order, nr);
+    d.A = dcopy(p->A, nr);
+    d.b = dcopy(p->b, nr);
+    d.Ea = dcopy(p->Ea, nr);
+    d.A2 = dcopy(p->A2, nr);
+    d.b2 = dcopy(p->b2, nr);
+    d.Ea2 = dcopy(p->Ea2, nr);
+    fill_matrix(d.third_body_coeff, p->third_body_coeff, nr, ns);
+    d.troe_alpha = dcopy(p->troe_alpha, nr);
+    d.troe_t3 = dcopy(p->troe_t3, nr);
+    d.troe_t1 = dcopy(p->troe_t1, nr);
+    d.troe_t2 = dcopy(p->troe_t2, nr);
+  }
+  cudaMalloc(&c.d_param, sizeof(DParameter));
+  cudaMemcpy(c.d_param, &c.h_param, sizeof(DParameter), cudaMemcpyHostToDevice);
+}
+
+void build_zone(RefCtx &c, const ostc_zone *z, const ostc_param *p) {
+  DZone &h = c.h;
+  const int mx = z->mx, my = z->my, mz = z->mz, g = z->ngg;
+  h.mx = mx;
+  h.my = my;
+  h.mz = mz;
+  h.ngg = g;
+  const size_t P = plane(mx, my, mz, g);
+  h.jac.allocate_memory(mx, my, mz, g);
+  cudaMemcpy(h.jac.data(), z->jac, sizeof(double) * P, cudaMemcpyHostToDevice);
+  h.metric.allocate_memory(mx, my, mz, g);
+  static_assert(sizeof(gxl::Matrix<real, 3, 3, 1>) == 80, "metric record");
+  cudaMemcpy(h.metric.data(), z->metric, 80 * P, cudaMemcpyHostToDevice);
+  h.cv.allocate_memory(mx, my, mz, p->n_var, g);
+  h.bv.allocate_memory(mx, my, mz, 6, g);
+  cudaMemcpy(h.bv.data(), z->bv, sizeof(double) * P * 6, cudaMemcpyHostToDevice);
+  h.bv_last.allocate_memory(mx, my, mz, 4, 0);
+  h.vel.allocate_memory(mx, my, mz, g);
+  h.acoustic_speed.allocate_memory(mx, my, mz, g);
+  h.mach.allocate_memory(mx, my, mz, g);
+  h.mul.allocate_memory(mx, my, mz, g);
+  h.thermal_conductivity.allocate_memory(mx, my, mz, g);
+  h.sv.allocate_memory(mx, my, mz, p->n_scalar, g);
+  if (p->n_scalar) cudaMemcpy(h.sv.data(), z->sv, sizeof(double) * P * p->n_scalar, cudaMemcpyHostToDevice);
+  h.rho_D.allocate_memory(mx, my, mz, p->n_spec, g);
+  if (p->n_spec > 0) {
+    h.gamma.allocate_memory(mx, my, mz, g);
+    h.cp.allocate_memory(mx, my, mz, g);
+    if (p->mix_model == OSTC_MIX_FR) {
+      if (p->chemSrcMethod == 1)
+        h.chem_src_jac.allocate_memory(mx, my, mz, p->n_spec * p->n_spec, 0);
+      else if (p->chemSrcMethod == 2)
+        h.chem_src_jac.allocate_memory(mx, my, mz, p->n_spec, 0);
+    }
+  }
+  h.dq.allocate_memory(mx, my, mz, p->n_var, 0);
+  h.inv_spectr_rad.allocate_memory(mx, my, mz, 0);
+  h.visc_spectr_rad.allocate_memory(mx, my, mz, 0);
+  h.dt_local.allocate_memory(mx, my, mz, 0);
+  h.unphysical.allocate_memory(mx, my, mz, 0);
+  h.qn.allocate_memory(mx, my, mz, p->n_var, g);
+  h.boundary = nullptr;
+  if (!c.faces.empty()) h.boundary = dcopy(c.faces.data(), c.faces.size());
+  cudaMalloc(&c.d_zone, sizeof(DZone));
+  cudaMemcpy(c.d_zone, &h, sizeof(DZone), cudaMemcpyHostToDevice);
+}
+
+// one kernel launch per face, launch shape of DBoundCond::apply_boundary_conditions
+template <MixtureModel mix, bool with_cv>
+void apply_bcs(RefCtx &c) {
+  const int order[] = {4, 6, 9, 5, 7, 3, 2};
+  for (int t : order) {
+    for (size_t q = 0; q < c.faces.size(); ++q) {
+      const Boundary &f = c.faces[q];
+      if (f.type_label != t) continue;
+      uint tpb[3], bpg[3];
+      for (int j = 0; j < 3; ++j) {
+        const int n = f.range_end[j] - f.range_start[j] + 1;
+        tpb[j] = n <= (2 * c.ngg + 1) ? 1 : 16;
+        bpg[j] = (n - 1) / tpb[j] + 1;
+      }
+      dim3 TPB{tpb[0], tpb[1], tpb[2]}, BPG{bpg[0], bpg[1], bpg[2]};
+      switch (t) {
+        case 6: apply_outflow<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (integer)q, c.d_param); break;
+        case 5:
+          apply_inflow<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, c.d_inflows[c.face_inflow[q]], (integer)q,
+                                                              c.d_param);
+          break;
+        case 3: apply_symmetry<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (integer)q, c.d_param); break;
+        default: break;
+      }
+    }
+  }
+}
+
+template <MixtureModel mix>
+void initialize(RefCtx &c) {
+  // Driver::initialize_computation (Driver.cu:39-98) + RK3_bv pre-loop (RK.cuh:235-244)
+  dim3 tpb{8, 8, 4};
+  const int ng_1 = 2 * c.ngg - 1;
+  apply_bcs<mix, false>(c);
+  dim3 bpg{(unsigned)((c.mx + ng_1) / tpb.x + 1), (unsigned)((c.my + ng_1) / tpb.y + 1),
+           (unsigned)((c.mz + ng_1) / tpb.z + 1)};
+  compute_velocity<<<bpg, tpb>>>(c.d_zone);
+  update_physical_properties<mix><<<bpg, tpb>>>(c.d_zone, c.d_param);
+  dim3 bpg0{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
+  store_last_step<<<bpg0, tpb>>>(c.d_zone);
+  compute_cv_from_bv<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param);
+  cudaDeviceSynchronize();
+}
+
+template <MixtureModel mix>
+void rhs(RefCtx &c) {
+  dim3 tpb{8, 8, 4};
+  dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
+  cudaMemset(c.h.dq.data(), 0, c.h.dq.size() * c.n_var * sizeof(real));
+  compute_source<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param);
+  compute_inviscid_flux<mix, Laminar>(*c.block, c.d_zone, c.d_param, c.n_var, *c.parameter);
+  compute_viscous_flux<mix, Laminar>(*c.block, c.d_zone, c.d_param, c.n_var);
+}
+
+double global_dt(RefCtx &c) {  // global_time_step (TimeAdvanceFunc.cu:155-182) for one block
+  constexpr integer TPB{128};
+  int num_sms, per_sm;
+  cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, min_of_arr, TPB, 0);
+  const integer size = c.mx * c.my * c.mz;
+  const int n_blocks = std::min(per_sm * num_sms, (size + TPB - 1) / TPB);
+  min_of_arr<<<n_blocks, TPB>>>(c.h.dt_local.data(), size);
+  min_of_arr<<<1, TPB>>>(c.h.dt_local.data(), n_blocks);
+  double dt_block;
+  cudaMemcpy(&dt_block, c.h.dt_local.data(), sizeof(real), cudaMemcpyDeviceToHost);
+  return std::min(1e+6, dt_block);
+}
+
+template <MixtureModel mix>
+void residual(RefCtx &c, double *res) {  // compute_residual (Residual.cuh:57-111) before normalisation
+  dim3 tpb{8, 8, 4};
+  dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
+  compute_square_of_dbv<<<bpg, tpb>>>(c.d_zone);
+  constexpr integer TPB{128};
+  int num_sms, per_sm;
+  cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reduction_of_dv_squared, TPB, 0);
+  const integer size = c.mx * c.my * c.mz;
+  const int n_blocks = std::min(per_sm * num_sms, (size + TPB - 1) / TPB);
+  reduction_of_dv_squared<<<n_blocks, TPB>>>(c.h.bv_last.data(), size);
+  reduction_of_dv_squared<<<1, TPB>>>(c.h.bv_last.data(), n_blocks);
+  double r[4];
+  cudaMemcpy(r, c.h.bv_last.data(), 4 * sizeof(real), cudaMemcpyDeviceToHost);
+  for (int l = 0; l < 4; ++l) res[l] = std::sqrt(r[l] / (double)size);
+}
+
+template <MixtureModel mix>
+int steps(RefCtx &c, int n, double *res_hist, double *dt_hist) {
+  // the body of RK3_bv's while loop (RK.cuh:284-357)
+  dim3 tpb{8, 8, 4};
+  dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
+  dim3 bpgp{(unsigned)((c.mx + 1) / tpb.x + 1), (unsigned)((c.my + 1) / tpb.y + 1), (unsigned)((c.mz + 1) / tpb.z + 1)};
+  double dt = c.cfg.fixed_time_step ? c.cfg.dt : 1e+6;
+  for (int s = 0; s < n; ++s) {
+    if (res_hist) store_last_step<<<bpg, tpb>>>(c.d_zone);
+    cudaMemcpy(c.h.qn.data(), c.h.cv.data(), c.h.cv.size() * sizeof(real) * c.n_var, cudaMemcpyDeviceToDevice);
+    for (integer rk = 0; rk < 3; ++rk) {
+      rhs<mix>(c);
+      if (!c.cfg.fixed_time_step) {
+        local_time_step<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param);
+        dt = global_dt(c);
+      }
+      update_cv_and_bv_rk<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param, dt, rk);
+      apply_bcs<mix, true>(c);
+      update_physical_properties<mix><<<bpgp, tpb>>>(c.d_zone, c.d_param);
+    }
+    if (res_hist) residual<mix>(c, res_hist + 4 * s);
+    if (dt_hist) dt_hist[s] = dt;
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  return e == cudaSuccess ? 0 : 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, const ostc_bc_face *f, int nf,
+               void **out) {
+  if (!cfg || !p || !z || !out) return 1;
+  if (p->turbulence || p->inviscid_type == 2 || (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_FR))
+    return 5;
+  auto *c = new RefCtx;
+  c->cfg = *cfg;
+  c->mix = p->mix_model;
+  c->n_var = p->n_var;
+  c->n_scalar = p->n_scalar;
+  c->n_spec = p->n_spec;
+  c->ngg = z->ngg;
+  c->mx = z->mx;
+  c->my = z->my;
+  c->mz = z->mz;
+  c->parameter = new Parameter(std::string("/dev/null"));
+  c->parameter->update_parameter("inviscid_type", p->inviscid_type);
+  c->parameter->update_parameter("n_spec", p->n_spec);
+  c->block = new Block(z->mx, z->my, z->mz, z->ngg, 0);
+  for (int q = 0; q < nf; ++q) {
+    if (f[q].type_label != 3 && f[q].type_label != 5 && f[q].type_label != 6) {
+      delete c;
+      return 5;  // the reference has no periodic boundary (quirk A13)
+    }
+    Boundary b;
+    for (int d = 0; d < 3; ++d) {
+      b.range_start[d] = f[q].range_start[d];
+      b.range_end[d] = f[q].range_end[d];
+    }
+    b.type_label = f[q].type_label;
+    b.face = f[q].face;
+    b.direction = f[q].direction;
+    c->faces.push_back(b);
+    c->face_inflow.push_back(-1);
+    if (f[q].type_label == 5) {
+      // cfd::Inflow has no default constructor; fill a zeroed record of its layout
+      alignas(Inflow) unsigned char buf[sizeof(Inflow)];
+      std::memset(buf, 0, sizeof(buf));
+      Inflow *in = reinterpret_cast<Inflow *>(buf);
+      in->label = 5;
+      in->density = f[q].density;
+      in->u = f[q].u;
+      in->v = f[q].v;
+      in->w = f[q].w;
+      in->pressure = f[q].pressure;
+      in->temperature = f[q].temperature;
+      in->velocity = f[q].velocity;
+      in->mut = f[q].mut;
+      double *dsv = nullptr;
+      if (p->n_scalar) dsv = dcopy(f[q].sv, p->n_scalar);
+      in->sv = dsv;
+      c->d_inflow_sv.push_back(dsv);
+      c->d_inflows.push_back(dcopy(in, 1));
+      c->face_inflow.back() = (int)c->d_inflows.size() - 1;
+    }
+  }
+  build_param(*c, p);
+  build_zone(*c, z, p);
+  if (cudaDeviceSynchronize() != cudaSuccess) return 2;
+  *out = c;
+  return 0;
+}
+
+int ref_initialize(void *h) {
+  auto *c = (RefCtx *)h;
+  if (c->mix == OSTC_MIX_AIR) initialize<MixtureModel::Air>(*c); else initialize<MixtureModel::FR>(*c);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int ref_rhs(void *h) {
+  auto *c = (RefCtx *)h;
+  if (c->mix == OSTC_MIX_AIR) rhs<MixtureModel::Air>(*c); else rhs<MixtureModel::FR>(*c);
+  return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+
+int ref_steps(void *h, int n, double *res_hist, double *dt_hist) {
+  auto *c = (RefCtx *)h;
+  return c->mix == OSTC_MIX_AIR ? steps<MixtureModel::Air>(*c, n, res_hist, dt_hist)
+                                : steps<MixtureModel::FR>(*c, n, res_hist, dt_hist);
+}
+
+// device time of n steps (CUDA events around the loop, as bench.py does for ours)
+double ref_time_steps(void *h, int n) {
+  auto *c = (RefCtx *)h;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaDeviceSynchronize();
+  cudaEventRecord(e0);
+  if (ref_steps(h, n, nullptr, nullptr)) return -1;
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  (void)c;
+  return ms;
+}
+
+// copy a DZone array to the host: name in {bv, sv, cv, dq, mul, thermal_conductivity, vel, acoustic_speed, rho_D}
+int ref_download(void *h, const char *name, double *dst) {
+  auto *c = (RefCtx *)h;
+  DZone &z = c->h;
+  const size_t P = plane(c->mx, c->my, c->mz, c->ngg);
+  const size_t I = plane(c->mx, c->my, c->mz, 0);
+  const void *src = nullptr;
+  size_t n = 0;
+  if (!strcmp(name, "bv")) src = z.bv.data(), n = 6 * P;
+  else if (!strcmp(name, "sv")) src = z.sv.data(), n = c->n_scalar * P;
+  else if (!strcmp(name, "cv")) src = z.cv.data(), n = c->n_var * P;
+  else if (!strcmp(name, "dq")) src = z.dq.data(), n = c->n_var * I;
+  else if (!strcmp(name, "mul")) src = z.mul.data(), n = P;
+  else if (!strcmp(name, "thermal_conductivity")) src = z.thermal_conductivity.data(), n = P;
+  else if (!strcmp(name, "vel")) src = z.vel.data(), n = P;
+  else if (!strcmp(name, "acoustic_speed")) src = z.acoustic_speed.data(), n = P;
+  else if (!strcmp(name, "rho_D")) src = z.rho_D.data(), n = c->n_spec * P;
+  else return 1;
+  return cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : 2;
+}
+
+// bytes of device memory the reference arrays of this context hold
+double ref_device_bytes(void *h) {
+  auto *c = (RefCtx *)h;
+  const double P = (double)plane(c->mx, c->my, c->mz, c->ngg), I = (double)plane(c->mx, c->my, c->mz, 0);
+  double b = 8 * P * (1 + 10 + c->n_var * 2 + 6 + c->n_scalar + 5 + c->n_spec) + 8 * I * (4 + c->n_var + 5);
+  if (c->mix == OSTC_MIX_FR && c->h_param.chemSrcMethod == 1) b += 8 * I * c->n_spec * c->n_spec;
+  return b;
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+"""ctypes binding of the reference's own CUDA kernels driven by
+oracle/ref_cuda_harness.cu (oracle/_ref/libostc_ref_cuda.so, built from the
+reference sources by oracle/build_ref.sh). Test and measurement
+infrastructure: the tight GPU oracle and the reference-build timing."""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+import ostc
+
+REPO = Path(__file__).resolve().parents[1]
+REF_CUDA = REPO / "oracle" / "_ref" / "libostc_ref_cuda.so"
+_r = None
+
+
+def available():
+    return REF_CUDA.exists()
+
+
+def ref():
+    global _r
+    if _r is None:
+        L = C.CDLL(str(REF_CUDA))
+        vp = C.c_void_p
+        d = C.POINTER(C.c_double)
+        L.ref_create.argtypes = [C.POINTER(ostc.Config), C.POINTER(ostc.Param), C.POINTER(ostc.Zone),
+                                 C.POINTER(ostc.BcFaceC), C.c_int, C.POINTER(vp)]
+        L.ref_create.restype = C.c_int
+        for n in ("ref_initialize", "ref_rhs"):
+            getattr(L, n).argtypes = [vp]
+            getattr(L, n).restype = C.c_int
+        L.ref_steps.argtypes = [vp, C.c_int, d, d]
+        L.ref_steps.restype = C.c_int
+        L.ref_time_steps.argtypes = [vp, C.c_int]
+        L.ref_time_steps.restype = C.c_double
+        L.ref_download.argtypes = [vp, C.c_char_p, d]
+        L.ref_download.restype = C.c_int
+        _r = L
+    return _r
+
+
+class RefCudaRun:
+    """The reference build on one block of a Case (single-rank)."""
+
+    def __init__(self, case):
+        self.case = case
+        b = case.blocks[0]
+        self.block = b
+        self.param, self._keep = ostc.make_param(case.scheme, case.mech)
+        self.config = ostc.make_config(case.scheme)
+        self.zone = b.zone()
+        self.faces = (ostc.BcFaceC * max(len(case.faces), 1))(*case.faces)
+        h = C.c_void_p()
+        st = ref().ref_create(C.byref(self.config), C.byref(self.param), C.byref(self.zone), self.faces,
+                              len(case.faces), C.byref(h))
+        if st != 0:
+            raise RuntimeError("ref_create -> %d" % st)
+        self.h = h
+
+    def initialize(self):
+        assert ref().ref_initialize(self.h) == 0
+
+    def compute_rhs(self):
+        assert ref().ref_rhs(self.h) == 0
+
+    def rk3_steps(self, n):
+        res = (C.c_double * (4 * n))()
+        dts = (C.c_double * n)()
+        assert ref().ref_steps(self.h, n, res, dts) == 0
+        return np.array(res).reshape(n, 4), np.array(dts)
+
+    def time_steps(self, n):
+        return ref().ref_time_steps(self.h, n)
+
+    def download(self, name):
+        b = self.block
+        P = ostc.plane_shape(b.mx, b.my, b.mz, b.ngg)
+        I = ostc.plane_shape(b.mx, b.my, b.mz, 0)
+        shapes = {"bv": (6,) + P, "sv": (b.n_spec,) + P, "cv": (b.n_var,) + P, "dq": (b.n_var,) + I, "mul": P,
+                  "thermal_conductivity": P, "vel": P, "acoustic_speed": P, "rho_D": (b.n_spec,) + P}
+        out = np.zeros(shapes[name])
+        assert ref().ref_download(self.h, name.encode(), out.ctypes.data_as(C.POINTER(C.c_double))) == 0
+        return out
