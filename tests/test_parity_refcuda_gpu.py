@@ -19,9 +19,9 @@ pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not ref_bind.available(), reason="reference build (oracle/_ref) not present")]
 
 
-def _cases():
+def _cases(mixing_shape=(28, 24, 10)):
     v = ostc.case_vortex(40, 32, 10, k_bc="symmetry")
-    m = ostc.case_mixing_layer(28, 24, 10, full_host=True)
+    m = ostc.case_mixing_layer(*mixing_shape, full_host=True)
     for f in m.faces:
         if f.type_label == ostc.BC_PERIODIC:
             f.type_label = ostc.BC_OUTFLOW
@@ -48,9 +48,23 @@ def test_rhs_matches_reference_build(name):
     assert max(rhs_errors(o.blocks[0].arrays["dq"], dq_ref, scale)) <= 1e-11
 
 
-@pytest.mark.parametrize("name,n", [("vortex", 100), ("mixing", 20)])
-def test_residual_history_matches_reference_build(name, n):
-    case = _cases()[name]
+def _reduction_well_defined(cells):
+    # The reference's residual sums (reduction_of_dv_squared + block_reduce_sum,
+    # src/gxl_lib/MyAtomic.cuh:12-32) read the partial sum of one warp too many
+    # when the last block of a pass holds a whole number of warps short of a
+    # full block (n_warp = v/32 + 1): that slot of the static shared array was
+    # never written by the kernel. Its residual is defined only when the valid
+    # thread count v of the last block of both passes is 128 or not a multiple
+    # of 32 (block count of the second pass = ceil(cells/128) here).
+    nb = (cells + 127) // 128
+    v1, v2 = cells - (nb - 1) * 128, nb
+    return all(v == 128 or v % 32 for v in (v1, v2))
+
+
+@pytest.mark.parametrize("name,n,shape", [("vortex", 100, None), ("mixing", 20, (28, 24, 10)),
+                                          ("mixing", 20, (30, 26, 10))])
+def test_history_matches_reference_build(name, n, shape):
+    case = _cases(shape or (28, 24, 10))[name]
     r = ref_bind.RefCudaRun(case)
     r.initialize()
     res_r, dt_r = r.rk3_steps(n)
@@ -59,6 +73,8 @@ def test_residual_history_matches_reference_build(name, n):
     s.initialize()
     res_g, dt_g = s.rk3_steps(n, history=True)
     assert np.max(np.abs(dt_g - dt_r) / dt_r) <= 1e-9
-    assert np.max(np.abs(res_g - res_r) / res_r) <= 1e-9
-    err = normwise(blocks[0].download("bv"), r.download("bv"))
-    assert max(err) <= 1e-9, err
+    for name_ in ("bv", "sv") if case.mech else ("bv",):
+        err = normwise(blocks[0].download(name_), r.download(name_))
+        assert max(err) <= 1e-9, (name_, err)
+    if _reduction_well_defined(case.cells):
+        assert np.max(np.abs(res_g - res_r) / res_r) <= 1e-9
