@@ -267,6 +267,24 @@ ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream);
  * the residual epilogue); captures the graph if it does not exist yet.     */
 ostc_status ostc_step_kernel_count(ostc_ctx *ctx, int with_hist, int *count);
 
+/* Residual of one block without any device allocation. No counterpart in
+ * the reference: for callers that cannot allocate device memory when the
+ * residual is wanted (a host solver that reserves its whole device budget at
+ * start-up, or one sharing a fixed memory pool with other codes). Writes to
+ * res_out (DEVICE pointer, 4 doubles) sqrt(sum(d^2)/cells) of rho, |V|, p, T
+ * between zone->bv_last (written by store_last_step at the start of a step)
+ * and the current zone->bv / zone->vel: the same quantity as the residual
+ * history of ostc_rk3_steps. Partial sums go to a fixed array in the
+ * library's own device memory (OSTC_NOALLOC_MAX_PARTIALS x 4 doubles =
+ * 512 KiB, held on every GPU that loads the library until exit); blocks of
+ * more than OSTC_NOALLOC_MAX_CELLS cells are rejected with
+ * OSTC_ERR_INVALID_ARG. The first call on a device looks up the array's
+ * address, so make that first call before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race.                     */
+#define OSTC_NOALLOC_MAX_PARTIALS 16384
+#define OSTC_NOALLOC_MAX_CELLS (OSTC_NOALLOC_MAX_PARTIALS * 2048LL)
+ostc_status ostc_compute_residual_noalloc(const ostc_zone *zone, double *res_out, void *stream);
+
 /* Library version string. */
 const char *ostc_version(void);
 
