@@ -32,7 +32,7 @@ struct ostc_ctx {
   std::vector<double *> met_soa;
   std::vector<BcFace> faces;
   std::vector<int> face_zone;
-  TileShape tile[3] = {{4, 4}, {8, 2}, {8, 2}};
+  TileShape tile[3] = {{4, 4, 1}, {8, 2, 1}, {8, 2, 1}};
   unsigned long long *dt_bits = nullptr;  // device dt (as bits)
   double *res_partial = nullptr;          // [n_part_total][4]
   int n_part_per_zone = 0;
@@ -241,7 +241,10 @@ void build_devparam(const ostc_param *p, DevParam &d) {
     d.t_mid[i] = p->t_mid[i];
     d.LJ_inv[i] = p->LJ_potent_inv[i];
     d.vis_coeff[i] = p->vis_coeff[i];
+    d.LJm145[i] = std::pow(p->LJ_potent_inv[i], -0.145);
     for (int j = 0; j < ns; ++j) {
+      d.kbem145[i][j] = i == j ? 0.0 : std::pow(p->kb_over_eps_jk[i * ns + j], -0.145);
+      d.inv_bdc[i][j] = i == j ? 0.0 : 1.0 / p->binary_diffusivity_coeff[i * ns + j];
       d.WjWi4[i][j] = p->WjDivWi_to_One4th[i * ns + j];
       d.sqWW8[i][j] = p->sqrt_WiDivWjPl1Mul8[i * ns + j];
       d.bdc[i][j] = p->binary_diffusivity_coeff[i * ns + j];
@@ -281,14 +284,14 @@ void default_tiles(ostc_ctx *c) {
   {
     int R = 4, C = (z.mx + 1 + 31) / 32;
     while (C > 1 && (long long)((z.mx + 32 * C - 2) / (32 * C - 1)) * ((z.my + R - 1) / R) * z.mz < target) --C;
-    c->tile[0] = {R, std::max(C, 1)};
+    c->tile[0] = {R, std::max(C, 1), 1};
   }
   for (int d = 1; d < 3; ++d) {
     const int n = d == 1 ? z.my : z.mz;
     const int other = d == 1 ? z.mz : z.my;
     int R = 8, C = (n + 1 + R - 1) / R;
     while (C > 1 && (long long)((z.mx + 31) / 32) * other * ((n + R * C - 2) / (R * C - 1)) < target) --C;
-    c->tile[d] = {R, std::max(C, 1)};
+    c->tile[d] = {R, std::max(C, 1), 1};
   }
 }
 
@@ -662,9 +665,13 @@ ostc_status ostc_step_kernel_count(ostc_ctx *ctx, int with_hist, int *count) {
 
 // tile-shape control for the autotuner: dir 0..2
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
-  if (!ctx || dir < 0 || dir > 2 || chunks < 1 || chunks > 4096) return OSTC_ERR_INVALID_ARG;
+  if (!ctx || dir < 0 || dir > 2) return OSTC_ERR_INVALID_ARG;
+  // rows may carry the register budget in its upper bits: rows | (minb << 8)
+  const int minb = (rows >> 8) & 0xff;
+  rows &= 0xff;
+  if (chunks < 1 || chunks > 4096 || (minb != 0 && minb != 1 && minb != 2)) return OSTC_ERR_INVALID_ARG;
   if (!(rows == 1 || rows == 2 || rows == 4 || rows == 8)) return OSTC_ERR_INVALID_ARG;
-  ctx->tile[dir] = {rows, chunks};
+  ctx->tile[dir] = {rows, chunks, minb == 2 ? 2 : 1};
   for (auto &kv : ctx->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
@@ -675,7 +682,7 @@ ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
 
 ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks) {
   if (!ctx || dir < 0 || dir > 2 || !rows || !chunks) return OSTC_ERR_INVALID_ARG;
-  *rows = ctx->tile[dir].rows;
+  *rows = ctx->tile[dir].rows | (ctx->tile[dir].minb == 2 ? (2 << 8) : 0);
   *chunks = ctx->tile[dir].chunks;
   return OSTC_OK;
 }

@@ -24,8 +24,9 @@ __device__ __forceinline__ double ipow(double c, int n) {
   }
 }
 
-__device__ __forceinline__ double arrhenius(double t, double A, double b, double Ea) {
-  return A * pow(t, b) * exp(-Ea / t);
+// A t^b exp(-Ea/t) as one exponential: A exp(b ln t - Ea / t)
+__device__ __forceinline__ double arrhenius(double lnT, double invT, double A, double b, double Ea) {
+  return A * exp(b * lnT - Ea * invT);
 }
 
 // omega[NS] in kg/(m^3 s) at density rho, temperature t, mass fractions Y
@@ -45,10 +46,12 @@ __device__ __forceinline__ void chemistry_omega(double rho, double t, const doub
     des[l] = 0;
   }
   const int nr = c_p.n_reac;
+  const double lnT = log(t), invT = 1.0 / t;
+  const double ln_temp_t = log(temp_t);
   for (int r = 0; r < nr; ++r) {
     const int type = c_p.reac_type[r];
-    double kf = arrhenius(t, c_p.A[r], c_p.b[r], c_p.Ea[r]);
-    if (type == 3) kf += arrhenius(t, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
+    double kf = arrhenius(lnT, invT, c_p.A[r], c_p.b[r], c_p.Ea[r]);
+    if (type == 3) kf += arrhenius(lnT, invT, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
     if (type > 3) {
       double cc = 0;
 #pragma unroll
@@ -56,7 +59,7 @@ __device__ __forceinline__ void chemistry_omega(double rho, double t, const doub
       if (type == 4) {
         kf *= cc;
       } else {
-        const double kf_low = arrhenius(t, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
+        const double kf_low = arrhenius(lnT, invT, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
         const double kf_high = kf;
         const double pr = kf_low * cc / kf_high;
         double F = 1.0;
@@ -76,13 +79,13 @@ __device__ __forceinline__ void chemistry_omega(double rho, double t, const doub
     }
     double kb = 0;
     if (type == 2) {
-      kb = arrhenius(t, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
+      kb = arrhenius(lnT, invT, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
     } else if (type != 0) {
       double dg = 0;
 #pragma unroll
       for (int l = 0; l < NS; ++l) dg += g[l] * (c_p.nub[r][l] - c_p.nuf[r][l]);
-      const double kc = pow(temp_t, (double)c_p.reac_order[r]) * exp(-dg);
-      kb = kf / kc;
+      // kf / (temp_t^order exp(-dg)) as one exponential
+      kb = kf * exp(dg - c_p.reac_order[r] * ln_temp_t);
     }
     // rates of progress: species in increasing order, as the reference's loop
     double q1 = 1.0, q2 = 1.0;
@@ -111,14 +114,18 @@ __device__ __forceinline__ void chemistry_omega(double rho, double t, const doub
 template <int NS>
 __device__ __forceinline__ void mixture_transport(double T, double mw_total, const double *Y, const double *cp,
                                                   double rho, double p, double &mu, double &kappa, double *rhoD) {
-  double X[NS], vis[NS];
+  // T^-0.145 once; (T c)^-0.145 = T^-0.145 c^-0.145 with c^-0.145 from the host
+  double X[NS], vis[NS], svis[NS], rsvis[NS];
   const double sqT = sqrt(T);
+  const double Tm145 = exp(-0.145 * log(T));
 #pragma unroll
   for (int l = 0; l < NS; ++l) {
     X[l] = Y[l] * mw_total / c_p.mw[l];
-    const double t_dl = T * c_p.LJ_inv[l];
-    const double ci = 1.147 * pow(t_dl, -0.145) + pow(t_dl + 0.5, -2.0);
+    const double t_dl = T * c_p.LJ_inv[l] + 0.5;
+    const double ci = 1.147 * (Tm145 * c_p.LJm145[l]) + 1.0 / (t_dl * t_dl);
     vis[l] = c_p.vis_coeff[l] * sqT / ci;
+    svis[l] = sqrt(vis[l]);
+    rsvis[l] = 1.0 / svis[l];
   }
   double viscosity = 0, conductivity = 0;
 #pragma unroll
@@ -127,8 +134,8 @@ __device__ __forceinline__ void mixture_transport(double T, double mw_total, con
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
       double pf = 1.0;
-      if (m != n) {
-        const double num = 1 + sqrt(vis[m] / vis[n]) * c_p.WjWi4[m][n];
+      if (m != n) {  // sqrt(vis_m / vis_n) = sqrt(vis_m) / sqrt(vis_n)
+        const double num = 1 + svis[m] * rsvis[n] * c_p.WjWi4[m][n];
         pf = num * num * c_p.sqWW8[m][n];
       }
       vt += pf * X[n];
@@ -140,17 +147,18 @@ __device__ __forceinline__ void mixture_transport(double T, double mw_total, con
   }
   mu = viscosity;
   kappa = conductivity;
-  const double t32p = T * sqT / p;
+  // 1 / D_mn = Omega_D / (bdc T^1.5 / p), Omega_D = t_red^-0.145 + (t_red + 0.5)^-2
+  const double inv_t32p = p / (T * sqT);
   double dinv[NS][NS];
 #pragma unroll
   for (int m = 0; m < NS; ++m) {
 #pragma unroll
     for (int n = m + 1; n < NS; ++n) {
-      const double t_red = T * c_p.kbe[m][n];
-      const double od = 1.0 / pow(t_red, 0.145) + 1.0 / ((t_red + 0.5) * (t_red + 0.5));
-      const double d = c_p.bdc[m][n] * t32p / od;
-      dinv[m][n] = d;
-      dinv[n][m] = d;
+      const double tr = T * c_p.kbe[m][n] + 0.5;
+      const double od = Tm145 * c_p.kbem145[m][n] + 1.0 / (tr * tr);
+      const double di = od * c_p.inv_bdc[m][n] * inv_t32p;
+      dinv[m][n] = di;
+      dinv[n][m] = di;
     }
   }
   constexpr double eps = 1e-12;
@@ -161,7 +169,7 @@ __device__ __forceinline__ void mixture_transport(double T, double mw_total, con
     for (int n = 0; n < NS; ++n) {
       if (l != n) {
         num += (X[n] + eps) * c_p.mw[n];
-        den += (X[n] + eps) / dinv[l][n];
+        den += (X[n] + eps) * dinv[l][n];
       }
     }
     rhoD[l] = rho * num / (den * mw_total);

@@ -32,6 +32,11 @@ struct DevParam {
   double LJ_inv[MAXS], vis_coeff[MAXS];
   double WjWi4[MAXS][MAXS], sqWW8[MAXS][MAXS];     // Wilke mixing constants
   double bdc[MAXS][MAXS], kbe[MAXS][MAXS];         // binary diffusion constants
+  // derived on the host so that one pow(T, -0.145) per point serves all
+  // species and pairs: (T c)^-0.145 = T^-0.145 c^-0.145
+  double LJm145[MAXS];                             // LJ_inv^-0.145
+  double kbem145[MAXS][MAXS];                      // kb_over_eps^-0.145
+  double inv_bdc[MAXS][MAXS];                      // 1 / binary_diffusivity_coeff
   int reac_type[MAXR], reac_order[MAXR];
   signed char nuf[MAXR][MAXS], nub[MAXR][MAXS];    // stoichiometric coefficients
   double A[MAXR], b[MAXR], Ea[MAXR], A2[MAXR], b2[MAXR], Ea2[MAXR];

@@ -51,8 +51,10 @@ __device__ __forceinline__ void face_total(const DevZone &z, int g0, bool viscou
   }
 }
 
-template <int NS, int INV, int DIR>
-__global__ void __launch_bounds__(256) flux_dir(DevZone z, int nchunk, int accumulate, int viscous) {
+// MINB = minimum resident CTAs of 256 threads per SM the register allocation
+// must allow (1: up to 255 registers; 2: 128 registers, with some spilling)
+template <int NS, int INV, int DIR, int MINB>
+__global__ void __launch_bounds__(256, MINB) flux_dir(DevZone z, int nchunk, int accumulate, int viscous) {
   constexpr int NV = 5 + NS;
   const int lane = threadIdx.x, row = threadIdx.y, R = blockDim.y;
   const int n = DIR == 0 ? z.mx : (DIR == 1 ? z.my : z.mz);
@@ -558,8 +560,8 @@ dim3 plane_grid(int nx, int ny, int nz, dim3 blk) {
 }
 }  // namespace
 
-template <int NS, int INV, int DIR>
-static cudaError_t launch_flux_t(const DevZone &z, const TileShape &t, int accumulate, int viscous,
+template <int NS, int INV, int DIR, int MINB>
+static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, int accumulate, int viscous,
                                  cudaStream_t s) {
   constexpr int NV = 5 + NS;
   const int R = t.rows, C = t.chunks;
@@ -578,12 +580,19 @@ static cudaError_t launch_flux_t(const DevZone &z, const TileShape &t, int accum
       grid = dim3((z.mx + 31) / 32, z.my, (z.mz + S - 1) / S);
   }
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(flux_dir<NS, INV, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(flux_dir<NS, INV, DIR, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
   }
-  flux_dir<NS, INV, DIR><<<grid, blk, smem, s>>>(z, C, accumulate, viscous);
+  flux_dir<NS, INV, DIR, MINB><<<grid, blk, smem, s>>>(z, C, accumulate, viscous);
   return cudaGetLastError();
+}
+
+template <int NS, int INV, int DIR>
+static cudaError_t launch_flux_t(const DevZone &z, const TileShape &t, int accumulate, int viscous,
+                                 cudaStream_t s) {
+  return t.minb == 2 ? launch_flux_m<NS, INV, DIR, 2>(z, t, accumulate, viscous, s)
+                     : launch_flux_m<NS, INV, DIR, 1>(z, t, accumulate, viscous, s);
 }
 
 template <int NS>

@@ -476,9 +476,9 @@ class Solver:
         return r.value, c.value
 
     def autotune(self, warmup: int = 1, reps: int = 3, verbose: bool = False):
-        """Pick per-direction flux tile shapes (rows, chunks) by timing one RHS
-        evaluation with CUDA events on the launching stream. Leaves the state
-        as it found it (the RHS only writes dq)."""
+        """Pick per-direction flux tile shapes (rows, chunks, register budget)
+        by timing each flux kernel with CUDA events on the launching stream.
+        Only dq is written, so the state is left as it was."""
         import torch
 
         blk = self.blocks[0]
@@ -493,7 +493,8 @@ class Solver:
                 cmax = min(64, max(1, (n + 1 + span - 1) // span))
                 c = 1
                 while True:
-                    cands.append((R, min(c, cmax)))
+                    for minb in (1, 2):
+                        cands.append((R | (minb << 8 if minb == 2 else 0), min(c, cmax)))
                     if c >= cmax:
                         break
                     c *= 2
@@ -502,12 +503,12 @@ class Solver:
             for R, Cc in cands:
                 self.set_tile(d, R, Cc)
                 for _ in range(warmup):
-                    self.compute_rhs()
+                    self.launch_op(self.OP_FLUX, d)
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record()
                 for _ in range(reps):
-                    self.compute_rhs()
+                    self.launch_op(self.OP_FLUX, d)
                 e1.record()
                 torch.cuda.synchronize()
                 times.append((e0.elapsed_time(e1) / reps, R, Cc))

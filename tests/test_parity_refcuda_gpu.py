@@ -61,10 +61,12 @@ def _reduction_well_defined(cells):
     return all(v == 128 or v % 32 for v in (v1, v2))
 
 
-@pytest.mark.parametrize("name,n,shape", [("vortex", 100, None), ("mixing", 20, (28, 24, 10)),
-                                          ("mixing", 20, (30, 26, 10))])
+@pytest.mark.parametrize("name,n,shape", [("vortex", 100, None), ("mixing", 20, (30, 26, 10))])
 def test_history_matches_reference_build(name, n, shape):
+    # sizes where the reference's block reductions (dt minimum, residual sums)
+    # are well defined; see test_reference_reduction_defect_arbitrated_by_oracle
     case = _cases(shape or (28, 24, 10))[name]
+    assert _reduction_well_defined(case.cells)
     r = ref_bind.RefCudaRun(case)
     r.initialize()
     res_r, dt_r = r.rk3_steps(n)
@@ -78,3 +80,21 @@ def test_history_matches_reference_build(name, n, shape):
         assert max(err) <= 1e-9, (name_, err)
     if _reduction_well_defined(case.cells):
         assert np.max(np.abs(res_g - res_r) / res_r) <= 1e-9
+
+
+def test_reference_reduction_defect_arbitrated_by_oracle():
+    """At 28x24x10 = 6720 cells the last block of the reference's first
+    reduction pass holds 64 valid threads, so block_reduce_min reads a shared
+    slot no thread wrote (n_warp = 64/32 + 1) and its CFL time step can take
+    a stale value in some stages. The B200 path follows the CPU oracle here;
+    the reference build departs from both."""
+    case = _cases((28, 24, 10))["mixing"]
+    assert not _reduction_well_defined(case.cells)
+    o = OracleRun(case)
+    o.initialize()
+    o.rk3_steps(2)
+    blocks = [ostc.DeviceBlock(b) for b in case.blocks]
+    s = ostc.Solver(case.scheme, case.mech, blocks, case.faces)
+    s.initialize()
+    s.rk3_steps(2)
+    assert max(normwise(blocks[0].download("bv"), o.blocks[0].arrays["bv"])) <= 1e-9
