@@ -156,10 +156,10 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
     return OSTC_ERR_UNSUPPORTED;
   }
   if (p->turbulence) return OSTC_ERR_UNSUPPORTED;
-  if (p->inviscid_type == 2) return OSTC_ERR_UNSUPPORTED;  // Roe
   if (p->inviscid_type == 1 && p->mix_model != OSTC_MIX_AIR) return OSTC_ERR_UNSUPPORTED;  // quirk A2
   if (p->inviscid_type == 1 && p->reconstruction != 4) return OSTC_ERR_INVALID_ARG;
-  if (p->inviscid_scheme == 1 && p->mix_model != OSTC_MIX_AIR) return OSTC_ERR_UNSUPPORTED;
+  if (p->inviscid_type == 0 && p->inviscid_scheme == 1 && p->mix_model != OSTC_MIX_AIR) return OSTC_ERR_UNSUPPORTED;
+  if (p->inviscid_type == 2 && p->inviscid_scheme != 2) return OSTC_ERR_INVALID_ARG;
   if (p->inviscid_scheme < 1 || p->inviscid_scheme > 4) return OSTC_ERR_INVALID_ARG;
   if (p->limiter != 0) return OSTC_ERR_INVALID_ARG;
   if (cfg->steady || cfg->temporal_scheme != 3) return OSTC_ERR_UNSUPPORTED;

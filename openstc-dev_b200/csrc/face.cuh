@@ -190,10 +190,9 @@ __device__ __forceinline__ void riemann(const double *pl, const double *pr, cons
 // Reconstruction.cu:5-46 + Reconstruction.cuh:20-72)
 // ---------------------------------------------------------------------------
 template <int NS, int DIR>
-__device__ __forceinline__ void inviscid_face_pv(const DevZone &z, int g0, double *F) {
+__device__ __forceinline__ void reconstruct_pv(const DevZone &z, int g0, double *pl, double *pr) {
   constexpr int NV = 5 + NS;
   const int sd = dir_stride<DIR>(z);
-  double pl[NV + 2], pr[NV + 2];
   const int rec = c_p.reconstruction;
 #pragma unroll
   for (int l = 0; l < NV; ++l) {
@@ -256,7 +255,154 @@ __device__ __forceinline__ void inviscid_face_pv(const DevZone &z, int g0, doubl
     pl[NV + 1] = gamma_air;
     pr[NV + 1] = gamma_air;
   }
-  riemann<NV, NS>(pl, pr, z, g0, g0 + sd, DIR, F);
+}
+
+template <int NS, int DIR>
+__device__ __forceinline__ void inviscid_face_pv(const DevZone &z, int g0, double *F) {
+  constexpr int NV = 5 + NS;
+  double pl[NV + 2], pr[NV + 2];
+  reconstruct_pv<NS, DIR>(z, g0, pl, pr);
+  riemann<NV, NS>(pl, pr, z, g0, g0 + dir_stride<DIR>(z), DIR, F);
+}
+
+// Harten entropy-fix width at one point (compute_entropy_fix_delta, Roe.cu:61-85), 3-D form;
+// evaluated here at the two points of a face instead of a separate pass and array
+__device__ __forceinline__ double entropy_fix_delta(const DevZone &z, int g) {
+  const double u = bvl(z, g, 1), v = bvl(z, g, 2), w = bvl(z, g, 3);
+  double m[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) m[c] = met(z, g, c);
+  const double U = fabs(u * m[0] + v * m[1] + w * m[2]);
+  const double V = fabs(u * m[3] + v * m[4] + w * m[5]);
+  const double W = fabs(u * m[6] + v * m[7] + w * m[8]);
+  const double kx = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+  const double ky = sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
+  const double kz = sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
+  return c_p.entropy_fix_factor * (U + V + W + ld(z.a + g) * (kx + ky + kz) / 3.0);
+}
+
+// Roe flux-difference splitting (Roe_compute_half_point_flux + compute_half_sum_left_right_flux,
+// Roe.cu:186-375)
+template <int NS, int DIR>
+__device__ __forceinline__ void inviscid_face_roe(const DevZone &z, int g0, double *F) {
+  constexpr int NV = 5 + NS;
+  const int g1 = g0 + dir_stride<DIR>(z);
+  double pl[NV + 2], pr[NV + 2];
+  reconstruct_pv<NS, DIR>(z, g0, pl, pr);
+  const double j0 = ld(z.jac + g0), j1 = ld(z.jac + g1);
+  const double m0x = met(z, g0, 3 * DIR), m0y = met(z, g0, 3 * DIR + 1), m0z = met(z, g0, 3 * DIR + 2);
+  const double m1x = met(z, g1, 3 * DIR), m1y = met(z, g1, 3 * DIR + 1), m1z = met(z, g1, 3 * DIR + 2);
+  {  // half sum of the left and right physical fluxes, each with its own point's metric
+    double Jx = j0 * m0x, Jy = j0 * m0y, Jz = j0 * m0z;
+    double Uk = pl[1] * Jx + pl[2] * Jy + pl[3] * Jz;
+    double co = Uk * pl[0];
+    F[0] = 0.5 * co;
+    F[1] = 0.5 * (co * pl[1] + pl[4] * Jx);
+    F[2] = 0.5 * (co * pl[2] + pl[4] * Jy);
+    F[3] = 0.5 * (co * pl[3] + pl[4] * Jz);
+    F[4] = 0.5 * Uk * (pl[4] + pl[NV]);
+#pragma unroll
+    for (int l = 5; l < NV; ++l) F[l] = 0.5 * co * pl[l];
+    Jx = j1 * m1x;
+    Jy = j1 * m1y;
+    Jz = j1 * m1z;
+    Uk = pr[1] * Jx + pr[2] * Jy + pr[3] * Jz;
+    co = Uk * pr[0];
+    F[0] += 0.5 * co;
+    F[1] += 0.5 * (co * pr[1] + pr[4] * Jx);
+    F[2] += 0.5 * (co * pr[2] + pr[4] * Jy);
+    F[3] += 0.5 * (co * pr[3] + pr[4] * Jz);
+    F[4] += 0.5 * Uk * (pr[4] + pr[NV]);
+#pragma unroll
+    for (int l = 5; l < NV; ++l) F[l] += 0.5 * co * pr[l];
+  }
+  const double dl = sqrt(pl[0]), dr = sqrt(pr[0]);
+  const double inv_den = 1.0 / (dl + dr);
+  const double u = (dl * pl[1] + dr * pr[1]) * inv_den;
+  const double v = (dl * pl[2] + dr * pr[2]) * inv_den;
+  const double w = (dl * pl[3] + dr * pr[3]) * inv_den;
+  const double ek = 0.5 * (u * u + v * v + w * w);
+  const double hl = (pl[NV] + pl[4]) / pl[0], hr = (pr[NV] + pr[4]) / pr[0];
+  const double h = (dl * hl + dr * hr) * inv_den;
+  double gamma = gamma_air;
+  double c = sqrt((gamma - 1) * (h - ek));
+  double mw = mw_air;
+  double svm[NS > 0 ? NS : 1], h_i[NS > 0 ? NS : 1];
+  if constexpr (NS > 0) {
+    double mw_inv = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      svm[l] = (dl * pl[l + 5] + dr * pr[l + 5]) * inv_den;
+      mw_inv += svm[l] / c_p.mw[l];
+    }
+    const double tl = pl[4] / pl[0], tr = pr[4] / pr[0];
+    const double t = (dl * tl + dr * tr) * inv_den / (R_u * mw_inv);
+    double cp_i[NS];
+    enthalpy_cp<NS>(t, h_i, cp_i);
+    double cv = 0, cp = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      cp += cp_i[l] * svm[l];
+      cv += svm[l] * (cp_i[l] - c_p.Rmw[l]);
+    }
+    gamma = cp / cv;
+    c = sqrt(gamma * R_u * mw_inv * t);
+    mw = 1.0 / mw_inv;
+  }
+  double kx = 0.5 * (m0x + m1x), ky = 0.5 * (m0y + m1y), kz = 0.5 * (m0z + m1z);
+  const double gradK = sqrt(kx * kx + ky * ky + kz * kz);
+  double Uk = kx * u + ky * v + kz * w;
+  double ch[3] = {Uk - gradK * c, Uk, Uk + gradK * c};
+  const double dfix = 0.5 * (entropy_fix_delta(z, g0) + entropy_fix_delta(z, g1));
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    ch[q] = fabs(ch[q]);
+    if (ch[q] < dfix) ch[q] = 0.5 * (ch[q] * ch[q] / dfix + dfix);
+  }
+  kx /= gradK;
+  ky /= gradK;
+  kz /= gradK;
+  Uk /= gradK;
+  const double jac_ave = 0.5 * (j0 + j1);
+  double dq[NV];
+  dq[0] = jac_ave * (pr[0] - pl[0]);
+#pragma unroll
+  for (int l = 1; l < NV; ++l) dq[l] = jac_ave * (pr[0] * pr[l] - pl[0] * pl[l]);
+  dq[4] = jac_ave * (pr[NV] - pl[NV]);
+  double c1 = (gamma - 1) * (ek * dq[0] - u * dq[1] - v * dq[2] - w * dq[3] + dq[4]) / (c * c);
+  double c2 = (kx * dq[1] + ky * dq[2] + kz * dq[3] - Uk * dq[0]) / c;
+#pragma unroll
+  for (int l = 0; l < NS; ++l) c1 += (mw / c_p.mw[l] - h_i[l] * (gamma - 1) / (c * c)) * dq[l + 5];
+  double c3 = dq[0] - c1;
+  double b[NV];
+  {
+    double L[NV];
+    L[0] = 0.5 * (c1 - c2);
+    L[1] = kx * c3 - ((kz * v - ky * w) * dq[0] - kz * dq[2] + ky * dq[3]) / c;
+    L[2] = ky * c3 - ((kx * w - kz * u) * dq[0] - kx * dq[3] + kz * dq[1]) / c;
+    L[3] = kz * c3 - ((ky * u - kx * v) * dq[0] - ky * dq[1] + kx * dq[2]) / c;
+    L[4] = 0.5 * (c1 + c2);
+#pragma unroll
+    for (int l = 0; l < NS; ++l) L[l + 5] = dq[l + 5] - svm[l] * dq[0];
+    b[0] = -ch[0] * L[0];
+#pragma unroll
+    for (int l = 1; l < NV; ++l) b[l] = -ch[1] * L[l];
+    b[4] = -ch[2] * L[4];
+  }
+  const double c0 = kx * b[1] + ky * b[2] + kz * b[3];
+  c1 = c0 + b[0] + b[4];
+  c2 = c * (b[4] - b[0]);
+  c3 = 0;
+#pragma unroll
+  for (int l = 0; l < NS; ++l) c3 += (h_i[l] - mw / c_p.mw[l] * c * c / (gamma - 1)) * b[l + 5];
+  F[0] += 0.5 * c1;
+  F[1] += 0.5 * (u * c1 + kx * c2 - c * (kz * b[2] - ky * b[3]));
+  F[2] += 0.5 * (v * c1 + ky * c2 - c * (kx * b[3] - kz * b[1]));
+  F[3] += 0.5 * (w * c1 + kz * c2 - c * (ky * b[1] - kx * b[2]));
+  F[4] += 0.5 * (h * c1 + Uk * c2 - c * c * c0 / (gamma - 1) +
+                 c * ((kz * v - ky * w) * b[1] + (kx * w - kz * u) * b[2] + (ky * u - kx * v) * b[3]) + c3);
+#pragma unroll
+  for (int l = 0; l < NS; ++l) F[5 + l] += 0.5 * (b[l + 5] + svm[l] * c1);
 }
 
 // ---------------------------------------------------------------------------

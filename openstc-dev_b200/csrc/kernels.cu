@@ -38,6 +38,8 @@ __device__ __forceinline__ void face_total(const DevZone &z, int g0, bool viscou
   double Fi[NV];
   if constexpr (INV == 1)
     inviscid_face_aweno<DIR>(z, g0, Fi);
+  else if constexpr (INV == 2)
+    inviscid_face_roe<NS, DIR>(z, g0, Fi);
   else
     inviscid_face_pv<NS, DIR>(z, g0, Fi);
   if (viscous) {
@@ -605,6 +607,13 @@ cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, 
         case 1: return launch_flux_t<0, 1, 1>(z, t, accumulate, viscous, s);
         default: return launch_flux_t<0, 1, 2>(z, t, accumulate, viscous, s);
       }
+    }
+  }
+  if (inv == 2) {
+    switch (dir) {
+      case 0: return launch_flux_t<NS, 2, 0>(z, t, accumulate, viscous, s);
+      case 1: return launch_flux_t<NS, 2, 1>(z, t, accumulate, viscous, s);
+      default: return launch_flux_t<NS, 2, 2>(z, t, accumulate, viscous, s);
     }
   }
   switch (dir) {

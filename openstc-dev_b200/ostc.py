@@ -566,15 +566,19 @@ def air_state(mach, T, p):
     return dict(density=rho, u=mach * a, v=0.0, w=0.0, pressure=p, temperature=T, velocity=mach * a, mut=0.0)
 
 
-def case_vortex(mx=128, my=128, mz=8, dx=1e-3, k_bc="periodic", steps=100, fixed_dt=None) -> Case:
+def case_vortex(mx=128, my=128, mz=8, dx=1e-3, k_bc="periodic", steps=100, fixed_dt=None, reconstruction=4,
+                inviscid_scheme=2) -> Case:
     """The single-species air workload: a Mach 2 stream (T = 300 K,
     p = 101325 Pa) along +x with an isentropic vortex (strength 0.3 U_inf,
     radius 5 dx) at the domain centre; AWENO-5 with the Roe tag (which runs
     AUSM+ in the reference, quirk A1), laminar Sutherland viscosity, RK3 at
     CFL 0.5. Supersonic inlet at i-min, supersonic outlet at i-max, symmetry
     on the j faces, periodic in k (k_bc="periodic") or symmetry in k
-    (k_bc="symmetry", a configuration the reference itself can run)."""
-    s = Scheme(mix_model=MIX_AIR, inviscid_scheme=2, reconstruction=4, viscous_order=2, cfl=0.5)
+    (k_bc="symmetry", a configuration the reference itself can run).
+    Other reconstruction / flux tags give the other air schemes (2 + 2 is the
+    Roe flux-difference splitting with MUSCL)."""
+    s = Scheme(mix_model=MIX_AIR, inviscid_scheme=inviscid_scheme, reconstruction=reconstruction, viscous_order=2,
+               cfl=0.5)
     if fixed_dt:
         s.fixed_time_step, s.dt = 1, fixed_dt
     ng = s.ngg

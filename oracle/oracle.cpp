@@ -590,6 +590,110 @@ void lax_friedrichs(const ostc_param *P, const double *pl, const double *pr, con
   fci[4] = ((pl[nv] + pl[4]) * Ukl + (pr[nv] + pr[4]) * Ukr - sr * (pr[nv] - pl[nv])) * hj;
 }
 
+// Roe flux-difference splitting with the Harten entropy fix: compute_half_sum_left_right_flux
+// (Roe.cu:339-375) + Roe_compute_half_point_flux (Roe.cu:186-337). delta: entropy-fix width per point.
+void roe_flux(const ostc_param *P, const double *pl, const double *pr, const double *met, const double *jac,
+              const double *delta, int is, double *fc) {
+  const int nv = P->n_var;
+  double JacKx = jac[is] * met[is * 3], JacKy = jac[is] * met[is * 3 + 1], JacKz = jac[is] * met[is * 3 + 2];
+  double Uk = pl[1] * JacKx + pl[2] * JacKy + pl[3] * JacKz;
+  double coeff = Uk * pl[0];
+  fc[0] = 0.5 * coeff;
+  fc[1] = 0.5 * (coeff * pl[1] + pl[4] * JacKx);
+  fc[2] = 0.5 * (coeff * pl[2] + pl[4] * JacKy);
+  fc[3] = 0.5 * (coeff * pl[3] + pl[4] * JacKz);
+  fc[4] = 0.5 * Uk * (pl[4] + pl[nv]);
+  for (int l = 5; l < nv; ++l) fc[l] = 0.5 * coeff * pl[l];
+  JacKx = jac[is + 1] * met[(is + 1) * 3];
+  JacKy = jac[is + 1] * met[(is + 1) * 3 + 1];
+  JacKz = jac[is + 1] * met[(is + 1) * 3 + 2];
+  Uk = pr[1] * JacKx + pr[2] * JacKy + pr[3] * JacKz;
+  coeff = Uk * pr[0];
+  fc[0] += 0.5 * coeff;
+  fc[1] += 0.5 * (coeff * pr[1] + pr[4] * JacKx);
+  fc[2] += 0.5 * (coeff * pr[2] + pr[4] * JacKy);
+  fc[3] += 0.5 * (coeff * pr[3] + pr[4] * JacKz);
+  fc[4] += 0.5 * Uk * (pr[4] + pr[nv]);
+  for (int l = 5; l < nv; ++l) fc[l] += 0.5 * coeff * pr[l];
+
+  const double dl = std::sqrt(pl[0]), dr = std::sqrt(pr[0]);
+  const double inv_den = 1.0 / (dl + dr);
+  const double u = (dl * pl[1] + dr * pr[1]) * inv_den;
+  const double v = (dl * pl[2] + dr * pr[2]) * inv_den;
+  const double w = (dl * pl[3] + dr * pr[3]) * inv_den;
+  const double ek = 0.5 * (u * u + v * v + w * w);
+  const double hl = (pl[nv] + pl[4]) / pl[0], hr = (pr[nv] + pr[4]) / pr[0];
+  const double h = (dl * hl + dr * hr) * inv_den;
+  double gamma = gamma_air;
+  double c = std::sqrt((gamma - 1) * (h - ek));
+  double mw = mw_air;
+  double svm[MAXS + 4] = {0}, h_i[MAXS] = {0};
+  for (int l = 0; l < nv - 5; ++l) svm[l] = (dl * pl[l + 5] + dr * pr[l + 5]) * inv_den;
+  if (P->mix_model != OSTC_MIX_AIR) {
+    double mw_inv = 0;
+    for (int l = 0; l < P->n_spec; ++l) mw_inv += svm[l] / P->mw[l];
+    const double tl = pl[4] / pl[0], tr = pr[4] / pr[0];
+    const double t = (dl * tl + dr * tr) * inv_den / (R_u * mw_inv);
+    double cp_i[MAXS];
+    enthalpy_and_cp(P, t, h_i, cp_i);
+    double cv = 0, cp = 0;
+    for (int l = 0; l < P->n_spec; ++l) {
+      cp += cp_i[l] * svm[l];
+      cv += svm[l] * (cp_i[l] - R_u / P->mw[l]);
+    }
+    gamma = cp / cv;
+    c = std::sqrt(gamma * R_u * mw_inv * t);
+    mw = 1.0 / mw_inv;
+  }
+  double kx = 0.5 * (met[is * 3] + met[(is + 1) * 3]);
+  double ky = 0.5 * (met[is * 3 + 1] + met[(is + 1) * 3 + 1]);
+  double kz = 0.5 * (met[is * 3 + 2] + met[(is + 1) * 3 + 2]);
+  const double gradK = std::sqrt(kx * kx + ky * ky + kz * kz);
+  Uk = kx * u + ky * v + kz * w;
+  double ch[3] = {Uk - gradK * c, Uk, Uk + gradK * c};
+  const double dfix = 0.5 * (delta[is] + delta[is + 1]);
+  for (double &cc : ch) {
+    cc = std::abs(cc);
+    if (cc < dfix) cc = 0.5 * (cc * cc / dfix + dfix);
+  }
+  kx /= gradK;
+  ky /= gradK;
+  kz /= gradK;
+  Uk /= gradK;
+  const double jac_ave = 0.5 * (jac[is] + jac[is + 1]);
+  double dq[5 + MAXS + 4] = {0};
+  dq[0] = jac_ave * (pr[0] - pl[0]);
+  for (int l = 1; l < nv; ++l) dq[l] = jac_ave * (pr[0] * pr[l] - pl[0] * pl[l]);
+  dq[4] = jac_ave * (pr[nv] - pl[nv]);
+  double c1 = (gamma - 1) * (ek * dq[0] - u * dq[1] - v * dq[2] - w * dq[3] + dq[4]) / (c * c);
+  double c2 = (kx * dq[1] + ky * dq[2] + kz * dq[3] - Uk * dq[0]) / c;
+  for (int l = 0; l < P->n_spec; ++l) c1 += (mw / P->mw[l] - h_i[l] * (gamma - 1) / (c * c)) * dq[l + 5];
+  double c3 = dq[0] - c1;
+  double L[5 + MAXS + 4] = {0};
+  L[0] = 0.5 * (c1 - c2);
+  L[1] = kx * c3 - ((kz * v - ky * w) * dq[0] - kz * dq[2] + ky * dq[3]) / c;
+  L[2] = ky * c3 - ((kx * w - kz * u) * dq[0] - kx * dq[3] + kz * dq[1]) / c;
+  L[3] = kz * c3 - ((ky * u - kx * v) * dq[0] - ky * dq[1] + kx * dq[2]) / c;
+  L[4] = 0.5 * (c1 + c2);
+  for (int l = 0; l < P->n_scalar; ++l) L[l + 5] = dq[l + 5] - svm[l] * dq[0];
+  double *b = dq;
+  b[0] = -ch[0] * L[0];
+  for (int l = 1; l < nv; ++l) b[l] = -ch[1] * L[l];
+  b[4] = -ch[2] * L[4];
+  const double c0 = kx * b[1] + ky * b[2] + kz * b[3];
+  c1 = c0 + b[0] + b[4];
+  c2 = c * (b[4] - b[0]);
+  c3 = 0;
+  for (int l = 0; l < P->n_spec; ++l) c3 += (h_i[l] - mw / P->mw[l] * c * c / (gamma - 1)) * b[l + 5];
+  fc[0] += 0.5 * c1;
+  fc[1] += 0.5 * (u * c1 + kx * c2 - c * (kz * b[2] - ky * b[3]));
+  fc[2] += 0.5 * (v * c1 + ky * c2 - c * (kx * b[3] - kz * b[1]));
+  fc[3] += 0.5 * (w * c1 + kz * c2 - c * (ky * b[1] - kx * b[2]));
+  fc[4] += 0.5 * (h * c1 + Uk * c2 - c * c * c0 / (gamma - 1) +
+                  c * ((kz * v - ky * w) * b[1] + (kx * w - kz * u) * b[2] + (ky * u - kx * v) * b[3]) + c3);
+  for (int l = 0; l < nv - 5; ++l) fc[5 + l] += 0.5 * (b[l + 5] + svm[l] * c1);
+}
+
 void riemann(const ostc_param *P, const double *pl, const double *pr, const double *met,
              const double *jac, int is, double *fci) {  // InviscidScheme.cu:137-150
   switch (P->inviscid_scheme) {
@@ -759,11 +863,12 @@ void inviscid_direction(const ostc_param *P, Z &Zn, int d) {
   const int na = ext[oa], nb = ext[ob];
   const int nv = P->n_var;
   const bool aweno = P->inviscid_type == 1;
+  const bool roe = P->inviscid_type == 2;
   const int nrow = aweno ? nv + 2 : nv;
   const int npt = n + 2 * ngg;  // line points -ngg .. n+ngg-1 at index s+ngg
 #pragma omp parallel
   {
-    std::vector<double> rows(npt * nrow), met(npt * 3), jac(npt), fc((n + 1) * nv), f(npt * 5);
+    std::vector<double> rows(npt * nrow), met(npt * 3), jac(npt), fc((n + 1) * nv), f(npt * 5), delta(npt);
     double pl[MAXS + 11], pr[MAXS + 11];
 #pragma omp for collapse(2) schedule(static)
     for (int b = 0; b < nb; ++b) {
@@ -783,6 +888,16 @@ void inviscid_direction(const ostc_param *P, Z &Zn, int d) {
           const double *m = Zn.metric.at(i, j, k);
           for (int c = 0; c < 3; ++c) met[is * 3 + c] = m[3 * d + c];
           jac[is] = Zn.jac(i, j, k);
+          if (roe && s >= -1 && s <= n) {  // compute_entropy_fix_delta on [-1, m] (Roe.cu:61-85), 3-D
+            const double u = Zn.bv(i, j, k, 1), v = Zn.bv(i, j, k, 2), w = Zn.bv(i, j, k, 3);
+            const double U = std::abs(u * m[0] + v * m[1] + w * m[2]);
+            const double V = std::abs(u * m[3] + v * m[4] + w * m[5]);
+            const double W = std::abs(u * m[6] + v * m[7] + w * m[8]);
+            const double kx = std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+            const double ky = std::sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
+            const double kz = std::sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
+            delta[is] = P->entropy_fix_factor * (U + V + W + Zn.a(i, j, k) * (kx + ky + kz) / 3.0);
+          }
         }
         // face fluxes for s = -1 .. n-1 (face between s and s+1), stored at s+1
         for (int s = -1; s < n; ++s) {
@@ -791,7 +906,10 @@ void inviscid_direction(const ostc_param *P, Z &Zn, int d) {
             aweno_interpolation(P, rows.data(), pl, pr, is, met.data());
           else
             reconstruct(P, rows.data(), pl, pr, is, nv);
-          riemann(P, pl, pr, met.data(), jac.data(), is, &fc[(s + 1) * nv]);
+          if (roe)
+            roe_flux(P, pl, pr, met.data(), jac.data(), delta.data(), is, &fc[(s + 1) * nv]);
+          else
+            riemann(P, pl, pr, met.data(), jac.data(), is, &fc[(s + 1) * nv]);
           note_scale(&fc[(s + 1) * nv], nv);
         }
         for (int s = 0; s < n; ++s) {
@@ -1242,7 +1360,6 @@ int oracle_flux_scale(const ostc_param *P, ostc_zone *z, double *scale) {
 }
 
 int oracle_compute_rhs(const ostc_param *P, ostc_zone *z) {
-  if (P->inviscid_type == 2) return OSTC_ERR_UNSUPPORTED;  // Roe: not restated yet
   if (P->inviscid_type == 1 && P->mix_model != OSTC_MIX_AIR) return OSTC_ERR_UNSUPPORTED;  // A2
   if (P->inviscid_scheme == 1 && P->mix_model != OSTC_MIX_AIR) return OSTC_ERR_UNSUPPORTED;
   Z Zn(z);

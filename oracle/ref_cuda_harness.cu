@@ -172,6 +172,7 @@ void build_zone(RefCtx &c, const ostc_zone *z, const ostc_param *p) {
   h.dt_local.allocate_memory(mx, my, mz, 0);
   h.unphysical.allocate_memory(mx, my, mz, 0);
   h.qn.allocate_memory(mx, my, mz, p->n_var, g);
+  if (p->inviscid_scheme == 2) h.entropy_fix_delta.allocate_memory(mx, my, mz, 1);  // Field.cu:223-226
   h.boundary = nullptr;
   if (!c.faces.empty()) h.boundary = dcopy(c.faces.data(), c.faces.size());
   cudaMalloc(&c.d_zone, sizeof(DZone));
@@ -298,7 +299,7 @@ extern "C" {
 int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, const ostc_bc_face *f, int nf,
                void **out) {
   if (!cfg || !p || !z || !out) return 1;
-  if (p->turbulence || p->inviscid_type == 2 || (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_FR))
+  if (p->turbulence || (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_FR))
     return 5;
   auto *c = new RefCtx;
   c->cfg = *cfg;

@@ -48,8 +48,8 @@ def test_create_rejects_bad_face():
 def test_create_rejects_unsupported_scheme():
     case = ostc.case_vortex(16, 12, 8)
     s = case.scheme
-    s.reconstruction = 2  # inviscid_scheme 2 without WENO -> Roe line kernels, not built
     p, keep = ostc.make_param(s, None)
+    p.turbulence = 1  # RANS / SST is not built: refused before any device use
     cfg = ostc.make_config(s)
     zones = (ostc.Zone * 1)(case.blocks[0].zone())
     ctx = C.c_void_p()

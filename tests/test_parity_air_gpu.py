@@ -121,3 +121,25 @@ def test_deterministic_rerun():
         s.rk3_steps(3)
         outs.append(blocks[0].download("cv"))
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("rec,flux", [(2, 2), (3, 2), (1, 2), (2, 1), (3, 1), (2, 3), (2, 4)])
+def test_rhs_other_air_schemes(rec, flux):
+    # Roe flux-difference splitting (inviscid_type 2), Lax-Friedrichs, AUSM+ and HLLC on
+    # primitive-variable reconstructions
+    case = ostc.case_vortex(36, 28, 9, reconstruction=rec, inviscid_scheme=flux)
+    ref, s, blocks = _rhs_pair(case)
+    err = rhs_errors(blocks[0].download("dq"), ref.blocks[0].arrays["dq"], ref.scale)
+    assert max(err) <= RHS_TOL, err
+
+
+def test_rk3_history_roe():
+    case = ostc.case_vortex(32, 24, 8, reconstruction=2, inviscid_scheme=2)
+    ref = OracleRun(case)
+    ref.initialize()
+    res_o, dt_o = ref.rk3_steps(8)
+    s, blocks = _gpu_solver(case)
+    s.initialize()
+    res_g, dt_g = s.rk3_steps(8, history=True)
+    assert np.max(np.abs(res_g - res_o) / res_o) <= STEP_TOL
+    assert max(normwise(blocks[0].download("bv"), ref.blocks[0].arrays["bv"])) <= STEP_TOL

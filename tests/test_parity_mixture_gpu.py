@@ -39,7 +39,7 @@ def test_properties_match():
         assert np.max(np.abs(got - hb[name])) <= 1e-12 * den, name
 
 
-@pytest.mark.parametrize("rec,flux", [(2, 3), (3, 3), (1, 3), (2, 4), (3, 4)])
+@pytest.mark.parametrize("rec,flux", [(2, 3), (3, 3), (1, 3), (2, 4), (3, 4), (2, 2), (1, 2)])
 @pytest.mark.parametrize("shape", [(24, 20, 8), (33, 17, 10)])
 def test_rhs_matches_oracle(shape, rec, flux):
     case = _case(shape)

@@ -21,14 +21,18 @@ pytestmark = [pytest.mark.gpu,
 
 def _cases(mixing_shape=(28, 24, 10)):
     v = ostc.case_vortex(40, 32, 10, k_bc="symmetry")
+    vr = ostc.case_vortex(40, 32, 10, k_bc="symmetry", reconstruction=2, inviscid_scheme=2)
     m = ostc.case_mixing_layer(*mixing_shape, full_host=True)
-    for f in m.faces:
-        if f.type_label == ostc.BC_PERIODIC:
-            f.type_label = ostc.BC_OUTFLOW
-    return {"vortex": v, "mixing": m}
+    mr = ostc.case_mixing_layer(*mixing_shape, full_host=True)
+    mr.scheme.inviscid_scheme = 2
+    for c in (m, mr):
+        for f in c.faces:
+            if f.type_label == ostc.BC_PERIODIC:
+                f.type_label = ostc.BC_OUTFLOW
+    return {"vortex": v, "mixing": m, "vortex_roe": vr, "mixing_roe": mr}
 
 
-@pytest.mark.parametrize("name", ["vortex", "mixing"])
+@pytest.mark.parametrize("name", ["vortex", "mixing", "vortex_roe", "mixing_roe"])
 def test_rhs_matches_reference_build(name):
     case = _cases()[name]
     r = ref_bind.RefCudaRun(case)
@@ -61,7 +65,8 @@ def _reduction_well_defined(cells):
     return all(v == 128 or v % 32 for v in (v1, v2))
 
 
-@pytest.mark.parametrize("name,n,shape", [("vortex", 100, None), ("mixing", 20, (30, 26, 10))])
+@pytest.mark.parametrize("name,n,shape", [("vortex", 100, None), ("mixing", 20, (30, 26, 10)),
+                                          ("vortex_roe", 30, None), ("mixing_roe", 10, (30, 26, 10))])
 def test_history_matches_reference_build(name, n, shape):
     # sizes where the reference's block reductions (dt minimum, residual sums)
     # are well defined; see test_reference_reduction_defect_arbitrated_by_oracle
