@@ -132,8 +132,9 @@ typedef struct ostc_param {
 } ostc_param;
 
 /* One boundary face of one block: cfd::Boundary (src/Mesh.h:9-31) after
- * register_boundary (ranges already widened by ngg on tangential axes),
- * with the state of the boundary condition attached (src/BoundCond.h).    */
+ * register_boundary (ranges already widened by ngg on tangential axes; wall
+ * faces trimmed back by ngg as DBoundCond::initialize_bc_on_GPU does,
+ * src/BoundCond.cu:369-387), with the state of its condition (src/BoundCond.h). */
 typedef struct ostc_bc_face {
   int block;                 /* zone index                                   */
   int type_label;            /* OSTC_BC_*                                    */
@@ -146,6 +147,12 @@ typedef struct ostc_bc_face {
   /* wall (cfd::Wall): isothermal flag and temperature                       */
   int wall_isothermal;
   double wall_temperature;
+  /* farfield (cfd::FarField, src/BoundCond.h:65-87): free-stream sound speed,
+   * entropy p/rho^gamma, gamma and molar mass; subsonic inflow
+   * (cfd::SubsonicInflow): total pressure and temperature, u/v/w = direction;
+   * back pressure (cfd::BackPressure): the pressure field above             */
+  double acoustic_speed, entropy, specific_heat_ratio, mw;
+  double total_pressure, total_temperature;
 } ostc_bc_face;
 
 /* Options of the time-advance path (the relevant keys of 2_scheme.txt). */

@@ -196,7 +196,13 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
     switch (f.type_label) {
       case OSTC_BC_INFLOW:
       case OSTC_BC_OUTFLOW:
-      case OSTC_BC_SYMMETRY: break;
+      case OSTC_BC_SYMMETRY:
+      case OSTC_BC_WALL:
+      case OSTC_BC_FARFIELD:
+      case OSTC_BC_BACK_PRESSURE: break;
+      case OSTC_BC_SUBSONIC_INFLOW:
+        if (p->n_spec > 0) return OSTC_ERR_UNSUPPORTED;  // air only (BoundCond.cpp:300-305)
+        break;
       case OSTC_BC_PERIODIC:
         if (ext[f.face] < z.ngg) return OSTC_ERR_INVALID_ARG;
         break;
@@ -377,6 +383,14 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
     b.velocity = f.velocity;
     b.mut = f.mut;
     for (int l = 0; l < OSTC_MAX_SPEC + 4; ++l) b.sv[l] = f.sv[l];
+    b.wall_isothermal = f.wall_isothermal;
+    b.wall_temperature = f.wall_temperature;
+    b.acoustic_speed = f.acoustic_speed;
+    b.entropy = f.entropy;
+    b.specific_heat_ratio = f.specific_heat_ratio;
+    b.mw = f.mw;
+    b.total_pressure = f.total_pressure;
+    b.total_temperature = f.total_temperature;
     c->faces.push_back(b);
     c->face_zone.push_back(f.block);
   }

@@ -495,6 +495,243 @@ __global__ void bc_periodic_kernel(DevZone z, BcFace b, int with_cv) {
   }
 }
 
+// isothermal / adiabatic no-slip wall, laminar (BoundCond.cuh:415-526)
+template <int NS>
+__global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
+  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = b.rs[2] + blockIdx.z;
+  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+  const int g = gidx(z, i, j, k);
+  const int step = b.dir_stride;
+  const int gin = g - step;
+  double t_wall = b.wall_temperature;
+  if (!b.wall_isothermal) t_wall = z.bv[5 * z.sz + gin];
+  const double p = z.bv[4 * z.sz + gin];
+  double mw = mw_air;
+  if constexpr (NS > 0) {
+    mw = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      z.sv[l * z.sz + g] = z.sv[l * z.sz + gin];
+      mw += z.sv[l * z.sz + g] / c_p.mw[l];
+    }
+    mw = 1 / mw;
+  }
+  const double rho_wall = p * mw / (t_wall * R_u);
+  z.bv[g] = rho_wall;
+  z.bv[z.sz + g] = 0;
+  z.bv[2 * z.sz + g] = 0;
+  z.bv[3 * z.sz + g] = 0;
+  z.bv[4 * z.sz + g] = p;
+  z.bv[5 * z.sz + g] = t_wall;
+  z.vel[g] = 0;
+  if (with_cv) cv_from_bv_point<NS>(z, g);
+  for (int gg = 1; gg <= z.ngg; ++gg) {
+    const int gi = g - gg * step, go = g + gg * step;
+    const double u_i = z.bv[z.sz + gi], v_i = z.bv[2 * z.sz + gi], w_i = z.bv[3 * z.sz + gi];
+    const double p_i = z.bv[4 * z.sz + gi], t_i = z.bv[5 * z.sz + gi];
+    double t_g = t_i;
+    if (b.wall_isothermal) {
+      t_g = 2 * t_wall - t_i;
+      if (t_g <= 0.1 * t_wall) t_g = t_wall;
+    }
+    if constexpr (NS > 0) {
+      mw = 0;
+#pragma unroll
+      for (int l = 0; l < NS; ++l) {
+        z.sv[l * z.sz + go] = z.sv[l * z.sz + gi];
+        mw += z.sv[l * z.sz + go] / c_p.mw[l];
+      }
+      mw = 1 / mw;
+    }
+    z.bv[go] = p_i * mw / (t_g * R_u);
+    z.bv[z.sz + go] = -u_i;
+    z.bv[2 * z.sz + go] = -v_i;
+    z.bv[3 * z.sz + go] = -w_i;
+    z.bv[4 * z.sz + go] = p_i;
+    z.bv[5 * z.sz + go] = t_g;
+    if (with_cv) cv_from_bv_point<NS>(z, go);
+  }
+}
+
+// Riemann-invariant far field (BoundCond.cuh:212-413); like the reference, it
+// never recomputes cv. The mixture's gamma iteration, unbounded in the
+// reference, stops after 100 sweeps here.
+template <int NS>
+__global__ void bc_farfield_kernel(DevZone z, BcFace b) {
+  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = b.rs[2] + blockIdx.z;
+  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+  const int g = gidx(z, i, j, k);
+  const int step = b.dir_stride;
+  double nx = z.met[(3 * b.face) * z.sz + g], ny = z.met[(3 * b.face + 1) * z.sz + g];
+  double nz = z.met[(3 * b.face + 2) * z.sz + g];
+  const double gni = b.direction / sqrt(nx * nx + ny * ny + nz * nz);
+  nx *= gni;
+  ny *= gni;
+  nz *= gni;
+  const double u_b = z.bv[z.sz + g], v_b = z.bv[2 * z.sz + g], w_b = z.bv[3 * z.sz + g];
+  const double u_face = nx * u_b + ny * v_b + nz * w_b;
+  double gamma_b = gamma_air, mw = mw_air;
+  double sv_b[NS > 0 ? NS : 1];
+  if constexpr (NS > 0) {
+    double mw_inv = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      sv_b[l] = z.sv[l * z.sz + g];
+      mw_inv += sv_b[l] / c_p.mw[l];
+    }
+    gamma_b = z.gam[g];
+    mw = 1.0 / mw_inv;
+  }
+  const double p_b = z.bv[4 * z.sz + g], rho_b = z.bv[g];
+  const double a_b = sqrt(gamma_b * p_b / rho_b);
+  const double mach_b = u_face / a_b;
+  auto fill = [&](double rho, double u, double v, double w, double p, double T, const double *svv, bool node) {
+    for (int gg = node ? 0 : 1; gg <= z.ngg; ++gg) {
+      const int go = g + gg * step;
+      z.bv[go] = rho;
+      z.bv[z.sz + go] = u;
+      z.bv[2 * z.sz + go] = v;
+      z.bv[3 * z.sz + go] = w;
+      z.bv[4 * z.sz + go] = p;
+      z.bv[5 * z.sz + go] = T;
+      for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = svv[l];
+    }
+    if (node) z.vel[g] = sqrt(u * u + v * v + w * w);
+  };
+  if (mach_b <= -1) {
+    fill(b.density, b.u, b.v, b.w, b.pressure, b.temperature, b.sv, true);
+  } else if (mach_b >= 1) {
+    for (int gg = 1; gg <= z.ngg; ++gg) {
+      const int go = g + gg * step;
+      for (int l = 0; l < 6; ++l) z.bv[l * z.sz + go] = z.bv[l * z.sz + g];
+      for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = z.sv[l * z.sz + g];
+    }
+  } else {
+    const double r_pos = u_face + 2 * a_b / (gamma_b - 1);
+    const double u_inf = b.u * nx + b.v * ny + b.w * nz;
+    const double r_neg = u_inf - 2 * b.acoustic_speed / (b.specific_heat_ratio - 1);
+    const double Un = 0.5 * (r_pos + r_neg);
+    double s_b, rho, p, T, u, v, w;
+    if constexpr (NS == 0) {
+      const double c_b = 0.25 * (gamma_air - 1) * (r_pos - r_neg);
+      if (mach_b <= 0) {
+        s_b = b.entropy;
+        u = b.u + (Un - u_inf) * nx;
+        v = b.v + (Un - u_inf) * ny;
+        w = b.w + (Un - u_inf) * nz;
+      } else {
+        s_b = p_b / pow(rho_b, gamma_air);
+        u = u_b + (Un - u_face) * nx;
+        v = v_b + (Un - u_face) * ny;
+        w = w_b + (Un - u_face) * nz;
+      }
+      rho = pow(c_b * c_b / (gamma_air * s_b), 1 / (gamma_air - 1));
+      p = rho * c_b * c_b / gamma_air;
+      T = p * mw_air / (rho * R_u);
+      fill(rho, u, v, w, p, T, sv_b, true);
+    } else {
+      if (mach_b < 0) {
+        u = b.u + (Un - u_inf) * nx;
+        v = b.v + (Un - u_inf) * ny;
+        w = b.w + (Un - u_inf) * nz;
+#pragma unroll
+        for (int l = 0; l < NS; ++l) sv_b[l] = b.sv[l];
+        mw = b.mw;
+      } else {
+        u = u_b + (Un - u_face) * nx;
+        v = v_b + (Un - u_face) * ny;
+        w = w_b + (Un - u_face) * nz;
+      }
+      double gamma = gamma_air, err = 1, gamma_last;
+      for (int it = 0; it < 100 && err > 1e-4; ++it) {
+        gamma_last = gamma;
+        const double c_b = 0.25 * (gamma - 1) * (r_pos - r_neg);
+        s_b = mach_b <= 0 ? b.entropy : p_b / pow(rho_b, gamma);
+        rho = pow(c_b * c_b / (gamma * s_b), 1 / (gamma - 1));
+        p = rho * c_b * c_b / gamma;
+        T = p * mw / (rho * R_u);
+        double cp[NS];
+        cp_only<NS>(T, cp);
+        double cp_tot = 0;
+#pragma unroll
+        for (int l = 0; l < NS; ++l) cp_tot += cp[l] * sv_b[l];
+        gamma = cp_tot / (cp_tot - R_u / mw);
+        err = fabs(1 - gamma / gamma_last);
+      }
+      fill(rho, u, v, w, p, T, sv_b, true);
+    }
+  }
+}
+
+// back pressure: extrapolate all but p (BoundCond.cuh:636-671)
+template <int NS>
+__global__ void bc_back_pressure_kernel(DevZone z, BcFace b, int with_cv) {
+  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = b.rs[2] + blockIdx.z;
+  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+  const int g = gidx(z, i, j, k);
+  for (int gg = 1; gg <= z.ngg; ++gg) {
+    const int go = g + gg * b.dir_stride;
+    for (int l = 0; l < 4; ++l) z.bv[l * z.sz + go] = z.bv[l * z.sz + g];
+    z.bv[4 * z.sz + go] = b.pressure;
+    z.bv[5 * z.sz + go] = z.bv[5 * z.sz + g];
+    for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = z.sv[l * z.sz + g];
+    if (with_cv) cv_from_bv_point<NS>(z, go);
+  }
+}
+
+// subsonic inflow from total conditions, air (BoundCond.cuh:528-634)
+__global__ void bc_subsonic_inflow_kernel(DevZone z, BcFace b, int with_cv) {
+  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = b.rs[2] + blockIdx.z;
+  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+  const int g = gidx(z, i, j, k);
+  double nx = z.met[(3 * b.face) * z.sz + g], ny = z.met[(3 * b.face + 1) * z.sz + g];
+  double nz = z.met[(3 * b.face + 2) * z.sz + g];
+  const double gni = b.direction / sqrt(nx * nx + ny * ny + nz * nz);
+  nx *= gni;
+  ny *= gni;
+  nz *= gni;
+  const double rho0 = z.bv[g], u0 = z.bv[z.sz + g], v0 = z.bv[2 * z.sz + g], w0 = z.bv[3 * z.sz + g];
+  const double p0 = z.bv[4 * z.sz + g];
+  const double u_face = nx * u0 + ny * v0 + nz * w0;
+  const double a = sqrt(gamma_air * p0 / rho0);
+  const double r_neg = fabs(u_face) - 2 * a / (gamma_air - 1);
+  const double hti = p0 / rho0 * gamma_air / (gamma_air - 1) + 0.5 * (u0 * u0 + v0 * v0 + w0 * w0);
+  constexpr double qa = 1 + 2.0 / (gamma_air - 1);
+  const double qb = 2 * r_neg;
+  const double qc = (gamma_air - 1) * (0.5 * r_neg * r_neg - hti);
+  const double delta = qb * qb - 4 * qa * qc;
+  double a_new = a;
+  if (delta >= 0) {
+    const double ap = (-qb + sqrt(delta)) / (2 * qa), am = (-qb - sqrt(delta)) / (2 * qa);
+    a_new = ap > am ? ap : am;
+  }
+  const double u_new = r_neg + 2 * a_new / (gamma_air - 1);
+  const double mach = u_new / a_new;
+  const double p = b.total_pressure * pow(1 + 0.5 * (gamma_air - 1) * mach * mach, -gamma_air / (gamma_air - 1));
+  const double T = b.total_temperature * pow(p / b.total_pressure, (gamma_air - 1) / gamma_air);
+  const double rho = p * mw_air / (T * R_u);
+  for (int gg = 1; gg <= z.ngg; ++gg) {
+    const int go = g + gg * b.dir_stride;
+    z.bv[go] = rho;
+    z.bv[z.sz + go] = u_new * b.u;
+    z.bv[2 * z.sz + go] = u_new * b.v;
+    z.bv[3 * z.sz + go] = u_new * b.w;
+    z.bv[4 * z.sz + go] = p;
+    z.bv[5 * z.sz + go] = T;
+    const double u_bar = z.bv[z.sz + go] * nx + z.bv[2 * z.sz + go] * ny + z.bv[3 * z.sz + go] * nz;
+    for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = u_bar > 0 ? z.sv[l * z.sz + g] : b.sv[l];
+    if (with_cv) cv_from_bv_point<0>(z, go);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // residual: store_last_step (TimeAdvanceFunc.cu:6-17), square of the change
 // and deterministic two-level sums (Residual.cuh:57-111, Residual.cu:49-89)
@@ -674,6 +911,10 @@ cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream
     case OSTC_BC_INFLOW: bc_inflow_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
     case OSTC_BC_SYMMETRY: bc_symmetry_kernel<<<grid, blk, 0, s>>>(z, b); break;
     case OSTC_BC_PERIODIC: bc_periodic_kernel<<<grid, blk, 0, s>>>(z, b, with_cv); break;
+    case OSTC_BC_WALL: bc_wall_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
+    case OSTC_BC_FARFIELD: bc_farfield_kernel<NS><<<grid, blk, 0, s>>>(z, b); break;
+    case OSTC_BC_BACK_PRESSURE: bc_back_pressure_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
+    case OSTC_BC_SUBSONIC_INFLOW: bc_subsonic_inflow_kernel<<<grid, blk, 0, s>>>(z, b, with_cv); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -21,6 +21,10 @@ struct BcFace {
   int period_stride;  // periodic: ghosted-index stride of n cells along the normal
   double density, u, v, w, pressure, temperature, velocity, mut;
   double sv[OSTC_MAX_SPEC + 4];
+  int wall_isothermal;
+  double wall_temperature;
+  double acoustic_speed, entropy, specific_heat_ratio, mw;
+  double total_pressure, total_temperature;
 };
 
 enum class CellOp { Source, UpdateRK, Properties, CvFromBv, Velocity, Dt, DtReset, StoreLast, ResidualPartial };

@@ -78,7 +78,9 @@ class BcFaceC(C.Structure):
                 ("density", C.c_double), ("u", C.c_double), ("v", C.c_double), ("w", C.c_double),
                 ("pressure", C.c_double), ("temperature", C.c_double), ("velocity", C.c_double),
                 ("mut", C.c_double), ("sv", C.c_double * (MAX_SPEC + 4)),
-                ("wall_isothermal", C.c_int), ("wall_temperature", C.c_double)]
+                ("wall_isothermal", C.c_int), ("wall_temperature", C.c_double),
+                ("acoustic_speed", C.c_double), ("entropy", C.c_double), ("specific_heat_ratio", C.c_double),
+                ("mw", C.c_double), ("total_pressure", C.c_double), ("total_temperature", C.c_double)]
 
 
 class Config(C.Structure):
@@ -365,23 +367,54 @@ class DeviceBlock:
 # ---------------------------------------------------------------------------
 def bc_face(block: int, label: int, face: int, direction: int, ext, ngg, state: Optional[dict] = None) -> BcFaceC:
     """A face of one block after Boundary::register_boundary (src/Mesh.cpp:14-32):
-    the tangential ranges are widened by ngg."""
+    the tangential ranges are widened by ngg; wall faces are trimmed back by
+    ngg as DBoundCond::initialize_bc_on_GPU does (src/BoundCond.cu:369-387)."""
     f = BcFaceC()
     f.block, f.type_label, f.face, f.direction = block, label, face, direction
+    trim = ngg if label == BC_WALL else 0
     for d in range(3):
         if d == face:
             v = 0 if direction < 0 else ext[d] - 1
             f.range_start[d] = v
             f.range_end[d] = v
         else:
-            f.range_start[d] = -ngg
-            f.range_end[d] = ext[d] - 1 + ngg
+            f.range_start[d] = -ngg + trim
+            f.range_end[d] = ext[d] - 1 + ngg - trim
     if state:
-        for k in ("density", "u", "v", "w", "pressure", "temperature", "velocity", "mut"):
+        for k in ("density", "u", "v", "w", "pressure", "temperature", "velocity", "mut", "acoustic_speed", "entropy",
+                  "specific_heat_ratio", "mw", "total_pressure", "total_temperature", "wall_temperature"):
             setattr(f, k, float(state.get(k, 0.0)))
+        f.wall_isothermal = int(state.get("wall_isothermal", 0))
         for l, y in enumerate(state.get("sv", [])):
             f.sv[l] = float(y)
     return f
+
+
+def farfield_state(mach, T, p, direction=(1.0, 0.0, 0.0), mech: Optional[Mechanism] = None, Y=None):
+    """The state of cfd::FarField for (mach, pressure, temperature) input
+    (src/BoundCond.cpp:184-266): sound speed, velocity, density, entropy."""
+    mw, gamma, sv = MW_AIR, GAMMA_AIR, []
+    if mech is not None:
+        Y = np.asarray(Y, dtype=float)
+        t = mech.tables
+        mw = 1.0 / float(np.sum(Y / t["mw"]))
+        cp_i = np.empty(len(Y))
+        for i in range(len(Y)):
+            if T < t["t_low"][i]:
+                c, tt = t["low_temp_coeff"][i], t["t_low"][i]
+            else:
+                c, tt = (t["low_temp_coeff"][i] if T < t["t_mid"][i] else t["high_temp_coeff"][i]), T
+            cp_i[i] = (c[0] + c[1] * tt + c[2] * tt ** 2 + c[3] * tt ** 3 + c[4] * tt ** 4) * R_U / t["mw"][i]
+        cp = float(np.sum(Y * cp_i))
+        cv = float(np.sum(Y * (cp_i - R_U / t["mw"])))
+        gamma = cp / cv
+        sv = list(Y)
+    a = math.sqrt(gamma * R_U / mw * T)
+    vel = mach * a
+    rho = p * mw / (R_U * T)
+    return dict(density=rho, u=direction[0] * vel, v=direction[1] * vel, w=direction[2] * vel, pressure=p,
+                temperature=T, velocity=vel, acoustic_speed=a, entropy=p / rho ** gamma, specific_heat_ratio=gamma,
+                mw=mw, sv=sv)
 
 
 # ---------------------------------------------------------------------------
@@ -611,6 +644,47 @@ def case_vortex(mx=128, my=128, mz=8, dx=1e-3, k_bc="periodic", steps=100, fixed
     else:
         faces += [bc_face(0, BC_SYMMETRY, 2, -1, ext, ng), bc_face(0, BC_SYMMETRY, 2, 1, ext, ng)]
     return Case("vortex_air_%dx%dx%d" % (mx, my, mz), s, None, [b], faces, steps)
+
+
+def case_bc_box(kind="wall_farfield", mx=40, my=32, mz=10, dx=1e-3) -> Case:
+    """Air box exercising the wall, far-field, back-pressure and subsonic
+    inflow conditions: a Mach 0.5 stream (300 K, 1 atm) with the vortex of
+    case_vortex, MUSCL + AUSM+, laminar; symmetry in k (runnable by the
+    reference build).
+    kind="wall_farfield": far field at i-min and j-max, back pressure at
+    i-max, isothermal 300 K wall at j-min.
+    kind="subsonic": subsonic inflow (total conditions of the stream) at i-min,
+    back pressure at i-max, adiabatic wall at j-min, symmetry at j-max."""
+    c = case_vortex(mx, my, mz, dx, k_bc="symmetry", reconstruction=2, inviscid_scheme=3)
+    b = c.blocks[0]
+    ng = b.ngg
+    ff = farfield_state(0.5, 300.0, 101325.0)
+    # re-scale the vortex field to the Mach 0.5 stream
+    bv = b.arrays["bv"]
+    scale = ff["u"] / air_state(2.0, 300.0, 101325.0)["u"]
+    bv[1] *= scale
+    bv[2] *= scale
+    Rg = R_U / MW_AIR
+    bv[5] = 300.0 - (300.0 - bv[5]) * scale ** 2
+    bv[0] = ff["density"] * (bv[5] / 300.0) ** (1 / (GAMMA_AIR - 1))
+    bv[4] = bv[0] * Rg * bv[5]
+    ext = (mx, my, mz)
+    wall = dict(wall_isothermal=1, wall_temperature=300.0)
+    bp = dict(pressure=101325.0)
+    if kind == "wall_farfield":
+        faces = [bc_face(0, BC_FARFIELD, 0, -1, ext, ng, ff), bc_face(0, BC_BACK_PRESSURE, 0, 1, ext, ng, bp),
+                 bc_face(0, BC_WALL, 1, -1, ext, ng, wall), bc_face(0, BC_FARFIELD, 1, 1, ext, ng, ff)]
+    else:
+        M = 0.5
+        tot = dict(total_pressure=101325.0 * (1 + 0.2 * M * M) ** 3.5, total_temperature=300.0 * (1 + 0.2 * M * M),
+                   u=1.0, v=0.0, w=0.0)
+        faces = [bc_face(0, BC_SUBSONIC_INFLOW, 0, -1, ext, ng, tot), bc_face(0, BC_BACK_PRESSURE, 0, 1, ext, ng, bp),
+                 bc_face(0, BC_WALL, 1, -1, ext, ng, dict(wall_isothermal=0)),
+                 bc_face(0, BC_SYMMETRY, 1, 1, ext, ng)]
+    faces += [bc_face(0, BC_SYMMETRY, 2, -1, ext, ng), bc_face(0, BC_SYMMETRY, 2, 1, ext, ng)]
+    c.faces = faces
+    c.name = "bc_box_%s_%dx%dx%d" % (kind, mx, my, mz)
+    return c
 
 
 # ---------------------------------------------------------------------------

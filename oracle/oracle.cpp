@@ -1265,6 +1265,236 @@ void bc_inflow(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
       }
 }
 
+// no-slip wall, laminar (BoundCond.cuh:415-526)
+void bc_wall(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
+  int dir[3] = {0, 0, 0};
+  dir[b.face] = b.direction;
+  const int ns = P->n_spec;
+  for (int k = b.range_start[2]; k <= b.range_end[2]; ++k)
+    for (int j = b.range_start[1]; j <= b.range_end[1]; ++j)
+      for (int i = b.range_start[0]; i <= b.range_end[0]; ++i) {
+        const int ii = i - dir[0], ij = j - dir[1], ik = k - dir[2];
+        double t_wall = b.wall_temperature;
+        if (!b.wall_isothermal) t_wall = Zn.bv(ii, ij, ik, 5);
+        const double p = Zn.bv(ii, ij, ik, 4);
+        double mw = mw_air;
+        if (P->mix_model != OSTC_MIX_AIR) {
+          mw = 0;
+          for (int l = 0; l < ns; ++l) {
+            Zn.sv(i, j, k, l) = Zn.sv(ii, ij, ik, l);
+            mw += Zn.sv(i, j, k, l) / P->mw[l];
+          }
+          mw = 1 / mw;
+        }
+        const double rho_wall = p * mw / (t_wall * R_u);
+        Zn.bv(i, j, k, 0) = rho_wall;
+        Zn.bv(i, j, k, 1) = 0;
+        Zn.bv(i, j, k, 2) = 0;
+        Zn.bv(i, j, k, 3) = 0;
+        Zn.bv(i, j, k, 4) = p;
+        Zn.bv(i, j, k, 5) = t_wall;
+        Zn.vel(i, j, k) = 0;
+        if (with_cv) cv_from_bv_point(P, Zn, i, j, k);
+        for (int g = 1; g <= Zn.ngg; ++g) {
+          const int ai = i - g * dir[0], aj = j - g * dir[1], ak = k - g * dir[2];
+          const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
+          const double u_i = Zn.bv(ai, aj, ak, 1), v_i = Zn.bv(ai, aj, ak, 2), w_i = Zn.bv(ai, aj, ak, 3);
+          const double p_i = Zn.bv(ai, aj, ak, 4), t_i = Zn.bv(ai, aj, ak, 5);
+          double t_g = t_i;
+          if (b.wall_isothermal) {
+            t_g = 2 * t_wall - t_i;
+            if (t_g <= 0.1 * t_wall) t_g = t_wall;
+          }
+          if (P->mix_model != OSTC_MIX_AIR) {
+            mw = 0;
+            for (int l = 0; l < ns; ++l) {
+              Zn.sv(gi, gj, gk, l) = Zn.sv(ai, aj, ak, l);
+              mw += Zn.sv(gi, gj, gk, l) / P->mw[l];
+            }
+            mw = 1 / mw;
+          }
+          Zn.bv(gi, gj, gk, 0) = p_i * mw / (t_g * R_u);
+          Zn.bv(gi, gj, gk, 1) = -u_i;
+          Zn.bv(gi, gj, gk, 2) = -v_i;
+          Zn.bv(gi, gj, gk, 3) = -w_i;
+          Zn.bv(gi, gj, gk, 4) = p_i;
+          Zn.bv(gi, gj, gk, 5) = t_g;
+          if (with_cv) cv_from_bv_point(P, Zn, gi, gj, gk);
+        }
+      }
+}
+
+// Riemann-invariant far field (BoundCond.cuh:212-413); never recomputes cv
+void bc_farfield(const ostc_param *P, Z &Zn, const ostc_bc_face &b) {
+  int dir[3] = {0, 0, 0};
+  dir[b.face] = b.direction;
+  const int ns = P->n_spec, nsc = P->n_scalar;
+  for (int k = b.range_start[2]; k <= b.range_end[2]; ++k)
+    for (int j = b.range_start[1]; j <= b.range_end[1]; ++j)
+      for (int i = b.range_start[0]; i <= b.range_end[0]; ++i) {
+        const double *m = Zn.metric.at(i, j, k);
+        double nx = m[3 * b.face], ny = m[3 * b.face + 1], nz = m[3 * b.face + 2];
+        const double gni = b.direction / std::sqrt(nx * nx + ny * ny + nz * nz);
+        nx *= gni;
+        ny *= gni;
+        nz *= gni;
+        const double u_b = Zn.bv(i, j, k, 1), v_b = Zn.bv(i, j, k, 2), w_b = Zn.bv(i, j, k, 3);
+        const double u_face = nx * u_b + ny * v_b + nz * w_b;
+        double gamma_b = gamma_air, mw = mw_air, sv_b[MAXS + 4] = {0}, cp[MAXS];
+        if (P->mix_model != OSTC_MIX_AIR) {
+          for (int l = 0; l < nsc; ++l) sv_b[l] = Zn.sv(i, j, k, l);
+          gamma_b = Zn.gam(i, j, k);
+          double mw_inv = 0;
+          for (int l = 0; l < ns; ++l) mw_inv += sv_b[l] / P->mw[l];
+          mw = 1.0 / mw_inv;
+        }
+        const double p_b = Zn.bv(i, j, k, 4), rho_b = Zn.bv(i, j, k, 0);
+        const double a_b = std::sqrt(gamma_b * p_b / rho_b);
+        const double mach_b = u_face / a_b;
+        auto set = [&](int gi, int gj, int gk, double rho, double u, double v, double w, double p, double T,
+                       const double *svv) {
+          Zn.bv(gi, gj, gk, 0) = rho;
+          Zn.bv(gi, gj, gk, 1) = u;
+          Zn.bv(gi, gj, gk, 2) = v;
+          Zn.bv(gi, gj, gk, 3) = w;
+          Zn.bv(gi, gj, gk, 4) = p;
+          Zn.bv(gi, gj, gk, 5) = T;
+          for (int l = 0; l < nsc; ++l) Zn.sv(gi, gj, gk, l) = svv[l];
+        };
+        if (mach_b <= -1) {
+          set(i, j, k, b.density, b.u, b.v, b.w, b.pressure, b.temperature, b.sv);
+          Zn.vel(i, j, k) = std::sqrt(b.u * b.u + b.v * b.v + b.w * b.w);
+          for (int g = 1; g <= Zn.ngg; ++g)
+            set(i + g * dir[0], j + g * dir[1], k + g * dir[2], b.density, b.u, b.v, b.w, b.pressure, b.temperature,
+                b.sv);
+        } else if (mach_b >= 1) {
+          for (int g = 1; g <= Zn.ngg; ++g) {
+            const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
+            for (int l = 0; l < 6; ++l) Zn.bv(gi, gj, gk, l) = Zn.bv(i, j, k, l);
+            for (int l = 0; l < nsc; ++l) Zn.sv(gi, gj, gk, l) = Zn.sv(i, j, k, l);
+          }
+        } else {
+          const double r_pos = u_face + 2 * a_b / (gamma_b - 1);
+          const double u_inf = b.u * nx + b.v * ny + b.w * nz;
+          const double r_neg = u_inf - 2 * b.acoustic_speed / (b.specific_heat_ratio - 1);
+          const double Un = 0.5 * (r_pos + r_neg);
+          double s_b, rho = 0, p = 0, T = 0, u, v, w;
+          if (P->mix_model == OSTC_MIX_AIR) {
+            const double c_b = 0.25 * (gamma_air - 1) * (r_pos - r_neg);
+            if (mach_b <= 0) {
+              s_b = b.entropy;
+              u = b.u + (Un - u_inf) * nx;
+              v = b.v + (Un - u_inf) * ny;
+              w = b.w + (Un - u_inf) * nz;
+              for (int l = 0; l < nsc; ++l) sv_b[l] = b.sv[l];
+            } else {
+              s_b = p_b / std::pow(rho_b, gamma_air);
+              u = u_b + (Un - u_face) * nx;
+              v = v_b + (Un - u_face) * ny;
+              w = w_b + (Un - u_face) * nz;
+            }
+            rho = std::pow(c_b * c_b / (gamma_air * s_b), 1 / (gamma_air - 1));
+            p = rho * c_b * c_b / gamma_air;
+            T = p * mw_air / (rho * R_u);
+          } else {
+            if (mach_b < 0) {
+              u = b.u + (Un - u_inf) * nx;
+              v = b.v + (Un - u_inf) * ny;
+              w = b.w + (Un - u_inf) * nz;
+              for (int l = 0; l < nsc; ++l) sv_b[l] = b.sv[l];
+              mw = b.mw;
+            } else {
+              u = u_b + (Un - u_face) * nx;
+              v = v_b + (Un - u_face) * ny;
+              w = w_b + (Un - u_face) * nz;
+            }
+            double gamma = gamma_air, err = 1, gamma_last;
+            for (int it = 0; it < 100 && err > 1e-4; ++it) {
+              gamma_last = gamma;
+              const double c_b = 0.25 * (gamma - 1) * (r_pos - r_neg);
+              s_b = mach_b <= 0 ? b.entropy : p_b / std::pow(rho_b, gamma);
+              rho = std::pow(c_b * c_b / (gamma * s_b), 1 / (gamma - 1));
+              p = rho * c_b * c_b / gamma;
+              T = p * mw / (rho * R_u);
+              cp_only(P, T, cp);
+              double cp_tot = 0;
+              for (int l = 0; l < ns; ++l) cp_tot += cp[l] * sv_b[l];
+              gamma = cp_tot / (cp_tot - R_u / mw);
+              err = std::abs(1 - gamma / gamma_last);
+            }
+          }
+          set(i, j, k, rho, u, v, w, p, T, sv_b);
+          Zn.vel(i, j, k) = std::sqrt(u * u + v * v + w * w);
+          for (int g = 1; g <= Zn.ngg; ++g) set(i + g * dir[0], j + g * dir[1], k + g * dir[2], rho, u, v, w, p, T, sv_b);
+        }
+      }
+}
+
+// back pressure (BoundCond.cuh:636-671)
+void bc_back_pressure(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
+  int dir[3] = {0, 0, 0};
+  dir[b.face] = b.direction;
+  for (int k = b.range_start[2]; k <= b.range_end[2]; ++k)
+    for (int j = b.range_start[1]; j <= b.range_end[1]; ++j)
+      for (int i = b.range_start[0]; i <= b.range_end[0]; ++i)
+        for (int g = 1; g <= Zn.ngg; ++g) {
+          const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
+          for (int l = 0; l < 4; ++l) Zn.bv(gi, gj, gk, l) = Zn.bv(i, j, k, l);
+          Zn.bv(gi, gj, gk, 4) = b.pressure;
+          Zn.bv(gi, gj, gk, 5) = Zn.bv(i, j, k, 5);
+          for (int l = 0; l < P->n_scalar; ++l) Zn.sv(gi, gj, gk, l) = Zn.sv(i, j, k, l);
+          if (with_cv) cv_from_bv_point(P, Zn, gi, gj, gk);
+        }
+}
+
+// subsonic inflow from total conditions, air (BoundCond.cuh:528-634)
+void bc_subsonic_inflow(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
+  int dir[3] = {0, 0, 0};
+  dir[b.face] = b.direction;
+  for (int k = b.range_start[2]; k <= b.range_end[2]; ++k)
+    for (int j = b.range_start[1]; j <= b.range_end[1]; ++j)
+      for (int i = b.range_start[0]; i <= b.range_end[0]; ++i) {
+        const double *m = Zn.metric.at(i, j, k);
+        double nx = m[3 * b.face], ny = m[3 * b.face + 1], nz = m[3 * b.face + 2];
+        const double gni = b.direction / std::sqrt(nx * nx + ny * ny + nz * nz);
+        nx *= gni;
+        ny *= gni;
+        nz *= gni;
+        const double rho0 = Zn.bv(i, j, k, 0), u0 = Zn.bv(i, j, k, 1), v0 = Zn.bv(i, j, k, 2), w0 = Zn.bv(i, j, k, 3);
+        const double p0 = Zn.bv(i, j, k, 4);
+        const double u_face = nx * u0 + ny * v0 + nz * w0;
+        const double a = std::sqrt(gamma_air * p0 / rho0);
+        const double r_neg = std::abs(u_face) - 2 * a / (gamma_air - 1);
+        const double hti = p0 / rho0 * gamma_air / (gamma_air - 1) + 0.5 * (u0 * u0 + v0 * v0 + w0 * w0);
+        constexpr double qa = 1 + 2.0 / (gamma_air - 1);
+        const double qb = 2 * r_neg;
+        const double qc = (gamma_air - 1) * (0.5 * r_neg * r_neg - hti);
+        const double delta = qb * qb - 4 * qa * qc;
+        double a_new = a;
+        if (delta >= 0) {
+          const double ap = (-qb + std::sqrt(delta)) / (2 * qa), am = (-qb - std::sqrt(delta)) / (2 * qa);
+          a_new = ap > am ? ap : am;
+        }
+        const double u_new = r_neg + 2 * a_new / (gamma_air - 1);
+        const double mach = u_new / a_new;
+        const double p = b.total_pressure * std::pow(1 + 0.5 * (gamma_air - 1) * mach * mach, -gamma_air / (gamma_air - 1));
+        const double T = b.total_temperature * std::pow(p / b.total_pressure, (gamma_air - 1) / gamma_air);
+        const double rho = p * mw_air / (T * R_u);
+        for (int g = 1; g <= Zn.ngg; ++g) {
+          const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
+          Zn.bv(gi, gj, gk, 0) = rho;
+          Zn.bv(gi, gj, gk, 1) = u_new * b.u;
+          Zn.bv(gi, gj, gk, 2) = u_new * b.v;
+          Zn.bv(gi, gj, gk, 3) = u_new * b.w;
+          Zn.bv(gi, gj, gk, 4) = p;
+          Zn.bv(gi, gj, gk, 5) = T;
+          const double u_bar = Zn.bv(gi, gj, gk, 1) * nx + Zn.bv(gi, gj, gk, 2) * ny + Zn.bv(gi, gj, gk, 3) * nz;
+          for (int l = 0; l < P->n_scalar; ++l) Zn.sv(gi, gj, gk, l) = u_bar > 0 ? Zn.sv(i, j, k, l) : b.sv[l];
+          if (with_cv) cv_from_bv_point(P, Zn, gi, gj, gk);
+        }
+      }
+}
+
 // periodic (no reference counterpart): ghost layers wrap from the opposite side
 void bc_periodic(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
   const int ext[3] = {Zn.mx, Zn.my, Zn.mz};
@@ -1440,7 +1670,8 @@ int oracle_apply_boundary_conditions(const ostc_param *P, ostc_zone *zones, int 
                                      const ostc_bc_face *f, int n_faces, int with_cv) {
   // priority order of BoundCond.cuh:673-822: farfield, outflow, back pressure,
   // inflow, subsonic inflow, symmetry, wall; periodic wraps last.
-  static const int order[] = {OSTC_BC_OUTFLOW, OSTC_BC_INFLOW, OSTC_BC_SYMMETRY, OSTC_BC_PERIODIC};
+  static const int order[] = {OSTC_BC_FARFIELD, OSTC_BC_OUTFLOW, OSTC_BC_BACK_PRESSURE, OSTC_BC_INFLOW,
+                              OSTC_BC_SUBSONIC_INFLOW, OSTC_BC_SYMMETRY, OSTC_BC_WALL, OSTC_BC_PERIODIC};
   for (int t : order) {
     for (int q = 0; q < n_faces; ++q) {
       if (f[q].type_label != t) continue;
@@ -1451,14 +1682,14 @@ int oracle_apply_boundary_conditions(const ostc_param *P, ostc_zone *zones, int 
         case OSTC_BC_INFLOW: bc_inflow(P, Zn, f[q], with_cv); break;
         case OSTC_BC_SYMMETRY: bc_symmetry(P, Zn, f[q]); break;  // ignores with_cv (quirk A5)
         case OSTC_BC_PERIODIC: bc_periodic(P, Zn, f[q], with_cv); break;
+        case OSTC_BC_WALL: bc_wall(P, Zn, f[q], with_cv); break;
+        case OSTC_BC_FARFIELD: bc_farfield(P, Zn, f[q]); break;
+        case OSTC_BC_BACK_PRESSURE: bc_back_pressure(P, Zn, f[q], with_cv); break;
+        case OSTC_BC_SUBSONIC_INFLOW: bc_subsonic_inflow(P, Zn, f[q], with_cv); break;
       }
     }
   }
-  for (int q = 0; q < n_faces; ++q) {
-    const int t = f[q].type_label;
-    if (t != OSTC_BC_OUTFLOW && t != OSTC_BC_INFLOW && t != OSTC_BC_SYMMETRY && t != OSTC_BC_PERIODIC)
-      return OSTC_ERR_UNSUPPORTED;
-  }
+
   return 0;
 }
 

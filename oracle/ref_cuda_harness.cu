@@ -52,6 +52,7 @@ struct RefCtx {
   std::vector<int> face_inflow;  // index into inflows, or -1
   std::vector<Inflow *> d_inflows;
   std::vector<double *> d_inflow_sv;
+  std::vector<void *> d_cond;  // per face: device Wall / FarField / SubsonicInflow / BackPressure
 };
 
 template <typename T>
@@ -201,6 +202,21 @@ void apply_bcs(RefCtx &c) {
                                                               c.d_param);
           break;
         case 3: apply_symmetry<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (integer)q, c.d_param); break;
+        case 2:
+          apply_wall<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (Wall *)c.d_cond[q], c.d_param, (integer)q);
+          break;
+        case 4:
+          apply_farfield<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (FarField *)c.d_cond[q], (integer)q,
+                                                                c.d_param);
+          break;
+        case 7:
+          apply_subsonic_inflow<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (SubsonicInflow *)c.d_cond[q],
+                                                                       c.d_param, (integer)q);
+          break;
+        case 9:
+          apply_back_pressure<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (BackPressure *)c.d_cond[q], c.d_param,
+                                                                     (integer)q);
+          break;
         default: break;
       }
     }
@@ -316,7 +332,8 @@ int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, 
   c->parameter->update_parameter("n_spec", p->n_spec);
   c->block = new Block(z->mx, z->my, z->mz, z->ngg, 0);
   for (int q = 0; q < nf; ++q) {
-    if (f[q].type_label != 3 && f[q].type_label != 5 && f[q].type_label != 6) {
+    const int t = f[q].type_label;
+    if (t != 2 && t != 3 && t != 4 && t != 5 && t != 6 && t != 7 && t != 9) {
       delete c;
       return 5;  // the reference has no periodic boundary (quirk A13)
     }
@@ -330,6 +347,58 @@ int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, 
     b.direction = f[q].direction;
     c->faces.push_back(b);
     c->face_inflow.push_back(-1);
+    c->d_cond.push_back(nullptr);
+    // the condition structs have no default constructor: fill zeroed records of their layout
+    double *dsv_c = nullptr;
+    if ((t == 4 || t == 7) && p->n_scalar) dsv_c = dcopy(f[q].sv, p->n_scalar);
+    if (t == 2) {
+      alignas(Wall) unsigned char buf[sizeof(Wall)];
+      std::memset(buf, 0, sizeof(buf));
+      Wall *wl = reinterpret_cast<Wall *>(buf);
+      wl->label = 2;
+      wl->thermal_type = f[q].wall_isothermal ? Wall::ThermalType::isothermal : Wall::ThermalType::adiabatic;
+      wl->temperature = f[q].wall_temperature;
+      c->d_cond.back() = dcopy(wl, 1);
+    } else if (t == 4) {
+      alignas(FarField) unsigned char buf[sizeof(FarField)];
+      std::memset(buf, 0, sizeof(buf));
+      FarField *ff = reinterpret_cast<FarField *>(buf);
+      ff->label = 4;
+      ff->pressure = f[q].pressure;
+      ff->temperature = f[q].temperature;
+      ff->velocity = f[q].velocity;
+      ff->density = f[q].density;
+      ff->u = f[q].u;
+      ff->v = f[q].v;
+      ff->w = f[q].w;
+      ff->acoustic_speed = f[q].acoustic_speed;
+      ff->entropy = f[q].entropy;
+      ff->sv = dsv_c;
+      ff->mw = f[q].mw;
+      ff->mut = f[q].mut;
+      ff->specific_heat_ratio = f[q].specific_heat_ratio;
+      c->d_cond.back() = dcopy(ff, 1);
+    } else if (t == 7) {
+      alignas(SubsonicInflow) unsigned char buf[sizeof(SubsonicInflow)];
+      std::memset(buf, 0, sizeof(buf));
+      SubsonicInflow *si = reinterpret_cast<SubsonicInflow *>(buf);
+      si->label = 7;
+      si->total_pressure = f[q].total_pressure;
+      si->total_temperature = f[q].total_temperature;
+      si->u = f[q].u;
+      si->v = f[q].v;
+      si->w = f[q].w;
+      si->sv = dsv_c;
+      si->mut = f[q].mut;
+      c->d_cond.back() = dcopy(si, 1);
+    } else if (t == 9) {
+      alignas(BackPressure) unsigned char buf[sizeof(BackPressure)];
+      std::memset(buf, 0, sizeof(buf));
+      BackPressure *bp = reinterpret_cast<BackPressure *>(buf);
+      bp->label = 9;
+      bp->pressure = f[q].pressure;
+      c->d_cond.back() = dcopy(bp, 1);
+    }
     if (f[q].type_label == 5) {
       // cfd::Inflow has no default constructor; fill a zeroed record of its layout
       alignas(Inflow) unsigned char buf[sizeof(Inflow)];
