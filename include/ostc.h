@@ -155,6 +155,21 @@ typedef struct ostc_bc_face {
   double total_pressure, total_temperature;
 } ostc_bc_face;
 
+/* One 1-to-1 interface of a block with a block of the same context:
+ * cfd::InnerFace (src/Mesh.h:33-58) after InnerFace::register_boundary
+ * (src/Mesh.cpp:34-178). range_* spans the ghost layers and the coincident
+ * face plane along `face`; point n of the range (n = 0..n_point-1 per axis)
+ * is idx = range_start + loop_dir*n, and its partner in `target` is
+ * target_start[a] + target_loop_dir[a] * (loop_dir*n)[src_tar[a]].        */
+typedef struct ostc_interface {
+  int block, target;
+  int face, direction;
+  int range_start[3], range_end[3];
+  int target_start[3];
+  int loop_dir[3], target_loop_dir[3], src_tar[3];
+  int n_point[3];
+} ostc_interface;
+
 /* Options of the time-advance path (the relevant keys of 2_scheme.txt). */
 typedef struct ostc_config {
   int steady;                /* 0 unsteady (RK3), 1 steady                   */
@@ -186,6 +201,11 @@ ostc_status ostc_destroy(ostc_ctx *ctx);
 /* Which optional ostc_zone arrays the given param/config needs (bit mask in
  * the order of ostc_zone's pointer members starting at bit 0 = x).         */
 uint64_t ostc_zone_required(const ostc_config *cfg, const ostc_param *param);
+
+/* Attach the 1-to-1 interfaces between the context's blocks (replaces any
+ * previous set; resets the cached step graphs). Used by ostc_initialize,
+ * ostc_data_communication and every RK3 stage.                             */
+ostc_status ostc_set_interfaces(ostc_ctx *ctx, const ostc_interface *faces, int n_faces);
 
 /* Last error recorded on the context: status, CUDA error code, and the
  * first failing block/cell when the status is OSTC_ERR_NONPHYSICAL.        */
@@ -220,7 +240,9 @@ ostc_status ostc_update_cv_and_bv_rk(ostc_ctx *ctx, double dt, int rk, void *str
 ostc_status ostc_apply_boundary_conditions(ostc_ctx *ctx, int with_cv, void *stream);
 
 /* data_communication<mix,turb,with_cv> for same-device 1-to-1 interfaces
- * (src/DataCommunication.cuh:27-110). A no-op without interfaces.          */
+ * (src/DataCommunication.cuh:27-110): ghost layers take the partner block's
+ * values, the coincident plane takes the average of both blocks (quirk A10).
+ * A no-op without interfaces.                                              */
 ostc_status ostc_data_communication(ostc_ctx *ctx, int with_cv, void *stream);
 
 /* update_physical_properties<mix> over [-1, m] (src/FieldOperation.cuh:112-146). */

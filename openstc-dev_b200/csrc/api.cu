@@ -32,6 +32,8 @@ struct ostc_ctx {
   std::vector<double *> met_soa;
   std::vector<BcFace> faces;
   std::vector<int> face_zone;
+  std::vector<Iface> ifaces;
+  std::vector<int> iface_zone, iface_target;
   TileShape tile[3] = {{4, 4, 1}, {8, 2, 1}, {8, 2, 1}};
   unsigned long long *dt_bits = nullptr;  // device dt (as bits)
   double *res_partial = nullptr;          // [n_part_total][4]
@@ -508,10 +510,70 @@ ostc_status ostc_apply_boundary_conditions(ostc_ctx *ctx, int with_cv, void *str
 }
 
 ostc_status ostc_data_communication(ostc_ctx *ctx, int with_cv, void *stream) {
-  (void)with_cv;
-  (void)stream;
   if (!ctx) return OSTC_ERR_INVALID_ARG;
-  return OSTC_OK;  // no 1-to-1 interfaces in a context built from single blocks
+  if (ctx->ifaces.empty()) return OSTC_OK;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  // per block, per face, in order (DataCommunication.cuh:30-49)
+  for (size_t b = 0; b < ctx->dz.size(); ++b)
+    for (size_t q = 0; q < ctx->ifaces.size(); ++q) {
+      if (ctx->iface_zone[q] != (int)b) continue;
+      const DevZone &z = ctx->dz[b], &t = ctx->dz[ctx->iface_target[q]];
+      CK(dispatch_ns(ctx->ns, [&](auto n) {
+        return launch_interface<decltype(n)::value>(z, t, ctx->ifaces[q], with_cv, S(stream));
+      }));
+    }
+  return OSTC_OK;
+}
+
+ostc_status ostc_set_interfaces(ostc_ctx *ctx, const ostc_interface *f, int n) {
+  if (!ctx || n < 0 || (n > 0 && !f)) return OSTC_ERR_INVALID_ARG;
+  std::vector<Iface> v;
+  std::vector<int> zb, tb;
+  const int nz = (int)ctx->zones.size();
+  for (int q = 0; q < n; ++q) {
+    const ostc_interface &a = f[q];
+    if (a.block < 0 || a.block >= nz || a.target < 0 || a.target >= nz || a.face < 0 || a.face > 2 ||
+        (a.direction != 1 && a.direction != -1))
+      return OSTC_ERR_INVALID_ARG;
+    const ostc_zone &z = ctx->zones[a.block], &t = ctx->zones[a.target];
+    const int ez[3] = {z.mx, z.my, z.mz}, et[3] = {t.mx, t.my, t.mz};
+    Iface g{};
+    g.face = a.face;
+    g.direction = a.direction;
+    for (int d = 0; d < 3; ++d) {
+      if (a.n_point[d] < 1 || (a.loop_dir[d] != 1 && a.loop_dir[d] != -1) ||
+          (a.target_loop_dir[d] != 1 && a.target_loop_dir[d] != -1) || a.src_tar[d] < 0 || a.src_tar[d] > 2)
+        return OSTC_ERR_INVALID_ARG;
+      g.rs[d] = a.range_start[d];
+      g.ts[d] = a.target_start[d];
+      g.ld[d] = a.loop_dir[d];
+      g.tld[d] = a.target_loop_dir[d];
+      g.st[d] = a.src_tar[d];
+      g.np[d] = a.n_point[d];
+    }
+    // every point of the range and of its partner must lie inside the ghosted arrays
+    for (int d = 0; d < 3; ++d) {
+      const int lo = std::min(g.rs[d], g.rs[d] + g.ld[d] * (g.np[d] - 1));
+      const int hi = std::max(g.rs[d], g.rs[d] + g.ld[d] * (g.np[d] - 1));
+      if (lo < -z.ngg || hi > ez[d] - 1 + z.ngg) return OSTC_ERR_INVALID_ARG;
+      const int span = g.np[g.st[d]] - 1;
+      const int tlo = std::min(g.ts[d], g.ts[d] + g.tld[d] * g.ld[g.st[d]] * span);
+      const int thi = std::max(g.ts[d], g.ts[d] + g.tld[d] * g.ld[g.st[d]] * span);
+      if (tlo < -t.ngg || thi > et[d] - 1 + t.ngg) return OSTC_ERR_INVALID_ARG;
+    }
+    v.push_back(g);
+    zb.push_back(a.block);
+    tb.push_back(a.target);
+  }
+  ctx->ifaces.swap(v);
+  ctx->iface_zone.swap(zb);
+  ctx->iface_target.swap(tb);
+  for (auto &kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  ctx->graphs.clear();
+  return OSTC_OK;
 }
 
 ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream) {

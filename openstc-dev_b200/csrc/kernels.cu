@@ -732,6 +732,48 @@ __global__ void bc_subsonic_inflow_kernel(DevZone z, BcFace b, int with_cv) {
   }
 }
 
+// 1-to-1 interface (inner_communication, DataCommunication.cuh:58-110): ghosts
+// take the partner's values, the coincident plane the average of both blocks
+template <int NS>
+__global__ void interface_kernel(DevZone z, DevZone t, Iface f, int with_cv) {
+  const int n0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n1 = blockIdx.y * blockDim.y + threadIdx.y;
+  const int n2 = blockIdx.z;
+  if (n0 >= f.np[0] || n1 >= f.np[1] || n2 >= f.np[2]) return;
+  const int n[3] = {n0, n1, n2};
+  int idx[3], d[3], it[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    d[a] = f.ld[a] * n[a];
+    idx[a] = f.rs[a] + d[a];
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) it[a] = f.ts[a] + f.tld[a] * d[f.st[a]];
+  const int g = gidx(z, idx[0], idx[1], idx[2]);
+  const int gt = gidx(t, it[0], it[1], it[2]);
+  const int plane = f.direction > 0 ? f.rs[f.face] : f.rs[f.face] + f.ld[f.face] * (f.np[f.face] - 1);
+  if (idx[f.face] == plane) {
+    for (int l = 0; l < 6; ++l) {
+      const double ave = 0.5 * (t.bv[l * t.sz + gt] + z.bv[l * z.sz + g]);
+      z.bv[l * z.sz + g] = ave;
+      t.bv[l * t.sz + gt] = ave;
+    }
+    for (int l = 0; l < c_p.n_scalar; ++l) {
+      const double ave = 0.5 * (t.sv[l * t.sz + gt] + z.sv[l * z.sz + g]);
+      z.sv[l * z.sz + g] = ave;
+      t.sv[l * t.sz + gt] = ave;
+    }
+    const double u = z.bv[z.sz + g], v = z.bv[2 * z.sz + g], w = z.bv[3 * z.sz + g];
+    const double vel = sqrt(u * u + v * v + w * w);
+    z.vel[g] = vel;
+    t.vel[gt] = vel;
+  } else {
+    for (int l = 0; l < 6; ++l) z.bv[l * z.sz + g] = t.bv[l * t.sz + gt];
+    for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + g] = t.sv[l * t.sz + gt];
+  }
+  if (with_cv) cv_from_bv_point<NS>(z, g);
+}
+
 // ---------------------------------------------------------------------------
 // residual: store_last_step (TimeAdvanceFunc.cu:6-17), square of the change
 // and deterministic two-level sums (Residual.cuh:57-111, Residual.cu:49-89)
@@ -920,6 +962,15 @@ cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream
   return cudaGetLastError();
 }
 
+template <int NS>
+cudaError_t launch_interface(const DevZone &self, const DevZone &tar, const Iface &f, int with_cv, cudaStream_t s) {
+  // launch shape of data_communication (DataCommunication.cuh:36-45)
+  const dim3 blk(f.np[0] <= 2 * self.ngg + 1 ? 1 : 16, f.np[1] <= 2 * self.ngg + 1 ? 1 : 16);
+  const dim3 grid((f.np[0] + blk.x - 1) / blk.x, (f.np[1] + blk.y - 1) / blk.y, f.np[2]);
+  interface_kernel<NS><<<grid, blk, 0, s>>>(self, tar, f, with_cv);
+  return cudaGetLastError();
+}
+
 cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   return cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
 }
@@ -927,7 +978,8 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
 #define OSTC_INSTANTIATE(NS)                                                                                  \
   template cudaError_t launch_flux<NS>(const DevZone &, int, int, const TileShape &, int, int, cudaStream_t); \
   template cudaError_t launch_cells<NS>(CellOp, const DevZone &, const CellArgs &, cudaStream_t);            \
-  template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);
+  template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);                    \
+  template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t);
 
 OSTC_INSTANTIATE(0)
 OSTC_INSTANTIATE(9)

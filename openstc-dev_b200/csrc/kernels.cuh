@@ -27,6 +27,11 @@ struct BcFace {
   double total_pressure, total_temperature;
 };
 
+struct Iface {
+  int face, direction;
+  int rs[3], ts[3], ld[3], tld[3], st[3], np[3];
+};
+
 enum class CellOp { Source, UpdateRK, Properties, CvFromBv, Velocity, Dt, DtReset, StoreLast, ResidualPartial };
 
 struct CellArgs {
@@ -45,6 +50,8 @@ template <int NS>
 cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStream_t s);
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s);
+template <int NS>
+cudaError_t launch_interface(const DevZone &self, const DevZone &tar, const Iface &f, int with_cv, cudaStream_t s);
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
 cudaError_t upload_param(const DevParam &p, cudaStream_t s);
 

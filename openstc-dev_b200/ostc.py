@@ -83,6 +83,13 @@ class BcFaceC(C.Structure):
                 ("mw", C.c_double), ("total_pressure", C.c_double), ("total_temperature", C.c_double)]
 
 
+class IfaceC(C.Structure):
+    _fields_ = [("block", C.c_int), ("target", C.c_int), ("face", C.c_int), ("direction", C.c_int),
+                ("range_start", C.c_int * 3), ("range_end", C.c_int * 3), ("target_start", C.c_int * 3),
+                ("loop_dir", C.c_int * 3), ("target_loop_dir", C.c_int * 3), ("src_tar", C.c_int * 3),
+                ("n_point", C.c_int * 3)]
+
+
 class Config(C.Structure):
     _fields_ = [("steady", C.c_int), ("temporal_scheme", C.c_int), ("implicit_method", C.c_int),
                 ("DPLUR_inner_step", C.c_int), ("fixed_time_step", C.c_int), ("dt", C.c_double),
@@ -119,6 +126,7 @@ def lib():
             "ostc_set_tile": [vp, i, i, i],
             "ostc_get_tile": [vp, i, C.POINTER(i), C.POINTER(i)],
             "ostc_launch_op": [vp, i, i, vp],
+            "ostc_set_interfaces": [vp, C.POINTER(IfaceC), i],
             "ostc_step_kernel_count": [vp, i, C.POINTER(i)],
         }
         for name, args in sig.items():
@@ -422,7 +430,7 @@ def farfield_state(mach, T, p, direction=(1.0, 0.0, 0.0), mech: Optional[Mechani
 # ---------------------------------------------------------------------------
 class Solver:
     def __init__(self, scheme: Scheme, mech: Optional[Mechanism], blocks: List[DeviceBlock], faces: List[BcFaceC],
-                 output_screen: int = 1):
+                 output_screen: int = 1, interfaces: Optional[List["IfaceC"]] = None):
         import torch
 
         self.scheme = scheme
@@ -438,6 +446,10 @@ class Solver:
                                 C.byref(ctx)), "ostc_create")
         self.ctx = ctx
         self.stream = torch.cuda.current_stream().cuda_stream
+        if interfaces:
+            ia = (IfaceC * len(interfaces))(*interfaces)
+            self._ifaces = ia
+            check(lib().ostc_set_interfaces(self.ctx, ia, len(interfaces)), "ostc_set_interfaces")
 
     def close(self):
         if self.ctx:
@@ -587,6 +599,12 @@ class Case:
     blocks: List[HostBlock]
     faces: List[BcFaceC]
     steps: int
+    interfaces: List["IfaceC"] = field(default_factory=list)
+
+    def solver(self, **kw):
+        """A Solver on fresh device copies of the blocks."""
+        blocks = [DeviceBlock(b) for b in self.blocks]
+        return Solver(self.scheme, self.mech, blocks, self.faces, interfaces=self.interfaces, **kw), blocks
 
     @property
     def cells(self):
@@ -684,6 +702,92 @@ def case_bc_box(kind="wall_farfield", mx=40, my=32, mz=10, dx=1e-3) -> Case:
     faces += [bc_face(0, BC_SYMMETRY, 2, -1, ext, ng), bc_face(0, BC_SYMMETRY, 2, 1, ext, ng)]
     c.faces = faces
     c.name = "bc_box_%s_%dx%dx%d" % (kind, mx, my, mz)
+    return c
+
+
+def iface_aligned(block, target, face, direction, ext_self, ext_tar, ngg) -> IfaceC:
+    """The registered cfd::InnerFace (src/Mesh.cpp:34-178) of two blocks whose
+    axes are aligned and whose coincident planes are `face`-max of one and
+    `face`-min of the other; tangential ranges cover the interior only."""
+    f = IfaceC()
+    f.block, f.target, f.face, f.direction = block, target, face, direction
+    for d in range(3):
+        f.loop_dir[d] = 1
+        f.target_loop_dir[d] = 1
+        f.src_tar[d] = d
+        if d == face:
+            if direction > 0:
+                f.range_start[d], f.range_end[d] = ext_self[d] - 1, ext_self[d] - 1 + ngg
+                f.target_start[d] = 0
+            else:
+                f.range_start[d], f.range_end[d] = -ngg, 0
+                f.target_start[d] = ext_tar[d] - 1 - ngg
+            f.n_point[d] = ngg + 1
+        else:
+            f.range_start[d], f.range_end[d] = 0, ext_self[d] - 1
+            f.target_start[d] = 0
+            f.n_point[d] = ext_self[d]
+    return f
+
+
+def case_multiblock(nx=(20, 17, 13), ny=(15, 19), mz=8, dx=1e-3, reconstruction=4, inviscid_scheme=2) -> Case:
+    """The air vortex of case_vortex on a grid split into len(nx) x len(ny)
+    blocks of uneven sizes that share their face planes (1-to-1 interfaces,
+    averaged on the shared plane, quirk A10); inflow / outflow in i,
+    symmetry in j and k, so the reference build can run it."""
+    s = Scheme(mix_model=MIX_AIR, inviscid_scheme=inviscid_scheme, reconstruction=reconstruction, viscous_order=2,
+               cfl=0.5)
+    ng = s.ngg
+    NX = sum(nx) - (len(nx) - 1)
+    NY = sum(ny) - (len(ny) - 1)
+    xg, yg, zg = grid_coordinates(NX, NY, mz, ng + 1, dx, periodic_k=True)
+    inf = air_state(2.0, 300.0, 101325.0)
+    xs, ys = xg[1:-1, 1:-1, 1:-1], yg[1:-1, 1:-1, 1:-1]
+    xc, yc = (NX // 2) * dx, (NY // 2) * dx
+    R, beta, U = 5 * dx, 0.3, inf["u"]
+    r2 = ((xs - xc) ** 2 + (ys - yc) ** 2) / R ** 2
+    ex = np.exp(0.5 * (1 - r2))
+    Rg = R_U / MW_AIR
+    T = 300.0 - (GAMMA_AIR - 1) / (2 * GAMMA_AIR) * (beta * U) ** 2 / Rg * ex ** 2
+    rho = inf["density"] * (T / 300.0) ** (1 / (GAMMA_AIR - 1))
+    gbv = np.stack([rho, U - beta * U * (ys - yc) / R * ex, beta * U * (xs - xc) / R * ex, 0 * rho, rho * Rg * T, T])
+    blocks, faces, ifaces, ids = [], [], [], {}
+    ox = np.cumsum([0] + [n - 1 for n in nx])
+    oy = np.cumsum([0] + [n - 1 for n in ny])
+    for bj, my in enumerate(ny):
+        for bi, mx in enumerate(nx):
+            b = HostBlock.allocate(mx, my, mz, ng, 5, 0)
+            i0, j0 = ox[bi], oy[bj]
+            sl = (slice(None), slice(j0, j0 + my + 2 * ng + 2), slice(i0, i0 + mx + 2 * ng + 2))
+            fill_metric(b, np.ascontiguousarray(xg[sl]), np.ascontiguousarray(yg[sl]), np.ascontiguousarray(zg[sl]))
+            b.arrays["bv"][...] = gbv[:, :, j0:j0 + my + 2 * ng, i0:i0 + mx + 2 * ng]
+            ids[(bi, bj)] = len(blocks)
+            blocks.append(b)
+    for (bi, bj), q in ids.items():
+        ext = (nx[bi], ny[bj], mz)
+        if bi == 0:
+            faces.append(bc_face(q, BC_INFLOW, 0, -1, ext, ng, inf))
+        else:
+            t = ids[(bi - 1, bj)]
+            ifaces.append(iface_aligned(q, t, 0, -1, ext, (nx[bi - 1], ny[bj], mz), ng))
+        if bi == len(nx) - 1:
+            faces.append(bc_face(q, BC_OUTFLOW, 0, 1, ext, ng))
+        else:
+            t = ids[(bi + 1, bj)]
+            ifaces.append(iface_aligned(q, t, 0, 1, ext, (nx[bi + 1], ny[bj], mz), ng))
+        if bj == 0:
+            faces.append(bc_face(q, BC_SYMMETRY, 1, -1, ext, ng))
+        else:
+            t = ids[(bi, bj - 1)]
+            ifaces.append(iface_aligned(q, t, 1, -1, ext, (nx[bi], ny[bj - 1], mz), ng))
+        if bj == len(ny) - 1:
+            faces.append(bc_face(q, BC_SYMMETRY, 1, 1, ext, ng))
+        else:
+            t = ids[(bi, bj + 1)]
+            ifaces.append(iface_aligned(q, t, 1, 1, ext, (nx[bi], ny[bj + 1], mz), ng))
+        faces += [bc_face(q, BC_SYMMETRY, 2, -1, ext, ng), bc_face(q, BC_SYMMETRY, 2, 1, ext, ng)]
+    c = Case("multiblock_air_%dx%d_blocks" % (len(nx), len(ny)), s, None, blocks, faces, 100)
+    c.interfaces = ifaces
     return c
 
 

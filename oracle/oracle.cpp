@@ -1517,6 +1517,45 @@ void bc_periodic(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv)
         }
 }
 
+std::vector<ostc_interface> g_ifaces;
+
+// inner_communication (DataCommunication.cuh:58-110) for one interface
+void interface_exchange(const ostc_param *P, Z &Zs, Z &Zt, const ostc_interface &f, int with_cv) {
+  const int plane = f.direction > 0 ? f.range_start[f.face] : f.range_end[f.face];
+  for (int n2 = 0; n2 < f.n_point[2]; ++n2)
+    for (int n1 = 0; n1 < f.n_point[1]; ++n1)
+      for (int n0 = 0; n0 < f.n_point[0]; ++n0) {
+        const int n[3] = {n0, n1, n2};
+        int idx[3], d[3], it[3];
+        for (int a = 0; a < 3; ++a) {
+          d[a] = f.loop_dir[a] * n[a];
+          idx[a] = f.range_start[a] + d[a];
+        }
+        for (int a = 0; a < 3; ++a) it[a] = f.target_start[a] + f.target_loop_dir[a] * d[f.src_tar[a]];
+        if (idx[f.face] == plane) {
+          for (int l = 0; l < 6; ++l) {
+            const double ave = 0.5 * (Zt.bv(it[0], it[1], it[2], l) + Zs.bv(idx[0], idx[1], idx[2], l));
+            Zs.bv(idx[0], idx[1], idx[2], l) = ave;
+            Zt.bv(it[0], it[1], it[2], l) = ave;
+          }
+          for (int l = 0; l < P->n_scalar; ++l) {
+            const double ave = 0.5 * (Zt.sv(it[0], it[1], it[2], l) + Zs.sv(idx[0], idx[1], idx[2], l));
+            Zs.sv(idx[0], idx[1], idx[2], l) = ave;
+            Zt.sv(it[0], it[1], it[2], l) = ave;
+          }
+          const double u = Zs.bv(idx[0], idx[1], idx[2], 1), v = Zs.bv(idx[0], idx[1], idx[2], 2),
+                       w = Zs.bv(idx[0], idx[1], idx[2], 3);
+          const double vel = std::sqrt(u * u + v * v + w * w);
+          Zs.vel(idx[0], idx[1], idx[2]) = vel;
+          Zt.vel(it[0], it[1], it[2]) = vel;
+        } else {
+          for (int l = 0; l < 6; ++l) Zs.bv(idx[0], idx[1], idx[2], l) = Zt.bv(it[0], it[1], it[2], l);
+          for (int l = 0; l < P->n_scalar; ++l) Zs.sv(idx[0], idx[1], idx[2], l) = Zt.sv(it[0], it[1], it[2], l);
+        }
+        if (with_cv) cv_from_bv_point(P, Zs, idx[0], idx[1], idx[2]);
+      }
+}
+
 void compute_rhs_zone(const ostc_param *P, Z &Zn) {
   const long nint = (long)Zn.mx * Zn.my * Zn.mz;
   const int nv = P->n_var;
@@ -1693,6 +1732,22 @@ int oracle_apply_boundary_conditions(const ostc_param *P, ostc_zone *zones, int 
   return 0;
 }
 
+int oracle_set_interfaces(const ostc_interface *f, int n) {
+  g_ifaces.assign(f, f + (n > 0 ? n : 0));
+  return 0;
+}
+
+int oracle_data_communication(const ostc_param *P, ostc_zone *zones, int n_zones, int with_cv) {
+  for (int b = 0; b < n_zones; ++b)
+    for (const auto &f : g_ifaces) {
+      if (f.block != b) continue;
+      if (f.target < 0 || f.target >= n_zones) return OSTC_ERR_INVALID_ARG;
+      Z Zs(&zones[b]), Zt(&zones[f.target]);
+      interface_exchange(P, Zs, Zt, f, with_cv);
+    }
+  return 0;
+}
+
 int oracle_update_physical_properties(const ostc_param *P, ostc_zone *z) {
   Z Zn(z);
 #pragma omp parallel for collapse(2) schedule(static)
@@ -1718,6 +1773,7 @@ int oracle_initialize(const ostc_config *c, const ostc_param *P, ostc_zone *zone
           Zn.vel(i, j, k) = std::sqrt(Zn.bv(i, j, k, 1) * Zn.bv(i, j, k, 1) + Zn.bv(i, j, k, 2) * Zn.bv(i, j, k, 2) +
                                       Zn.bv(i, j, k, 3) * Zn.bv(i, j, k, 3));
   }
+  oracle_data_communication(P, zones, n_zones, 0);
   for (int b = 0; b < n_zones; ++b) oracle_update_physical_properties(P, &zones[b]);
   for (int b = 0; b < n_zones; ++b) oracle_compute_cv_from_bv(P, &zones[b]);
   return 0;
@@ -1755,6 +1811,7 @@ int oracle_rk3_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zones
       for (int b = 0; b < n_zones; ++b) oracle_update_cv_and_bv_rk(P, &zones[b], dt, rk);
       int st = oracle_apply_boundary_conditions(P, zones, n_zones, f, n_faces, 1);
       if (st) return st;
+      oracle_data_communication(P, zones, n_zones, 1);
       for (int b = 0; b < n_zones; ++b) oracle_update_physical_properties(P, &zones[b]);
     }
     if (dt_hist) dt_hist[step] = dt;

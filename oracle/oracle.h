@@ -44,6 +44,10 @@ int oracle_initialize(const ostc_config *c, const ostc_param *p, ostc_zone *zone
 int oracle_rk3_steps(const ostc_config *c, const ostc_param *p, ostc_zone *zones, int n_zones,
                      const ostc_bc_face *f, int n_faces, int n_steps,
                      double *res_hist, double *dt_hist);
+/* 1-to-1 interfaces used by oracle_initialize / oracle_rk3_steps (copied) */
+int oracle_set_interfaces(const ostc_interface *f, int n);
+/* data_communication over the registered interfaces (DataCommunication.cuh:27-110) */
+int oracle_data_communication(const ostc_param *p, ostc_zone *zones, int n_zones, int with_cv);
 /* chemistry source of one state (omega[n_spec], kg/m3/s), for known-answer tests */
 int oracle_chemical_source(const ostc_param *p, double rho, double T, const double *Y,
                            double *omega);

@@ -39,7 +39,7 @@ using namespace cfd;
 
 namespace {
 
-struct RefCtx {
+struct RefCtx {  // one block
   ostc_config cfg{};
   int mix = 0, n_var = 5, n_scalar = 0, n_spec = 0, ngg = 2, mx = 0, my = 0, mz = 0;
   Parameter *parameter = nullptr;
@@ -53,6 +53,12 @@ struct RefCtx {
   std::vector<Inflow *> d_inflows;
   std::vector<double *> d_inflow_sv;
   std::vector<void *> d_cond;  // per face: device Wall / FarField / SubsonicInflow / BackPressure
+  std::vector<InnerFace> inner;  // host copies of this block's 1-to-1 faces
+  std::vector<int> inner_target;
+};
+
+struct RefMulti {  // all blocks of a run
+  std::vector<RefCtx *> blk;
 };
 
 template <typename T>
@@ -176,6 +182,8 @@ void build_zone(RefCtx &c, const ostc_zone *z, const ostc_param *p) {
   if (p->inviscid_scheme == 2) h.entropy_fix_delta.allocate_memory(mx, my, mz, 1);  // Field.cu:223-226
   h.boundary = nullptr;
   if (!c.faces.empty()) h.boundary = dcopy(c.faces.data(), c.faces.size());
+  h.innerface = nullptr;
+  if (!c.inner.empty()) h.innerface = dcopy(c.inner.data(), c.inner.size());
   cudaMalloc(&c.d_zone, sizeof(DZone));
   cudaMemcpy(c.d_zone, &h, sizeof(DZone), cudaMemcpyHostToDevice);
 }

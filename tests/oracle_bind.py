@@ -35,6 +35,7 @@ def oracle():
             "oracle_enthalpy_cp": ([P, C.c_double, d, d], C.c_int),
             "oracle_transport": ([P, C.c_double, C.c_double, C.c_double, d, d, d, d], C.c_int),
             "oracle_set_threads": ([C.c_int], None),
+            "oracle_set_interfaces": ([C.POINTER(ostc.IfaceC), C.c_int], C.c_int),
             "oracle_get_threads": ([], C.c_int),
         }
         for n, (a, r) in sig.items():
@@ -64,7 +65,13 @@ class OracleRun:
         if st != 0:
             raise RuntimeError("%s -> %d" % (what, st))
 
+    def _ifaces(self):
+        ifs = list(getattr(self.case, "interfaces", []) or [])
+        arr = (ostc.IfaceC * max(len(ifs), 1))(*ifs)
+        oracle().oracle_set_interfaces(arr, len(ifs))
+
     def initialize(self):
+        self._ifaces()
         self._ck(oracle().oracle_initialize(C.byref(self.config), C.byref(self.param), self.zones, len(self.blocks),
                                             self.faces, self.nf), "oracle_initialize")
 
@@ -82,6 +89,7 @@ class OracleRun:
         return oracle().oracle_global_time_step(C.byref(self.param), self.zones, len(self.blocks))
 
     def rk3_steps(self, n):
+        self._ifaces()
         res = (C.c_double * (4 * n))()
         dts = (C.c_double * n)()
         self._ck(oracle().oracle_rk3_steps(C.byref(self.config), C.byref(self.param), self.zones, len(self.blocks),
