@@ -3,7 +3,7 @@
  * the OpenSTC-dev structured-grid compressible reacting-flow solver.
  *
  * The ABI keeps the reference's device data model so that the path is a
- * drop-in for the per-stage calls made by RK3_bv (src/RK.cuh:301-355):
+ * drop-in for the per-stage calls made by RK3_bv (src/RK.cuh:107-161):
  *
  *   - every field array is a ColMajor ggxl::VectorField3D / Array3D
  *     (src/gxl_lib/Array.hpp:128-194): one plane per variable, i fastest,
@@ -178,7 +178,7 @@ typedef struct ostc_config {
   int DPLUR_inner_step;
   int fixed_time_step;       /* 1: dt given; 0: CFL dt each stage (quirk A12) */
   double dt;
-  int output_screen;         /* residual cadence, RK.cuh:289                 */
+  int output_screen;         /* residual cadence, RK.cuh:94                 */
   int compat;                /* 1: replicate reference quirks (Appendix A)   */
 } ostc_config;
 
@@ -220,7 +220,7 @@ ostc_status ostc_get_error(const ostc_ctx *ctx, int *cuda_error, int *block,
 ostc_status ostc_compute_cv_from_bv(ostc_ctx *ctx, void *stream);
 
 /* cudaMemset(dq) + compute_source + compute_inviscid_flux +
- * compute_viscous_flux (src/RK.cuh:303-311): the right-hand side of every
+ * compute_viscous_flux (src/RK.cuh:110-116): the right-hand side of every
  * block into dq, in fused sm_100a kernels.                                 */
 ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream);
 
@@ -231,7 +231,7 @@ ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream);
 ostc_status ostc_global_time_step(ostc_ctx *ctx, double *dt_host, void *stream);
 const double *ostc_dt_device(const ostc_ctx *ctx);
 
-/* update_cv_and_bv_rk (src/RK.cuh:392-448) for SSPRK3 stage rk in {0,1,2}.
+/* update_cv_and_bv_rk (src/RK.cuh:197-253) for SSPRK3 stage rk in {0,1,2}.
  * dt < 0 reads the device dt written by ostc_global_time_step.            */
 ostc_status ostc_update_cv_and_bv_rk(ostc_ctx *ctx, double dt, int rk, void *stream);
 
@@ -253,7 +253,7 @@ ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream);
 /* ----------------------------------------------------------------------- */
 
 /* Driver::initialize_computation (src/Driver.cu:39-98) followed by the
- * pre-loop of RK3_bv (src/RK.cuh:235-244). Also re-reads the metric records
+ * pre-loop of RK3_bv (src/RK.cuh:40-49). Also re-reads the metric records
  * (so they may be written after ostc_create).                             */
 ostc_status ostc_initialize(ostc_ctx *ctx, void *stream);
 
@@ -261,7 +261,7 @@ ostc_status ostc_initialize(ostc_ctx *ctx, void *stream);
 ostc_status ostc_rk3_stage(ostc_ctx *ctx, int rk, void *stream);
 
 /* n_steps full RK3 steps (the body of the while loop in RK3_bv,
- * src/RK.cuh:284-357), captured once as a CUDA graph and replayed.
+ * src/RK.cuh:89-170), captured once as a CUDA graph and replayed.
  * If res_hist is non-NULL it receives 4 doubles per step (the RMS change of
  * rho, |V|, p, T, src/Residual.cuh:57-161, unnormalised) and dt_hist one dt
  * per step; both synchronise the stream at the end.                        */
@@ -289,7 +289,7 @@ ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks);
  * OSTC_OP_FLUX (arg = direction, accumulates into dq), OSTC_OP_SOURCE,
  * OSTC_OP_PROPERTIES, OSTC_OP_UPDATE (arg = rk stage), OSTC_OP_DT,
  * OSTC_OP_BC (arg = with_cv). No reference counterpart: the reference
- * launches these only from its stage loop (src/RK.cuh:301-355).            */
+ * launches these only from its stage loop (src/RK.cuh:107-161).            */
 enum { OSTC_OP_FLUX = 0, OSTC_OP_SOURCE = 1, OSTC_OP_PROPERTIES = 2, OSTC_OP_UPDATE = 3, OSTC_OP_DT = 4,
        OSTC_OP_BC = 5 };
 ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream);

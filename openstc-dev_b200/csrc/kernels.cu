@@ -3,7 +3,7 @@
 //  flux_dir<NS,INV,DIR>   fused inviscid + viscous flux difference along one
 //                         direction (InviscidScheme.cu, AWENO.cu, ViscousScheme.cuh)
 //  source_kernel<NS>      finite-rate chemistry source, starts dq (SourceTerm.cuh:11-37)
-//  update_rk_kernel<NS>   SSPRK3 stage update, cv -> bv/sv, T and p (RK.cuh:392-448)
+//  update_rk_kernel<NS>   SSPRK3 stage update, cv -> bv/sv, T and p (RK.cuh:197-253)
 //  properties_kernel<NS>  cp, gamma, a, mu, kappa, rho*D, Mach over [-1, m] (FieldOperation.cuh:112-146)
 //  cv_from_bv_kernel<NS>  conservative from primitive, ghosts included (FieldOperation.cuh:43-79)
 //  dt_kernel<NS>          local time step + block min + atomic min (TimeAdvanceFunc.cuh:50-100, .cu:155-201)

@@ -2,7 +2,7 @@
 in include/ostc.h, block storage in the reference's DZone layout, and the
 synthetic workloads.
 
-The binding mirrors the reference's operator API (src/RK.cuh:301-355):
+The binding mirrors the reference's operator API (src/RK.cuh:107-161):
 ``Solver.compute_rhs`` is compute_source + compute_inviscid_flux +
 compute_viscous_flux, ``Solver.rk3_stage`` one SSPRK3 stage, and so on. All
 arithmetic runs in libostc.so (sm_100a); torch only owns device memory.

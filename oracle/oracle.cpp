@@ -1559,7 +1559,7 @@ void interface_exchange(const ostc_param *P, Z &Zs, Z &Zt, const ostc_interface 
 void compute_rhs_zone(const ostc_param *P, Z &Zn) {
   const long nint = (long)Zn.mx * Zn.my * Zn.mz;
   const int nv = P->n_var;
-  // cudaMemset(dq, 0) (RK.cuh:305): dq carries dq_ngg ghosts
+  // cudaMemset(dq, 0) (RK.cuh:110): dq carries dq_ngg ghosts
   const View &dq = Zn.dq;
   std::fill(dq.p, dq.p + dq.sz * nv, 0.0);
   (void)nint;
@@ -1676,7 +1676,7 @@ double oracle_global_time_step(const ostc_param *P, ostc_zone *zones, int n_zone
 
 int oracle_update_cv_and_bv_rk(const ostc_param *P, ostc_zone *z, double dt, int rk) {
   static const double A[3] = {1.0, 0.75, 1.0 / 3.0}, B[3] = {0.0, 0.25, 2.0 / 3.0},
-                      C[3] = {1.0, 0.25, 2.0 / 3.0};  // RK.cuh:205-209
+                      C[3] = {1.0, 0.25, 2.0 / 3.0};  // RK.cuh:11-13
   Z Zn(z);
 #pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < Zn.mz; ++k)
@@ -1761,7 +1761,7 @@ int oracle_initialize(const ostc_config *c, const ostc_param *P, ostc_zone *zone
                       const ostc_bc_face *f, int n_faces) {
   (void)c;
   // Driver::initialize_computation (Driver.cu:39-98): BCs without cv, velocity
-  // everywhere, interfaces, properties; then RK3_bv pre-loop (RK.cuh:235-244).
+  // everywhere, interfaces, properties; then RK3_bv pre-loop (RK.cuh:40-49).
   int st = oracle_apply_boundary_conditions(P, zones, n_zones, f, n_faces, 0);
   if (st) return st;
   for (int b = 0; b < n_zones; ++b) {
@@ -1798,7 +1798,7 @@ int oracle_rk3_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zones
             last[b][q + 2 * n] = Zn.bv(i, j, k, 4);
             last[b][q + 3 * n] = Zn.bv(i, j, k, 5);
           }
-      // qn <- cv over the whole ghosted array (RK.cuh:296-299)
+      // qn <- cv over the whole ghosted array (RK.cuh:101-104)
       std::memcpy(Zn.qn.p, Zn.cv.p, sizeof(double) * Zn.cv.sz * P->n_var);
     }
     double dt = c->dt;

@@ -23,14 +23,14 @@ extern "C" {
 
 /* compute_cv_from_bv over [-ngg, m+ngg) (src/FieldOperation.cuh:43-79) */
 int oracle_compute_cv_from_bv(const ostc_param *p, ostc_zone *z);
-/* memset(dq) + compute_source + inviscid + viscous (src/RK.cuh:303-311) */
+/* memset(dq) + compute_source + inviscid + viscous (src/RK.cuh:110-116) */
 int oracle_compute_rhs(const ostc_param *p, ostc_zone *z);
 /* same as oracle_compute_rhs, and scale[l] = max |face flux| of variable l:
  * the magnitude whose differences form dq_l (its conditioning scale) */
 int oracle_flux_scale(const ostc_param *p, ostc_zone *z, double *scale);
 /* local_time_step on every zone, then the global minimum (capped at 1e6) */
 double oracle_global_time_step(const ostc_param *p, ostc_zone *zones, int n_zones);
-/* update_cv_and_bv_rk (src/RK.cuh:392-448) */
+/* update_cv_and_bv_rk (src/RK.cuh:197-253) */
 int oracle_update_cv_and_bv_rk(const ostc_param *p, ostc_zone *z, double dt, int rk);
 /* BCs in the reference priority order, then periodic faces */
 int oracle_apply_boundary_conditions(const ostc_param *p, ostc_zone *zones, int n_zones,

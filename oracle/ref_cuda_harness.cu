@@ -6,13 +6,15 @@
 // It rebuilds what Driver<mix,turb> sets up (src/Driver.cu:10-35,
 // src/Field.cu:133-251, src/DParameter.cu:7-159) from ostc_param /
 // ostc_zone host data, and repeats the per-step sequence of RK3_bv
-// (src/RK.cuh:284-357) calling the reference's launchers and kernels:
+// (src/RK.cuh:89-170) calling the reference's launchers and kernels:
 // compute_source, compute_inviscid_flux, compute_viscous_flux,
 // local_time_step + min_of_arr, update_cv_and_bv_rk, the apply_* boundary
 // kernels in the priority order of DBoundCond::apply_boundary_conditions
 // (src/BoundCond.cuh:673-822) with its launch shapes, and
 // update_physical_properties. Everything runs on the legacy default stream
 // with the reference's implicit synchronisations (the per-stage dt D2H copy).
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -27,6 +29,7 @@
 #include "Parameter.h"
 #include "BoundCond.cuh"
 #include "FieldOperation.cuh"
+#include "DataCommunication.cuh"
 #include "TimeAdvanceFunc.cuh"
 #include "IOManager.h"
 #include "RK.cuh"
@@ -58,6 +61,8 @@ struct RefCtx {  // one block
 };
 
 struct RefMulti {  // all blocks of a run
+  ostc_config cfg{};
+  int mix = 0;
   std::vector<RefCtx *> blk;
 };
 
@@ -231,19 +236,55 @@ void apply_bcs(RefCtx &c) {
   }
 }
 
+// data_communication (DataCommunication.cuh:27-56), inner faces only: one
+// inner_communication launch per face of every block, in block order
+template <MixtureModel mix, bool with_cv>
+void communicate(RefMulti &m) {
+  for (RefCtx *c : m.blk) {
+    for (size_t l = 0; l < c->inner.size(); ++l) {
+      const InnerFace &fc = c->inner[l];
+      uint tpb[3], bpg[3];
+      for (int j = 0; j < 3; ++j) {
+        tpb[j] = fc.n_point[j] <= (2 * c->ngg + 1) ? 1 : 16;
+        bpg[j] = (fc.n_point[j] - 1) / tpb[j] + 1;
+      }
+      dim3 TPB{tpb[0], tpb[1], tpb[2]}, BPG{bpg[0], bpg[1], bpg[2]};
+      RefCtx *t = m.blk[c->inner_target[l]];
+      inner_communication<mix, Laminar, with_cv><<<BPG, TPB>>>(c->d_zone, t->d_zone, (integer)l, c->d_param);
+    }
+  }
+}
+
 template <MixtureModel mix>
-void initialize(RefCtx &c) {
-  // Driver::initialize_computation (Driver.cu:39-98) + RK3_bv pre-loop (RK.cuh:235-244)
+void initialize(RefMulti &m) {
+  // Driver::initialize_computation (Driver.cu:39-98) + RK3_bv pre-loop (RK.cuh:40-49)
   dim3 tpb{8, 8, 4};
-  const int ng_1 = 2 * c.ngg - 1;
-  apply_bcs<mix, false>(c);
-  dim3 bpg{(unsigned)((c.mx + ng_1) / tpb.x + 1), (unsigned)((c.my + ng_1) / tpb.y + 1),
-           (unsigned)((c.mz + ng_1) / tpb.z + 1)};
-  compute_velocity<<<bpg, tpb>>>(c.d_zone);
-  update_physical_properties<mix><<<bpg, tpb>>>(c.d_zone, c.d_param);
-  dim3 bpg0{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
-  store_last_step<<<bpg0, tpb>>>(c.d_zone);
-  compute_cv_from_bv<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param);
+  for (RefCtx *c : m.blk) apply_bcs<mix, false>(*c);
+  for (RefCtx *c : m.blk) {
+    const int ng_1 = 2 * c->ngg - 1;
+    dim3 bpg{(unsigned)((c->mx + ng_1) / tpb.x + 1), (unsigned)((c->my + ng_1) / tpb.y + 1),
+             (unsigned)((c->mz + ng_1) / tpb.z + 1)};
+    compute_velocity<<<bpg, tpb>>>(c->d_zone);
+  }
+  cudaDeviceSynchronize();
+  communicate<mix, false>(m);
+  cudaDeviceSynchronize();
+  for (RefCtx *c : m.blk) {
+    const int ng_1 = 2 * c->ngg - 1;
+    dim3 bpg{(unsigned)((c->mx + ng_1) / tpb.x + 1), (unsigned)((c->my + ng_1) / tpb.y + 1),
+             (unsigned)((c->mz + ng_1) / tpb.z + 1)};
+    update_physical_properties<mix><<<bpg, tpb>>>(c->d_zone, c->d_param);
+  }
+  cudaDeviceSynchronize();
+  for (RefCtx *c : m.blk) {
+    const int ng_1 = 2 * c->ngg - 1;
+    dim3 bpg{(unsigned)((c->mx + ng_1) / tpb.x + 1), (unsigned)((c->my + ng_1) / tpb.y + 1),
+             (unsigned)((c->mz + ng_1) / tpb.z + 1)};
+    dim3 bpg0{(unsigned)((c->mx - 1) / tpb.x + 1), (unsigned)((c->my - 1) / tpb.y + 1),
+              (unsigned)((c->mz - 1) / tpb.z + 1)};
+    store_last_step<<<bpg0, tpb>>>(c->d_zone);
+    compute_cv_from_bv<mix, Laminar><<<bpg, tpb>>>(c->d_zone, c->d_param);
+  }
   cudaDeviceSynchronize();
 }
 
@@ -257,7 +298,7 @@ void rhs(RefCtx &c) {
   compute_viscous_flux<mix, Laminar>(*c.block, c.d_zone, c.d_param, c.n_var);
 }
 
-double global_dt(RefCtx &c) {  // global_time_step (TimeAdvanceFunc.cu:155-182) for one block
+double block_dt(RefCtx &c) {  // one block of global_time_step (TimeAdvanceFunc.cu:155-182)
   constexpr integer TPB{128};
   int num_sms, per_sm;
   cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, 0);
@@ -268,11 +309,11 @@ double global_dt(RefCtx &c) {  // global_time_step (TimeAdvanceFunc.cu:155-182) 
   min_of_arr<<<1, TPB>>>(c.h.dt_local.data(), n_blocks);
   double dt_block;
   cudaMemcpy(&dt_block, c.h.dt_local.data(), sizeof(real), cudaMemcpyDeviceToHost);
-  return std::min(1e+6, dt_block);
+  return dt_block;
 }
 
-template <MixtureModel mix>
-void residual(RefCtx &c, double *res) {  // compute_residual (Residual.cuh:57-111) before normalisation
+// one block of compute_residual (Residual.cuh:57-111): the summed squares
+void block_residual(RefCtx &c, double *r) {
   dim3 tpb{8, 8, 4};
   dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
   compute_square_of_dbv<<<bpg, tpb>>>(c.d_zone);
@@ -284,47 +325,58 @@ void residual(RefCtx &c, double *res) {  // compute_residual (Residual.cuh:57-11
   const int n_blocks = std::min(per_sm * num_sms, (size + TPB - 1) / TPB);
   reduction_of_dv_squared<<<n_blocks, TPB>>>(c.h.bv_last.data(), size);
   reduction_of_dv_squared<<<1, TPB>>>(c.h.bv_last.data(), n_blocks);
-  double r[4];
   cudaMemcpy(r, c.h.bv_last.data(), 4 * sizeof(real), cudaMemcpyDeviceToHost);
-  for (int l = 0; l < 4; ++l) res[l] = std::sqrt(r[l] / (double)size);
 }
 
 template <MixtureModel mix>
-int steps(RefCtx &c, int n, double *res_hist, double *dt_hist) {
-  // the body of RK3_bv's while loop (RK.cuh:284-357)
+int steps(RefMulti &m, int n, double *res_hist, double *dt_hist) {
+  // the body of RK3_bv's while loop (RK.cuh:89-170), all blocks
   dim3 tpb{8, 8, 4};
-  dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
-  dim3 bpgp{(unsigned)((c.mx + 1) / tpb.x + 1), (unsigned)((c.my + 1) / tpb.y + 1), (unsigned)((c.mz + 1) / tpb.z + 1)};
-  double dt = c.cfg.fixed_time_step ? c.cfg.dt : 1e+6;
+  auto bpg = [&](RefCtx *c, int e) {
+    return dim3{(unsigned)((c->mx + e) / tpb.x + 1), (unsigned)((c->my + e) / tpb.y + 1),
+                (unsigned)((c->mz + e) / tpb.z + 1)};
+  };
+  double n_total = 0;
+  for (RefCtx *c : m.blk) n_total += (double)c->mx * c->my * c->mz;
+  double dt = m.cfg.fixed_time_step ? m.cfg.dt : 1e+6;
   for (int s = 0; s < n; ++s) {
-    if (res_hist) store_last_step<<<bpg, tpb>>>(c.d_zone);
-    cudaMemcpy(c.h.qn.data(), c.h.cv.data(), c.h.cv.size() * sizeof(real) * c.n_var, cudaMemcpyDeviceToDevice);
+    if (res_hist)
+      for (RefCtx *c : m.blk) store_last_step<<<bpg(c, -1), tpb>>>(c->d_zone);
+    for (RefCtx *c : m.blk)
+      cudaMemcpy(c->h.qn.data(), c->h.cv.data(), c->h.cv.size() * sizeof(real) * c->n_var, cudaMemcpyDeviceToDevice);
     for (integer rk = 0; rk < 3; ++rk) {
-      rhs<mix>(c);
-      if (!c.cfg.fixed_time_step) {
-        local_time_step<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param);
-        dt = global_dt(c);
+      for (RefCtx *c : m.blk) rhs<mix>(*c);
+      if (!m.cfg.fixed_time_step) {
+        for (RefCtx *c : m.blk) local_time_step<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
+        dt = 1e+6;
+        for (RefCtx *c : m.blk) dt = std::min(dt, block_dt(*c));
       }
-      update_cv_and_bv_rk<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param, dt, rk);
-      apply_bcs<mix, true>(c);
-      update_physical_properties<mix><<<bpgp, tpb>>>(c.d_zone, c.d_param);
+      for (RefCtx *c : m.blk) {
+        update_cv_and_bv_rk<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param, dt, rk);
+        apply_bcs<mix, true>(*c);
+      }
+      communicate<mix, true>(m);
+      for (RefCtx *c : m.blk) update_physical_properties<mix><<<bpg(c, 1), tpb>>>(c->d_zone, c->d_param);
     }
-    if (res_hist) residual<mix>(c, res_hist + 4 * s);
+    if (res_hist) {
+      double acc[4] = {0, 0, 0, 0};
+      for (RefCtx *c : m.blk) {
+        double r[4];
+        block_residual(*c, r);
+        for (int l = 0; l < 4; ++l) acc[l] += r[l];
+      }
+      for (int l = 0; l < 4; ++l) res_hist[4 * s + l] = std::sqrt(acc[l] / n_total);
+    }
     if (dt_hist) dt_hist[s] = dt;
   }
   cudaError_t e = cudaDeviceSynchronize();
   return e == cudaSuccess ? 0 : 2;
 }
 
-}  // namespace
-
-extern "C" {
-
-int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, const ostc_bc_face *f, int nf,
-               void **out) {
-  if (!cfg || !p || !z || !out) return 1;
-  if (p->turbulence || (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_FR))
-    return 5;
+// one block: its DZone, DParameter, boundary records and condition structs;
+// f holds this block's faces only (their index is the reference's i_face)
+RefCtx *make_block(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z,
+                   const std::vector<ostc_bc_face> &f, const std::vector<ostc_interface> &inner, int *status) {
   auto *c = new RefCtx;
   c->cfg = *cfg;
   c->mix = p->mix_model;
@@ -339,11 +391,13 @@ int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, 
   c->parameter->update_parameter("inviscid_type", p->inviscid_type);
   c->parameter->update_parameter("n_spec", p->n_spec);
   c->block = new Block(z->mx, z->my, z->mz, z->ngg, 0);
+  const int nf = (int)f.size();
   for (int q = 0; q < nf; ++q) {
     const int t = f[q].type_label;
     if (t != 2 && t != 3 && t != 4 && t != 5 && t != 6 && t != 7 && t != 9) {
       delete c;
-      return 5;  // the reference has no periodic boundary (quirk A13)
+      *status = 5;  // the reference has no periodic boundary (quirk A13)
+      return nullptr;
     }
     Boundary b;
     for (int d = 0; d < 3; ++d) {
@@ -429,34 +483,98 @@ int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, 
       c->face_inflow.back() = (int)c->d_inflows.size() - 1;
     }
   }
+  // InnerFace after register_boundary (Mesh.cpp:34-178); no default constructor either
+  for (const ostc_interface &s : inner) {
+    alignas(InnerFace) unsigned char buf[sizeof(InnerFace)];
+    std::memset(buf, 0, sizeof(buf));
+    InnerFace *fc = reinterpret_cast<InnerFace *>(buf);
+    for (int d = 0; d < 3; ++d) {
+      fc->range_start[d] = s.range_start[d];
+      fc->range_end[d] = s.range_end[d];
+      fc->target_start[d] = s.target_start[d];
+      fc->loop_dir[d] = s.loop_dir[d];
+      fc->target_loop_dir[d] = s.target_loop_dir[d];
+      fc->src_tar[d] = s.src_tar[d];
+      fc->n_point[d] = s.n_point[d];
+    }
+    fc->face = s.face;
+    fc->direction = s.direction;
+    fc->target_block = s.target;
+    c->inner.push_back(*fc);
+    c->inner_target.push_back(s.target);
+  }
   build_param(*c, p);
   build_zone(*c, z, p);
+  *status = 0;
+  return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+// all blocks of a run: faces[q].block and ifaces[q].block pick the block
+int ref_create_multi(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, int nz, const ostc_bc_face *f,
+                     int nf, const ostc_interface *ifc, int nif, void **out) {
+  if (!cfg || !p || !z || !out || nz < 1) return 1;
+  if (p->turbulence || (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_FR)) return 5;
+  for (int q = 0; q < nf; ++q)
+    if (f[q].block < 0 || f[q].block >= nz) return 1;
+  for (int q = 0; q < nif; ++q)
+    if (ifc[q].block < 0 || ifc[q].block >= nz || ifc[q].target < 0 || ifc[q].target >= nz) return 1;
+  auto *m = new RefMulti;
+  m->cfg = *cfg;
+  m->mix = p->mix_model;
+  for (int b = 0; b < nz; ++b) {
+    std::vector<ostc_bc_face> fb;
+    std::vector<ostc_interface> ib;
+    for (int q = 0; q < nf; ++q)
+      if (f[q].block == b) fb.push_back(f[q]);
+    for (int q = 0; q < nif; ++q)
+      if (ifc[q].block == b) ib.push_back(ifc[q]);
+    int st = 0;
+    RefCtx *c = make_block(cfg, p, z + b, fb, ib, &st);
+    if (!c) {
+      delete m;
+      return st;
+    }
+    m->blk.push_back(c);
+  }
   if (cudaDeviceSynchronize() != cudaSuccess) return 2;
-  *out = c;
+  *out = m;
   return 0;
 }
 
+int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, const ostc_bc_face *f, int nf,
+               void **out) {
+  if (!z) return 1;
+  for (int q = 0; q < nf; ++q)
+    if (f[q].block != 0) return 1;
+  return ref_create_multi(cfg, p, z, 1, f, nf, nullptr, 0, out);
+}
+
 int ref_initialize(void *h) {
-  auto *c = (RefCtx *)h;
-  if (c->mix == OSTC_MIX_AIR) initialize<MixtureModel::Air>(*c); else initialize<MixtureModel::FR>(*c);
+  auto *m = (RefMulti *)h;
+  if (m->mix == OSTC_MIX_AIR) initialize<MixtureModel::Air>(*m); else initialize<MixtureModel::FR>(*m);
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 int ref_rhs(void *h) {
-  auto *c = (RefCtx *)h;
-  if (c->mix == OSTC_MIX_AIR) rhs<MixtureModel::Air>(*c); else rhs<MixtureModel::FR>(*c);
+  auto *m = (RefMulti *)h;
+  for (RefCtx *c : m->blk) {
+    if (m->mix == OSTC_MIX_AIR) rhs<MixtureModel::Air>(*c); else rhs<MixtureModel::FR>(*c);
+  }
   return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
 }
 
 int ref_steps(void *h, int n, double *res_hist, double *dt_hist) {
-  auto *c = (RefCtx *)h;
-  return c->mix == OSTC_MIX_AIR ? steps<MixtureModel::Air>(*c, n, res_hist, dt_hist)
-                                : steps<MixtureModel::FR>(*c, n, res_hist, dt_hist);
+  auto *m = (RefMulti *)h;
+  return m->mix == OSTC_MIX_AIR ? steps<MixtureModel::Air>(*m, n, res_hist, dt_hist)
+                                : steps<MixtureModel::FR>(*m, n, res_hist, dt_hist);
 }
 
 // device time of n steps (CUDA events around the loop, as bench.py does for ours)
 double ref_time_steps(void *h, int n) {
-  auto *c = (RefCtx *)h;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -469,13 +587,15 @@ double ref_time_steps(void *h, int n) {
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  (void)c;
   return ms;
 }
 
-// copy a DZone array to the host: name in {bv, sv, cv, dq, mul, thermal_conductivity, vel, acoustic_speed, rho_D}
-int ref_download(void *h, const char *name, double *dst) {
-  auto *c = (RefCtx *)h;
+// copy a DZone array of block b to the host: name in {bv, sv, cv, dq, mul,
+// thermal_conductivity, vel, acoustic_speed, rho_D}
+int ref_download_block(void *h, int b, const char *name, double *dst) {
+  auto *m = (RefMulti *)h;
+  if (b < 0 || b >= (int)m->blk.size()) return 1;
+  RefCtx *c = m->blk[b];
   DZone &z = c->h;
   const size_t P = plane(c->mx, c->my, c->mz, c->ngg);
   const size_t I = plane(c->mx, c->my, c->mz, 0);
@@ -494,12 +614,17 @@ int ref_download(void *h, const char *name, double *dst) {
   return cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : 2;
 }
 
-// bytes of device memory the reference arrays of this context hold
+int ref_download(void *h, const char *name, double *dst) { return ref_download_block(h, 0, name, dst); }
+
+// bytes of device memory the reference arrays of this run hold
 double ref_device_bytes(void *h) {
-  auto *c = (RefCtx *)h;
-  const double P = (double)plane(c->mx, c->my, c->mz, c->ngg), I = (double)plane(c->mx, c->my, c->mz, 0);
-  double b = 8 * P * (1 + 10 + c->n_var * 2 + 6 + c->n_scalar + 5 + c->n_spec) + 8 * I * (4 + c->n_var + 5);
-  if (c->mix == OSTC_MIX_FR && c->h_param.chemSrcMethod == 1) b += 8 * I * c->n_spec * c->n_spec;
+  auto *m = (RefMulti *)h;
+  double b = 0;
+  for (RefCtx *c : m->blk) {
+    const double P = (double)plane(c->mx, c->my, c->mz, c->ngg), I = (double)plane(c->mx, c->my, c->mz, 0);
+    b += 8 * P * (1 + 10 + c->n_var * 2 + 6 + c->n_scalar + 5 + c->n_spec) + 8 * I * (4 + c->n_var + 5);
+    if (c->mix == OSTC_MIX_FR && c->h_param.chemSrcMethod == 1) b += 8 * I * c->n_spec * c->n_spec;
+  }
   return b;
 }
 

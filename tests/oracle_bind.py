@@ -79,10 +79,10 @@ class OracleRun:
         for b in range(len(self.blocks)):
             self._ck(oracle().oracle_compute_rhs(C.byref(self.param), C.byref(self.zones[b])), "oracle_compute_rhs")
 
-    def flux_scale(self):
-        """per-variable max |face flux| of the first block (recomputes dq)"""
-        out = (C.c_double * self.blocks[0].n_var)()
-        self._ck(oracle().oracle_flux_scale(C.byref(self.param), C.byref(self.zones[0]), out), "oracle_flux_scale")
+    def flux_scale(self, block=0):
+        """per-variable max |face flux| of one block (recomputes its dq)"""
+        out = (C.c_double * self.blocks[block].n_var)()
+        self._ck(oracle().oracle_flux_scale(C.byref(self.param), C.byref(self.zones[block]), out), "oracle_flux_scale")
         return np.array(out)
 
     def global_time_step(self):

@@ -27,6 +27,12 @@ def ref():
         L.ref_create.argtypes = [C.POINTER(ostc.Config), C.POINTER(ostc.Param), C.POINTER(ostc.Zone),
                                  C.POINTER(ostc.BcFaceC), C.c_int, C.POINTER(vp)]
         L.ref_create.restype = C.c_int
+        L.ref_create_multi.argtypes = [C.POINTER(ostc.Config), C.POINTER(ostc.Param), C.POINTER(ostc.Zone), C.c_int,
+                                       C.POINTER(ostc.BcFaceC), C.c_int, C.POINTER(ostc.IfaceC), C.c_int,
+                                       C.POINTER(vp)]
+        L.ref_create_multi.restype = C.c_int
+        L.ref_download_block.argtypes = [vp, C.c_int, C.c_char_p, d]
+        L.ref_download_block.restype = C.c_int
         for n in ("ref_initialize", "ref_rhs"):
             getattr(L, n).argtypes = [vp]
             getattr(L, n).restype = C.c_int
@@ -41,21 +47,24 @@ def ref():
 
 
 class RefCudaRun:
-    """The reference build on one block of a Case (single-rank)."""
+    """The reference build on all blocks of a Case (single-rank); blocks
+    exchange through the reference's inner_communication kernel."""
 
     def __init__(self, case):
         self.case = case
-        b = case.blocks[0]
-        self.block = b
+        self.blocks = case.blocks
+        self.block = case.blocks[0]
         self.param, self._keep = ostc.make_param(case.scheme, case.mech)
         self.config = ostc.make_config(case.scheme)
-        self.zone = b.zone()
+        self.zones = (ostc.Zone * len(case.blocks))(*[b.zone() for b in case.blocks])
         self.faces = (ostc.BcFaceC * max(len(case.faces), 1))(*case.faces)
+        ifs = list(getattr(case, "interfaces", []) or [])
+        self.ifaces = (ostc.IfaceC * max(len(ifs), 1))(*ifs)
         h = C.c_void_p()
-        st = ref().ref_create(C.byref(self.config), C.byref(self.param), C.byref(self.zone), self.faces,
-                              len(case.faces), C.byref(h))
+        st = ref().ref_create_multi(C.byref(self.config), C.byref(self.param), self.zones, len(case.blocks),
+                                    self.faces, len(case.faces), self.ifaces, len(ifs), C.byref(h))
         if st != 0:
-            raise RuntimeError("ref_create -> %d" % st)
+            raise RuntimeError("ref_create_multi -> %d" % st)
         self.h = h
 
     def initialize(self):
@@ -73,12 +82,12 @@ class RefCudaRun:
     def time_steps(self, n):
         return ref().ref_time_steps(self.h, n)
 
-    def download(self, name):
-        b = self.block
+    def download(self, name, block=0):
+        b = self.blocks[block]
         P = ostc.plane_shape(b.mx, b.my, b.mz, b.ngg)
         I = ostc.plane_shape(b.mx, b.my, b.mz, 0)
         shapes = {"bv": (6,) + P, "sv": (b.n_spec,) + P, "cv": (b.n_var,) + P, "dq": (b.n_var,) + I, "mul": P,
                   "thermal_conductivity": P, "vel": P, "acoustic_speed": P, "rho_D": (b.n_spec,) + P}
         out = np.zeros(shapes[name])
-        assert ref().ref_download(self.h, name.encode(), out.ctypes.data_as(C.POINTER(C.c_double))) == 0
+        assert ref().ref_download_block(self.h, block, name.encode(), out.ctypes.data_as(C.POINTER(C.c_double))) == 0
         return out
