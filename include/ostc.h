@@ -268,6 +268,36 @@ ostc_status ostc_rk3_stage(ostc_ctx *ctx, int rk, void *stream);
 ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist,
                            double *dt_hist, void *stream);
 
+/* ---- steady path (cfg.steady = 1; src/SteadySim.cuh:15-137) ------------ */
+
+/* local_time_step (src/TimeAdvanceFunc.cuh:50-100) on every block: per-cell
+ * dt_local (zone.dt_local, required when steady) and the inviscid spectral
+ * radii DPLUR reuses (kept in context-owned planes; zone.inv_spectr_rad and
+ * zone.visc_spectr_rad are not written).                                   */
+ostc_status ostc_local_time_step(ostc_ctx *ctx, void *stream);
+
+/* implicit_treatment (src/ImplicitTreatmentHPP.cuh:8-52) on every block.
+ * implicit_method 0: point-implicit chemistry of the explicit steady step,
+ * EPI (chemSrcMethod 1, src/FiniteRateChem.cu:234-256) or DA (2,
+ * src/FiniteRateChem.cu:421-432), applied to the species rows of dq.
+ * implicit_method 1: DPLUR (src/DPLUR.cuh:283-312) with DPLUR_inner_step
+ * Jacobi sweeps, wall dq set to 0 before each sweep, no exchange between
+ * blocks inside the sweeps; zone.dq0 / zone.dqk are used when given, else
+ * the context allocates them. The chemical Jacobian is rebuilt from the
+ * state inside the kernels (zone.chem_src_jac is neither read nor written);
+ * DPLUR keeps the LU factors of (diag I - dt J) for its sweeps.            */
+ostc_status ostc_implicit_treatment(ostc_ctx *ctx, void *stream);
+
+/* update_bv (src/FieldOperation.cuh:221-296): bv, sv (and T, p by the
+ * Newton solve of src/FieldOperation.cu:3-39) from dq * dt_local / jac.   */
+ostc_status ostc_update_bv(ostc_ctx *ctx, void *stream);
+
+/* n_steps steady iterations (the loop body of steady_simulation,
+ * src/SteadySim.cuh:51-126: RHS, local dt, implicit treatment, update_bv,
+ * BCs and interfaces without cv, properties), captured as a CUDA graph.
+ * res_hist as for ostc_rk3_steps; the caller tests convergence on it.      */
+ostc_status ostc_steady_steps(ostc_ctx *ctx, int n_steps, double *res_hist, void *stream);
+
 /* Metric and Jacobian from grid coordinates that carry ngg+1 ghost layers
  * (x,y,z as host arrays with ghost count ngg+1), as Block::compute_jac_metric
  * (src/Mesh.cpp:259-521). Host-only helper: fills host jac (g=ngg) and host

@@ -42,7 +42,12 @@ struct ostc_ctx {
   int *hist_counter = nullptr;
   int hist_cap = 0;
   double n_total = 0;
-  std::map<int, GraphEntry> graphs;  // key: with_residual
+  std::map<int, GraphEntry> graphs;  // key: with_residual (+2 for the steady step)
+  // steady path: spectral radii (3 interior planes), DPLUR buffers (dq layout),
+  // DPLUR point-implicit chemistry (LU factors + pivots, or DA divisors)
+  std::vector<double *> isr, dq0, dqk, lu, da;
+  std::vector<unsigned char *> piv;
+  std::vector<void *> owned;  // allocations of this context to free
   ostc_status last = OSTC_OK;
   int last_cuda = 0;
   int err_block = -1, err_i = 0, err_j = 0, err_k = 0;
@@ -142,6 +147,7 @@ void fill_devzone(const ostc_zone &z, DevZone &d) {
   d.wall = z.wall_distance;
   d.dt_local = z.dt_local;
   d.bv_last = z.bv_last;
+  d.isr = nullptr;
   d.jac = z.jac;
 }
 
@@ -164,7 +170,15 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
   if (p->inviscid_type == 2 && p->inviscid_scheme != 2) return OSTC_ERR_INVALID_ARG;
   if (p->inviscid_scheme < 1 || p->inviscid_scheme > 4) return OSTC_ERR_INVALID_ARG;
   if (p->limiter != 0) return OSTC_ERR_INVALID_ARG;
-  if (cfg->steady || cfg->temporal_scheme != 3) return OSTC_ERR_UNSUPPORTED;
+  if (cfg->steady) {
+    if (cfg->implicit_method != 0 && cfg->implicit_method != 1) return OSTC_ERR_UNSUPPORTED;
+    if (cfg->implicit_method == 1 && cfg->DPLUR_inner_step < 0) return OSTC_ERR_INVALID_ARG;
+    // quirk A6: the reference's steady path never computes cv, which AWENO reads
+    if (p->inviscid_type == 1) return OSTC_ERR_UNSUPPORTED;
+    if (p->chemSrcMethod < 0 || p->chemSrcMethod > 2) return OSTC_ERR_INVALID_ARG;
+  } else if (cfg->temporal_scheme != 3) {
+    return OSTC_ERR_UNSUPPORTED;
+  }
   if (!(p->cfl > 0) && !cfg->fixed_time_step) return OSTC_ERR_INVALID_ARG;
   const int need_ngg = p->inviscid_type == 1 ? 3 : 2;
   for (int b = 0; b < n_zones; ++b) {
@@ -176,6 +190,8 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
         !z.mul || !z.thermal_conductivity)
       return OSTC_ERR_INVALID_ARG;
     if (p->n_spec > 0 && (!z.sv || !z.rho_D || !z.gamma || !z.cp)) return OSTC_ERR_INVALID_ARG;
+    if (cfg->steady && !z.dt_local) return OSTC_ERR_INVALID_ARG;
+    if (cfg->steady && cfg->implicit_method == 1 && z.dq_ngg != 1) return OSTC_ERR_INVALID_ARG;  // Field.cu:213-221
     // int32 ghosted index space
     const double np = (double)(z.mx + 2 * z.ngg) * (z.my + 2 * z.ngg) * (z.mz + 2 * z.ngg);
     if (np * std::max(p->n_var, 6) >= 2147483647.0) return OSTC_ERR_INVALID_ARG;
@@ -397,6 +413,44 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
     c->face_zone.push_back(f.block);
   }
   if ((st = repack_metrics(ctx, nullptr))) return st;
+  if (cfg->steady) {
+    auto alloc = [&](size_t bytes) -> void * {
+      void *p = nullptr;
+      if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+      c->owned.push_back(p);
+      return p;
+    };
+    const int nv = param->n_var, ns = param->n_spec;
+    const bool dplur = cfg->implicit_method == 1;
+    const bool chem = param->mix_model == OSTC_MIX_FR && c->dp.n_reac > 0;
+    for (int b = 0; b < n_zones; ++b) {
+      DevZone &z = c->dz[b];
+      double *isr = (double *)alloc(sizeof(double) * 3 * z.nsz);
+      if (!isr) return fail(ctx, OSTC_ERR_CUDA, cudaErrorMemoryAllocation);
+      z.isr = isr;
+      c->isr.push_back(isr);
+      double *d0 = nullptr, *dk = nullptr, *lu = nullptr, *da = nullptr;
+      unsigned char *pv = nullptr;
+      if (dplur) {
+        d0 = zones[b].dq0 ? zones[b].dq0 : (double *)alloc(sizeof(double) * nv * z.qsz);
+        dk = zones[b].dqk ? zones[b].dqk : (double *)alloc(sizeof(double) * nv * z.qsz);
+        if (!d0 || !dk) return fail(ctx, OSTC_ERR_CUDA, cudaErrorMemoryAllocation);
+        if (chem && param->chemSrcMethod == 1) {
+          lu = (double *)alloc(sizeof(double) * ns * ns * z.nsz);
+          pv = (unsigned char *)alloc((size_t)ns * z.nsz);
+          if (!lu || !pv) return fail(ctx, OSTC_ERR_CUDA, cudaErrorMemoryAllocation);
+        } else if (chem && param->chemSrcMethod == 2) {
+          da = (double *)alloc(sizeof(double) * ns * z.nsz);
+          if (!da) return fail(ctx, OSTC_ERR_CUDA, cudaErrorMemoryAllocation);
+        }
+      }
+      c->dq0.push_back(d0);
+      c->dqk.push_back(dk);
+      c->lu.push_back(lu);
+      c->piv.push_back(pv);
+      c->da.push_back(da);
+    }
+  }
   CK(cudaMalloc(&c->dt_bits, sizeof(unsigned long long)));
   c->n_part_per_zone = 148 * 2;
   CK(cudaMalloc(&c->res_partial, sizeof(double) * 4 * c->n_part_per_zone * n_zones));
@@ -415,6 +469,7 @@ ostc_status ostc_destroy(ostc_ctx *ctx) {
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
   for (double *p : ctx->met_soa) cudaFree(p);
+  for (void *p : ctx->owned) cudaFree(p);
   cudaFree(ctx->dt_bits);
   cudaFree(ctx->res_partial);
   cudaFree(ctx->hist_counter);
@@ -653,14 +708,16 @@ static ostc_status ensure_hist(ostc_ctx *ctx, int n_steps) {
   return OSTC_OK;
 }
 
-static ostc_status ensure_graph(ostc_ctx *ctx, bool hist, GraphEntry **out) {
-  GraphEntry &ge = ctx->graphs[hist ? 1 : 0];
+static ostc_status enqueue_steady_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s);
+
+static ostc_status ensure_graph(ostc_ctx *ctx, bool hist, GraphEntry **out, bool steady = false) {
+  GraphEntry &ge = ctx->graphs[(hist ? 1 : 0) + (steady ? 2 : 0)];
   if (!ge.exec) {
     // a legacy default stream cannot be captured: capture on a private stream
     cudaStream_t cs;
     CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    ostc_status st = enqueue_step(ctx, hist, cs);
+    ostc_status st = steady ? enqueue_steady_step(ctx, hist, cs) : enqueue_step(ctx, hist, cs);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
@@ -675,6 +732,7 @@ static ostc_status ensure_graph(ostc_ctx *ctx, bool hist, GraphEntry **out) {
 
 ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist, double *dt_hist, void *stream) {
   if (!ctx || n_steps < 0) return OSTC_ERR_INVALID_ARG;
+  if (ctx->cfg.steady) return OSTC_ERR_INVALID_ARG;
   cudaStream_t s = S(stream);
   const bool hist = res_hist || dt_hist;
   ostc_status st;
@@ -687,6 +745,115 @@ ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist, double 
   if (hist) {
     if (res_hist) CK(cudaMemcpyAsync(res_hist, ctx->hist_res, sizeof(double) * 4 * n_steps, cudaMemcpyDeviceToHost, s));
     if (dt_hist) CK(cudaMemcpyAsync(dt_hist, ctx->hist_dt, sizeof(double) * n_steps, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  return OSTC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// steady path (SteadySim.cuh:15-137)
+// ---------------------------------------------------------------------------
+ostc_status ostc_local_time_step(ostc_ctx *ctx, void *stream) {
+  if (!ctx || !ctx->cfg.steady) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  CellArgs a;
+  a.dt_bits = ctx->dt_bits;
+  CK(launch_cells<0>(CellOp::DtReset, ctx->dz[0], a, S(stream)));
+  for (auto &z : ctx->dz)
+    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Dt, z, a, S(stream)); }));
+  return OSTC_OK;
+}
+
+ostc_status ostc_implicit_treatment(ostc_ctx *ctx, void *stream) {
+  if (!ctx || !ctx->cfg.steady) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  cudaStream_t s = S(stream);
+  if (ctx->cfg.implicit_method == 0) {
+    if (!ctx->has_source || ctx->prm.chemSrcMethod == 0) return OSTC_OK;
+    for (auto &z : ctx->dz)
+      CK(dispatch_ns(ctx->ns, [&](auto n) {
+        return launch_steady<decltype(n)::value>(SteadyOp::ChemImplicit, z, SteadyArgs{}, nullptr, s);
+      }));
+    return OSTC_OK;
+  }
+  // DPLUR (DPLUR.cuh:283-312): no exchange between blocks inside the sweeps (quirk A11)
+  for (size_t b = 0; b < ctx->dz.size(); ++b) {
+    const DevZone &z = ctx->dz[b];
+    SteadyArgs a;
+    a.dq0 = ctx->dq0[b];
+    a.lu = ctx->lu[b];
+    a.piv = ctx->piv[b];
+    a.da = ctx->da[b];
+    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_steady<decltype(n)::value>(SteadyOp::DplurDq0, z, a, nullptr, s); }));
+    double *cur = z.dq, *nxt = ctx->dqk[b];
+    for (int it = 0; it < ctx->cfg.DPLUR_inner_step; ++it) {
+      for (size_t q = 0; q < ctx->faces.size(); ++q) {
+        if (ctx->face_zone[q] != (int)b || ctx->faces[q].type != OSTC_BC_WALL) continue;
+        SteadyArgs w;
+        w.dq_out = cur;
+        CK(dispatch_ns(ctx->ns, [&](auto n) {
+          return launch_steady<decltype(n)::value>(SteadyOp::WallDqZero, z, w, &ctx->faces[q], s);
+        }));
+      }
+      a.dq_in = cur;
+      a.dq_out = nxt;
+      CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_steady<decltype(n)::value>(SteadyOp::DplurSweep, z, a, nullptr, s); }));
+      std::swap(cur, nxt);
+    }
+    a.dq_in = cur;
+    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_steady<decltype(n)::value>(SteadyOp::DplurFinish, z, a, nullptr, s); }));
+  }
+  return OSTC_OK;
+}
+
+ostc_status ostc_update_bv(ostc_ctx *ctx, void *stream) {
+  if (!ctx || !ctx->cfg.steady) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  for (auto &z : ctx->dz)
+    CK(dispatch_ns(ctx->ns, [&](auto n) {
+      return launch_steady<decltype(n)::value>(SteadyOp::UpdateBv, z, SteadyArgs{}, nullptr, S(stream));
+    }));
+  return OSTC_OK;
+}
+
+static ostc_status enqueue_steady_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
+  ostc_status st;
+  if (with_hist)
+    for (auto &z : ctx->dz) CK(launch_cells<0>(CellOp::StoreLast, z, {}, s));
+  if ((st = ostc_compute_rhs(ctx, s))) return st;
+  if ((st = ostc_local_time_step(ctx, s))) return st;
+  if ((st = ostc_implicit_treatment(ctx, s))) return st;
+  if ((st = ostc_update_bv(ctx, s))) return st;
+  if ((st = ostc_apply_boundary_conditions(ctx, 0, s))) return st;
+  if ((st = ostc_data_communication(ctx, 0, s))) return st;
+  if ((st = ostc_update_physical_properties(ctx, s))) return st;
+  if (with_hist) {
+    CellArgs a;
+    a.n_part = ctx->n_part_per_zone;
+    for (size_t b = 0; b < ctx->dz.size(); ++b) {
+      a.partial = ctx->res_partial + 4 * ctx->n_part_per_zone * b;
+      CK(launch_cells<0>(CellOp::ResidualPartial, ctx->dz[b], a, s));
+    }
+    step_end_kernel<<<1, 32, 0, s>>>(ctx->res_partial, ctx->n_part_per_zone * (int)ctx->dz.size(), ctx->n_total,
+                                     nullptr, 0.0, ctx->hist_res, nullptr, ctx->hist_counter, ctx->hist_cap);
+    CK(cudaGetLastError());
+  }
+  return OSTC_OK;
+}
+
+ostc_status ostc_steady_steps(ostc_ctx *ctx, int n_steps, double *res_hist, void *stream) {
+  if (!ctx || n_steps < 0 || !ctx->cfg.steady) return OSTC_ERR_INVALID_ARG;
+  cudaStream_t s = S(stream);
+  const bool hist = res_hist != nullptr;
+  ostc_status st;
+  if (hist && (st = ensure_hist(ctx, n_steps))) return st;
+  if (ensure_param(ctx, s)) return ctx->last;
+  if (hist) CK(cudaMemsetAsync(ctx->hist_counter, 0, sizeof(int), s));
+  GraphEntry *ge = nullptr;
+  if ((st = ensure_graph(ctx, hist, &ge, true))) return st;
+  for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(ge->exec, s));
+  if (hist) {
+    CK(cudaMemcpyAsync(res_hist, ctx->hist_res, sizeof(double) * 4 * n_steps, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
   }
   return OSTC_OK;

@@ -29,16 +29,83 @@ __device__ __forceinline__ double arrhenius(double lnT, double invT, double A, d
   return A * exp(b * lnT - Ea * invT);
 }
 
-// omega[NS] in kg/(m^3 s) at density rho, temperature t, mass fractions Y
+// rate of progress of reaction r: q1 = kf prod c^nu', q2 = kb prod c^nu''
+// (forward_reaction_rate, backward_reaction_rate and rate_of_progress of
+// FiniteRateChem.cu:65-176 for one reaction); g is the Gibbs energy / RT
 template <int NS>
-__device__ __forceinline__ void chemistry_omega(double rho, double t, const double *Y, double *omega) {
-  double c[NS];
+__device__ __forceinline__ void reaction_q(int r, double t, double lnT, double invT, double ln_temp_t,
+                                           const double *c, const double *g, double &q1, double &q2) {
+  const int type = c_p.reac_type[r];
+  double kf = arrhenius(lnT, invT, c_p.A[r], c_p.b[r], c_p.Ea[r]);
+  if (type == 3) kf += arrhenius(lnT, invT, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
+  if (type > 3) {
+    double cc = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) cc += c[l] * c_p.tb[r][l];
+    if (type == 4) {
+      kf *= cc;
+    } else {
+      const double kf_low = arrhenius(lnT, invT, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
+      const double kf_high = kf;
+      const double pr = kf_low * cc / kf_high;
+      double F = 1.0;
+      if (type > 5) {
+        double f_cent = (1 - c_p.troe_alpha[r]) * exp(-t / c_p.troe_t3[r]) + c_p.troe_alpha[r] * exp(-t / c_p.troe_t1[r]);
+        if (type == 7) f_cent += exp(-c_p.troe_t2[r] / t);
+        const double logFc = log10(f_cent);
+        const double cc2 = -0.4 - 0.67 * logFc;
+        const double nn = 0.75 - 1.27 * logFc;
+        const double logPr = log10(pr);
+        const double tempo = (logPr + cc2) / (nn - 0.14 * (logPr + cc2));
+        const double pp = logFc / (1.0 + tempo * tempo);
+        F = pow(10.0, pp);
+      }
+      kf = kf_high * pr / (1.0 + pr) * F;
+    }
+  }
+  double kb = 0;
+  if (type == 2) {
+    kb = arrhenius(lnT, invT, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
+  } else if (type != 0) {
+    double dg = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) dg += g[l] * (c_p.nub[r][l] - c_p.nuf[r][l]);
+    // kf / (temp_t^order exp(-dg)) as one exponential
+    kb = kf * exp(dg - c_p.reac_order[r] * ln_temp_t);
+  }
+  // species in increasing order, as the reference's loop
+  q1 = 1.0;
+  q2 = 1.0;
+#pragma unroll
+  for (int l = 0; l < NS; ++l) {
+    const int nf = c_p.nuf[r][l], nb = c_p.nub[r][l];
+    if (nf) q1 *= ipow(c[l], nf);
+    if (nb && type != 0) q2 *= ipow(c[l], nb);
+  }
+  q1 *= kf;
+  if (type != 0) q2 *= kb; else q2 = 0.0;
+}
+
+// concentrations in mol/cm^3 and the Gibbs terms shared by all reactions
+template <int NS>
+__device__ __forceinline__ void chemistry_setup(double rho, double t, const double *Y, double *c, double *g,
+                                                double &lnT, double &invT, double &ln_temp_t) {
 #pragma unroll
   for (int l = 0; l < NS; ++l) c[l] = rho * Y[l] / c_p.mw[l] * 1e-3;
-  double g[NS];
   if (c_p.need_gibbs) gibbs_div_rt<NS>(t, g);
   constexpr double temp_p = p_atm / R_u * 1e-3;
   const double temp_t = temp_p / t;
+  lnT = log(t);
+  invT = 1.0 / t;
+  ln_temp_t = log(temp_t);
+}
+
+// omega[NS] in kg/(m^3 s) at density rho, temperature t, mass fractions Y
+template <int NS>
+__device__ __forceinline__ void chemistry_omega(double rho, double t, const double *Y, double *omega) {
+  double c[NS], g[NS];
+  double lnT, invT, ln_temp_t;
+  chemistry_setup<NS>(rho, t, Y, c, g, lnT, invT, ln_temp_t);
   double cre[NS], des[NS];
 #pragma unroll
   for (int l = 0; l < NS; ++l) {
@@ -46,57 +113,9 @@ __device__ __forceinline__ void chemistry_omega(double rho, double t, const doub
     des[l] = 0;
   }
   const int nr = c_p.n_reac;
-  const double lnT = log(t), invT = 1.0 / t;
-  const double ln_temp_t = log(temp_t);
   for (int r = 0; r < nr; ++r) {
-    const int type = c_p.reac_type[r];
-    double kf = arrhenius(lnT, invT, c_p.A[r], c_p.b[r], c_p.Ea[r]);
-    if (type == 3) kf += arrhenius(lnT, invT, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
-    if (type > 3) {
-      double cc = 0;
-#pragma unroll
-      for (int l = 0; l < NS; ++l) cc += c[l] * c_p.tb[r][l];
-      if (type == 4) {
-        kf *= cc;
-      } else {
-        const double kf_low = arrhenius(lnT, invT, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
-        const double kf_high = kf;
-        const double pr = kf_low * cc / kf_high;
-        double F = 1.0;
-        if (type > 5) {
-          double f_cent = (1 - c_p.troe_alpha[r]) * exp(-t / c_p.troe_t3[r]) + c_p.troe_alpha[r] * exp(-t / c_p.troe_t1[r]);
-          if (type == 7) f_cent += exp(-c_p.troe_t2[r] / t);
-          const double logFc = log10(f_cent);
-          const double cc2 = -0.4 - 0.67 * logFc;
-          const double nn = 0.75 - 1.27 * logFc;
-          const double logPr = log10(pr);
-          const double tempo = (logPr + cc2) / (nn - 0.14 * (logPr + cc2));
-          const double pp = logFc / (1.0 + tempo * tempo);
-          F = pow(10.0, pp);
-        }
-        kf = kf_high * pr / (1.0 + pr) * F;
-      }
-    }
-    double kb = 0;
-    if (type == 2) {
-      kb = arrhenius(lnT, invT, c_p.A2[r], c_p.b2[r], c_p.Ea2[r]);
-    } else if (type != 0) {
-      double dg = 0;
-#pragma unroll
-      for (int l = 0; l < NS; ++l) dg += g[l] * (c_p.nub[r][l] - c_p.nuf[r][l]);
-      // kf / (temp_t^order exp(-dg)) as one exponential
-      kb = kf * exp(dg - c_p.reac_order[r] * ln_temp_t);
-    }
-    // rates of progress: species in increasing order, as the reference's loop
-    double q1 = 1.0, q2 = 1.0;
-#pragma unroll
-    for (int l = 0; l < NS; ++l) {
-      const int nf = c_p.nuf[r][l], nb = c_p.nub[r][l];
-      if (nf) q1 *= ipow(c[l], nf);
-      if (nb && type != 0) q2 *= ipow(c[l], nb);
-    }
-    q1 *= kf;
-    if (type != 0) q2 *= kb; else q2 = 0.0;
+    double q1, q2;
+    reaction_q<NS>(r, t, lnT, invT, ln_temp_t, c, g, q1, q2);
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
       const int nf = c_p.nuf[r][l], nb = c_p.nub[r][l];
@@ -108,6 +127,117 @@ __device__ __forceinline__ void chemistry_omega(double rho, double t, const doub
   }
 #pragma unroll
   for (int l = 0; l < NS; ++l) omega[l] = cre[l] * (c_p.mw[l] * 1e+3) - des[l] * (c_p.mw[l] * 1e+3);
+}
+
+// Rates of progress of all reactions plus omega and its destruction part
+// omega_d (chemical_source, FiniteRateChem.cu:178-194): the inputs of the
+// chemical Jacobians.
+template <int NS>
+__device__ __forceinline__ void chemistry_rates(double rho, double t, const double *Y, double *q1, double *q2,
+                                                double *omega, double *omega_d) {
+  double c[NS], g[NS];
+  double lnT, invT, ln_temp_t;
+  chemistry_setup<NS>(rho, t, Y, c, g, lnT, invT, ln_temp_t);
+  double cre[NS], des[NS];
+#pragma unroll
+  for (int l = 0; l < NS; ++l) {
+    cre[l] = 0;
+    des[l] = 0;
+  }
+  const int nr = c_p.n_reac;
+  for (int r = 0; r < nr; ++r) {
+    reaction_q<NS>(r, t, lnT, invT, ln_temp_t, c, g, q1[r], q2[r]);
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      const int nf = c_p.nuf[r][l], nb = c_p.nub[r][l];
+      if (nf | nb) {
+        cre[l] += q2[r] * nf + q1[r] * nb;
+        des[l] += q1[r] * nf + q2[r] * nb;
+      }
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < NS; ++l) {
+    omega[l] = cre[l] * (c_p.mw[l] * 1e+3) - des[l] * (c_p.mw[l] * 1e+3);
+    omega_d[l] = des[l] * (c_p.mw[l] * 1e+3);
+  }
+}
+
+// d omega_m / d (rho Y_n), row-major m * NS + n (compute_chem_src_jacobian,
+// FiniteRateChem.cu:196-216): q in mol/(cm^3 s); columns of absent species
+// (Y_n <= 1e-25) are zero
+template <int NS>
+__device__ __forceinline__ void chemistry_jacobian(double rho, const double *Y, const double *q1, const double *q2,
+                                                   double *J) {
+  const int nr = c_p.n_reac;
+#pragma unroll 1
+  for (int m = 0; m < NS; ++m) {
+#pragma unroll 1
+    for (int n = 0; n < NS; ++n) {
+      double zz = 0;
+      if (Y[n] > 1e-25) {
+        for (int r = 0; r < nr; ++r)
+          zz += (c_p.nub[r][m] - c_p.nuf[r][m]) * (c_p.nuf[r][n] * q1[r] - c_p.nub[r][n] * q2[r]);
+        zz /= rho * Y[n];
+      }
+      J[m * NS + n] = c_p.mw[m] * zz * 1e+3;
+    }
+  }
+}
+
+// Column-pivoted Crout LU factorisation in place (A row-major NS x NS) in
+// the operation order of solve_chem_system (FiniteRateChem.cu:324-419)
+template <int NS>
+__device__ __forceinline__ void lu_factor(double *A, int *ipiv) {
+#pragma unroll 1
+  for (int n = 0; n < NS; ++n) {
+    int ik = n;
+    for (int m = n; m < NS; ++m) {
+      for (int t = 0; t < n; ++t) A[m * NS + n] -= A[m * NS + t] * A[t * NS + n];
+      if (fabs(A[m * NS + n]) > fabs(A[ik * NS + n])) ik = m;
+    }
+    ipiv[n] = ik;
+    if (ik != n) {
+      for (int t = 0; t < NS; ++t) {
+        const double mid = A[ik * NS + t];
+        A[ik * NS + t] = A[n * NS + t];
+        A[n * NS + t] = mid;
+      }
+    }
+    for (int p = n + 1; p < NS; ++p)
+      for (int t = 0; t < n; ++t) A[n * NS + p] -= A[n * NS + t] * A[t * NS + p];
+    for (int m = n + 1; m < NS; ++m) A[m * NS + n] /= A[n * NS + n];
+  }
+}
+
+// b <- A^-1 b with the factors and pivots of lu_factor
+template <int NS>
+__device__ __forceinline__ void lu_apply(const double *A, const int *ipiv, double *b) {
+#pragma unroll 1
+  for (int m = 0; m < NS; ++m) {
+    const int t = ipiv[m];
+    if (t != m) {
+      const double mid = b[t];
+      b[t] = b[m];
+      b[m] = mid;
+    }
+  }
+#pragma unroll 1
+  for (int m = 1; m < NS; ++m)
+    for (int t = 0; t < m; ++t) b[m] -= A[m * NS + t] * b[t];
+  b[NS - 1] /= A[NS * NS - 1];
+#pragma unroll 1
+  for (int m = NS - 2; m >= 0; --m) {
+    for (int t = m + 1; t < NS; ++t) b[m] -= A[m * NS + t] * b[t];
+    b[m] /= A[m * NS + m];
+  }
+}
+
+template <int NS>
+__device__ __forceinline__ void lu_solve(double *A, double *b) {
+  int ipiv[NS];
+  lu_factor<NS>(A, ipiv);
+  lu_apply<NS>(A, ipiv, b);
 }
 
 // mixture transport at one state (Transport.cu:40-109)

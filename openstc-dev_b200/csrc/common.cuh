@@ -61,6 +61,7 @@ struct DevZone {
   double *bv, *sv, *cv, *qn, *dq;
   double *vel, *a, *mach, *mul, *kappa, *rhoD, *gam, *cp, *mut, *ttc, *wall;
   double *dt_local, *bv_last;
+  double *isr;  // inviscid spectral radii, 3 interior planes (steady path; null otherwise)
   const double *jac;
   const double *met;  // 9 SoA planes (context-owned copy), ghosted layout
   int block_id;

@@ -370,6 +370,12 @@ __global__ void __launch_bounds__(256) dt_kernel(DevZone z, unsigned long long *
     srv *= c1 * c2;
     dtl = c_p.cfl / (sri + srv);
     if (z.dt_local) z.dt_local[nidx(z, i, j, k)] = dtl;
+    if (z.isr) {  // the radii DPLUR reuses (TimeAdvanceFunc.cuh:72-77)
+      const int n = nidx(z, i, j, k);
+      z.isr[n] = fabs(U) + a * gx;
+      z.isr[z.nsz + n] = fabs(V) + a * ge;
+      z.isr[2 * z.nsz + n] = d3 ? fabs(W) + a * gz : 0.0;
+    }
   }
   // warp then block min
 #pragma unroll
@@ -832,6 +838,12 @@ __global__ void residual_final_kernel(const double *partial, int n_part, double 
   out[l] = sqrt(s / n_total);
 }
 
+}  // namespace ostc
+
+#include "steady.cuh"
+
+namespace ostc {
+
 // ---------------------------------------------------------------------------
 // host-side launchers (kernels.cuh)
 // ---------------------------------------------------------------------------
@@ -971,6 +983,38 @@ cudaError_t launch_interface(const DevZone &self, const DevZone &tar, const Ifac
   return cudaGetLastError();
 }
 
+template <int NS>
+cudaError_t launch_steady(SteadyOp op, const DevZone &z, const SteadyArgs &a, const BcFace *wall, cudaStream_t s) {
+  const dim3 blk(32, 8), blk4(32, 4);
+  switch (op) {
+    case SteadyOp::ChemImplicit:
+      chem_implicit_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk4), blk4, 0, s>>>(z);
+      break;
+    case SteadyOp::UpdateBv:
+      update_bv_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z);
+      break;
+    case SteadyOp::DplurDq0:
+      dplur_dq0_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk4), blk4, 0, s>>>(z, a);
+      break;
+    case SteadyOp::DplurSweep:
+      dplur_sweep_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk4), blk4, 0, s>>>(z, a);
+      break;
+    case SteadyOp::DplurFinish:
+      dplur_finish_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z, a.dq_in);
+      break;
+    case SteadyOp::WallDqZero: {
+      if (!wall) return cudaErrorInvalidValue;
+      const BcFace &b = *wall;
+      const int n0 = b.re[0] - b.rs[0] + 1, n1 = b.re[1] - b.rs[1] + 1, n2 = b.re[2] - b.rs[2] + 1;
+      const dim3 wb(n0 >= 32 ? 32 : (n0 >= 8 ? 8 : 1), n1 >= 8 ? 8 : 1);
+      wall_dq_zero_kernel<NS><<<dim3((n0 + wb.x - 1) / wb.x, (n1 + wb.y - 1) / wb.y, n2), wb, 0, s>>>(
+          z, b, a.dq_out);
+      break;
+    }
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   return cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
 }
@@ -979,7 +1023,8 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   template cudaError_t launch_flux<NS>(const DevZone &, int, int, const TileShape &, int, int, cudaStream_t); \
   template cudaError_t launch_cells<NS>(CellOp, const DevZone &, const CellArgs &, cudaStream_t);            \
   template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);                    \
-  template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t);
+  template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t); \
+  template cudaError_t launch_steady<NS>(SteadyOp, const DevZone &, const SteadyArgs &, const BcFace *, cudaStream_t);
 
 OSTC_INSTANTIATE(0)
 OSTC_INSTANTIATE(9)

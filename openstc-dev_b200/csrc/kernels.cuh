@@ -43,6 +43,18 @@ struct CellArgs {
   int n_part = 0;
 };
 
+// the steady path (steady.cuh)
+enum class SteadyOp { ChemImplicit, UpdateBv, DplurDq0, DplurSweep, DplurFinish, WallDqZero };
+struct SteadyArgs {
+  const double *dq_in = nullptr;  // DPLUR sweep: current iterate (dq layout)
+  double *dq_out = nullptr;       // DPLUR sweep: next iterate
+  double *dq0 = nullptr;          // DPLUR: dq after compute_DQ_0 (dq layout)
+  double *lu = nullptr;           // DPLUR + EPI: NS*NS interior planes of LU factors
+  unsigned char *piv = nullptr;   // DPLUR + EPI: NS interior planes of pivot rows
+  double *da = nullptr;           // DPLUR + DA: NS interior planes of diag - dt J_ll
+  int final_div = 0;              // DPLUR sweep: write (dq0 + ...) / dt_local into dq_out
+};
+
 template <int NS>
 cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, int accumulate, int viscous,
                         cudaStream_t s);
@@ -52,6 +64,8 @@ template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s);
 template <int NS>
 cudaError_t launch_interface(const DevZone &self, const DevZone &tar, const Iface &f, int with_cv, cudaStream_t s);
+template <int NS>
+cudaError_t launch_steady(SteadyOp op, const DevZone &z, const SteadyArgs &a, const BcFace *wall, cudaStream_t s);
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
 cudaError_t upload_param(const DevParam &p, cudaStream_t s);
 

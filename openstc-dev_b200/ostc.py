@@ -128,6 +128,10 @@ def lib():
             "ostc_launch_op": [vp, i, i, vp],
             "ostc_set_interfaces": [vp, C.POINTER(IfaceC), i],
             "ostc_step_kernel_count": [vp, i, C.POINTER(i)],
+            "ostc_local_time_step": [vp, vp],
+            "ostc_implicit_treatment": [vp, vp],
+            "ostc_update_bv": [vp, vp],
+            "ostc_steady_steps": [vp, i, C.POINTER(d), vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -194,6 +198,14 @@ class Scheme:
     entropy_fix_factor: float = 0.125
     fixed_time_step: int = 0
     dt: float = 1e-6
+    steady: int = 0               # 1: local time stepping (steady_simulation)
+    implicit_method: int = 0      # steady: 0 explicit (+ EPI/DA chemistry), 1 DPLUR
+    dplur_inner_step: int = 3
+
+    @property
+    def dq_ngg(self):
+        # dq carries one ghost layer under DPLUR (Field.cu:213-221)
+        return 1 if (self.steady and self.implicit_method == 1) else 0
 
     @property
     def inviscid_type(self):
@@ -245,10 +257,10 @@ def make_param(s: Scheme, mech: Optional[Mechanism]):
 
 def make_config(s: Scheme, output_screen: int = 1) -> Config:
     c = Config()
-    c.steady = 0
+    c.steady = s.steady
     c.temporal_scheme = 3
-    c.implicit_method = 0
-    c.DPLUR_inner_step = 3
+    c.implicit_method = s.implicit_method
+    c.DPLUR_inner_step = s.dplur_inner_step
     c.fixed_time_step = s.fixed_time_step
     c.dt = s.dt
     c.output_screen = output_screen
@@ -269,18 +281,20 @@ class HostBlock:
     n_var: int
     n_spec: int
     arrays: Dict[str, np.ndarray] = field(default_factory=dict)
+    dq_ngg: int = 0
 
     def plane(self, g=None):
         return plane_shape(self.mx, self.my, self.mz, self.ngg if g is None else g)
 
     @staticmethod
-    def specs(mx, my, mz, ngg, n_var, n_spec):
+    def specs(mx, my, mz, ngg, n_var, n_spec, dq_ngg=0):
         """name -> (shape, dtype) of every array of a block (Field::setup_device_memory)."""
         P = plane_shape(mx, my, mz, ngg)
         I = plane_shape(mx, my, mz, 0)
+        Q = plane_shape(mx, my, mz, dq_ngg)
         f8 = np.float64
         sp = {"bv": ((6,) + P, f8), "sv": ((n_spec,) + P, f8), "cv": ((n_var,) + P, f8),
-              "qn": ((n_var,) + P, f8), "dq": ((n_var,) + I, f8), "jac": (P, f8), "metric": (P, METRIC_DTYPE)}
+              "qn": ((n_var,) + P, f8), "dq": ((n_var,) + Q, f8), "jac": (P, f8), "metric": (P, METRIC_DTYPE)}
         for n in ("vel", "acoustic_speed", "mach", "mul", "thermal_conductivity"):
             sp[n] = (P, f8)
         if n_spec:
@@ -294,18 +308,19 @@ class HostBlock:
     INPUTS = ("bv", "sv", "jac", "metric")
 
     @staticmethod
-    def allocate(mx, my, mz, ngg, n_var, n_spec, full=True) -> "HostBlock":
+    def allocate(mx, my, mz, ngg, n_var, n_spec, full=True, dq_ngg=0) -> "HostBlock":
         """full=False holds only the inputs (bv, sv, jac, metric); the device
         block creates the rest zero-filled."""
-        b = HostBlock(mx, my, mz, ngg, n_var, n_spec)
-        for n, (shape, dt) in HostBlock.specs(mx, my, mz, ngg, n_var, n_spec).items():
+        b = HostBlock(mx, my, mz, ngg, n_var, n_spec, dq_ngg=dq_ngg)
+        for n, (shape, dt) in HostBlock.specs(mx, my, mz, ngg, n_var, n_spec, dq_ngg).items():
             if full or n in HostBlock.INPUTS:
                 b.arrays[n] = np.zeros(shape, dtype=dt)
         return b
 
     def complete(self) -> "HostBlock":
         """a full copy (all arrays) for the oracle"""
-        b = HostBlock.allocate(self.mx, self.my, self.mz, self.ngg, self.n_var, self.n_spec, full=True)
+        b = HostBlock.allocate(self.mx, self.my, self.mz, self.ngg, self.n_var, self.n_spec, full=True,
+                               dq_ngg=self.dq_ngg)
         for n, v in self.arrays.items():
             b.arrays[n][...] = v
         return b
@@ -315,7 +330,7 @@ class HostBlock:
 
     def zone(self) -> Zone:
         z = Zone()
-        z.mx, z.my, z.mz, z.ngg, z.dq_ngg = self.mx, self.my, self.mz, self.ngg, 0
+        z.mx, z.my, z.mz, z.ngg, z.dq_ngg = self.mx, self.my, self.mz, self.ngg, self.dq_ngg
         for n, v in self.arrays.items():
             if v.size:
                 setattr(z, n, v.ctypes.data)
@@ -330,7 +345,8 @@ class DeviceBlock:
 
         self.host_shape = host
         self.mx, self.my, self.mz, self.ngg = host.mx, host.my, host.mz, host.ngg
-        self.specs = HostBlock.specs(host.mx, host.my, host.mz, host.ngg, host.n_var, host.n_spec)
+        self.dq_ngg = host.dq_ngg
+        self.specs = HostBlock.specs(host.mx, host.my, host.mz, host.ngg, host.n_var, host.n_spec, host.dq_ngg)
         self.t = {}
         for n, (shape, dt) in self.specs.items():
             if n == "metric":
@@ -352,7 +368,7 @@ class DeviceBlock:
 
     def zone(self) -> Zone:
         z = Zone()
-        z.mx, z.my, z.mz, z.ngg, z.dq_ngg = self.mx, self.my, self.mz, self.ngg, 0
+        z.mx, z.my, z.mz, z.ngg, z.dq_ngg = self.mx, self.my, self.mz, self.ngg, self.dq_ngg
         for n, v in self.t.items():
             if v.numel():
                 setattr(z, n, v.data_ptr())
@@ -500,6 +516,24 @@ class Solver:
             check(lib().ostc_rk3_steps(self.ctx, n, res, dts, self._s()), "ostc_rk3_steps")
             return np.array(res).reshape(n, 4), np.array(dts)
         check(lib().ostc_rk3_steps(self.ctx, n, None, None, self._s()), "ostc_rk3_steps")
+        return None
+
+    # steady path (SteadySim.cuh:15-137)
+    def local_time_step(self):
+        check(lib().ostc_local_time_step(self.ctx, self._s()), "ostc_local_time_step")
+
+    def implicit_treatment(self):
+        check(lib().ostc_implicit_treatment(self.ctx, self._s()), "ostc_implicit_treatment")
+
+    def update_bv(self):
+        check(lib().ostc_update_bv(self.ctx, self._s()), "ostc_update_bv")
+
+    def steady_steps(self, n: int, history: bool = False):
+        if history:
+            res = (C.c_double * (4 * n))()
+            check(lib().ostc_steady_steps(self.ctx, n, res, self._s()), "ostc_steady_steps")
+            return np.array(res).reshape(n, 4)
+        check(lib().ostc_steady_steps(self.ctx, n, None, self._s()), "ostc_steady_steps")
         return None
 
     OP_FLUX, OP_SOURCE, OP_PROPERTIES, OP_UPDATE, OP_DT, OP_BC = range(6)
@@ -791,6 +825,32 @@ def case_multiblock(nx=(20, 17, 13), ny=(15, 19), mz=8, dx=1e-3, reconstruction=
     return c
 
 
+def make_steady(case: Case, implicit_method: int = 0, chem_src_method: Optional[int] = None,
+                dplur_inner_step: int = 3, cfl: Optional[float] = None) -> Case:
+    """The same blocks, faces and initial state advanced by the steady path
+    (steady_simulation, src/SteadySim.cuh:15-137): local time stepping,
+    explicit (implicit_method 0, with EPI / DA chemistry by chemSrcMethod)
+    or DPLUR (1). Blocks are re-allocated with the one-ghost dq of DPLUR."""
+    import copy
+
+    s = copy.deepcopy(case.scheme)
+    s.steady, s.implicit_method, s.dplur_inner_step = 1, implicit_method, dplur_inner_step
+    if chem_src_method is not None:
+        s.chemSrcMethod = chem_src_method
+    if cfl is not None:
+        s.cfl = cfl
+    blocks = []
+    for b in case.blocks:
+        nb = HostBlock.allocate(b.mx, b.my, b.mz, b.ngg, b.n_var, b.n_spec, full=True, dq_ngg=s.dq_ngg)
+        for n, v in b.arrays.items():
+            if n != "dq":
+                nb.arrays[n][...] = v
+        blocks.append(nb)
+    c = Case(case.name + "_steady%d" % implicit_method, s, case.mech, blocks, list(case.faces), case.steps)
+    c.interfaces = list(getattr(case, "interfaces", []) or [])
+    return c
+
+
 # ---------------------------------------------------------------------------
 # the reacting mixing layer (9-species H2-air)
 # ---------------------------------------------------------------------------
@@ -866,3 +926,47 @@ def case_mixing_layer(mx=256, my=256, mz=256, dx=1e-4, seed=2024, steps=200, ful
              bc_face(0, BC_OUTFLOW, 1, -1, ext, ng), bc_face(0, BC_OUTFLOW, 1, 1, ext, ng),
              bc_face(0, BC_PERIODIC, 2, -1, ext, ng), bc_face(0, BC_PERIODIC, 2, 1, ext, ng)]
     return Case("mixing_layer_h2air_%dx%dx%d" % (mx, my, mz), s, mech, [b], faces, steps)
+
+
+def case_premixed_box(mx=16, my=14, mz=8, dx=2e-3, T0=1400.0, seed=7, mech=None, chem_src_method=1,
+                      cfl=0.4) -> Case:
+    """A stoichiometric H2-air box (H2/O2/N2 mole 2/1/3.76) at T0 and 1 atm
+    with +-5 % temperature and 10 m/s velocity noise (numpy PCG64, seeded).
+    At dx = 2 mm the local time step (about 3e-7 s) makes the point-implicit
+    chemistry treatments (EPI, DA) differ visibly from the explicit one while
+    all of them stay bounded; at dx = 1 cm the chemistry is stiff enough that
+    the explicit steady update diverges. MUSCL + AUSM+, laminar, extrapolation
+    on every face."""
+    import chemdata
+
+    mech = mech or chemdata.h2_air_9sp()
+    s = Scheme(mix_model=MIX_FR, inviscid_scheme=3, reconstruction=2, limiter=0, viscous_order=2,
+               chemSrcMethod=chem_src_method, cfl=cfl)
+    ng = s.ngg
+    ns = mech.n_spec
+    b = HostBlock.allocate(mx, my, mz, ng, 5 + ns, ns, full=True)
+    x, y, z = grid_coordinates(mx, my, mz, ng + 1, dx, warp=0.0)
+    fill_metric(b, x, y, z)
+    names = mech.names
+    W = mech.tables["mw"]
+    X = np.zeros(ns)
+    X[names.index("H2")], X[names.index("O2")], X[names.index("N2")] = 2.0, 1.0, 3.76
+    Y = X * W / np.sum(X * W)
+    P = b.plane()
+    rng = np.random.default_rng(seed)
+    T = T0 * (1 + 0.05 * rng.uniform(-1, 1, P))
+    sv = b.arrays["sv"]
+    for l in range(ns):
+        sv[l] = Y[l]
+    mw_inv = float(np.sum(Y / W))
+    p0 = 101325.0
+    bv = b.arrays["bv"]
+    bv[0] = p0 / (R_U * mw_inv * T)
+    bv[1] = 10.0 * rng.uniform(-1, 1, P)
+    bv[2] = 10.0 * rng.uniform(-1, 1, P)
+    bv[3] = 10.0 * rng.uniform(-1, 1, P)
+    bv[4] = p0
+    bv[5] = T
+    ext = (mx, my, mz)
+    faces = [bc_face(0, BC_OUTFLOW, d, e, ext, ng) for d in range(3) for e in (-1, 1)]
+    return Case("premixed_h2air_%dx%dx%d" % (mx, my, mz), s, mech, [b], faces, 10)

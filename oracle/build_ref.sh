@@ -25,7 +25,7 @@ FLAGS=(-gencode arch=compute_100a,code=sm_100a -rdc=true -std=c++20 -O3 -Xcompil
        -DMAX_SPEC_NUMBER=20 -DMAX_REAC_NUMBER=50 -DGPU -DFMT_HEADER_ONLY
        -I"$HERE/ref_shim" -I"$REF/depends/include" -I"$SRC" -w)
 UNITS=(Thermo.cu Transport.cu FiniteRateChem.cu AusmP.cu HLLC.cu LaxFriedrichs.cu AWENO.cu Reconstruction.cu
-       InviscidScheme.cu Roe.cu FieldOperation.cu SST.cu TimeAdvanceFunc.cu Residual.cu Parameter.cpp
+       InviscidScheme.cu Roe.cu FieldOperation.cu SST.cu TimeAdvanceFunc.cu Residual.cu DPLUR.cu Parameter.cpp
        gxl_lib/MyString.cpp gxl_lib/Time.cpp Mesh.cpp Parallel.cpp Parallel.cu)
 # host-only units go through the host compiler: nvcc's front end rejects the
 # consteval format strings of header-only fmt 10

@@ -243,7 +243,7 @@ double arrhenius(double t, double A, double b, double Ea) {  // FiniteRateChem.c
 }
 
 void chemistry_omega(const ostc_param *P, double density, double t, const double *Y,
-                     double *omega, double *q1o, double *q2o) {  // FiniteRateChem.cu:7-63
+                     double *omega, double *q1o, double *q2o, double *odo = nullptr) {  // FiniteRateChem.cu:7-63
   const int ns = P->n_spec, nr = P->n_reac;
   double c[MAXS] = {0};
   for (int l = 0; l < ns; ++l) c[l] = density * Y[l] / P->mw[l] * 1e-3;
@@ -333,6 +333,7 @@ void chemistry_omega(const ostc_param *P, double density, double t, const double
     creation *= P->mw[i] * 1e+3;
     od *= P->mw[i] * 1e+3;
     omega[i] = creation - od;
+    if (odo) odo[i] = od;
   }
   if (q1o) for (int i = 0; i < nr; ++i) q1o[i] = q1[i];
   if (q2o) for (int i = 0; i < nr; ++i) q2o[i] = q2[i];
@@ -1587,6 +1588,333 @@ void compute_rhs_zone(const ostc_param *P, Z &Zn) {
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// steady path: SteadySim.cuh:15-137 with its implicit treatments
+// ---------------------------------------------------------------------------
+// compute_chem_src_jacobian (FiniteRateChem.cu:196-216), row-major m*ns+n
+void chem_jacobian(const ostc_param *P, double rho, const double *Y, const double *q1, const double *q2,
+                   double *J) {
+  const int ns = P->n_spec, nr = P->n_reac;
+  for (int m = 0; m < ns; ++m)
+    for (int n = 0; n < ns; ++n) {
+      double zz = 0;
+      if (Y[n] > 1e-25) {
+        for (int r = 0; r < nr; ++r)
+          zz += (P->stoi_b[r * ns + m] - P->stoi_f[r * ns + m]) *
+                (P->stoi_f[r * ns + n] * q1[r] - P->stoi_b[r * ns + n] * q2[r]);
+        zz /= rho * Y[n];
+      }
+      J[m * ns + n] = P->mw[m] * zz * 1e+3;
+    }
+}
+
+// solve_chem_system (FiniteRateChem.cu:324-419): column-pivoted LU, then solve
+void lu_factor(double *A, int *ipiv, int dim) {
+  for (int n = 0; n < dim; ++n) {
+    int ik = n;
+    for (int m = n; m < dim; ++m) {
+      for (int t = 0; t < n; ++t) A[m * dim + n] -= A[m * dim + t] * A[t * dim + n];
+      if (std::abs(A[m * dim + n]) > std::abs(A[ik * dim + n])) ik = m;
+    }
+    ipiv[n] = ik;
+    if (ik != n)
+      for (int t = 0; t < dim; ++t) std::swap(A[ik * dim + t], A[n * dim + t]);
+    for (int p = n + 1; p < dim; ++p)
+      for (int t = 0; t < n; ++t) A[n * dim + p] -= A[n * dim + t] * A[t * dim + p];
+    for (int m = n + 1; m < dim; ++m) A[m * dim + n] /= A[n * dim + n];
+  }
+}
+void lu_apply(const double *A, const int *ipiv, double *b, int dim) {
+  for (int m = 0; m < dim; ++m)
+    if (ipiv[m] != m) std::swap(b[ipiv[m]], b[m]);
+  for (int m = 1; m < dim; ++m)
+    for (int t = 0; t < m; ++t) b[m] -= A[m * dim + t] * b[t];
+  b[dim - 1] /= A[dim * dim - 1];
+  for (int m = dim - 2; m >= 0; --m) {
+    for (int t = m + 1; t < dim; ++t) b[m] -= A[m * dim + t] * b[t];
+    b[m] /= A[m * dim + m];
+  }
+}
+
+// local_time_step (TimeAdvanceFunc.cuh:50-100): dt_local and the inviscid
+// spectral radii (3 per interior point)
+void local_time_step_zone(const ostc_param *P, Z &Zn, std::vector<double> &isr) {
+  const int dim = Zn.mz == 1 ? 2 : 3;
+  isr.assign(3 * (size_t)Zn.mx * Zn.my * Zn.mz, 0.0);
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < Zn.mz; ++k)
+    for (int j = 0; j < Zn.my; ++j)
+      for (int i = 0; i < Zn.mx; ++i) {
+        const double *m = Zn.metric.at(i, j, k);
+        const double gx = std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+        const double ge = std::sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
+        const double gz = std::sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
+        const double u = Zn.bv(i, j, k, 1), v = Zn.bv(i, j, k, 2), w = Zn.bv(i, j, k, 3);
+        const double U = u * m[0] + v * m[1] + w * m[2];
+        const double V = u * m[3] + v * m[4] + w * m[5];
+        const double W = u * m[6] + v * m[7] + w * m[8];
+        const double a = Zn.a(i, j, k);
+        const size_t q = 3 * (((size_t)k * Zn.my + j) * Zn.mx + i);
+        isr[q] = std::abs(U) + a * gx;
+        isr[q + 1] = std::abs(V) + a * ge;
+        isr[q + 2] = dim == 3 ? std::abs(W) + a * gz : 0.0;
+        const double sri = isr[q] + isr[q + 1] + isr[q + 2];
+        double gamma = gamma_air;
+        if (P->mix_model != OSTC_MIX_AIR) gamma = Zn.gam(i, j, k);
+        const double c1 = std::max(gamma, 4.0 / 3.0) / Zn.bv(i, j, k, 0);
+        const double c2 = Zn.mul(i, j, k) / P->Pr;
+        double srv = gx * gx + ge * ge;
+        if (dim == 3) srv += gz * gz;
+        srv *= c1 * c2;
+        Zn.dt_local(i, j, k) = P->cfl / (sri + srv);
+      }
+}
+
+// rates, omega_d and (optionally) the full Jacobian at one cell
+void cell_chemistry(const ostc_param *P, Z &Zn, int i, int j, int k, double *Y, double &rho, double *J,
+                    double *od) {
+  const int ns = P->n_spec;
+  rho = Zn.bv(i, j, k, 0);
+  for (int l = 0; l < ns; ++l) Y[l] = Zn.sv(i, j, k, l);
+  double om[MAXS], q1[MAXR], q2[MAXR];
+  chemistry_omega(P, rho, Zn.bv(i, j, k, 5), Y, om, q1, q2, od);
+  if (J) chem_jacobian(P, rho, Y, q1, q2, J);
+}
+
+// EPI / DA of the explicit steady step (FiniteRateChem.cu:234-256, 421-432)
+void chem_implicit_zone(const ostc_param *P, Z &Zn) {
+  const int ns = P->n_spec;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < Zn.mz; ++k)
+    for (int j = 0; j < Zn.my; ++j)
+      for (int i = 0; i < Zn.mx; ++i) {
+        double Y[MAXS], J[MAXS * MAXS], od[MAXS], rho;
+        const double dt = Zn.dt_local(i, j, k);
+        if (P->chemSrcMethod == 1) {
+          cell_chemistry(P, Zn, i, j, k, Y, rho, J, od);
+          for (int m = 0; m < ns; ++m)
+            for (int n = 0; n < ns; ++n) J[m * ns + n] = m == n ? 1.0 - dt * J[m * ns + n] : -dt * J[m * ns + n];
+          double b[MAXS];
+          int ipiv[MAXS];
+          for (int l = 0; l < ns; ++l) b[l] = Zn.dq(i, j, k, 5 + l);
+          lu_factor(J, ipiv, ns);
+          lu_apply(J, ipiv, b, ns);
+          for (int l = 0; l < ns; ++l) Zn.dq(i, j, k, 5 + l) = b[l];
+        } else if (P->chemSrcMethod == 2) {
+          cell_chemistry(P, Zn, i, j, k, Y, rho, nullptr, od);
+          for (int l = 0; l < ns; ++l) {
+            const double jd = Y[l] > 1e-25 ? -od[l] / (Y[l] * rho) : 0.0;
+            Zn.dq(i, j, k, 5 + l) /= 1 - dt * jd;
+          }
+        }
+      }
+}
+
+// update_bv (FieldOperation.cuh:221-296)
+void update_bv_zone(const ostc_param *P, Z &Zn) {
+  const int ns = P->n_spec;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < Zn.mz; ++k)
+    for (int j = 0; j < Zn.my; ++j)
+      for (int i = 0; i < Zn.mx; ++i) {
+        const double rho_n = Zn.bv(i, j, k, 0);
+        const double u_n = Zn.bv(i, j, k, 1), v_n = Zn.bv(i, j, k, 2), w_n = Zn.bv(i, j, k, 3);
+        double E = 0.5 * (u_n * u_n + v_n * v_n + w_n * w_n);
+        if (P->mix_model != OSTC_MIX_AIR) {
+          double h[MAXS];
+          enthalpy(P, Zn.bv(i, j, k, 5), h);
+          for (int l = 0; l < ns; ++l) E += h[l] * Zn.sv(i, j, k, l);
+          E *= rho_n;
+          E -= Zn.bv(i, j, k, 4);
+        } else {
+          E *= rho_n;
+          E += Zn.bv(i, j, k, 4) / (gamma_air - 1);
+        }
+        const double dtj = Zn.dt_local(i, j, k) / Zn.jac(i, j, k);
+        Zn.bv(i, j, k, 0) += Zn.dq(i, j, k, 0) * dtj;
+        const double ri = 1.0 / Zn.bv(i, j, k, 0);
+        Zn.bv(i, j, k, 1) = ri * (rho_n * Zn.bv(i, j, k, 1) + Zn.dq(i, j, k, 1) * dtj);
+        Zn.bv(i, j, k, 2) = ri * (rho_n * Zn.bv(i, j, k, 2) + Zn.dq(i, j, k, 2) * dtj);
+        if (Zn.mz == 1)
+          Zn.bv(i, j, k, 3) = 0;
+        else
+          Zn.bv(i, j, k, 3) = ri * (rho_n * Zn.bv(i, j, k, 3) + Zn.dq(i, j, k, 3) * dtj);
+        const double Et = E + Zn.dq(i, j, k, 4) * dtj;
+        for (int l = 0; l < P->n_scalar; ++l)
+          Zn.sv(i, j, k, l) = ri * (rho_n * Zn.sv(i, j, k, l) + Zn.dq(i, j, k, 5 + l) * dtj);
+        const double V2 = Zn.bv(i, j, k, 1) * Zn.bv(i, j, k, 1) + Zn.bv(i, j, k, 2) * Zn.bv(i, j, k, 2) +
+                          Zn.bv(i, j, k, 3) * Zn.bv(i, j, k, 3);
+        if (P->mix_model != OSTC_MIX_AIR) {
+          temperature_and_pressure(P, Zn, i, j, k, Et);
+        } else {
+          Zn.bv(i, j, k, 4) = (gamma_air - 1) * (Et - 0.5 * Zn.bv(i, j, k, 0) * V2);
+          Zn.bv(i, j, k, 5) = Zn.bv(i, j, k, 4) * mw_air * ri / R_u;
+        }
+        Zn.vel(i, j, k) = std::sqrt(V2);
+      }
+}
+
+// compute_jacobian_times_dq (DPLUR.cuh:81-140) at (i,j,k), direction dir
+void jacobian_times_dq(const ostc_param *P, Z &Zn, const View &dqv, int i, int j, int k, int dir, double lam,
+                       double *out) {
+  const int ns = P->n_spec;
+  const double *m = Zn.metric.at(i, j, k);
+  const double kx = m[3 * dir], ky = m[3 * dir + 1], kz = m[3 * dir + 2];
+  const double u = Zn.bv(i, j, k, 1), v = Zn.bv(i, j, k, 2), w = Zn.bv(i, j, k, 3);
+  const double U = kx * u + ky * v + kz * w;
+  const double lmd1 = U + lam;
+  const double e = 0.5 * Zn.vel(i, j, k) * Zn.vel(i, j, k);
+  double gamma = gamma_air, b3 = 0, b4 = 0, h = 0;
+  if (P->mix_model == OSTC_MIX_AIR) {
+    h = gamma / (gamma - 1) * Zn.bv(i, j, k, 4) / Zn.bv(i, j, k, 0) + e;
+  } else {
+    const double t = Zn.bv(i, j, k, 5);
+    double hk[MAXS];
+    enthalpy(P, t, hk);
+    gamma = Zn.gam(i, j, k);
+    for (int l = 0; l < ns; ++l) {
+      b3 += R_u * t / P->mw[l] * dqv(i, j, k, 5 + l);
+      b4 += hk[l] * dqv(i, j, k, 5 + l);
+      h += Zn.sv(i, j, k, l) * hk[l];
+    }
+    b3 *= gamma;
+    b4 *= gamma - 1;
+    h += e;
+  }
+  const double b1 = kx * dqv(i, j, k, 1) + ky * dqv(i, j, k, 2) + kz * dqv(i, j, k, 3) - U * dqv(i, j, k, 0);
+  const double b2 = (gamma - 1) * (e * dqv(i, j, k, 0) - u * dqv(i, j, k, 1) - v * dqv(i, j, k, 2) -
+                                   w * dqv(i, j, k, 3) + dqv(i, j, k, 4));
+  out[0] = b1 + lmd1 * dqv(i, j, k, 0);
+  out[1] = u * b1 + kx * b2 + lmd1 * dqv(i, j, k, 1) + kx * (b3 - b4);
+  out[2] = v * b1 + ky * b2 + lmd1 * dqv(i, j, k, 2) + ky * (b3 - b4);
+  out[3] = w * b1 + kz * b2 + lmd1 * dqv(i, j, k, 3) + kz * (b3 - b4);
+  out[4] = h * b1 + U * b2 + lmd1 * dqv(i, j, k, 4) + U * (b3 - b4);
+  for (int l = 0; l < P->n_scalar; ++l) out[5 + l] = lmd1 * dqv(i, j, k, 5 + l) + Zn.sv(i, j, k, l) * b1;
+}
+
+// DPLUR (DPLUR.cuh:14-314, DPLUR.cu:5-52) on one block
+void dplur_zone(const ostc_config *c, const ostc_param *P, Z &Zn, const std::vector<double> &isr,
+                const ostc_bc_face *f, int n_faces, int block) {
+  const int nv = P->n_var, ns = P->n_spec;
+  const int g = Zn.z->dq_ngg;
+  const size_t nq = (size_t)(Zn.mx + 2 * g) * (Zn.my + 2 * g) * (Zn.mz + 2 * g) * nv;
+  std::vector<double> dq0v(nq, 0.0), dqkv(nq, 0.0);
+  View dq0(dq0v.data(), Zn.mx, Zn.my, Zn.mz, g), dqk(dqkv.data(), Zn.mx, Zn.my, Zn.mz, g);
+  const bool chem = P->mix_model == OSTC_MIX_FR && P->n_reac > 0;
+  auto R = [&](int i, int j, int k, int d) { return isr[3 * (((size_t)k * Zn.my + j) * Zn.mx + i) + d]; };
+  // compute_DQ_0
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < Zn.mz; ++k)
+    for (int j = 0; j < Zn.my; ++j)
+      for (int i = 0; i < Zn.mx; ++i) {
+        const double dt = Zn.dt_local(i, j, k);
+        for (int l = 0; l < nv; ++l) Zn.dq(i, j, k, l) *= dt;
+        const double diag = 1 + dt * (R(i, j, k, 0) + R(i, j, k, 1) + R(i, j, k, 2));
+        for (int l = 0; l < 5; ++l) Zn.dq(i, j, k, l) /= diag;
+        if (ns > 0) {
+          if (chem && P->chemSrcMethod == 1) {
+            double Y[MAXS], J[MAXS * MAXS], od[MAXS], rho, b[MAXS];
+            int ipiv[MAXS];
+            cell_chemistry(P, Zn, i, j, k, Y, rho, J, od);
+            for (int m = 0; m < ns; ++m)
+              for (int n = 0; n < ns; ++n) J[m * ns + n] = m == n ? diag - dt * J[m * ns + n] : -dt * J[m * ns + n];
+            for (int l = 0; l < ns; ++l) b[l] = Zn.dq(i, j, k, 5 + l);
+            lu_factor(J, ipiv, ns);
+            lu_apply(J, ipiv, b, ns);
+            for (int l = 0; l < ns; ++l) Zn.dq(i, j, k, 5 + l) = b[l];
+          } else if (chem && P->chemSrcMethod == 2) {
+            double Y[MAXS], od[MAXS], rho;
+            cell_chemistry(P, Zn, i, j, k, Y, rho, nullptr, od);
+            for (int l = 0; l < ns; ++l) {
+              const double jd = Y[l] > 1e-25 ? -od[l] / (Y[l] * rho) : 0.0;
+              Zn.dq(i, j, k, 5 + l) /= diag - dt * jd;
+            }
+          } else {
+            for (int l = 5; l < nv; ++l) Zn.dq(i, j, k, l) /= diag;
+          }
+        }
+        for (int l = 0; l < nv; ++l) dq0(i, j, k, l) = Zn.dq(i, j, k, l);
+      }
+  for (int it = 0; it < c->DPLUR_inner_step; ++it) {
+    // set_wall_dq_to_0 (DPLUR.cu:33-52)
+    for (int q = 0; q < n_faces; ++q) {
+      if (f[q].block != block || f[q].type_label != OSTC_BC_WALL) continue;
+      for (int k = f[q].range_start[2]; k <= f[q].range_end[2]; ++k)
+        for (int j = f[q].range_start[1]; j <= f[q].range_end[1]; ++j)
+          for (int i = f[q].range_start[0]; i <= f[q].range_end[0]; ++i) {
+            if (i < -g || j < -g || k < -g || i >= Zn.mx + g || j >= Zn.my + g || k >= Zn.mz + g) continue;
+            for (int l = 0; l < nv; ++l) Zn.dq(i, j, k, l) = 0;
+          }
+    }
+    // DPLUR_inner_iteration (DPLUR.cuh:161-280)
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Zn.mz; ++k)
+      for (int j = 0; j < Zn.my; ++j)
+        for (int i = 0; i < Zn.mx; ++i) {
+          double tot[MAXS + 5] = {0}, cj[MAXS + 5];
+          auto add = [&](double s) {
+            for (int l = 0; l < nv; ++l) tot[l] += s * cj[l];
+          };
+          if (i > 0) { jacobian_times_dq(P, Zn, Zn.dq, i - 1, j, k, 0, R(i - 1, j, k, 0), cj); add(0.5); }
+          if (j > 0) { jacobian_times_dq(P, Zn, Zn.dq, i, j - 1, k, 1, R(i, j - 1, k, 1), cj); add(0.5); }
+          if (k > 0) { jacobian_times_dq(P, Zn, Zn.dq, i, j, k - 1, 2, R(i, j, k - 1, 2), cj); add(0.5); }
+          if (i != Zn.mx - 1) {
+            jacobian_times_dq(P, Zn, Zn.dq, i + 1, j, k, 0, -R(i + 1, j, k, 0), cj);
+            for (int l = 0; l < nv; ++l) tot[l] -= 0.5 * cj[l];
+          }
+          if (j != Zn.my - 1) {
+            jacobian_times_dq(P, Zn, Zn.dq, i, j + 1, k, 1, -R(i, j + 1, k, 1), cj);
+            for (int l = 0; l < nv; ++l) tot[l] -= 0.5 * cj[l];
+          }
+          if (k != Zn.mz - 1) {
+            jacobian_times_dq(P, Zn, Zn.dq, i, j, k + 1, 2, -R(i, j, k + 1, 2), cj);
+            for (int l = 0; l < nv; ++l) tot[l] -= 0.5 * cj[l];
+          }
+          const double dt = Zn.dt_local(i, j, k);
+          const double diag = 1 + dt * (R(i, j, k, 0) + R(i, j, k, 1) + R(i, j, k, 2));
+          for (int l = 0; l < 5; ++l) dqk(i, j, k, l) = dq0(i, j, k, l) + dt * tot[l] / diag;
+          if (ns > 0) {
+            if (chem && P->chemSrcMethod == 1) {
+              double Y[MAXS], J[MAXS * MAXS], od[MAXS], rho, b[MAXS];
+              int ipiv[MAXS];
+              cell_chemistry(P, Zn, i, j, k, Y, rho, J, od);
+              for (int m = 0; m < ns; ++m)
+                for (int n = 0; n < ns; ++n)
+                  J[m * ns + n] = m == n ? diag - dt * J[m * ns + n] : -dt * J[m * ns + n];
+              for (int l = 0; l < ns; ++l) b[l] = tot[5 + l] * dt;
+              lu_factor(J, ipiv, ns);
+              lu_apply(J, ipiv, b, ns);
+              for (int l = 0; l < ns; ++l) dqk(i, j, k, 5 + l) = dq0(i, j, k, 5 + l) + b[l];
+            } else if (chem && P->chemSrcMethod == 2) {
+              double Y[MAXS], od[MAXS], rho;
+              cell_chemistry(P, Zn, i, j, k, Y, rho, nullptr, od);
+              for (int l = 0; l < ns; ++l) {
+                const double jd = Y[l] > 1e-25 ? -od[l] / (Y[l] * rho) : 0.0;
+                dqk(i, j, k, 5 + l) = dq0(i, j, k, 5 + l) + dt * tot[5 + l] / (diag - dt * jd);
+              }
+            } else {
+              for (int l = 5; l < nv; ++l) dqk(i, j, k, l) = dq0(i, j, k, l) + dt * tot[l] / diag;
+            }
+          }
+        }
+    // dq <- dqk over the interior (the ghost layer of dq is never read)
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Zn.mz; ++k)
+      for (int j = 0; j < Zn.my; ++j)
+        for (int i = 0; i < Zn.mx; ++i)
+          for (int l = 0; l < nv; ++l) Zn.dq(i, j, k, l) = dqk(i, j, k, l);
+  }
+  // convert_dq_back_to_dqDt (DPLUR.cu:5-17)
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < Zn.mz; ++k)
+    for (int j = 0; j < Zn.my; ++j)
+      for (int i = 0; i < Zn.mx; ++i) {
+        const double dt = Zn.dt_local(i, j, k);
+        for (int l = 0; l < nv; ++l) Zn.dq(i, j, k, l) /= dt;
+      }
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1816,6 +2144,72 @@ int oracle_rk3_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zones
     }
     if (dt_hist) dt_hist[step] = dt;
     if (res_hist) {  // compute_square_of_dbv + reductions (Residual.cuh:57-111)
+      double res[4] = {0, 0, 0, 0};
+      for (int b = 0; b < n_zones; ++b) {
+        Z Zn(&zones[b]);
+        const long n = (long)Zn.mx * Zn.my * Zn.mz;
+        long q = 0;
+        for (int k = 0; k < Zn.mz; ++k)
+          for (int j = 0; j < Zn.my; ++j)
+            for (int i = 0; i < Zn.mx; ++i, ++q) {
+              const double d0 = Zn.bv(i, j, k, 0) - last[b][q];
+              const double d1 = Zn.vel(i, j, k) - last[b][q + n];
+              const double d2 = Zn.bv(i, j, k, 4) - last[b][q + 2 * n];
+              const double d3 = Zn.bv(i, j, k, 5) - last[b][q + 3 * n];
+              res[0] += d0 * d0;
+              res[1] += d1 * d1;
+              res[2] += d2 * d2;
+              res[3] += d3 * d3;
+            }
+      }
+      for (int l = 0; l < 4; ++l) res_hist[4 * step + l] = std::sqrt(res[l] / (double)n_total);
+    }
+  }
+  return 0;
+}
+
+
+int oracle_steady_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zones, int n_zones,
+                        const ostc_bc_face *f, int n_faces, int n_steps, double *res_hist) {
+  // the loop body of steady_simulation (SteadySim.cuh:51-126)
+  if (P->inviscid_type == 1) return OSTC_ERR_UNSUPPORTED;  // quirk A6
+  for (int step = 0; step < n_steps; ++step) {
+    long n_total = 0;
+    std::vector<std::vector<double>> last(n_zones);
+    if (res_hist)
+      for (int b = 0; b < n_zones; ++b) {  // store_last_step (TimeAdvanceFunc.cu:6-17)
+        Z Zn(&zones[b]);
+        const long n = (long)Zn.mx * Zn.my * Zn.mz;
+        n_total += n;
+        last[b].resize(4 * n);
+        long q = 0;
+        for (int k = 0; k < Zn.mz; ++k)
+          for (int j = 0; j < Zn.my; ++j)
+            for (int i = 0; i < Zn.mx; ++i, ++q) {
+              last[b][q] = Zn.bv(i, j, k, 0);
+              last[b][q + n] = Zn.vel(i, j, k);
+              last[b][q + 2 * n] = Zn.bv(i, j, k, 4);
+              last[b][q + 3 * n] = Zn.bv(i, j, k, 5);
+            }
+      }
+    for (int b = 0; b < n_zones; ++b) {
+      int st = oracle_compute_rhs(P, &zones[b]);
+      if (st) return st;
+      Z Zn(&zones[b]);
+      std::vector<double> isr;
+      local_time_step_zone(P, Zn, isr);
+      if (c->implicit_method == 1) {
+        dplur_zone(c, P, Zn, isr, f, n_faces, b);
+      } else if (P->mix_model == OSTC_MIX_FR && P->n_reac > 0 && P->chemSrcMethod != 0) {
+        chem_implicit_zone(P, Zn);
+      }
+      update_bv_zone(P, Zn);
+    }
+    int st = oracle_apply_boundary_conditions(P, zones, n_zones, f, n_faces, 0);
+    if (st) return st;
+    oracle_data_communication(P, zones, n_zones, 0);
+    for (int b = 0; b < n_zones; ++b) oracle_update_physical_properties(P, &zones[b]);
+    if (res_hist) {
       double res[4] = {0, 0, 0, 0};
       for (int b = 0; b < n_zones; ++b) {
         Z Zn(&zones[b]);

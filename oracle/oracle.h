@@ -44,6 +44,11 @@ int oracle_initialize(const ostc_config *c, const ostc_param *p, ostc_zone *zone
 int oracle_rk3_steps(const ostc_config *c, const ostc_param *p, ostc_zone *zones, int n_zones,
                      const ostc_bc_face *f, int n_faces, int n_steps,
                      double *res_hist, double *dt_hist);
+/* n steady iterations (SteadySim.cuh:51-126): RHS, local dt, EPI/DA or
+ * DPLUR (c->implicit_method, c->DPLUR_inner_step), update_bv, BCs and
+ * interfaces without cv, properties; res_hist: 4 per step or NULL */
+int oracle_steady_steps(const ostc_config *c, const ostc_param *p, ostc_zone *zones, int n_zones,
+                        const ostc_bc_face *f, int n_faces, int n_steps, double *res_hist);
 /* 1-to-1 interfaces used by oracle_initialize / oracle_rk3_steps (copied) */
 int oracle_set_interfaces(const ostc_interface *f, int n);
 /* data_communication over the registered interfaces (DataCommunication.cuh:27-110) */

@@ -34,11 +34,18 @@
 #include "IOManager.h"
 #include "RK.cuh"
 #include "Residual.cuh"
+#include "DPLUR.cuh"
+#include "FiniteRateChem.cuh"
 #include "SchemeSelector.cuh"
 #include "SourceTerm.cuh"
 #include "../include/ostc.h"
 
 using namespace cfd;
+
+namespace cfd {
+// defined in DPLUR.cu without a header declaration
+__global__ void set_dq_to_0(const DParameter *param, DZone *zone, integer i_face);
+}  // namespace cfd
 
 namespace {
 
@@ -178,9 +185,15 @@ void build_zone(RefCtx &c, const ostc_zone *z, const ostc_param *p) {
         h.chem_src_jac.allocate_memory(mx, my, mz, p->n_spec, 0);
     }
   }
-  h.dq.allocate_memory(mx, my, mz, p->n_var, 0);
-  h.inv_spectr_rad.allocate_memory(mx, my, mz, 0);
-  h.visc_spectr_rad.allocate_memory(mx, my, mz, 0);
+  // DPLUR: one ghost layer on dq, dq0, dqk and the spectral radii (Field.cu:209-221)
+  const bool dplur = c.cfg.steady && c.cfg.implicit_method == 1;
+  h.dq.allocate_memory(mx, my, mz, p->n_var, dplur ? 1 : 0);
+  h.inv_spectr_rad.allocate_memory(mx, my, mz, dplur ? 1 : 0);
+  h.visc_spectr_rad.allocate_memory(mx, my, mz, dplur ? 1 : 0);
+  if (dplur) {
+    h.dq0.allocate_memory(mx, my, mz, p->n_var, 1);
+    h.dqk.allocate_memory(mx, my, mz, p->n_var, 1);
+  }
   h.dt_local.allocate_memory(mx, my, mz, 0);
   h.unphysical.allocate_memory(mx, my, mz, 0);
   h.qn.allocate_memory(mx, my, mz, p->n_var, g);
@@ -368,6 +381,78 @@ int steps(RefMulti &m, int n, double *res_hist, double *dt_hist) {
       for (int l = 0; l < 4; ++l) res_hist[4 * s + l] = std::sqrt(acc[l] / n_total);
     }
     if (dt_hist) dt_hist[s] = dt;
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  return e == cudaSuccess ? 0 : 2;
+}
+
+
+// implicit_treatment (ImplicitTreatmentHPP.cuh:8-52) for one block; DPLUR's
+// host loop (DPLUR.cuh:283-312) with set_wall_dq_to_0 (DPLUR.cu:33-52) over
+// this block's wall faces
+template <MixtureModel mix>
+void implicit_treatment_block(RefMulti &m, RefCtx &c) {
+  dim3 tpb{8, 8, 4};
+  dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
+  if (m.cfg.implicit_method == 0) {
+    if constexpr (mix == MixtureModel::FR) {
+      if (c.h_param.n_reac > 0 && c.h_param.chemSrcMethod == 1) EPI<<<bpg, tpb>>>(c.d_zone, c.n_spec);
+      if (c.h_param.n_reac > 0 && c.h_param.chemSrcMethod == 2) DA<<<bpg, tpb>>>(c.d_zone, c.n_spec);
+    }
+    return;
+  }
+  compute_DQ_0<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param);
+  const size_t mem = c.h.dq.size() * c.n_var * sizeof(real);
+  cudaMemcpy(c.h.dq0.data(), c.h.dq.data(), mem, cudaMemcpyDeviceToDevice);
+  for (int it = 0; it < m.cfg.DPLUR_inner_step; ++it) {
+    for (size_t q = 0; q < c.faces.size(); ++q) {
+      if (c.faces[q].type_label != 2) continue;
+      const Boundary &hf = c.faces[q];
+      uint tp[3], bp[3];
+      for (int j = 0; j < 3; ++j) {
+        const int n = hf.range_end[j] - hf.range_start[j] + 1;
+        tp[j] = n <= (2 * c.ngg + 1) ? 1 : 16;
+        bp[j] = (n - 1) / tp[j] + 1;
+      }
+      set_dq_to_0<<<dim3{bp[0], bp[1], bp[2]}, dim3{tp[0], tp[1], tp[2]}>>>(c.d_param, c.d_zone, (integer)q);
+    }
+    DPLUR_inner_iteration<mix, Laminar><<<bpg, tpb>>>(c.d_param, c.d_zone);
+    cudaMemcpy(c.h.dq.data(), c.h.dqk.data(), mem, cudaMemcpyDeviceToDevice);
+  }
+  convert_dq_back_to_dqDt<<<bpg, tpb>>>(c.d_zone, c.d_param);
+}
+
+template <MixtureModel mix>
+int steady_steps(RefMulti &m, int n, double *res_hist) {
+  // the loop body of steady_simulation (SteadySim.cuh:51-126), all blocks
+  dim3 tpb{8, 8, 4};
+  auto bpg = [&](RefCtx *c, int e) {
+    return dim3{(unsigned)((c->mx + e) / tpb.x + 1), (unsigned)((c->my + e) / tpb.y + 1),
+                (unsigned)((c->mz + e) / tpb.z + 1)};
+  };
+  double n_total = 0;
+  for (RefCtx *c : m.blk) n_total += (double)c->mx * c->my * c->mz;
+  for (int s = 0; s < n; ++s) {
+    if (res_hist)
+      for (RefCtx *c : m.blk) store_last_step<<<bpg(c, -1), tpb>>>(c->d_zone);
+    for (RefCtx *c : m.blk) {
+      rhs<mix>(*c);
+      local_time_step<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
+      implicit_treatment_block<mix>(m, *c);
+      update_bv<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
+      apply_bcs<mix, false>(*c);
+    }
+    communicate<mix, false>(m);
+    for (RefCtx *c : m.blk) update_physical_properties<mix><<<bpg(c, 1), tpb>>>(c->d_zone, c->d_param);
+    if (res_hist) {
+      double acc[4] = {0, 0, 0, 0};
+      for (RefCtx *c : m.blk) {
+        double r[4];
+        block_residual(*c, r);
+        for (int l = 0; l < 4; ++l) acc[l] += r[l];
+      }
+      for (int l = 0; l < 4; ++l) res_hist[4 * s + l] = std::sqrt(acc[l] / n_total);
+    }
   }
   cudaError_t e = cudaDeviceSynchronize();
   return e == cudaSuccess ? 0 : 2;
@@ -571,6 +656,13 @@ int ref_steps(void *h, int n, double *res_hist, double *dt_hist) {
   auto *m = (RefMulti *)h;
   return m->mix == OSTC_MIX_AIR ? steps<MixtureModel::Air>(*m, n, res_hist, dt_hist)
                                 : steps<MixtureModel::FR>(*m, n, res_hist, dt_hist);
+}
+
+int ref_steady_steps(void *h, int n, double *res_hist) {
+  auto *m = (RefMulti *)h;
+  if (!m->cfg.steady) return 1;
+  return m->mix == OSTC_MIX_AIR ? steady_steps<MixtureModel::Air>(*m, n, res_hist)
+                                : steady_steps<MixtureModel::FR>(*m, n, res_hist);
 }
 
 // device time of n steps (CUDA events around the loop, as bench.py does for ours)

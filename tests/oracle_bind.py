@@ -36,6 +36,8 @@ def oracle():
             "oracle_transport": ([P, C.c_double, C.c_double, C.c_double, d, d, d, d], C.c_int),
             "oracle_set_threads": ([C.c_int], None),
             "oracle_set_interfaces": ([C.POINTER(ostc.IfaceC), C.c_int], C.c_int),
+            "oracle_steady_steps": ([C.POINTER(ostc.Config), C.POINTER(ostc.Param), C.POINTER(ostc.Zone), C.c_int,
+                                     C.POINTER(ostc.BcFaceC), C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
             "oracle_get_threads": ([], C.c_int),
         }
         for n, (a, r) in sig.items():
@@ -95,6 +97,14 @@ class OracleRun:
         self._ck(oracle().oracle_rk3_steps(C.byref(self.config), C.byref(self.param), self.zones, len(self.blocks),
                                            self.faces, self.nf, n, res, dts), "oracle_rk3_steps")
         return np.array(res).reshape(n, 4), np.array(dts)
+
+
+    def steady_steps(self, n):
+        self._ifaces()
+        res = (C.c_double * (4 * n))()
+        self._ck(oracle().oracle_steady_steps(C.byref(self.config), C.byref(self.param), self.zones, len(self.blocks),
+                                              self.faces, self.nf, n, res), "oracle_steady_steps")
+        return np.array(res).reshape(n, 4)
 
 
 def rhs_errors(got, ref, scale, cancel=1e-2):

@@ -38,6 +38,8 @@ def ref():
             getattr(L, n).restype = C.c_int
         L.ref_steps.argtypes = [vp, C.c_int, d, d]
         L.ref_steps.restype = C.c_int
+        L.ref_steady_steps.argtypes = [vp, C.c_int, d]
+        L.ref_steady_steps.restype = C.c_int
         L.ref_time_steps.argtypes = [vp, C.c_int]
         L.ref_time_steps.restype = C.c_double
         L.ref_download.argtypes = [vp, C.c_char_p, d]
@@ -79,6 +81,11 @@ class RefCudaRun:
         assert ref().ref_steps(self.h, n, res, dts) == 0
         return np.array(res).reshape(n, 4), np.array(dts)
 
+    def steady_steps(self, n):
+        res = (C.c_double * (4 * n))()
+        assert ref().ref_steady_steps(self.h, n, res) == 0
+        return np.array(res).reshape(n, 4)
+
     def time_steps(self, n):
         return ref().ref_time_steps(self.h, n)
 
@@ -86,7 +93,8 @@ class RefCudaRun:
         b = self.blocks[block]
         P = ostc.plane_shape(b.mx, b.my, b.mz, b.ngg)
         I = ostc.plane_shape(b.mx, b.my, b.mz, 0)
-        shapes = {"bv": (6,) + P, "sv": (b.n_spec,) + P, "cv": (b.n_var,) + P, "dq": (b.n_var,) + I, "mul": P,
+        Q = ostc.plane_shape(b.mx, b.my, b.mz, getattr(b, "dq_ngg", 0))
+        shapes = {"bv": (6,) + P, "sv": (b.n_spec,) + P, "cv": (b.n_var,) + P, "dq": (b.n_var,) + Q, "mul": P,
                   "thermal_conductivity": P, "vel": P, "acoustic_speed": P, "rho_D": (b.n_spec,) + P}
         out = np.zeros(shapes[name])
         assert ref().ref_download_block(self.h, block, name.encode(), out.ctypes.data_as(C.POINTER(C.c_double))) == 0
