@@ -1,5 +1,5 @@
 /*
- * oracle.h — CPU oracle for the OpenSTC-dev RHS and RK3 time-advance path.
+ * oracle.h — CPU oracle for the OpenSTC-dev RHS, RK3 and steady time-advance paths.
  *
  * TEST INFRASTRUCTURE ONLY. This is a plain FP64 restatement of the
  * reference's algorithm on HOST arrays laid out exactly like the device
@@ -8,10 +8,13 @@
  * check and bench.py's cpu_baseline / reference legs may load it; the
  * product library never links or calls it.
  *
- * Parity: this port is pinned against the reference's own physics functions
- * compiled as host code (oracle/_ref, built by oracle/build_ref.sh from the
- * reference sources) and against golden vectors generated from them
- * (tests/golden/, made by tests/golden/make_golden.py).
+ * Parity: this port is pinned against the reference itself. The reference
+ * sources are compiled unchanged for sm_100a (oracle/build_ref.sh ->
+ * oracle/_ref/libostc_ref_cuda.so, driven by oracle/ref_cuda_harness.cu);
+ * the GPU tests compare this port with that build case by case, and
+ * tests/golden/make_golden.py stores the build's outputs on small seeded
+ * cases as golden vectors (tests/golden/*.npz) that tests/test_golden_cpu.py
+ * checks this port against without a GPU.
  */
 #ifndef OSTC_ORACLE_H
 #define OSTC_ORACLE_H

@@ -696,7 +696,8 @@ int ref_download_block(void *h, int b, const char *name, double *dst) {
   if (!strcmp(name, "bv")) src = z.bv.data(), n = 6 * P;
   else if (!strcmp(name, "sv")) src = z.sv.data(), n = c->n_scalar * P;
   else if (!strcmp(name, "cv")) src = z.cv.data(), n = c->n_var * P;
-  else if (!strcmp(name, "dq")) src = z.dq.data(), n = c->n_var * I;
+  else if (!strcmp(name, "dq"))  // one ghost layer under DPLUR (Field.cu:209-221)
+    src = z.dq.data(), n = c->n_var * plane(c->mx, c->my, c->mz, c->cfg.steady && c->cfg.implicit_method == 1 ? 1 : 0);
   else if (!strcmp(name, "mul")) src = z.mul.data(), n = P;
   else if (!strcmp(name, "thermal_conductivity")) src = z.thermal_conductivity.data(), n = P;
   else if (!strcmp(name, "vel")) src = z.vel.data(), n = P;
