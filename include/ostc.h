@@ -298,6 +298,24 @@ ostc_status ostc_update_bv(ostc_ctx *ctx, void *stream);
  * res_hist as for ostc_rk3_steps; the caller tests convergence on it.      */
 ostc_status ostc_steady_steps(ostc_ctx *ctx, int n_steps, double *res_hist, void *stream);
 
+/* ---- FP64 point-implicit chemistry integrator -------------------------- */
+
+/* One point-implicit step of the finite-rate chemistry of each of n states
+ * at constant density and internal energy: rho from (T, p, Y), omega and
+ * J = d omega / d(rho Y) as compute_chem_src_jacobian builds them
+ * (src/FiniteRateChem.cu:7-216), d(rho Y) = (I - dt J)^-1 dt omega with the
+ * column-pivoted LU of solve_chem_system (src/FiniteRateChem.cu:324-419),
+ * Y' = Y + d(rho Y)/rho, and T' from e(T', Y') = e(T, Y) by the Newton
+ * iteration of compute_temperature_and_pressure (src/FieldOperation.cu:
+ * 3-39) run to a relative 1e-13. The reference has no single function for
+ * this composition; it is the labeller, fallback and judge of the chemistry
+ * surrogate. All pointers are DEVICE arrays: T, p, dt, dT of n doubles, Y
+ * and dY of n_spec x n (species-major). dT is NaN where the Newton solve did
+ * not converge. Needs a context with a finite-rate mechanism.              */
+ostc_status ostc_chem_point_implicit(ostc_ctx *ctx, int n, const double *T, const double *p,
+                                     const double *Y, const double *dt, double *dY, double *dT,
+                                     void *stream);
+
 /* Metric and Jacobian from grid coordinates that carry ngg+1 ghost layers
  * (x,y,z as host arrays with ghost count ngg+1), as Block::compute_jac_metric
  * (src/Mesh.cpp:259-521). Host-only helper: fills host jac (g=ngg) and host

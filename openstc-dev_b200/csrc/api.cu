@@ -859,6 +859,17 @@ ostc_status ostc_steady_steps(ostc_ctx *ctx, int n_steps, double *res_hist, void
   return OSTC_OK;
 }
 
+ostc_status ostc_chem_point_implicit(ostc_ctx *ctx, int n, const double *T, const double *p, const double *Y,
+                                     const double *dt, double *dY, double *dT, void *stream) {
+  if (!ctx || n < 0 || (n > 0 && (!T || !p || !Y || !dt || !dY || !dT))) return OSTC_ERR_INVALID_ARG;
+  if (!ctx->has_source) return OSTC_ERR_INVALID_ARG;  // needs a finite-rate mechanism
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  CK(dispatch_ns(ctx->ns, [&](auto m) {
+    return launch_chem_integrator<decltype(m)::value>(n, T, p, Y, dt, dY, dT, S(stream));
+  }));
+  return OSTC_OK;
+}
+
 // one kernel family on every block, for per-kernel timing and the autotuner
 ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;

@@ -240,6 +240,68 @@ __device__ __forceinline__ void lu_solve(double *A, double *b) {
   lu_apply<NS>(A, ipiv, b);
 }
 
+
+// The FP64 point-implicit chemistry integrator of one state over dt at
+// constant density and internal energy (no single reference function: it
+// composes finite_rate_chemistry, compute_chem_src_jacobian and
+// solve_chem_system, FiniteRateChem.cu:7-419, with the energy / temperature
+// relation of compute_temperature_and_pressure, FieldOperation.cu:3-39):
+//   rho from p = rho R_u T sum(Y/W); omega, J = d omega / d(rho Y) at (T, Y);
+//   d(rho Y) = (I - dt J)^-1 dt omega; Y' = Y + d(rho Y) / rho;
+//   T' solves e(T', Y') = e(T, Y), e = sum Y h(T) - R_u T sum(Y/W), by Newton
+//   to |1 - T1/T| <= 1e-13 (at most 100 iterations; the reference's 1e-3
+//   tolerance would leave kelvin-sized errors in an integrator used as judge).
+// Returns dY (NS) and dT; `iters` is the Newton count (0 if it failed).
+template <int NS>
+__device__ __forceinline__ void point_implicit_increment(double T, double p, const double *Y, double dt, double *dY,
+                                                         double &dT, int &iters) {
+  double mwinv = 0;
+#pragma unroll
+  for (int l = 0; l < NS; ++l) mwinv += Y[l] / c_p.mw[l];
+  const double rho = p / (R_u * T * mwinv);
+  double q1[OSTC_MAX_REAC], q2[OSTC_MAX_REAC], om[NS], od[NS];
+  chemistry_rates<NS>(rho, T, Y, q1, q2, om, od);
+  double A[NS * NS], b[NS];
+  chemistry_jacobian<NS>(rho, Y, q1, q2, A);
+#pragma unroll 1
+  for (int m = 0; m < NS; ++m)
+    for (int n = 0; n < NS; ++n) A[m * NS + n] = m == n ? 1.0 - dt * A[m * NS + n] : -dt * A[m * NS + n];
+#pragma unroll
+  for (int l = 0; l < NS; ++l) b[l] = dt * om[l];
+  lu_solve<NS>(A, b);
+  double Y1[NS], h[NS], cp[NS];
+  enthalpy<NS>(T, h);
+  double e0 = 0, mwinv1 = 0;
+#pragma unroll
+  for (int l = 0; l < NS; ++l) {
+    dY[l] = b[l] / rho;
+    Y1[l] = Y[l] + dY[l];
+    e0 += Y[l] * h[l];
+    mwinv1 += Y1[l] / c_p.mw[l];
+  }
+  e0 -= R_u * T * mwinv;
+  const double R1 = R_u * mwinv1;
+  double t = T;
+  iters = 0;
+  for (int it = 1; it <= 100; ++it) {
+    enthalpy_cp<NS>(t, h, cp);
+    double hs = 0, cps = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      hs += Y1[l] * h[l];
+      cps += Y1[l] * cp[l];
+    }
+    const double t1 = t - (hs - R1 * t - e0) / (cps - R1);
+    const double err = fabs(1 - t1 / t);
+    t = t1;
+    if (err <= 1e-13) {
+      iters = it;
+      break;
+    }
+  }
+  dT = t - T;
+}
+
 // mixture transport at one state (Transport.cu:40-109)
 template <int NS>
 __device__ __forceinline__ void mixture_transport(double T, double mw_total, const double *Y, const double *cp,

@@ -177,6 +177,26 @@ __global__ void __launch_bounds__(256) source_kernel(DevZone z) {
   (void)NV;
 }
 
+
+// batched FP64 point-implicit chemistry integrator (point_implicit_increment)
+// over n states held as SoA device arrays: Y and dY are [NS][n]
+template <int NS>
+__global__ void __launch_bounds__(128) chem_integrator_kernel(int n, const double *T, const double *p, const double *Y,
+                                                              const double *dt, double *dY, double *dT) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  if constexpr (NS > 0) {
+    double y[NS], d[NS], dtq;
+    int it;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) y[l] = Y[(long long)l * n + q];
+    point_implicit_increment<NS>(T[q], p[q], y, dt[q], d, dtq, it);
+#pragma unroll
+    for (int l = 0; l < NS; ++l) dY[(long long)l * n + q] = d[l];
+    dT[q] = it ? dtq : __longlong_as_double(0x7ff8000000000000ll);  // NaN marks a failed Newton solve
+  }
+}
+
 __constant__ double c_rk_a[3] = {1.0, 0.75, 1.0 / 3.0};
 __constant__ double c_rk_b[3] = {0.0, 0.25, 2.0 / 3.0};
 __constant__ double c_rk_c[3] = {1.0, 0.25, 2.0 / 3.0};
@@ -1015,6 +1035,14 @@ cudaError_t launch_steady(SteadyOp op, const DevZone &z, const SteadyArgs &a, co
   return cudaGetLastError();
 }
 
+template <int NS>
+cudaError_t launch_chem_integrator(int n, const double *T, const double *p, const double *Y, const double *dt,
+                                   double *dY, double *dT, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  chem_integrator_kernel<NS><<<(n + 127) / 128, 128, 0, s>>>(n, T, p, Y, dt, dY, dT);
+  return cudaGetLastError();
+}
+
 cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   return cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
 }
@@ -1024,7 +1052,9 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   template cudaError_t launch_cells<NS>(CellOp, const DevZone &, const CellArgs &, cudaStream_t);            \
   template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);                    \
   template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t); \
-  template cudaError_t launch_steady<NS>(SteadyOp, const DevZone &, const SteadyArgs &, const BcFace *, cudaStream_t);
+  template cudaError_t launch_steady<NS>(SteadyOp, const DevZone &, const SteadyArgs &, const BcFace *, cudaStream_t); \
+  template cudaError_t launch_chem_integrator<NS>(int, const double *, const double *, const double *, const double *, \
+                                                  double *, double *, cudaStream_t);
 
 OSTC_INSTANTIATE(0)
 OSTC_INSTANTIATE(9)

@@ -66,6 +66,9 @@ template <int NS>
 cudaError_t launch_interface(const DevZone &self, const DevZone &tar, const Iface &f, int with_cv, cudaStream_t s);
 template <int NS>
 cudaError_t launch_steady(SteadyOp op, const DevZone &z, const SteadyArgs &a, const BcFace *wall, cudaStream_t s);
+template <int NS>
+cudaError_t launch_chem_integrator(int n, const double *T, const double *p, const double *Y, const double *dt,
+                                   double *dY, double *dT, cudaStream_t s);
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
 cudaError_t upload_param(const DevParam &p, cudaStream_t s);
 

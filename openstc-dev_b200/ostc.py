@@ -132,6 +132,7 @@ def lib():
             "ostc_implicit_treatment": [vp, vp],
             "ostc_update_bv": [vp, vp],
             "ostc_steady_steps": [vp, i, C.POINTER(d), vp],
+            "ostc_chem_point_implicit": [vp, i, vp, vp, vp, vp, vp, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -535,6 +536,18 @@ class Solver:
             return np.array(res).reshape(n, 4)
         check(lib().ostc_steady_steps(self.ctx, n, None, self._s()), "ostc_steady_steps")
         return None
+
+    def chem_point_implicit(self, T, p, Y, dt):
+        """FP64 point-implicit chemistry step of each state (torch CUDA tensors:
+        T, p, dt [n]; Y [n_spec, n]); returns (dY [n_spec, n], dT [n])."""
+        import torch
+
+        n = T.numel()
+        dY = torch.empty_like(Y)
+        dT = torch.empty_like(T)
+        check(lib().ostc_chem_point_implicit(self.ctx, n, T.data_ptr(), p.data_ptr(), Y.data_ptr(), dt.data_ptr(),
+                                             dY.data_ptr(), dT.data_ptr(), self._s()), "ostc_chem_point_implicit")
+        return dY, dT
 
     OP_FLUX, OP_SOURCE, OP_PROPERTIES, OP_UPDATE, OP_DT, OP_BC = range(6)
 
@@ -970,3 +983,57 @@ def case_premixed_box(mx=16, my=14, mz=8, dx=2e-3, T0=1400.0, seed=7, mech=None,
     ext = (mx, my, mz)
     faces = [bc_face(0, BC_OUTFLOW, d, e, ext, ng) for d in range(3) for e in (-1, 1)]
     return Case("premixed_h2air_%dx%dx%d" % (mx, my, mz), s, mech, [b], faces, 10)
+
+
+# ---------------------------------------------------------------------------
+# chemistry states for the point-implicit integrator and its surrogate
+# ---------------------------------------------------------------------------
+def species_elements(names):
+    """element counts {element: array over species} parsed from species names
+    like H2O2 (the elements of the H2-air mechanism: H, O, N)."""
+    import re
+
+    out = {}
+    for k, nm in enumerate(names):
+        for el, cnt in re.findall(r"([A-Z][a-z]?)(\d*)", nm):
+            out.setdefault(el, np.zeros(len(names)))[k] += int(cnt or 1)
+    return out
+
+
+def sample_chem_states(mech: Mechanism, n: int, seed: int = 11, T_range=(300.0, 3000.0), p_atm=(0.5, 3.0),
+                       dt_range=(1e-9, 1e-7)):
+    """Seeded synthetic cell states with the value ranges of the mixing-layer
+    runs: mixture fraction Z between the air stream (O2/N2 mass 0.233/0.767)
+    and the fuel stream (H2/N2 mole 0.3/0.7), a progress variable c moving the
+    unburnt mixture toward complete combustion products, radicals H, O, OH,
+    HO2, H2O2 at log-uniform 1e-8..1e-3 (mass fractions renormalised), T
+    uniform in T_range, p uniform in p_atm (atm), dt log-uniform in dt_range.
+    Returns T[n], p[n], Y[n_spec][n], dt[n] as float64 numpy arrays."""
+    rng = np.random.default_rng(seed)
+    names, W = mech.names, mech.tables["mw"]
+    ns = len(names)
+    ix = {nm: names.index(nm) for nm in names}
+    Y_air = np.zeros(ns)
+    Y_air[ix["O2"]], Y_air[ix["N2"]] = 0.233, 0.767
+    X_f = np.zeros(ns)
+    X_f[ix["H2"]], X_f[ix["N2"]] = 0.3, 0.7
+    Y_fuel = X_f * W / np.sum(X_f * W)
+    Z = rng.uniform(0, 1, n)
+    c = rng.uniform(0, 1, n)
+    Yu = np.outer(Y_air, 1 - Z) + np.outer(Y_fuel, Z)  # [ns][n]
+    # complete combustion 2 H2 + O2 -> 2 H2O of the limiting reactant
+    nH2 = Yu[ix["H2"]] / W[ix["H2"]]
+    nO2 = Yu[ix["O2"]] / W[ix["O2"]]
+    burn = np.minimum(nH2, 2 * nO2) * c  # mol of H2 consumed per kg
+    Y = Yu.copy()
+    Y[ix["H2"]] -= burn * W[ix["H2"]]
+    Y[ix["O2"]] -= 0.5 * burn * W[ix["O2"]]
+    Y[ix["H2O"]] += burn * W[ix["H2O"]]
+    for r in ("H", "O", "OH", "HO2", "H2O2"):
+        Y[ix[r]] += 10 ** rng.uniform(-8, -3, n)
+    Y = np.maximum(Y, 0)
+    Y /= Y.sum(axis=0, keepdims=True)
+    T = rng.uniform(T_range[0], T_range[1], n)
+    p = 101325.0 * rng.uniform(p_atm[0], p_atm[1], n)
+    dt = 10 ** rng.uniform(np.log10(dt_range[0]), np.log10(dt_range[1]), n)
+    return T, p, np.ascontiguousarray(Y), dt

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -2230,6 +2231,64 @@ int oracle_steady_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zo
       }
       for (int l = 0; l < 4; ++l) res_hist[4 * step + l] = std::sqrt(res[l] / (double)n_total);
     }
+  }
+  return 0;
+}
+
+
+int oracle_chem_point_implicit(const ostc_param *P, int n, const double *T, const double *p, const double *Y,
+                               const double *dt, double *dY, double *dT) {
+  // the point-implicit chemistry integrator of ostc_chem_point_implicit:
+  // omega and J (FiniteRateChem.cu:7-216), the LU solve of solve_chem_system
+  // (FiniteRateChem.cu:324-419), T' at constant e by the Newton update of
+  // compute_temperature_and_pressure (FieldOperation.cu:3-39) run to 1e-13
+  if (P->mix_model != OSTC_MIX_FR || P->n_reac <= 0) return OSTC_ERR_INVALID_ARG;
+  const int ns = P->n_spec;
+#pragma omp parallel for schedule(static)
+  for (int q = 0; q < n; ++q) {
+    double y[MAXS], mwinv = 0;
+    for (int l = 0; l < ns; ++l) {
+      y[l] = Y[(long)l * n + q];
+      mwinv += y[l] / P->mw[l];
+    }
+    const double rho = p[q] / (R_u * T[q] * mwinv);
+    double om[MAXS], q1[MAXR], q2[MAXR], od[MAXS], J[MAXS * MAXS], b[MAXS];
+    int ipiv[MAXS];
+    chemistry_omega(P, rho, T[q], y, om, q1, q2, od);
+    chem_jacobian(P, rho, y, q1, q2, J);
+    for (int m = 0; m < ns; ++m)
+      for (int c = 0; c < ns; ++c) J[m * ns + c] = m == c ? 1.0 - dt[q] * J[m * ns + c] : -dt[q] * J[m * ns + c];
+    for (int l = 0; l < ns; ++l) b[l] = dt[q] * om[l];
+    lu_factor(J, ipiv, ns);
+    lu_apply(J, ipiv, b, ns);
+    double y1[MAXS], h[MAXS], cp[MAXS], e0 = 0, mwinv1 = 0;
+    enthalpy(P, T[q], h);
+    for (int l = 0; l < ns; ++l) {
+      dY[(long)l * n + q] = b[l] / rho;
+      y1[l] = y[l] + b[l] / rho;
+      e0 += y[l] * h[l];
+      mwinv1 += y1[l] / P->mw[l];
+    }
+    e0 -= R_u * T[q] * mwinv;
+    const double R1 = R_u * mwinv1;
+    double t = T[q];
+    bool ok = false;
+    for (int it = 1; it <= 100; ++it) {
+      enthalpy_and_cp(P, t, h, cp);
+      double hs = 0, cps = 0;
+      for (int l = 0; l < ns; ++l) {
+        hs += y1[l] * h[l];
+        cps += y1[l] * cp[l];
+      }
+      const double t1 = t - (hs - R1 * t - e0) / (cps - R1);
+      const double err = std::abs(1 - t1 / t);
+      t = t1;
+      if (err <= 1e-13) {
+        ok = true;
+        break;
+      }
+    }
+    dT[q] = ok ? t - T[q] : std::numeric_limits<double>::quiet_NaN();
   }
   return 0;
 }

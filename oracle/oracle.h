@@ -56,6 +56,10 @@ int oracle_steady_steps(const ostc_config *c, const ostc_param *p, ostc_zone *zo
 int oracle_set_interfaces(const ostc_interface *f, int n);
 /* data_communication over the registered interfaces (DataCommunication.cuh:27-110) */
 int oracle_data_communication(const ostc_param *p, ostc_zone *zones, int n_zones, int with_cv);
+/* point-implicit chemistry step of n states (host SoA arrays; Y, dY are
+ * [n_spec][n]), as ostc_chem_point_implicit */
+int oracle_chem_point_implicit(const ostc_param *p, int n, const double *T, const double *p_,
+                               const double *Y, const double *dt, double *dY, double *dT);
 /* chemistry source of one state (omega[n_spec], kg/m3/s), for known-answer tests */
 int oracle_chemical_source(const ostc_param *p, double rho, double T, const double *Y,
                            double *omega);

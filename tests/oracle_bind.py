@@ -39,6 +39,7 @@ def oracle():
             "oracle_steady_steps": ([C.POINTER(ostc.Config), C.POINTER(ostc.Param), C.POINTER(ostc.Zone), C.c_int,
                                      C.POINTER(ostc.BcFaceC), C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
             "oracle_get_threads": ([], C.c_int),
+            "oracle_chem_point_implicit": ([P, C.c_int, d, d, d, d, d, d], C.c_int),
         }
         for n, (a, r) in sig.items():
             f = getattr(L, n)
@@ -105,6 +106,21 @@ class OracleRun:
         self._ck(oracle().oracle_steady_steps(C.byref(self.config), C.byref(self.param), self.zones, len(self.blocks),
                                               self.faces, self.nf, n, res), "oracle_steady_steps")
         return np.array(res).reshape(n, 4)
+
+
+def chem_point_implicit(mech, T, p, Y, dt):
+    """the oracle's point-implicit chemistry step of n states (numpy arrays)"""
+    sch = ostc.Scheme(mix_model=ostc.MIX_FR)
+    prm, keep = ostc.make_param(sch, mech)
+    n = T.size
+    dY = np.zeros_like(Y)
+    dT = np.zeros_like(T)
+    ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    T, p, Y, dt = [np.ascontiguousarray(a, dtype=np.float64) for a in (T, p, Y, dt)]
+    st = oracle().oracle_chem_point_implicit(C.byref(prm), n, ptr(T), ptr(p), ptr(Y), ptr(dt), ptr(dY), ptr(dT))
+    if st != 0:
+        raise RuntimeError("oracle_chem_point_implicit -> %d" % st)
+    return dY, dT
 
 
 def rhs_errors(got, ref, scale, cancel=1e-2):
