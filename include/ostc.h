@@ -316,6 +316,44 @@ ostc_status ostc_chem_point_implicit(ostc_ctx *ctx, int n, const double *T, cons
                                      const double *Y, const double *dt, double *dY, double *dT,
                                      void *stream);
 
+/* ---- chemistry surrogate: network and training ------------------------- */
+/* A 12-256-256-256-10 perceptron with SiLU activations that maps the
+ * standardised features of a cell state (log T, log p, 9 transformed Y_k,
+ * log dt) to the standardised increments (9 dY_k, dT) of
+ * ostc_chem_point_implicit. BF16 weights and activations, FP32 accumulation
+ * on the tensor cores, FP32 master weights, Adam. No reference counterpart:
+ * the reference integrates chemistry only with the FP64 path above.        */
+typedef struct ostc_surrogate ostc_surrogate;
+#define OSTC_SURR_IN 12
+#define OSTC_SURR_OUT 10
+#define OSTC_SURR_HIDDEN 256
+#define OSTC_SURR_PARAMS 137482  /* W1[256][12] b1 W2[256][256] b2 W3 b3 W4[10][256] b4[10] */
+
+/* He-uniform weights from a seeded generator, zero biases; buffers for
+ * training batches of up to max_batch rows. Allocates device memory.      */
+ostc_status ostc_surrogate_create(int max_batch, unsigned long long seed, ostc_surrogate **out);
+ostc_status ostc_surrogate_destroy(ostc_surrogate *s);
+/* Feature / target scaling (HOST arrays): x_std = (x - in_mean) / in_std,
+ * y = out_mean + out_std * net(x_std); in_min / in_max bound the training
+ * envelope in raw feature units (states outside it take the FP64 path).   */
+ostc_status ostc_surrogate_set_scaling(ostc_surrogate *s, const double *in_mean, const double *in_std,
+                                       const double *out_mean, const double *out_std,
+                                       const double *in_min, const double *in_max);
+/* FP32 master parameters in the flat order of OSTC_SURR_PARAMS (HOST).
+ * set_params also resets the Adam moments.                                */
+ostc_status ostc_surrogate_get_params(const ostc_surrogate *s, float *host_out);
+ostc_status ostc_surrogate_set_params(ostc_surrogate *s, const float *host_in);
+/* Network on n standardised rows: xs [n][12] -> ys [n][10] (DEVICE).     */
+ostc_status ostc_surrogate_forward(ostc_surrogate *s, const float *xs, int n, float *ys, void *stream);
+/* Gradients of the mean squared error over n rows (xs, ys DEVICE) in the
+ * flat parameter order (grad_host, HOST) and the loss; synchronises.      */
+ostc_status ostc_surrogate_gradients(ostc_surrogate *s, const float *xs, const float *ys, int n,
+                                     float *grad_host, float *loss_host, void *stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) at learning rate lr on n rows;
+ * loss_dev (DEVICE, optional) receives the batch's sum of squared errors. */
+ostc_status ostc_surrogate_train_step(ostc_surrogate *s, const float *xs, const float *ys, int n, float lr,
+                                      float *loss_dev, void *stream);
+
 /* Metric and Jacobian from grid coordinates that carry ngg+1 ghost layers
  * (x,y,z as host arrays with ghost count ngg+1), as Block::compute_jac_metric
  * (src/Mesh.cpp:259-521). Host-only helper: fills host jac (g=ngg) and host

@@ -1,0 +1,54 @@
+// mlp.cuh — shapes and device parameters of the chemistry surrogate network
+// (12-256-256-256-10 perceptron, SiLU), shared by the training kernels
+// (mlp.cu) and the fused inference kernel (surrogate.cuh).
+#pragma once
+#include <cuda_bf16.h>
+
+struct ostc_surrogate;
+
+namespace ostc {
+namespace mlp {
+
+constexpr int NIN = 12;    // features: log T, log p, 9 transformed Y_k, log dt
+constexpr int KIN = 16;    // the first layer's K, padded to one MMA K-step
+constexpr int NH = 256;    // hidden width
+constexpr int NOUT = 10;   // dY_k (9) and dT, standardised
+constexpr int NOUTP = 16;  // the last layer's N, padded
+
+// flat padded parameter layout: W1[256][16] b1[256] W2[256][256] b2 W3 b3 W4[16][256] b4[16]
+constexpr long long OFF_W1 = 0, OFF_B1 = OFF_W1 + (long long)NH * KIN, OFF_W2 = OFF_B1 + NH,
+                    OFF_B2 = OFF_W2 + (long long)NH * NH, OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + (long long)NH * NH,
+                    OFF_W4 = OFF_B3 + NH, OFF_B4 = OFF_W4 + (long long)NOUTP * NH, NPAR = OFF_B4 + NOUTP;
+
+// feature / target scaling (doubles): means, standard deviations and the
+// training envelope (min / max of the raw features)
+enum {
+  SC_IN_MEAN = 0,
+  SC_IN_STD = SC_IN_MEAN + NIN,
+  SC_IN_MIN = SC_IN_STD + NIN,
+  SC_IN_MAX = SC_IN_MIN + NIN,
+  SC_OUT_MEAN = SC_IN_MAX + NIN,
+  SC_OUT_STD = SC_OUT_MEAN + NOUT,
+  SCALE_COUNT = SC_OUT_STD + NOUT
+};
+
+struct Net {
+  __nv_bfloat16 *wb = nullptr;  // BF16 copy of every parameter (padded layout)
+  float *wf = nullptr;          // FP32 master parameters (padded layout; biases are read from here)
+  double *scale = nullptr;      // SCALE_COUNT doubles
+  __device__ __host__ const __nv_bfloat16 *w1() const { return wb + OFF_W1; }
+  __device__ __host__ const __nv_bfloat16 *w2() const { return wb + OFF_W2; }
+  __device__ __host__ const __nv_bfloat16 *w3() const { return wb + OFF_W3; }
+  __device__ __host__ const __nv_bfloat16 *w4() const { return wb + OFF_W4; }
+  __device__ __host__ const float *b1() const { return wf + OFF_B1; }
+  __device__ __host__ const float *b2() const { return wf + OFF_B2; }
+  __device__ __host__ const float *b3() const { return wf + OFF_B3; }
+  __device__ __host__ const float *b4() const { return wf + OFF_B4; }
+};
+
+}  // namespace mlp
+
+// the device parameters of a surrogate (mlp.cu), for the inference path
+const mlp::Net *surrogate_net(const ostc_surrogate *s);
+
+}  // namespace ostc

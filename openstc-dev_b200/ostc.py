@@ -133,6 +133,15 @@ def lib():
             "ostc_update_bv": [vp, vp],
             "ostc_steady_steps": [vp, i, C.POINTER(d), vp],
             "ostc_chem_point_implicit": [vp, i, vp, vp, vp, vp, vp, vp, vp],
+            "ostc_surrogate_create": [i, C.c_ulonglong, C.POINTER(vp)],
+            "ostc_surrogate_destroy": [vp],
+            "ostc_surrogate_set_scaling": [vp, C.POINTER(d), C.POINTER(d), C.POINTER(d), C.POINTER(d),
+                                           C.POINTER(d), C.POINTER(d)],
+            "ostc_surrogate_get_params": [vp, vp],
+            "ostc_surrogate_set_params": [vp, vp],
+            "ostc_surrogate_forward": [vp, vp, i, vp, vp],
+            "ostc_surrogate_gradients": [vp, vp, vp, i, vp, vp, vp],
+            "ostc_surrogate_train_step": [vp, vp, vp, i, C.c_float, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -1037,3 +1046,72 @@ def sample_chem_states(mech: Mechanism, n: int, seed: int = 11, T_range=(300.0, 
     p = 101325.0 * rng.uniform(p_atm[0], p_atm[1], n)
     dt = 10 ** rng.uniform(np.log10(dt_range[0]), np.log10(dt_range[1]), n)
     return T, p, np.ascontiguousarray(Y), dt
+
+
+# ---------------------------------------------------------------------------
+# the chemistry surrogate's network (csrc/mlp.cu)
+# ---------------------------------------------------------------------------
+SURR_IN, SURR_OUT, SURR_PARAMS = 12, 10, 137482
+
+
+class Surrogate:
+    """The 12-256-256-256-10 SiLU network of the chemistry surrogate on the
+    GPU (BF16 weights and activations, FP32 accumulation and masters)."""
+
+    def __init__(self, max_batch: int = 65536, seed: int = 1):
+        h = C.c_void_p()
+        check(lib().ostc_surrogate_create(max_batch, seed, C.byref(h)), "ostc_surrogate_create")
+        self.h = h
+        self.max_batch = max_batch
+
+    def close(self):
+        if self.h:
+            lib().ostc_surrogate_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _s():
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+
+    def set_scaling(self, in_mean, in_std, out_mean, out_std, in_min, in_max):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (in_mean, in_std, out_mean, out_std, in_min, in_max)]
+        self._scaling = arrs
+        ptrs = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+        check(lib().ostc_surrogate_set_scaling(self.h, *ptrs), "ostc_surrogate_set_scaling")
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(SURR_PARAMS, dtype=np.float32)
+        check(lib().ostc_surrogate_get_params(self.h, out.ctypes.data), "ostc_surrogate_get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib().ostc_surrogate_set_params(self.h, p.ctypes.data), "ostc_surrogate_set_params")
+
+    def forward(self, xs):
+        import torch
+
+        ys = torch.empty((xs.shape[0], SURR_OUT), dtype=torch.float32, device=xs.device)
+        check(lib().ostc_surrogate_forward(self.h, xs.data_ptr(), xs.shape[0], ys.data_ptr(), self._s()),
+              "ostc_surrogate_forward")
+        return ys
+
+    def gradients(self, xs, ys):
+        g = np.zeros(SURR_PARAMS, dtype=np.float32)
+        loss = C.c_float()
+        check(lib().ostc_surrogate_gradients(self.h, xs.data_ptr(), ys.data_ptr(), xs.shape[0], g.ctypes.data,
+                                             C.byref(loss), self._s()), "ostc_surrogate_gradients")
+        return g, loss.value
+
+    def train_step(self, xs, ys, lr, loss_dev=None):
+        check(lib().ostc_surrogate_train_step(self.h, xs.data_ptr(), ys.data_ptr(), xs.shape[0], float(lr),
+                                              loss_dev.data_ptr() if loss_dev is not None else None, self._s()),
+              "ostc_surrogate_train_step")
