@@ -345,6 +345,11 @@ ostc_status ostc_surrogate_get_params(const ostc_surrogate *s, float *host_out);
 ostc_status ostc_surrogate_set_params(ostc_surrogate *s, const float *host_in);
 /* Network on n standardised rows: xs [n][12] -> ys [n][10] (DEVICE).     */
 ostc_status ostc_surrogate_forward(ostc_surrogate *s, const float *xs, int n, float *ys, void *stream);
+/* The same network on the tcgen05 tensor cores (128-row tiles, TMEM
+ * accumulators; the inference kernel of the chemistry surrogate) on n
+ * standardised rows; synchronises. OSTC_ERR_TIMEOUT if a bounded wait on the
+ * tensor cores ran out (the outputs are then undefined).                  */
+ostc_status ostc_surrogate_forward_tc(ostc_surrogate *s, const float *xs, int n, float *ys, void *stream);
 /* Gradients of the mean squared error over n rows (xs, ys DEVICE) in the
  * flat parameter order (grad_host, HOST) and the loss; synchronises.      */
 ostc_status ostc_surrogate_gradients(ostc_surrogate *s, const float *xs, const float *ys, int n,

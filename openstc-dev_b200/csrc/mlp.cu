@@ -27,6 +27,7 @@
 
 #include "../../include/ostc.h"
 #include "mlp.cuh"
+#include "tc_mlp.cuh"
 
 namespace ostc {
 namespace mlp {
@@ -259,6 +260,32 @@ __global__ void to_bf16_kernel(const float *w, long long count, __nv_bfloat16 *w
 
 unsigned blocks(long long n) { return (unsigned)((n + 255) / 256); }
 
+// the tensor-core forward on standardised rows (x [n][12] -> y [n][10])
+struct RawIo {
+  const float *x;
+  float *y;
+  int n;
+  __device__ bool load(int tile, int row, float *f) const {
+    const long long q = (long long)tile * tc::ROWS + row;
+    if (q >= n) return false;
+#pragma unroll
+    for (int i = 0; i < NIN; ++i) f[i] = x[q * NIN + i];
+    return true;
+  }
+  __device__ void store(int tile, int row, const float *o) const {
+    const long long q = (long long)tile * tc::ROWS + row;
+    if (q >= n) return;
+#pragma unroll
+    for (int i = 0; i < NOUT; ++i) y[q * NOUT + i] = o[i];
+  }
+};
+
+__global__ void __launch_bounds__(tc::THREADS, 1) surrogate_raw_kernel(Net net, const float *x, float *y, int n,
+                                                                        int *err) {
+  RawIo io{x, y, n};
+  tc::mlp_tiles(net, (n + tc::ROWS - 1) / tc::ROWS, io, err);
+}
+
 }  // namespace mlp
 }  // namespace ostc
 
@@ -279,6 +306,7 @@ struct ostc_surrogate {
   __nv_bfloat16 *x0 = nullptr, *a[3] = {nullptr, nullptr, nullptr}, *dzb[4] = {nullptr, nullptr, nullptr, nullptr};
   float *z[4] = {nullptr, nullptr, nullptr, nullptr}, *dz[4] = {nullptr, nullptr, nullptr, nullptr};
   float *da = nullptr, *loss = nullptr;
+  int *err = nullptr;  // set by a tensor-core kernel whose bounded wait ran out
   std::vector<void *> owned;
 };
 
@@ -403,7 +431,8 @@ ostc_status ostc_surrogate_create(int max_batch, unsigned long long seed, ostc_s
             dalloc(s, (void **)&s->net.scale, sizeof(double) * SCALE_COUNT) == cudaSuccess &&
             dalloc(s, (void **)&s->x0, sizeof(__nv_bfloat16) * B * KIN) == cudaSuccess &&
             dalloc(s, (void **)&s->da, sizeof(float) * B * NH) == cudaSuccess &&
-            dalloc(s, (void **)&s->loss, sizeof(float)) == cudaSuccess;
+            dalloc(s, (void **)&s->loss, sizeof(float)) == cudaSuccess &&
+            dalloc(s, (void **)&s->err, sizeof(int)) == cudaSuccess;
   for (int l = 0; l < 4 && ok; ++l) {
     const long long w = l == 3 ? NOUTP : NH;
     ok = dalloc(s, (void **)&s->z[l], sizeof(float) * B * w) == cudaSuccess &&
@@ -508,6 +537,29 @@ ostc_status ostc_surrogate_forward(ostc_surrogate *s, const float *xs, int n, fl
   SK(cudaMemcpy2DAsync(ys, sizeof(float) * NOUT, s->z[3], sizeof(float) * NOUTP, sizeof(float) * NOUT, n,
                        cudaMemcpyDeviceToDevice, st));
   return OSTC_OK;
+}
+
+ostc_status ostc_surrogate_forward_tc(ostc_surrogate *s, const float *xs, int n, float *ys, void *stream) {
+  if (!s || !xs || !ys || n < 0) return OSTC_ERR_INVALID_ARG;
+  if (n == 0) return OSTC_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  static int configured_dev = -1;
+  int dev = 0;
+  SK(cudaGetDevice(&dev));
+  if (configured_dev != dev) {
+    SK(cudaFuncSetAttribute(surrogate_raw_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SM_BYTES));
+    configured_dev = dev;
+  }
+  int sms = 148;
+  SK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int tiles = (n + tc::ROWS - 1) / tc::ROWS;
+  SK(cudaMemsetAsync(s->err, 0, sizeof(int), st));
+  surrogate_raw_kernel<<<tiles < sms ? tiles : sms, tc::THREADS, tc::SM_BYTES, st>>>(s->net, xs, ys, n, s->err);
+  SK(cudaGetLastError());
+  int e = 0;
+  SK(cudaMemcpyAsync(&e, s->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SK(cudaStreamSynchronize(st));
+  return e ? OSTC_ERR_TIMEOUT : OSTC_OK;
 }
 
 ostc_status ostc_surrogate_gradients(ostc_surrogate *s, const float *xs, const float *ys, int n, float *grad_host,

@@ -141,6 +141,7 @@ def lib():
             "ostc_surrogate_set_params": [vp, vp],
             "ostc_surrogate_forward": [vp, vp, i, vp, vp],
             "ostc_surrogate_gradients": [vp, vp, vp, i, vp, vp, vp],
+            "ostc_surrogate_forward_tc": [vp, vp, i, vp, vp],
             "ostc_surrogate_train_step": [vp, vp, vp, i, C.c_float, vp, vp],
         }
         for name, args in sig.items():
@@ -1102,6 +1103,15 @@ class Surrogate:
         ys = torch.empty((xs.shape[0], SURR_OUT), dtype=torch.float32, device=xs.device)
         check(lib().ostc_surrogate_forward(self.h, xs.data_ptr(), xs.shape[0], ys.data_ptr(), self._s()),
               "ostc_surrogate_forward")
+        return ys
+
+    def forward_tc(self, xs):
+        """the same network on the tcgen05 inference kernel"""
+        import torch
+
+        ys = torch.empty((xs.shape[0], SURR_OUT), dtype=torch.float32, device=xs.device)
+        check(lib().ostc_surrogate_forward_tc(self.h, xs.data_ptr(), xs.shape[0], ys.data_ptr(), self._s()),
+              "ostc_surrogate_forward_tc")
         return ys
 
     def gradients(self, xs, ys):

@@ -54,6 +54,30 @@ def test_forward_and_gradients_match_oracle(n):
     s.close()
 
 
+@pytest.mark.parametrize("n", [1, 127, 128, 5000, 300000])
+def test_tensor_core_forward_matches(n):
+    """The tcgen05 inference kernel (TMEM accumulators, 128-row tiles, ragged
+    last tile) against the mma.sync forward and the BF16-emulating oracle."""
+    import torch
+
+    s = ostc.Surrogate(max_batch=max(n, 8), seed=11)
+    p = s.params().astype(np.float64)
+    # trained-like scale: random weights with a spread of magnitudes
+    rng = np.random.default_rng(n)
+    s.set_params((p * rng.uniform(0.5, 2.0, p.size)).astype(np.float32))
+    p = s.params().astype(np.float64)
+    x, _ = _data(n, 9)
+    xt = torch.from_numpy(x).cuda()
+    y_tc = s.forward_tc(xt).cpu().numpy()
+    y_mma = s.forward(xt).cpu().numpy() if n <= s.max_batch else None
+    ref, _ = M.forward(p, x.astype(np.float64))
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(y_tc - ref)) / scale <= 2e-3
+    if y_mma is not None:
+        assert np.max(np.abs(y_tc - y_mma)) / scale <= 2e-3
+    s.close()
+
+
 def test_adam_reduces_loss():
     import torch
 
