@@ -180,6 +180,12 @@ typedef struct ostc_config {
   double dt;
   int output_screen;         /* residual cadence, RK.cuh:94                 */
   int compat;                /* 1: replicate reference quirks (Appendix A)   */
+  int chem_mode;             /* RK3 chemistry: 0 source term in the RHS (the
+                              * reference, explicit); 1 operator split: the
+                              * FP64 point-implicit integrator over each
+                              * step's dt after the three stages; 2 split
+                              * with the learned surrogate and FP64 fallback
+                              * (ostc_set_chem_surrogate)                    */
 } ostc_config;
 
 typedef struct ostc_ctx ostc_ctx;
@@ -358,6 +364,33 @@ ostc_status ostc_surrogate_gradients(ostc_surrogate *s, const float *xs, const f
  * loss_dev (DEVICE, optional) receives the batch's sum of squared errors. */
 ostc_status ostc_surrogate_train_step(ostc_surrogate *s, const float *xs, const float *ys, int n, float lr,
                                       float *loss_dev, void *stream);
+
+/* Acceptance tests of the surrogate's increments: n_elem (<= 4) elements
+ * with counts elem_counts[e][n_spec] and atomic masses elem_mass[e]; an
+ * increment is rejected when an element's mass fraction changes by more
+ * than tol_elem, or when the internal energy at constant density changes
+ * by more than tol_T kelvin worth of cv (HOST arrays).                     */
+ostc_status ostc_surrogate_set_checks(ostc_surrogate *s, int n_elem, int n_spec, const double *elem_counts,
+                                      const double *elem_mass, double tol_elem, double tol_T);
+
+/* The learned chemistry step of n states (DEVICE arrays laid out as for
+ * ostc_chem_point_implicit): features, training-envelope test, the network
+ * on the tensor cores, element and energy checks; every state that fails a
+ * test is redone by the FP64 point-implicit integrator. n_fallback (HOST,
+ * optional) receives the number of redone states and makes the call
+ * synchronise; OSTC_ERR_TIMEOUT then reports a bounded tensor-core wait that
+ * ran out. Needs the 9-species finite-rate context of the surrogate.       */
+ostc_status ostc_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur, int n, const double *T, const double *p,
+                                const double *Y, const double *dt, double *dY, double *dT, int *n_fallback,
+                                void *stream);
+
+/* The surrogate used by chem_mode 2 (the context keeps the pointer; the
+ * surrogate must outlive it). Resets the cached step graphs.               */
+ostc_status ostc_set_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur);
+/* Totals of the split chemistry since the context was created: states
+ * integrated and states the surrogate handed to the FP64 fallback (HOST
+ * outputs; synchronises the stream).                                       */
+ostc_status ostc_chem_stats(ostc_ctx *ctx, long long *states, long long *fallbacks, void *stream);
 
 /* Metric and Jacobian from grid coordinates that carry ngg+1 ghost layers
  * (x,y,z as host arrays with ghost count ngg+1), as Block::compute_jac_metric

@@ -48,6 +48,11 @@ struct ostc_ctx {
   std::vector<double *> isr, dq0, dqk, lu, da;
   std::vector<unsigned char *> piv;
   std::vector<void *> owned;  // allocations of this context to free
+  // split chemistry (chem_mode 1, 2): SoA staging of the largest block and totals
+  ostc_surrogate *sur = nullptr;
+  double *chem_buf = nullptr;
+  long long *chem_stats = nullptr;
+  long long max_cells = 0;
   ostc_status last = OSTC_OK;
   int last_cuda = 0;
   int err_block = -1, err_i = 0, err_j = 0, err_k = 0;
@@ -170,6 +175,11 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
   if (p->inviscid_type == 2 && p->inviscid_scheme != 2) return OSTC_ERR_INVALID_ARG;
   if (p->inviscid_scheme < 1 || p->inviscid_scheme > 4) return OSTC_ERR_INVALID_ARG;
   if (p->limiter != 0) return OSTC_ERR_INVALID_ARG;
+  if (cfg->chem_mode < 0 || cfg->chem_mode > 2) return OSTC_ERR_INVALID_ARG;
+  if (cfg->chem_mode != 0) {
+    if (cfg->steady || p->mix_model != OSTC_MIX_FR || p->n_reac <= 0) return OSTC_ERR_INVALID_ARG;
+    if (cfg->chem_mode == 2 && p->n_spec != 9) return OSTC_ERR_UNSUPPORTED;  // the surrogate's species count
+  }
   if (cfg->steady) {
     if (cfg->implicit_method != 0 && cfg->implicit_method != 1) return OSTC_ERR_UNSUPPORTED;
     if (cfg->implicit_method == 1 && cfg->DPLUR_inner_step < 0) return OSTC_ERR_INVALID_ARG;
@@ -451,6 +461,15 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
       c->da.push_back(da);
     }
   }
+  if (cfg->chem_mode != 0) {
+    for (auto &z : c->dz) c->max_cells = std::max(c->max_cells, (long long)z.nsz);
+    const size_t per = 2 * (size_t)param->n_spec + 4;  // T p Y dt dY dT
+    CK(cudaMalloc(&c->chem_buf, sizeof(double) * per * c->max_cells));
+    c->owned.push_back(c->chem_buf);
+    CK(cudaMalloc(&c->chem_stats, sizeof(long long) * 2));
+    c->owned.push_back(c->chem_stats);
+    CK(cudaMemset(c->chem_stats, 0, sizeof(long long) * 2));
+  }
   CK(cudaMalloc(&c->dt_bits, sizeof(unsigned long long)));
   c->n_part_per_zone = 148 * 2;
   CK(cudaMalloc(&c->res_partial, sizeof(double) * 4 * c->n_part_per_zone * n_zones));
@@ -508,7 +527,7 @@ ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream) {
   for (auto &z : ctx->dz) {
     if (z.qt != 0) CK(cudaMemsetAsync(z.dq, 0, sizeof(double) * z.qsz * ctx->prm.n_var, S(stream)));
     bool acc = z.qt != 0;
-    if (ctx->has_source) {
+    if (ctx->has_source && ctx->cfg.chem_mode == 0) {
       CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, {}, S(stream)); }));
       acc = true;
     }
@@ -676,6 +695,38 @@ static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
     CK(cudaMemcpyAsync(z.qn, z.cv, sizeof(double) * z.sz * ctx->prm.n_var, cudaMemcpyDeviceToDevice, s));
   for (int rk = 0; rk < 3; ++rk)
     if ((st = ostc_rk3_stage(ctx, rk, s))) return st;
+  if (ctx->cfg.chem_mode != 0) {
+    // operator-split chemistry over the step's dt (the last stage's dt, quirk A12)
+    if (ctx->cfg.chem_mode == 2 && !ctx->sur) return fail(ctx, OSTC_ERR_INVALID_ARG);
+    const double *dt_dev = ctx->cfg.fixed_time_step ? nullptr : (const double *)ctx->dt_bits;
+    constexpr int NS = mlp::NIN - 3;
+    for (auto &z : ctx->dz) {
+      const long long n = z.nsz;
+      double *T = ctx->chem_buf, *p = T + n, *Y = p + n, *dt = Y + NS * n, *dY = dt + n, *dT = dY + NS * n;
+      int *count = nullptr;
+      CK(dispatch_ns(ctx->ns, [&](auto m) {
+        return launch_chem_split<decltype(m)::value>(0, z, dt_dev, ctx->cfg.dt, ctx->chem_buf, nullptr, nullptr, s);
+      }));
+      if (ctx->cfg.chem_mode == 1) {
+        CK(dispatch_ns(ctx->ns, [&](auto m) {
+          return launch_chem_integrator<decltype(m)::value>((int)n, T, p, Y, dt, dY, dT, s);
+        }));
+      } else {
+        int *list = nullptr, *err = nullptr;
+        CK(surrogate_scratch(ctx->sur, (int)n, &list, &count, &err));
+        CK(launch_chem_surrogate<NS>(*surrogate_net(ctx->sur), (int)n, T, p, Y, dt, dY, dT, list, count, err, s));
+      }
+      CK(dispatch_ns(ctx->ns, [&](auto m) {
+        return launch_chem_split<decltype(m)::value>(2, z, nullptr, 0, nullptr, ctx->chem_stats, count, s);
+      }));
+      CK(dispatch_ns(ctx->ns, [&](auto m) {
+        return launch_chem_split<decltype(m)::value>(1, z, nullptr, 0, ctx->chem_buf, nullptr, nullptr, s);
+      }));
+    }
+    if ((st = ostc_apply_boundary_conditions(ctx, 1, s))) return st;
+    if ((st = ostc_data_communication(ctx, 1, s))) return st;
+    if ((st = ostc_update_physical_properties(ctx, s))) return st;
+  }
   if (with_hist) {
     CellArgs a;
     a.n_part = ctx->n_part_per_zone;
@@ -867,6 +918,59 @@ ostc_status ostc_chem_point_implicit(ostc_ctx *ctx, int n, const double *T, cons
   CK(dispatch_ns(ctx->ns, [&](auto m) {
     return launch_chem_integrator<decltype(m)::value>(n, T, p, Y, dt, dY, dT, S(stream));
   }));
+  return OSTC_OK;
+}
+
+ostc_status ostc_set_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur) {
+  if (!ctx || !sur) return OSTC_ERR_INVALID_ARG;
+  if (!ctx->has_source || ctx->ns != mlp::NIN - 3) return OSTC_ERR_INVALID_ARG;
+  // everything a captured step needs is set up here, outside any capture
+  CK(prepare_chem_surrogate());
+  int *list = nullptr, *count = nullptr, *err = nullptr;
+  long long cells = 1;
+  for (auto &z : ctx->dz) cells = std::max(cells, (long long)z.nsz);
+  if (cells > 2147483647ll) return OSTC_ERR_INVALID_ARG;
+  CK(surrogate_scratch(sur, (int)cells, &list, &count, &err));
+  ctx->sur = sur;
+  for (auto &kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  ctx->graphs.clear();
+  return OSTC_OK;
+}
+
+ostc_status ostc_chem_stats(ostc_ctx *ctx, long long *states, long long *fallbacks, void *stream) {
+  if (!ctx || !states || !fallbacks) return OSTC_ERR_INVALID_ARG;
+  long long h[2] = {0, 0};
+  if (ctx->chem_stats) {
+    CK(cudaMemcpyAsync(h, ctx->chem_stats, sizeof(h), cudaMemcpyDeviceToHost, S(stream)));
+    CK(cudaStreamSynchronize(S(stream)));
+  }
+  *states = h[0];
+  *fallbacks = h[1];
+  return OSTC_OK;
+}
+
+ostc_status ostc_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur, int n, const double *T, const double *p,
+                                const double *Y, const double *dt, double *dY, double *dT, int *n_fallback,
+                                void *stream) {
+  if (!ctx || !sur || n < 0 || (n > 0 && (!T || !p || !Y || !dt || !dY || !dT))) return OSTC_ERR_INVALID_ARG;
+  if (!ctx->has_source || ctx->ns != mlp::NIN - 3) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  CK(prepare_chem_surrogate());
+  int *list = nullptr, *count = nullptr, *err = nullptr;
+  CK(surrogate_scratch(sur, n > 0 ? n : 1, &list, &count, &err));
+  CK(cudaMemsetAsync(err, 0, sizeof(int), S(stream)));
+  CK(launch_chem_surrogate<mlp::NIN - 3>(*surrogate_net(sur), n, T, p, Y, dt, dY, dT, list, count, err, S(stream)));
+  if (n_fallback) {
+    int h[2] = {0, 0};
+    CK(cudaMemcpyAsync(&h[0], count, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+    CK(cudaMemcpyAsync(&h[1], err, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+    CK(cudaStreamSynchronize(S(stream)));
+    *n_fallback = h[0];
+    if (h[1]) return fail(ctx, OSTC_ERR_TIMEOUT);
+  }
   return OSTC_OK;
 }
 

@@ -197,6 +197,55 @@ __global__ void __launch_bounds__(128) chem_integrator_kernel(int n, const doubl
   }
 }
 
+
+// operator-split chemistry on a block: gather the interior states as SoA
+// arrays (T, p, Y [NS][n], dt), and scatter the increments back at constant
+// density and internal energy (Y, T, p, the species cv; rho E unchanged)
+template <int NS>
+__global__ void __launch_bounds__(256) chem_gather_kernel(DevZone z, const double *dt_dev, double dt_fixed, double *T,
+                                                          double *p, double *Y, double *dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
+  const int g = gidx(z, i, j, k);
+  const long long q = nidx(z, i, j, k), n = z.nsz;
+  T[q] = z.bv[5 * z.sz + g];
+  p[q] = z.bv[4 * z.sz + g];
+#pragma unroll
+  for (int l = 0; l < NS; ++l) Y[l * n + q] = z.sv[l * z.sz + g];
+  dt[q] = dt_dev ? *dt_dev : dt_fixed;
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256) chem_scatter_kernel(DevZone z, const double *dY, const double *dT) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
+  if constexpr (NS > 0) {
+    const int g = gidx(z, i, j, k);
+    const long long q = nidx(z, i, j, k), n = z.nsz;
+    const double rho = z.bv[g];
+    double mwinv = 0;
+#pragma unroll
+    for (int l = 0; l < NS; ++l) {
+      const double y = z.sv[l * z.sz + g] + dY[l * n + q];
+      z.sv[l * z.sz + g] = y;
+      z.cv[(5 + l) * z.sz + g] = rho * y;
+      mwinv += y / c_p.mw[l];
+    }
+    const double t = z.bv[5 * z.sz + g] + dT[q];
+    z.bv[5 * z.sz + g] = t;
+    z.bv[4 * z.sz + g] = rho * R_u * mwinv * t;
+  }
+}
+
+__global__ void chem_stats_kernel(long long *stats, long long n, const int *count) {
+  stats[0] += n;
+  if (count) stats[1] += *count;
+}
+
 __constant__ double c_rk_a[3] = {1.0, 0.75, 1.0 / 3.0};
 __constant__ double c_rk_b[3] = {0.0, 0.25, 2.0 / 3.0};
 __constant__ double c_rk_c[3] = {1.0, 0.25, 2.0 / 3.0};
@@ -861,6 +910,7 @@ __global__ void residual_final_kernel(const double *partial, int n_part, double 
 }  // namespace ostc
 
 #include "steady.cuh"
+#include "surrogate.cuh"
 
 namespace ostc {
 
@@ -1043,6 +1093,54 @@ cudaError_t launch_chem_integrator(int n, const double *T, const double *p, cons
   return cudaGetLastError();
 }
 
+template <int NS>
+cudaError_t launch_chem_surrogate(const mlp::Net &net, int n, const double *T, const double *p, const double *Y,
+                                  const double *dt, double *dY, double *dT, int *list, int *count, int *err,
+                                  cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  if constexpr (NS != mlp::NIN - 3) {
+    return cudaErrorInvalidValue;
+  } else {
+    // the kernel's shared-memory attribute is set by prepare_chem_surrogate
+    int dev = 0, sms = 148;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(count, 0, sizeof(int), s)) != cudaSuccess) return e;
+    ChemIo<NS> io{};
+    io.T = T, io.p = p, io.Y = Y, io.dt = dt, io.dY = dY, io.dT = dT, io.n = n;
+    io.scale = net.scale, io.ck = net.checks, io.list = list, io.count = count;
+    const int tiles = (n + tc::ROWS - 1) / tc::ROWS;
+    surrogate_chem_kernel<NS><<<tiles < sms ? tiles : sms, tc::THREADS, tc::SM_BYTES, s>>>(net, io, err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int fb = (n + 127) / 128;
+    chem_fallback_kernel<NS><<<fb < 8 * sms ? fb : 8 * sms, 128, 0, s>>>(list, count, n, T, p, Y, dt, dY, dT);
+    return cudaGetLastError();
+  }
+}
+
+template <int NS>
+cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, double dt_fixed, double *buf,
+                              long long *stats, const int *count, cudaStream_t s) {
+  // buf: T [n], p [n], Y [NS][n], dt [n], dY [NS][n], dT [n]
+  const long long n = z.nsz;
+  double *T = buf, *p = T + n, *Y = p + n, *dt = Y + NS * n, *dY = dt + n, *dT = dY + NS * n;
+  const dim3 blk(32, 8);
+  if (op == 0) {
+    chem_gather_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z, dt_dev, dt_fixed, T, p, Y, dt);
+  } else if (op == 1) {
+    chem_scatter_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z, dY, dT);
+  } else {
+    chem_stats_kernel<<<1, 1, 0, s>>>(stats, n, count);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t prepare_chem_surrogate() {
+  return cudaFuncSetAttribute(surrogate_chem_kernel<mlp::NIN - 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              tc::SM_BYTES);
+}
+
 cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   return cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
 }
@@ -1054,7 +1152,11 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t); \
   template cudaError_t launch_steady<NS>(SteadyOp, const DevZone &, const SteadyArgs &, const BcFace *, cudaStream_t); \
   template cudaError_t launch_chem_integrator<NS>(int, const double *, const double *, const double *, const double *, \
-                                                  double *, double *, cudaStream_t);
+                                                  double *, double *, cudaStream_t);                                  \
+  template cudaError_t launch_chem_surrogate<NS>(const mlp::Net &, int, const double *, const double *, const double *, \
+                                                 const double *, double *, double *, int *, int *, int *, cudaStream_t); \
+  template cudaError_t launch_chem_split<NS>(int, const DevZone &, const double *, double, double *, long long *,        \
+                                             const int *, cudaStream_t);
 
 OSTC_INSTANTIATE(0)
 OSTC_INSTANTIATE(9)

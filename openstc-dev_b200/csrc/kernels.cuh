@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "mlp.cuh"
 
 namespace ostc {
 
@@ -69,6 +70,16 @@ cudaError_t launch_steady(SteadyOp op, const DevZone &z, const SteadyArgs &a, co
 template <int NS>
 cudaError_t launch_chem_integrator(int n, const double *T, const double *p, const double *Y, const double *dt,
                                    double *dY, double *dT, cudaStream_t s);
+template <int NS>
+cudaError_t launch_chem_surrogate(const mlp::Net &net, int n, const double *T, const double *p, const double *Y,
+                                  const double *dt, double *dY, double *dT, int *list, int *count, int *err,
+                                  cudaStream_t s);
+// split chemistry of a block: op 0 gathers the interior states into buf,
+// 1 scatters the increments back, 2 adds the block's counts to stats
+template <int NS>
+cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, double dt_fixed, double *buf,
+                              long long *stats, const int *count, cudaStream_t s);
+cudaError_t prepare_chem_surrogate();
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
 cudaError_t upload_param(const DevParam &p, cudaStream_t s);
 

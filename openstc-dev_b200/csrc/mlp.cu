@@ -307,6 +307,9 @@ struct ostc_surrogate {
   float *z[4] = {nullptr, nullptr, nullptr, nullptr}, *dz[4] = {nullptr, nullptr, nullptr, nullptr};
   float *da = nullptr, *loss = nullptr;
   int *err = nullptr;  // set by a tensor-core kernel whose bounded wait ran out
+  Checks *checks = nullptr;  // device copy of the acceptance tests
+  int *list = nullptr, *count = nullptr;
+  int list_cap = 0;
   std::vector<void *> owned;
 };
 
@@ -432,7 +435,9 @@ ostc_status ostc_surrogate_create(int max_batch, unsigned long long seed, ostc_s
             dalloc(s, (void **)&s->x0, sizeof(__nv_bfloat16) * B * KIN) == cudaSuccess &&
             dalloc(s, (void **)&s->da, sizeof(float) * B * NH) == cudaSuccess &&
             dalloc(s, (void **)&s->loss, sizeof(float)) == cudaSuccess &&
-            dalloc(s, (void **)&s->err, sizeof(int)) == cudaSuccess;
+            dalloc(s, (void **)&s->err, sizeof(int)) == cudaSuccess &&
+            dalloc(s, (void **)&s->count, sizeof(int)) == cudaSuccess &&
+            dalloc(s, (void **)&s->checks, sizeof(Checks)) == cudaSuccess;
   for (int l = 0; l < 4 && ok; ++l) {
     const long long w = l == 3 ? NOUTP : NH;
     ok = dalloc(s, (void **)&s->z[l], sizeof(float) * B * w) == cudaSuccess &&
@@ -445,6 +450,7 @@ ostc_status ostc_surrogate_create(int max_batch, unsigned long long seed, ostc_s
     return OSTC_ERR_CUDA;
   }
   s->net.wf = s->master;
+  s->net.checks = s->checks;
   // He-uniform initialisation from a seeded 64-bit LCG (biases zero)
   std::vector<float> host(NPAR, 0.f);
   std::vector<unsigned char> mask(NPAR, 0);
@@ -466,7 +472,9 @@ ostc_status ostc_surrogate_create(int max_batch, unsigned long long seed, ostc_s
   for (int i = 0; i < SCALE_COUNT; ++i) scale[i] = 0.0;
   for (int i = 0; i < NIN; ++i) scale[SC_IN_STD + i] = 1.0, scale[SC_IN_MIN + i] = -1e300, scale[SC_IN_MAX + i] = 1e300;
   for (int i = 0; i < NOUT; ++i) scale[SC_OUT_STD + i] = 1.0;
-  if (cudaMemcpy(s->master, host.data(), sizeof(float) * NPAR, cudaMemcpyHostToDevice) != cudaSuccess ||
+  Checks ck;
+  if (cudaMemcpy(s->checks, &ck, sizeof(Checks), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(s->master, host.data(), sizeof(float) * NPAR, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(s->mask, mask.data(), NPAR, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(s->net.scale, scale, sizeof(scale), cudaMemcpyHostToDevice) != cudaSuccess ||
       refresh_bf16(s, nullptr) != OSTC_OK || cudaDeviceSynchronize() != cudaSuccess) {
@@ -503,6 +511,23 @@ ostc_status ostc_surrogate_set_scaling(ostc_surrogate *s, const double *in_mean,
     scale[SC_OUT_STD + i] = out_std[i];
   }
   SK(cudaMemcpy(s->net.scale, scale, sizeof(scale), cudaMemcpyHostToDevice));
+  return OSTC_OK;
+}
+
+ostc_status ostc_surrogate_set_checks(ostc_surrogate *s, int n_elem, int n_spec, const double *elem_counts,
+                                      const double *elem_mass, double tol_elem, double tol_T) {
+  if (!s || n_elem < 0 || n_elem > 4 || n_spec < 1 || n_spec > OSTC_MAX_SPEC || (n_elem && (!elem_counts || !elem_mass)))
+    return OSTC_ERR_INVALID_ARG;
+  if (!(tol_elem >= 0) || !(tol_T >= 0)) return OSTC_ERR_INVALID_ARG;
+  Checks ck;
+  ck.n_elem = n_elem;
+  for (int e = 0; e < n_elem; ++e) {
+    ck.m[e] = elem_mass[e];
+    for (int l = 0; l < n_spec; ++l) ck.a[e][l] = elem_counts[e * n_spec + l];
+  }
+  ck.tol_el = tol_elem;
+  ck.tol_T = tol_T;
+  SK(cudaMemcpy(s->checks, &ck, sizeof(Checks), cudaMemcpyHostToDevice));
   return OSTC_OK;
 }
 
@@ -597,4 +622,24 @@ ostc_status ostc_surrogate_train_step(ostc_surrogate *s, const float *xs, const 
 
 namespace ostc {
 const Net *surrogate_net(const ostc_surrogate *s) { return s ? &s->net : nullptr; }
+
+cudaError_t surrogate_scratch(ostc_surrogate *s, int n, int **list, int **count, int **err) {
+  if (n > s->list_cap) {
+    if (s->list) {
+      cudaFree(s->list);
+      for (auto &p : s->owned)
+        if (p == s->list) p = nullptr;
+    }
+    s->list = nullptr;
+    s->list_cap = 0;
+    cudaError_t e = cudaMalloc(&s->list, sizeof(int) * (size_t)n);
+    if (e != cudaSuccess) return e;
+    s->owned.push_back(s->list);
+    s->list_cap = n;
+  }
+  *list = s->list;
+  *count = s->count;
+  *err = s->err;
+  return cudaSuccess;
+}
 }  // namespace ostc

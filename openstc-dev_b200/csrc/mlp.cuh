@@ -3,6 +3,9 @@
 // (mlp.cu) and the fused inference kernel (surrogate.cuh).
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/ostc.h"
 
 struct ostc_surrogate;
 
@@ -32,7 +35,17 @@ enum {
   SCALE_COUNT = SC_OUT_STD + NOUT
 };
 
+// acceptance tests of a surrogate increment (device copy in the surrogate)
+struct Checks {
+  int n_elem = 0;
+  double a[4][OSTC_MAX_SPEC] = {};  // element counts per species
+  double m[4] = {};                 // element atomic masses (kg/kmol)
+  double tol_el = 1e-4;             // largest element mass fraction imbalance
+  double tol_T = 1.0;               // largest implied temperature error (K)
+};
+
 struct Net {
+  const Checks *checks = nullptr;  // device
   __nv_bfloat16 *wb = nullptr;  // BF16 copy of every parameter (padded layout)
   float *wf = nullptr;          // FP32 master parameters (padded layout; biases are read from here)
   double *scale = nullptr;      // SCALE_COUNT doubles
@@ -50,5 +63,8 @@ struct Net {
 
 // the device parameters of a surrogate (mlp.cu), for the inference path
 const mlp::Net *surrogate_net(const ostc_surrogate *s);
+// per-call scratch of the surrogate chemistry step: a fallback list of at
+// least n entries (grown on demand), its counter and the error word
+cudaError_t surrogate_scratch(ostc_surrogate *s, int n, int **list, int **count, int **err);
 
 }  // namespace ostc

@@ -34,7 +34,8 @@ constexpr unsigned SM_W = SM_ACT + ROWS * NH * 2;    // 256 x 256 bf16 (W2 or W3
 constexpr unsigned SM_W1 = SM_W + NH * NH * 2;       // 256 x 16 bf16
 constexpr unsigned SM_W4 = SM_W1 + NH * KIN * 2;     // 16 x 256 bf16
 constexpr unsigned SM_X0 = SM_W4 + NOUTP * NH * 2;   // 128 x 16 bf16
-constexpr unsigned SM_BAR = SM_X0 + ROWS * KIN * 2;  // mbarrier (8 B)
+constexpr unsigned SM_BIAS = SM_X0 + ROWS * KIN * 2;  // b1, b2, b3 (FP32), b4 (16)
+constexpr unsigned SM_BAR = SM_BIAS + (3 * NH + NOUTP) * 4;  // mbarrier (8 B)
 constexpr unsigned SM_TMEM = SM_BAR + 8;             // allocated tensor-memory base (4 B)
 constexpr unsigned SM_BYTES = SM_TMEM + 8;
 constexpr unsigned TMEM_COLS = 512;
@@ -161,9 +162,16 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // resident weights
+  // resident weights and biases
   load_weights(smem, SM_W1, net.w1(), NH, KIN);
   load_weights(smem, SM_W4, net.w4(), NOUTP, NH);
+  float *sbias = (float *)(smem + SM_BIAS);
+  for (int c = tid; c < NH; c += THREADS) {
+    sbias[c] = net.b1()[c];
+    sbias[NH + c] = net.b2()[c];
+    sbias[2 * NH + c] = net.b3()[c];
+  }
+  if (tid < NOUTP) sbias[3 * NH + tid] = net.b4()[tid];
   cp_async_wait_all();
   fence_async_smem();
   fence_before();
@@ -176,7 +184,6 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
   const int row = (warp & 3) * 32 + lane;   // the TMEM lane this thread reads
   const int col0 = (warp >> 2) * (NH / 2);  // first of its 128 columns
   const unsigned lane_addr = (unsigned)((warp & 3) * 32) << 16;
-  const float *bias[3] = {net.b1(), net.b2(), net.b3()};
 
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     // stream W2 while the features and layer 1 run
@@ -184,18 +191,15 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
     if (tid < ROWS) {
       float x[12];
       const bool has = io.load(tile, tid, x);
-      unsigned *dst = (unsigned *)(smem + SM_X0 + core_off(tid, 0, KIN));
-      unsigned *dst2 = (unsigned *)(smem + SM_X0 + core_off(tid, 8, KIN));
       float xs[16];
 #pragma unroll
       for (int i = 0; i < 12; ++i) xs[i] = has ? x[i] : 0.f;
 #pragma unroll
       for (int i = 12; i < 16; ++i) xs[i] = 0.f;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        dst[i] = pack_bf16(xs[2 * i], xs[2 * i + 1]);
-        dst2[i] = pack_bf16(xs[8 + 2 * i], xs[8 + 2 * i + 1]);
-      }
+      *(uint4 *)(smem + SM_X0 + core_off(tid, 0, KIN)) = make_uint4(
+          pack_bf16(xs[0], xs[1]), pack_bf16(xs[2], xs[3]), pack_bf16(xs[4], xs[5]), pack_bf16(xs[6], xs[7]));
+      *(uint4 *)(smem + SM_X0 + core_off(tid, 8, KIN)) = make_uint4(
+          pack_bf16(xs[8], xs[9]), pack_bf16(xs[10], xs[11]), pack_bf16(xs[12], xs[13]), pack_bf16(xs[14], xs[15]));
     }
     fence_async_smem();
     fence_before();
@@ -212,7 +216,7 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
       fence_after();
       if (layer == 1) load_weights(smem, SM_W, net.w3(), NH, NH);  // W2 is no longer read
       // epilogue: bias + SiLU -> BF16 activations (the next layer's A operand)
-      const float *b = bias[layer];
+      const float *b = sbias + layer * NH;
 #pragma unroll 1
       for (int ch = 0; ch < NH / 2; ch += 32) {
         float v[32];
@@ -223,7 +227,7 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
 #pragma unroll
           for (int e = 0; e < 8; e += 2) {
             const float z0 = v[q + e] + b[col0 + ch + q + e], z1 = v[q + e + 1] + b[col0 + ch + q + e + 1];
-            w4[e / 2] = pack_bf16(z0 / (1.0f + __expf(-z0)), z1 / (1.0f + __expf(-z1)));
+            w4[e / 2] = pack_bf16(__fdividef(z0, 1.0f + __expf(-z0)), __fdividef(z1, 1.0f + __expf(-z1)));
           }
           *(uint4 *)(smem + SM_ACT + core_off(row, col0 + ch + q, NH)) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
         }
@@ -249,9 +253,8 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
     if (warp < 4) {
       float v[16], y[10];
       tmem_ld16(tmem_d4 + lane_addr, v);
-      const float *b4 = net.b4();
 #pragma unroll
-      for (int i = 0; i < 10; ++i) y[i] = v[i] + b4[i];
+      for (int i = 0; i < 10; ++i) y[i] = v[i] + sbias[3 * NH + i];
       io.store(tile, row, y);
     }
     fence_before();

@@ -93,7 +93,7 @@ class IfaceC(C.Structure):
 class Config(C.Structure):
     _fields_ = [("steady", C.c_int), ("temporal_scheme", C.c_int), ("implicit_method", C.c_int),
                 ("DPLUR_inner_step", C.c_int), ("fixed_time_step", C.c_int), ("dt", C.c_double),
-                ("output_screen", C.c_int), ("compat", C.c_int)]
+                ("output_screen", C.c_int), ("compat", C.c_int), ("chem_mode", C.c_int)]
 
 
 _lib = None
@@ -142,6 +142,10 @@ def lib():
             "ostc_surrogate_forward": [vp, vp, i, vp, vp],
             "ostc_surrogate_gradients": [vp, vp, vp, i, vp, vp, vp],
             "ostc_surrogate_forward_tc": [vp, vp, i, vp, vp],
+            "ostc_surrogate_set_checks": [vp, i, i, C.POINTER(d), C.POINTER(d), d, d],
+            "ostc_chem_surrogate": [vp, vp, i, vp, vp, vp, vp, vp, vp, C.POINTER(i), vp],
+            "ostc_set_chem_surrogate": [vp, vp],
+            "ostc_chem_stats": [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), vp],
             "ostc_surrogate_train_step": [vp, vp, vp, i, C.c_float, vp, vp],
         }
         for name, args in sig.items():
@@ -209,6 +213,7 @@ class Scheme:
     entropy_fix_factor: float = 0.125
     fixed_time_step: int = 0
     dt: float = 1e-6
+    chem_mode: int = 0            # RK3 chemistry: 0 source in the RHS, 1 split FP64, 2 split surrogate
     steady: int = 0               # 1: local time stepping (steady_simulation)
     implicit_method: int = 0      # steady: 0 explicit (+ EPI/DA chemistry), 1 DPLUR
     dplur_inner_step: int = 3
@@ -276,6 +281,7 @@ def make_config(s: Scheme, output_screen: int = 1) -> Config:
     c.dt = s.dt
     c.output_screen = output_screen
     c.compat = 1
+    c.chem_mode = s.chem_mode
     return c
 
 
@@ -546,6 +552,29 @@ class Solver:
             return np.array(res).reshape(n, 4)
         check(lib().ostc_steady_steps(self.ctx, n, None, self._s()), "ostc_steady_steps")
         return None
+
+    def set_chem_surrogate(self, sur):
+        """the surrogate of chem_mode 2 (kept alive by this solver)"""
+        check(lib().ostc_set_chem_surrogate(self.ctx, sur.h), "ostc_set_chem_surrogate")
+        self._sur = sur
+
+    def chem_stats(self):
+        a, b = C.c_longlong(), C.c_longlong()
+        check(lib().ostc_chem_stats(self.ctx, C.byref(a), C.byref(b), self._s()), "ostc_chem_stats")
+        return a.value, b.value
+
+    def chem_surrogate(self, sur, T, p, Y, dt):
+        """learned chemistry step with FP64 fallback (torch CUDA tensors as for
+        chem_point_implicit); returns (dY, dT, number of states redone)."""
+        import torch
+
+        n = T.numel()
+        dY = torch.empty_like(Y)
+        dT = torch.empty_like(T)
+        nfb = C.c_int()
+        check(lib().ostc_chem_surrogate(self.ctx, sur.h, n, T.data_ptr(), p.data_ptr(), Y.data_ptr(), dt.data_ptr(),
+                                        dY.data_ptr(), dT.data_ptr(), C.byref(nfb), self._s()), "ostc_chem_surrogate")
+        return dY, dT, nfb.value
 
     def chem_point_implicit(self, T, p, Y, dt):
         """FP64 point-implicit chemistry step of each state (torch CUDA tensors:
@@ -1087,6 +1116,14 @@ class Surrogate:
         self._scaling = arrs
         ptrs = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
         check(lib().ostc_surrogate_set_scaling(self.h, *ptrs), "ostc_surrogate_set_scaling")
+
+    def set_checks(self, elem_counts, elem_mass, tol_elem=1e-4, tol_T=1.0):
+        a = np.ascontiguousarray(elem_counts, dtype=np.float64)
+        m = np.ascontiguousarray(elem_mass, dtype=np.float64)
+        self._checks = (a, m)
+        check(lib().ostc_surrogate_set_checks(self.h, a.shape[0], a.shape[1], a.ctypes.data_as(C.POINTER(C.c_double)),
+                                              m.ctypes.data_as(C.POINTER(C.c_double)), tol_elem, tol_T),
+              "ostc_surrogate_set_checks")
 
     def params(self) -> np.ndarray:
         out = np.zeros(SURR_PARAMS, dtype=np.float32)

@@ -1558,6 +1558,9 @@ void interface_exchange(const ostc_param *P, Z &Zs, Z &Zt, const ostc_interface 
       }
 }
 
+// operator-split chemistry (config chem_mode != 0) takes the source out of the RHS
+bool g_skip_source = false;
+
 void compute_rhs_zone(const ostc_param *P, Z &Zn) {
   const long nint = (long)Zn.mx * Zn.my * Zn.mz;
   const int nv = P->n_var;
@@ -1566,7 +1569,7 @@ void compute_rhs_zone(const ostc_param *P, Z &Zn) {
   std::fill(dq.p, dq.p + dq.sz * nv, 0.0);
   (void)nint;
   // compute_source<mix, Laminar>: finite-rate chemistry (SourceTerm.cuh:11-37)
-  if (P->mix_model == OSTC_MIX_FR && P->n_reac > 0) {
+  if (P->mix_model == OSTC_MIX_FR && P->n_reac > 0 && !g_skip_source) {
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < Zn.mz; ++k)
       for (int j = 0; j < Zn.my; ++j)
@@ -2110,6 +2113,11 @@ int oracle_initialize(const ostc_config *c, const ostc_param *P, ostc_zone *zone
 
 int oracle_rk3_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zones, int n_zones,
                      const ostc_bc_face *f, int n_faces, int n_steps, double *res_hist, double *dt_hist) {
+  if (c->chem_mode == 2) return OSTC_ERR_UNSUPPORTED;  // the oracle judges the surrogate through chem_mode 1
+  struct SkipGuard {
+    explicit SkipGuard(bool on) { g_skip_source = on; }
+    ~SkipGuard() { g_skip_source = false; }
+  } guard(c->chem_mode != 0);
   for (int step = 0; step < n_steps; ++step) {
     long n_total = 0;
     std::vector<std::vector<double>> last(n_zones);
@@ -2138,6 +2146,45 @@ int oracle_rk3_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zones
       }
       if (!c->fixed_time_step) dt = oracle_global_time_step(P, zones, n_zones);
       for (int b = 0; b < n_zones; ++b) oracle_update_cv_and_bv_rk(P, &zones[b], dt, rk);
+      int st = oracle_apply_boundary_conditions(P, zones, n_zones, f, n_faces, 1);
+      if (st) return st;
+      oracle_data_communication(P, zones, n_zones, 1);
+      for (int b = 0; b < n_zones; ++b) oracle_update_physical_properties(P, &zones[b]);
+    }
+    if (c->chem_mode == 1) {
+      // operator-split chemistry: the point-implicit integrator over the step's dt
+      // at constant density and internal energy, then BCs, interfaces, properties
+      for (int b = 0; b < n_zones; ++b) {
+        Z Zn(&zones[b]);
+        const int ns = P->n_spec;
+        const long n = (long)Zn.mx * Zn.my * Zn.mz;
+        std::vector<double> T(n), p(n), Y(ns * n), dts(n, dt), dY(ns * n), dT(n);
+        long q = 0;
+        for (int k = 0; k < Zn.mz; ++k)
+          for (int j = 0; j < Zn.my; ++j)
+            for (int i = 0; i < Zn.mx; ++i, ++q) {
+              T[q] = Zn.bv(i, j, k, 5);
+              p[q] = Zn.bv(i, j, k, 4);
+              for (int l = 0; l < ns; ++l) Y[l * n + q] = Zn.sv(i, j, k, l);
+            }
+        oracle_chem_point_implicit(P, (int)n, T.data(), p.data(), Y.data(), dts.data(), dY.data(), dT.data());
+        q = 0;
+        for (int k = 0; k < Zn.mz; ++k)
+          for (int j = 0; j < Zn.my; ++j)
+            for (int i = 0; i < Zn.mx; ++i, ++q) {
+              const double rho = Zn.bv(i, j, k, 0);
+              double mwinv = 0;
+              for (int l = 0; l < ns; ++l) {
+                const double y = Zn.sv(i, j, k, l) + dY[l * n + q];
+                Zn.sv(i, j, k, l) = y;
+                Zn.cv(i, j, k, 5 + l) = rho * y;
+                mwinv += y / P->mw[l];
+              }
+              const double t = Zn.bv(i, j, k, 5) + dT[q];
+              Zn.bv(i, j, k, 5) = t;
+              Zn.bv(i, j, k, 4) = rho * R_u * mwinv * t;
+            }
+      }
       int st = oracle_apply_boundary_conditions(P, zones, n_zones, f, n_faces, 1);
       if (st) return st;
       oracle_data_communication(P, zones, n_zones, 1);
