@@ -265,6 +265,7 @@ struct RawIo {
   const float *x;
   float *y;
   int n;
+  __device__ void setup(unsigned char *) {}
   __device__ bool load(int tile, int row, float *f) const {
     const long long q = (long long)tile * tc::ROWS + row;
     if (q >= n) return false;

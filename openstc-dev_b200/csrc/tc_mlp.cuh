@@ -35,7 +35,9 @@ constexpr unsigned SM_W1 = SM_W + NH * NH * 2;       // 256 x 16 bf16
 constexpr unsigned SM_W4 = SM_W1 + NH * KIN * 2;     // 16 x 256 bf16
 constexpr unsigned SM_X0 = SM_W4 + NOUTP * NH * 2;   // 128 x 16 bf16
 constexpr unsigned SM_BIAS = SM_X0 + ROWS * KIN * 2;  // b1, b2, b3 (FP32), b4 (16)
-constexpr unsigned SM_BAR = SM_BIAS + (3 * NH + NOUTP) * 4;  // mbarrier (8 B)
+constexpr unsigned SM_IO = SM_BIAS + (3 * NH + NOUTP) * 4;  // tables of the Io (IO_BYTES)
+constexpr unsigned IO_BYTES = 2048;
+constexpr unsigned SM_BAR = SM_IO + IO_BYTES;  // mbarrier (8 B)
 constexpr unsigned SM_TMEM = SM_BAR + 8;             // allocated tensor-memory base (4 B)
 constexpr unsigned SM_BYTES = SM_TMEM + 8;
 constexpr unsigned TMEM_COLS = 512;
@@ -142,7 +144,10 @@ __device__ __forceinline__ void load_weights(unsigned char *smem, unsigned off, 
   }
 }
 
-// The network core. `Io` supplies, per tile,
+// The network core. `Io` supplies
+//   void setup(unsigned char *tables)          fills IO_BYTES of shared memory
+//                                              (all threads, once per CTA)
+// and, per tile,
 //   bool load(int tile, int row, float *x12)   standardised features of a row
 //                                              (threads 0..127); false: no row
 //   void store(int tile, int row, const float *y10)   standardised outputs
@@ -172,6 +177,7 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
     sbias[2 * NH + c] = net.b3()[c];
   }
   if (tid < NOUTP) sbias[3 * NH + tid] = net.b4()[tid];
+  io.setup(smem + SM_IO);
   cp_async_wait_all();
   fence_async_smem();
   fence_before();
