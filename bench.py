@@ -44,6 +44,8 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-refcuda", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the operator-split comparison (FP64 point-implicit vs learned chemistry)")
     return ap.parse_args()
 
 
@@ -255,6 +257,12 @@ def run_ours(a):
     if not a.no_e2e:
         e2e = run_e2e(a, case, tiles)
 
+    surr = None
+    if rank == 0 and world == 1 and not a.no_surrogate and case.mech is not None:
+        try:
+            surr = run_surrogate_compare(a, tiles)
+        except Exception as exc:  # reported, not fatal for the headline line
+            surr = {"error": repr(exc)[:300]}
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_baseline(a)
@@ -277,10 +285,86 @@ def run_ours(a):
                 "gpu_launches": launches_per_step * a.steps, "launches_per_step": launches_per_step,
                 "tiles": tiles,
                 "clocks": ck, "roofline": roofline, "step_roofline": step_roofline, "kernels_ms": {k: round(v["ms"], 4) for k, v in ktab.items()},
-                "e2e": e2e, "cpu_baseline": cpu, "reference_cuda_build": refcuda}
+                "e2e": e2e, "cpu_baseline": cpu, "reference_cuda_build": refcuda, "surrogate_chem": surr}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_surrogate_compare(a, tiles):
+    """Plain vs learned chemistry on the same workload, both operator-split
+    (the flow's three RK3 stages, then each cell's chemistry over the step's
+    dt): chem_mode 1 runs the FP64 point-implicit integrator, chem_mode 2 the
+    tcgen05 surrogate with FP64 fallback. The surrogate is first trained
+    (timed separately) on 4M labelled states: 3M from the synthetic sampler
+    over the training envelope plus 1M cells of this workload's initial
+    field with log-uniform dt. Both runs start from the same state; the
+    final fields are compared after warm-up + timed steps."""
+    import numpy as np
+    import torch
+
+    import ostc
+    import surrogate as S
+
+    lab_case = ostc.case_premixed_box(8, 8, 4)
+    lab_solver, _ = lab_case.solver()
+    case = _make_case(a.workload)
+    mech = case.mech
+    b = case.blocks[0]
+    g = b.ngg
+    rng = np.random.default_rng(17)
+    bv = b.arrays["bv"][:, g:-g, g:-g, g:-g].reshape(6, -1)
+    sv = b.arrays["sv"][:, g:-g, g:-g, g:-g].reshape(b.n_spec, -1)
+    pick = rng.choice(bv.shape[1], 1_000_000, replace=False)
+    field_states = (bv[5, pick].copy(), bv[4, pick].copy(), np.ascontiguousarray(sv[:, pick]),
+                    10 ** rng.uniform(-9, -7, pick.size))
+    torch.cuda.synchronize()
+    t0 = time.time()
+    sur, sc, log = S.build(lab_solver, mech, n_train=3_000_000, epochs=20, seed=1, extra_states=field_states)
+    torch.cuda.synchronize()
+    train_s = time.time() - t0
+    n_samples = log.steps * 65536
+    out = {"train": {"states": 4_000_000, "epochs": 20, "batch": 65536, "steps": log.steps,
+                     "train_seconds": round(log.seconds, 3), "pipeline_seconds": round(train_s, 3),
+                     "samples_per_s": round(n_samples / log.seconds, 1),
+                     "tflops": round(3 * 273408 * n_samples / log.seconds / 1e12, 2),
+                     "final_loss": log.loss[-1]}}
+    finals, rates = {}, {}
+    for mode in (1, 2):
+        c = _make_case(a.workload)
+        c.scheme.chem_mode = mode
+        s, blocks = c.solver()
+        for d, (r, cc) in enumerate(tiles or []):
+            s.set_tile(d, r, cc)
+        if mode == 2:
+            s.set_chem_surrogate(sur)
+        s.initialize()
+        s.rk3_steps(max(a.warmup, 3))
+        n0, f0 = s.chem_stats()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.rk3_steps(a.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        n1, f1 = s.chem_stats()
+        rates[mode] = {"value": round(c.cells * a.steps / (ms * 1e-3) / 1e6, 2), "ms_per_step": round(ms / a.steps, 3),
+                       "fallback_fraction": round((f1 - f0) / max(1, n1 - n0), 5)}
+        finals[mode] = (blocks[0].t["bv"][5].clone(), blocks[0].t["sv"].clone())
+        s.close()
+        del blocks
+        torch.cuda.empty_cache()
+    dT = (finals[2][0] - finals[1][0]).abs()
+    dY = (finals[2][1] - finals[1][1]).abs()
+    out.update({"unit": "Mcell-updates/s", "plain_split_fp64": rates[1], "surrogate_split": rates[2],
+                "speedup_surrogate_over_plain_split": round(rates[2]["value"] / rates[1]["value"], 3),
+                "final_field_vs_plain": {"steps": max(a.warmup, 3) + a.steps, "max_abs_dT_K": float(dT.max()),
+                                         "mean_abs_dT_K": float(dT.mean()), "max_abs_dY": float(dY.max()),
+                                         "mean_abs_dY": float(dY.mean())}})
+    sur.close()
+    lab_solver.close()
+    return out
 
 
 def step_bytes_per_cell(case):

@@ -340,11 +340,13 @@ typedef struct ostc_surrogate ostc_surrogate;
 ostc_status ostc_surrogate_create(int max_batch, unsigned long long seed, ostc_surrogate **out);
 ostc_status ostc_surrogate_destroy(ostc_surrogate *s);
 /* Feature / target scaling (HOST arrays): x_std = (x - in_mean) / in_std,
- * y = out_mean + out_std * net(x_std); in_min / in_max bound the training
- * envelope in raw feature units (states outside it take the FP64 path).   */
+ * z = out_mean + out_std * net(x_std), and the predicted rate (increment
+ * per unit dt) is r0 sinh(z) where out_r0 > 0 (out_r0 NULL or 0: r = z);
+ * in_min / in_max bound the training envelope in raw feature units (states
+ * outside it take the FP64 path).                                          */
 ostc_status ostc_surrogate_set_scaling(ostc_surrogate *s, const double *in_mean, const double *in_std,
                                        const double *out_mean, const double *out_std,
-                                       const double *in_min, const double *in_max);
+                                       const double *in_min, const double *in_max, const double *out_r0);
 /* FP32 master parameters in the flat order of OSTC_SURR_PARAMS (HOST).
  * set_params also resets the Adam moments.                                */
 ostc_status ostc_surrogate_get_params(const ostc_surrogate *s, float *host_out);

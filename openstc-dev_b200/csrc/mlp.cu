@@ -496,7 +496,7 @@ ostc_status ostc_surrogate_destroy(ostc_surrogate *s) {
 
 ostc_status ostc_surrogate_set_scaling(ostc_surrogate *s, const double *in_mean, const double *in_std,
                                        const double *out_mean, const double *out_std, const double *in_min,
-                                       const double *in_max) {
+                                       const double *in_max, const double *out_r0) {
   if (!s || !in_mean || !in_std || !out_mean || !out_std || !in_min || !in_max) return OSTC_ERR_INVALID_ARG;
   double scale[SCALE_COUNT];
   for (int i = 0; i < NIN; ++i) {
@@ -510,6 +510,8 @@ ostc_status ostc_surrogate_set_scaling(ostc_surrogate *s, const double *in_mean,
     if (!(out_std[i] > 0)) return OSTC_ERR_INVALID_ARG;
     scale[SC_OUT_MEAN + i] = out_mean[i];
     scale[SC_OUT_STD + i] = out_std[i];
+    scale[SC_OUT_R0 + i] = out_r0 ? out_r0[i] : 0.0;
+    if (!(scale[SC_OUT_R0 + i] >= 0)) return OSTC_ERR_INVALID_ARG;
   }
   SK(cudaMemcpy(s->net.scale, scale, sizeof(scale), cudaMemcpyHostToDevice));
   return OSTC_OK;

@@ -23,8 +23,11 @@ constexpr long long OFF_W1 = 0, OFF_B1 = OFF_W1 + (long long)NH * KIN, OFF_W2 = 
                     OFF_B2 = OFF_W2 + (long long)NH * NH, OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + (long long)NH * NH,
                     OFF_W4 = OFF_B3 + NH, OFF_B4 = OFF_W4 + (long long)NOUTP * NH, NPAR = OFF_B4 + NOUTP;
 
-// feature / target scaling (doubles): means, standard deviations and the
-// training envelope (min / max of the raw features)
+// feature / target scaling (doubles): means, standard deviations, the
+// training envelope (min / max of the raw features) and the target
+// transform: with r0 > 0 the network learns z = asinh(rate / r0), so small
+// rates keep relative precision and large ones are compressed
+// logarithmically; rate = r0 sinh(mean + std * y)
 enum {
   SC_IN_MEAN = 0,
   SC_IN_STD = SC_IN_MEAN + NIN,
@@ -32,7 +35,8 @@ enum {
   SC_IN_MAX = SC_IN_MIN + NIN,
   SC_OUT_MEAN = SC_IN_MAX + NIN,
   SC_OUT_STD = SC_OUT_MEAN + NOUT,
-  SCALE_COUNT = SC_OUT_STD + NOUT
+  SC_OUT_R0 = SC_OUT_STD + NOUT,  // > 0: the target is asinh(rate / r0)
+  SCALE_COUNT = SC_OUT_R0 + NOUT
 };
 
 // acceptance tests of a surrogate increment (device copy in the surrogate)

@@ -20,13 +20,14 @@ namespace ostc {
 
 
 // the 12 raw features of a state (the formula of the training data,
-// surrogate.py: features), evaluated in FP32 for the network's input
+// surrogate.py: features), evaluated in FP32 for the network's input;
+// round-off negatives of absent species count as zero
 template <int NS>
 __device__ __forceinline__ void surrogate_features(float T, float p, const float *Y, float dt, float *f) {
   f[0] = __logf(T);
   f[1] = __logf(p);
 #pragma unroll
-  for (int l = 0; l < NS; ++l) f[2 + l] = __logf(Y[l] + 1e-10f);
+  for (int l = 0; l < NS; ++l) f[2 + l] = __logf(fmaxf(Y[l], 0.f) + 1e-10f);
   f[2 + NS] = __logf(dt);
 }
 
@@ -83,9 +84,10 @@ struct ChemIo {
       for (int i = 0; i < mlp::NIN; ++i) {
         t->in_mean[i] = (float)scale[mlp::SC_IN_MEAN + i];
         t->in_istd[i] = (float)(1.0 / scale[mlp::SC_IN_STD + i]);
-        // the envelope rounded outward to FP32
-        t->in_min[i] = __double2float_rd(scale[mlp::SC_IN_MIN + i]);
-        t->in_max[i] = __double2float_ru(scale[mlp::SC_IN_MAX + i]);
+        // the envelope, widened by 1e-4 in log units so that the FP32
+        // features of states on its boundary (Y_k = 0, the coldest T) pass
+        t->in_min[i] = __double2float_rd(scale[mlp::SC_IN_MIN + i] - 1e-4);
+        t->in_max[i] = __double2float_ru(scale[mlp::SC_IN_MAX + i] + 1e-4);
       }
       for (int l = 0; l < NS; ++l) {
         for (int c = 0; c < 7; ++c) {
@@ -132,11 +134,21 @@ struct ChemIo {
     const long long q = (long long)tile * tc::ROWS + row;
     if (q >= n) return;
     if constexpr (NS == mlp::NIN - 3) {
-      // the network predicts rates: increments are dt * (mean + std * y)
-      double d[NS], dTq;
+      // the network predicts (transformed) rates; increments are dt * rate
+      double d[NS + 1];
 #pragma unroll
-      for (int l = 0; l < NS; ++l) d[l] = h * (scale[mlp::SC_OUT_MEAN + l] + scale[mlp::SC_OUT_STD + l] * (double)y[l]);
-      dTq = h * (scale[mlp::SC_OUT_MEAN + NS] + scale[mlp::SC_OUT_STD + NS] * (double)y[NS]);
+      for (int l = 0; l <= NS; ++l) {
+        const double z = scale[mlp::SC_OUT_MEAN + l] + scale[mlp::SC_OUT_STD + l] * (double)y[l];
+        const double r0 = scale[mlp::SC_OUT_R0 + l];
+        d[l] = h * (r0 > 0 ? r0 * sinh(z) : z);
+      }
+      const double dTq = d[NS];
+      // a learned increment never drives a mass fraction below zero
+#pragma unroll
+      for (int l = 0; l < NS; ++l) {
+        const double y0 = Y[(long long)l * n + q];
+        if (y0 + d[l] < 0) d[l] = y0 > 0 ? -y0 : 0.0;
+      }
       // acceptance tests in FP32: element mass balance, internal energy at
       // constant density as a temperature error
       const ChemTables<NS> &t = *tb;

@@ -136,7 +136,7 @@ def lib():
             "ostc_surrogate_create": [i, C.c_ulonglong, C.POINTER(vp)],
             "ostc_surrogate_destroy": [vp],
             "ostc_surrogate_set_scaling": [vp, C.POINTER(d), C.POINTER(d), C.POINTER(d), C.POINTER(d),
-                                           C.POINTER(d), C.POINTER(d)],
+                                           C.POINTER(d), C.POINTER(d), C.POINTER(d)],
             "ostc_surrogate_get_params": [vp, vp],
             "ostc_surrogate_set_params": [vp, vp],
             "ostc_surrogate_forward": [vp, vp, i, vp, vp],
@@ -1111,8 +1111,11 @@ class Surrogate:
 
         return torch.cuda.current_stream().cuda_stream
 
-    def set_scaling(self, in_mean, in_std, out_mean, out_std, in_min, in_max):
-        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (in_mean, in_std, out_mean, out_std, in_min, in_max)]
+    def set_scaling(self, in_mean, in_std, out_mean, out_std, in_min, in_max, out_r0=None):
+        if out_r0 is None:
+            out_r0 = np.zeros(SURR_OUT)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64)
+                for a in (in_mean, in_std, out_mean, out_std, in_min, in_max, out_r0)]
         self._scaling = arrs
         ptrs = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
         check(lib().ostc_surrogate_set_scaling(self.h, *ptrs), "ostc_surrogate_set_scaling")

@@ -2,10 +2,14 @@
 point-implicit integrator, feature / target scaling, the training loop on
 the library's own kernels (ostc.Surrogate.train_step), and its evaluation.
 
-Inputs of the network (12): log T, log p, log(Y_k + 1e-10) for the nine
-species, log dt. Outputs (10): the integrator's rates dY_k / dt and dT / dt
-(increments vary over the two decades of dt mostly through the dt factor,
-which the rates remove). Both are standardised with the training set's mean and standard deviation; the
+Inputs of the network (12): log T, log p, log(max(Y_k, 0) + 1e-10) for the nine
+species, log dt. Outputs (10): the integrator's rates r = dY_k / dt and
+dT / dt (increments vary over the two decades of dt mostly through the dt
+factor, which the rates remove), learned as z = asinh(r / r0) with r0 a
+thousandth of the rate's standard deviation: small rates keep relative
+precision (a radical's formation enthalpy turns a 1e-6 error in its mass
+fraction into a kelvin of temperature), large ones are compressed
+logarithmically. Features and z are standardised with the training set's mean and standard deviation; the
 envelope (per-feature min / max of the training inputs) bounds where the
 network is trusted. The formula of the features is the one of
 csrc/surrogate.cuh: surrogate_features.
@@ -30,11 +34,13 @@ def features(T, p, Y, dt):
         import torch
 
         if isinstance(T, torch.Tensor):
-            return torch.stack([torch.log(T), torch.log(p)] + [torch.log(Y[l] + 1e-10) for l in range(Y.shape[0])] +
-                               [torch.log(dt)], dim=1)
+            return torch.stack([torch.log(T), torch.log(p)] +
+                               [torch.log(Y[l].clamp_min(0) + 1e-10) for l in range(Y.shape[0])] + [torch.log(dt)],
+                               dim=1)
     except ImportError:  # pragma: no cover
         pass
-    return np.stack([np.log(T), np.log(p)] + [np.log(Y[l] + 1e-10) for l in range(Y.shape[0])] + [np.log(dt)], axis=1)
+    return np.stack([np.log(T), np.log(p)] + [np.log(np.maximum(Y[l], 0) + 1e-10) for l in range(Y.shape[0])] +
+                    [np.log(dt)], axis=1)
 
 
 @dataclass
@@ -76,23 +82,38 @@ class Scaling:
     out_std: np.ndarray
     in_min: np.ndarray
     in_max: np.ndarray
+    out_r0: np.ndarray
+
+
+R0_FRACTION = 1e-3
+
+
+def _transform(G, r0):
+    import torch
+
+    return torch.asinh(G / r0)
 
 
 def fit_scaling(d: Dataset) -> Scaling:
+    import torch
+
     F = d.F.double()
     G = d.G.double()
+    r0 = (R0_FRACTION * G.std(0)).clamp_min(1e-30)
+    Z = _transform(G, r0)
     fm, fs = F.mean(0), F.std(0).clamp_min(1e-12)
-    gm, gs = G.mean(0), G.std(0).clamp_min(1e-30)
+    gm, gs = Z.mean(0), Z.std(0).clamp_min(1e-12)
     return Scaling(fm.cpu().numpy(), fs.cpu().numpy(), gm.cpu().numpy(), gs.cpu().numpy(),
-                   F.min(0).values.cpu().numpy(), F.max(0).values.cpu().numpy())
+                   F.min(0).values.cpu().numpy(), F.max(0).values.cpu().numpy(), r0.cpu().numpy())
 
 
 def standardise(d: Dataset, sc: Scaling):
     import torch
 
     dev = d.F.device
-    X = ((d.F - torch.from_numpy(sc.in_mean).to(dev)) / torch.from_numpy(sc.in_std).to(dev)).float().contiguous()
-    Yt = ((d.G - torch.from_numpy(sc.out_mean).to(dev)) / torch.from_numpy(sc.out_std).to(dev)).float().contiguous()
+    t = lambda a: torch.from_numpy(a).to(dev)  # noqa: E731
+    X = ((d.F - t(sc.in_mean)) / t(sc.in_std)).float().contiguous()
+    Yt = ((_transform(d.G, t(sc.out_r0)) - t(sc.out_mean)) / t(sc.out_std)).float().contiguous()
     return X, Yt
 
 
@@ -158,7 +179,7 @@ def build(solver: "ostc.Solver", mech: "ostc.Mechanism", n_train: int = 4_000_00
     sc = fit_scaling(d)
     X, Yt = standardise(d, sc)
     sur = ostc.Surrogate(max_batch=batch, seed=seed)
-    sur.set_scaling(sc.in_mean, sc.in_std, sc.out_mean, sc.out_std, sc.in_min, sc.in_max)
+    sur.set_scaling(sc.in_mean, sc.in_std, sc.out_mean, sc.out_std, sc.in_min, sc.in_max, sc.out_r0)
     set_checks(sur, mech)
     log = train(sur, X, Yt, epochs=epochs, batch=batch, lr=lr, seed=seed)
     return sur, sc, log
@@ -179,15 +200,15 @@ def errors(solver, sur, T, p, Y, dt):
 
 def save(path, sur: "ostc.Surrogate", sc: Scaling):
     np.savez(path, params=sur.params(), in_mean=sc.in_mean, in_std=sc.in_std, out_mean=sc.out_mean,
-             out_std=sc.out_std, in_min=sc.in_min, in_max=sc.in_max)
+             out_std=sc.out_std, in_min=sc.in_min, in_max=sc.in_max, out_r0=sc.out_r0)
 
 
 def load(path, mech: "ostc.Mechanism", max_batch: int = 65536):
     z = np.load(path)
-    sc = Scaling(z["in_mean"], z["in_std"], z["out_mean"], z["out_std"], z["in_min"], z["in_max"])
+    sc = Scaling(z["in_mean"], z["in_std"], z["out_mean"], z["out_std"], z["in_min"], z["in_max"], z["out_r0"])
     sur = ostc.Surrogate(max_batch=max_batch)
     sur.set_params(z["params"])
-    sur.set_scaling(sc.in_mean, sc.in_std, sc.out_mean, sc.out_std, sc.in_min, sc.in_max)
+    sur.set_scaling(sc.in_mean, sc.in_std, sc.out_mean, sc.out_std, sc.in_min, sc.in_max, sc.out_r0)
     set_checks(sur, mech)
     return sur, sc
 
