@@ -315,12 +315,14 @@ def run_surrogate_compare(a, tiles):
     rng = np.random.default_rng(17)
     bv = b.arrays["bv"][:, g:-g, g:-g, g:-g].reshape(6, -1)
     sv = b.arrays["sv"][:, g:-g, g:-g, g:-g].reshape(b.n_spec, -1)
-    pick = rng.choice(bv.shape[1], 1_000_000, replace=False)
+    n_field = min(1_000_000, bv.shape[1])
+    pick = rng.choice(bv.shape[1], n_field, replace=False)
     field_states = (bv[5, pick].copy(), bv[4, pick].copy(), np.ascontiguousarray(sv[:, pick]),
                     10 ** rng.uniform(-9, -7, pick.size))
     torch.cuda.synchronize()
     t0 = time.time()
-    sur, sc, log = S.build(lab_solver, mech, n_train=3_000_000, epochs=20, seed=1, extra_states=field_states)
+    sur, sc, log = S.build(lab_solver, mech, n_train=4_000_000 - n_field, epochs=20, seed=1,
+                           extra_states=field_states)
     torch.cuda.synchronize()
     train_s = time.time() - t0
     n_samples = log.steps * 65536
