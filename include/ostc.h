@@ -394,6 +394,15 @@ ostc_status ostc_set_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur);
  * outputs; synchronises the stream).                                       */
 ostc_status ostc_chem_stats(ostc_ctx *ctx, long long *states, long long *fallbacks, void *stream);
 
+/* The chemistry source of the RHS has a second, generated form for the
+ * 9-species / 19-reaction H2-air mechanism's structure (straight-line code
+ * from openstc-dev_b200/gen_mechanism.py; rate parameters still come from
+ * ostc_param). ostc_create selects it when the mechanism's reaction types,
+ * stoichiometry and orders match; on = 0 forces the generic form, on = 1
+ * returns OSTC_ERR_INVALID_ARG for another mechanism. No reference
+ * counterpart: the reference always runs the generic loops.               */
+ostc_status ostc_use_generated_chemistry(ostc_ctx *ctx, int on);
+
 /* Metric and Jacobian from grid coordinates that carry ngg+1 ghost layers
  * (x,y,z as host arrays with ghost count ngg+1), as Block::compute_jac_metric
  * (src/Mesh.cpp:259-521). Host-only helper: fills host jac (g=ngg) and host

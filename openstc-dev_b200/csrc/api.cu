@@ -27,6 +27,8 @@ struct ostc_ctx {
   DevParam dp{};
   int ns = 0;  // compile-time species count selecting the kernel instantiation
   bool has_source = false;
+  int spec_ok = 0;    // the mechanism has the structure of the generated chemistry code
+  int spec_mech = 0;  // ... and the source kernel uses it
   std::vector<ostc_zone> zones;
   std::vector<DevZone> dz;
   std::vector<double *> met_soa;
@@ -376,6 +378,11 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
   build_devparam(param, c->dp);
   c->ns = param->n_spec;
   c->has_source = param->mix_model == OSTC_MIX_FR && c->dp.n_reac > 0;
+  c->spec_ok = c->has_source && mechanism_is_h2air9(param->reac_type, param->stoi_f, param->stoi_b,
+                                                    param->reac_order, param->n_reac, param->n_spec)
+                   ? 1
+                   : 0;
+  c->spec_mech = c->spec_ok;
   c->zones.assign(zones, zones + n_zones);
   c->dz.resize(n_zones);
   for (int b = 0; b < n_zones; ++b) {
@@ -528,7 +535,9 @@ ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream) {
     if (z.qt != 0) CK(cudaMemsetAsync(z.dq, 0, sizeof(double) * z.qsz * ctx->prm.n_var, S(stream)));
     bool acc = z.qt != 0;
     if (ctx->has_source && ctx->cfg.chem_mode == 0) {
-      CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, {}, S(stream)); }));
+      CellArgs src;
+      src.spec = ctx->spec_mech;
+      CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, src, S(stream)); }));
       acc = true;
     }
     for (int d = 0; d < (z.mz > 1 ? 3 : 2); ++d) {
@@ -921,6 +930,18 @@ ostc_status ostc_chem_point_implicit(ostc_ctx *ctx, int n, const double *T, cons
   return OSTC_OK;
 }
 
+ostc_status ostc_use_generated_chemistry(ostc_ctx *ctx, int on) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  if (on && !ctx->spec_ok) return OSTC_ERR_INVALID_ARG;
+  ctx->spec_mech = on ? 1 : 0;
+  for (auto &kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  ctx->graphs.clear();
+  return OSTC_OK;
+}
+
 ostc_status ostc_set_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur) {
   if (!ctx || !sur) return OSTC_ERR_INVALID_ARG;
   if (!ctx->has_source || ctx->ns != mlp::NIN - 3) return OSTC_ERR_INVALID_ARG;
@@ -988,10 +1009,13 @@ ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream) {
           return launch_flux<decltype(n)::value>(z, inv, arg, ctx->tile[arg], 1, vis, S(stream));
         }));
       return OSTC_OK;
-    case OSTC_OP_SOURCE:
+    case OSTC_OP_SOURCE: {
+      CellArgs src;
+      src.spec = ctx->spec_mech;
       for (auto &z : ctx->dz)
-        CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, {}, S(stream)); }));
+        CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, src, S(stream)); }));
       return OSTC_OK;
+    }
     case OSTC_OP_PROPERTIES: return ostc_update_physical_properties(ctx, stream);
     case OSTC_OP_UPDATE: return ostc_update_cv_and_bv_rk(ctx, ctx->cfg.fixed_time_step ? ctx->cfg.dt : -1, arg, stream);
     case OSTC_OP_DT: return ostc_global_time_step(ctx, nullptr, stream);

@@ -23,6 +23,7 @@ __constant__ DevParam c_p;
 }
 
 #include "chem.cuh"
+#include "mech_h2air9.cuh"
 #include "face.cuh"
 #include "kernels.cuh"
 #include "thermo.cuh"
@@ -154,7 +155,9 @@ __global__ void __launch_bounds__(256, MINB) flux_dir(DevZone z, int nchunk, int
 // ---------------------------------------------------------------------------
 // per-cell kernels
 // ---------------------------------------------------------------------------
-template <int NS>
+// SPEC = 1: the mechanism-specialised chemistry (mech_h2air9.cuh), for
+// contexts whose mechanism has that structure
+template <int NS, int SPEC>
 __global__ void __launch_bounds__(256) source_kernel(DevZone z) {
   constexpr int NV = 5 + NS;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -169,7 +172,10 @@ __global__ void __launch_bounds__(256) source_kernel(DevZone z) {
     double Y[NS], om[NS];
 #pragma unroll
     for (int l = 0; l < NS; ++l) Y[l] = svl(z, g, l);
-    chemistry_omega<NS>(bvl(z, g, 0), bvl(z, g, 5), Y, om);
+    if constexpr (SPEC == 1 && NS == mech_h2air9::NS)
+      mech_h2air9::omega(bvl(z, g, 0), bvl(z, g, 5), Y, om);
+    else
+      chemistry_omega<NS>(bvl(z, g, 0), bvl(z, g, 5), Y, om);
     const double jc = ld(z.jac + g);
 #pragma unroll
     for (int l = 0; l < NS; ++l) dq[(5 + l) * z.qsz] = jc * om[l];
@@ -989,7 +995,10 @@ cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStr
   const dim3 blk(32, 8);
   switch (op) {
     case CellOp::Source:
-      source_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z);
+      if (a.spec)
+        source_kernel<NS, 1><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z);
+      else
+        source_kernel<NS, 0><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z);
       break;
     case CellOp::UpdateRK:
       update_rk_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z, a.dt, a.dt_dev, a.rk);
@@ -1139,6 +1148,19 @@ cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, do
 cudaError_t prepare_chem_surrogate() {
   return cudaFuncSetAttribute(surrogate_chem_kernel<mlp::NIN - 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               tc::SM_BYTES);
+}
+
+bool mechanism_is_h2air9(const int *reac_type, const int *stoi_f, const int *stoi_b, const int *reac_order, int nr,
+                         int ns) {
+  using namespace mech_h2air9;
+  if (nr != NR || ns != NS || !reac_type || !stoi_f || !stoi_b || !reac_order) return false;
+  for (int r = 0; r < NR; ++r) {
+    if (reac_type[r] != mech_h2air9::reac_type[r] || reac_order[r] != mech_h2air9::reac_order[r]) return false;
+    for (int l = 0; l < NS; ++l)
+      if (stoi_f[r * NS + l] != mech_h2air9::stoi_f[r][l] || stoi_b[r * NS + l] != mech_h2air9::stoi_b[r][l])
+        return false;
+  }
+  return true;
 }
 
 cudaError_t upload_param(const DevParam &p, cudaStream_t s) {

@@ -42,6 +42,7 @@ struct CellArgs {
   unsigned long long *dt_bits = nullptr;
   double *partial = nullptr;
   int n_part = 0;
+  int spec = 0;  // Source: use the mechanism-specialised chemistry
 };
 
 // the steady path (steady.cuh)
@@ -82,5 +83,8 @@ cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, do
 cudaError_t prepare_chem_surrogate();
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
 cudaError_t upload_param(const DevParam &p, cudaStream_t s);
+// whether a mechanism has the structure of the generated mech_h2air9.cuh
+bool mechanism_is_h2air9(const int *reac_type, const int *stoi_f, const int *stoi_b, const int *reac_order, int nr,
+                         int ns);
 
 }  // namespace ostc

@@ -145,6 +145,7 @@ def lib():
             "ostc_surrogate_set_checks": [vp, i, i, C.POINTER(d), C.POINTER(d), d, d],
             "ostc_chem_surrogate": [vp, vp, i, vp, vp, vp, vp, vp, vp, C.POINTER(i), vp],
             "ostc_set_chem_surrogate": [vp, vp],
+            "ostc_use_generated_chemistry": [vp, i],
             "ostc_chem_stats": [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), vp],
             "ostc_surrogate_train_step": [vp, vp, vp, i, C.c_float, vp, vp],
         }
@@ -552,6 +553,9 @@ class Solver:
             return np.array(res).reshape(n, 4)
         check(lib().ostc_steady_steps(self.ctx, n, None, self._s()), "ostc_steady_steps")
         return None
+
+    def use_generated_chemistry(self, on: bool):
+        check(lib().ostc_use_generated_chemistry(self.ctx, int(on)), "ostc_use_generated_chemistry")
 
     def set_chem_surrogate(self, sur):
         """the surrogate of chem_mode 2 (kept alive by this solver)"""

@@ -81,3 +81,25 @@ def test_inviscid_only_and_no_reactions():
     s.initialize()
     s.compute_rhs()
     assert max(rhs_errors(blocks[0].download("dq"), ref.blocks[0].arrays["dq"], scale)) <= RHS_TOL
+
+
+def test_generated_chemistry_matches_generic():
+    """The generated straight-line chemistry (mech_h2air9.cuh) against the
+    generic loops on the same RHS: the same operations up to FMA
+    contraction, so agreement to 1e-13 of the flux scale."""
+    from oracle_bind import OracleRun, rhs_errors
+
+    case = ostc.case_premixed_box(16, 14, 8, dx=1e-3, T0=1500.0)
+    o = OracleRun(case)
+    o.initialize()
+    scale = o.flux_scale()
+    out = []
+    for gen in (True, False):
+        s, blocks = case.solver()
+        s.use_generated_chemistry(gen)
+        s.initialize()
+        s.compute_rhs()
+        out.append(blocks[0].download("dq"))
+        s.close()
+    assert max(rhs_errors(out[0], out[1], scale)) <= 1e-13
+    assert max(rhs_errors(out[0], o.blocks[0].arrays["dq"], scale)) <= 1e-11
