@@ -414,8 +414,8 @@ ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg,
 
 /* Tile shape of the flux kernel of direction dir (0 x, 1 y, 2 z): rows of
  * 32 threads per CTA (1, 2, 4 or 8) and chunks marched per CTA; rows may be
- * OR-ed with (2 << 8) to select the build limited to 128 registers (two
- * 256-thread CTAs per SM). Set by the autotuner (openstc-dev_b200/ostc.py:
+ * OR-ed with (2 << 8) or (3 << 8) to select the builds limited to 128 or 80
+ * registers (two or three 256-thread CTAs per SM). Set by the autotuner (openstc-dev_b200/ostc.py:
  * Solver.autotune) or by hand; resets the cached graphs.                  */
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks);
 ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks);

@@ -1051,9 +1051,9 @@ ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
   // rows may carry the register budget in its upper bits: rows | (minb << 8)
   const int minb = (rows >> 8) & 0xff;
   rows &= 0xff;
-  if (chunks < 1 || chunks > 4096 || (minb != 0 && minb != 1 && minb != 2)) return OSTC_ERR_INVALID_ARG;
+  if (chunks < 1 || chunks > 4096 || minb < 0 || minb > 3) return OSTC_ERR_INVALID_ARG;
   if (!(rows == 1 || rows == 2 || rows == 4 || rows == 8)) return OSTC_ERR_INVALID_ARG;
-  ctx->tile[dir] = {rows, chunks, minb == 2 ? 2 : 1};
+  ctx->tile[dir] = {rows, chunks, minb < 1 ? 1 : minb};
   for (auto &kv : ctx->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
@@ -1064,7 +1064,7 @@ ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
 
 ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks) {
   if (!ctx || dir < 0 || dir > 2 || !rows || !chunks) return OSTC_ERR_INVALID_ARG;
-  *rows = ctx->tile[dir].rows | (ctx->tile[dir].minb == 2 ? (2 << 8) : 0);
+  *rows = ctx->tile[dir].rows | (ctx->tile[dir].minb > 1 ? (ctx->tile[dir].minb << 8) : 0);
   *chunks = ctx->tile[dir].chunks;
   return OSTC_OK;
 }

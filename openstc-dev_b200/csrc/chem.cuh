@@ -91,7 +91,7 @@ template <int NS>
 __device__ __forceinline__ void chemistry_setup(double rho, double t, const double *Y, double *c, double *g,
                                                 double &lnT, double &invT, double &ln_temp_t) {
 #pragma unroll
-  for (int l = 0; l < NS; ++l) c[l] = rho * Y[l] / c_p.mw[l] * 1e-3;
+  for (int l = 0; l < NS; ++l) c[l] = rho * Y[l] * c_p.imw[l] * 1e-3;
   if (c_p.need_gibbs) gibbs_div_rt<NS>(t, g);
   constexpr double temp_p = p_atm / R_u * 1e-3;
   const double temp_t = temp_p / t;
@@ -257,7 +257,7 @@ __device__ __forceinline__ void point_implicit_increment(double T, double p, con
                                                          double &dT, int &iters) {
   double mwinv = 0;
 #pragma unroll
-  for (int l = 0; l < NS; ++l) mwinv += Y[l] / c_p.mw[l];
+  for (int l = 0; l < NS; ++l) mwinv += Y[l] * c_p.imw[l];
   const double rho = p / (R_u * T * mwinv);
   double q1[OSTC_MAX_REAC], q2[OSTC_MAX_REAC], om[NS], od[NS];
   chemistry_rates<NS>(rho, T, Y, q1, q2, om, od);
@@ -277,7 +277,7 @@ __device__ __forceinline__ void point_implicit_increment(double T, double p, con
     dY[l] = b[l] / rho;
     Y1[l] = Y[l] + dY[l];
     e0 += Y[l] * h[l];
-    mwinv1 += Y1[l] / c_p.mw[l];
+    mwinv1 += Y1[l] * c_p.imw[l];
   }
   e0 -= R_u * T * mwinv;
   const double R1 = R_u * mwinv1;
@@ -312,7 +312,7 @@ __device__ __forceinline__ void mixture_transport(double T, double mw_total, con
   const double Tm145 = exp(-0.145 * log(T));
 #pragma unroll
   for (int l = 0; l < NS; ++l) {
-    X[l] = Y[l] * mw_total / c_p.mw[l];
+    X[l] = Y[l] * mw_total * c_p.imw[l];
     const double t_dl = T * c_p.LJ_inv[l] + 0.5;
     const double ci = 1.147 * (Tm145 * c_p.LJm145[l]) + 1.0 / (t_dl * t_dl);
     vis[l] = c_p.vis_coeff[l] * sqT / ci;

@@ -96,7 +96,7 @@ __device__ __forceinline__ void hllc(const double *pl, const double *pr, double 
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
       svm[l] = rlc * pl[l + 5] + rrc * pr[l + 5];
-      mw_inv += svm[l] / c_p.mw[l];
+      mw_inv += svm[l] * c_p.imw[l];
     }
     const double t = (rlc * (pl[4] / pl[0]) + rrc * (pr[4] / pr[0])) / (R_u * mw_inv);
     double h_i[NS], cp_i[NS];
@@ -220,8 +220,8 @@ __device__ __forceinline__ void reconstruct_pv(const DevZone &z, int g0, double 
     double mwl = 0, mwr = 0;
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
-      mwl += pl[5 + l] / c_p.mw[l];
-      mwr += pr[5 + l] / c_p.mw[l];
+      mwl += pl[5 + l] * c_p.imw[l];
+      mwr += pr[5 + l] * c_p.imw[l];
     }
     const double tl = pl[4] / (pl[0] * R_u * mwl), tr = pr[4] / (pr[0] * R_u * mwr);
     double cpl = 0, cpr = 0, cvl = 0, cvr = 0;
@@ -278,7 +278,7 @@ __device__ __forceinline__ double entropy_fix_delta(const DevZone &z, int g) {
   const double kx = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
   const double ky = sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
   const double kz = sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
-  return c_p.entropy_fix_factor * (U + V + W + ld(z.a + g) * (kx + ky + kz) / 3.0);
+  return c_p.entropy_fix_factor * (U + V + W + ld(z.a + g) * (kx + ky + kz) * (1.0 / 3));
 }
 
 // Roe flux-difference splitting (Roe_compute_half_point_flux + compute_half_sum_left_right_flux,
@@ -333,7 +333,7 @@ __device__ __forceinline__ void inviscid_face_roe(const DevZone &z, int g0, doub
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
       svm[l] = (dl * pl[l + 5] + dr * pr[l + 5]) * inv_den;
-      mw_inv += svm[l] / c_p.mw[l];
+      mw_inv += svm[l] * c_p.imw[l];
     }
     const double tl = pl[4] / pl[0], tr = pr[4] / pr[0];
     const double t = (dl * tl + dr * tr) * inv_den / (R_u * mw_inv);
@@ -372,7 +372,7 @@ __device__ __forceinline__ void inviscid_face_roe(const DevZone &z, int g0, doub
   double c1 = (gamma - 1) * (ek * dq[0] - u * dq[1] - v * dq[2] - w * dq[3] + dq[4]) / (c * c);
   double c2 = (kx * dq[1] + ky * dq[2] + kz * dq[3] - Uk * dq[0]) / c;
 #pragma unroll
-  for (int l = 0; l < NS; ++l) c1 += (mw / c_p.mw[l] - h_i[l] * (gamma - 1) / (c * c)) * dq[l + 5];
+  for (int l = 0; l < NS; ++l) c1 += (mw * c_p.imw[l] - h_i[l] * (gamma - 1) / (c * c)) * dq[l + 5];
   double c3 = dq[0] - c1;
   double b[NV];
   {
@@ -394,7 +394,7 @@ __device__ __forceinline__ void inviscid_face_roe(const DevZone &z, int g0, doub
   c2 = c * (b[4] - b[0]);
   c3 = 0;
 #pragma unroll
-  for (int l = 0; l < NS; ++l) c3 += (h_i[l] - mw / c_p.mw[l] * c * c / (gamma - 1)) * b[l + 5];
+  for (int l = 0; l < NS; ++l) c3 += (h_i[l] - mw * c_p.imw[l] * c * c / (gamma - 1)) * b[l + 5];
   F[0] += 0.5 * c1;
   F[1] += 0.5 * (u * c1 + kx * c2 - c * (kz * b[2] - ky * b[3]));
   F[2] += 0.5 * (v * c1 + ky * c2 - c * (kx * b[3] - kz * b[1]));
@@ -633,9 +633,9 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
   const double w_y = dw[0] * mm[1] + dw[1] * mm[4] + dw[2] * mm[7];
   const double w_z = dw[0] * mm[2] + dw[1] * mm[5] + dw[2] * mm[8];
   const double mu = 0.5 * (ld(z.mul + g0) + ld(z.mul + g1));
-  const double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
-  const double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
-  const double tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  const double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) * (1.0 / 3);
+  const double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) * (1.0 / 3);
+  const double tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) * (1.0 / 3);
   const double txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
   const double j0 = ld(z.jac + g0), j1 = ld(z.jac + g1);
   const double kxj = 0.5 * (met(z, g0, 3 * DIR) * j0 + met(z, g1, 3 * DIR) * j1);
@@ -669,8 +669,8 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
       const double g = kxj * y_x + kyj * y_y + kzj * y_z;
       ddf[l] = g;
       corr += diff[l] * g;
-      sgw += g / c_p.mw[l];
-      mwt += yk[l] / c_p.mw[l];
+      sgw += g * c_p.imw[l];
+      mwt += yk[l] * c_p.imw[l];
       srdy += diff[l] * yk[l];
     }
     mwt = 1.0 / mwt;
@@ -684,8 +684,8 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
       const double gp = (kxj * p_x + kyj * p_y + kzj * p_z) / (0.5 * (bvl(z, g1, 4) + bvl(z, g0, 4)));
 #pragma unroll
       for (int l = 0; l < NS; ++l) {
-        ddf[l] += (mwt / c_p.mw[l] - 1) * yk[l] * gp;
-        corr += (mwt / c_p.mw[l] - 1) * yk[l] * gp * diff[l];
+        ddf[l] += (mwt * c_p.imw[l] - 1) * yk[l] * gp;
+        corr += (mwt * c_p.imw[l] - 1) * yk[l] * gp * diff[l];
       }
     }
     double h[NS];

@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(256) chem_scatter_kernel(DevZone z, const doub
       const double y = z.sv[l * z.sz + g] + dY[l * n + q];
       z.sv[l * z.sz + g] = y;
       z.cv[(5 + l) * z.sz + g] = rho * y;
-      mwinv += y / c_p.mw[l];
+      mwinv += y * c_p.imw[l];
     }
     const double t = z.bv[5 * z.sz + g] + dT[q];
     z.bv[5 * z.sz + g] = t;
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(256) update_rk_kernel(DevZone z, double dt_in,
     // compute_temperature_and_pressure (FieldOperation.cu:3-39)
     double mw = 0;
 #pragma unroll
-    for (int l = 0; l < NS; ++l) mw += Y[l] / c_p.mw[l];
+    for (int l = 0; l < NS; ++l) mw += Y[l] * c_p.imw[l];
     mw = 1 / mw;
     const double R = R_u / mw;
     const double e = cv[4] / rho - 0.5 * V2;
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(256) properties_kernel(DevZone z) {
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
       Y[l] = z.sv[l * z.sz + g];
-      mw += Y[l] / c_p.mw[l];
+      mw += Y[l] * c_p.imw[l];
       cpt += Y[l] * cp[l];
       cvv += Y[l] * (cp[l] - c_p.Rmw[l]);
     }
@@ -595,7 +595,7 @@ __global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
       z.sv[l * z.sz + g] = z.sv[l * z.sz + gin];
-      mw += z.sv[l * z.sz + g] / c_p.mw[l];
+      mw += z.sv[l * z.sz + g] * c_p.imw[l];
     }
     mw = 1 / mw;
   }
@@ -622,7 +622,7 @@ __global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
 #pragma unroll
       for (int l = 0; l < NS; ++l) {
         z.sv[l * z.sz + go] = z.sv[l * z.sz + gi];
-        mw += z.sv[l * z.sz + go] / c_p.mw[l];
+        mw += z.sv[l * z.sz + go] * c_p.imw[l];
       }
       mw = 1 / mw;
     }
@@ -662,7 +662,7 @@ __global__ void bc_farfield_kernel(DevZone z, BcFace b) {
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
       sv_b[l] = z.sv[l * z.sz + g];
-      mw_inv += sv_b[l] / c_p.mw[l];
+      mw_inv += sv_b[l] * c_p.imw[l];
     }
     gamma_b = z.gam[g];
     mw = 1.0 / mw_inv;
@@ -960,8 +960,11 @@ static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, int accum
 template <int NS, int INV, int DIR>
 static cudaError_t launch_flux_t(const DevZone &z, const TileShape &t, int accumulate, int viscous,
                                  cudaStream_t s) {
-  return t.minb == 2 ? launch_flux_m<NS, INV, DIR, 2>(z, t, accumulate, viscous, s)
-                     : launch_flux_m<NS, INV, DIR, 1>(z, t, accumulate, viscous, s);
+  switch (t.minb) {
+    case 3: return launch_flux_m<NS, INV, DIR, 3>(z, t, accumulate, viscous, s);
+    case 2: return launch_flux_m<NS, INV, DIR, 2>(z, t, accumulate, viscous, s);
+    default: return launch_flux_m<NS, INV, DIR, 1>(z, t, accumulate, viscous, s);
+  }
 }
 
 template <int NS>

@@ -11,7 +11,7 @@ namespace ostc {
 struct TileShape {
   int rows;
   int chunks;
-  int minb = 1;  // register budget: 1 (<=255 regs) or 2 (<=128 regs) CTAs of 256 threads per SM
+  int minb = 1;  // register budget: 1 (<=255 regs), 2 (<=128) or 3 (<=80) CTAs of 256 threads per SM
 };
 
 // one boundary face as the kernels see it

@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(256) update_bv_kernel(DevZone z) {
     // compute_temperature_and_pressure (FieldOperation.cu:3-39)
     double mw = 0;
 #pragma unroll
-    for (int l = 0; l < NS; ++l) mw += Y[l] / c_p.mw[l];
+    for (int l = 0; l < NS; ++l) mw += Y[l] * c_p.imw[l];
     mw = 1 / mw;
     const double R = R_u / mw;
     const double e = Et / rho - 0.5 * V2;
@@ -233,7 +233,7 @@ __device__ __forceinline__ void jacobian_times_dq(const DevZone &z, const double
     gamma = z.gam[g];
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
-      b3 += R_u * t / c_p.mw[l] * dqp[5 + l];
+      b3 += R_u * t * c_p.imw[l] * dqp[5 + l];
       b4 += hk[l] * dqp[5 + l];
       h += z.sv[l * S + g] * hk[l];
     }

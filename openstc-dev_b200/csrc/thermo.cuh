@@ -1,5 +1,8 @@
 // thermo.cuh — NASA-7 thermodynamics and mixture transport on the device.
 //
+// Divisions by constants (1/3, 1/6, 1/12) and by molecular weights are
+// multiplications by reciprocals here and in the flux, chemistry and update
+// kernels (at most one rounding apart from the reference's quotients).
 // Arithmetic follows src/Thermo.cu:5-79 and src/Transport.cu:6-145 term by
 // term; the species count NS is a compile-time constant so that every
 // per-species array lives in registers (the reference keeps MAX_SPEC_NUMBER-
@@ -25,7 +28,7 @@ __device__ __forceinline__ void enthalpy_cp(double t, double *h, double *cp) {
     } else if (t < c_p.t_mid[i]) {
       c = c_p.lo[i];
     }
-    double hi = c[0] * tt + 0.5 * c[1] * tt2 + c[2] * tt3 / 3 + 0.25 * c[3] * tt4 + 0.2 * c[4] * tt5 + c[5];
+    double hi = c[0] * tt + 0.5 * c[1] * tt2 + c[2] * tt3 * (1.0 / 3) + 0.25 * c[3] * tt4 + 0.2 * c[4] * tt5 + c[5];
     const double cpi = c[0] + c[1] * tt + c[2] * tt2 + c[3] * tt3 + c[4] * tt4;
     if (below) hi += cpi * (t - tt);
     h[i] = hi * c_p.Rmw[i];
@@ -49,7 +52,7 @@ __device__ __forceinline__ void enthalpy(double t, double *h) {
     } else if (t < c_p.t_mid[i]) {
       c = c_p.lo[i];
     }
-    double hi = c[0] * tt + 0.5 * c[1] * tt2 + c[2] * tt3 / 3 + 0.25 * c[3] * tt4 + 0.2 * c[4] * tt5 + c[5];
+    double hi = c[0] * tt + 0.5 * c[1] * tt2 + c[2] * tt3 * (1.0 / 3) + 0.25 * c[3] * tt4 + 0.2 * c[4] * tt5 + c[5];
     if (below) {
       const double cpi = c[0] + c[1] * tt + c[2] * tt2 + c[3] * tt3 + c[4] * tt4;
       hi += cpi * (t - tt);
@@ -86,11 +89,11 @@ __device__ __forceinline__ void gibbs_div_rt(double t, double *g) {
       const double tt = c_p.t_low[i];
       const double tt2 = tt * tt, tt3 = tt2 * tt, tt4 = tt3 * tt, tt_inv = 1 / tt, log_tt = log(tt);
       const double *c = c_p.lo[i];
-      g[i] = c[0] * (1.0 - log_tt) - 0.5 * c[1] * tt - c[2] * tt2 / 6.0 - c[3] * tt3 / 12.0 - c[4] * tt4 * 0.05 +
+      g[i] = c[0] * (1.0 - log_tt) - 0.5 * c[1] * tt - c[2] * tt2 * (1.0 / 6) - c[3] * tt3 * (1.0 / 12) - c[4] * tt4 * 0.05 +
              c[5] * tt_inv - c[6];
     } else {
       const double *c = t < c_p.t_mid[i] ? c_p.lo[i] : c_p.hi[i];
-      g[i] = c[0] * (1.0 - log_t) - 0.5 * c[1] * t - c[2] * t2 / 6.0 - c[3] * t3 / 12.0 - c[4] * t4 * 0.05 +
+      g[i] = c[0] * (1.0 - log_t) - 0.5 * c[1] * t - c[2] * t2 * (1.0 / 6) - c[3] * t3 * (1.0 / 12) - c[4] * t4 * 0.05 +
              c[5] * t_inv - c[6];
     }
   }

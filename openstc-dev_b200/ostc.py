@@ -628,8 +628,8 @@ class Solver:
                 cmax = min(64, max(1, (n + 1 + span - 1) // span))
                 c = 1
                 while True:
-                    for minb in (1, 2):
-                        cands.append((R | (minb << 8 if minb == 2 else 0), min(c, cmax)))
+                    for minb in (1, 2, 3):
+                        cands.append((R | (minb << 8 if minb > 1 else 0), min(c, cmax)))
                     if c >= cmax:
                         break
                     c *= 2
