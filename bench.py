@@ -249,7 +249,7 @@ def run_ours(a):
                      "peak": hbm, "unit": "GB/s", "frac": round(value * 1e6 * b_alg / 1e9 / hbm, 4)}
 
     # end to end through the public API from host buffers
-    tiles = [solver.get_tile(d) for d in range(3)]
+    tiles = solver.tiles()
     solver.close()
     del blocks
     torch.cuda.empty_cache()
@@ -336,8 +336,7 @@ def run_surrogate_compare(a, tiles):
         c = _make_case(a.workload)
         c.scheme.chem_mode = mode
         s, blocks = c.solver()
-        for d, (r, cc) in enumerate(tiles or []):
-            s.set_tile(d, r, cc)
+        s.set_tiles(tiles)
         if mode == 2:
             s.set_chem_surrogate(sur)
         s.initialize()
@@ -407,8 +406,7 @@ def run_e2e(a, case, tiles=None):
         blocks[0].t[n].copy_(t.view(blocks[0].t[n].dtype).reshape(blocks[0].t[n].shape), non_blocking=True)
         h2d += t.numel() * t.element_size()
     solver = ostc.Solver(case.scheme, case.mech, blocks, case.faces)
-    for d, (r, c) in enumerate(tiles or []):
-        solver.set_tile(d, r, c)
+    solver.set_tiles(tiles)
     solver.initialize()
     res, dts = solver.rk3_steps(a.steps, history=True)
     out_bv.copy_(blocks[0].t["bv"], non_blocking=True)

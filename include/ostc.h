@@ -415,13 +415,20 @@ ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg,
 /* Tile shape of the flux kernel of direction dir (0 x, 1 y, 2 z): rows of
  * 32 threads per CTA (1, 2, 4 or 8) and chunks marched per CTA; rows may be
  * OR-ed with (2 << 8) or (3 << 8) to select the builds limited to 128 or 80
- * registers (two or three 256-thread CTAs per SM). Set by the autotuner (openstc-dev_b200/ostc.py:
+ * registers (two or three 256-thread CTAs per SM), or with (4 << 8) for the
+ * build limited to 168 registers (three CTAs of at most 4 rows per SM).
+ * dir 3, 4, 5: a tile for a separate viscous-flux kernel of direction
+ * dir - 3; with one set, a viscous flow runs the inviscid flux (tile of dir
+ * - 3) and the viscous flux as two kernels instead of the fused one. rows = 0
+ * there returns to the fused kernel (get_tile reports 0, 0 then).
+ * Set by the autotuner (openstc-dev_b200/ostc.py:
  * Solver.autotune) or by hand; resets the cached graphs.                  */
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks);
 ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks);
 
 /* Launch one kernel family on every block (timing and autotuning aid):
- * OSTC_OP_FLUX (arg = direction, accumulates into dq), OSTC_OP_SOURCE,
+ * OSTC_OP_FLUX (arg = direction, accumulates into dq; arg + 3: the inviscid
+ * flux kernel alone, arg + 6: the viscous flux kernel alone), OSTC_OP_SOURCE,
  * OSTC_OP_PROPERTIES, OSTC_OP_UPDATE (arg = rk stage), OSTC_OP_DT,
  * OSTC_OP_BC (arg = with_cv). No reference counterpart: the reference
  * launches these only from its stage loop (src/RK.cuh:107-161).            */

@@ -542,7 +542,7 @@ ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream) {
     }
     for (int d = 0; d < (z.mz > 1 ? 3 : 2); ++d) {
       CK(dispatch_ns(ctx->ns, [&](auto n) {
-        return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], (acc || d > 0) ? 1 : 0, vis, S(stream));
+        return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], (acc || d > 0) ? 1 : 0, vis, 0, S(stream));
       }));
     }
   }
@@ -1002,13 +1002,17 @@ ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream) {
   const int inv = ctx->prm.inviscid_type;
   const int vis = ctx->prm.viscous_scheme != 0;
   switch (op) {
-    case OSTC_OP_FLUX:
-      if (arg < 0 || arg > 2) return OSTC_ERR_INVALID_ARG;
+    case OSTC_OP_FLUX: {
+      // arg 0..2: the direction's face flux; 3..5: its inviscid kernel alone; 6..8: its viscous kernel alone
+      if (arg < 0 || arg > 8) return OSTC_ERR_INVALID_ARG;
+      const int d = arg % 3, part = arg / 3;
+      if (part == 2 && !vis) return OSTC_ERR_INVALID_ARG;
       for (auto &z : ctx->dz)
         CK(dispatch_ns(ctx->ns, [&](auto n) {
-          return launch_flux<decltype(n)::value>(z, inv, arg, ctx->tile[arg], 1, vis, S(stream));
+          return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], 1, vis, part, S(stream));
         }));
       return OSTC_OK;
+    }
     case OSTC_OP_SOURCE: {
       CellArgs src;
       src.spec = ctx->spec_mech;
@@ -1047,13 +1051,23 @@ ostc_status ostc_step_kernel_count(ostc_ctx *ctx, int with_hist, int *count) {
 
 // tile-shape control for the autotuner: dir 0..2
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
-  if (!ctx || dir < 0 || dir > 2) return OSTC_ERR_INVALID_ARG;
+  if (!ctx || dir < 0 || dir > 5) return OSTC_ERR_INVALID_ARG;
   // rows may carry the register budget in its upper bits: rows | (minb << 8)
   const int minb = (rows >> 8) & 0xff;
   rows &= 0xff;
-  if (chunks < 1 || chunks > 4096 || minb < 0 || minb > 3) return OSTC_ERR_INVALID_ARG;
-  if (!(rows == 1 || rows == 2 || rows == 4 || rows == 8)) return OSTC_ERR_INVALID_ARG;
-  ctx->tile[dir] = {rows, chunks, minb < 1 ? 1 : minb};
+  TileShape &t = ctx->tile[dir % 3];
+  if (dir > 2 && rows == 0) {  // back to the fused kernel
+    t.vrows = 0;
+  } else {
+    if (chunks < 1 || chunks > 4096 || minb < 0 || minb > 4) return OSTC_ERR_INVALID_ARG;
+    if (!(rows == 1 || rows == 2 || rows == 4 || rows == 8)) return OSTC_ERR_INVALID_ARG;
+    if (minb == 4 && rows > 4) return OSTC_ERR_INVALID_ARG;  // the 168-register build takes <= 128 threads
+    if (dir > 2) {
+      t.vrows = rows, t.vchunks = chunks, t.vminb = minb < 1 ? 1 : minb;
+    } else {
+      t.rows = rows, t.chunks = chunks, t.minb = minb < 1 ? 1 : minb;
+    }
+  }
   for (auto &kv : ctx->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
@@ -1063,9 +1077,15 @@ ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
 }
 
 ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks) {
-  if (!ctx || dir < 0 || dir > 2 || !rows || !chunks) return OSTC_ERR_INVALID_ARG;
-  *rows = ctx->tile[dir].rows | (ctx->tile[dir].minb > 1 ? (ctx->tile[dir].minb << 8) : 0);
-  *chunks = ctx->tile[dir].chunks;
+  if (!ctx || dir < 0 || dir > 5 || !rows || !chunks) return OSTC_ERR_INVALID_ARG;
+  const TileShape &t = ctx->tile[dir % 3];
+  if (dir > 2) {
+    *rows = t.vrows == 0 ? 0 : (t.vrows | (t.vminb > 1 ? (t.vminb << 8) : 0));
+    *chunks = t.vrows == 0 ? 0 : t.vchunks;
+    return OSTC_OK;
+  }
+  *rows = t.rows | (t.minb > 1 ? (t.minb << 8) : 0);
+  *chunks = t.chunks;
   return OSTC_OK;
 }
 

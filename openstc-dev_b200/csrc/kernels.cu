@@ -1,7 +1,6 @@
-// kernels.cu — sm_100a kernels of the RHS / RK3 stage.
+// kernels.cu — sm_100a kernels of the RHS / RK3 stage (the flux kernels,
+// flux_dir in flux.cuh, are built in flux0.cu and flux9.cu).
 //
-//  flux_dir<NS,INV,DIR>   fused inviscid + viscous flux difference along one
-//                         direction (InviscidScheme.cu, AWENO.cu, ViscousScheme.cuh)
 //  source_kernel<NS>      finite-rate chemistry source, starts dq (SourceTerm.cuh:11-37)
 //  update_rk_kernel<NS>   SSPRK3 stage update, cv -> bv/sv, T and p (RK.cuh:197-253)
 //  properties_kernel<NS>  cp, gamma, a, mu, kappa, rho*D, Mach over [-1, m] (FieldOperation.cuh:112-146)
@@ -9,11 +8,6 @@
 //  dt_kernel<NS>          local time step + block min + atomic min (TimeAdvanceFunc.cuh:50-100, .cu:155-201)
 //  bc_*_kernel            boundary conditions (BoundCond.cuh:52-210) and periodic wrap
 //  residual kernels       store_last_step / square of d(bv) / deterministic sums (Residual.cuh:57-161)
-//
-// Flux kernels march along the sweep direction: a CTA owns a segment of
-// S = R*C - 1 cells of 32 (or R) lines, computes the R*C faces that bound
-// them chunk by chunk, and carries the last face flux of each chunk into the
-// next, so every face is evaluated once and dq is touched once per direction.
 #include <cstdio>
 
 #include "common.cuh"
@@ -29,128 +23,6 @@ __constant__ DevParam c_p;
 #include "thermo.cuh"
 
 namespace ostc {
-
-// ---------------------------------------------------------------------------
-// flux kernels
-// ---------------------------------------------------------------------------
-template <int NS, int INV, int DIR>
-__device__ __forceinline__ void face_total(const DevZone &z, int g0, bool viscous, double *G) {
-  constexpr int NV = 5 + NS;
-  double Fi[NV];
-  if constexpr (INV == 1)
-    inviscid_face_aweno<DIR>(z, g0, Fi);
-  else if constexpr (INV == 2)
-    inviscid_face_roe<NS, DIR>(z, g0, Fi);
-  else
-    inviscid_face_pv<NS, DIR>(z, g0, Fi);
-  if (viscous) {
-    double Fv[NV];
-    viscous_face<NS, DIR>(z, g0, Fv);
-#pragma unroll
-    for (int l = 0; l < NV; ++l) G[l] = Fv[l] - Fi[l];
-  } else {
-#pragma unroll
-    for (int l = 0; l < NV; ++l) G[l] = -Fi[l];
-  }
-}
-
-// MINB = minimum resident CTAs of 256 threads per SM the register allocation
-// must allow (1: up to 255 registers; 2: 128 registers, with some spilling)
-template <int NS, int INV, int DIR, int MINB>
-__global__ void __launch_bounds__(256, MINB) flux_dir(DevZone z, int nchunk, int accumulate, int viscous) {
-  constexpr int NV = 5 + NS;
-  const int lane = threadIdx.x, row = threadIdx.y, R = blockDim.y;
-  const int n = DIR == 0 ? z.mx : (DIR == 1 ? z.my : z.mz);
-  const int cds_limit = n - 2 * z.ngg;  // quirk A4: no central correction on the last 2*ngg cells
-  const bool vis = viscous != 0;
-  if constexpr (DIR == 0) {
-    const int S = 32 * nchunk - 1;
-    const int c0 = blockIdx.x * S;
-    const int j = blockIdx.y * R + row, k = blockIdx.z;
-    const bool line_ok = j < z.my;
-    double carry[NV];
-#pragma unroll
-    for (int l = 0; l < NV; ++l) carry[l] = 0;
-    for (int ch = 0; ch < nchunk; ++ch) {
-      const int f = c0 - 1 + 32 * ch + lane;
-      const bool active = line_ok && f <= n - 1;
-      double G[NV];
-      if (active) {
-        face_total<NS, INV, DIR>(z, gidx(z, f, j, k), vis, G);
-      } else {
-#pragma unroll
-        for (int l = 0; l < NV; ++l) G[l] = 0;
-      }
-      double Gm[NV];
-#pragma unroll
-      for (int l = 0; l < NV; ++l) {
-        const double up = __shfl_up_sync(0xffffffffu, G[l], 1);
-        Gm[l] = lane == 0 ? carry[l] : up;
-        carry[l] = __shfl_sync(0xffffffffu, G[l], 31);
-      }
-      if (active && f >= c0 && f >= 0) {
-        double corr[5] = {0, 0, 0, 0, 0};
-        if constexpr (INV == 1) {
-          if (f < cds_limit) cds_correction<DIR>(z, gidx(z, f, j, k), corr);
-        }
-        double *dq = z.dq + qidx(z, f, j, k);
-#pragma unroll
-        for (int l = 0; l < NV; ++l) {
-          double d = G[l] - Gm[l];
-          if (INV == 1 && l < 5) d -= corr[l];
-          if (accumulate)
-            dq[l * z.qsz] += d;
-          else
-            dq[l * z.qsz] = d;
-        }
-      }
-    }
-  } else {
-    extern __shared__ double sG[];  // [R+1][NV][32]
-    const int S = R * nchunk - 1;
-    const int i = blockIdx.x * 32 + lane;
-    const int c0 = (DIR == 1 ? blockIdx.y : blockIdx.z) * S;
-    const int j_fixed = blockIdx.y, k_fixed = blockIdx.z;
-    const bool col_ok = i < z.mx;
-    for (int ch = 0; ch < nchunk; ++ch) {
-      const int f = c0 - 1 + R * ch + row;
-      const bool active = col_ok && f <= n - 1;
-      const int ci = i, cj = DIR == 1 ? f : j_fixed, ck = DIR == 2 ? f : k_fixed;
-      double G[NV];
-      if (active) {
-        face_total<NS, INV, DIR>(z, gidx(z, ci, cj, ck), vis, G);
-      } else {
-#pragma unroll
-        for (int l = 0; l < NV; ++l) G[l] = 0;
-      }
-#pragma unroll
-      for (int l = 0; l < NV; ++l) sG[((row + 1) * NV + l) * 32 + lane] = G[l];
-      __syncthreads();
-      if (active && f >= c0 && f >= 0 && !(ch == 0 && row == 0)) {
-        double corr[5] = {0, 0, 0, 0, 0};
-        if constexpr (INV == 1) {
-          if (f < cds_limit) cds_correction<DIR>(z, gidx(z, ci, cj, ck), corr);
-        }
-        double *dq = z.dq + qidx(z, ci, cj, ck);
-#pragma unroll
-        for (int l = 0; l < NV; ++l) {
-          double d = G[l] - sG[(row * NV + l) * 32 + lane];
-          if (INV == 1 && l < 5) d -= corr[l];
-          if (accumulate)
-            dq[l * z.qsz] += d;
-          else
-            dq[l * z.qsz] = d;
-        }
-      }
-      __syncthreads();
-      if (row == 0) {
-#pragma unroll
-        for (int l = 0; l < NV; ++l) sG[l * 32 + lane] = sG[(R * NV + l) * 32 + lane];
-      }
-      __syncthreads();
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // per-cell kernels
@@ -929,70 +801,6 @@ dim3 plane_grid(int nx, int ny, int nz, dim3 blk) {
 }
 }  // namespace
 
-template <int NS, int INV, int DIR, int MINB>
-static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, int accumulate, int viscous,
-                                 cudaStream_t s) {
-  constexpr int NV = 5 + NS;
-  const int R = t.rows, C = t.chunks;
-  dim3 blk(32, R);
-  dim3 grid;
-  size_t smem = 0;
-  if (DIR == 0) {
-    const int S = 32 * C - 1;
-    grid = dim3((z.mx + S - 1) / S, (z.my + R - 1) / R, z.mz);
-  } else {
-    const int S = R * C - 1;
-    smem = sizeof(double) * (R + 1) * NV * 32;
-    if (DIR == 1)
-      grid = dim3((z.mx + 31) / 32, (z.my + S - 1) / S, z.mz);
-    else
-      grid = dim3((z.mx + 31) / 32, z.my, (z.mz + S - 1) / S);
-  }
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(flux_dir<NS, INV, DIR, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  flux_dir<NS, INV, DIR, MINB><<<grid, blk, smem, s>>>(z, C, accumulate, viscous);
-  return cudaGetLastError();
-}
-
-template <int NS, int INV, int DIR>
-static cudaError_t launch_flux_t(const DevZone &z, const TileShape &t, int accumulate, int viscous,
-                                 cudaStream_t s) {
-  switch (t.minb) {
-    case 3: return launch_flux_m<NS, INV, DIR, 3>(z, t, accumulate, viscous, s);
-    case 2: return launch_flux_m<NS, INV, DIR, 2>(z, t, accumulate, viscous, s);
-    default: return launch_flux_m<NS, INV, DIR, 1>(z, t, accumulate, viscous, s);
-  }
-}
-
-template <int NS>
-cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, int accumulate, int viscous,
-                        cudaStream_t s) {
-  if constexpr (NS == 0) {
-    if (inv == 1) {
-      switch (dir) {
-        case 0: return launch_flux_t<0, 1, 0>(z, t, accumulate, viscous, s);
-        case 1: return launch_flux_t<0, 1, 1>(z, t, accumulate, viscous, s);
-        default: return launch_flux_t<0, 1, 2>(z, t, accumulate, viscous, s);
-      }
-    }
-  }
-  if (inv == 2) {
-    switch (dir) {
-      case 0: return launch_flux_t<NS, 2, 0>(z, t, accumulate, viscous, s);
-      case 1: return launch_flux_t<NS, 2, 1>(z, t, accumulate, viscous, s);
-      default: return launch_flux_t<NS, 2, 2>(z, t, accumulate, viscous, s);
-    }
-  }
-  switch (dir) {
-    case 0: return launch_flux_t<NS, 0, 0>(z, t, accumulate, viscous, s);
-    case 1: return launch_flux_t<NS, 0, 1>(z, t, accumulate, viscous, s);
-    default: return launch_flux_t<NS, 0, 2>(z, t, accumulate, viscous, s);
-  }
-}
-
 template <int NS>
 cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStream_t s) {
   const dim3 blk(32, 8);
@@ -1166,12 +974,15 @@ bool mechanism_is_h2air9(const int *reac_type, const int *stoi_f, const int *sto
   return true;
 }
 
+// this unit's parameters and those of the flux units (flux0.cu, flux9.cu)
 cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
-  return cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
+  cudaError_t e = cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = upload_param_flux0(p, s);
+  if (e == cudaSuccess) e = upload_param_flux9(p, s);
+  return e;
 }
 
 #define OSTC_INSTANTIATE(NS)                                                                                  \
-  template cudaError_t launch_flux<NS>(const DevZone &, int, int, const TileShape &, int, int, cudaStream_t); \
   template cudaError_t launch_cells<NS>(CellOp, const DevZone &, const CellArgs &, cudaStream_t);            \
   template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);                    \
   template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t); \

@@ -11,7 +11,13 @@ namespace ostc {
 struct TileShape {
   int rows;
   int chunks;
-  int minb = 1;  // register budget: 1 (<=255 regs), 2 (<=128) or 3 (<=80) CTAs of 256 threads per SM
+  int minb = 1;  // register budget: 1 (<=255 regs), 2 (<=128) or 3 (<=80) CTAs of 256 threads per SM,
+                 // 4 (<=168 regs, CTAs of at most 128 threads)
+  // viscous flow: vrows > 0 splits the face flux into an inviscid kernel
+  // (the shape above) and a viscous kernel of this shape
+  int vrows = 0;
+  int vchunks = 1;
+  int vminb = 1;
 };
 
 // one boundary face as the kernels see it
@@ -57,8 +63,10 @@ struct SteadyArgs {
   int final_div = 0;              // DPLUR sweep: write (dq0 + ...) / dt_local into dq_out
 };
 
+// part 0: the face flux of the flow; 1: its inviscid half alone; 2: its
+// viscous half alone (flux.cuh: launch_flux_t)
 template <int NS>
-cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, int accumulate, int viscous,
+cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, int accumulate, int viscous, int part,
                         cudaStream_t s);
 template <int NS>
 cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStream_t s);
@@ -83,6 +91,8 @@ cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, do
 cudaError_t prepare_chem_surrogate();
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
 cudaError_t upload_param(const DevParam &p, cudaStream_t s);
+cudaError_t upload_param_flux0(const DevParam &p, cudaStream_t s);  // flux0.cu
+cudaError_t upload_param_flux9(const DevParam &p, cudaStream_t s);  // flux9.cu
 // whether a mechanism has the structure of the generated mech_h2air9.cuh
 bool mechanism_is_h2air9(const int *reac_type, const int *stoi_f, const int *stoi_b, const int *reac_order, int nr,
                          int ns);

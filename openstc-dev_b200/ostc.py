@@ -610,48 +610,81 @@ class Solver:
         check(lib().ostc_get_tile(self.ctx, d, C.byref(r), C.byref(c)), "ostc_get_tile")
         return r.value, c.value
 
+    def tiles(self):
+        """the six tile settings: fused/inviscid flux of x, y, z, then the
+        separate viscous flux of x, y, z ((0, 0) = fused)"""
+        return [self.get_tile(d) for d in range(6)]
+
+    def set_tiles(self, tiles):
+        for d, (r, c) in enumerate(tiles or []):
+            self.set_tile(d, r, c)
+
+    def _time_flux(self, arg, warmup, reps):
+        import torch
+
+        for _ in range(warmup):
+            self.launch_op(self.OP_FLUX, arg)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            self.launch_op(self.OP_FLUX, arg)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
     def autotune(self, warmup: int = 1, reps: int = 3, verbose: bool = False):
         """Pick per-direction flux tile shapes (rows, chunks, register budget)
         by timing each flux kernel with CUDA events on the launching stream.
-        Only dq is written, so the state is left as it was."""
-        import torch
-
+        For a viscous flow the fused kernel competes with the pair of
+        separate inviscid and viscous kernels, each tuned on its own. Only
+        dq is written, so the state is left as it was."""
         blk = self.blocks[0]
         ext = (blk.mx, blk.my, blk.mz)
+        viscous = self.scheme.viscous_order != 0
         best = {}
         for d in range(3):
             n = ext[d]
-            cands = []
-            rows_list = (2, 4, 8) if d == 0 else (4, 8)
-            for R in rows_list:
-                span = 32 if d == 0 else R
-                cmax = min(64, max(1, (n + 1 + span - 1) // span))
-                c = 1
-                while True:
-                    for minb in (1, 2, 3):
-                        cands.append((R | (minb << 8 if minb > 1 else 0), min(c, cmax)))
-                    if c >= cmax:
-                        break
-                    c *= 2
-            cands = sorted(set(cands))
-            times = []
-            for R, Cc in cands:
+
+            def cands(budgets):
+                out = []
+                for R in ((2, 4, 8) if d == 0 else (4, 8)):
+                    span = 32 if d == 0 else R
+                    cmax = min(64, max(1, (n + 1 + span - 1) // span))
+                    c = 1
+                    while True:
+                        for minb in budgets:
+                            if minb == 4 and R > 4:
+                                continue
+                            out.append((R | (minb << 8 if minb > 1 else 0), min(c, cmax)))
+                        if c >= cmax:
+                            break
+                        c *= 2
+                return sorted(set(out))
+
+            self.set_tile(d + 3, 0, 0)
+            fused = []
+            for R, Cc in cands((1, 2, 3, 4)):
                 self.set_tile(d, R, Cc)
-                for _ in range(warmup):
-                    self.launch_op(self.OP_FLUX, d)
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                for _ in range(reps):
-                    self.launch_op(self.OP_FLUX, d)
-                e1.record()
-                torch.cuda.synchronize()
-                times.append((e0.elapsed_time(e1) / reps, R, Cc))
-            times.sort()
-            best[d] = times[0]
-            self.set_tile(d, times[0][1], times[0][2])
+                fused.append((self._time_flux(d, warmup, reps), R, Cc))
+            fused.sort()
+            choice = (fused[0][0], fused[0][1:], (0, 0))
+            if viscous:
+                inv, vis = [], []
+                for R, Cc in cands((2, 3, 4)):
+                    self.set_tile(d, R, Cc)
+                    inv.append((self._time_flux(d + 3, warmup, reps), R, Cc))
+                    self.set_tile(d + 3, R, Cc)
+                    vis.append((self._time_flux(d + 6, warmup, reps), R, Cc))
+                inv.sort()
+                vis.sort()
+                if inv[0][0] + vis[0][0] < choice[0]:
+                    choice = (inv[0][0] + vis[0][0], inv[0][1:], vis[0][1:])
+            self.set_tile(d, *choice[1])
+            self.set_tile(d + 3, *choice[2])
+            best[d] = (choice[0], choice[1], choice[2])
             if verbose:
-                print("dir", d, "best", times[0], "of", len(times))
+                print("dir", d, "fused", fused[0], "chosen", best[d])
         return best
 
 
