@@ -426,6 +426,20 @@ ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg,
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks);
 ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks);
 
+/* Batched multi-block launches. on = 1: every block of the context is
+ * processed by one persistent launch per kernel (flux of each direction,
+ * source, stage update, properties, time step, conservative variables): the
+ * grid fills the device's resident CTA slots and walks a device tile table
+ * of {block, tile} entries built from the blocks' extents and the flux tile
+ * shapes. Results are identical to the per-block launches (on = 0, the
+ * default): every cell sees the same operations in the same order. Boundary
+ * faces and interfaces keep their per-face launches (their order matters,
+ * DataCommunication.cuh:30-49, BoundCond.cuh:673-822). At most 64 blocks:
+ * OSTC_ERR_UNSUPPORTED beyond. No reference counterpart: the reference
+ * launches every kernel per block (RK.cuh:107-161).                       */
+ostc_status ostc_set_batching(ostc_ctx *ctx, int on);
+ostc_status ostc_get_batching(const ostc_ctx *ctx, int *on);
+
 /* Launch one kernel family on every block (timing and autotuning aid):
  * OSTC_OP_FLUX (arg = direction, accumulates into dq; arg + 3: the inviscid
  * flux kernel alone, arg + 6: the viscous flux kernel alone), OSTC_OP_SOURCE,

@@ -37,6 +37,14 @@ struct ostc_ctx {
   std::vector<Iface> ifaces;
   std::vector<int> iface_zone, iface_target;
   TileShape tile[3] = {{4, 4, 1}, {8, 2, 1}, {8, 2, 1}};
+  // tile-table launches (ostc_set_batching): every zone in one persistent
+  // launch per kernel; tables of the interior, properties and ghosted cell
+  // ranges and of each flux direction (shape of tile[d], viscous shape)
+  int batched = 0;
+  int4 *tab_dev = nullptr;
+  size_t tab_cap = 0;
+  CellTable cell_tab[3];
+  FluxTable flux_tab[3][2];
   unsigned long long *dt_bits = nullptr;  // device dt (as bits)
   double *res_partial = nullptr;          // [n_part_total][4]
   int n_part_per_zone = 0;
@@ -81,10 +89,74 @@ ostc_status fail(ostc_ctx *c, ostc_status s, cudaError_t e = cudaSuccess) {
 ostc_status ensure_param(ostc_ctx *ctx, cudaStream_t s) {
   if (g_uploaded != ctx) {
     CK(upload_param(ctx->dp, s));
+    if (ctx->batched) CK(upload_zones(ctx->dz.data(), (int)ctx->dz.size(), s));
     g_uploaded = ctx;
   }
   return OSTC_OK;
 }
+
+// the tile tables of ctx (cell ranges and flux segments of every zone),
+// rebuilt when batching is switched on or a tile shape changes
+ostc_status build_tables(ostc_ctx *ctx) {
+  std::vector<int4> all;
+  std::vector<std::pair<size_t, size_t>> spans;  // [begin, end) of each table in `all`
+  auto cells = [&](int ext_add_xy, bool ghosted) {
+    const size_t b0 = all.size();
+    for (size_t b = 0; b < ctx->dz.size(); ++b) {
+      const DevZone &z = ctx->dz[b];
+      const int add = ghosted ? 2 * z.ngg : ext_add_xy;
+      const int ex = z.mx + add, ey = z.my + add, ez = z.mz + add;
+      const int gx = (ex + 31) / 32, gy = (ey + 7) / 8;
+      for (int bz = 0; bz < ez; ++bz)
+        for (int by = 0; by < gy; ++by)
+          for (int bx = 0; bx < gx; ++bx) all.push_back(make_int4((int)b, bx, by, bz));
+    }
+    spans.push_back({b0, all.size()});
+  };
+  cells(0, false);  // interior
+  cells(2, false);  // properties: [-1, m]
+  cells(0, true);   // ghosted
+  for (int d = 0; d < 3; ++d)
+    for (int v = 0; v < 2; ++v) {
+      const size_t b0 = all.size();
+      const TileShape &t = ctx->tile[d];
+      const int R = v ? t.vrows : t.rows, C = v ? t.vchunks : t.chunks;
+      if (R > 0)
+        for (size_t b = 0; b < ctx->dz.size(); ++b) {
+          const DevZone &z = ctx->dz[b];
+          if (d == 2 && z.mz <= 1) continue;
+          const dim3 g = flux_grid(z.mx, z.my, z.mz, d, R, C);
+          for (unsigned bz = 0; bz < g.z; ++bz)
+            for (unsigned by = 0; by < g.y; ++by)
+              for (unsigned bx = 0; bx < g.x; ++bx) all.push_back(make_int4((int)b, bx, by, bz));
+        }
+      spans.push_back({b0, all.size()});
+    }
+  if (all.size() > (size_t)INT32_MAX) return fail(ctx, OSTC_ERR_UNSUPPORTED);
+  if (all.size() > ctx->tab_cap) {
+    cudaFree(ctx->tab_dev);
+    ctx->tab_dev = nullptr;
+    ctx->tab_cap = 0;
+    CK(cudaMalloc(&ctx->tab_dev, sizeof(int4) * all.size()));
+    ctx->tab_cap = all.size();
+  }
+  if (!all.empty()) CK(cudaMemcpy(ctx->tab_dev, all.data(), sizeof(int4) * all.size(), cudaMemcpyHostToDevice));
+  auto table = [&](size_t q) {
+    FluxTable t;
+    t.tiles = ctx->tab_dev + spans[q].first;
+    t.n = (int)(spans[q].second - spans[q].first);
+    return t;
+  };
+  for (int c = 0; c < 3; ++c) ctx->cell_tab[c] = table(c);
+  for (int d = 0; d < 3; ++d)
+    for (int v = 0; v < 2; ++v) ctx->flux_tab[d][v] = table(3 + 2 * d + v);
+  return OSTC_OK;
+}
+
+// one per-cell kernel family over every zone: a tile-table launch when
+// batched (table: 0 interior, 1 properties range, 2 ghosted), else one
+// launch per zone
+ostc_status cells_all(ostc_ctx *ctx, CellOp op, int table, const CellArgs &a, cudaStream_t s);
 
 template <typename F>
 cudaError_t dispatch_ns(int ns, F &&f) {
@@ -93,6 +165,17 @@ cudaError_t dispatch_ns(int ns, F &&f) {
     case 9: return f(std::integral_constant<int, 9>{});
     default: return cudaErrorInvalidValue;
   }
+}
+
+ostc_status cells_all(ostc_ctx *ctx, CellOp op, int table, const CellArgs &a, cudaStream_t s) {
+  if (ctx->batched) {
+    CK(dispatch_ns(ctx->ns, [&](auto n) {
+      return launch_cells_table<decltype(n)::value>(op, ctx->cell_tab[table], a, s);
+    }));
+    return OSTC_OK;
+  }
+  for (auto &z : ctx->dz) CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(op, z, a, s); }));
+  return OSTC_OK;
 }
 
 // repack the reference's 80-byte gxl::Matrix<real,3,3,1> records into 9 planes
@@ -497,6 +580,7 @@ ostc_status ostc_destroy(ostc_ctx *ctx) {
   for (double *p : ctx->met_soa) cudaFree(p);
   for (void *p : ctx->owned) cudaFree(p);
   cudaFree(ctx->dt_bits);
+  cudaFree(ctx->tab_dev);
   cudaFree(ctx->res_partial);
   cudaFree(ctx->hist_counter);
   cudaFree(ctx->hist_res);
@@ -521,9 +605,7 @@ const double *ostc_dt_device(const ostc_ctx *ctx) { return ctx ? (const double *
 ostc_status ostc_compute_cv_from_bv(ostc_ctx *ctx, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;
   if (ensure_param(ctx, S(stream))) return ctx->last;
-  for (auto &z : ctx->dz)
-    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::CvFromBv, z, {}, S(stream)); }));
-  return OSTC_OK;
+  return cells_all(ctx, CellOp::CvFromBv, 2, {}, S(stream));
 }
 
 ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream) {
@@ -531,18 +613,36 @@ ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream) {
   if (ensure_param(ctx, S(stream))) return ctx->last;
   const int inv = ctx->prm.inviscid_type;
   const int vis = ctx->prm.viscous_scheme != 0;
+  const bool source = ctx->has_source && ctx->cfg.chem_mode == 0;
+  CellArgs src;
+  src.spec = ctx->spec_mech;
+  if (ctx->batched) {
+    // every zone per launch: the same per-cell order (source, x, y, z) as below
+    for (auto &z : ctx->dz)
+      if (z.qt != 0) CK(cudaMemsetAsync(z.dq, 0, sizeof(double) * z.qsz * ctx->prm.n_var, S(stream)));
+    const bool acc = ctx->dz[0].qt != 0 || source;
+    if (source) {
+      ostc_status st = cells_all(ctx, CellOp::Source, 0, src, S(stream));
+      if (st) return st;
+    }
+    for (int d = 0; d < 3; ++d)
+      CK(dispatch_ns(ctx->ns, [&](auto n) {
+        return launch_flux<decltype(n)::value>(ctx->dz[0], inv, d, ctx->tile[d], ctx->flux_tab[d],
+                                               (acc || d > 0) ? 1 : 0, vis, 0, S(stream));
+      }));
+    return OSTC_OK;
+  }
   for (auto &z : ctx->dz) {
     if (z.qt != 0) CK(cudaMemsetAsync(z.dq, 0, sizeof(double) * z.qsz * ctx->prm.n_var, S(stream)));
     bool acc = z.qt != 0;
-    if (ctx->has_source && ctx->cfg.chem_mode == 0) {
-      CellArgs src;
-      src.spec = ctx->spec_mech;
+    if (source) {
       CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, src, S(stream)); }));
       acc = true;
     }
     for (int d = 0; d < (z.mz > 1 ? 3 : 2); ++d) {
       CK(dispatch_ns(ctx->ns, [&](auto n) {
-        return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], (acc || d > 0) ? 1 : 0, vis, 0, S(stream));
+        return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], nullptr, (acc || d > 0) ? 1 : 0, vis, 0,
+                                               S(stream));
       }));
     }
   }
@@ -555,8 +655,8 @@ ostc_status ostc_global_time_step(ostc_ctx *ctx, double *dt_host, void *stream) 
   CellArgs a;
   a.dt_bits = ctx->dt_bits;
   CK(launch_cells<0>(CellOp::DtReset, ctx->dz[0], a, S(stream)));
-  for (auto &z : ctx->dz)
-    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Dt, z, a, S(stream)); }));
+  ostc_status st = cells_all(ctx, CellOp::Dt, 0, a, S(stream));
+  if (st) return st;
   if (dt_host) {
     CK(cudaMemcpyAsync(dt_host, ctx->dt_bits, sizeof(double), cudaMemcpyDeviceToHost, S(stream)));
     CK(cudaStreamSynchronize(S(stream)));
@@ -571,9 +671,7 @@ ostc_status ostc_update_cv_and_bv_rk(ostc_ctx *ctx, double dt, int rk, void *str
   a.dt = dt;
   a.dt_dev = dt < 0 ? (const double *)ctx->dt_bits : nullptr;
   a.rk = rk;
-  for (auto &z : ctx->dz)
-    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::UpdateRK, z, a, S(stream)); }));
-  return OSTC_OK;
+  return cells_all(ctx, CellOp::UpdateRK, 0, a, S(stream));
 }
 
 ostc_status ostc_apply_boundary_conditions(ostc_ctx *ctx, int with_cv, void *stream) {
@@ -662,9 +760,7 @@ ostc_status ostc_set_interfaces(ostc_ctx *ctx, const ostc_interface *f, int n) {
 ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;
   if (ensure_param(ctx, S(stream))) return ctx->last;
-  for (auto &z : ctx->dz)
-    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Properties, z, {}, S(stream)); }));
-  return OSTC_OK;
+  return cells_all(ctx, CellOp::Properties, 1, {}, S(stream));
 }
 
 ostc_status ostc_initialize(ostc_ctx *ctx, void *stream) {
@@ -673,8 +769,7 @@ ostc_status ostc_initialize(ostc_ctx *ctx, void *stream) {
   if ((st = repack_metrics(ctx, S(stream)))) return st;
   if ((st = ostc_apply_boundary_conditions(ctx, 0, stream))) return st;
   if (ensure_param(ctx, S(stream))) return ctx->last;
-  for (auto &z : ctx->dz)
-    CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Velocity, z, {}, S(stream)); }));
+  if ((st = cells_all(ctx, CellOp::Velocity, 2, {}, S(stream)))) return st;
   if ((st = ostc_data_communication(ctx, 0, stream))) return st;
   if ((st = ostc_update_physical_properties(ctx, stream))) return st;
   return ostc_compute_cv_from_bv(ctx, stream);
@@ -698,8 +793,7 @@ ostc_status ostc_rk3_stage(ostc_ctx *ctx, int rk, void *stream) {
 // one full step as enqueued work (captured into a graph by ostc_rk3_steps)
 static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
   ostc_status st;
-  if (with_hist)
-    for (auto &z : ctx->dz) CK(launch_cells<0>(CellOp::StoreLast, z, {}, s));
+  if (with_hist && (st = cells_all(ctx, CellOp::StoreLast, 0, {}, s))) return st;
   for (auto &z : ctx->dz)
     CK(cudaMemcpyAsync(z.qn, z.cv, sizeof(double) * z.sz * ctx->prm.n_var, cudaMemcpyDeviceToDevice, s));
   for (int rk = 0; rk < 3; ++rk)
@@ -1007,18 +1101,23 @@ ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream) {
       if (arg < 0 || arg > 8) return OSTC_ERR_INVALID_ARG;
       const int d = arg % 3, part = arg / 3;
       if (part == 2 && !vis) return OSTC_ERR_INVALID_ARG;
+      if (ctx->batched) {
+        CK(dispatch_ns(ctx->ns, [&](auto n) {
+          return launch_flux<decltype(n)::value>(ctx->dz[0], inv, d, ctx->tile[d], ctx->flux_tab[d], 1, vis, part,
+                                                 S(stream));
+        }));
+        return OSTC_OK;
+      }
       for (auto &z : ctx->dz)
         CK(dispatch_ns(ctx->ns, [&](auto n) {
-          return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], 1, vis, part, S(stream));
+          return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], nullptr, 1, vis, part, S(stream));
         }));
       return OSTC_OK;
     }
     case OSTC_OP_SOURCE: {
       CellArgs src;
       src.spec = ctx->spec_mech;
-      for (auto &z : ctx->dz)
-        CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, src, S(stream)); }));
-      return OSTC_OK;
+      return cells_all(ctx, CellOp::Source, 0, src, S(stream));
     }
     case OSTC_OP_PROPERTIES: return ostc_update_physical_properties(ctx, stream);
     case OSTC_OP_UPDATE: return ostc_update_cv_and_bv_rk(ctx, ctx->cfg.fixed_time_step ? ctx->cfg.dt : -1, arg, stream);
@@ -1073,6 +1172,26 @@ ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
   ctx->graphs.clear();
+  if (ctx->batched) return build_tables(ctx);
+  return OSTC_OK;
+}
+
+ostc_status ostc_set_batching(ostc_ctx *ctx, int on) {
+  if (!ctx || (on != 0 && on != 1)) return OSTC_ERR_INVALID_ARG;
+  if (on && ctx->dz.size() > (size_t)kMaxTableZones) return OSTC_ERR_UNSUPPORTED;
+  ctx->batched = on;
+  for (auto &kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  ctx->graphs.clear();
+  g_uploaded = nullptr;  // the next launch uploads this context's zone table
+  return on ? build_tables(ctx) : OSTC_OK;
+}
+
+ostc_status ostc_get_batching(const ostc_ctx *ctx, int *on) {
+  if (!ctx || !on) return OSTC_ERR_INVALID_ARG;
+  *on = ctx->batched;
   return OSTC_OK;
 }
 

@@ -55,9 +55,10 @@ struct FluxBounds {
 
 // PART selects the fused face flux or one of its halves (face_total); the
 // viscous half (PART 2) does not depend on INV and is built for INV 0 only
-template <int NS, int INV, int DIR, int MINB, int PART>
-__global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::blocks)
-    flux_dir(DevZone z, int nchunk, int accumulate, int viscous) {
+// the work of one CTA: segment (bx, by, bz) of zone z
+template <int NS, int INV, int DIR, int PART>
+__device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const int by, const int bz, int nchunk,
+                                          int accumulate, int viscous) {
   constexpr int NV = 5 + NS;
   constexpr bool CDS = INV == 1 && PART != 2;  // AWENO's central correction belongs to the inviscid flux
   const int lane = threadIdx.x, row = threadIdx.y, R = blockDim.y;
@@ -66,8 +67,8 @@ __global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::b
   const bool vis = viscous != 0;
   if constexpr (DIR == 0) {
     const int S = 32 * nchunk - 1;
-    const int c0 = blockIdx.x * S;
-    const int j = blockIdx.y * R + row, k = blockIdx.z;
+    const int c0 = bx * S;
+    const int j = by * R + row, k = bz;
     const bool line_ok = j < z.my;
     // the last face flux of the previous chunk of each row (lane 31 -> lane 0)
     __shared__ double carry[8][NV];
@@ -116,9 +117,9 @@ __global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::b
   } else {
     extern __shared__ double sG[];  // [R+1][NV][32]
     const int S = R * nchunk - 1;
-    const int i = blockIdx.x * 32 + lane;
-    const int c0 = (DIR == 1 ? blockIdx.y : blockIdx.z) * S;
-    const int j_fixed = blockIdx.y, k_fixed = blockIdx.z;
+    const int i = bx * 32 + lane;
+    const int c0 = (DIR == 1 ? by : bz) * S;
+    const int j_fixed = by, k_fixed = bz;
     const bool col_ok = i < z.mx;
     for (int ch = 0; ch < nchunk; ++ch) {
       const int f = c0 - 1 + R * ch + row;
@@ -160,88 +161,115 @@ __global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::b
   }
 }
 
+template <int NS, int INV, int DIR, int MINB, int PART>
+__global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::blocks)
+    flux_dir(DevZone z, int nchunk, int accumulate, int viscous) {
+  flux_tile<NS, INV, DIR, PART>(z, blockIdx.x, blockIdx.y, blockIdx.z, nchunk, accumulate, viscous);
+}
+
+// all zones of the context in one launch: a persistent grid walks the tile
+// table of {zone, bx, by, bz} segments (zones in c_zones)
+template <int NS, int INV, int DIR, int MINB, int PART>
+__global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::blocks)
+    flux_dir_table(const int4 *tiles, int n_tiles, int nchunk, int accumulate, int viscous) {
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const int4 c = tiles[t];
+    flux_tile<NS, INV, DIR, PART>(c_zones[c.x], c.y, c.z, c.w, nchunk, accumulate, viscous);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host-side launchers (kernels.cuh)
 // ---------------------------------------------------------------------------
 template <int NS, int INV, int DIR, int MINB, int PART>
-static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, int accumulate, int viscous,
-                                 cudaStream_t s) {
+static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
+                                 int viscous, cudaStream_t s) {
   constexpr int NV = 5 + NS;
   const int R = t.rows, C = t.chunks;
   if (32 * R > FluxBounds<MINB>::threads) return cudaErrorInvalidConfiguration;
-  dim3 blk(32, R);
-  dim3 grid;
-  size_t smem = 0;
-  if (DIR == 0) {
-    const int S = 32 * C - 1;
-    grid = dim3((z.mx + S - 1) / S, (z.my + R - 1) / R, z.mz);
-  } else {
-    const int S = R * C - 1;
-    smem = sizeof(double) * (R + 1) * NV * 32;
-    if (DIR == 1)
-      grid = dim3((z.mx + 31) / 32, (z.my + S - 1) / S, z.mz);
-    else
-      grid = dim3((z.mx + 31) / 32, z.my, (z.mz + S - 1) / S);
-  }
+  const dim3 blk(32, R);
+  const size_t smem = DIR == 0 ? 0 : sizeof(double) * (R + 1) * NV * 32;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(flux_dir<NS, INV, DIR, MINB, PART>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = tab ? cudaFuncSetAttribute(flux_dir_table<NS, INV, DIR, MINB, PART>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                        : cudaFuncSetAttribute(flux_dir<NS, INV, DIR, MINB, PART>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  flux_dir<NS, INV, DIR, MINB, PART><<<grid, blk, smem, s>>>(z, C, accumulate, viscous);
+  if (!tab) {
+    flux_dir<NS, INV, DIR, MINB, PART><<<flux_grid(z.mx, z.my, z.mz, DIR, R, C), blk, smem, s>>>(z, C, accumulate,
+                                                                                                 viscous);
+    return cudaGetLastError();
+  }
+  if (tab->n <= 0) return cudaSuccess;
+  // persistent grid: every resident CTA slot of the device, no more than there are tiles
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flux_dir_table<NS, INV, DIR, MINB, PART>,
+                                                                32 * R, smem);
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const int slots = per_sm * sms;
+  if (slots <= 0) return cudaErrorInvalidConfiguration;
+  const int grid = tab->n < slots ? tab->n : slots;
+  flux_dir_table<NS, INV, DIR, MINB, PART><<<grid, blk, smem, s>>>(tab->tiles, tab->n, C, accumulate, viscous);
   return cudaGetLastError();
 }
 
 template <int NS, int INV, int DIR, int PART>
-static cudaError_t launch_flux_p(const DevZone &z, const TileShape &t, int accumulate, int viscous,
-                                 cudaStream_t s) {
+static cudaError_t launch_flux_p(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
+                                 int viscous, cudaStream_t s) {
   switch (t.minb) {
-    case 4: return launch_flux_m<NS, INV, DIR, 4, PART>(z, t, accumulate, viscous, s);
-    case 3: return launch_flux_m<NS, INV, DIR, 3, PART>(z, t, accumulate, viscous, s);
-    case 2: return launch_flux_m<NS, INV, DIR, 2, PART>(z, t, accumulate, viscous, s);
-    default: return launch_flux_m<NS, INV, DIR, 1, PART>(z, t, accumulate, viscous, s);
+    case 4: return launch_flux_m<NS, INV, DIR, 4, PART>(z, t, tab, accumulate, viscous, s);
+    case 3: return launch_flux_m<NS, INV, DIR, 3, PART>(z, t, tab, accumulate, viscous, s);
+    case 2: return launch_flux_m<NS, INV, DIR, 2, PART>(z, t, tab, accumulate, viscous, s);
+    default: return launch_flux_m<NS, INV, DIR, 1, PART>(z, t, tab, accumulate, viscous, s);
   }
 }
 
 // part 0: the face flux of the flow — the fused kernel, or (viscous flow with
 // a viscous tile set) the inviscid half followed by the viscous half, which
 // accumulates; part 1: the inviscid half alone; part 2: the viscous half
-// alone (tile t.vrows/vchunks/vminb, or t when no viscous tile is set)
+// alone (tile t.vrows/vchunks/vminb, or t when no viscous tile is set).
+// With tables (tab[0] for the shape t, tab[1] for the viscous shape) every
+// zone of the context is processed by one launch per kernel.
 template <int NS, int INV, int DIR>
-static cudaError_t launch_flux_t(const DevZone &z, const TileShape &t, int accumulate, int viscous, int part,
-                                 cudaStream_t s) {
+static cudaError_t launch_flux_t(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
+                                 int viscous, int part, cudaStream_t s) {
   const TileShape tv = t.vrows ? TileShape{t.vrows, t.vchunks, t.vminb} : TileShape{t.rows, t.chunks, t.minb};
-  if (part == 1) return launch_flux_p<NS, INV, DIR, 1>(z, t, accumulate, 0, s);
-  if (part == 2) return launch_flux_p<NS, 0, DIR, 2>(z, tv, accumulate, 1, s);
-  if (!viscous || t.vrows == 0) return launch_flux_p<NS, INV, DIR, 0>(z, t, accumulate, viscous, s);
-  cudaError_t e = launch_flux_p<NS, INV, DIR, 1>(z, t, accumulate, 0, s);
+  const FluxTable *tp = tab ? &tab[0] : nullptr;
+  const FluxTable *tq = tab ? (t.vrows ? &tab[1] : &tab[0]) : nullptr;
+  if (part == 1) return launch_flux_p<NS, INV, DIR, 1>(z, t, tp, accumulate, 0, s);
+  if (part == 2) return launch_flux_p<NS, 0, DIR, 2>(z, tv, tq, accumulate, 1, s);
+  if (!viscous || t.vrows == 0) return launch_flux_p<NS, INV, DIR, 0>(z, t, tp, accumulate, viscous, s);
+  cudaError_t e = launch_flux_p<NS, INV, DIR, 1>(z, t, tp, accumulate, 0, s);
   if (e != cudaSuccess) return e;
-  return launch_flux_p<NS, 0, DIR, 2>(z, tv, 1, 1, s);
+  return launch_flux_p<NS, 0, DIR, 2>(z, tv, tq, 1, 1, s);
 }
 
 template <int NS>
-cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, int accumulate, int viscous, int part,
-                        cudaStream_t s) {
+cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, const FluxTable *tab, int accumulate,
+                        int viscous, int part, cudaStream_t s) {
   if constexpr (NS == 0) {
     if (inv == 1) {
       switch (dir) {
-        case 0: return launch_flux_t<0, 1, 0>(z, t, accumulate, viscous, part, s);
-        case 1: return launch_flux_t<0, 1, 1>(z, t, accumulate, viscous, part, s);
-        default: return launch_flux_t<0, 1, 2>(z, t, accumulate, viscous, part, s);
+        case 0: return launch_flux_t<0, 1, 0>(z, t, tab, accumulate, viscous, part, s);
+        case 1: return launch_flux_t<0, 1, 1>(z, t, tab, accumulate, viscous, part, s);
+        default: return launch_flux_t<0, 1, 2>(z, t, tab, accumulate, viscous, part, s);
       }
     }
   }
   if (inv == 2) {
     switch (dir) {
-      case 0: return launch_flux_t<NS, 2, 0>(z, t, accumulate, viscous, part, s);
-      case 1: return launch_flux_t<NS, 2, 1>(z, t, accumulate, viscous, part, s);
-      default: return launch_flux_t<NS, 2, 2>(z, t, accumulate, viscous, part, s);
+      case 0: return launch_flux_t<NS, 2, 0>(z, t, tab, accumulate, viscous, part, s);
+      case 1: return launch_flux_t<NS, 2, 1>(z, t, tab, accumulate, viscous, part, s);
+      default: return launch_flux_t<NS, 2, 2>(z, t, tab, accumulate, viscous, part, s);
     }
   }
   switch (dir) {
-    case 0: return launch_flux_t<NS, 0, 0>(z, t, accumulate, viscous, part, s);
-    case 1: return launch_flux_t<NS, 0, 1>(z, t, accumulate, viscous, part, s);
-    default: return launch_flux_t<NS, 0, 2>(z, t, accumulate, viscous, part, s);
+    case 0: return launch_flux_t<NS, 0, 0>(z, t, tab, accumulate, viscous, part, s);
+    case 1: return launch_flux_t<NS, 0, 1>(z, t, tab, accumulate, viscous, part, s);
+    default: return launch_flux_t<NS, 0, 2>(z, t, tab, accumulate, viscous, part, s);
   }
 }
 

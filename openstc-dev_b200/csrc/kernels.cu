@@ -24,17 +24,20 @@ __constant__ DevParam c_p;
 
 namespace ostc {
 
+// the zones of tile-table launches (upload_zones)
+static __constant__ DevZone c_zones[kMaxTableZones];
+
 // ---------------------------------------------------------------------------
 // per-cell kernels
 // ---------------------------------------------------------------------------
 // SPEC = 1: the mechanism-specialised chemistry (mech_h2air9.cuh), for
 // contexts whose mechanism has that structure
 template <int NS, int SPEC>
-__global__ void __launch_bounds__(256) source_kernel(DevZone z) {
+__device__ __forceinline__ void source_cells(const DevZone &z, const int bx, const int by, const int bz) {
   constexpr int NV = 5 + NS;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz;
   if (i >= z.mx || j >= z.my) return;
   const int g = gidx(z, i, j, k);
   double *dq = z.dq + qidx(z, i, j, k);
@@ -53,6 +56,11 @@ __global__ void __launch_bounds__(256) source_kernel(DevZone z) {
     for (int l = 0; l < NS; ++l) dq[(5 + l) * z.qsz] = jc * om[l];
   }
   (void)NV;
+}
+
+template <int NS, int SPEC>
+__global__ void __launch_bounds__(256) source_kernel(DevZone z) {
+  source_cells<NS, SPEC>(z, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 
@@ -129,11 +137,11 @@ __constant__ double c_rk_b[3] = {0.0, 0.25, 2.0 / 3.0};
 __constant__ double c_rk_c[3] = {1.0, 0.25, 2.0 / 3.0};
 
 template <int NS>
-__global__ void __launch_bounds__(256) update_rk_kernel(DevZone z, double dt_in, const double *dt_dev, int rk) {
+__device__ __forceinline__ void update_rk_cells(const DevZone &z, const int bx, const int by, const int bz, double dt_in, const double *dt_dev, int rk) {
   constexpr int NV = 5 + NS;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz;
   if (i >= z.mx || j >= z.my) return;
   const double dt = dt_dev ? *dt_dev : dt_in;
   const int g = gidx(z, i, j, k);
@@ -196,10 +204,15 @@ __global__ void __launch_bounds__(256) update_rk_kernel(DevZone z, double dt_in,
 }
 
 template <int NS>
-__global__ void __launch_bounds__(256) properties_kernel(DevZone z) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
-  const int k = blockIdx.z - 1;
+__global__ void __launch_bounds__(256) update_rk_kernel(DevZone z, double dt_in, const double *dt_dev, int rk) {
+  update_rk_cells<NS>(z, blockIdx.x, blockIdx.y, blockIdx.z, dt_in, dt_dev, rk);
+}
+
+template <int NS>
+__device__ __forceinline__ void properties_cells(const DevZone &z, const int bx, const int by, const int bz) {
+  const int i = bx * blockDim.x + threadIdx.x - 1;
+  const int j = by * blockDim.y + threadIdx.y - 1;
+  const int k = bz - 1;
   if (i > z.mx || j > z.my) return;
   const int g = gidx(z, i, j, k);
   const double T = z.bv[5 * z.sz + g];
@@ -239,6 +252,11 @@ __global__ void __launch_bounds__(256) properties_kernel(DevZone z) {
 }
 
 template <int NS>
+__global__ void __launch_bounds__(256) properties_kernel(DevZone z) {
+  properties_cells<NS>(z, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <int NS>
 __device__ __forceinline__ void cv_from_bv_point(const DevZone &z, int g) {
   const double rho = z.bv[g], u = z.bv[z.sz + g], v = z.bv[2 * z.sz + g], w = z.bv[3 * z.sz + g];
   const double p = z.bv[4 * z.sz + g];
@@ -268,31 +286,40 @@ __device__ __forceinline__ void cv_from_bv_point(const DevZone &z, int g) {
 }
 
 template <int NS>
-__global__ void __launch_bounds__(256) cv_from_bv_kernel(DevZone z) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - z.ngg;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y - z.ngg;
-  const int k = blockIdx.z - z.ngg;
+__device__ __forceinline__ void cv_from_bv_cells(const DevZone &z, const int bx, const int by, const int bz) {
+  const int i = bx * blockDim.x + threadIdx.x - z.ngg;
+  const int j = by * blockDim.y + threadIdx.y - z.ngg;
+  const int k = bz - z.ngg;
   if (i >= z.mx + z.ngg || j >= z.my + z.ngg) return;
   cv_from_bv_point<NS>(z, gidx(z, i, j, k));
 }
 
-__global__ void __launch_bounds__(256) velocity_kernel(DevZone z) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x - z.ngg;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y - z.ngg;
-  const int k = blockIdx.z - z.ngg;
+template <int NS>
+__global__ void __launch_bounds__(256) cv_from_bv_kernel(DevZone z) {
+  cv_from_bv_cells<NS>(z, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+__device__ __forceinline__ void velocity_cells(const DevZone &z, const int bx, const int by, const int bz) {
+  const int i = bx * blockDim.x + threadIdx.x - z.ngg;
+  const int j = by * blockDim.y + threadIdx.y - z.ngg;
+  const int k = bz - z.ngg;
   if (i >= z.mx + z.ngg || j >= z.my + z.ngg) return;
   const int g = gidx(z, i, j, k);
   const double u = z.bv[z.sz + g], v = z.bv[2 * z.sz + g], w = z.bv[3 * z.sz + g];
   z.vel[g] = sqrt(u * u + v * v + w * w);
 }
 
+__global__ void __launch_bounds__(256) velocity_kernel(DevZone z) {
+  velocity_cells(z, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // local time step and global minimum; dt_bits holds the IEEE bits of a
 // positive double, whose unsigned order equals the numeric order
 template <int NS>
-__global__ void __launch_bounds__(256) dt_kernel(DevZone z, unsigned long long *dt_bits) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+__device__ __forceinline__ void dt_cells(const DevZone &z, const int bx, const int by, const int bz, unsigned long long *dt_bits) {
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz;
   double dtl = 1e6;
   if (i < z.mx && j < z.my) {
     const int g = gidx(z, i, j, k);
@@ -338,6 +365,12 @@ __global__ void __launch_bounds__(256) dt_kernel(DevZone z, unsigned long long *
     for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (tid == 0) atomicMin(dt_bits, (unsigned long long)__double_as_longlong(v));
   }
+  __syncthreads();  // wmin is reused by the next tile of a tile-table launch
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256) dt_kernel(DevZone z, unsigned long long *dt_bits) {
+  dt_cells<NS>(z, blockIdx.x, blockIdx.y, blockIdx.z, dt_bits);
 }
 
 __global__ void dt_reset_kernel(unsigned long long *dt_bits) {
@@ -731,16 +764,20 @@ __global__ void interface_kernel(DevZone z, DevZone t, Iface f, int with_cv) {
 // residual: store_last_step (TimeAdvanceFunc.cu:6-17), square of the change
 // and deterministic two-level sums (Residual.cuh:57-111, Residual.cu:49-89)
 // ---------------------------------------------------------------------------
-__global__ void store_last_kernel(DevZone z) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z;
+__device__ __forceinline__ void store_last_cells(const DevZone &z, const int bx, const int by, const int bz) {
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = bz;
   if (i >= z.mx || j >= z.my) return;
   const int g = gidx(z, i, j, k), n = nidx(z, i, j, k);
   z.bv_last[n] = z.bv[g];
   z.bv_last[z.nsz + n] = z.vel[g];
   z.bv_last[2 * z.nsz + n] = z.bv[4 * z.sz + g];
   z.bv_last[3 * z.nsz + n] = z.bv[5 * z.sz + g];
+}
+
+__global__ void store_last_kernel(DevZone z) {
+  store_last_cells(z, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // one partial sum of the 4 squared changes per CTA (256 threads, grid-stride)
@@ -785,6 +822,51 @@ __global__ void residual_final_kernel(const double *partial, int n_part, double 
   out[l] = sqrt(s / n_total);
 }
 
+// ---------------------------------------------------------------------------
+// tile-table form of the per-cell kernels: a persistent grid of 32 x 8
+// CTAs walks {zone, bx, by, bz} tiles of every zone (zones in c_zones)
+// ---------------------------------------------------------------------------
+template <class Op>
+__global__ void __launch_bounds__(256) cells_table_kernel(const int4 *tiles, int n_tiles, Op op) {
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const int4 c = tiles[t];
+    op(c_zones[c.x], c.y, c.z, c.w);
+  }
+}
+
+template <int NS, int SPEC>
+struct SourceOp {
+  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { source_cells<NS, SPEC>(z, bx, by, bz); }
+};
+template <int NS>
+struct UpdateOp {
+  double dt;
+  const double *dt_dev;
+  int rk;
+  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const {
+    update_rk_cells<NS>(z, bx, by, bz, dt, dt_dev, rk);
+  }
+};
+template <int NS>
+struct PropertiesOp {
+  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { properties_cells<NS>(z, bx, by, bz); }
+};
+template <int NS>
+struct CvOp {
+  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { cv_from_bv_cells<NS>(z, bx, by, bz); }
+};
+struct VelocityOp {
+  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { velocity_cells(z, bx, by, bz); }
+};
+template <int NS>
+struct DtOp {
+  unsigned long long *dt_bits;
+  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { dt_cells<NS>(z, bx, by, bz, dt_bits); }
+};
+struct StoreLastOp {
+  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { store_last_cells(z, bx, by, bz); }
+};
+
 }  // namespace ostc
 
 #include "steady.cuh"
@@ -799,7 +881,46 @@ namespace {
 dim3 plane_grid(int nx, int ny, int nz, dim3 blk) {
   return dim3((nx + blk.x - 1) / blk.x, (ny + blk.y - 1) / blk.y, nz);
 }
+
+// persistent launch of cells_table_kernel<Op>: every resident CTA slot, at most one per tile
+template <class Op>
+cudaError_t launch_table(const CellTable &tab, const Op &op, cudaStream_t s) {
+  if (tab.n <= 0) return cudaSuccess;
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cells_table_kernel<Op>, 256, 0);
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const int slots = per_sm * sms;
+  if (slots <= 0) return cudaErrorInvalidConfiguration;
+  cells_table_kernel<Op><<<tab.n < slots ? tab.n : slots, dim3(32, 8), 0, s>>>(tab.tiles, tab.n, op);
+  return cudaGetLastError();
+}
 }  // namespace
+
+cudaError_t upload_zones(const DevZone *z, int n, cudaStream_t s) {
+  if (n < 0 || n > kMaxTableZones) return cudaErrorInvalidValue;
+  cudaError_t e = n ? cudaMemcpyToSymbolAsync(c_zones, z, sizeof(DevZone) * n, 0, cudaMemcpyHostToDevice, s)
+                    : cudaSuccess;
+  if (e == cudaSuccess) e = upload_zones_flux0(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_flux9(z, n, s);
+  return e;
+}
+
+template <int NS>
+cudaError_t launch_cells_table(CellOp op, const CellTable &tab, const CellArgs &a, cudaStream_t s) {
+  switch (op) {
+    case CellOp::Source:
+      return a.spec ? launch_table(tab, SourceOp<NS, 1>{}, s) : launch_table(tab, SourceOp<NS, 0>{}, s);
+    case CellOp::UpdateRK: return launch_table(tab, UpdateOp<NS>{a.dt, a.dt_dev, a.rk}, s);
+    case CellOp::Properties: return launch_table(tab, PropertiesOp<NS>{}, s);
+    case CellOp::CvFromBv: return launch_table(tab, CvOp<NS>{}, s);
+    case CellOp::Velocity: return launch_table(tab, VelocityOp{}, s);
+    case CellOp::Dt: return launch_table(tab, DtOp<NS>{a.dt_bits}, s);
+    case CellOp::StoreLast: return launch_table(tab, StoreLastOp{}, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
 
 template <int NS>
 cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStream_t s) {
@@ -984,6 +1105,7 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
 
 #define OSTC_INSTANTIATE(NS)                                                                                  \
   template cudaError_t launch_cells<NS>(CellOp, const DevZone &, const CellArgs &, cudaStream_t);            \
+  template cudaError_t launch_cells_table<NS>(CellOp, const CellTable &, const CellArgs &, cudaStream_t);    \
   template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);                    \
   template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t); \
   template cudaError_t launch_steady<NS>(SteadyOp, const DevZone &, const SteadyArgs &, const BcFace *, cudaStream_t); \

@@ -20,6 +20,28 @@ struct TileShape {
   int vminb = 1;
 };
 
+// tile-table launches: all zones of a context in one persistent launch per
+// kernel; the zones live in a __constant__ table of each kernel unit
+constexpr int kMaxTableZones = 64;
+
+// a device array of {zone, bx, by, bz} CTA tiles
+struct FluxTable {
+  const int4 *tiles = nullptr;
+  int n = 0;
+};
+using CellTable = FluxTable;
+
+// grid of one flux-direction kernel over a zone of mx x my x mz cells
+inline dim3 flux_grid(int mx, int my, int mz, int dir, int R, int C) {
+  if (dir == 0) {
+    const int S = 32 * C - 1;
+    return dim3((mx + S - 1) / S, (my + R - 1) / R, mz);
+  }
+  const int S = R * C - 1;
+  if (dir == 1) return dim3((mx + 31) / 32, (my + S - 1) / S, mz);
+  return dim3((mx + 31) / 32, my, (mz + S - 1) / S);
+}
+
 // one boundary face as the kernels see it
 struct BcFace {
   int type, face, direction;
@@ -64,12 +86,24 @@ struct SteadyArgs {
 };
 
 // part 0: the face flux of the flow; 1: its inviscid half alone; 2: its
-// viscous half alone (flux.cuh: launch_flux_t)
+// viscous half alone (flux.cuh: launch_flux_t). tab = nullptr: zone z alone;
+// else tab[0] (shape t) and tab[1] (viscous shape) hold the tiles of every
+// zone of the uploaded table and z is not used
 template <int NS>
-cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, int accumulate, int viscous, int part,
-                        cudaStream_t s);
+cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, const FluxTable *tab, int accumulate,
+                        int viscous, int part, cudaStream_t s);
 template <int NS>
 cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStream_t s);
+// the per-cell kernels of Source, UpdateRK, Properties, CvFromBv, Velocity,
+// Dt and StoreLast over a tile table of (32 x 8)-thread tiles; the table's
+// extents per zone: interior (mx, my, mz) for Source, UpdateRK, Dt,
+// StoreLast; (mx+2, my+2, mz+2) for Properties; ghosted for CvFromBv, Velocity
+template <int NS>
+cudaError_t launch_cells_table(CellOp op, const CellTable &tab, const CellArgs &a, cudaStream_t s);
+// the zone tables of every kernel unit
+cudaError_t upload_zones(const DevZone *z, int n, cudaStream_t s);
+cudaError_t upload_zones_flux0(const DevZone *z, int n, cudaStream_t s);  // flux0.cu
+cudaError_t upload_zones_flux9(const DevZone *z, int n, cudaStream_t s);  // flux9.cu
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s);
 template <int NS>

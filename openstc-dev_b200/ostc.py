@@ -125,6 +125,8 @@ def lib():
             "ostc_get_error": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)],
             "ostc_set_tile": [vp, i, i, i],
             "ostc_get_tile": [vp, i, C.POINTER(i), C.POINTER(i)],
+            "ostc_set_batching": [vp, i],
+            "ostc_get_batching": [vp, C.POINTER(i)],
             "ostc_launch_op": [vp, i, i, vp],
             "ostc_set_interfaces": [vp, C.POINTER(IfaceC), i],
             "ostc_step_kernel_count": [vp, i, C.POINTER(i)],
@@ -601,6 +603,16 @@ class Solver:
         n = C.c_int()
         check(lib().ostc_step_kernel_count(self.ctx, int(with_hist), C.byref(n)), "ostc_step_kernel_count")
         return n.value
+
+    def set_batching(self, on: bool):
+        """one persistent tile-table launch per kernel over all blocks (True)
+        or one launch per block (False)"""
+        check(lib().ostc_set_batching(self.ctx, int(bool(on))), "ostc_set_batching")
+
+    def batching(self) -> bool:
+        v = C.c_int()
+        check(lib().ostc_get_batching(self.ctx, C.byref(v)), "ostc_get_batching")
+        return bool(v.value)
 
     def set_tile(self, d, rows, chunks):
         check(lib().ostc_set_tile(self.ctx, d, rows, chunks), "ostc_set_tile")
