@@ -431,8 +431,9 @@ ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks);
  * source, stage update, properties, time step, conservative variables): the
  * grid fills the device's resident CTA slots and walks a device tile table
  * of {block, tile} entries built from the blocks' extents and the flux tile
- * shapes. Results are identical to the per-block launches (on = 0, the
- * default): every cell sees the same operations in the same order. Boundary
+ * shapes. Results are identical to the per-block launches (on = 0): every
+ * cell sees the same operations in the same order. Default: on for 2 to 64
+ * blocks, off for one. Boundary
  * faces and interfaces keep their per-face launches (their order matters,
  * DataCommunication.cuh:30-49, BoundCond.cuh:673-822). At most 64 blocks:
  * OSTC_ERR_UNSUPPORTED beyond. No reference counterpart: the reference

@@ -566,6 +566,11 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
   CK(cudaMalloc(&c->hist_counter, sizeof(int)));
   CK(cudaDeviceSynchronize());
   default_tiles(ctx);
+  // several blocks: one tile-table launch per kernel over all of them
+  if (n_zones > 1 && n_zones <= kMaxTableZones) {
+    c->batched = 1;
+    if ((st = build_tables(ctx))) return st;
+  }
   *out = c.release();
   return OSTC_OK;
 }

@@ -926,6 +926,153 @@ def case_multiblock(nx=(20, 17, 13), ny=(15, 19), mz=8, dx=1e-3, reconstruction=
     return c
 
 
+def _partition(total, k, lo, hi, rng, fixed=()):
+    """k block sizes in points, each in [lo, hi], whose shared-plane union
+    spans `total` points (sum - (k - 1) == total); fixed: {index: size}."""
+    fixed = dict(fixed)
+    for _ in range(10000):
+        sizes = [fixed.get(i, int(rng.integers(lo, hi + 1))) for i in range(k)]
+        free = [i for i in range(k) if i not in fixed]
+        short = total + k - 1 - sum(sizes)
+        for i in free:  # spread the difference over the free sizes
+            step = max(lo - sizes[i], min(hi - sizes[i], short))
+            sizes[i] += step
+            short -= step
+        if short == 0:
+            return sizes
+    raise ValueError("no partition of %d points into %d sizes in [%d, %d]" % (total, k, lo, hi))
+
+
+def block_layout(seed=37, n_layers=4, n_cols=3, rows=(3, 3, 3), extra_row=(1, 0), dims=(306, 200, 165),
+                 ranges=((16, 192), (16, 96), (16, 64)), anchors=True):
+    """Seeded uneven block layout of a box of dims points (shared planes):
+    n_layers layers in k, each split in i into n_cols columns (its own
+    split), each column split in j into rows[c] blocks (one more in the
+    column extra_row = (layer, column)). Block sizes lie in `ranges`; with
+    anchors, layer 0 holds a 16^3 block and layer 1 a 192 x 96 x 64 block.
+    Returns a list of ((i0, j0, k0), (mx, my, mz)) in global point indices."""
+    rng = np.random.default_rng(seed)
+    NX, NY, NZ = dims
+    (xlo, xhi), (ylo, yhi), (zlo, zhi) = ranges
+    zs = _partition(NZ, n_layers, zlo, zhi, rng, {0: 16, 1: 64} if anchors else {})
+    out = []
+    k0 = 0
+    for L in range(n_layers):
+        fx = ({0: 16} if L == 0 else ({1: 192} if L == 1 else {})) if anchors else {}
+        xs = _partition(NX, n_cols, xlo, xhi, rng, fx)
+        i0 = 0
+        for c in range(n_cols):
+            nr = rows[c] + (1 if (L, c) == tuple(extra_row) else 0)
+            fy = ({0: 16} if (L, c) == (0, 0) else ({0: 96} if (L, c) == (1, 1) else {})) if anchors else {}
+            ys = _partition(NY, nr, ylo, yhi, rng, fy)
+            j0 = 0
+            for r in range(nr):
+                out.append(((i0, j0, k0), (xs[c], ys[r], zs[L])))
+                j0 += ys[r] - 1
+            i0 += xs[c] - 1
+        k0 += zs[L] - 1
+    return out
+
+
+def case_uneven_blocks(seed=37, dx=1e-4, reconstruction=2, inviscid_scheme=4, mach=3.0, reynolds=1e7, T=300.0,
+                       layout=None) -> Case:
+    """Uneven multi-block air case: the seeded layout of block_layout (37
+    blocks from 16^3 to 192 x 96 x 64 joined by 1-to-1 interfaces, partial
+    faces where neighbouring splits differ) in a warped box. Mach 3 air at
+    Re = 1e7 / m (density from Sutherland's viscosity at T), a smooth
+    tanh(y / 20 dy) boundary-layer profile, supersonic inflow at i-min,
+    outflow at i-max, isothermal walls at T on every j-min block face (the
+    12 blocks of the bottom row), far field at j-max, symmetry in k. layout:
+    another block_layout (parity-sized runs). HLLC + MUSCL by default (the
+    variant the reference build runs), laminar viscous fluxes."""
+    s = Scheme(mix_model=MIX_AIR, inviscid_scheme=inviscid_scheme, reconstruction=reconstruction, viscous_order=2,
+               cfl=0.5)
+    ng = s.ngg
+    if layout is None:
+        layout = block_layout(seed)
+    for (_, e) in layout:
+        if min(e) < 2 * ng + 2:
+            raise ValueError("block too small for the stencil: %s" % (e,))
+    NX = max(o[0] + e[0] for o, e in layout)
+    NY = max(o[1] + e[1] for o, e in layout)
+    NZ = max(o[2] + e[2] for o, e in layout)
+    xg, yg, zg = grid_coordinates(NX, NY, NZ, ng + 1, dx, periodic_k=False)
+    a = math.sqrt(GAMMA_AIR * R_U / MW_AIR * T)
+    U = mach * a
+    mu = 1.716e-5 * (T / 273) ** 1.5 * (273 + 111) / (T + 111)
+    rho = reynolds * mu / U
+    p = rho * R_U / MW_AIR * T
+    ff = farfield_state(mach, T, p)
+    Ys = yg[1:-1, 1:-1, 1:-1]
+    prof = np.tanh(np.maximum(Ys, 0.0) / (20 * dx))
+    gbv = np.stack([np.full_like(Ys, rho), U * prof, 0 * Ys, 0 * Ys, np.full_like(Ys, p), np.full_like(Ys, T)])
+    blocks, faces, ifaces = [], [], []
+    for q, (o, e) in enumerate(layout):
+        mx, my, mz = e
+        b = HostBlock.allocate(mx, my, mz, ng, 5, 0)
+        i0, j0, k0 = o
+        sl = (slice(k0, k0 + mz + 2 * ng + 2), slice(j0, j0 + my + 2 * ng + 2), slice(i0, i0 + mx + 2 * ng + 2))
+        fill_metric(b, np.ascontiguousarray(xg[sl]), np.ascontiguousarray(yg[sl]), np.ascontiguousarray(zg[sl]))
+        b.arrays["bv"][...] = gbv[:, k0:k0 + mz + 2 * ng, j0:j0 + my + 2 * ng, i0:i0 + mx + 2 * ng]
+        blocks.append(b)
+    wall = dict(wall_isothermal=1, wall_temperature=T)
+    glob_hi = (NX - 1, NY - 1, NZ - 1)
+    for q, (o, e) in enumerate(layout):
+        lo = o
+        hi = tuple(o[d] + e[d] - 1 for d in range(3))
+        for d in range(3):
+            for direction in (-1, 1):
+                plane = lo[d] if direction < 0 else hi[d]
+                if plane == (0 if direction < 0 else glob_hi[d]):
+                    if d == 0:
+                        faces.append(bc_face(q, BC_INFLOW if direction < 0 else BC_OUTFLOW, 0, direction, e, ng,
+                                             ff if direction < 0 else None))
+                    elif d == 1:
+                        faces.append(bc_face(q, BC_WALL, 1, -1, e, ng, wall) if direction < 0 else
+                                     bc_face(q, BC_FARFIELD, 1, 1, e, ng, ff))
+                    else:
+                        faces.append(bc_face(q, BC_SYMMETRY, 2, direction, e, ng))
+                    continue
+                # interior face: one interface patch per neighbour sharing this plane
+                for t, (ot, et) in enumerate(layout):
+                    if t == q:
+                        continue
+                    tlo = ot
+                    thi = tuple(ot[c] + et[c] - 1 for c in range(3))
+                    if (thi[d] if direction < 0 else tlo[d]) != plane:
+                        continue
+                    ov = []
+                    for c in range(3):
+                        if c == d:
+                            continue
+                        s0, s1 = max(lo[c], tlo[c]), min(hi[c], thi[c])
+                        ov.append((c, s0, s1))
+                    if any(s1 - s0 + 1 < 2 for _, s0, s1 in ov):
+                        continue
+                    f = IfaceC()
+                    f.block, f.target, f.face, f.direction = q, t, d, direction
+                    for c in range(3):
+                        f.loop_dir[c] = 1
+                        f.target_loop_dir[c] = 1
+                        f.src_tar[c] = c
+                    if direction > 0:
+                        f.range_start[d], f.range_end[d] = e[d] - 1, e[d] - 1 + ng
+                        f.target_start[d] = 0
+                    else:
+                        f.range_start[d], f.range_end[d] = -ng, 0
+                        f.target_start[d] = et[d] - 1 - ng
+                    f.n_point[d] = ng + 1
+                    for c, s0, s1 in ov:
+                        f.range_start[c], f.range_end[c] = s0 - lo[c], s1 - lo[c]
+                        f.target_start[c] = s0 - tlo[c]
+                        f.n_point[c] = s1 - s0 + 1
+                    ifaces.append(f)
+    c = Case("uneven_blocks_%d_air_%dcells" % (len(layout), sum(e[0] * e[1] * e[2] for _, e in layout)), s, None,
+             blocks, faces, 500)
+    c.interfaces = ifaces
+    return c
+
+
 def make_steady(case: Case, implicit_method: int = 0, chem_src_method: Optional[int] = None,
                 dplur_inner_step: int = 3, cfl: Optional[float] = None) -> Case:
     """The same blocks, faces and initial state advanced by the steady path
