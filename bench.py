@@ -39,7 +39,7 @@ def _args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mixing256", choices=["mixing256", "vortex128", "mixing96"],
+    ap.add_argument("--workload", default="mixing256", choices=["mixing256", "vortex128", "mixing96", "blocks37"],
                     help="mixing96: the 96^3 mixing layer the kernel profiles are captured on")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -67,7 +67,23 @@ def _make_case(name, full_host=False):
         return ostc.case_mixing_layer(256, 256, 256, full_host=full_host)
     if name == "mixing96":
         return ostc.case_mixing_layer(96, 96, 96, full_host=full_host)
+    if name == "blocks37":
+        return ostc.case_uneven_blocks()
     return ostc.case_vortex(128, 128, 8)
+
+
+def _scheme_text(case):
+    import ostc
+
+    sc = case.scheme
+    rec = {1: "first order", 2: "MUSCL(minmod)", 3: "NND2", 4: "AWENO5"}[sc.reconstruction]
+    inv = {1: "L-F", 2: "Roe", 3: "AUSM+", 4: "HLLC"}[sc.inviscid_scheme]
+    if sc.reconstruction == 4 and sc.inviscid_scheme == 2:
+        inv = "AUSM+"  # quirk A1
+    vis = "laminar" if sc.viscous_order else "inviscid"
+    chem = ", finite-rate chemistry" if case.mech is not None else ""
+    blocks = ", %d blocks" % len(case.blocks) if len(case.blocks) > 1 else ""
+    return "%s+%s, %s%s, SSPRK3 CFL %.1f%s" % (rec, inv, vis, chem, sc.cfl, blocks)
 
 
 # ---------------------------------------------------------------------------
@@ -146,10 +162,9 @@ def kernel_table(solver, case, reps=3):
 def algorithmic_bytes(name, case):
     """Minimum HBM bytes of one launch of a kernel family on this workload
     (each input plane read once, each output plane written once)."""
-    b = case.blocks[0]
     ns = case.mech.n_spec if case.mech else 0
     nv = 5 + ns
-    cells = b.mx * b.my * b.mz
+    cells = case.cells  # one launch covers every block (tile-table launches)
     props = 2 + (ns + 2 if ns else 0)  # mu, kappa (+ rho*D_k, cp, gamma)
     per_cell = {
         # state (bv 6, sv), geometry (9 metric + jac), properties read; dq read+written
@@ -186,7 +201,7 @@ def run_ours(a):
 
     case = _make_case(a.workload)
     blocks = [ostc.DeviceBlock(b) for b in case.blocks]
-    solver = ostc.Solver(case.scheme, case.mech, blocks, case.faces)
+    solver = ostc.Solver(case.scheme, case.mech, blocks, case.faces, interfaces=case.interfaces)
     solver.initialize()
     solver.autotune(warmup=1, reps=2)
     solver.initialize()  # autotuning ran RHS evaluations only; re-derive the same start state
@@ -216,6 +231,29 @@ def run_ours(a):
         ms = float(t.item())
     cells = case.cells
     value = cells * a.steps * world / (ms * 1e-3) / 1e6
+
+    # several blocks: the same steps with one launch per block instead of the
+    # tile-table launches (same tiles, same start state)
+    per_block = None
+    if len(case.blocks) > 1:
+        solver.initialize()
+        solver.set_batching(False)
+        solver.rk3_steps(max(a.warmup, 3))
+        torch.cuda.synchronize()
+        lpb = solver.step_kernel_count(False)
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record()
+        solver.rk3_steps(a.steps)
+        p1.record()
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        per_block = {"value": round(case.cells * a.steps / (pms * 1e-3) / 1e6, 2), "unit": "Mcell-updates/s",
+                     "ms_per_step": round(pms / a.steps, 4), "launches_per_step": lpb,
+                     "tile_table_speedup": round(pms / ms, 3)}
+        solver.set_batching(True)
+        solver.initialize()
+        solver.rk3_steps(1)
+        torch.cuda.synchronize()
 
     # per-kernel table and roofline of the dominant kernel (the family with the
     # largest share of the step; the three flux directions are one kernel template)
@@ -278,14 +316,15 @@ def run_ours(a):
                 "config": {"workload": case.name, "cells_per_gpu": cells,
                            "n_spec": case.mech.n_spec if case.mech else 0,
                            "n_reac": case.mech.n_reac if case.mech else 0,
-                           "scheme": "MUSCL(minmod)+AUSM+, laminar, finite-rate chemistry, SSPRK3 CFL %.1f"
-                                     % case.scheme.cfl if case.mech else "AWENO5+AUSM+, laminar, SSPRK3",
+                           "scheme": _scheme_text(case),
                            "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs larger than L2 (%.1f GB state), no flush" % (state_bytes(case) / 1e9)},
                 "gpu_launches": launches_per_step * a.steps, "launches_per_step": launches_per_step,
                 "tiles": tiles,
                 "clocks": ck, "roofline": roofline, "step_roofline": step_roofline, "kernels_ms": {k: round(v["ms"], 4) for k, v in ktab.items()},
                 "e2e": e2e, "cpu_baseline": cpu, "reference_cuda_build": refcuda, "surrogate_chem": surr}
+        if per_block is not None:
+            line["per_block_launches"] = per_block
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
@@ -378,9 +417,9 @@ def step_bytes_per_cell(case):
 
 
 def state_bytes(case):
-    b = case.blocks[0]
     ns = case.mech.n_spec if case.mech else 0
-    return 8.0 * (6 + ns + 10 + 2 * (5 + ns)) * (b.mx + 2 * b.ngg) * (b.my + 2 * b.ngg) * (b.mz + 2 * b.ngg)
+    return sum(8.0 * (6 + ns + 10 + 2 * (5 + ns)) * (b.mx + 2 * b.ngg) * (b.my + 2 * b.ngg) * (b.mz + 2 * b.ngg)
+               for b in case.blocks)
 
 
 def run_e2e(a, case, tiles=None):
@@ -392,29 +431,30 @@ def run_e2e(a, case, tiles=None):
 
     import ostc
 
-    host = case.blocks[0]
-    pinned = {n: torch.from_numpy(v.view(np.uint8).reshape(-1) if n == "metric" else v).pin_memory()
-              for n, v in host.arrays.items()}
-    blocks = [ostc.DeviceBlock(ostc.HostBlock(host.mx, host.my, host.mz, host.ngg, host.n_var, host.n_spec))]
-    out_bv = torch.empty_like(blocks[0].t["bv"], device="cpu").pin_memory()
-    out_sv = torch.empty_like(blocks[0].t["sv"], device="cpu").pin_memory()
+    pinned = [{n: torch.from_numpy(v.view(np.uint8).reshape(-1) if n == "metric" else v).pin_memory()
+               for n, v in host.arrays.items()} for host in case.blocks]
+    blocks = [ostc.DeviceBlock(ostc.HostBlock(h.mx, h.my, h.mz, h.ngg, h.n_var, h.n_spec)) for h in case.blocks]
+    out_bv = [torch.empty_like(b.t["bv"], device="cpu").pin_memory() for b in blocks]
+    out_sv = [torch.empty_like(b.t["sv"], device="cpu").pin_memory() for b in blocks]
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     h2d = 0
-    for n, t in pinned.items():
-        blocks[0].t[n].copy_(t.view(blocks[0].t[n].dtype).reshape(blocks[0].t[n].shape), non_blocking=True)
-        h2d += t.numel() * t.element_size()
-    solver = ostc.Solver(case.scheme, case.mech, blocks, case.faces)
+    for b, pin in zip(blocks, pinned):
+        for n, t in pin.items():
+            b.t[n].copy_(t.view(b.t[n].dtype).reshape(b.t[n].shape), non_blocking=True)
+            h2d += t.numel() * t.element_size()
+    solver = ostc.Solver(case.scheme, case.mech, blocks, case.faces, interfaces=case.interfaces)
     solver.set_tiles(tiles)
     solver.initialize()
     res, dts = solver.rk3_steps(a.steps, history=True)
-    out_bv.copy_(blocks[0].t["bv"], non_blocking=True)
-    out_sv.copy_(blocks[0].t["sv"], non_blocking=True)
+    for b, ob, os_ in zip(blocks, out_bv, out_sv):
+        ob.copy_(b.t["bv"], non_blocking=True)
+        os_.copy_(b.t["sv"], non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    d2h = out_bv.numel() * 8 + out_sv.numel() * 8 + res.size * 8 + dts.size * 8
+    d2h = sum(t.numel() * 8 for t in out_bv + out_sv) + res.size * 8 + dts.size * 8
     solver.close()
     assert np.all(np.isfinite(res)), "non-finite residual in the e2e run"
     return {"value": round(case.cells * a.steps / (ms * 1e-3) / 1e6, 2), "unit": "Mcell-updates/s",
@@ -445,6 +485,10 @@ def cpu_sample(a, budget_s=15.0):
     kind, Run = _cpu_engine()
     if a.workload == "mixing256":
         case = ostc.case_mixing_layer(64, 64, 64, full_host=True)
+    elif a.workload == "blocks37":
+        case = ostc.case_uneven_blocks(layout=ostc.block_layout(5, dims=(80, 64, 64), ranges=((16, 40), (16, 28),
+                                                                                              (16, 20)),
+                                                                anchors=False))
     else:
         case = ostc.case_vortex(128, 128, 8)
     r = Run(case)
@@ -517,8 +561,8 @@ def run_reference(a):
 
 
 def _make_case_name(w):
-    return {"mixing256": "mixing_layer_h2air_256x256x256", "mixing96": "mixing_layer_h2air_96x96x96"}.get(
-        w, "vortex_air_128x128x8")
+    return {"mixing256": "mixing_layer_h2air_256x256x256", "mixing96": "mixing_layer_h2air_96x96x96",
+            "blocks37": "uneven_blocks_37_air_10453312cells"}.get(w, "vortex_air_128x128x8")
 
 
 if __name__ == "__main__":
