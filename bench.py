@@ -433,7 +433,8 @@ def run_e2e(a, case, tiles=None):
 
     pinned = [{n: torch.from_numpy(v.view(np.uint8).reshape(-1) if n == "metric" else v).pin_memory()
                for n, v in host.arrays.items()} for host in case.blocks]
-    blocks = [ostc.DeviceBlock(ostc.HostBlock(h.mx, h.my, h.mz, h.ngg, h.n_var, h.n_spec)) for h in case.blocks]
+    blocks = [ostc.DeviceBlock(ostc.HostBlock(h.mx, h.my, h.mz, h.ngg, h.n_var, h.n_spec, n_turb=h.n_turb))
+              for h in case.blocks]
     out_bv = [torch.empty_like(b.t["bv"], device="cpu").pin_memory() for b in blocks]
     out_sv = [torch.empty_like(b.t["sv"], device="cpu").pin_memory() for b in blocks]
     torch.cuda.synchronize()

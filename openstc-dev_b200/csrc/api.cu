@@ -26,6 +26,7 @@ struct ostc_ctx {
   ostc_param prm{};
   DevParam dp{};
   int ns = 0;  // compile-time species count selecting the kernel instantiation
+  int nt = 0;  // turbulence scalars after the species (2 with SST)
   bool has_source = false;
   int spec_ok = 0;    // the mechanism has the structure of the generated chemistry code
   int spec_mech = 0;  // ... and the source kernel uses it
@@ -167,6 +168,17 @@ cudaError_t dispatch_ns(int ns, F &&f) {
   }
 }
 
+// the flux kernels of the context's build: species count and turbulence scalars
+cudaError_t flux_launch(const ostc_ctx *ctx, const DevZone &z, int d, const FluxTable *tab, int accumulate, int part,
+                        cudaStream_t s) {
+  const int inv = ctx->prm.inviscid_type;
+  const int vis = ctx->prm.viscous_scheme != 0;
+  if (ctx->nt == 2) return launch_flux_nt<0, 2>(z, inv, d, ctx->tile[d], tab, accumulate, vis, part, s);
+  return dispatch_ns(ctx->ns, [&](auto n) {
+    return launch_flux_nt<decltype(n)::value, 0>(z, inv, d, ctx->tile[d], tab, accumulate, vis, part, s);
+  });
+}
+
 ostc_status cells_all(ostc_ctx *ctx, CellOp op, int table, const CellArgs &a, cudaStream_t s) {
   if (ctx->batched) {
     CK(dispatch_ns(ctx->ns, [&](auto n) {
@@ -244,7 +256,17 @@ void fill_devzone(const ostc_zone &z, DevZone &d) {
 ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zone *zones, int n_zones,
                      const ostc_bc_face *faces, int n_faces) {
   if (!cfg || !p || !zones || n_zones <= 0 || (n_faces > 0 && !faces)) return OSTC_ERR_INVALID_ARG;
-  if (p->mix_model == OSTC_MIX_AIR) {
+  const bool sst = p->turbulence != 0;
+  if (sst) {
+    // k-omega SST (rans_model 2): air, RK3, primitive-variable reconstruction with AUSM+ or HLLC
+    if (p->rans_model != 2) return OSTC_ERR_UNSUPPORTED;
+    if (p->mix_model != OSTC_MIX_AIR || cfg->steady || cfg->chem_mode != 0) return OSTC_ERR_UNSUPPORTED;
+    if (p->inviscid_type != 0 || (p->inviscid_scheme != 3 && p->inviscid_scheme != 4)) return OSTC_ERR_UNSUPPORTED;
+    if (p->viscous_scheme == 0) return OSTC_ERR_UNSUPPORTED;
+    if (p->n_spec != 0 || p->n_scalar != 2 || p->n_var != 7 || p->i_turb_cv != 5) return OSTC_ERR_INVALID_ARG;
+    if (p->compressibility_correction < 0 || p->compressibility_correction > 3) return OSTC_ERR_INVALID_ARG;
+    if (!(p->Prt > 0)) return OSTC_ERR_INVALID_ARG;
+  } else if (p->mix_model == OSTC_MIX_AIR) {
     if (p->n_spec != 0 || p->n_var != 5 || p->n_scalar != 0) return OSTC_ERR_INVALID_ARG;
   } else if (p->mix_model == OSTC_MIX_MIXTURE || p->mix_model == OSTC_MIX_FR) {
     if (p->n_spec != 9) return OSTC_ERR_UNSUPPORTED;
@@ -253,7 +275,6 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
   } else {
     return OSTC_ERR_UNSUPPORTED;
   }
-  if (p->turbulence) return OSTC_ERR_UNSUPPORTED;
   if (p->inviscid_type == 1 && p->mix_model != OSTC_MIX_AIR) return OSTC_ERR_UNSUPPORTED;  // quirk A2
   if (p->inviscid_type == 1 && p->reconstruction != 4) return OSTC_ERR_INVALID_ARG;
   if (p->inviscid_type == 0 && p->inviscid_scheme == 1 && p->mix_model != OSTC_MIX_AIR) return OSTC_ERR_UNSUPPORTED;
@@ -285,6 +306,7 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
         !z.mul || !z.thermal_conductivity)
       return OSTC_ERR_INVALID_ARG;
     if (p->n_spec > 0 && (!z.sv || !z.rho_D || !z.gamma || !z.cp)) return OSTC_ERR_INVALID_ARG;
+    if (sst && (!z.sv || !z.mut || !z.turb_therm_cond || !z.wall_distance)) return OSTC_ERR_INVALID_ARG;
     if (cfg->steady && !z.dt_local) return OSTC_ERR_INVALID_ARG;
     if (cfg->steady && cfg->implicit_method == 1 && z.dq_ngg != 1) return OSTC_ERR_INVALID_ARG;  // Field.cu:213-221
     // int32 ghosted index space
@@ -341,6 +363,8 @@ void build_devparam(const ostc_param *p, DevParam &d) {
   d.gradP = p->gradPInDiffusionFlux;
   d.dimension = p->dimension;
   d.turbulence = p->turbulence;
+  d.sst = p->turbulence && p->rans_model == 2 ? 1 : 0;
+  d.comp_corr = d.sst ? p->compressibility_correction : 0;
   d.Pr = p->Pr;
   d.Prt = p->Prt;
   d.Sct = p->Sct;
@@ -460,6 +484,7 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
   c->prm = *param;
   build_devparam(param, c->dp);
   c->ns = param->n_spec;
+  c->nt = c->dp.sst ? 2 : 0;
   c->has_source = param->mix_model == OSTC_MIX_FR && c->dp.n_reac > 0;
   c->spec_ok = c->has_source && mechanism_is_h2air9(param->reac_type, param->stoi_f, param->stoi_b,
                                                     param->reac_order, param->n_reac, param->n_spec)
@@ -616,9 +641,8 @@ ostc_status ostc_compute_cv_from_bv(ostc_ctx *ctx, void *stream) {
 ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;
   if (ensure_param(ctx, S(stream))) return ctx->last;
-  const int inv = ctx->prm.inviscid_type;
-  const int vis = ctx->prm.viscous_scheme != 0;
-  const bool source = ctx->has_source && ctx->cfg.chem_mode == 0;
+  // the source kernel: finite-rate chemistry and / or the SST source with mut
+  const bool source = (ctx->has_source && ctx->cfg.chem_mode == 0) || ctx->nt > 0;
   CellArgs src;
   src.spec = ctx->spec_mech;
   if (ctx->batched) {
@@ -631,10 +655,7 @@ ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream) {
       if (st) return st;
     }
     for (int d = 0; d < 3; ++d)
-      CK(dispatch_ns(ctx->ns, [&](auto n) {
-        return launch_flux<decltype(n)::value>(ctx->dz[0], inv, d, ctx->tile[d], ctx->flux_tab[d],
-                                               (acc || d > 0) ? 1 : 0, vis, 0, S(stream));
-      }));
+      CK(flux_launch(ctx, ctx->dz[0], d, ctx->flux_tab[d], (acc || d > 0) ? 1 : 0, 0, S(stream)));
     return OSTC_OK;
   }
   for (auto &z : ctx->dz) {
@@ -644,12 +665,8 @@ ostc_status ostc_compute_rhs(ostc_ctx *ctx, void *stream) {
       CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_cells<decltype(n)::value>(CellOp::Source, z, src, S(stream)); }));
       acc = true;
     }
-    for (int d = 0; d < (z.mz > 1 ? 3 : 2); ++d) {
-      CK(dispatch_ns(ctx->ns, [&](auto n) {
-        return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], nullptr, (acc || d > 0) ? 1 : 0, vis, 0,
-                                               S(stream));
-      }));
-    }
+    for (int d = 0; d < (z.mz > 1 ? 3 : 2); ++d)
+      CK(flux_launch(ctx, z, d, nullptr, (acc || d > 0) ? 1 : 0, 0, S(stream)));
   }
   return OSTC_OK;
 }
@@ -775,6 +792,8 @@ ostc_status ostc_initialize(ostc_ctx *ctx, void *stream) {
   if ((st = ostc_apply_boundary_conditions(ctx, 0, stream))) return st;
   if (ensure_param(ctx, S(stream))) return ctx->last;
   if ((st = cells_all(ctx, CellOp::Velocity, 2, {}, S(stream)))) return st;
+  // SST: the initial turbulent viscosity over [-1, m] (Driver.cu:69-78)
+  if (ctx->nt > 0 && (st = cells_all(ctx, CellOp::InitMut, 1, {}, S(stream)))) return st;
   if ((st = ostc_data_communication(ctx, 0, stream))) return st;
   if ((st = ostc_update_physical_properties(ctx, stream))) return st;
   return ostc_compute_cv_from_bv(ctx, stream);
@@ -1107,16 +1126,10 @@ ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream) {
       const int d = arg % 3, part = arg / 3;
       if (part == 2 && !vis) return OSTC_ERR_INVALID_ARG;
       if (ctx->batched) {
-        CK(dispatch_ns(ctx->ns, [&](auto n) {
-          return launch_flux<decltype(n)::value>(ctx->dz[0], inv, d, ctx->tile[d], ctx->flux_tab[d], 1, vis, part,
-                                                 S(stream));
-        }));
+        CK(flux_launch(ctx, ctx->dz[0], d, ctx->flux_tab[d], 1, part, S(stream)));
         return OSTC_OK;
       }
-      for (auto &z : ctx->dz)
-        CK(dispatch_ns(ctx->ns, [&](auto n) {
-          return launch_flux<decltype(n)::value>(z, inv, d, ctx->tile[d], nullptr, 1, vis, part, S(stream));
-        }));
+      for (auto &z : ctx->dz) CK(flux_launch(ctx, z, d, nullptr, 1, part, S(stream)));
       return OSTC_OK;
     }
     case OSTC_OP_SOURCE: {

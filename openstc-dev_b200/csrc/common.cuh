@@ -24,7 +24,8 @@ constexpr int MAXR = OSTC_MAX_REAC;
 struct DevParam {
   int n_var, n_scalar, n_spec, n_reac;
   int mix, inviscid_scheme, reconstruction, limiter, inviscid_type, viscous_scheme;
-  int chemSrcMethod, gradP, dimension, turbulence, need_gibbs, pad_;
+  int chemSrcMethod, gradP, dimension, turbulence, need_gibbs, sst;  // sst: k-omega SST scalars in sv
+  int comp_corr, pad_;                                                // SST compressibility correction 0..3
   double Pr, Prt, Sct, Sc, cfl, entropy_fix_factor;
   double mw[MAXS], imw[MAXS], Rmw[MAXS];           // W_k, 1/W_k, R_u/W_k
   double lo[MAXS][7], hi[MAXS][7];                 // NASA-7 low / high ranges

@@ -7,6 +7,7 @@
 // always differ in i, so every load is a coalesced 32-wide row.
 #pragma once
 #include "common.cuh"
+#include "sst.cuh"
 #include "thermo.cuh"
 
 namespace ostc {
@@ -189,9 +190,10 @@ __device__ __forceinline__ void riemann(const double *pl, const double *pr, cons
 // primitive-variable reconstruction face (InviscidScheme.cu:48-158 +
 // Reconstruction.cu:5-46 + Reconstruction.cuh:20-72)
 // ---------------------------------------------------------------------------
-template <int NS, int DIR>
+// NT: turbulence scalars (k, omega) after the NS species, reconstructed alike
+template <int NS, int DIR, int NT = 0>
 __device__ __forceinline__ void reconstruct_pv(const DevZone &z, int g0, double *pl, double *pr) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = 5 + NS + NT;
   const int sd = dir_stride<DIR>(z);
   const int rec = c_p.reconstruction;
 #pragma unroll
@@ -257,11 +259,11 @@ __device__ __forceinline__ void reconstruct_pv(const DevZone &z, int g0, double 
   }
 }
 
-template <int NS, int DIR>
+template <int NS, int DIR, int NT = 0>
 __device__ __forceinline__ void inviscid_face_pv(const DevZone &z, int g0, double *F) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = 5 + NS + NT;
   double pl[NV + 2], pr[NV + 2];
-  reconstruct_pv<NS, DIR>(z, g0, pl, pr);
+  reconstruct_pv<NS, DIR, NT>(z, g0, pl, pr);
   riemann<NV, NS>(pl, pr, z, g0, g0 + dir_stride<DIR>(z), DIR, F);
 }
 
@@ -595,11 +597,13 @@ __device__ __forceinline__ void cds_correction(const DevZone &z, int g, double *
 }
 
 // ---------------------------------------------------------------------------
-// laminar viscous face flux (ViscousScheme.cuh:22-821, compute_{f,g,h}v_2nd_order)
+// viscous face flux (ViscousScheme.cuh:22-821, compute_{f,g,h}v_2nd_order);
+// NT = 2: the SST terms (turbulent viscosity and conductivity, the -2/3 rho k
+// normal stresses, k and omega diffusion with the F1 blend)
 // ---------------------------------------------------------------------------
-template <int NS, int DIR>
+template <int NS, int DIR, int NT = 0>
 __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = 5 + NS + NT;
   const int sd = dir_stride<DIR>(z);
   const int g1 = g0 + sd;
   // tangential strides
@@ -632,11 +636,22 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
   const double w_x = dw[0] * mm[0] + dw[1] * mm[3] + dw[2] * mm[6];
   const double w_y = dw[0] * mm[1] + dw[1] * mm[4] + dw[2] * mm[7];
   const double w_z = dw[0] * mm[2] + dw[1] * mm[5] + dw[2] * mm[8];
-  const double mu = 0.5 * (ld(z.mul + g0) + ld(z.mul + g1));
-  const double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) * (1.0 / 3);
-  const double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) * (1.0 / 3);
-  const double tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) * (1.0 / 3);
+  const double mul = 0.5 * (ld(z.mul + g0) + ld(z.mul + g1));
+  const double mut = NT > 0 ? 0.5 * (ld(z.mut + g0) + ld(z.mut + g1)) : 0.0;
+  const double mu = NT > 0 ? mul + mut : mul;
+  double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) * (1.0 / 3);
+  double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) * (1.0 / 3);
+  double tzz = mu * (4 * w_z - 2 * u_x - 2 * v_y) * (1.0 / 3);
   const double txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
+  if constexpr (NT > 0) {  // ViscousScheme.cuh:82-95
+    constexpr double delta_d = 1e-3;
+    const double dy_div_delta = fmin(0.5 * (ld(z.wall + g0) + ld(z.wall + g1)) / delta_d, 1.0);
+    const double twoThirdrhoKm =
+        -2.0 / 3 * 0.5 * (bvl(z, g0, 0) * svl(z, g0, NS) + bvl(z, g1, 0) * svl(z, g1, NS)) * dy_div_delta;
+    txx += twoThirdrhoKm;
+    tyy += twoThirdrhoKm;
+    tzz += twoThirdrhoKm;
+  }
   const double j0 = ld(z.jac + g0), j1 = ld(z.jac + g1);
   const double kxj = 0.5 * (met(z, g0, 3 * DIR) * j0 + met(z, g1, 3 * DIR) * j1);
   const double kyj = 0.5 * (met(z, g0, 3 * DIR + 1) * j0 + met(z, g1, 3 * DIR + 1) * j1);
@@ -651,7 +666,8 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
   const double t_x = dt[0] * mm[0] + dt[1] * mm[3] + dt[2] * mm[6];
   const double t_y = dt[0] * mm[1] + dt[1] * mm[4] + dt[2] * mm[7];
   const double t_z = dt[0] * mm[2] + dt[1] * mm[5] + dt[2] * mm[8];
-  const double cond = 0.5 * (ld(z.kappa + g0) + ld(z.kappa + g1));
+  double cond = 0.5 * (ld(z.kappa + g0) + ld(z.kappa + g1));
+  if constexpr (NT > 0) cond += 0.5 * (ld(z.ttc + g0) + ld(z.ttc + g1));
   F[4] = um * F[1] + vm * F[2] + wm * F[3] + cond * (kxj * t_x + kyj * t_y + kzj * t_z);
   if constexpr (NS > 0) {
     double yk[NS], diff[NS], ddf[NS];
@@ -696,6 +712,36 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
       F[5 + l] = flux;
       F[4] += h[l] * flux;
     }
+  }
+  if constexpr (NT > 0) {  // k and omega diffusion (ViscousScheme.cuh:200-251)
+    double dk[3], dw[3];
+    der(z.sv + NS * z.sz, dk);
+    der(z.sv + (NS + 1) * z.sz, dw);
+    const double k_x = dk[0] * mm[0] + dk[1] * mm[3] + dk[2] * mm[6];
+    const double k_y = dk[0] * mm[1] + dk[1] * mm[4] + dk[2] * mm[7];
+    const double k_z = dk[0] * mm[2] + dk[1] * mm[5] + dk[2] * mm[8];
+    const double omega_x = dw[0] * mm[0] + dw[1] * mm[3] + dw[2] * mm[6];
+    const double omega_y = dw[0] * mm[1] + dw[1] * mm[4] + dw[2] * mm[7];
+    const double omega_z = dw[0] * mm[2] + dw[1] * mm[5] + dw[2] * mm[8];
+    const double wall_dist = 0.5 * (ld(z.wall + g0) + ld(z.wall + g1));
+    double f1 = 1;
+    if (wall_dist > 1e-25) {
+      const double km = 0.5 * (svl(z, g0, NS) + svl(z, g1, NS));
+      const double omegam = 0.5 * (svl(z, g0, NS + 1) + svl(z, g1, NS + 1));
+      const double param1 = sqrt(km) / (0.09 * omegam * wall_dist);
+      const double rhom = 0.5 * (bvl(z, g0, 0) + bvl(z, g1, 0));
+      const double d2 = wall_dist * wall_dist;
+      const double param2 = 500 * mul / (rhom * d2 * omegam);
+      const double CDkomega =
+          fmax(1e-20, 2 * rhom * sst::sigma_omega2 / omegam * (k_x * omega_x + k_y * omega_y + k_z * omega_z));
+      const double param3 = 4 * rhom * sst::sigma_omega2 * km / (CDkomega * d2);
+      const double arg1 = fmin(fmax(param1, param2), param3);
+      f1 = tanh(arg1 * arg1 * arg1 * arg1);
+    }
+    const double sigma_k = sst::sigma_k2 + sst::delta_sigma_k * f1;
+    const double sigma_omega = sst::sigma_omega2 + sst::delta_sigma_omega * f1;
+    F[5 + NS] = (mul + mut * sigma_k) * (kxj * k_x + kyj * k_y + kzj * k_z);
+    F[6 + NS] = (mul + mut * sigma_omega) * (kxj * omega_x + kyj * omega_y + kzj * omega_z);
   }
   (void)NV;
 }

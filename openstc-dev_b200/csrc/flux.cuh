@@ -19,11 +19,14 @@ namespace ostc {
 // ---------------------------------------------------------------------------
 // PART 0: inviscid and (when `viscous`) viscous flux of the face;
 // PART 1: the inviscid flux alone; PART 2: the viscous flux alone
-template <int NS, int INV, int DIR, int PART>
+// NT: turbulence scalars after the species (2 for SST; primitive-variable
+// reconstruction only)
+template <int NS, int INV, int DIR, int PART, int NT>
 __device__ __forceinline__ void face_total(const DevZone &z, int g0, bool viscous, double *G) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = 5 + NS + NT;
+  static_assert(NT == 0 || INV == 0, "turbulence scalars take the primitive-variable reconstruction");
   if constexpr (PART == 2) {
-    viscous_face<NS, DIR>(z, g0, G);
+    viscous_face<NS, DIR, NT>(z, g0, G);
     return;
   }
   double Fi[NV];
@@ -32,10 +35,10 @@ __device__ __forceinline__ void face_total(const DevZone &z, int g0, bool viscou
   else if constexpr (INV == 2)
     inviscid_face_roe<NS, DIR>(z, g0, Fi);
   else
-    inviscid_face_pv<NS, DIR>(z, g0, Fi);
+    inviscid_face_pv<NS, DIR, NT>(z, g0, Fi);
   if (PART == 0 && viscous) {
     double Fv[NV];
-    viscous_face<NS, DIR>(z, g0, Fv);
+    viscous_face<NS, DIR, NT>(z, g0, Fv);
 #pragma unroll
     for (int l = 0; l < NV; ++l) G[l] = Fv[l] - Fi[l];
   } else {
@@ -56,10 +59,10 @@ struct FluxBounds {
 // PART selects the fused face flux or one of its halves (face_total); the
 // viscous half (PART 2) does not depend on INV and is built for INV 0 only
 // the work of one CTA: segment (bx, by, bz) of zone z
-template <int NS, int INV, int DIR, int PART>
+template <int NS, int INV, int DIR, int PART, int NT>
 __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const int by, const int bz, int nchunk,
                                           int accumulate, int viscous) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = 5 + NS + NT;
   constexpr bool CDS = INV == 1 && PART != 2;  // AWENO's central correction belongs to the inviscid flux
   const int lane = threadIdx.x, row = threadIdx.y, R = blockDim.y;
   const int n = DIR == 0 ? z.mx : (DIR == 1 ? z.my : z.mz);
@@ -81,7 +84,7 @@ __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const 
       const bool active = line_ok && f <= n - 1;
       double G[NV];
       if (active) {
-        face_total<NS, INV, DIR, PART>(z, gidx(z, f, j, k), vis, G);
+        face_total<NS, INV, DIR, PART, NT>(z, gidx(z, f, j, k), vis, G);
       } else {
 #pragma unroll
         for (int l = 0; l < NV; ++l) G[l] = 0;
@@ -127,7 +130,7 @@ __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const 
       const int ci = i, cj = DIR == 1 ? f : j_fixed, ck = DIR == 2 ? f : k_fixed;
       double G[NV];
       if (active) {
-        face_total<NS, INV, DIR, PART>(z, gidx(z, ci, cj, ck), vis, G);
+        face_total<NS, INV, DIR, PART, NT>(z, gidx(z, ci, cj, ck), vis, G);
       } else {
 #pragma unroll
         for (int l = 0; l < NV; ++l) G[l] = 0;
@@ -161,50 +164,50 @@ __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const 
   }
 }
 
-template <int NS, int INV, int DIR, int MINB, int PART>
+template <int NS, int INV, int DIR, int MINB, int PART, int NT>
 __global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::blocks)
     flux_dir(DevZone z, int nchunk, int accumulate, int viscous) {
-  flux_tile<NS, INV, DIR, PART>(z, blockIdx.x, blockIdx.y, blockIdx.z, nchunk, accumulate, viscous);
+  flux_tile<NS, INV, DIR, PART, NT>(z, blockIdx.x, blockIdx.y, blockIdx.z, nchunk, accumulate, viscous);
 }
 
 // all zones of the context in one launch: a persistent grid walks the tile
 // table of {zone, bx, by, bz} segments (zones in c_zones)
-template <int NS, int INV, int DIR, int MINB, int PART>
+template <int NS, int INV, int DIR, int MINB, int PART, int NT>
 __global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::blocks)
     flux_dir_table(const int4 *tiles, int n_tiles, int nchunk, int accumulate, int viscous) {
   for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
     const int4 c = tiles[t];
-    flux_tile<NS, INV, DIR, PART>(c_zones[c.x], c.y, c.z, c.w, nchunk, accumulate, viscous);
+    flux_tile<NS, INV, DIR, PART, NT>(c_zones[c.x], c.y, c.z, c.w, nchunk, accumulate, viscous);
   }
 }
 
 // ---------------------------------------------------------------------------
 // host-side launchers (kernels.cuh)
 // ---------------------------------------------------------------------------
-template <int NS, int INV, int DIR, int MINB, int PART>
+template <int NS, int INV, int DIR, int MINB, int PART, int NT>
 static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
                                  int viscous, cudaStream_t s) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = 5 + NS + NT;
   const int R = t.rows, C = t.chunks;
   if (32 * R > FluxBounds<MINB>::threads) return cudaErrorInvalidConfiguration;
   const dim3 blk(32, R);
   const size_t smem = DIR == 0 ? 0 : sizeof(double) * (R + 1) * NV * 32;
   if (smem > 48 * 1024) {
-    cudaError_t e = tab ? cudaFuncSetAttribute(flux_dir_table<NS, INV, DIR, MINB, PART>,
+    cudaError_t e = tab ? cudaFuncSetAttribute(flux_dir_table<NS, INV, DIR, MINB, PART, NT>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                        : cudaFuncSetAttribute(flux_dir<NS, INV, DIR, MINB, PART>,
+                        : cudaFuncSetAttribute(flux_dir<NS, INV, DIR, MINB, PART, NT>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
   if (!tab) {
-    flux_dir<NS, INV, DIR, MINB, PART><<<flux_grid(z.mx, z.my, z.mz, DIR, R, C), blk, smem, s>>>(z, C, accumulate,
+    flux_dir<NS, INV, DIR, MINB, PART, NT><<<flux_grid(z.mx, z.my, z.mz, DIR, R, C), blk, smem, s>>>(z, C, accumulate,
                                                                                                  viscous);
     return cudaGetLastError();
   }
   if (tab->n <= 0) return cudaSuccess;
   // persistent grid: every resident CTA slot of the device, no more than there are tiles
   int per_sm = 0, dev = 0, sms = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flux_dir_table<NS, INV, DIR, MINB, PART>,
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flux_dir_table<NS, INV, DIR, MINB, PART, NT>,
                                                                 32 * R, smem);
   if (e == cudaSuccess) e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -212,18 +215,18 @@ static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, const Flu
   const int slots = per_sm * sms;
   if (slots <= 0) return cudaErrorInvalidConfiguration;
   const int grid = tab->n < slots ? tab->n : slots;
-  flux_dir_table<NS, INV, DIR, MINB, PART><<<grid, blk, smem, s>>>(tab->tiles, tab->n, C, accumulate, viscous);
+  flux_dir_table<NS, INV, DIR, MINB, PART, NT><<<grid, blk, smem, s>>>(tab->tiles, tab->n, C, accumulate, viscous);
   return cudaGetLastError();
 }
 
-template <int NS, int INV, int DIR, int PART>
+template <int NS, int INV, int DIR, int PART, int NT>
 static cudaError_t launch_flux_p(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
                                  int viscous, cudaStream_t s) {
   switch (t.minb) {
-    case 4: return launch_flux_m<NS, INV, DIR, 4, PART>(z, t, tab, accumulate, viscous, s);
-    case 3: return launch_flux_m<NS, INV, DIR, 3, PART>(z, t, tab, accumulate, viscous, s);
-    case 2: return launch_flux_m<NS, INV, DIR, 2, PART>(z, t, tab, accumulate, viscous, s);
-    default: return launch_flux_m<NS, INV, DIR, 1, PART>(z, t, tab, accumulate, viscous, s);
+    case 4: return launch_flux_m<NS, INV, DIR, 4, PART, NT>(z, t, tab, accumulate, viscous, s);
+    case 3: return launch_flux_m<NS, INV, DIR, 3, PART, NT>(z, t, tab, accumulate, viscous, s);
+    case 2: return launch_flux_m<NS, INV, DIR, 2, PART, NT>(z, t, tab, accumulate, viscous, s);
+    default: return launch_flux_m<NS, INV, DIR, 1, PART, NT>(z, t, tab, accumulate, viscous, s);
   }
 }
 
@@ -233,43 +236,52 @@ static cudaError_t launch_flux_p(const DevZone &z, const TileShape &t, const Flu
 // alone (tile t.vrows/vchunks/vminb, or t when no viscous tile is set).
 // With tables (tab[0] for the shape t, tab[1] for the viscous shape) every
 // zone of the context is processed by one launch per kernel.
-template <int NS, int INV, int DIR>
+template <int NS, int INV, int DIR, int NT>
 static cudaError_t launch_flux_t(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
                                  int viscous, int part, cudaStream_t s) {
   const TileShape tv = t.vrows ? TileShape{t.vrows, t.vchunks, t.vminb} : TileShape{t.rows, t.chunks, t.minb};
   const FluxTable *tp = tab ? &tab[0] : nullptr;
   const FluxTable *tq = tab ? (t.vrows ? &tab[1] : &tab[0]) : nullptr;
-  if (part == 1) return launch_flux_p<NS, INV, DIR, 1>(z, t, tp, accumulate, 0, s);
-  if (part == 2) return launch_flux_p<NS, 0, DIR, 2>(z, tv, tq, accumulate, 1, s);
-  if (!viscous || t.vrows == 0) return launch_flux_p<NS, INV, DIR, 0>(z, t, tp, accumulate, viscous, s);
-  cudaError_t e = launch_flux_p<NS, INV, DIR, 1>(z, t, tp, accumulate, 0, s);
+  if (part == 1) return launch_flux_p<NS, INV, DIR, 1, NT>(z, t, tp, accumulate, 0, s);
+  if (part == 2) return launch_flux_p<NS, 0, DIR, 2, NT>(z, tv, tq, accumulate, 1, s);
+  if (!viscous || t.vrows == 0) return launch_flux_p<NS, INV, DIR, 0, NT>(z, t, tp, accumulate, viscous, s);
+  cudaError_t e = launch_flux_p<NS, INV, DIR, 1, NT>(z, t, tp, accumulate, 0, s);
   if (e != cudaSuccess) return e;
-  return launch_flux_p<NS, 0, DIR, 2>(z, tv, tq, 1, 1, s);
+  return launch_flux_p<NS, 0, DIR, 2, NT>(z, tv, tq, 1, 1, s);
 }
 
-template <int NS>
-cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, const FluxTable *tab, int accumulate,
-                        int viscous, int part, cudaStream_t s) {
-  if constexpr (NS == 0) {
-    if (inv == 1) {
-      switch (dir) {
-        case 0: return launch_flux_t<0, 1, 0>(z, t, tab, accumulate, viscous, part, s);
-        case 1: return launch_flux_t<0, 1, 1>(z, t, tab, accumulate, viscous, part, s);
-        default: return launch_flux_t<0, 1, 2>(z, t, tab, accumulate, viscous, part, s);
+template <int NS, int NT>
+cudaError_t launch_flux_nt(const DevZone &z, int inv, int dir, const TileShape &t, const FluxTable *tab, int accumulate,
+                           int viscous, int part, cudaStream_t s) {
+  if constexpr (NT > 0) {
+    if (inv != 0) return cudaErrorInvalidValue;  // turbulence scalars: primitive-variable reconstruction only
+    switch (dir) {
+      case 0: return launch_flux_t<NS, 0, 0, NT>(z, t, tab, accumulate, viscous, part, s);
+      case 1: return launch_flux_t<NS, 0, 1, NT>(z, t, tab, accumulate, viscous, part, s);
+      default: return launch_flux_t<NS, 0, 2, NT>(z, t, tab, accumulate, viscous, part, s);
+    }
+  } else {
+    if constexpr (NS == 0) {
+      if (inv == 1) {
+        switch (dir) {
+          case 0: return launch_flux_t<0, 1, 0, 0>(z, t, tab, accumulate, viscous, part, s);
+          case 1: return launch_flux_t<0, 1, 1, 0>(z, t, tab, accumulate, viscous, part, s);
+          default: return launch_flux_t<0, 1, 2, 0>(z, t, tab, accumulate, viscous, part, s);
+        }
       }
     }
-  }
-  if (inv == 2) {
-    switch (dir) {
-      case 0: return launch_flux_t<NS, 2, 0>(z, t, tab, accumulate, viscous, part, s);
-      case 1: return launch_flux_t<NS, 2, 1>(z, t, tab, accumulate, viscous, part, s);
-      default: return launch_flux_t<NS, 2, 2>(z, t, tab, accumulate, viscous, part, s);
+    if (inv == 2) {
+      switch (dir) {
+        case 0: return launch_flux_t<NS, 2, 0, 0>(z, t, tab, accumulate, viscous, part, s);
+        case 1: return launch_flux_t<NS, 2, 1, 0>(z, t, tab, accumulate, viscous, part, s);
+        default: return launch_flux_t<NS, 2, 2, 0>(z, t, tab, accumulate, viscous, part, s);
+      }
     }
-  }
-  switch (dir) {
-    case 0: return launch_flux_t<NS, 0, 0>(z, t, tab, accumulate, viscous, part, s);
-    case 1: return launch_flux_t<NS, 0, 1>(z, t, tab, accumulate, viscous, part, s);
-    default: return launch_flux_t<NS, 0, 2>(z, t, tab, accumulate, viscous, part, s);
+    switch (dir) {
+      case 0: return launch_flux_t<NS, 0, 0, 0>(z, t, tab, accumulate, viscous, part, s);
+      case 1: return launch_flux_t<NS, 0, 1, 0>(z, t, tab, accumulate, viscous, part, s);
+      default: return launch_flux_t<NS, 0, 2, 0>(z, t, tab, accumulate, viscous, part, s);
+    }
   }
 }
 

@@ -1,4 +1,4 @@
-// flux0.cu — the flux kernel family (flux.cuh) built for NS = 0 species.
+// flux0.cu — the flux kernel family (flux.cuh) built for NS = 0 species (air).
 #include "common.cuh"
 
 namespace ostc {
@@ -17,8 +17,8 @@ static __constant__ DevZone c_zones[kMaxTableZones];
 
 namespace ostc {
 
-template cudaError_t launch_flux<0>(const DevZone &, int, int, const TileShape &, const FluxTable *, int, int, int,
-                                     cudaStream_t);
+template cudaError_t launch_flux_nt<0, 0>(const DevZone &, int, int, const TileShape &, const FluxTable *, int,
+                                            int, int, cudaStream_t);
 
 cudaError_t upload_param_flux0(const DevParam &p, cudaStream_t s) {
   return cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);

@@ -1,7 +1,7 @@
 // kernels.cu — sm_100a kernels of the RHS / RK3 stage (the flux kernels,
-// flux_dir in flux.cuh, are built in flux0.cu and flux9.cu).
+// flux_dir in flux.cuh, are built in flux0.cu, flux9.cu and flux0t.cu).
 //
-//  source_kernel<NS>      finite-rate chemistry source, starts dq (SourceTerm.cuh:11-37)
+//  source_kernel<NS>      finite-rate chemistry or SST source, starts dq (SourceTerm.cuh:11-37)
 //  update_rk_kernel<NS>   SSPRK3 stage update, cv -> bv/sv, T and p (RK.cuh:197-253)
 //  properties_kernel<NS>  cp, gamma, a, mu, kappa, rho*D, Mach over [-1, m] (FieldOperation.cuh:112-146)
 //  cv_from_bv_kernel<NS>  conservative from primitive, ghosts included (FieldOperation.cuh:43-79)
@@ -43,6 +43,17 @@ __device__ __forceinline__ void source_cells(const DevZone &z, const int bx, con
   double *dq = z.dq + qidx(z, i, j, k);
 #pragma unroll
   for (int l = 0; l < 5; ++l) dq[l * z.qsz] = 0;
+  if constexpr (NS == 0) {
+    if (c_p.sst) {  // SST::compute_source_and_mut and the turbulent conductivity (SourceTerm.cuh:19-27)
+      double mut, sk, sw;
+      sst::source_point(z, g, mut, sk, sw);
+      z.mut[g] = mut;
+      constexpr double cpa = gamma_air * R_u / mw_air / (gamma_air - 1);
+      z.ttc[g] = mut * cpa / c_p.Prt;
+      dq[5 * z.qsz] = sk;
+      dq[6 * z.qsz] = sw;
+    }
+  }
   if constexpr (NS > 0) {
     double Y[NS], om[NS];
 #pragma unroll
@@ -158,6 +169,12 @@ __device__ __forceinline__ void update_rk_cells(const DevZone &z, const int bx, 
   for (int l = 0; l < NV; ++l) z.cv[l * z.sz + g] = cv[l];
   const double rho = cv[0];
   const double ri = 1.0 / rho;
+  // scalars after the species (SST k, omega): cv update and sv = cv / rho (RK.cuh:209-235)
+  for (int l = NV; l < c_p.n_var; ++l) {
+    const double c_l = a * z.qn[l * z.sz + g] + b * z.cv[l * z.sz + g] + c * dtj * z.dq[l * z.qsz + q];
+    z.cv[l * z.sz + g] = c_l;
+    z.sv[(l - 5) * z.sz + g] = c_l * ri;
+  }
   const double u = cv[1] * ri, v = cv[2] * ri, w = cv[3] * ri;
   z.bv[g] = rho;
   z.bv[z.sz + g] = u;
@@ -256,6 +273,21 @@ __global__ void __launch_bounds__(256) properties_kernel(DevZone z) {
   properties_cells<NS>(z, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// initialize_mut (FieldOperation.cuh:175-195) over [-1, m]: the SST turbulent
+// viscosity from the initial field, air (Sutherland viscosity)
+__device__ __forceinline__ void init_mut_cells(const DevZone &z, const int bx, const int by, const int bz) {
+  const int i = bx * blockDim.x + threadIdx.x - 1;
+  const int j = by * blockDim.y + threadIdx.y - 1;
+  const int k = bz - 1;
+  if (i > z.mx || j > z.my) return;
+  const int g = gidx(z, i, j, k);
+  z.mut[g] = sst::mut_point(z, g, sutherland(z.bv[5 * z.sz + g]));
+}
+
+__global__ void __launch_bounds__(256) init_mut_kernel(DevZone z) {
+  init_mut_cells(z, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 template <int NS>
 __device__ __forceinline__ void cv_from_bv_point(const DevZone &z, int g) {
   const double rho = z.bv[g], u = z.bv[z.sz + g], v = z.bv[2 * z.sz + g], w = z.bv[3 * z.sz + g];
@@ -264,6 +296,7 @@ __device__ __forceinline__ void cv_from_bv_point(const DevZone &z, int g) {
   z.cv[z.sz + g] = rho * u;
   z.cv[2 * z.sz + g] = rho * v;
   z.cv[3 * z.sz + g] = rho * w;
+  for (int l = NS; l < c_p.n_scalar; ++l) z.cv[(5 + l) * z.sz + g] = rho * z.sv[l * z.sz + g];  // SST k, omega
   const double V2 = u * u + v * v + w * w;
   double E = 0.5 * V2;
   if constexpr (NS == 0) {
@@ -338,7 +371,8 @@ __device__ __forceinline__ void dt_cells(const DevZone &z, const int bx, const i
     const double sri = (fabs(U) + a * gx) + (fabs(V) + a * ge) + (d3 ? fabs(W) + a * gz : 0.0);
     const double gamma = NS == 0 ? gamma_air : ld(z.gam + g);
     const double c1 = fmax(gamma, 4.0 / 3.0) / bvl(z, g, 0);
-    const double c2 = ld(z.mul + g) / c_p.Pr;
+    double c2 = ld(z.mul + g) / c_p.Pr;
+    if (c_p.sst) c2 += ld(z.mut + g) / c_p.Prt;
     double srv = gx * gx + ge * ge;
     if (d3) srv += gz * gz;
     srv *= c1 * c2;
@@ -392,6 +426,7 @@ __global__ void bc_outflow_kernel(DevZone z, BcFace b, int with_cv) {  // BoundC
     const int gi = g + gg * step;
     for (int l = 0; l < 6; ++l) z.bv[l * z.sz + gi] = z.bv[l * z.sz + g];
     for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + gi] = z.sv[l * z.sz + g];
+    if (c_p.sst) z.mut[gi] = z.mut[g];
     if (with_cv) cv_from_bv_point<NS>(z, gi);
   }
 }
@@ -413,6 +448,7 @@ __global__ void bc_inflow_kernel(DevZone z, BcFace b, int with_cv) {  // BoundCo
     z.bv[4 * z.sz + gi] = b.pressure;
     z.bv[5 * z.sz + gi] = b.temperature;
     for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + gi] = b.sv[l];
+    if (c_p.sst) z.mut[gi] = b.mut;
     if (gg == 0) z.vel[gi] = b.velocity;
     if (with_cv) {
       // compute_cv_from_bv_1_point also rewrites vel from bv (FieldOperation.cuh:40)
@@ -459,6 +495,7 @@ __global__ void bc_symmetry_kernel(DevZone z, BcFace b) {  // BoundCond.cuh:52-1
     z.bv[4 * z.sz + go] = z.bv[4 * z.sz + gi];
     z.bv[5 * z.sz + go] = z.bv[5 * z.sz + gi];
     for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = z.sv[l * z.sz + gi];
+    if (c_p.sst) z.mut[go] = z.mut[gi];
   }
 }
 
@@ -475,13 +512,16 @@ __global__ void bc_periodic_kernel(DevZone z, BcFace b, int with_cv) {
     const int gs = go - b.period_stride;
     for (int l = 0; l < 6; ++l) z.bv[l * z.sz + go] = z.bv[l * z.sz + gs];
     for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = z.sv[l * z.sz + gs];
+    if (c_p.sst) z.mut[go] = z.mut[gs];
     z.vel[go] = z.vel[gs];
     if (with_cv)
       for (int l = 0; l < c_p.n_var; ++l) z.cv[l * z.sz + go] = z.cv[l * z.sz + gs];
   }
 }
 
-// isothermal / adiabatic no-slip wall, laminar (BoundCond.cuh:415-526)
+// isothermal / adiabatic no-slip wall (BoundCond.cuh:415-541); with SST, k = 0
+// on the wall and in the ghosts, omega = 60 mu_w / (rho_w beta_1 d^2) from the
+// wall distance d of the first interior point, mut = 0 in the ghosts
 template <int NS>
 __global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
   const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
@@ -512,6 +552,14 @@ __global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
   z.bv[4 * z.sz + g] = p;
   z.bv[5 * z.sz + g] = t_wall;
   z.vel[g] = 0;
+  if constexpr (NS == 0) {
+    if (c_p.sst) {
+      const double mu_wall = sutherland(t_wall);
+      const double dy = z.wall[gin];
+      z.sv[g] = 0;
+      z.sv[z.sz + g] = dy > 1e-25 ? 60 * mu_wall / (rho_wall * sst::beta_1 * dy * dy) : z.sv[z.sz + gin];
+    }
+  }
   if (with_cv) cv_from_bv_point<NS>(z, g);
   for (int gg = 1; gg <= z.ngg; ++gg) {
     const int gi = g - gg * step, go = g + gg * step;
@@ -537,6 +585,13 @@ __global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
     z.bv[3 * z.sz + go] = -w_i;
     z.bv[4 * z.sz + go] = p_i;
     z.bv[5 * z.sz + go] = t_g;
+    if constexpr (NS == 0) {
+      if (c_p.sst) {
+        z.sv[go] = 0;
+        z.sv[z.sz + go] = z.sv[z.sz + g];
+        z.mut[go] = 0;
+      }
+    }
     if (with_cv) cv_from_bv_point<NS>(z, go);
   }
 }
@@ -561,21 +616,23 @@ __global__ void bc_farfield_kernel(DevZone z, BcFace b) {
   const double u_b = z.bv[z.sz + g], v_b = z.bv[2 * z.sz + g], w_b = z.bv[3 * z.sz + g];
   const double u_face = nx * u_b + ny * v_b + nz * w_b;
   double gamma_b = gamma_air, mw = mw_air;
-  double sv_b[NS > 0 ? NS : 1];
+  // boundary scalars start from the point's own; for air with SST the
+  // reference leaves them unset on subsonic outflow (uninitialised sv_b,
+  // BoundCond.cuh:244, 330-336), where the point's own values are kept here
+  double sv_b[NS + 2];
+  for (int l = 0; l < c_p.n_scalar && l < NS + 2; ++l) sv_b[l] = z.sv[l * z.sz + g];
   if constexpr (NS > 0) {
     double mw_inv = 0;
 #pragma unroll
-    for (int l = 0; l < NS; ++l) {
-      sv_b[l] = z.sv[l * z.sz + g];
-      mw_inv += sv_b[l] * c_p.imw[l];
-    }
+    for (int l = 0; l < NS; ++l) mw_inv += sv_b[l] * c_p.imw[l];
     gamma_b = z.gam[g];
     mw = 1.0 / mw_inv;
   }
   const double p_b = z.bv[4 * z.sz + g], rho_b = z.bv[g];
   const double a_b = sqrt(gamma_b * p_b / rho_b);
   const double mach_b = u_face / a_b;
-  auto fill = [&](double rho, double u, double v, double w, double p, double T, const double *svv, bool node) {
+  auto fill = [&](double rho, double u, double v, double w, double p, double T, const double *svv, double mut,
+                  bool node) {
     for (int gg = node ? 0 : 1; gg <= z.ngg; ++gg) {
       const int go = g + gg * step;
       z.bv[go] = rho;
@@ -585,16 +642,18 @@ __global__ void bc_farfield_kernel(DevZone z, BcFace b) {
       z.bv[4 * z.sz + go] = p;
       z.bv[5 * z.sz + go] = T;
       for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = svv[l];
+      if (c_p.sst) z.mut[go] = mut;
     }
     if (node) z.vel[g] = sqrt(u * u + v * v + w * w);
   };
   if (mach_b <= -1) {
-    fill(b.density, b.u, b.v, b.w, b.pressure, b.temperature, b.sv, true);
+    fill(b.density, b.u, b.v, b.w, b.pressure, b.temperature, b.sv, b.mut, true);
   } else if (mach_b >= 1) {
     for (int gg = 1; gg <= z.ngg; ++gg) {
       const int go = g + gg * step;
       for (int l = 0; l < 6; ++l) z.bv[l * z.sz + go] = z.bv[l * z.sz + g];
       for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = z.sv[l * z.sz + g];
+      if (c_p.sst) z.mut[go] = z.mut[g];
     }
   } else {
     const double r_pos = u_face + 2 * a_b / (gamma_b - 1);
@@ -602,6 +661,7 @@ __global__ void bc_farfield_kernel(DevZone z, BcFace b) {
     const double r_neg = u_inf - 2 * b.acoustic_speed / (b.specific_heat_ratio - 1);
     const double Un = 0.5 * (r_pos + r_neg);
     double s_b, rho, p, T, u, v, w;
+    const double mut_b = mach_b <= 0 && (NS == 0 || mach_b < 0) ? b.mut : (c_p.sst ? z.mut[g] : 0.0);
     if constexpr (NS == 0) {
       const double c_b = 0.25 * (gamma_air - 1) * (r_pos - r_neg);
       if (mach_b <= 0) {
@@ -609,6 +669,7 @@ __global__ void bc_farfield_kernel(DevZone z, BcFace b) {
         u = b.u + (Un - u_inf) * nx;
         v = b.v + (Un - u_inf) * ny;
         w = b.w + (Un - u_inf) * nz;
+        for (int l = 0; l < c_p.n_scalar && l < NS + 2; ++l) sv_b[l] = b.sv[l];
       } else {
         s_b = p_b / pow(rho_b, gamma_air);
         u = u_b + (Un - u_face) * nx;
@@ -618,7 +679,7 @@ __global__ void bc_farfield_kernel(DevZone z, BcFace b) {
       rho = pow(c_b * c_b / (gamma_air * s_b), 1 / (gamma_air - 1));
       p = rho * c_b * c_b / gamma_air;
       T = p * mw_air / (rho * R_u);
-      fill(rho, u, v, w, p, T, sv_b, true);
+      fill(rho, u, v, w, p, T, sv_b, mut_b, true);
     } else {
       if (mach_b < 0) {
         u = b.u + (Un - u_inf) * nx;
@@ -648,7 +709,7 @@ __global__ void bc_farfield_kernel(DevZone z, BcFace b) {
         gamma = cp_tot / (cp_tot - R_u / mw);
         err = fabs(1 - gamma / gamma_last);
       }
-      fill(rho, u, v, w, p, T, sv_b, true);
+      fill(rho, u, v, w, p, T, sv_b, mut_b, true);
     }
   }
 }
@@ -667,6 +728,7 @@ __global__ void bc_back_pressure_kernel(DevZone z, BcFace b, int with_cv) {
     z.bv[4 * z.sz + go] = b.pressure;
     z.bv[5 * z.sz + go] = z.bv[5 * z.sz + g];
     for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = z.sv[l * z.sz + g];
+    if (c_p.sst) z.mut[go] = z.mut[g];
     if (with_cv) cv_from_bv_point<NS>(z, go);
   }
 }
@@ -714,6 +776,7 @@ __global__ void bc_subsonic_inflow_kernel(DevZone z, BcFace b, int with_cv) {
     z.bv[5 * z.sz + go] = T;
     const double u_bar = z.bv[z.sz + go] * nx + z.bv[2 * z.sz + go] * ny + z.bv[3 * z.sz + go] * nz;
     for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = u_bar > 0 ? z.sv[l * z.sz + g] : b.sv[l];
+    if (c_p.sst) z.mut[go] = z.mut[g];
     if (with_cv) cv_from_bv_point<0>(z, go);
   }
 }
@@ -866,6 +929,9 @@ struct DtOp {
 struct StoreLastOp {
   __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { store_last_cells(z, bx, by, bz); }
 };
+struct InitMutOp {
+  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { init_mut_cells(z, bx, by, bz); }
+};
 
 }  // namespace ostc
 
@@ -904,6 +970,7 @@ cudaError_t upload_zones(const DevZone *z, int n, cudaStream_t s) {
                     : cudaSuccess;
   if (e == cudaSuccess) e = upload_zones_flux0(z, n, s);
   if (e == cudaSuccess) e = upload_zones_flux9(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_flux0t(z, n, s);
   return e;
 }
 
@@ -918,6 +985,7 @@ cudaError_t launch_cells_table(CellOp op, const CellTable &tab, const CellArgs &
     case CellOp::Velocity: return launch_table(tab, VelocityOp{}, s);
     case CellOp::Dt: return launch_table(tab, DtOp<NS>{a.dt_bits}, s);
     case CellOp::StoreLast: return launch_table(tab, StoreLastOp{}, s);
+    case CellOp::InitMut: return launch_table(tab, InitMutOp{}, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -937,6 +1005,9 @@ cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStr
       break;
     case CellOp::Properties:
       properties_kernel<NS><<<plane_grid(z.mx + 2, z.my + 2, z.mz + 2, blk), blk, 0, s>>>(z);
+      break;
+    case CellOp::InitMut:
+      init_mut_kernel<<<plane_grid(z.mx + 2, z.my + 2, z.mz + 2, blk), blk, 0, s>>>(z);
       break;
     case CellOp::CvFromBv:
       cv_from_bv_kernel<NS>
@@ -1100,6 +1171,7 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   cudaError_t e = cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = upload_param_flux0(p, s);
   if (e == cudaSuccess) e = upload_param_flux9(p, s);
+  if (e == cudaSuccess) e = upload_param_flux0t(p, s);
   return e;
 }
 

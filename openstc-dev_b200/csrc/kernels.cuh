@@ -61,7 +61,7 @@ struct Iface {
   int rs[3], ts[3], ld[3], tld[3], st[3], np[3];
 };
 
-enum class CellOp { Source, UpdateRK, Properties, CvFromBv, Velocity, Dt, DtReset, StoreLast, ResidualPartial };
+enum class CellOp { Source, UpdateRK, Properties, CvFromBv, Velocity, Dt, DtReset, StoreLast, ResidualPartial, InitMut };
 
 struct CellArgs {
   double dt = 0;
@@ -89,21 +89,25 @@ struct SteadyArgs {
 // viscous half alone (flux.cuh: launch_flux_t). tab = nullptr: zone z alone;
 // else tab[0] (shape t) and tab[1] (viscous shape) hold the tiles of every
 // zone of the uploaded table and z is not used
-template <int NS>
-cudaError_t launch_flux(const DevZone &z, int inv, int dir, const TileShape &t, const FluxTable *tab, int accumulate,
-                        int viscous, int part, cudaStream_t s);
+// NT: turbulence scalars after the NS species (0, or 2 for SST with NS = 0);
+// built in flux0.cu (NS 0, NT 0), flux9.cu (9, 0) and flux0t.cu (0, 2)
+template <int NS, int NT>
+cudaError_t launch_flux_nt(const DevZone &z, int inv, int dir, const TileShape &t, const FluxTable *tab,
+                           int accumulate, int viscous, int part, cudaStream_t s);
 template <int NS>
 cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStream_t s);
 // the per-cell kernels of Source, UpdateRK, Properties, CvFromBv, Velocity,
 // Dt and StoreLast over a tile table of (32 x 8)-thread tiles; the table's
 // extents per zone: interior (mx, my, mz) for Source, UpdateRK, Dt,
-// StoreLast; (mx+2, my+2, mz+2) for Properties; ghosted for CvFromBv, Velocity
+// StoreLast; (mx+2, my+2, mz+2) for Properties and InitMut; ghosted for
+// CvFromBv, Velocity
 template <int NS>
 cudaError_t launch_cells_table(CellOp op, const CellTable &tab, const CellArgs &a, cudaStream_t s);
 // the zone tables of every kernel unit
 cudaError_t upload_zones(const DevZone *z, int n, cudaStream_t s);
-cudaError_t upload_zones_flux0(const DevZone *z, int n, cudaStream_t s);  // flux0.cu
-cudaError_t upload_zones_flux9(const DevZone *z, int n, cudaStream_t s);  // flux9.cu
+cudaError_t upload_zones_flux0(const DevZone *z, int n, cudaStream_t s);   // flux0.cu
+cudaError_t upload_zones_flux9(const DevZone *z, int n, cudaStream_t s);   // flux9.cu
+cudaError_t upload_zones_flux0t(const DevZone *z, int n, cudaStream_t s);  // flux0t.cu
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s);
 template <int NS>
@@ -125,8 +129,9 @@ cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, do
 cudaError_t prepare_chem_surrogate();
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
 cudaError_t upload_param(const DevParam &p, cudaStream_t s);
-cudaError_t upload_param_flux0(const DevParam &p, cudaStream_t s);  // flux0.cu
-cudaError_t upload_param_flux9(const DevParam &p, cudaStream_t s);  // flux9.cu
+cudaError_t upload_param_flux0(const DevParam &p, cudaStream_t s);   // flux0.cu
+cudaError_t upload_param_flux9(const DevParam &p, cudaStream_t s);   // flux9.cu
+cudaError_t upload_param_flux0t(const DevParam &p, cudaStream_t s);  // flux0t.cu
 // whether a mechanism has the structure of the generated mech_h2air9.cuh
 bool mechanism_is_h2air9(const int *reac_type, const int *stoi_f, const int *stoi_b, const int *reac_order, int nr,
                          int ns);

@@ -217,6 +217,8 @@ class Scheme:
     fixed_time_step: int = 0
     dt: float = 1e-6
     chem_mode: int = 0            # RK3 chemistry: 0 source in the RHS, 1 split FP64, 2 split surrogate
+    rans_model: int = 0           # 0 laminar, 2 k-omega SST (air)
+    compressibility_correction: int = 0  # SST: 0 none, 1 Wilcox, 2 Sarkar, 3 Zeman
     steady: int = 0               # 1: local time stepping (steady_simulation)
     implicit_method: int = 0      # steady: 0 explicit (+ EPI/DA chemistry), 1 DPLUR
     dplur_inner_step: int = 3
@@ -243,11 +245,12 @@ def make_param(s: Scheme, mech: Optional[Mechanism]):
     """Returns (Param, keepalive) with host tables packed as the ABI expects."""
     p = Param()
     ns = mech.n_spec if (mech is not None and s.mix_model != MIX_AIR) else 0
+    nt = 2 if s.rans_model == 2 else 0
     p.mix_model = s.mix_model
-    p.turbulence = 0
+    p.turbulence = 1 if nt else 0
     p.n_spec = ns
-    p.n_scalar = ns
-    p.n_var = 5 + ns
+    p.n_scalar = ns + nt
+    p.n_var = 5 + ns + nt
     p.n_reac = mech.n_reac if (mech is not None and s.mix_model == MIX_FR) else 0
     p.i_turb_cv = 5 + ns
     p.inviscid_scheme = s.inviscid_scheme
@@ -255,9 +258,9 @@ def make_param(s: Scheme, mech: Optional[Mechanism]):
     p.limiter = s.limiter
     p.inviscid_type = s.inviscid_type
     p.viscous_scheme = s.viscous_order
-    p.rans_model = 0
+    p.rans_model = s.rans_model
     p.turb_implicit = 0
-    p.compressibility_correction = 0
+    p.compressibility_correction = s.compressibility_correction if nt else 0
     p.chemSrcMethod = s.chemSrcMethod
     p.gradPInDiffusionFlux = s.gradPInDiffusionFlux
     p.dimension = 3
@@ -302,18 +305,19 @@ class HostBlock:
     n_spec: int
     arrays: Dict[str, np.ndarray] = field(default_factory=dict)
     dq_ngg: int = 0
+    n_turb: int = 0  # turbulence scalars after the species in sv (2 with SST)
 
     def plane(self, g=None):
         return plane_shape(self.mx, self.my, self.mz, self.ngg if g is None else g)
 
     @staticmethod
-    def specs(mx, my, mz, ngg, n_var, n_spec, dq_ngg=0):
+    def specs(mx, my, mz, ngg, n_var, n_spec, dq_ngg=0, n_turb=0):
         """name -> (shape, dtype) of every array of a block (Field::setup_device_memory)."""
         P = plane_shape(mx, my, mz, ngg)
         I = plane_shape(mx, my, mz, 0)
         Q = plane_shape(mx, my, mz, dq_ngg)
         f8 = np.float64
-        sp = {"bv": ((6,) + P, f8), "sv": ((n_spec,) + P, f8), "cv": ((n_var,) + P, f8),
+        sp = {"bv": ((6,) + P, f8), "sv": ((n_spec + n_turb,) + P, f8), "cv": ((n_var,) + P, f8),
               "qn": ((n_var,) + P, f8), "dq": ((n_var,) + Q, f8), "jac": (P, f8), "metric": (P, METRIC_DTYPE)}
         for n in ("vel", "acoustic_speed", "mach", "mul", "thermal_conductivity"):
             sp[n] = (P, f8)
@@ -321,18 +325,21 @@ class HostBlock:
             sp["rho_D"] = ((n_spec,) + P, f8)
             sp["gamma"] = (P, f8)
             sp["cp"] = (P, f8)
+        if n_turb:
+            for n in ("mut", "turb_therm_cond", "wall_distance"):
+                sp[n] = (P, f8)
         sp["dt_local"] = (I, f8)
         sp["bv_last"] = ((4,) + I, f8)
         return sp
 
-    INPUTS = ("bv", "sv", "jac", "metric")
+    INPUTS = ("bv", "sv", "jac", "metric", "wall_distance")
 
     @staticmethod
-    def allocate(mx, my, mz, ngg, n_var, n_spec, full=True, dq_ngg=0) -> "HostBlock":
-        """full=False holds only the inputs (bv, sv, jac, metric); the device
-        block creates the rest zero-filled."""
-        b = HostBlock(mx, my, mz, ngg, n_var, n_spec, dq_ngg=dq_ngg)
-        for n, (shape, dt) in HostBlock.specs(mx, my, mz, ngg, n_var, n_spec, dq_ngg).items():
+    def allocate(mx, my, mz, ngg, n_var, n_spec, full=True, dq_ngg=0, n_turb=0) -> "HostBlock":
+        """full=False holds only the inputs (bv, sv, jac, metric, wall
+        distance); the device block creates the rest zero-filled."""
+        b = HostBlock(mx, my, mz, ngg, n_var, n_spec, dq_ngg=dq_ngg, n_turb=n_turb)
+        for n, (shape, dt) in HostBlock.specs(mx, my, mz, ngg, n_var, n_spec, dq_ngg, n_turb).items():
             if full or n in HostBlock.INPUTS:
                 b.arrays[n] = np.zeros(shape, dtype=dt)
         return b
@@ -340,7 +347,7 @@ class HostBlock:
     def complete(self) -> "HostBlock":
         """a full copy (all arrays) for the oracle"""
         b = HostBlock.allocate(self.mx, self.my, self.mz, self.ngg, self.n_var, self.n_spec, full=True,
-                               dq_ngg=self.dq_ngg)
+                               dq_ngg=self.dq_ngg, n_turb=self.n_turb)
         for n, v in self.arrays.items():
             b.arrays[n][...] = v
         return b
@@ -366,7 +373,8 @@ class DeviceBlock:
         self.host_shape = host
         self.mx, self.my, self.mz, self.ngg = host.mx, host.my, host.mz, host.ngg
         self.dq_ngg = host.dq_ngg
-        self.specs = HostBlock.specs(host.mx, host.my, host.mz, host.ngg, host.n_var, host.n_spec, host.dq_ngg)
+        self.specs = HostBlock.specs(host.mx, host.my, host.mz, host.ngg, host.n_var, host.n_spec, host.dq_ngg,
+                                     host.n_turb)
         self.t = {}
         for n, (shape, dt) in self.specs.items():
             if n == "metric":
@@ -974,8 +982,37 @@ def block_layout(seed=37, n_layers=4, n_cols=3, rows=(3, 3, 3), extra_row=(1, 0)
     return out
 
 
+def sst_freestream(state: dict, turbulence_intensity=0.01, viscosity_ratio=10.0) -> dict:
+    """k, omega and mut of a free stream from its turbulence intensity and
+    turbulent-to-laminar viscosity ratio (BoundCond.cpp:84-93): mut = ratio
+    mu(T), k = 1.5 (U Tu)^2, omega = rho k / mut; air, Sutherland mu."""
+    T = state["temperature"]
+    mu = 1.716e-5 * (T / 273) ** 1.5 * (273 + 111) / (T + 111)
+    mut = viscosity_ratio * mu
+    k = 1.5 * state["velocity"] ** 2 * turbulence_intensity ** 2
+    omega = state["density"] * k / mut
+    out = dict(state)
+    out.update(sv=[k, omega], mut=mut)
+    return out
+
+
+def wall_distance_j0(yg_shape_xyz, xs, ys, zs, i0, j0, k0, mx, my, mz, ng):
+    """Distance of every ghosted point of a block to the wall node (global
+    j = 0) of its own (i, k) grid line: the SST wall distance input of cases
+    whose walls are the j = 0 plane (the reference's wall-distance search is
+    pre-processing, outside this path)."""
+    X = xs[k0:k0 + mz + 2 * ng, j0:j0 + my + 2 * ng, i0:i0 + mx + 2 * ng]
+    Y = ys[k0:k0 + mz + 2 * ng, j0:j0 + my + 2 * ng, i0:i0 + mx + 2 * ng]
+    Zc = zs[k0:k0 + mz + 2 * ng, j0:j0 + my + 2 * ng, i0:i0 + mx + 2 * ng]
+    jw = ng  # global j = 0 in the ghosted global arrays
+    Xw = xs[k0:k0 + mz + 2 * ng, jw:jw + 1, i0:i0 + mx + 2 * ng]
+    Yw = ys[k0:k0 + mz + 2 * ng, jw:jw + 1, i0:i0 + mx + 2 * ng]
+    Zw = zs[k0:k0 + mz + 2 * ng, jw:jw + 1, i0:i0 + mx + 2 * ng]
+    return np.sqrt((X - Xw) ** 2 + (Y - Yw) ** 2 + (Zc - Zw) ** 2)
+
+
 def case_uneven_blocks(seed=37, dx=1e-4, reconstruction=2, inviscid_scheme=4, mach=3.0, reynolds=1e7, T=300.0,
-                       layout=None) -> Case:
+                       layout=None, rans_model=0, compressibility_correction=0) -> Case:
     """Uneven multi-block air case: the seeded layout of block_layout (37
     blocks from 16^3 to 192 x 96 x 64 joined by 1-to-1 interfaces, partial
     faces where neighbouring splits differ) in a warped box. Mach 3 air at
@@ -984,9 +1021,12 @@ def case_uneven_blocks(seed=37, dx=1e-4, reconstruction=2, inviscid_scheme=4, ma
     outflow at i-max, isothermal walls at T on every j-min block face (the
     12 blocks of the bottom row), far field at j-max, symmetry in k. layout:
     another block_layout (parity-sized runs). HLLC + MUSCL by default (the
-    variant the reference build runs), laminar viscous fluxes."""
+    variant the reference build runs), laminar viscous fluxes, or k-omega SST
+    with rans_model=2 (free stream at 1 % turbulence intensity and viscosity
+    ratio 10, wall distance from wall_distance_j0)."""
     s = Scheme(mix_model=MIX_AIR, inviscid_scheme=inviscid_scheme, reconstruction=reconstruction, viscous_order=2,
-               cfl=0.5)
+               cfl=0.5, rans_model=rans_model, compressibility_correction=compressibility_correction)
+    nt = 2 if rans_model == 2 else 0
     ng = s.ngg
     if layout is None:
         layout = block_layout(seed)
@@ -1003,17 +1043,23 @@ def case_uneven_blocks(seed=37, dx=1e-4, reconstruction=2, inviscid_scheme=4, ma
     rho = reynolds * mu / U
     p = rho * R_U / MW_AIR * T
     ff = farfield_state(mach, T, p)
-    Ys = yg[1:-1, 1:-1, 1:-1]
+    if nt:
+        ff = sst_freestream(ff)
+    Xs, Ys, Zs = xg[1:-1, 1:-1, 1:-1], yg[1:-1, 1:-1, 1:-1], zg[1:-1, 1:-1, 1:-1]
     prof = np.tanh(np.maximum(Ys, 0.0) / (20 * dx))
     gbv = np.stack([np.full_like(Ys, rho), U * prof, 0 * Ys, 0 * Ys, np.full_like(Ys, p), np.full_like(Ys, T)])
     blocks, faces, ifaces = [], [], []
     for q, (o, e) in enumerate(layout):
         mx, my, mz = e
-        b = HostBlock.allocate(mx, my, mz, ng, 5, 0)
+        b = HostBlock.allocate(mx, my, mz, ng, 5 + nt, 0, n_turb=nt)
         i0, j0, k0 = o
         sl = (slice(k0, k0 + mz + 2 * ng + 2), slice(j0, j0 + my + 2 * ng + 2), slice(i0, i0 + mx + 2 * ng + 2))
         fill_metric(b, np.ascontiguousarray(xg[sl]), np.ascontiguousarray(yg[sl]), np.ascontiguousarray(zg[sl]))
         b.arrays["bv"][...] = gbv[:, k0:k0 + mz + 2 * ng, j0:j0 + my + 2 * ng, i0:i0 + mx + 2 * ng]
+        if nt:
+            b.arrays["sv"][0] = ff["sv"][0]
+            b.arrays["sv"][1] = ff["sv"][1]
+            b.arrays["wall_distance"][...] = wall_distance_j0(None, Xs, Ys, Zs, i0, j0, k0, mx, my, mz, ng)
         blocks.append(b)
     wall = dict(wall_isothermal=1, wall_temperature=T)
     glob_hi = (NX - 1, NY - 1, NZ - 1)
@@ -1067,7 +1113,8 @@ def case_uneven_blocks(seed=37, dx=1e-4, reconstruction=2, inviscid_scheme=4, ma
                         f.target_start[c] = s0 - tlo[c]
                         f.n_point[c] = s1 - s0 + 1
                     ifaces.append(f)
-    c = Case("uneven_blocks_%d_air_%dcells" % (len(layout), sum(e[0] * e[1] * e[2] for _, e in layout)), s, None,
+    c = Case("uneven_blocks_%d_air%s_%dcells" % (len(layout), "_sst" if nt else "",
+                                                  sum(e[0] * e[1] * e[2] for _, e in layout)), s, None,
              blocks, faces, 500)
     c.interfaces = ifaces
     return c
@@ -1089,7 +1136,8 @@ def make_steady(case: Case, implicit_method: int = 0, chem_src_method: Optional[
         s.cfl = cfl
     blocks = []
     for b in case.blocks:
-        nb = HostBlock.allocate(b.mx, b.my, b.mz, b.ngg, b.n_var, b.n_spec, full=True, dq_ngg=s.dq_ngg)
+        nb = HostBlock.allocate(b.mx, b.my, b.mz, b.ngg, b.n_var, b.n_spec, full=True, dq_ngg=s.dq_ngg,
+                                n_turb=b.n_turb)
         for n, v in b.arrays.items():
             if n != "dq":
                 nb.arrays[n][...] = v

@@ -60,7 +60,7 @@ struct MetricView {
 struct Z {  // a zone with views
   const ostc_zone *z;
   int mx, my, mz, ngg;
-  View bv, sv, cv, qn, dq, jac, vel, a, mach, mul, kappa, rhoD, gam, cp, dt_local, bv_last, mut, ttc;
+  View bv, sv, cv, qn, dq, jac, vel, a, mach, mul, kappa, rhoD, gam, cp, dt_local, bv_last, mut, ttc, wall;
   MetricView metric;
   explicit Z(const ostc_zone *zz) : z(zz), mx(zz->mx), my(zz->my), mz(zz->mz), ngg(zz->ngg) {
     const int g = ngg;
@@ -80,6 +80,7 @@ struct Z {  // a zone with views
     cp = View(zz->cp, mx, my, mz, g);
     mut = View(zz->mut, mx, my, mz, g);
     ttc = View(zz->turb_therm_cond, mx, my, mz, g);
+    wall = View(zz->wall_distance, mx, my, mz, g);
     dt_local = View(zz->dt_local, mx, my, mz, 0);
     bv_last = View(zz->bv_last, mx, my, mz, 0);
     metric = MetricView(zz->metric, mx, my, mz, g);
@@ -960,6 +961,135 @@ void inviscid_direction(const ostc_param *P, Z &Zn, int d) {
 // viscous face flux, laminar: compute_{fv,gv,hv}_2nd_order (ViscousScheme.cuh:22-821)
 // for the face between p0 = (i,j,k) and p1 = p0 + e_d.
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// k-omega SST, air (SST.cu:8-247, SST.cuh:12-45)
+// ---------------------------------------------------------------------------
+inline bool is_sst(const ostc_param *P) { return P->turbulence && P->rans_model == 2; }
+
+namespace sst {
+constexpr double beta_star = 0.09, sqrt_beta_star = 0.3, kappa = 0.41;
+constexpr double sigma_k1 = 0.85, sigma_omega1 = 0.5, beta_1 = 0.0750, a_1 = 0.31;
+constexpr double gamma1 = beta_1 / beta_star - sigma_omega1 * kappa * kappa / sqrt_beta_star;
+constexpr double sigma_k2 = 1, sigma_omega2 = 0.856, beta_2 = 0.0828;
+constexpr double gamma2 = beta_2 / beta_star - sigma_omega2 * kappa * kappa / sqrt_beta_star;
+constexpr double delta_sigma_k = sigma_k1 - sigma_k2, delta_sigma_omega = sigma_omega1 - sigma_omega2;
+constexpr double delta_beta = beta_1 - beta_2, delta_gamma = gamma1 - gamma2;
+
+// 0.5 * (xi_c (V(i+1)-V(i-1)) + eta_c (V(j+1)-V(j-1)) + zeta_c (V(k+1)-V(k-1))), SST.cu:52-69
+double grad(const Z &Zn, const View &V, int l, const double *m, int c, int i, int j, int k) {
+  return 0.5 * (m[c] * (V(i + 1, j, k, l) - V(i - 1, j, k, l)) + m[3 + c] * (V(i, j + 1, k, l) - V(i, j - 1, k, l)) +
+                m[6 + c] * (V(i, j, k + 1, l) - V(i, j, k - 1, l)));
+}
+
+double compute_mut(const Z &Zn, int i, int j, int k, double mul) {  // SST.cu:44-97
+  const double *m = Zn.metric.at(i, j, k);
+  const double u_y = grad(Zn, Zn.bv, 1, m, 1, i, j, k), u_z = grad(Zn, Zn.bv, 1, m, 2, i, j, k);
+  const double v_x = grad(Zn, Zn.bv, 2, m, 0, i, j, k), v_z = grad(Zn, Zn.bv, 2, m, 2, i, j, k);
+  const double w_x = grad(Zn, Zn.bv, 3, m, 0, i, j, k), w_y = grad(Zn, Zn.bv, 3, m, 1, i, j, k);
+  const double density = Zn.bv(i, j, k, 0), tke = Zn.sv(i, j, k, 0), omega = Zn.sv(i, j, k, 1);
+  const double rhoK = density * tke;
+  const double vorticity =
+      std::sqrt((v_x - u_y) * (v_x - u_y) + (w_x - u_z) * (w_x - u_z) + (w_y - v_z) * (w_y - v_z));
+  double f2 = 1;
+  const double dy = Zn.wall(i, j, k);
+  if (dy > 1e-25) {
+    const double param1 = 2 * std::sqrt(tke) / (0.09 * omega * dy);
+    const double param2 = 500 * mul / (density * dy * dy * omega);
+    const double arg2 = std::max(param1, param2);
+    f2 = std::tanh(arg2 * arg2);
+  }
+  double mut = 0;
+  const double denominator = std::max(a_1 * omega, vorticity * f2);
+  if (denominator > 1e-25) mut = a_1 * rhoK / denominator;
+  return mut;
+}
+
+double wilcox(double Mt) {  // SST.cu:24-31
+  constexpr double Mt0 = 0.25;
+  return Mt - Mt0 > 0 ? beta_star * 2 * (Mt * Mt - Mt0 * Mt0) : 0.0;
+}
+double zeman(double Mt, double gammaP1) {  // SST.cu:33-42
+  const double Mt0 = 0.25 * std::sqrt(2.0 / gammaP1);
+  const double DMt = Mt - Mt0;
+  if (DMt > 0) {
+    constexpr double Lambda2 = 0.66 * 0.66;
+    return beta_star * 0.75 * (1 - std::exp(-0.5 * gammaP1 * DMt * DMt / Lambda2));
+  }
+  return 0.0;
+}
+
+// compute_source_and_mut (SST.cu:99-247) + the turbulent conductivity (SourceTerm.cuh:19-27)
+void source_and_mut(const ostc_param *P, Z &Zn, int i, int j, int k) {
+  const double *m = Zn.metric.at(i, j, k);
+  const View &bv = Zn.bv, &sv = Zn.sv;
+  const double u_x = grad(Zn, bv, 1, m, 0, i, j, k), u_y = grad(Zn, bv, 1, m, 1, i, j, k);
+  const double u_z = grad(Zn, bv, 1, m, 2, i, j, k);
+  const double v_x = grad(Zn, bv, 2, m, 0, i, j, k), v_y = grad(Zn, bv, 2, m, 1, i, j, k);
+  const double v_z = grad(Zn, bv, 2, m, 2, i, j, k);
+  const double w_x = grad(Zn, bv, 3, m, 0, i, j, k), w_y = grad(Zn, bv, 3, m, 1, i, j, k);
+  const double w_z = grad(Zn, bv, 3, m, 2, i, j, k);
+  const double density = bv(i, j, k, 0);
+  const double omega = sv(i, j, k, 1);
+  const double k_x = grad(Zn, sv, 0, m, 0, i, j, k), k_y = grad(Zn, sv, 0, m, 1, i, j, k);
+  const double k_z = grad(Zn, sv, 0, m, 2, i, j, k);
+  const double omega_x = grad(Zn, sv, 1, m, 0, i, j, k), omega_y = grad(Zn, sv, 1, m, 1, i, j, k);
+  const double omega_z = grad(Zn, sv, 1, m, 2, i, j, k);
+  const double inter_var = 2 * density * sigma_omega2 / omega * (k_x * omega_x + k_y * omega_y + k_z * omega_z);
+  const double tke = sv(i, j, k, 0);
+  const double rhoK = density * tke;
+  const double vorticity =
+      std::sqrt((v_x - u_y) * (v_x - u_y) + (w_x - u_z) * (w_x - u_z) + (w_y - v_z) * (w_y - v_z));
+  double f1 = 1, f2 = 1;
+  const double dy = Zn.wall(i, j, k);
+  if (dy > 1e-25) {
+    const double param1 = std::sqrt(tke) / (0.09 * omega * dy);
+    const double d2 = dy * dy;
+    const double param2 = 500 * Zn.mul(i, j, k) / (density * d2 * omega);
+    const double arg2 = std::max(2 * param1, param2);
+    f2 = std::tanh(arg2 * arg2);
+    const double CDkomega = std::max(1e-20, inter_var);
+    const double param3 = 4 * density * sigma_omega2 * tke / (CDkomega * d2);
+    const double arg1 = std::min(std::max(param1, param2), param3);
+    f1 = std::tanh(arg1 * arg1 * arg1 * arg1);
+  }
+  double mut = 0;
+  const double denominator = std::max(a_1 * omega, vorticity * f2);
+  if (denominator > 1e-25) mut = a_1 * rhoK / denominator;
+  Zn.mut(i, j, k) = mut;
+  double beta = beta_2 + delta_beta * f1;
+  double betaStar = beta_star;
+  if (const int correction = P->compressibility_correction) {
+    const double Mt = std::sqrt(2 * tke / (gamma_air * bv(i, j, k, 4) / density));
+    double c;
+    switch (correction) {
+      case 1: c = wilcox(Mt); break;
+      case 2: c = beta_star * Mt * Mt; break;
+      default: c = zeman(Mt, gamma_air + 1.0); break;
+    }
+    betaStar += c;
+    beta -= c;
+  }
+  if (mut > 1e-25) {
+    const double divU = u_x + v_y + w_z;
+    const double divU2 = divU * divU;
+    double prod_k = mut * (2 * (u_x * u_x + v_y * v_y + w_z * w_z) - 2.0 / 3 * divU2 + (u_y + v_x) * (u_y + v_x) +
+                           (u_z + w_x) * (u_z + w_x) + (v_z + w_y) * (v_z + w_y)) -
+                    2.0 / 3 * rhoK * divU;
+    const double prod_k2 = mut * vorticity * vorticity;
+    if (prod_k > 10 * prod_k2) prod_k = prod_k2;
+    const double diss_k = betaStar * rhoK * omega;
+    const double jac = Zn.jac(i, j, k);
+    Zn.dq(i, j, k, 5) += jac * (prod_k - diss_k);
+    const double gamma = gamma2 + delta_gamma * f1;
+    const double prod_omega = gamma * density / mut * prod_k + (1 - f1) * inter_var;
+    const double diss_omega = beta * density * omega * omega;
+    Zn.dq(i, j, k, 6) += jac * (prod_omega - diss_omega);
+  }
+  constexpr double cp = gamma_air * R_u / mw_air / (gamma_air - 1);
+  Zn.ttc(i, j, k) = Zn.mut(i, j, k) * cp / P->Prt;
+}
+}  // namespace sst
+
 void viscous_face(const ostc_param *P, const Z &Zn, int d, int i, int j, int k, double *fv) {
   const int e[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
   const int i1 = i + e[d][0], j1 = j + e[d][1], k1 = k + e[d][2];
@@ -996,10 +1126,22 @@ void viscous_face(const ostc_param *P, const Z &Zn, int d, int i, int j, int k, 
   const double w_y = dw[0] * xi_y + dw[1] * eta_y + dw[2] * zeta_y;
   const double w_z = dw[0] * xi_z + dw[1] * eta_z + dw[2] * zeta_z;
   const double mul = 0.5 * (Zn.mul(i, j, k) + Zn.mul(i1, j1, k1));
-  const double viscosity = mul;
-  const double tau_xx = viscosity * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
-  const double tau_yy = viscosity * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
-  const double tau_zz = viscosity * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  const bool turb = is_sst(P);
+  const double mut = turb ? 0.5 * (Zn.mut(i, j, k) + Zn.mut(i1, j1, k1)) : 0.0;
+  const double viscosity = mul + mut;
+  double tau_xx = viscosity * (4 * u_x - 2 * v_y - 2 * w_z) / 3.0;
+  double tau_yy = viscosity * (4 * v_y - 2 * u_x - 2 * w_z) / 3.0;
+  double tau_zz = viscosity * (4 * w_z - 2 * u_x - 2 * v_y) / 3.0;
+  if (turb) {  // ViscousScheme.cuh:82-95
+    constexpr double delta_d = 1e-3;
+    const double dy_div_delta = std::min(0.5 * (Zn.wall(i, j, k) + Zn.wall(i1, j1, k1)) / delta_d, 1.0);
+    const double twoThirdrhoKm =
+        -2.0 / 3 * 0.5 * (Zn.bv(i, j, k, 0) * Zn.sv(i, j, k, 0) + Zn.bv(i1, j1, k1, 0) * Zn.sv(i1, j1, k1, 0)) *
+        dy_div_delta;
+    tau_xx += twoThirdrhoKm;
+    tau_yy += twoThirdrhoKm;
+    tau_zz += twoThirdrhoKm;
+  }
   const double tau_xy = viscosity * (u_y + v_x);
   const double tau_xz = viscosity * (u_z + w_x);
   const double tau_yz = viscosity * (v_z + w_y);
@@ -1016,7 +1158,8 @@ void viscous_face(const ostc_param *P, const Z &Zn, int d, int i, int j, int k, 
   const double t_x = dt[0] * xi_x + dt[1] * eta_x + dt[2] * zeta_x;
   const double t_y = dt[0] * xi_y + dt[1] * eta_y + dt[2] * zeta_y;
   const double t_z = dt[0] * xi_z + dt[1] * eta_z + dt[2] * zeta_z;
-  const double cond = 0.5 * (Zn.kappa(i, j, k) + Zn.kappa(i1, j1, k1));
+  double cond = 0.5 * (Zn.kappa(i, j, k) + Zn.kappa(i1, j1, k1));
+  if (turb) cond += 0.5 * (Zn.ttc(i, j, k) + Zn.ttc(i1, j1, k1));
   fv[4] = um * fv[1] + vm * fv[2] + wm * fv[3] + cond * (kxj * t_x + kyj * t_y + kzj * t_z);
   if (P->mix_model != OSTC_MIX_AIR) {
     const int ns = P->n_spec;
@@ -1059,6 +1202,36 @@ void viscous_face(const ostc_param *P, const Z &Zn, int d, int i, int j, int k, 
       fv[5 + l] = flux;
       fv[4] += h[l] * flux;
     }
+  }
+  if (turb) {  // k and omega diffusion, ViscousScheme.cuh:200-251
+    double dk[3], dw[3];
+    der(Zn.sv, 0, dk);
+    der(Zn.sv, 1, dw);
+    const double k_x = dk[0] * xi_x + dk[1] * eta_x + dk[2] * zeta_x;
+    const double k_y = dk[0] * xi_y + dk[1] * eta_y + dk[2] * zeta_y;
+    const double k_z = dk[0] * xi_z + dk[1] * eta_z + dk[2] * zeta_z;
+    const double omega_x = dw[0] * xi_x + dw[1] * eta_x + dw[2] * zeta_x;
+    const double omega_y = dw[0] * xi_y + dw[1] * eta_y + dw[2] * zeta_y;
+    const double omega_z = dw[0] * xi_z + dw[1] * eta_z + dw[2] * zeta_z;
+    const double wall_dist = 0.5 * (Zn.wall(i, j, k) + Zn.wall(i1, j1, k1));
+    double f1 = 1;
+    if (wall_dist > 1e-25) {
+      const double km = 0.5 * (Zn.sv(i, j, k, 0) + Zn.sv(i1, j1, k1, 0));
+      const double omegam = 0.5 * (Zn.sv(i, j, k, 1) + Zn.sv(i1, j1, k1, 1));
+      const double param1 = std::sqrt(km) / (0.09 * omegam * wall_dist);
+      const double rhom = 0.5 * (Zn.bv(i, j, k, 0) + Zn.bv(i1, j1, k1, 0));
+      const double d2 = wall_dist * wall_dist;
+      const double param2 = 500 * mul / (rhom * d2 * omegam);
+      const double CDkomega =
+          std::max(1e-20, 2 * rhom * sst::sigma_omega2 / omegam * (k_x * omega_x + k_y * omega_y + k_z * omega_z));
+      const double param3 = 4 * rhom * sst::sigma_omega2 * km / (CDkomega * d2);
+      const double arg1 = std::min(std::max(param1, param2), param3);
+      f1 = std::tanh(arg1 * arg1 * arg1 * arg1);
+    }
+    const double sigma_k = sst::sigma_k2 + sst::delta_sigma_k * f1;
+    const double sigma_omega = sst::sigma_omega2 + sst::delta_sigma_omega * f1;
+    fv[5] = (mul + mut * sigma_k) * (kxj * k_x + kyj * k_y + kzj * k_z);
+    fv[6] = (mul + mut * sigma_omega) * (kxj * omega_x + kyj * omega_y + kzj * omega_z);
   }
 }
 
@@ -1223,6 +1396,7 @@ void bc_symmetry(const ostc_param *P, Z &Zn, const ostc_bc_face &b) {  // BoundC
           Zn.bv(gi, gj, gk, 4) = Zn.bv(ii, ij, ik, 4);
           Zn.bv(gi, gj, gk, 5) = Zn.bv(ii, ij, ik, 5);
           for (int l = 0; l < P->n_scalar; ++l) Zn.sv(gi, gj, gk, l) = Zn.sv(ii, ij, ik, l);
+          if (is_sst(P)) Zn.mut(gi, gj, gk) = Zn.mut(ii, ij, ik);
         }
       }
 }
@@ -1237,6 +1411,7 @@ void bc_outflow(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) 
           const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
           for (int l = 0; l < 6; ++l) Zn.bv(gi, gj, gk, l) = Zn.bv(i, j, k, l);
           for (int l = 0; l < P->n_scalar; ++l) Zn.sv(gi, gj, gk, l) = Zn.sv(i, j, k, l);
+          if (is_sst(P)) Zn.mut(gi, gj, gk) = Zn.mut(i, j, k);
           if (with_cv) cv_from_bv_point(P, Zn, gi, gj, gk);
         }
 }
@@ -1252,6 +1427,7 @@ void bc_inflow(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
     Zn.bv(i, j, k, 4) = b.pressure;
     Zn.bv(i, j, k, 5) = b.temperature;
     for (int l = 0; l < P->n_scalar; ++l) Zn.sv(i, j, k, l) = b.sv[l];
+    if (is_sst(P)) Zn.mut(i, j, k) = b.mut;
   };
   for (int k = b.range_start[2]; k <= b.range_end[2]; ++k)
     for (int j = b.range_start[1]; j <= b.range_end[1]; ++j)
@@ -1296,6 +1472,12 @@ void bc_wall(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
         Zn.bv(i, j, k, 4) = p;
         Zn.bv(i, j, k, 5) = t_wall;
         Zn.vel(i, j, k) = 0;
+        if (is_sst(P)) {  // BoundCond.cuh:471-484
+          const double mu_wall = sutherland(t_wall);
+          const double dy = Zn.wall(ii, ij, ik);
+          Zn.sv(i, j, k, 0) = 0;
+          Zn.sv(i, j, k, 1) = dy > 1e-25 ? 60 * mu_wall / (rho_wall * sst::beta_1 * dy * dy) : Zn.sv(ii, ij, ik, 1);
+        }
         if (with_cv) cv_from_bv_point(P, Zn, i, j, k);
         for (int g = 1; g <= Zn.ngg; ++g) {
           const int ai = i - g * dir[0], aj = j - g * dir[1], ak = k - g * dir[2];
@@ -1321,6 +1503,11 @@ void bc_wall(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
           Zn.bv(gi, gj, gk, 3) = -w_i;
           Zn.bv(gi, gj, gk, 4) = p_i;
           Zn.bv(gi, gj, gk, 5) = t_g;
+          if (is_sst(P)) {  // BoundCond.cuh:536-541
+            Zn.sv(gi, gj, gk, 0) = 0;
+            Zn.sv(gi, gj, gk, 1) = Zn.sv(i, j, k, 1);
+            Zn.mut(gi, gj, gk) = 0;
+          }
           if (with_cv) cv_from_bv_point(P, Zn, gi, gj, gk);
         }
       }
@@ -1343,8 +1530,11 @@ void bc_farfield(const ostc_param *P, Z &Zn, const ostc_bc_face &b) {
         const double u_b = Zn.bv(i, j, k, 1), v_b = Zn.bv(i, j, k, 2), w_b = Zn.bv(i, j, k, 3);
         const double u_face = nx * u_b + ny * v_b + nz * w_b;
         double gamma_b = gamma_air, mw = mw_air, sv_b[MAXS + 4] = {0}, cp[MAXS];
+        // the point's own scalars; for air with SST the reference leaves sv_b
+        // unset on subsonic outflow (BoundCond.cuh:244, 330-336), where these are kept
+        for (int l = 0; l < nsc; ++l) sv_b[l] = Zn.sv(i, j, k, l);
+        const bool turb = is_sst(P);
         if (P->mix_model != OSTC_MIX_AIR) {
-          for (int l = 0; l < nsc; ++l) sv_b[l] = Zn.sv(i, j, k, l);
           gamma_b = Zn.gam(i, j, k);
           double mw_inv = 0;
           for (int l = 0; l < ns; ++l) mw_inv += sv_b[l] / P->mw[l];
@@ -1365,15 +1555,19 @@ void bc_farfield(const ostc_param *P, Z &Zn, const ostc_bc_face &b) {
         };
         if (mach_b <= -1) {
           set(i, j, k, b.density, b.u, b.v, b.w, b.pressure, b.temperature, b.sv);
+          if (turb) Zn.mut(i, j, k) = b.mut;
           Zn.vel(i, j, k) = std::sqrt(b.u * b.u + b.v * b.v + b.w * b.w);
-          for (int g = 1; g <= Zn.ngg; ++g)
+          for (int g = 1; g <= Zn.ngg; ++g) {
             set(i + g * dir[0], j + g * dir[1], k + g * dir[2], b.density, b.u, b.v, b.w, b.pressure, b.temperature,
                 b.sv);
+            if (turb) Zn.mut(i + g * dir[0], j + g * dir[1], k + g * dir[2]) = b.mut;
+          }
         } else if (mach_b >= 1) {
           for (int g = 1; g <= Zn.ngg; ++g) {
             const int gi = i + g * dir[0], gj = j + g * dir[1], gk = k + g * dir[2];
             for (int l = 0; l < 6; ++l) Zn.bv(gi, gj, gk, l) = Zn.bv(i, j, k, l);
             for (int l = 0; l < nsc; ++l) Zn.sv(gi, gj, gk, l) = Zn.sv(i, j, k, l);
+            if (turb) Zn.mut(gi, gj, gk) = Zn.mut(i, j, k);
           }
         } else {
           const double r_pos = u_face + 2 * a_b / (gamma_b - 1);
@@ -1381,6 +1575,8 @@ void bc_farfield(const ostc_param *P, Z &Zn, const ostc_bc_face &b) {
           const double r_neg = u_inf - 2 * b.acoustic_speed / (b.specific_heat_ratio - 1);
           const double Un = 0.5 * (r_pos + r_neg);
           double s_b, rho = 0, p = 0, T = 0, u, v, w;
+          double mut_b = 0;
+          if (turb) mut_b = (P->mix_model == OSTC_MIX_AIR ? mach_b <= 0 : mach_b < 0) ? b.mut : Zn.mut(i, j, k);
           if (P->mix_model == OSTC_MIX_AIR) {
             const double c_b = 0.25 * (gamma_air - 1) * (r_pos - r_neg);
             if (mach_b <= 0) {
@@ -1426,8 +1622,12 @@ void bc_farfield(const ostc_param *P, Z &Zn, const ostc_bc_face &b) {
             }
           }
           set(i, j, k, rho, u, v, w, p, T, sv_b);
+          if (turb) Zn.mut(i, j, k) = mut_b;
           Zn.vel(i, j, k) = std::sqrt(u * u + v * v + w * w);
-          for (int g = 1; g <= Zn.ngg; ++g) set(i + g * dir[0], j + g * dir[1], k + g * dir[2], rho, u, v, w, p, T, sv_b);
+          for (int g = 1; g <= Zn.ngg; ++g) {
+            set(i + g * dir[0], j + g * dir[1], k + g * dir[2], rho, u, v, w, p, T, sv_b);
+            if (turb) Zn.mut(i + g * dir[0], j + g * dir[1], k + g * dir[2]) = mut_b;
+          }
         }
       }
 }
@@ -1445,6 +1645,7 @@ void bc_back_pressure(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int wit
           Zn.bv(gi, gj, gk, 4) = b.pressure;
           Zn.bv(gi, gj, gk, 5) = Zn.bv(i, j, k, 5);
           for (int l = 0; l < P->n_scalar; ++l) Zn.sv(gi, gj, gk, l) = Zn.sv(i, j, k, l);
+          if (is_sst(P)) Zn.mut(gi, gj, gk) = Zn.mut(i, j, k);
           if (with_cv) cv_from_bv_point(P, Zn, gi, gj, gk);
         }
 }
@@ -1492,6 +1693,7 @@ void bc_subsonic_inflow(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int w
           Zn.bv(gi, gj, gk, 5) = T;
           const double u_bar = Zn.bv(gi, gj, gk, 1) * nx + Zn.bv(gi, gj, gk, 2) * ny + Zn.bv(gi, gj, gk, 3) * nz;
           for (int l = 0; l < P->n_scalar; ++l) Zn.sv(gi, gj, gk, l) = u_bar > 0 ? Zn.sv(i, j, k, l) : b.sv[l];
+          if (is_sst(P)) Zn.mut(gi, gj, gk) = Zn.mut(i, j, k);
           if (with_cv) cv_from_bv_point(P, Zn, gi, gj, gk);
         }
       }
@@ -1513,6 +1715,7 @@ void bc_periodic(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv)
           *s -= b.direction * n;
           for (int l = 0; l < 6; ++l) Zn.bv(gi, gj, gk, l) = Zn.bv(si, sj, sk, l);
           for (int l = 0; l < P->n_scalar; ++l) Zn.sv(gi, gj, gk, l) = Zn.sv(si, sj, sk, l);
+          if (is_sst(P)) Zn.mut(gi, gj, gk) = Zn.mut(si, sj, sk);
           Zn.vel(gi, gj, gk) = Zn.vel(si, sj, sk);
           if (with_cv)
             for (int l = 0; l < P->n_var; ++l) Zn.cv(gi, gj, gk, l) = Zn.cv(si, sj, sk, l);
@@ -1579,6 +1782,13 @@ void compute_rhs_zone(const ostc_param *P, Z &Zn) {
           chemistry_omega(P, Zn.bv(i, j, k, 0), Zn.bv(i, j, k, 5), Y, om, nullptr, nullptr);
           for (int l = 0; l < P->n_spec; ++l) Zn.dq(i, j, k, l + 5) += Zn.jac(i, j, k) * om[l];
         }
+  }
+  // compute_source<Air, SST>: mut, turbulent conductivity, k and omega sources
+  if (is_sst(P)) {
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < Zn.mz; ++k)
+      for (int j = 0; j < Zn.my; ++j)
+        for (int i = 0; i < Zn.mx; ++i) sst::source_and_mut(P, Zn, i, j, k);
   }
   // inviscid: x, y, then z when 3-D (InviscidScheme.cu:23-45, 176-204)
   inviscid_direction(P, Zn, 0);
@@ -1993,7 +2203,8 @@ double oracle_global_time_step(const ostc_param *P, ostc_zone *zones, int n_zone
           double gamma = gamma_air;
           if (P->mix_model != OSTC_MIX_AIR) gamma = Zn.gam(i, j, k);
           const double c1 = std::max(gamma, 4.0 / 3.0) / Zn.bv(i, j, k, 0);
-          const double c2 = Zn.mul(i, j, k) / P->Pr;
+          double c2 = Zn.mul(i, j, k) / P->Pr;
+          if (is_sst(P)) c2 += Zn.mut(i, j, k) / P->Prt;
           double srv = gx * gx + ge * ge;
           if (dim == 3) srv += gz * gz;
           srv *= c1 * c2;
@@ -2104,6 +2315,11 @@ int oracle_initialize(const ostc_config *c, const ostc_param *P, ostc_zone *zone
         for (int i = -g; i < Zn.mx + g; ++i)
           Zn.vel(i, j, k) = std::sqrt(Zn.bv(i, j, k, 1) * Zn.bv(i, j, k, 1) + Zn.bv(i, j, k, 2) * Zn.bv(i, j, k, 2) +
                                       Zn.bv(i, j, k, 3) * Zn.bv(i, j, k, 3));
+    if (is_sst(P))  // initialize_mut over [-1, m] (FieldOperation.cuh:175-195)
+      for (int k = -1; k <= Zn.mz; ++k)
+        for (int j = -1; j <= Zn.my; ++j)
+          for (int i = -1; i <= Zn.mx; ++i)
+            Zn.mut(i, j, k) = sst::compute_mut(Zn, i, j, k, sutherland(Zn.bv(i, j, k, 5)));
   }
   oracle_data_communication(P, zones, n_zones, 0);
   for (int b = 0; b < n_zones; ++b) oracle_update_physical_properties(P, &zones[b]);
