@@ -70,6 +70,7 @@ struct RefCtx {  // one block
 struct RefMulti {  // all blocks of a run
   ostc_config cfg{};
   int mix = 0;
+  int sst = 0;  // k-omega SST (air)
   std::vector<RefCtx *> blk;
 };
 
@@ -102,9 +103,9 @@ void build_param(RefCtx &c, const ostc_param *p) {
   d.limiter = p->limiter;
   d.entropy_fix_factor = p->entropy_fix_factor;
   d.viscous_scheme = p->viscous_scheme;
-  d.rans_model = 0;
+  d.rans_model = p->turbulence ? p->rans_model : 0;
   d.turb_implicit = 0;
-  d.compressibility_correction = 0;
+  d.compressibility_correction = p->turbulence ? p->compressibility_correction : 0;
   d.chemSrcMethod = p->chemSrcMethod;
   d.n_reac = p->mix_model == OSTC_MIX_FR ? p->n_reac : 0;
   d.Pr = p->Pr;
@@ -175,6 +176,14 @@ void build_zone(RefCtx &c, const ostc_zone *z, const ostc_param *p) {
   h.sv.allocate_memory(mx, my, mz, p->n_scalar, g);
   if (p->n_scalar) cudaMemcpy(h.sv.data(), z->sv, sizeof(double) * P * p->n_scalar, cudaMemcpyHostToDevice);
   h.rho_D.allocate_memory(mx, my, mz, p->n_spec, g);
+  if (p->turbulence) {  // SST arrays (Field.cu:196-207); the wall distance is an input here
+    h.wall_distance.allocate_memory(mx, my, mz, g);
+    cudaMemcpy(h.wall_distance.data(), z->wall_distance, sizeof(double) * P, cudaMemcpyHostToDevice);
+    h.mut.allocate_memory(mx, my, mz, g);
+    cudaMemset(h.mut.data(), 0, sizeof(double) * P);
+    h.turb_therm_cond.allocate_memory(mx, my, mz, g);
+    cudaMemset(h.turb_therm_cond.data(), 0, sizeof(double) * P);
+  }
   if (p->n_spec > 0) {
     h.gamma.allocate_memory(mx, my, mz, g);
     h.cp.allocate_memory(mx, my, mz, g);
@@ -207,7 +216,7 @@ void build_zone(RefCtx &c, const ostc_zone *z, const ostc_param *p) {
 }
 
 // one kernel launch per face, launch shape of DBoundCond::apply_boundary_conditions
-template <MixtureModel mix, bool with_cv>
+template <MixtureModel mix, class Turb, bool with_cv>
 void apply_bcs(RefCtx &c) {
   const int order[] = {4, 6, 9, 5, 7, 3, 2};
   for (int t : order) {
@@ -222,25 +231,25 @@ void apply_bcs(RefCtx &c) {
       }
       dim3 TPB{tpb[0], tpb[1], tpb[2]}, BPG{bpg[0], bpg[1], bpg[2]};
       switch (t) {
-        case 6: apply_outflow<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (integer)q, c.d_param); break;
+        case 6: apply_outflow<mix, Turb, with_cv><<<BPG, TPB>>>(c.d_zone, (integer)q, c.d_param); break;
         case 5:
-          apply_inflow<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, c.d_inflows[c.face_inflow[q]], (integer)q,
+          apply_inflow<mix, Turb, with_cv><<<BPG, TPB>>>(c.d_zone, c.d_inflows[c.face_inflow[q]], (integer)q,
                                                               c.d_param);
           break;
-        case 3: apply_symmetry<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (integer)q, c.d_param); break;
+        case 3: apply_symmetry<mix, Turb, with_cv><<<BPG, TPB>>>(c.d_zone, (integer)q, c.d_param); break;
         case 2:
-          apply_wall<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (Wall *)c.d_cond[q], c.d_param, (integer)q);
+          apply_wall<mix, Turb, with_cv><<<BPG, TPB>>>(c.d_zone, (Wall *)c.d_cond[q], c.d_param, (integer)q);
           break;
         case 4:
-          apply_farfield<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (FarField *)c.d_cond[q], (integer)q,
+          apply_farfield<mix, Turb, with_cv><<<BPG, TPB>>>(c.d_zone, (FarField *)c.d_cond[q], (integer)q,
                                                                 c.d_param);
           break;
         case 7:
-          apply_subsonic_inflow<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (SubsonicInflow *)c.d_cond[q],
+          apply_subsonic_inflow<mix, Turb, with_cv><<<BPG, TPB>>>(c.d_zone, (SubsonicInflow *)c.d_cond[q],
                                                                        c.d_param, (integer)q);
           break;
         case 9:
-          apply_back_pressure<mix, Laminar, with_cv><<<BPG, TPB>>>(c.d_zone, (BackPressure *)c.d_cond[q], c.d_param,
+          apply_back_pressure<mix, Turb, with_cv><<<BPG, TPB>>>(c.d_zone, (BackPressure *)c.d_cond[q], c.d_param,
                                                                      (integer)q);
           break;
         default: break;
@@ -251,7 +260,7 @@ void apply_bcs(RefCtx &c) {
 
 // data_communication (DataCommunication.cuh:27-56), inner faces only: one
 // inner_communication launch per face of every block, in block order
-template <MixtureModel mix, bool with_cv>
+template <MixtureModel mix, class Turb, bool with_cv>
 void communicate(RefMulti &m) {
   for (RefCtx *c : m.blk) {
     for (size_t l = 0; l < c->inner.size(); ++l) {
@@ -263,24 +272,25 @@ void communicate(RefMulti &m) {
       }
       dim3 TPB{tpb[0], tpb[1], tpb[2]}, BPG{bpg[0], bpg[1], bpg[2]};
       RefCtx *t = m.blk[c->inner_target[l]];
-      inner_communication<mix, Laminar, with_cv><<<BPG, TPB>>>(c->d_zone, t->d_zone, (integer)l, c->d_param);
+      inner_communication<mix, Turb, with_cv><<<BPG, TPB>>>(c->d_zone, t->d_zone, (integer)l, c->d_param);
     }
   }
 }
 
-template <MixtureModel mix>
+template <MixtureModel mix, class Turb>
 void initialize(RefMulti &m) {
   // Driver::initialize_computation (Driver.cu:39-98) + RK3_bv pre-loop (RK.cuh:40-49)
   dim3 tpb{8, 8, 4};
-  for (RefCtx *c : m.blk) apply_bcs<mix, false>(*c);
+  for (RefCtx *c : m.blk) apply_bcs<mix, Turb, false>(*c);
   for (RefCtx *c : m.blk) {
     const int ng_1 = 2 * c->ngg - 1;
     dim3 bpg{(unsigned)((c->mx + ng_1) / tpb.x + 1), (unsigned)((c->my + ng_1) / tpb.y + 1),
              (unsigned)((c->mz + ng_1) / tpb.z + 1)};
     compute_velocity<<<bpg, tpb>>>(c->d_zone);
+    if constexpr (TurbMethod<Turb>::hasMut) initialize_mut<mix, Turb><<<bpg, tpb>>>(c->d_zone, c->d_param);
   }
   cudaDeviceSynchronize();
-  communicate<mix, false>(m);
+  communicate<mix, Turb, false>(m);
   cudaDeviceSynchronize();
   for (RefCtx *c : m.blk) {
     const int ng_1 = 2 * c->ngg - 1;
@@ -296,19 +306,19 @@ void initialize(RefMulti &m) {
     dim3 bpg0{(unsigned)((c->mx - 1) / tpb.x + 1), (unsigned)((c->my - 1) / tpb.y + 1),
               (unsigned)((c->mz - 1) / tpb.z + 1)};
     store_last_step<<<bpg0, tpb>>>(c->d_zone);
-    compute_cv_from_bv<mix, Laminar><<<bpg, tpb>>>(c->d_zone, c->d_param);
+    compute_cv_from_bv<mix, Turb><<<bpg, tpb>>>(c->d_zone, c->d_param);
   }
   cudaDeviceSynchronize();
 }
 
-template <MixtureModel mix>
+template <MixtureModel mix, class Turb>
 void rhs(RefCtx &c) {
   dim3 tpb{8, 8, 4};
   dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
   cudaMemset(c.h.dq.data(), 0, c.h.dq.size() * c.n_var * sizeof(real));
-  compute_source<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param);
-  compute_inviscid_flux<mix, Laminar>(*c.block, c.d_zone, c.d_param, c.n_var, *c.parameter);
-  compute_viscous_flux<mix, Laminar>(*c.block, c.d_zone, c.d_param, c.n_var);
+  compute_source<mix, Turb><<<bpg, tpb>>>(c.d_zone, c.d_param);
+  compute_inviscid_flux<mix, Turb>(*c.block, c.d_zone, c.d_param, c.n_var, *c.parameter);
+  compute_viscous_flux<mix, Turb>(*c.block, c.d_zone, c.d_param, c.n_var);
 }
 
 double block_dt(RefCtx &c) {  // one block of global_time_step (TimeAdvanceFunc.cu:155-182)
@@ -341,7 +351,7 @@ void block_residual(RefCtx &c, double *r) {
   cudaMemcpy(r, c.h.bv_last.data(), 4 * sizeof(real), cudaMemcpyDeviceToHost);
 }
 
-template <MixtureModel mix>
+template <MixtureModel mix, class Turb>
 int steps(RefMulti &m, int n, double *res_hist, double *dt_hist) {
   // the body of RK3_bv's while loop (RK.cuh:89-170), all blocks
   dim3 tpb{8, 8, 4};
@@ -358,17 +368,17 @@ int steps(RefMulti &m, int n, double *res_hist, double *dt_hist) {
     for (RefCtx *c : m.blk)
       cudaMemcpy(c->h.qn.data(), c->h.cv.data(), c->h.cv.size() * sizeof(real) * c->n_var, cudaMemcpyDeviceToDevice);
     for (integer rk = 0; rk < 3; ++rk) {
-      for (RefCtx *c : m.blk) rhs<mix>(*c);
+      for (RefCtx *c : m.blk) rhs<mix, Turb>(*c);
       if (!m.cfg.fixed_time_step) {
-        for (RefCtx *c : m.blk) local_time_step<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
+        for (RefCtx *c : m.blk) local_time_step<mix, Turb><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
         dt = 1e+6;
         for (RefCtx *c : m.blk) dt = std::min(dt, block_dt(*c));
       }
       for (RefCtx *c : m.blk) {
-        update_cv_and_bv_rk<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param, dt, rk);
-        apply_bcs<mix, true>(*c);
+        update_cv_and_bv_rk<mix, Turb><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param, dt, rk);
+        apply_bcs<mix, Turb, true>(*c);
       }
-      communicate<mix, true>(m);
+      communicate<mix, Turb, true>(m);
       for (RefCtx *c : m.blk) update_physical_properties<mix><<<bpg(c, 1), tpb>>>(c->d_zone, c->d_param);
     }
     if (res_hist) {
@@ -436,13 +446,13 @@ int steady_steps(RefMulti &m, int n, double *res_hist) {
     if (res_hist)
       for (RefCtx *c : m.blk) store_last_step<<<bpg(c, -1), tpb>>>(c->d_zone);
     for (RefCtx *c : m.blk) {
-      rhs<mix>(*c);
+      rhs<mix, Laminar>(*c);
       local_time_step<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
       implicit_treatment_block<mix>(m, *c);
       update_bv<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
-      apply_bcs<mix, false>(*c);
+      apply_bcs<mix, Laminar, false>(*c);
     }
-    communicate<mix, false>(m);
+    communicate<mix, Laminar, false>(m);
     for (RefCtx *c : m.blk) update_physical_properties<mix><<<bpg(c, 1), tpb>>>(c->d_zone, c->d_param);
     if (res_hist) {
       double acc[4] = {0, 0, 0, 0};
@@ -602,7 +612,8 @@ extern "C" {
 int ref_create_multi(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, int nz, const ostc_bc_face *f,
                      int nf, const ostc_interface *ifc, int nif, void **out) {
   if (!cfg || !p || !z || !out || nz < 1) return 1;
-  if (p->turbulence || (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_FR)) return 5;
+  if (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_FR) return 5;
+  if (p->turbulence && (p->rans_model != 2 || p->mix_model != OSTC_MIX_AIR || cfg->steady)) return 5;
   for (int q = 0; q < nf; ++q)
     if (f[q].block < 0 || f[q].block >= nz) return 1;
   for (int q = 0; q < nif; ++q)
@@ -610,6 +621,7 @@ int ref_create_multi(const ostc_config *cfg, const ostc_param *p, const ostc_zon
   auto *m = new RefMulti;
   m->cfg = *cfg;
   m->mix = p->mix_model;
+  m->sst = p->turbulence ? 1 : 0;
   for (int b = 0; b < nz; ++b) {
     std::vector<ostc_bc_face> fb;
     std::vector<ostc_interface> ib;
@@ -640,22 +652,33 @@ int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, 
 
 int ref_initialize(void *h) {
   auto *m = (RefMulti *)h;
-  if (m->mix == OSTC_MIX_AIR) initialize<MixtureModel::Air>(*m); else initialize<MixtureModel::FR>(*m);
+  if (m->sst)
+    initialize<MixtureModel::Air, SST>(*m);
+  else if (m->mix == OSTC_MIX_AIR)
+    initialize<MixtureModel::Air, Laminar>(*m);
+  else
+    initialize<MixtureModel::FR, Laminar>(*m);
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 int ref_rhs(void *h) {
   auto *m = (RefMulti *)h;
   for (RefCtx *c : m->blk) {
-    if (m->mix == OSTC_MIX_AIR) rhs<MixtureModel::Air>(*c); else rhs<MixtureModel::FR>(*c);
+    if (m->sst)
+      rhs<MixtureModel::Air, SST>(*c);
+    else if (m->mix == OSTC_MIX_AIR)
+      rhs<MixtureModel::Air, Laminar>(*c);
+    else
+      rhs<MixtureModel::FR, Laminar>(*c);
   }
   return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
 }
 
 int ref_steps(void *h, int n, double *res_hist, double *dt_hist) {
   auto *m = (RefMulti *)h;
-  return m->mix == OSTC_MIX_AIR ? steps<MixtureModel::Air>(*m, n, res_hist, dt_hist)
-                                : steps<MixtureModel::FR>(*m, n, res_hist, dt_hist);
+  if (m->sst) return steps<MixtureModel::Air, SST>(*m, n, res_hist, dt_hist);
+  return m->mix == OSTC_MIX_AIR ? steps<MixtureModel::Air, Laminar>(*m, n, res_hist, dt_hist)
+                                : steps<MixtureModel::FR, Laminar>(*m, n, res_hist, dt_hist);
 }
 
 int ref_steady_steps(void *h, int n, double *res_hist) {
@@ -703,6 +726,8 @@ int ref_download_block(void *h, int b, const char *name, double *dst) {
   else if (!strcmp(name, "vel")) src = z.vel.data(), n = P;
   else if (!strcmp(name, "acoustic_speed")) src = z.acoustic_speed.data(), n = P;
   else if (!strcmp(name, "rho_D")) src = z.rho_D.data(), n = c->n_spec * P;
+  else if (!strcmp(name, "mut") && z.mut.data()) src = z.mut.data(), n = P;
+  else if (!strcmp(name, "turb_therm_cond") && z.turb_therm_cond.data()) src = z.turb_therm_cond.data(), n = P;
   else return 1;
   return cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : 2;
 }

@@ -94,8 +94,9 @@ class RefCudaRun:
         P = ostc.plane_shape(b.mx, b.my, b.mz, b.ngg)
         I = ostc.plane_shape(b.mx, b.my, b.mz, 0)
         Q = ostc.plane_shape(b.mx, b.my, b.mz, getattr(b, "dq_ngg", 0))
-        shapes = {"bv": (6,) + P, "sv": (b.n_spec,) + P, "cv": (b.n_var,) + P, "dq": (b.n_var,) + Q, "mul": P,
-                  "thermal_conductivity": P, "vel": P, "acoustic_speed": P, "rho_D": (b.n_spec,) + P}
+        shapes = {"bv": (6,) + P, "sv": (b.n_spec + b.n_turb,) + P, "cv": (b.n_var,) + P, "dq": (b.n_var,) + Q,
+                  "mul": P, "thermal_conductivity": P, "vel": P, "acoustic_speed": P, "rho_D": (b.n_spec,) + P,
+                  "mut": P, "turb_therm_cond": P}
         out = np.zeros(shapes[name])
         assert ref().ref_download_block(self.h, block, name.encode(), out.ctypes.data_as(C.POINTER(C.c_double))) == 0
         return out

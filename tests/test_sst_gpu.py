@@ -99,3 +99,49 @@ def test_sst_split_flux_kernels():
     for b in range(len(blocks)):
         assert max(rhs_errors(blocks[b].download("dq"), fused[b], scales[b])) <= 1e-13, b
     s.close()
+
+
+@pytest.mark.skipif(not __import__("ref_bind").available(), reason="reference build (oracle/_ref) not present")
+def test_sst_matches_reference_build():
+    """The reference's own SST kernels (Driver<Air, SST> sequence) on the same
+    blocks: initial mut, one RHS (1e-11), and the states after 5 steps at a
+    fixed dt (the reference's block reductions are undefined for some of
+    these block sizes, quirk A19). The far-field j-max faces are replaced by
+    outflow faces: for air with SST the reference's subsonic far field reads
+    uninitialised boundary scalars (BoundCond.cuh:244, 330-336)."""
+    import ref_bind
+
+    case = _case("hllc_muscl")
+    for f in case.faces:
+        if f.type_label == ostc.BC_FARFIELD:
+            f.type_label = ostc.BC_OUTFLOW
+    case.scheme.fixed_time_step = 1
+    case.scheme.dt = 2e-8
+    r = ref_bind.RefCudaRun(case)
+    r.initialize()
+    o = OracleRun(case)
+    o.initialize()
+    scales = [o.flux_scale(b) for b in range(len(case.blocks))]
+    s, blocks = case.solver()
+    s.initialize()
+    for b in range(len(blocks)):
+        mr = r.download("mut", b)
+        assert np.max(np.abs(blocks[b].download("mut") - mr)) <= 1e-12 * np.max(np.abs(mr)), b
+    r.compute_rhs()
+    s.compute_rhs()
+    for b in range(len(blocks)):
+        assert max(rhs_errors(blocks[b].download("dq"), r.download("dq", b), scales[b])) <= 1e-11, b
+        mr = r.download("mut", b)
+        assert np.max(np.abs(blocks[b].download("mut") - mr)) <= 1e-12 * np.max(np.abs(mr)), b
+    s.close()
+    n = 5
+    r2 = ref_bind.RefCudaRun(case)
+    r2.initialize()
+    r2.rk3_steps(n)
+    s2, blocks2 = case.solver()
+    s2.initialize()
+    s2.rk3_steps(n)
+    for b in range(len(blocks2)):
+        assert max(_state_errors(blocks2[b].download("bv"), r2.download("bv", b))) <= 1e-9, b
+        assert max(_state_errors(blocks2[b].download("sv"), r2.download("sv", b))) <= 1e-9, b
+    s2.close()
