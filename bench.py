@@ -68,7 +68,7 @@ def _make_case(name, full_host=False):
     if name == "mixing96":
         return ostc.case_mixing_layer(96, 96, 96, full_host=full_host)
     if name == "blocks37":
-        return ostc.case_uneven_blocks()
+        return ostc.case_uneven_blocks(rans_model=2)
     return ostc.case_vortex(128, 128, 8)
 
 
@@ -80,7 +80,7 @@ def _scheme_text(case):
     inv = {1: "L-F", 2: "Roe", 3: "AUSM+", 4: "HLLC"}[sc.inviscid_scheme]
     if sc.reconstruction == 4 and sc.inviscid_scheme == 2:
         inv = "AUSM+"  # quirk A1
-    vis = "laminar" if sc.viscous_order else "inviscid"
+    vis = ("k-omega SST" if sc.rans_model == 2 else "laminar") if sc.viscous_order else "inviscid"
     chem = ", finite-rate chemistry" if case.mech is not None else ""
     blocks = ", %d blocks" % len(case.blocks) if len(case.blocks) > 1 else ""
     return "%s+%s, %s%s, SSPRK3 CFL %.1f%s" % (rec, inv, vis, chem, sc.cfl, blocks)
@@ -143,7 +143,7 @@ def kernel_table(solver, case, reps=3):
     ops = [("flux_x", solver.OP_FLUX, 0, 3), ("flux_y", solver.OP_FLUX, 1, 3), ("flux_z", solver.OP_FLUX, 2, 3),
            ("properties", solver.OP_PROPERTIES, 0, 3), ("update_rk", solver.OP_UPDATE, 1, 3),
            ("dt", solver.OP_DT, 0, 3), ("bc", solver.OP_BC, 1, 3)]
-    if case.scheme.mix_model == 2:
+    if case.scheme.mix_model == 2 or case.scheme.rans_model == 2:  # chemistry or SST source
         ops.insert(3, ("source", solver.OP_SOURCE, 0, 3))
     out = {}
     for name, op, arg, per_step in ops:
@@ -163,17 +163,18 @@ def algorithmic_bytes(name, case):
     """Minimum HBM bytes of one launch of a kernel family on this workload
     (each input plane read once, each output plane written once)."""
     ns = case.mech.n_spec if case.mech else 0
-    nv = 5 + ns
+    nt = 2 if case.scheme.rans_model == 2 else 0
+    nv = 5 + ns + nt
     cells = case.cells  # one launch covers every block (tile-table launches)
-    props = 2 + (ns + 2 if ns else 0)  # mu, kappa (+ rho*D_k, cp, gamma)
+    props = 2 + (ns + 2 if ns else 0) + (3 if nt else 0)  # mu, kappa (+ rho*D_k, cp, gamma) (+ mut, kt, d)
     per_cell = {
         # state (bv 6, sv), geometry (9 metric + jac), properties read; dq read+written
-        "flux_x": 6 + ns + 10 + props + 2 * nv,
-        "flux_y": 6 + ns + 10 + props + 2 * nv,
-        "flux_z": 6 + ns + 10 + props + 2 * nv,
-        "source": 2 + ns + 1 + nv,
+        "flux_x": 6 + ns + nt + 10 + props + 2 * nv,
+        "flux_y": 6 + ns + nt + 10 + props + 2 * nv,
+        "flux_z": 6 + ns + nt + 10 + props + 2 * nv,
+        "source": (2 + ns + 1 + nv) if not nt else (6 + nt + 10 + 1 + 1 + nv + 2),
         "properties": 6 + ns + 1 + props + 3,
-        "update_rk": 3 * nv + 1 + nv + 6 + ns + 1,
+        "update_rk": 3 * nv + 1 + nv + 6 + ns + nt + 1,
         "dt": 9 + 6 + 3,
         "bc": 0,
     }[name]
@@ -412,14 +413,16 @@ def step_bytes_per_cell(case):
     sv) and geometry (9 metric + jac) read and bv, sv, cv written; stages 2-3
     read u^n. Derived properties are recomputed, not counted."""
     ns = case.mech.n_spec if case.mech else 0
-    nv = 5 + ns
-    return 8 * (3 * (6 + ns + 10) + 2 * nv + 3 * (6 + ns + nv))
+    nt = 2 if case.scheme.rans_model == 2 else 0  # SST: k, omega and the wall distance
+    nsc, nv, geo = ns + nt, 5 + ns + nt, 10 + (1 if nt else 0)
+    return 8 * (3 * (6 + nsc + geo) + 2 * nv + 3 * (6 + nsc + nv))
 
 
 def state_bytes(case):
     ns = case.mech.n_spec if case.mech else 0
-    return sum(8.0 * (6 + ns + 10 + 2 * (5 + ns)) * (b.mx + 2 * b.ngg) * (b.my + 2 * b.ngg) * (b.mz + 2 * b.ngg)
-               for b in case.blocks)
+    nt = 2 if case.scheme.rans_model == 2 else 0
+    return sum(8.0 * (6 + ns + nt + 10 + 2 * (5 + ns + nt)) * (b.mx + 2 * b.ngg) * (b.my + 2 * b.ngg) *
+               (b.mz + 2 * b.ngg) for b in case.blocks)
 
 
 def run_e2e(a, case, tiles=None):
@@ -489,7 +492,7 @@ def cpu_sample(a, budget_s=15.0):
     elif a.workload == "blocks37":
         case = ostc.case_uneven_blocks(layout=ostc.block_layout(5, dims=(80, 64, 64), ranges=((16, 40), (16, 28),
                                                                                               (16, 20)),
-                                                                anchors=False))
+                                                                anchors=False), rans_model=2)
     else:
         case = ostc.case_vortex(128, 128, 8)
     r = Run(case)
@@ -525,7 +528,9 @@ def reference_cuda_build(a, ours_value):
 
     case = _make_case(a.workload)
     for f in case.faces:
-        if f.type_label == ostc.BC_PERIODIC:
+        # no periodic boundary in the reference; its air + SST far field reads
+        # unset boundary scalars on subsonic outflow: both become outflow faces
+        if f.type_label == ostc.BC_PERIODIC or (case.scheme.rans_model and f.type_label == ostc.BC_FARFIELD):
             f.type_label = ostc.BC_OUTFLOW
     r = ref_bind.RefCudaRun(case)
     r.initialize()
@@ -535,7 +540,8 @@ def reference_cuda_build(a, ours_value):
     v = case.cells * n / (ms * 1e-3) / 1e6
     return {"value": round(v, 2), "unit": "Mcell-updates/s", "steps": n, "ms_per_step": round(ms / n, 3),
             "speedup_ours_over_reference_build": round(ours_value / v, 2),
-            "note": "reference sources compiled for sm_100a, same workload, extrapolation faces instead of periodic"}
+            "note": "reference sources compiled for sm_100a, same workload, extrapolation faces instead of periodic"
+                    " (and of the SST far field)"}
 
 
 def run_reference(a):
@@ -563,7 +569,7 @@ def run_reference(a):
 
 def _make_case_name(w):
     return {"mixing256": "mixing_layer_h2air_256x256x256", "mixing96": "mixing_layer_h2air_96x96x96",
-            "blocks37": "uneven_blocks_37_air_10453312cells"}.get(w, "vortex_air_128x128x8")
+            "blocks37": "uneven_blocks_37_air_sst_10453312cells"}.get(w, "vortex_air_128x128x8")
 
 
 if __name__ == "__main__":
