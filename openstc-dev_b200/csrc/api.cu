@@ -250,6 +250,7 @@ void fill_devzone(const ostc_zone &z, DevZone &d) {
   d.dt_local = z.dt_local;
   d.bv_last = z.bv_last;
   d.isr = nullptr;
+  d.tsj = z.turb_src_jac;
   d.jac = z.jac;
 }
 
@@ -260,7 +261,8 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
   if (sst) {
     // k-omega SST (rans_model 2): air, RK3, primitive-variable reconstruction with AUSM+ or HLLC
     if (p->rans_model != 2) return OSTC_ERR_UNSUPPORTED;
-    if (p->mix_model != OSTC_MIX_AIR || cfg->steady || cfg->chem_mode != 0) return OSTC_ERR_UNSUPPORTED;
+    if (p->mix_model != OSTC_MIX_AIR || cfg->chem_mode != 0) return OSTC_ERR_UNSUPPORTED;
+    if (p->turb_implicit != 0 && p->turb_implicit != 1) return OSTC_ERR_INVALID_ARG;
     if (p->inviscid_type != 0 || (p->inviscid_scheme != 3 && p->inviscid_scheme != 4)) return OSTC_ERR_UNSUPPORTED;
     if (p->viscous_scheme == 0) return OSTC_ERR_UNSUPPORTED;
     if (p->n_spec != 0 || p->n_scalar != 2 || p->n_var != 7 || p->i_turb_cv != 5) return OSTC_ERR_INVALID_ARG;
@@ -365,6 +367,7 @@ void build_devparam(const ostc_param *p, DevParam &d) {
   d.turbulence = p->turbulence;
   d.sst = p->turbulence && p->rans_model == 2 ? 1 : 0;
   d.comp_corr = d.sst ? p->compressibility_correction : 0;
+  d.turb_implicit = d.sst ? p->turb_implicit : 0;
   d.Pr = p->Pr;
   d.Prt = p->Prt;
   d.Sct = p->Sct;
@@ -554,6 +557,10 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
       if (!isr) return fail(ctx, OSTC_ERR_CUDA, cudaErrorMemoryAllocation);
       z.isr = isr;
       c->isr.push_back(isr);
+      if (c->dp.sst && c->dp.turb_implicit == 1 && !z.tsj) {  // SST source Jacobian, 2 interior planes
+        z.tsj = (double *)alloc(sizeof(double) * 2 * z.nsz);
+        if (!z.tsj) return fail(ctx, OSTC_ERR_CUDA, cudaErrorMemoryAllocation);
+      }
       double *d0 = nullptr, *dk = nullptr, *lu = nullptr, *da = nullptr;
       unsigned char *pv = nullptr;
       if (dplur) {
@@ -947,11 +954,14 @@ ostc_status ostc_implicit_treatment(ostc_ctx *ctx, void *stream) {
   if (ensure_param(ctx, S(stream))) return ctx->last;
   cudaStream_t s = S(stream);
   if (ctx->cfg.implicit_method == 0) {
-    if (!ctx->has_source || ctx->prm.chemSrcMethod == 0) return OSTC_OK;
-    for (auto &z : ctx->dz)
-      CK(dispatch_ns(ctx->ns, [&](auto n) {
-        return launch_steady<decltype(n)::value>(SteadyOp::ChemImplicit, z, SteadyArgs{}, nullptr, s);
-      }));
+    // ImplicitTreatmentHPP.cuh:11-48: the chemistry's EPI / DA, then SST's point-implicit k, omega sources
+    if (ctx->has_source && ctx->prm.chemSrcMethod != 0)
+      for (auto &z : ctx->dz)
+        CK(dispatch_ns(ctx->ns, [&](auto n) {
+          return launch_steady<decltype(n)::value>(SteadyOp::ChemImplicit, z, SteadyArgs{}, nullptr, s);
+        }));
+    if (ctx->dp.sst && ctx->dp.turb_implicit == 1)
+      for (auto &z : ctx->dz) CK(launch_steady<0>(SteadyOp::TurbImplicit, z, SteadyArgs{}, nullptr, s));
     return OSTC_OK;
   }
   // DPLUR (DPLUR.cuh:283-312): no exchange between blocks inside the sweeps (quirk A11)

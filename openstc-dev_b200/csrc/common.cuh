@@ -25,7 +25,7 @@ struct DevParam {
   int n_var, n_scalar, n_spec, n_reac;
   int mix, inviscid_scheme, reconstruction, limiter, inviscid_type, viscous_scheme;
   int chemSrcMethod, gradP, dimension, turbulence, need_gibbs, sst;  // sst: k-omega SST scalars in sv
-  int comp_corr, pad_;                                                // SST compressibility correction 0..3
+  int comp_corr, turb_implicit;  // SST: compressibility correction 0..3; point-implicit k, omega sources (steady)
   double Pr, Prt, Sct, Sc, cfl, entropy_fix_factor;
   double mw[MAXS], imw[MAXS], Rmw[MAXS];           // W_k, 1/W_k, R_u/W_k
   double lo[MAXS][7], hi[MAXS][7];                 // NASA-7 low / high ranges
@@ -63,6 +63,7 @@ struct DevZone {
   double *vel, *a, *mach, *mul, *kappa, *rhoD, *gam, *cp, *mut, *ttc, *wall;
   double *dt_local, *bv_last;
   double *isr;  // inviscid spectral radii, 3 interior planes (steady path; null otherwise)
+  double *tsj;  // SST source Jacobian diagonal, 2 interior planes (steady path with turb_implicit; else null)
   const double *jac;
   const double *met;  // 9 SoA planes (context-owned copy), ghosted layout
   int block_id;

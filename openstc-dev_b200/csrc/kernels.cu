@@ -45,9 +45,14 @@ __device__ __forceinline__ void source_cells(const DevZone &z, const int bx, con
   for (int l = 0; l < 5; ++l) dq[l * z.qsz] = 0;
   if constexpr (NS == 0) {
     if (c_p.sst) {  // SST::compute_source_and_mut and the turbulent conductivity (SourceTerm.cuh:19-27)
-      double mut, sk, sw;
-      sst::source_point(z, g, mut, sk, sw);
+      double mut, sk, sw, jk, jw;
+      sst::source_point(z, g, mut, sk, sw, jk, jw);
       z.mut[g] = mut;
+      if (c_p.turb_implicit == 1 && z.tsj) {  // SST.cu:243-246
+        const int n = nidx(z, i, j, k);
+        z.tsj[n] = jk;
+        z.tsj[z.nsz + n] = jw;
+      }
       constexpr double cpa = gamma_air * R_u / mw_air / (gamma_air - 1);
       z.ttc[g] = mut * cpa / c_p.Prt;
       dq[5 * z.qsz] = sk;
@@ -1074,6 +1079,9 @@ cudaError_t launch_steady(SteadyOp op, const DevZone &z, const SteadyArgs &a, co
       break;
     case SteadyOp::UpdateBv:
       update_bv_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z);
+      break;
+    case SteadyOp::TurbImplicit:
+      turb_implicit_kernel<<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z);
       break;
     case SteadyOp::DplurDq0:
       dplur_dq0_kernel<NS><<<plane_grid(z.mx, z.my, z.mz, blk4), blk4, 0, s>>>(z, a);

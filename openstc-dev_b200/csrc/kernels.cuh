@@ -74,7 +74,7 @@ struct CellArgs {
 };
 
 // the steady path (steady.cuh)
-enum class SteadyOp { ChemImplicit, UpdateBv, DplurDq0, DplurSweep, DplurFinish, WallDqZero };
+enum class SteadyOp { ChemImplicit, UpdateBv, DplurDq0, DplurSweep, DplurFinish, WallDqZero, TurbImplicit };
 struct SteadyArgs {
   const double *dq_in = nullptr;  // DPLUR sweep: current iterate (dq layout)
   double *dq_out = nullptr;       // DPLUR sweep: next iterate

@@ -74,10 +74,11 @@ __device__ __forceinline__ double mut_point(const DevZone &z, int g, double mul)
   return mut;
 }
 
-// SST::compute_source_and_mut (SST.cu:99-247) at interior point g: writes
-// mut and, through the caller, the k and omega sources (zero when mut <= 1e-25)
+// SST::compute_source_and_mut (SST.cu:99-247) at interior point g: mut, the k
+// and omega sources (zero when mut <= 1e-25) and the diagonal source Jacobian
+// (-2 beta* omega, -2 beta omega) the steady path's implicit treatment uses
 __device__ __forceinline__ void source_point(const DevZone &z, int g, double &mut_out, double &src_k,
-                                             double &src_w) {
+                                             double &src_w, double &jac_k, double &jac_w) {
   double m[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) m[c] = z.met[c * z.sz + g];
@@ -124,6 +125,8 @@ __device__ __forceinline__ void source_point(const DevZone &z, int g, double &mu
     betaStar += corr;
     beta -= corr;
   }
+  jac_k = -2 * betaStar * omega;
+  jac_w = -2 * beta * omega;
   src_k = 0;
   src_w = 0;
   if (mut > 1e-25) {

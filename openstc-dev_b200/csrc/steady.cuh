@@ -100,6 +100,8 @@ __global__ void __launch_bounds__(256) update_bv_kernel(DevZone z) {
   z.bv[3 * S + g] = w;
   const double Et = E + dq[4 * Q] * dtj;
   const double V2 = u * u + v * v + w * w;
+  // scalars after the species (SST k, omega), FieldOperation.cuh:252-257
+  for (int l = NS; l < c_p.n_scalar; ++l) z.sv[l * S + g] = ri * (rho_n * z.sv[l * S + g] + dq[(5 + l) * Q] * dtj);
   if constexpr (NS > 0) {
     double Y[NS];
 #pragma unroll
@@ -142,9 +144,30 @@ __global__ void __launch_bounds__(256) update_bv_kernel(DevZone z) {
 // ---------------------------------------------------------------------------
 // DPLUR
 // ---------------------------------------------------------------------------
+// NVX: the largest variable count of the build (air may carry the two SST
+// scalars); the variables beyond c_p.n_var are not touched
+template <int NS>
+constexpr int nvx() {
+  return 5 + NS + (NS == 0 ? 2 : 0);
+}
+
+// SST::implicit_treat_for_SST under the explicit steady path (SST.cu:8-22)
+__global__ void __launch_bounds__(256) turb_implicit_kernel(DevZone z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= z.mx || j >= z.my) return;
+  const int n = nidx(z, i, j, k);
+  double *dq = z.dq + qidx(z, i, j, k);
+  const double dt = z.dt_local[n];
+  dq[5 * z.qsz] /= 1 - dt * z.tsj[n];
+  dq[6 * z.qsz] /= 1 - dt * z.tsj[z.nsz + n];
+}
+
 template <int NS>
 __global__ void __launch_bounds__(128) dplur_dq0_kernel(DevZone z, SteadyArgs a) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = nvx<NS>();
+  const int nv = c_p.n_var;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -154,7 +177,7 @@ __global__ void __launch_bounds__(128) dplur_dq0_kernel(DevZone z, SteadyArgs a)
   const double dt = z.dt_local[n];
   double d[NV];
 #pragma unroll
-  for (int l = 0; l < NV; ++l) d[l] = dq[l * z.qsz] * dt;
+  for (int l = 0; l < NV; ++l) d[l] = l < nv ? dq[l * z.qsz] * dt : 0.0;
   const double diag = 1 + dt * (z.isr[n] + z.isr[z.nsz + n] + z.isr[2 * z.nsz + n]);
 #pragma unroll
   for (int l = 0; l < 5; ++l) d[l] /= diag;
@@ -198,10 +221,23 @@ __global__ void __launch_bounds__(128) dplur_dq0_kernel(DevZone z, SteadyArgs a)
       for (int l = 5; l < NV; ++l) d[l] /= diag;
     }
   }
+  if constexpr (NS == 0) {
+    if (c_p.sst) {  // DPLUR.cuh:72-84 with SST::implicit_treat_for_dq0 (SST.cu:249-258)
+      if (c_p.turb_implicit == 1) {
+        d[5] /= diag - dt * z.tsj[n];
+        d[6] /= diag - dt * z.tsj[z.nsz + n];
+      } else {
+        d[5] /= diag;
+        d[6] /= diag;
+      }
+    }
+  }
 #pragma unroll
   for (int l = 0; l < NV; ++l) {
-    dq[l * z.qsz] = d[l];
-    a.dq0[q + l * z.qsz] = d[l];
+    if (l < nv) {
+      dq[l * z.qsz] = d[l];
+      a.dq0[q + l * z.qsz] = d[l];
+    }
   }
 }
 
@@ -210,7 +246,8 @@ __global__ void __launch_bounds__(128) dplur_dq0_kernel(DevZone z, SteadyArgs a)
 template <int NS>
 __device__ __forceinline__ void jacobian_times_dq(const DevZone &z, const double *dqv, int i, int j, int k, int dir,
                                                   double lambda, double *out) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = nvx<NS>();
+  const int nv = c_p.n_var;
   const int g = gidx(z, i, j, k);
   const int q = qidx(z, i, j, k);
   const double kx = met(z, g, 3 * dir), ky = met(z, g, 3 * dir + 1), kz = met(z, g, 3 * dir + 2);
@@ -222,7 +259,7 @@ __device__ __forceinline__ void jacobian_times_dq(const DevZone &z, const double
   const double e = 0.5 * vel * vel;
   double dqp[NV];
 #pragma unroll
-  for (int l = 0; l < NV; ++l) dqp[l] = dqv[q + l * Q];
+  for (int l = 0; l < NV; ++l) dqp[l] = l < nv ? dqv[q + l * Q] : 0.0;
   double gamma = gamma_air, b3 = 0, b4 = 0, h = 0;
   if constexpr (NS == 0) {
     h = gamma / (gamma - 1) * z.bv[4 * S + g] / z.bv[g] + e;
@@ -250,11 +287,15 @@ __device__ __forceinline__ void jacobian_times_dq(const DevZone &z, const double
   out[4] = h * b1 + U * b2 + lmd1 * dqp[4] + U * (b3 - b4);
 #pragma unroll
   for (int l = 0; l < NS; ++l) out[5 + l] = lmd1 * dqp[5 + l] + z.sv[l * S + g] * b1;
+#pragma unroll
+  for (int l = NS; l < NV - 5; ++l)  // SST k, omega (n_scalar_transported rows, DPLUR.cuh:131-139)
+    out[5 + l] = l < c_p.n_scalar ? lmd1 * dqp[5 + l] + z.sv[l * S + g] * b1 : 0.0;
 }
 
 template <int NS>
 __global__ void __launch_bounds__(128) dplur_sweep_kernel(DevZone z, SteadyArgs a) {
-  constexpr int NV = 5 + NS;
+  constexpr int NV = nvx<NS>();
+  const int nv = c_p.n_var;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -323,12 +364,21 @@ __global__ void __launch_bounds__(128) dplur_sweep_kernel(DevZone z, SteadyArgs 
       for (int l = 5; l < NV; ++l) out[l] = a.dq0[q + l * z.qsz] + dt * tot[l] / diag;
     }
   }
+  if constexpr (NS == 0) {
+    if (c_p.sst) {  // DPLUR.cuh:262-276 with SST::implicit_treat_for_dqk (SST.cu:260-273)
+      const double d5 = c_p.turb_implicit == 1 ? diag - dt * z.tsj[n] : diag;
+      const double d6 = c_p.turb_implicit == 1 ? diag - dt * z.tsj[N + n] : diag;
+      out[5] = a.dq0[q + 5 * z.qsz] + dt * tot[5] / d5;
+      out[6] = a.dq0[q + 6 * z.qsz] + dt * tot[6] / d6;
+    }
+  }
   if (a.final_div) {
 #pragma unroll
     for (int l = 0; l < NV; ++l) out[l] /= dt;
   }
 #pragma unroll
-  for (int l = 0; l < NV; ++l) a.dq_out[q + l * z.qsz] = out[l];
+  for (int l = 0; l < NV; ++l)
+    if (l < nv) a.dq_out[q + l * z.qsz] = out[l];
 }
 
 // dq <- src / dt_local (src may be dq itself)
@@ -340,8 +390,7 @@ __global__ void __launch_bounds__(256) dplur_finish_kernel(DevZone z, const doub
   if (i >= z.mx || j >= z.my) return;
   const int q = qidx(z, i, j, k);
   const double dt = z.dt_local[nidx(z, i, j, k)];
-#pragma unroll
-  for (int l = 0; l < 5 + NS; ++l) z.dq[q + l * z.qsz] = src[q + l * z.qsz] / dt;
+  for (int l = 0; l < c_p.n_var; ++l) z.dq[q + l * z.qsz] = src[q + l * z.qsz] / dt;
 }
 
 // zero dq on a wall face range; points outside dq's allocation are skipped
@@ -354,8 +403,7 @@ __global__ void wall_dq_zero_kernel(DevZone z, BcFace b, double *dqv) {
   const int qg = z.qt == 0 ? 0 : 1;
   if (i < -qg || j < -qg || k < -qg || i >= z.mx + qg || j >= z.my + qg || k >= z.mz + qg) return;
   const int q = qidx(z, i, j, k);
-#pragma unroll
-  for (int l = 0; l < 5 + NS; ++l) dqv[q + l * z.qsz] = 0;
+  for (int l = 0; l < c_p.n_var; ++l) dqv[q + l * z.qsz] = 0;
 }
 
 }  // namespace ostc

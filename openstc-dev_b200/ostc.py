@@ -219,6 +219,7 @@ class Scheme:
     chem_mode: int = 0            # RK3 chemistry: 0 source in the RHS, 1 split FP64, 2 split surrogate
     rans_model: int = 0           # 0 laminar, 2 k-omega SST (air)
     compressibility_correction: int = 0  # SST: 0 none, 1 Wilcox, 2 Sarkar, 3 Zeman
+    turb_implicit: int = 1        # SST, steady path: point-implicit k and omega sources (DParameter default)
     steady: int = 0               # 1: local time stepping (steady_simulation)
     implicit_method: int = 0      # steady: 0 explicit (+ EPI/DA chemistry), 1 DPLUR
     dplur_inner_step: int = 3
@@ -259,7 +260,7 @@ def make_param(s: Scheme, mech: Optional[Mechanism]):
     p.inviscid_type = s.inviscid_type
     p.viscous_scheme = s.viscous_order
     p.rans_model = s.rans_model
-    p.turb_implicit = 0
+    p.turb_implicit = s.turb_implicit if nt else 0
     p.compressibility_correction = s.compressibility_correction if nt else 0
     p.chemSrcMethod = s.chemSrcMethod
     p.gradPInDiffusionFlux = s.gradPInDiffusionFlux
@@ -328,6 +329,7 @@ class HostBlock:
         if n_turb:
             for n in ("mut", "turb_therm_cond", "wall_distance"):
                 sp[n] = (P, f8)
+            sp["turb_src_jac"] = ((2,) + I, f8)
         sp["dt_local"] = (I, f8)
         sp["bv_last"] = ((4,) + I, f8)
         return sp

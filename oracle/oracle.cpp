@@ -60,7 +60,7 @@ struct MetricView {
 struct Z {  // a zone with views
   const ostc_zone *z;
   int mx, my, mz, ngg;
-  View bv, sv, cv, qn, dq, jac, vel, a, mach, mul, kappa, rhoD, gam, cp, dt_local, bv_last, mut, ttc, wall;
+  View bv, sv, cv, qn, dq, jac, vel, a, mach, mul, kappa, rhoD, gam, cp, dt_local, bv_last, mut, ttc, wall, tsj;
   MetricView metric;
   explicit Z(const ostc_zone *zz) : z(zz), mx(zz->mx), my(zz->my), mz(zz->mz), ngg(zz->ngg) {
     const int g = ngg;
@@ -81,6 +81,7 @@ struct Z {  // a zone with views
     mut = View(zz->mut, mx, my, mz, g);
     ttc = View(zz->turb_therm_cond, mx, my, mz, g);
     wall = View(zz->wall_distance, mx, my, mz, g);
+    tsj = View(zz->turb_src_jac, mx, my, mz, 0);
     dt_local = View(zz->dt_local, mx, my, mz, 0);
     bv_last = View(zz->bv_last, mx, my, mz, 0);
     metric = MetricView(zz->metric, mx, my, mz, g);
@@ -1085,6 +1086,10 @@ void source_and_mut(const ostc_param *P, Z &Zn, int i, int j, int k) {
     const double diss_omega = beta * density * omega * omega;
     Zn.dq(i, j, k, 6) += jac * (prod_omega - diss_omega);
   }
+  if (P->turb_implicit == 1 && Zn.tsj.p) {  // SST.cu:243-246
+    Zn.tsj(i, j, k, 0) = -2 * betaStar * omega;
+    Zn.tsj(i, j, k, 1) = -2 * beta * omega;
+  }
   constexpr double cp = gamma_air * R_u / mw_air / (gamma_air - 1);
   Zn.ttc(i, j, k) = Zn.mut(i, j, k) * cp / P->Prt;
 }
@@ -1877,7 +1882,8 @@ void local_time_step_zone(const ostc_param *P, Z &Zn, std::vector<double> &isr) 
         double gamma = gamma_air;
         if (P->mix_model != OSTC_MIX_AIR) gamma = Zn.gam(i, j, k);
         const double c1 = std::max(gamma, 4.0 / 3.0) / Zn.bv(i, j, k, 0);
-        const double c2 = Zn.mul(i, j, k) / P->Pr;
+        double c2 = Zn.mul(i, j, k) / P->Pr;
+        if (is_sst(P)) c2 += Zn.mut(i, j, k) / P->Prt;
         double srv = gx * gx + ge * ge;
         if (dim == 3) srv += gz * gz;
         srv *= c1 * c2;
@@ -2048,6 +2054,10 @@ void dplur_zone(const ostc_config *c, const ostc_param *P, Z &Zn, const std::vec
             for (int l = 5; l < nv; ++l) Zn.dq(i, j, k, l) /= diag;
           }
         }
+        if (is_sst(P)) {  // DPLUR.cuh:72-84, SST.cu:249-258
+          for (int t = 0; t < 2; ++t)
+            Zn.dq(i, j, k, 5 + t) /= P->turb_implicit == 1 ? diag - dt * Zn.tsj(i, j, k, t) : diag;
+        }
         for (int l = 0; l < nv; ++l) dq0(i, j, k, l) = Zn.dq(i, j, k, l);
       }
   for (int it = 0; it < c->DPLUR_inner_step; ++it) {
@@ -2110,6 +2120,11 @@ void dplur_zone(const ostc_config *c, const ostc_param *P, Z &Zn, const std::vec
             } else {
               for (int l = 5; l < nv; ++l) dqk(i, j, k, l) = dq0(i, j, k, l) + dt * tot[l] / diag;
             }
+          }
+          if (is_sst(P)) {  // DPLUR.cuh:262-276, SST.cu:260-273
+            for (int t = 0; t < 2; ++t)
+              dqk(i, j, k, 5 + t) = dq0(i, j, k, 5 + t) +
+                                    dt * tot[5 + t] / (P->turb_implicit == 1 ? diag - dt * Zn.tsj(i, j, k, t) : diag);
           }
         }
     // dq <- dqk over the interior (the ghost layer of dq is never read)
@@ -2464,8 +2479,17 @@ int oracle_steady_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zo
       local_time_step_zone(P, Zn, isr);
       if (c->implicit_method == 1) {
         dplur_zone(c, P, Zn, isr, f, n_faces, b);
-      } else if (P->mix_model == OSTC_MIX_FR && P->n_reac > 0 && P->chemSrcMethod != 0) {
-        chem_implicit_zone(P, Zn);
+      } else {
+        if (P->mix_model == OSTC_MIX_FR && P->n_reac > 0 && P->chemSrcMethod != 0) chem_implicit_zone(P, Zn);
+        if (is_sst(P) && P->turb_implicit == 1) {  // implicit_treat_for_SST (SST.cu:8-22)
+          for (int k = 0; k < Zn.mz; ++k)
+            for (int j = 0; j < Zn.my; ++j)
+              for (int i = 0; i < Zn.mx; ++i) {
+                const double dt = Zn.dt_local(i, j, k);
+                Zn.dq(i, j, k, 5) /= 1 - dt * Zn.tsj(i, j, k, 0);
+                Zn.dq(i, j, k, 6) /= 1 - dt * Zn.tsj(i, j, k, 1);
+              }
+        }
       }
       update_bv_zone(P, Zn);
     }

@@ -104,7 +104,7 @@ void build_param(RefCtx &c, const ostc_param *p) {
   d.entropy_fix_factor = p->entropy_fix_factor;
   d.viscous_scheme = p->viscous_scheme;
   d.rans_model = p->turbulence ? p->rans_model : 0;
-  d.turb_implicit = 0;
+  d.turb_implicit = p->turbulence ? p->turb_implicit : 0;
   d.compressibility_correction = p->turbulence ? p->compressibility_correction : 0;
   d.chemSrcMethod = p->chemSrcMethod;
   d.n_reac = p->mix_model == OSTC_MIX_FR ? p->n_reac : 0;
@@ -183,6 +183,7 @@ void build_zone(RefCtx &c, const ostc_zone *z, const ostc_param *p) {
     cudaMemset(h.mut.data(), 0, sizeof(double) * P);
     h.turb_therm_cond.allocate_memory(mx, my, mz, g);
     cudaMemset(h.turb_therm_cond.data(), 0, sizeof(double) * P);
+    if (p->turb_implicit == 1) h.turb_src_jac.allocate_memory(mx, my, mz, 2, 0);
   }
   if (p->n_spec > 0) {
     h.gamma.allocate_memory(mx, my, mz, g);
@@ -400,7 +401,7 @@ int steps(RefMulti &m, int n, double *res_hist, double *dt_hist) {
 // implicit_treatment (ImplicitTreatmentHPP.cuh:8-52) for one block; DPLUR's
 // host loop (DPLUR.cuh:283-312) with set_wall_dq_to_0 (DPLUR.cu:33-52) over
 // this block's wall faces
-template <MixtureModel mix>
+template <MixtureModel mix, class Turb>
 void implicit_treatment_block(RefMulti &m, RefCtx &c) {
   dim3 tpb{8, 8, 4};
   dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
@@ -409,9 +410,11 @@ void implicit_treatment_block(RefMulti &m, RefCtx &c) {
       if (c.h_param.n_reac > 0 && c.h_param.chemSrcMethod == 1) EPI<<<bpg, tpb>>>(c.d_zone, c.n_spec);
       if (c.h_param.n_reac > 0 && c.h_param.chemSrcMethod == 2) DA<<<bpg, tpb>>>(c.d_zone, c.n_spec);
     }
+    if constexpr (TurbMethod<Turb>::hasImplicitTreat)
+      if (c.h_param.turb_implicit == 1) implicit_treat_for_SST<<<bpg, tpb>>>(c.d_zone, c.d_param);
     return;
   }
-  compute_DQ_0<mix, Laminar><<<bpg, tpb>>>(c.d_zone, c.d_param);
+  compute_DQ_0<mix, Turb><<<bpg, tpb>>>(c.d_zone, c.d_param);
   const size_t mem = c.h.dq.size() * c.n_var * sizeof(real);
   cudaMemcpy(c.h.dq0.data(), c.h.dq.data(), mem, cudaMemcpyDeviceToDevice);
   for (int it = 0; it < m.cfg.DPLUR_inner_step; ++it) {
@@ -426,13 +429,13 @@ void implicit_treatment_block(RefMulti &m, RefCtx &c) {
       }
       set_dq_to_0<<<dim3{bp[0], bp[1], bp[2]}, dim3{tp[0], tp[1], tp[2]}>>>(c.d_param, c.d_zone, (integer)q);
     }
-    DPLUR_inner_iteration<mix, Laminar><<<bpg, tpb>>>(c.d_param, c.d_zone);
+    DPLUR_inner_iteration<mix, Turb><<<bpg, tpb>>>(c.d_param, c.d_zone);
     cudaMemcpy(c.h.dq.data(), c.h.dqk.data(), mem, cudaMemcpyDeviceToDevice);
   }
   convert_dq_back_to_dqDt<<<bpg, tpb>>>(c.d_zone, c.d_param);
 }
 
-template <MixtureModel mix>
+template <MixtureModel mix, class Turb>
 int steady_steps(RefMulti &m, int n, double *res_hist) {
   // the loop body of steady_simulation (SteadySim.cuh:51-126), all blocks
   dim3 tpb{8, 8, 4};
@@ -446,13 +449,13 @@ int steady_steps(RefMulti &m, int n, double *res_hist) {
     if (res_hist)
       for (RefCtx *c : m.blk) store_last_step<<<bpg(c, -1), tpb>>>(c->d_zone);
     for (RefCtx *c : m.blk) {
-      rhs<mix, Laminar>(*c);
-      local_time_step<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
-      implicit_treatment_block<mix>(m, *c);
-      update_bv<mix, Laminar><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
-      apply_bcs<mix, Laminar, false>(*c);
+      rhs<mix, Turb>(*c);
+      local_time_step<mix, Turb><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
+      implicit_treatment_block<mix, Turb>(m, *c);
+      update_bv<mix, Turb><<<bpg(c, -1), tpb>>>(c->d_zone, c->d_param);
+      apply_bcs<mix, Turb, false>(*c);
     }
-    communicate<mix, Laminar, false>(m);
+    communicate<mix, Turb, false>(m);
     for (RefCtx *c : m.blk) update_physical_properties<mix><<<bpg(c, 1), tpb>>>(c->d_zone, c->d_param);
     if (res_hist) {
       double acc[4] = {0, 0, 0, 0};
@@ -613,7 +616,7 @@ int ref_create_multi(const ostc_config *cfg, const ostc_param *p, const ostc_zon
                      int nf, const ostc_interface *ifc, int nif, void **out) {
   if (!cfg || !p || !z || !out || nz < 1) return 1;
   if (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_FR) return 5;
-  if (p->turbulence && (p->rans_model != 2 || p->mix_model != OSTC_MIX_AIR || cfg->steady)) return 5;
+  if (p->turbulence && (p->rans_model != 2 || p->mix_model != OSTC_MIX_AIR)) return 5;
   for (int q = 0; q < nf; ++q)
     if (f[q].block < 0 || f[q].block >= nz) return 1;
   for (int q = 0; q < nif; ++q)
@@ -684,8 +687,9 @@ int ref_steps(void *h, int n, double *res_hist, double *dt_hist) {
 int ref_steady_steps(void *h, int n, double *res_hist) {
   auto *m = (RefMulti *)h;
   if (!m->cfg.steady) return 1;
-  return m->mix == OSTC_MIX_AIR ? steady_steps<MixtureModel::Air>(*m, n, res_hist)
-                                : steady_steps<MixtureModel::FR>(*m, n, res_hist);
+  if (m->sst) return steady_steps<MixtureModel::Air, SST>(*m, n, res_hist);
+  return m->mix == OSTC_MIX_AIR ? steady_steps<MixtureModel::Air, Laminar>(*m, n, res_hist)
+                                : steady_steps<MixtureModel::FR, Laminar>(*m, n, res_hist);
 }
 
 // device time of n steps (CUDA events around the loop, as bench.py does for ours)

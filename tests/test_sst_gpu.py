@@ -145,3 +145,47 @@ def test_sst_matches_reference_build():
         assert max(_state_errors(blocks2[b].download("bv"), r2.download("bv", b))) <= 1e-9, b
         assert max(_state_errors(blocks2[b].download("sv"), r2.download("sv", b))) <= 1e-9, b
     s2.close()
+
+
+@pytest.mark.parametrize("implicit_method,turb_implicit", [(0, 1), (0, 0), (1, 1), (1, 0)])
+def test_sst_steady_matches_oracle_and_reference(implicit_method, turb_implicit):
+    """The steady path with SST (SteadySim.cuh:51-126): local time stepping,
+    explicit with implicit_treat_for_SST or DPLUR with the SST point-implicit
+    sources (turb_implicit 1) or plain division (0), on the walled 37-block
+    layout: 4 iterations against the oracle (states, mut and residuals to
+    1e-9) and against the reference's own kernels (states and mut; its
+    residual sums are undefined for some of these block sizes, quirk A19)."""
+    import ref_bind
+
+    base = _case("hllc_muscl")
+    for f in base.faces:  # the reference's air + SST far field reads unset scalars (A20)
+        if f.type_label == ostc.BC_FARFIELD:
+            f.type_label = ostc.BC_OUTFLOW
+    base.scheme.turb_implicit = turb_implicit
+    case = ostc.make_steady(base, implicit_method=implicit_method, dplur_inner_step=2)
+    n = 4
+    o = OracleRun(case)
+    o.initialize()
+    res_o = o.steady_steps(n)
+    s, blocks = case.solver()
+    s.initialize()
+    res_g = s.steady_steps(n, history=True)
+    assert np.max(np.abs(res_g - res_o) / res_o) <= 1e-9
+    for b in range(len(blocks)):
+        assert max(_state_errors(blocks[b].download("bv"), o.blocks[b].arrays["bv"])) <= 1e-9, b
+        assert max(_state_errors(blocks[b].download("sv"), o.blocks[b].arrays["sv"])) <= 1e-9, b
+        ref = o.blocks[b].arrays["mut"]
+        assert np.max(np.abs(blocks[b].download("mut") - ref)) <= 1e-9 * np.max(np.abs(ref)), b
+    s.close()
+    if not ref_bind.available():
+        return
+    r = ref_bind.RefCudaRun(case)
+    r.initialize()
+    r.steady_steps(n)
+    s2, blocks2 = case.solver()
+    s2.initialize()
+    s2.steady_steps(n)
+    for b in range(len(blocks2)):
+        assert max(_state_errors(blocks2[b].download("bv"), r.download("bv", b))) <= 1e-9, b
+        assert max(_state_errors(blocks2[b].download("sv"), r.download("sv", b))) <= 1e-9, b
+    s2.close()
