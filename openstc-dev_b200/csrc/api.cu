@@ -263,7 +263,10 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
     if (p->rans_model != 2) return OSTC_ERR_UNSUPPORTED;
     if (p->mix_model != OSTC_MIX_AIR || cfg->chem_mode != 0) return OSTC_ERR_UNSUPPORTED;
     if (p->turb_implicit != 0 && p->turb_implicit != 1) return OSTC_ERR_INVALID_ARG;
-    if (p->inviscid_type != 0 || (p->inviscid_scheme != 3 && p->inviscid_scheme != 4)) return OSTC_ERR_UNSUPPORTED;
+    // primitive-variable reconstruction with AUSM+ / HLLC, or AWENO (its Roe tag runs AUSM+, A1) with AUSM+ / HLLC
+    const bool pv = p->inviscid_type == 0 && (p->inviscid_scheme == 3 || p->inviscid_scheme == 4);
+    const bool aweno = p->inviscid_type == 1 && p->inviscid_scheme >= 2 && p->inviscid_scheme <= 4;
+    if (!pv && !aweno) return OSTC_ERR_UNSUPPORTED;
     if (p->viscous_scheme == 0) return OSTC_ERR_UNSUPPORTED;
     if (p->n_spec != 0 || p->n_scalar != 2 || p->n_var != 7 || p->i_turb_cv != 5) return OSTC_ERR_INVALID_ARG;
     if (p->compressibility_correction < 0 || p->compressibility_correction > 3) return OSTC_ERR_INVALID_ARG;

@@ -442,9 +442,14 @@ __device__ __forceinline__ void weno5_pair(const double v[6], double &vminus, do
   vplus = (a0 * v0 + a1 * v1 + a2 * v2) / (a0 + a1 + a2);
 }
 
-template <int DIR>
+// NT = 2 (SST): k and omega are not part of the reference's AWENO (quirk A3:
+// its WENO5 reads a 5-variable row stride); here their conservative values
+// rho k, rho omega are reconstructed component by component with the same
+// WENO5 weights and divided by the characteristically reconstructed density.
+template <int DIR, int NT = 0>
 __device__ __forceinline__ void inviscid_face_aweno(const DevZone &z, int g0, double *F) {
   constexpr double gm1 = gamma_air - 1;
+  constexpr int NV = 5 + NT;
   const int sd = dir_stride<DIR>(z);
   double U[6][5];
 #pragma unroll
@@ -542,26 +547,37 @@ __device__ __forceinline__ void inviscid_face_aweno(const DevZone &z, int g0, do
       }
     }
   }
-  double pl[7], pr[7];
+  double pl[NV + 2], pr[NV + 2];
   pl[0] = ql[0];
   pl[1] = ql[1] / ql[0];
   pl[2] = ql[2] / ql[0];
   pl[3] = ql[3] / ql[0];
   pl[4] = gm1 * (ql[4] - 0.5 * (pl[1] * pl[1] + pl[2] * pl[2] + pl[3] * pl[3]) * ql[0]);
-  pl[5] = ql[4];
-  pl[6] = gamma_air;
+  pl[NV] = ql[4];
+  pl[NV + 1] = gamma_air;
   pr[0] = qr[0];
   pr[1] = qr[1] / qr[0];
   pr[2] = qr[2] / qr[0];
   pr[3] = qr[3] / qr[0];
   pr[4] = gm1 * (qr[4] - 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]) * qr[0]);
-  pr[5] = qr[4];
-  pr[6] = gamma_air;
-  riemann<5, 0>(pl, pr, z, g0, g1, DIR, F);
+  pr[NV] = qr[4];
+  pr[NV + 1] = gamma_air;
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {  // componentwise WENO5 of rho k, rho omega
+    double v[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) v[s] = cvl(z, g0 + (s - 2) * sd, 5 + t);
+    double vmn = 0, vpl = 0;
+    if (c_p.reconstruction == 4) weno5_pair(v, vmn, vpl);
+    pl[5 + t] = vmn / ql[0];
+    pr[5 + t] = vpl / qr[0];
+  }
+  riemann<NV, 0>(pl, pr, z, g0, g1, DIR, F);
 }
 
-// physical flux of the AWENO central correction at one point (AWENO.cu:236-249)
-template <int DIR>
+// physical flux of the AWENO central correction at one point (AWENO.cu:236-249);
+// NT turbulence scalars: jac * rho U s
+template <int DIR, int NT = 0>
 __device__ __forceinline__ void cds_point_flux(const DevZone &z, int g, double *f) {
   const double kx = met(z, g, 3 * DIR), ky = met(z, g, 3 * DIR + 1), kz = met(z, g, 3 * DIR + 2);
   const double jac = ld(z.jac + g);
@@ -574,26 +590,29 @@ __device__ __forceinline__ void cds_point_flux(const DevZone &z, int g, double *
   f[2] = jac * (rUk * v + ky * p);
   f[3] = jac * (rUk * w + kz * p);
   f[4] = jac * Uk * (cvl(z, g, 4) + p);
+#pragma unroll
+  for (int t = 0; t < NT; ++t) f[5 + t] = jac * (rUk * svl(z, g, t));
 }
 
 // sum_m c_m (f(c+m) - f(c-m)), m = 3, 2, 1 (AWENO.cu:257-263)
-template <int DIR>
+template <int DIR, int NT = 0>
 __device__ __forceinline__ void cds_correction(const DevZone &z, int g, double *corr) {
+  constexpr int NC = 5 + NT;
   const int sd = dir_stride<DIR>(z);
   constexpr double c1 = 19.0 / 3840, c2 = -13.0 / 320, c3 = 17.0 / 256;
-  double fp[5], fm[5], d3[5], d2[5];
-  cds_point_flux<DIR>(z, g + 3 * sd, fp);
-  cds_point_flux<DIR>(z, g - 3 * sd, fm);
+  double fp[NC], fm[NC], d3[NC], d2[NC];
+  cds_point_flux<DIR, NT>(z, g + 3 * sd, fp);
+  cds_point_flux<DIR, NT>(z, g - 3 * sd, fm);
 #pragma unroll
-  for (int l = 0; l < 5; ++l) d3[l] = fp[l] - fm[l];
-  cds_point_flux<DIR>(z, g + 2 * sd, fp);
-  cds_point_flux<DIR>(z, g - 2 * sd, fm);
+  for (int l = 0; l < NC; ++l) d3[l] = fp[l] - fm[l];
+  cds_point_flux<DIR, NT>(z, g + 2 * sd, fp);
+  cds_point_flux<DIR, NT>(z, g - 2 * sd, fm);
 #pragma unroll
-  for (int l = 0; l < 5; ++l) d2[l] = fp[l] - fm[l];
-  cds_point_flux<DIR>(z, g + sd, fp);
-  cds_point_flux<DIR>(z, g - sd, fm);
+  for (int l = 0; l < NC; ++l) d2[l] = fp[l] - fm[l];
+  cds_point_flux<DIR, NT>(z, g + sd, fp);
+  cds_point_flux<DIR, NT>(z, g - sd, fm);
 #pragma unroll
-  for (int l = 0; l < 5; ++l) corr[l] = c1 * d3[l] + c2 * d2[l] + c3 * (fp[l] - fm[l]);
+  for (int l = 0; l < NC; ++l) corr[l] = c1 * d3[l] + c2 * d2[l] + c3 * (fp[l] - fm[l]);
 }
 
 // ---------------------------------------------------------------------------

@@ -20,18 +20,18 @@ namespace ostc {
 // PART 0: inviscid and (when `viscous`) viscous flux of the face;
 // PART 1: the inviscid flux alone; PART 2: the viscous flux alone
 // NT: turbulence scalars after the species (2 for SST; primitive-variable
-// reconstruction only)
+// or AWENO reconstruction)
 template <int NS, int INV, int DIR, int PART, int NT>
 __device__ __forceinline__ void face_total(const DevZone &z, int g0, bool viscous, double *G) {
   constexpr int NV = 5 + NS + NT;
-  static_assert(NT == 0 || INV == 0, "turbulence scalars take the primitive-variable reconstruction");
+  static_assert(NT == 0 || INV != 2, "turbulence scalars: primitive-variable or AWENO reconstruction");
   if constexpr (PART == 2) {
     viscous_face<NS, DIR, NT>(z, g0, G);
     return;
   }
   double Fi[NV];
   if constexpr (INV == 1)
-    inviscid_face_aweno<DIR>(z, g0, Fi);
+    inviscid_face_aweno<DIR, NT>(z, g0, Fi);
   else if constexpr (INV == 2)
     inviscid_face_roe<NS, DIR>(z, g0, Fi);
   else
@@ -101,15 +101,15 @@ __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const 
         for (int l = 0; l < NV; ++l) carry[row][l] = G[l];
       __syncwarp();
       if (active && f >= c0 && f >= 0) {
-        double corr[5] = {0, 0, 0, 0, 0};
+        double corr[5 + NT] = {};
         if constexpr (CDS) {
-          if (f < cds_limit) cds_correction<DIR>(z, gidx(z, f, j, k), corr);
+          if (f < cds_limit) cds_correction<DIR, NT>(z, gidx(z, f, j, k), corr);
         }
         double *dq = z.dq + qidx(z, f, j, k);
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           double d = G[l] - Gm[l];
-          if (CDS && l < 5) d -= corr[l];
+          if (CDS && l < 5 + NT) d -= corr[l];
           if (accumulate)
             dq[l * z.qsz] += d;
           else
@@ -139,15 +139,15 @@ __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const 
       for (int l = 0; l < NV; ++l) sG[((row + 1) * NV + l) * 32 + lane] = G[l];
       __syncthreads();
       if (active && f >= c0 && f >= 0 && !(ch == 0 && row == 0)) {
-        double corr[5] = {0, 0, 0, 0, 0};
+        double corr[5 + NT] = {};
         if constexpr (CDS) {
-          if (f < cds_limit) cds_correction<DIR>(z, gidx(z, ci, cj, ck), corr);
+          if (f < cds_limit) cds_correction<DIR, NT>(z, gidx(z, ci, cj, ck), corr);
         }
         double *dq = z.dq + qidx(z, ci, cj, ck);
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           double d = G[l] - sG[(row * NV + l) * 32 + lane];
-          if (CDS && l < 5) d -= corr[l];
+          if (CDS && l < 5 + NT) d -= corr[l];
           if (accumulate)
             dq[l * z.qsz] += d;
           else
@@ -254,7 +254,14 @@ template <int NS, int NT>
 cudaError_t launch_flux_nt(const DevZone &z, int inv, int dir, const TileShape &t, const FluxTable *tab, int accumulate,
                            int viscous, int part, cudaStream_t s) {
   if constexpr (NT > 0) {
-    if (inv != 0) return cudaErrorInvalidValue;  // turbulence scalars: primitive-variable reconstruction only
+    if (inv == 1) {  // AWENO with the scalars reconstructed component-wise
+      switch (dir) {
+        case 0: return launch_flux_t<NS, 1, 0, NT>(z, t, tab, accumulate, viscous, part, s);
+        case 1: return launch_flux_t<NS, 1, 1, NT>(z, t, tab, accumulate, viscous, part, s);
+        default: return launch_flux_t<NS, 1, 2, NT>(z, t, tab, accumulate, viscous, part, s);
+      }
+    }
+    if (inv != 0) return cudaErrorInvalidValue;  // no Roe with turbulence scalars
     switch (dir) {
       case 0: return launch_flux_t<NS, 0, 0, NT>(z, t, tab, accumulate, viscous, part, s);
       case 1: return launch_flux_t<NS, 0, 1, NT>(z, t, tab, accumulate, viscous, part, s);

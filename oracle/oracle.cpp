@@ -711,12 +711,20 @@ void riemann(const ostc_param *P, const double *pl, const double *pr, const doub
 // AWENO-5 for air: src/AWENO.cu:17-206. cvl rows hold n_var conservative
 // values followed by p and T (row stride nv + 2).
 // ---------------------------------------------------------------------------
+void weno5_values(const double *v, double *vm, double *vp);
+
 void weno5(const double *L, const double *cv, int stride, int is, int row, double *vm, double *vp) {
   double v[6] = {0};
   for (int i = -2; i < 4; ++i) {
     const double *U = &cv[(is + i) * stride];
     for (int j = 0; j < 5; ++j) v[i + 2] += L[row * 5 + j] * U[j];
   }
+  weno5_values(v, vm, vp);
+}
+
+// the WENO5 pair (left state of face is+1/2 from points is-2..is+2, right
+// state from is-1..is+3) of six point values v[0..5] = points is-2..is+3
+void weno5_values(const double *v, double *vm, double *vp) {
   double v0 = 0.125 * (3 * v[0] - 10 * v[1] + 15 * v[2]);
   double v1 = 0.125 * (-v[1] + 6 * v[2] + 3 * v[3]);
   double v2 = 0.125 * (3 * v[2] + 6 * v[3] - v[4]);
@@ -801,8 +809,9 @@ void aweno_interpolation(const ostc_param *P, const double *cv, double *pl, doub
   L[24] = gm1 / cm2 * 0.5;
   double vplus[5] = {0}, vminus[5] = {0};
   if (P->reconstruction == 4) {
-    // the reference passes n_var = 5 to WENO5, so the row stride is 7 (quirk A3)
-    for (int l = 0; l < 5; ++l) weno5(L, cv, 7, is, l, &vminus[l], &vplus[l]);
+    // the reference passes n_var = 5 to WENO5 and so reads rows of stride 7
+    // (quirk A3), which is the true stride n_var + 2 without turbulence scalars
+    for (int l = 0; l < 5; ++l) weno5(L, cv, st, is, l, &vminus[l], &vplus[l]);
   }
   double R[25];
   R[0] = 1.0; R[1] = kx; R[2] = ky; R[3] = kz; R[4] = 1.0;
@@ -835,6 +844,15 @@ void aweno_interpolation(const ostc_param *P, const double *cv, double *pl, doub
   pr[3] = qr[3] / qr[0];
   pr[4] = gm1 * (qr[4] - 0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]) * qr[0]);
   pr[nv] = qr[4];
+  // SST scalars (not in the reference's AWENO, quirk A3): component-wise WENO5
+  // of rho k, rho omega, divided by the reconstructed densities
+  for (int l = 5; l < nv; ++l) {
+    double v[6], sm = 0, sp = 0;
+    for (int i = -2; i < 4; ++i) v[i + 2] = cv[(is + i) * st + l];
+    if (P->reconstruction == 4) weno5_values(v, &sm, &sp);
+    pl[l] = sm / ql[0];
+    pr[l] = sp / qr[0];
+  }
 }
 
 // optional per-variable max |face flux| (conditioning scale of dq), see oracle_flux_scale
@@ -872,7 +890,7 @@ void inviscid_direction(const ostc_param *P, Z &Zn, int d) {
   const int npt = n + 2 * ngg;  // line points -ngg .. n+ngg-1 at index s+ngg
 #pragma omp parallel
   {
-    std::vector<double> rows(npt * nrow), met(npt * 3), jac(npt), fc((n + 1) * nv), f(npt * 5), delta(npt);
+    std::vector<double> rows(npt * nrow), met(npt * 3), jac(npt), fc((n + 1) * nv), f(npt * nv), delta(npt);
     double pl[MAXS + 11], pr[MAXS + 11];
 #pragma omp for collapse(2) schedule(static)
     for (int b = 0; b < nb; ++b) {
@@ -933,12 +951,13 @@ void inviscid_direction(const ostc_param *P, Z &Zn, int d) {
             const double Uk = kx * u + ky * v + kz * w;
             const double rUk = Zn.bv(i, j, k, 0) * Uk;
             const double p = Zn.bv(i, j, k, 4);
-            double *fi = &f[(s + ngg) * 5];
+            double *fi = &f[(s + ngg) * nv];
             fi[0] = rUk * jc;
             fi[1] = jc * (rUk * u + kx * p);
             fi[2] = jc * (rUk * v + ky * p);
             fi[3] = jc * (rUk * w + kz * p);
             fi[4] = jc * Uk * (Zn.cv(i, j, k, 4) + p);
+            for (int l = 5; l < nv; ++l) fi[l] = jc * (rUk * Zn.sv(i, j, k, l - 5));  // SST scalars
           }
           // central correction only on [0, n - 2 ngg) (quirk A4)
           constexpr double c1 = 19.0 / 3840, c2 = -13.0 / 320, c3 = 17.0 / 256;
@@ -947,9 +966,9 @@ void inviscid_direction(const ostc_param *P, Z &Zn, int d) {
             line_ijk(d, s, a, b, i, j, k);
             const int is = s + ngg;
             for (int l = 0; l < nv; ++l) {
-              Zn.dq(i, j, k, l) -= c1 * (f[(is + 3) * 5 + l] - f[(is - 3) * 5 + l]) +
-                                   c2 * (f[(is + 2) * 5 + l] - f[(is - 2) * 5 + l]) +
-                                   c3 * (f[(is + 1) * 5 + l] - f[(is - 1) * 5 + l]);
+              Zn.dq(i, j, k, l) -= c1 * (f[(is + 3) * nv + l] - f[(is - 3) * nv + l]) +
+                                   c2 * (f[(is + 2) * nv + l] - f[(is - 2) * nv + l]) +
+                                   c3 * (f[(is + 1) * nv + l] - f[(is - 1) * nv + l]);
             }
           }
         }
