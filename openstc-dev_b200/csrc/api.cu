@@ -231,6 +231,8 @@ void fill_devzone(const ostc_zone &z, DevZone &d) {
   strides(z.dq_ngg, d.q2, d.q1, d.qt, d.qsz);
   int dummy;
   strides(0, d.n2, d.n1, dummy, d.nsz);
+  d.isz = (int)d.sz;
+  d.iqsz = (int)d.qsz;
   d.bv = z.bv;
   d.sv = z.sv;
   d.cv = z.cv;

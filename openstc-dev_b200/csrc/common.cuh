@@ -67,6 +67,9 @@ struct DevZone {
   const double *jac;
   const double *met;  // 9 SoA planes (context-owned copy), ghosted layout
   int block_id;
+  // sz and qsz as 32-bit ints for the flux kernels' index arithmetic (every
+  // plane offset of a block is below 2^31: checked at ostc_create)
+  int isz, iqsz;
   int pad_;
 };
 

@@ -17,14 +17,19 @@ __device__ __forceinline__ int dir_stride(const DevZone &z) {
   return DIR == 0 ? 1 : (DIR == 1 ? z.d2 : z.d1);
 }
 
-__device__ __forceinline__ double bvl(const DevZone &z, int g, int l) { return ld(z.bv + l * z.sz + g); }
-__device__ __forceinline__ double svl(const DevZone &z, int g, int l) { return ld(z.sv + l * z.sz + g); }
-__device__ __forceinline__ double cvl(const DevZone &z, int g, int l) { return ld(z.cv + l * z.sz + g); }
-__device__ __forceinline__ double met(const DevZone &z, int g, int c) { return ld(z.met + c * z.sz + g); }
+__device__ __forceinline__ double bvl(const DevZone &z, int g, int l) { return ld(z.bv + l * z.isz + g); }
+__device__ __forceinline__ double svl(const DevZone &z, int g, int l) { return ld(z.sv + l * z.isz + g); }
+__device__ __forceinline__ double cvl(const DevZone &z, int g, int l) { return ld(z.cv + l * z.isz + g); }
+__device__ __forceinline__ double met(const DevZone &z, int g, int c) { return ld(z.met + c * z.isz + g); }
 
-__device__ __forceinline__ int sgn(double a) { return a < 0 ? -1 : 1; }
-__device__ __forceinline__ double minmod(double a, double b) {  // Limiter.cuh:13-16
-  return 0.5 * (sgn(a) + sgn(b)) * fmin(fabs(a), fabs(b));
+// 0.5 * (sgn(a) + sgn(b)) * min(|a|, |b|) with sgn(x) = (x < 0 ? -1 : 1)
+// (Limiter.cuh:13-16), written without the integer sum and its conversion:
+// the product is exactly +m, -m or +0, so the result is bit-identical;
+// symmetric in a and b
+__device__ __forceinline__ double minmod(double a, double b) {
+  const double m = fmin(fabs(a), fabs(b));
+  const bool na = a < 0, nb = b < 0;
+  return na != nb ? 0.0 : (na ? -m : m);
 }
 
 // ---------------------------------------------------------------------------
@@ -198,15 +203,16 @@ __device__ __forceinline__ void reconstruct_pv(const DevZone &z, int g0, double 
   const int rec = c_p.reconstruction;
 #pragma unroll
   for (int l = 0; l < NV; ++l) {
-    const double *base = l < 5 ? z.bv + l * z.sz : z.sv + (l - 5) * z.sz;
+    const double *base = l < 5 ? z.bv + l * z.isz : z.sv + (l - 5) * z.isz;
     const double v0 = ld(base + g0), v1 = ld(base + g0 + sd);
     if (rec == 2 || rec == 3) {
       const double vm = ld(base + g0 - sd), v2 = ld(base + g0 + 2 * sd);
       const double di = v0 - vm, di1 = v1 - v0, di2 = v2 - v1;
       if (rec == 2) {
         constexpr double kappa = 1.0 / 3.0;
-        pl[l] = v0 + 0.25 * ((1 - kappa) * minmod(di, di1) + (1 + kappa) * minmod(di1, di));
-        pr[l] = v1 - 0.25 * ((1 - kappa) * minmod(di2, di1) + (1 + kappa) * minmod(di1, di2));
+        const double ml = minmod(di, di1), mr = minmod(di2, di1);  // = minmod(di1, di), minmod(di1, di2)
+        pl[l] = v0 + 0.25 * ((1 - kappa) * ml + (1 + kappa) * ml);
+        pr[l] = v1 - 0.25 * ((1 - kappa) * mr + (1 + kappa) * mr);
       } else {
         pl[l] = v0 + 0.5 * minmod(di, di1);
         pr[l] = v1 - 0.5 * minmod(di1, di2);
@@ -642,10 +648,10 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
     out[TB] = db;
   };
   double du[3], dv[3], dw[3], dt[3];
-  der(z.bv + 1 * z.sz, du);
-  der(z.bv + 2 * z.sz, dv);
-  der(z.bv + 3 * z.sz, dw);
-  der(z.bv + 5 * z.sz, dt);
+  der(z.bv + 1 * z.isz, du);
+  der(z.bv + 2 * z.isz, dv);
+  der(z.bv + 3 * z.isz, dw);
+  der(z.bv + 5 * z.isz, dt);
   const double u_x = du[0] * mm[0] + du[1] * mm[3] + du[2] * mm[6];
   const double u_y = du[0] * mm[1] + du[1] * mm[4] + du[2] * mm[7];
   const double u_z = du[0] * mm[2] + du[1] * mm[5] + du[2] * mm[8];
@@ -693,9 +699,9 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
     double sgw = 0, srdy = 0, corr = 0, mwt = 0;
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
-      const double *ys = z.sv + l * z.sz;
+      const double *ys = z.sv + l * z.isz;
       yk[l] = 0.5 * (ld(ys + g0) + ld(ys + g1));
-      diff[l] = 0.5 * (ld(z.rhoD + l * z.sz + g0) + ld(z.rhoD + l * z.sz + g1));
+      diff[l] = 0.5 * (ld(z.rhoD + l * z.isz + g0) + ld(z.rhoD + l * z.isz + g1));
       double dy[3];
       der(ys, dy);
       const double y_x = dy[0] * mm[0] + dy[1] * mm[3] + dy[2] * mm[6];
@@ -712,7 +718,7 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
     corr -= mwt * srdy * sgw;
     if (c_p.gradP) {
       double dp[3];
-      der(z.bv + 4 * z.sz, dp);
+      der(z.bv + 4 * z.isz, dp);
       const double p_x = dp[0] * mm[0] + dp[1] * mm[3] + dp[2] * mm[6];
       const double p_y = dp[0] * mm[1] + dp[1] * mm[4] + dp[2] * mm[7];
       const double p_z = dp[0] * mm[2] + dp[1] * mm[5] + dp[2] * mm[8];
@@ -734,8 +740,8 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
   }
   if constexpr (NT > 0) {  // k and omega diffusion (ViscousScheme.cuh:200-251)
     double dk[3], dw[3];
-    der(z.sv + NS * z.sz, dk);
-    der(z.sv + (NS + 1) * z.sz, dw);
+    der(z.sv + NS * z.isz, dk);
+    der(z.sv + (NS + 1) * z.isz, dw);
     const double k_x = dk[0] * mm[0] + dk[1] * mm[3] + dk[2] * mm[6];
     const double k_y = dk[0] * mm[1] + dk[1] * mm[4] + dk[2] * mm[7];
     const double k_z = dk[0] * mm[2] + dk[1] * mm[5] + dk[2] * mm[8];

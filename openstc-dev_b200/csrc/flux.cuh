@@ -111,9 +111,9 @@ __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const 
           double d = G[l] - Gm[l];
           if (CDS && l < 5 + NT) d -= corr[l];
           if (accumulate)
-            dq[l * z.qsz] += d;
+            dq[l * z.iqsz] += d;
           else
-            dq[l * z.qsz] = d;
+            dq[l * z.iqsz] = d;
         }
       }
     }
@@ -149,9 +149,9 @@ __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const 
           double d = G[l] - sG[(row * NV + l) * 32 + lane];
           if (CDS && l < 5 + NT) d -= corr[l];
           if (accumulate)
-            dq[l * z.qsz] += d;
+            dq[l * z.iqsz] += d;
           else
-            dq[l * z.qsz] = d;
+            dq[l * z.iqsz] = d;
         }
       }
       __syncthreads();

@@ -12,6 +12,16 @@
 
 namespace ostc {
 
+// the NASA-7 coefficients c[0..n) of species i at temperature t: the low
+// range below t_mid (and below t_low, where the caller extends linearly), the
+// high range above. Selected by value from both rows, so that every
+// coefficient address is a compile-time constant of the unrolled species loop.
+template <int N>
+__device__ __forceinline__ void nasa_coeffs(int i, bool low, double *c) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) c[k] = low ? c_p.lo[i][k] : c_p.hi[i][k];
+}
+
 // enthalpy h_k (J/kg) and cp_k (J/kg/K) at temperature t (Thermo.cu:25-45)
 template <int NS>
 __device__ __forceinline__ void enthalpy_cp(double t, double *h, double *cp) {
@@ -19,15 +29,13 @@ __device__ __forceinline__ void enthalpy_cp(double t, double *h, double *cp) {
 #pragma unroll
   for (int i = 0; i < NS; ++i) {
     double tt = t, tt2 = t2, tt3 = t3, tt4 = t4, tt5 = t5;
-    const double *c = c_p.hi[i];
     const bool below = t < c_p.t_low[i];
     if (below) {
       tt = c_p.t_low[i];
       tt2 = tt * tt; tt3 = tt2 * tt; tt4 = tt3 * tt; tt5 = tt4 * tt;
-      c = c_p.lo[i];
-    } else if (t < c_p.t_mid[i]) {
-      c = c_p.lo[i];
     }
+    double c[6];
+    nasa_coeffs<6>(i, below || t < c_p.t_mid[i], c);
     double hi = c[0] * tt + 0.5 * c[1] * tt2 + c[2] * tt3 * (1.0 / 3) + 0.25 * c[3] * tt4 + 0.2 * c[4] * tt5 + c[5];
     const double cpi = c[0] + c[1] * tt + c[2] * tt2 + c[3] * tt3 + c[4] * tt4;
     if (below) hi += cpi * (t - tt);
@@ -43,15 +51,13 @@ __device__ __forceinline__ void enthalpy(double t, double *h) {
 #pragma unroll
   for (int i = 0; i < NS; ++i) {
     double tt = t, tt2 = t2, tt3 = t3, tt4 = t4, tt5 = t5;
-    const double *c = c_p.hi[i];
     const bool below = t < c_p.t_low[i];
     if (below) {
       tt = c_p.t_low[i];
       tt2 = tt * tt; tt3 = tt2 * tt; tt4 = tt3 * tt; tt5 = tt4 * tt;
-      c = c_p.lo[i];
-    } else if (t < c_p.t_mid[i]) {
-      c = c_p.lo[i];
     }
+    double c[6];
+    nasa_coeffs<6>(i, below || t < c_p.t_mid[i], c);
     double hi = c[0] * tt + 0.5 * c[1] * tt2 + c[2] * tt3 * (1.0 / 3) + 0.25 * c[3] * tt4 + 0.2 * c[4] * tt5 + c[5];
     if (below) {
       const double cpi = c[0] + c[1] * tt + c[2] * tt2 + c[3] * tt3 + c[4] * tt4;
