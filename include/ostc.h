@@ -415,8 +415,9 @@ ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg,
 /* Tile shape of the flux kernel of direction dir (0 x, 1 y, 2 z): rows of
  * 32 threads per CTA (1, 2, 4 or 8) and chunks marched per CTA; rows may be
  * OR-ed with (2 << 8) or (3 << 8) to select the builds limited to 128 or 80
- * registers (two or three 256-thread CTAs per SM), or with (4 << 8) for the
- * build limited to 168 registers (three CTAs of at most 4 rows per SM).
+ * registers (two or three 256-thread CTAs per SM), or with (4 << 8) / (5 << 8)
+ * for the builds limited to 168 / 96 registers (three / five CTAs of at most
+ * 4 rows per SM).
  * dir 3, 4, 5: a tile for a separate viscous-flux kernel of direction
  * dir - 3; with one set, a viscous flow runs the inviscid flux (tile of dir
  * - 3) and the viscous flux as two kernels instead of the fused one. rows = 0

@@ -1191,9 +1191,9 @@ ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
   if (dir > 2 && rows == 0) {  // back to the fused kernel
     t.vrows = 0;
   } else {
-    if (chunks < 1 || chunks > 4096 || minb < 0 || minb > 4) return OSTC_ERR_INVALID_ARG;
+    if (chunks < 1 || chunks > 4096 || minb < 0 || minb > 5) return OSTC_ERR_INVALID_ARG;
     if (!(rows == 1 || rows == 2 || rows == 4 || rows == 8)) return OSTC_ERR_INVALID_ARG;
-    if (minb == 4 && rows > 4) return OSTC_ERR_INVALID_ARG;  // the 168-register build takes <= 128 threads
+    if (minb >= 4 && rows > 4) return OSTC_ERR_INVALID_ARG;  // the 168- and 96-register builds take <= 128 threads
     if (dir > 2) {
       t.vrows = rows, t.vchunks = chunks, t.vminb = minb < 1 ? 1 : minb;
     } else {

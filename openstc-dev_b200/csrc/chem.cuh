@@ -284,7 +284,7 @@ __device__ __forceinline__ void point_implicit_increment(double T, double p, con
   double t = T;
   iters = 0;
   for (int it = 1; it <= 100; ++it) {
-    enthalpy_cp<NS>(t, h, cp);
+    enthalpy_cp<NS, false>(t, h, cp);
     double hs = 0, cps = 0;
 #pragma unroll
     for (int l = 0; l < NS; ++l) {

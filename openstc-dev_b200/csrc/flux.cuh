@@ -49,10 +49,11 @@ __device__ __forceinline__ void face_total(const DevZone &z, int g0, bool viscou
 
 // register budget of a flux build: MINB 1..3 = that many resident CTAs of 256
 // threads per SM (255, 128 or 80 registers); MINB 4 = three CTAs of at most
-// 128 threads (168 registers, 12 warps per SM)
+// 128 threads (168 registers, 12 warps per SM); MINB 5 = five CTAs of at most
+// 128 threads (96 registers, 20 warps per SM)
 template <int MINB>
 struct FluxBounds {
-  static constexpr int threads = MINB == 4 ? 128 : 256;
+  static constexpr int threads = MINB >= 4 ? 128 : 256;
   static constexpr int blocks = MINB == 4 ? 3 : MINB;
 };
 
@@ -223,6 +224,7 @@ template <int NS, int INV, int DIR, int PART, int NT>
 static cudaError_t launch_flux_p(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
                                  int viscous, cudaStream_t s) {
   switch (t.minb) {
+    case 5: return launch_flux_m<NS, INV, DIR, 5, PART, NT>(z, t, tab, accumulate, viscous, s);
     case 4: return launch_flux_m<NS, INV, DIR, 4, PART, NT>(z, t, tab, accumulate, viscous, s);
     case 3: return launch_flux_m<NS, INV, DIR, 3, PART, NT>(z, t, tab, accumulate, viscous, s);
     case 2: return launch_flux_m<NS, INV, DIR, 2, PART, NT>(z, t, tab, accumulate, viscous, s);

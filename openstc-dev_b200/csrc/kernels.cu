@@ -208,7 +208,7 @@ __device__ __forceinline__ void update_rk_cells(const DevZone &z, const int bx, 
     int iter = 0;
     while (err > 1e-3 && iter++ < 1000) {
       double h[NS], cp[NS];
-      enthalpy_cp<NS>(t, h, cp);
+      enthalpy_cp<NS, false>(t, h, cp);
       double cpt = 0, hh = 0;
 #pragma unroll
       for (int l = 0; l < NS; ++l) {

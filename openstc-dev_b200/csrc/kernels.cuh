@@ -12,7 +12,7 @@ struct TileShape {
   int rows;
   int chunks;
   int minb = 1;  // register budget: 1 (<=255 regs), 2 (<=128) or 3 (<=80) CTAs of 256 threads per SM,
-                 // 4 (<=168 regs, CTAs of at most 128 threads)
+                 // 4 (<=168 regs) or 5 (<=96 regs) with CTAs of at most 128 threads
   // viscous flow: vrows > 0 splits the face flux into an inviscid kernel
   // (the shape above) and a viscous kernel of this shape
   int vrows = 0;

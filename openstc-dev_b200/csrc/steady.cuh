@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(256) update_bv_kernel(DevZone z) {
     int iter = 0;
     while (err > 1e-3 && iter++ < 1000) {
       double hh[NS], cp[NS];
-      enthalpy_cp<NS>(t, hh, cp);
+      enthalpy_cp<NS, false>(t, hh, cp);
       double cpt = 0, hs = 0;
 #pragma unroll
       for (int l = 0; l < NS; ++l) {

@@ -22,8 +22,11 @@ __device__ __forceinline__ void nasa_coeffs(int i, bool low, double *c) {
   for (int k = 0; k < N; ++k) c[k] = low ? c_p.lo[i][k] : c_p.hi[i][k];
 }
 
-// enthalpy h_k (J/kg) and cp_k (J/kg/K) at temperature t (Thermo.cu:25-45)
-template <int NS>
+// enthalpy h_k (J/kg) and cp_k (J/kg/K) at temperature t (Thermo.cu:25-45).
+// SEL: coefficients selected by value (nasa_coeffs; the register-starved flux
+// kernels) or through a row pointer (one constant load per coefficient; the
+// per-cell Newton solves, where it measured faster)
+template <int NS, bool SEL = true>
 __device__ __forceinline__ void enthalpy_cp(double t, double *h, double *cp) {
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
 #pragma unroll
@@ -34,8 +37,10 @@ __device__ __forceinline__ void enthalpy_cp(double t, double *h, double *cp) {
       tt = c_p.t_low[i];
       tt2 = tt * tt; tt3 = tt2 * tt; tt4 = tt3 * tt; tt5 = tt4 * tt;
     }
-    double c[6];
-    nasa_coeffs<6>(i, below || t < c_p.t_mid[i], c);
+    const bool low = below || t < c_p.t_mid[i];
+    double cs[6];
+    if (SEL) nasa_coeffs<6>(i, low, cs);
+    const double *c = SEL ? cs : (low ? c_p.lo[i] : c_p.hi[i]);
     double hi = c[0] * tt + 0.5 * c[1] * tt2 + c[2] * tt3 * (1.0 / 3) + 0.25 * c[3] * tt4 + 0.2 * c[4] * tt5 + c[5];
     const double cpi = c[0] + c[1] * tt + c[2] * tt2 + c[3] * tt3 + c[4] * tt4;
     if (below) hi += cpi * (t - tt);

@@ -676,7 +676,7 @@ class Solver:
                     c = 1
                     while True:
                         for minb in budgets:
-                            if minb == 4 and R > 4:
+                            if minb >= 4 and R > 4:
                                 continue
                             out.append((R | (minb << 8 if minb > 1 else 0), min(c, cmax)))
                         if c >= cmax:
@@ -686,14 +686,14 @@ class Solver:
 
             self.set_tile(d + 3, 0, 0)
             fused = []
-            for R, Cc in cands((1, 2, 3, 4)):
+            for R, Cc in cands((1, 2, 3, 4, 5)):
                 self.set_tile(d, R, Cc)
                 fused.append((self._time_flux(d, warmup, reps), R, Cc))
             fused.sort()
             choice = (fused[0][0], fused[0][1:], (0, 0))
             if viscous:
                 inv, vis = [], []
-                for R, Cc in cands((2, 3, 4)):
+                for R, Cc in cands((2, 3, 4, 5)):
                     self.set_tile(d, R, Cc)
                     inv.append((self._time_flux(d + 3, warmup, reps), R, Cc))
                     self.set_tile(d + 3, R, Cc)
