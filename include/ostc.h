@@ -254,6 +254,21 @@ ostc_status ostc_data_communication(ostc_ctx *ctx, int with_cv, void *stream);
 /* update_physical_properties<mix> over [-1, m] (src/FieldOperation.cuh:112-146). */
 ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream);
 
+/* eliminate_k_gradient<with_cv> (src/FieldOperation.cuh:372-400): on 2-D
+ * blocks (mz == 1) every k ghost plane of bv, sv (and cv when with_cv) takes
+ * the values of the plane k = 0 over the whole ghosted (i, j) range, so
+ * nothing varies across k. A no-op for 3-D blocks. The drivers below call it
+ * where the reference does: before the boundary conditions of the
+ * initialisation (src/Driver.cu:54-60), and after the interface exchange of
+ * every RK3 stage (src/RK.cuh:147-153, with cv) and steady step
+ * (src/SteadySim.cuh:101-107, without).
+ * 2-D problems: every block has mz == 1 (the reference takes the dimension
+ * from its first block, src/Mesh.cpp:612-614); the z fluxes are skipped
+ * (src/InviscidScheme.cu:34, src/SchemeSelector.cuh:64), the time step and
+ * the Roe entropy fix drop their zeta terms (src/TimeAdvanceFunc.cuh:60-93,
+ * src/Roe.cu:79-81), and the stage update zeroes rho w (src/RK.cuh:213-215). */
+ostc_status ostc_eliminate_k_gradient(ostc_ctx *ctx, int with_cv, void *stream);
+
 /* ----------------------------------------------------------------------- */
 /* fused drivers                                                           */
 /* ----------------------------------------------------------------------- */
@@ -407,7 +422,9 @@ ostc_status ostc_use_generated_chemistry(ostc_ctx *ctx, int on);
  * (x,y,z as host arrays with ghost count ngg+1), as Block::compute_jac_metric
  * (src/Mesh.cpp:259-521). Host-only helper: fills host jac (g=ngg) and host
  * metric (80-byte records, g=ngg). Returns OSTC_ERR_NONPHYSICAL on a
- * non-positive interior Jacobian.                                           */
+ * non-positive interior Jacobian. mz == 1 is a 2-D block: its k ghost nodes
+ * sit at z(i,j,0) + k, as the reference's grid reader puts them
+ * (src/Mesh.cpp:840-854); otherwise mz >= 3.                               */
 ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg,
                                   const double *x, const double *y, const double *z,
                                   double *jac_out, void *metric_out);

@@ -308,7 +308,8 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
     const ostc_zone &z = zones[b];
     if (z.mx < 2 || z.my < 2 || z.mz < 1 || z.ngg < need_ngg || z.dq_ngg < 0 || z.dq_ngg > 1)
       return OSTC_ERR_INVALID_ARG;
-    if (z.mz == 1) return OSTC_ERR_UNSUPPORTED;  // 2-D path not built
+    // the problem is 2-D when the first block has mz == 1 (Mesh.cpp:612-614); every block alike
+    if ((z.mz == 1) != (zones[0].mz == 1)) return OSTC_ERR_INVALID_ARG;
     if (!z.bv || !z.cv || !z.qn || !z.dq || !z.jac || !z.metric || !z.vel || !z.acoustic_speed || !z.mach ||
         !z.mul || !z.thermal_conductivity)
       return OSTC_ERR_INVALID_ARG;
@@ -791,6 +792,13 @@ ostc_status ostc_set_interfaces(ostc_ctx *ctx, const ostc_interface *f, int n) {
   return OSTC_OK;
 }
 
+ostc_status ostc_eliminate_k_gradient(ostc_ctx *ctx, int with_cv, void *stream) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  if (ensure_param(ctx, S(stream))) return ctx->last;
+  for (auto &z : ctx->dz) CK(launch_eliminate_k(z, with_cv, S(stream)));
+  return OSTC_OK;
+}
+
 ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;
   if (ensure_param(ctx, S(stream))) return ctx->last;
@@ -801,6 +809,8 @@ ostc_status ostc_initialize(ostc_ctx *ctx, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;
   ostc_status st;
   if ((st = repack_metrics(ctx, S(stream)))) return st;
+  // 2-D: the k ghost planes copy the plane k = 0 first (Driver.cu:54-60)
+  if ((st = ostc_eliminate_k_gradient(ctx, 0, stream))) return st;
   if ((st = ostc_apply_boundary_conditions(ctx, 0, stream))) return st;
   if (ensure_param(ctx, S(stream))) return ctx->last;
   if ((st = cells_all(ctx, CellOp::Velocity, 2, {}, S(stream)))) return st;
@@ -823,6 +833,7 @@ ostc_status ostc_rk3_stage(ostc_ctx *ctx, int rk, void *stream) {
   if ((st = ostc_update_cv_and_bv_rk(ctx, dt, rk, stream))) return st;
   if ((st = ostc_apply_boundary_conditions(ctx, 1, stream))) return st;
   if ((st = ostc_data_communication(ctx, 1, stream))) return st;
+  if ((st = ostc_eliminate_k_gradient(ctx, 1, stream))) return st;  // 2-D only (RK.cuh:147-153)
   return ostc_update_physical_properties(ctx, stream);
 }
 
@@ -864,6 +875,7 @@ static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
     }
     if ((st = ostc_apply_boundary_conditions(ctx, 1, s))) return st;
     if ((st = ostc_data_communication(ctx, 1, s))) return st;
+    if ((st = ostc_eliminate_k_gradient(ctx, 1, s))) return st;
     if ((st = ostc_update_physical_properties(ctx, s))) return st;
   }
   if (with_hist) {
@@ -1019,6 +1031,7 @@ static ostc_status enqueue_steady_step(ostc_ctx *ctx, bool with_hist, cudaStream
   if ((st = ostc_update_bv(ctx, s))) return st;
   if ((st = ostc_apply_boundary_conditions(ctx, 0, s))) return st;
   if ((st = ostc_data_communication(ctx, 0, s))) return st;
+  if ((st = ostc_eliminate_k_gradient(ctx, 0, s))) return st;  // 2-D only (SteadySim.cuh:101-107)
   if ((st = ostc_update_physical_properties(ctx, s))) return st;
   if (with_hist) {
     CellArgs a;
@@ -1144,7 +1157,8 @@ ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream) {
         CK(flux_launch(ctx, ctx->dz[0], d, ctx->flux_tab[d], 1, part, S(stream)));
         return OSTC_OK;
       }
-      for (auto &z : ctx->dz) CK(flux_launch(ctx, z, d, nullptr, 1, part, S(stream)));
+      for (auto &z : ctx->dz)
+        if (d < 2 || z.mz > 1) CK(flux_launch(ctx, z, d, nullptr, 1, part, S(stream)));  // 2-D: no z flux
       return OSTC_OK;
     }
     case OSTC_OP_SOURCE: {

@@ -273,7 +273,8 @@ __device__ __forceinline__ void inviscid_face_pv(const DevZone &z, int g0, doubl
   riemann<NV, NS>(pl, pr, z, g0, g0 + dir_stride<DIR>(z), DIR, F);
 }
 
-// Harten entropy-fix width at one point (compute_entropy_fix_delta, Roe.cu:61-85), 3-D form;
+// Harten entropy-fix width at one point (compute_entropy_fix_delta, Roe.cu:61-85): the 3-D
+// form, or for 2-D blocks (mz == 1) the form without W and kz;
 // evaluated here at the two points of a face instead of a separate pass and array
 __device__ __forceinline__ double entropy_fix_delta(const DevZone &z, int g) {
   const double u = bvl(z, g, 1), v = bvl(z, g, 2), w = bvl(z, g, 3);
@@ -286,6 +287,7 @@ __device__ __forceinline__ double entropy_fix_delta(const DevZone &z, int g) {
   const double kx = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
   const double ky = sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
   const double kz = sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
+  if (z.mz == 1) return c_p.entropy_fix_factor * (U + V + ld(z.a + g) * 0.5 * (kx + ky));
   return c_p.entropy_fix_factor * (U + V + W + ld(z.a + g) * (kx + ky + kz) * (1.0 / 3));
 }
 

@@ -1042,6 +1042,33 @@ cudaError_t launch_residual_final(const double *partial, int n_part, double n_to
   return cudaGetLastError();
 }
 
+// 2-D blocks (mz == 1): eliminate_k_gradient (FieldOperation.cuh:372-400).
+// Every ghost plane k = +-1 .. +-ngg of bv, sv (and cv) becomes a copy of the
+// plane k = 0, over the whole ghosted (i, j) range, so every difference
+// across k vanishes.
+__global__ void eliminate_k_kernel(DevZone z, int with_cv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x - z.ngg;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y - z.ngg;
+  if (i >= z.mx + z.ngg || j >= z.my + z.ngg) return;
+  const int g0 = gidx(z, i, j, 0);
+  const long long S = z.sz;
+  for (int k = 1; k <= z.ngg; ++k) {
+    const int gp = g0 + k * z.d1, gm = g0 - k * z.d1;
+    for (int l = 0; l < 6; ++l) z.bv[l * S + gp] = z.bv[l * S + gm] = z.bv[l * S + g0];
+    for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * S + gp] = z.sv[l * S + gm] = z.sv[l * S + g0];
+    if (with_cv)
+      for (int l = 0; l < c_p.n_var; ++l) z.cv[l * S + gp] = z.cv[l * S + gm] = z.cv[l * S + g0];
+  }
+}
+
+cudaError_t launch_eliminate_k(const DevZone &z, int with_cv, cudaStream_t s) {
+  if (z.mz != 1) return cudaSuccess;
+  const dim3 blk(32, 8);
+  const dim3 grid((z.mx + 2 * z.ngg + 31) / 32, (z.my + 2 * z.ngg + 7) / 8);
+  eliminate_k_kernel<<<grid, blk, 0, s>>>(z, with_cv);
+  return cudaGetLastError();
+}
+
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s) {
   const int n0 = b.re[0] - b.rs[0] + 1, n1 = b.re[1] - b.rs[1] + 1, n2 = b.re[2] - b.rs[2] + 1;

@@ -128,6 +128,8 @@ cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, do
                               long long *stats, const int *count, cudaStream_t s);
 cudaError_t prepare_chem_surrogate();
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
+// 2-D blocks: copy the plane k = 0 into every k ghost plane (no-op when mz > 1)
+cudaError_t launch_eliminate_k(const DevZone &z, int with_cv, cudaStream_t s);
 cudaError_t upload_param(const DevParam &p, cudaStream_t s);
 cudaError_t upload_param_flux0(const DevParam &p, cudaStream_t s);   // flux0.cu
 cudaError_t upload_param_flux9(const DevParam &p, cudaStream_t s);   // flux9.cu

@@ -31,7 +31,11 @@ struct G {  // coordinates with ngg+1 ghost layers
 
 extern "C" ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg, const double *x, const double *y,
                                              const double *z, double *jac_out, void *metric_out) {
-  if (mx < 3 || my < 3 || mz < 3 || ngg < 1 || !x || !y || !z || !jac_out || !metric_out) return OSTC_ERR_INVALID_ARG;
+  // mz == 1: a 2-D block, whose k ghost nodes the caller places at z(i, j, 0) + k as the
+  // reference's grid reader does (Mesh.cpp:840-854); the plane k = 0 is then its interior
+  // (Mesh.cpp:264-268)
+  if (mx < 3 || my < 3 || (mz < 3 && mz != 1) || ngg < 1 || !x || !y || !z || !jac_out || !metric_out)
+    return OSTC_ERR_INVALID_ARG;
   const G X(x, mx, my, mz, ngg + 1), Y(y, mx, my, mz, ngg + 1), Z(z, mx, my, mz, ngg + 1);
   const long d2 = mx + 2 * ngg, d1 = (long)(my + 2 * ngg) * d2, dt = (d1 + d2 + 1) * ngg;
   unsigned char *mo = (unsigned char *)metric_out;

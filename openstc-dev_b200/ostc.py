@@ -118,6 +118,7 @@ def lib():
             "ostc_apply_boundary_conditions": [vp, i, vp],
             "ostc_data_communication": [vp, i, vp],
             "ostc_update_physical_properties": [vp, vp],
+            "ostc_eliminate_k_gradient": [vp, i, vp],
             "ostc_initialize": [vp, vp],
             "ostc_rk3_stage": [vp, i, vp],
             "ostc_rk3_steps": [vp, i, C.POINTER(d), C.POINTER(d), vp],
@@ -536,6 +537,10 @@ class Solver:
     def update_physical_properties(self):
         check(lib().ostc_update_physical_properties(self.ctx, self._s()), "ostc_update_physical_properties")
 
+    def eliminate_k_gradient(self, with_cv: bool):
+        """2-D blocks: the k ghost planes take the plane k = 0 (a no-op in 3-D)"""
+        check(lib().ostc_eliminate_k_gradient(self.ctx, int(with_cv), self._s()), "ostc_eliminate_k_gradient")
+
     def rk3_stage(self, rk: int):
         check(lib().ostc_rk3_stage(self.ctx, rk, self._s()), "ostc_rk3_stage")
 
@@ -716,13 +721,18 @@ class Solver:
 def grid_coordinates(mx, my, mz, ng, dx, warp=0.02, periodic_k=True):
     """Node coordinates with ng ghost layers: x = i dx plus a 2% sinusoidal
     curvilinear warp, periodic in k with period mz*dx (nodes k = 0..mz-1
-    are distinct), analytic in the ghost layers."""
+    are distinct), analytic in the ghost layers. mz == 1 is a 2-D grid: the
+    warp stays in the (x, y) plane and the k ghost nodes sit at z = k, as
+    the reference's grid reader places them (src/Mesh.cpp:840-854)."""
     i = np.arange(-ng, mx + ng, dtype=np.float64)
     j = np.arange(-ng, my + ng, dtype=np.float64)
     k = np.arange(-ng, mz + ng, dtype=np.float64)
     K, J, I = np.meshgrid(k, j, i, indexing="ij")
     Lx, Ly, Lz = (mx - 1) * dx, (my - 1) * dx, mz * dx
     x0, y0, z0 = I * dx, J * dx, K * dx
+    if mz == 1:
+        sx, sy = np.sin(2 * np.pi * x0 / Lx), np.sin(2 * np.pi * y0 / Ly)
+        return x0 + warp * dx * sy, y0 + warp * dx * sx, K.copy()
     sx, sy, sz = np.sin(2 * np.pi * x0 / Lx), np.sin(2 * np.pi * y0 / Ly), np.sin(2 * np.pi * z0 / Lz)
     x = x0 + warp * dx * sy * sz
     y = y0 + warp * dx * sx * sz
@@ -802,7 +812,9 @@ def case_vortex(mx=128, my=128, mz=8, dx=1e-3, k_bc="periodic", steps=100, fixed
     ext = (mx, my, mz)
     faces = [bc_face(0, BC_INFLOW, 0, -1, ext, ng, inf), bc_face(0, BC_OUTFLOW, 0, 1, ext, ng),
              bc_face(0, BC_SYMMETRY, 1, -1, ext, ng), bc_face(0, BC_SYMMETRY, 1, 1, ext, ng)]
-    if k_bc == "periodic":
+    if mz == 1:  # 2-D: no k faces (the k ghost planes copy k = 0)
+        pass
+    elif k_bc == "periodic":
         faces += [bc_face(0, BC_PERIODIC, 2, -1, ext, ng), bc_face(0, BC_PERIODIC, 2, 1, ext, ng)]
     else:
         faces += [bc_face(0, BC_SYMMETRY, 2, -1, ext, ng), bc_face(0, BC_SYMMETRY, 2, 1, ext, ng)]
@@ -844,7 +856,8 @@ def case_bc_box(kind="wall_farfield", mx=40, my=32, mz=10, dx=1e-3) -> Case:
         faces = [bc_face(0, BC_SUBSONIC_INFLOW, 0, -1, ext, ng, tot), bc_face(0, BC_BACK_PRESSURE, 0, 1, ext, ng, bp),
                  bc_face(0, BC_WALL, 1, -1, ext, ng, dict(wall_isothermal=0)),
                  bc_face(0, BC_SYMMETRY, 1, 1, ext, ng)]
-    faces += [bc_face(0, BC_SYMMETRY, 2, -1, ext, ng), bc_face(0, BC_SYMMETRY, 2, 1, ext, ng)]
+    if mz > 1:
+        faces += [bc_face(0, BC_SYMMETRY, 2, -1, ext, ng), bc_face(0, BC_SYMMETRY, 2, 1, ext, ng)]
     c.faces = faces
     c.name = "bc_box_%s_%dx%dx%d" % (kind, mx, my, mz)
     return c
@@ -984,6 +997,21 @@ def block_layout(seed=37, n_layers=4, n_cols=3, rows=(3, 3, 3), extra_row=(1, 0)
     return out
 
 
+def planar_layout(nx=(20, 17, 13), ny=(15, 19)):
+    """A 2-D block layout for case_uneven_blocks: columns of nx[c] points and
+    rows of ny[r] points sharing their face planes, every block one point
+    deep in k (mz = 1). Returns [((i0, j0, 0), (mx, my, 1)), ...]."""
+    out = []
+    i0 = 0
+    for mx in nx:
+        j0 = 0
+        for my in ny:
+            out.append(((i0, j0, 0), (mx, my, 1)))
+            j0 += my - 1
+        i0 += mx - 1
+    return out
+
+
 def sst_freestream(state: dict, turbulence_intensity=0.01, viscosity_ratio=10.0) -> dict:
     """k, omega and mut of a free stream from its turbulence intensity and
     turbulent-to-laminar viscosity ratio (BoundCond.cpp:84-93): mut = ratio
@@ -1032,12 +1060,13 @@ def case_uneven_blocks(seed=37, dx=1e-4, reconstruction=2, inviscid_scheme=4, ma
     ng = s.ngg
     if layout is None:
         layout = block_layout(seed)
-    for (_, e) in layout:
-        if min(e) < 2 * ng + 2:
-            raise ValueError("block too small for the stencil: %s" % (e,))
     NX = max(o[0] + e[0] for o, e in layout)
     NY = max(o[1] + e[1] for o, e in layout)
     NZ = max(o[2] + e[2] for o, e in layout)
+    planar = NZ == 1  # a 2-D problem: no k faces, interfaces over k = 0 only
+    for (_, e) in layout:
+        if min(e[:2] if planar else e) < 2 * ng + 2:
+            raise ValueError("block too small for the stencil: %s" % (e,))
     xg, yg, zg = grid_coordinates(NX, NY, NZ, ng + 1, dx, periodic_k=False)
     a = math.sqrt(GAMMA_AIR * R_U / MW_AIR * T)
     U = mach * a
@@ -1078,7 +1107,7 @@ def case_uneven_blocks(seed=37, dx=1e-4, reconstruction=2, inviscid_scheme=4, ma
                     elif d == 1:
                         faces.append(bc_face(q, BC_WALL, 1, -1, e, ng, wall) if direction < 0 else
                                      bc_face(q, BC_FARFIELD, 1, 1, e, ng, ff))
-                    else:
+                    elif not planar:
                         faces.append(bc_face(q, BC_SYMMETRY, 2, direction, e, ng))
                     continue
                 # interior face: one interface patch per neighbour sharing this plane
@@ -1095,7 +1124,7 @@ def case_uneven_blocks(seed=37, dx=1e-4, reconstruction=2, inviscid_scheme=4, ma
                             continue
                         s0, s1 = max(lo[c], tlo[c]), min(hi[c], thi[c])
                         ov.append((c, s0, s1))
-                    if any(s1 - s0 + 1 < 2 for _, s0, s1 in ov):
+                    if any(s1 - s0 + 1 < 2 and not (planar and c == 2) for c, s0, s1 in ov):
                         continue
                     f = IfaceC()
                     f.block, f.target, f.face, f.direction = q, t, d, direction
@@ -1174,7 +1203,8 @@ def case_mixing_layer(mx=256, my=256, mz=256, dx=1e-4, seed=2024, steps=200, ful
     """The reacting mixing layer: upper stream (y > 0) air (O2/N2 mass
     0.233/0.767) at 1500 K, Mach 2; lower stream H2/N2 (mole 0.3/0.7) at
     300 K, Mach 1.2; p = 1 atm; profiles blended by 0.5(1 + tanh(y / 8dy));
-    seeded 1 % white-noise velocity perturbation (numpy PCG64). 9-species,
+    seeded 1 % white-noise velocity perturbation (numpy PCG64; mz == 1: a 2-D
+    layer, w = 0 and no k faces). 9-species,
     19-reaction H2-air mechanism, MUSCL (minmod) + AUSM+, laminar viscous
     flux, point-implicit chemistry tag (explicit under RK3, quirk A8), RK3 at
     CFL 0.4. Uniform Cartesian grid dx = dy = dz. Extrapolation (outflow)
@@ -1216,13 +1246,14 @@ def case_mixing_layer(mx=256, my=256, mz=256, dx=1e-4, seed=2024, steps=200, ful
     bv[0] = p0 / (R_U * mw_inv * T)
     bv[1] = U * (1 + 0.01 * rng.uniform(-1, 1, P))
     bv[2] = 0.01 * U * rng.uniform(-1, 1, P)
-    bv[3] = 0.01 * U * rng.uniform(-1, 1, P)
+    bv[3] = 0.01 * U * rng.uniform(-1, 1, P) if mz > 1 else 0.0  # a 2-D layer (mz == 1) has no w
     bv[4] = p0
     bv[5] = T
     ext = (mx, my, mz)
     faces = [bc_face(0, BC_OUTFLOW, 0, -1, ext, ng), bc_face(0, BC_OUTFLOW, 0, 1, ext, ng),
-             bc_face(0, BC_OUTFLOW, 1, -1, ext, ng), bc_face(0, BC_OUTFLOW, 1, 1, ext, ng),
-             bc_face(0, BC_PERIODIC, 2, -1, ext, ng), bc_face(0, BC_PERIODIC, 2, 1, ext, ng)]
+             bc_face(0, BC_OUTFLOW, 1, -1, ext, ng), bc_face(0, BC_OUTFLOW, 1, 1, ext, ng)]
+    if mz > 1:
+        faces += [bc_face(0, BC_PERIODIC, 2, -1, ext, ng), bc_face(0, BC_PERIODIC, 2, 1, ext, ng)]
     return Case("mixing_layer_h2air_%dx%dx%d" % (mx, my, mz), s, mech, [b], faces, steps)
 
 

@@ -910,7 +910,7 @@ void inviscid_direction(const ostc_param *P, Z &Zn, int d) {
           const double *m = Zn.metric.at(i, j, k);
           for (int c = 0; c < 3; ++c) met[is * 3 + c] = m[3 * d + c];
           jac[is] = Zn.jac(i, j, k);
-          if (roe && s >= -1 && s <= n) {  // compute_entropy_fix_delta on [-1, m] (Roe.cu:61-85), 3-D
+          if (roe && s >= -1 && s <= n) {  // compute_entropy_fix_delta on [-1, m] (Roe.cu:61-85)
             const double u = Zn.bv(i, j, k, 1), v = Zn.bv(i, j, k, 2), w = Zn.bv(i, j, k, 3);
             const double U = std::abs(u * m[0] + v * m[1] + w * m[2]);
             const double V = std::abs(u * m[3] + v * m[4] + w * m[5]);
@@ -918,7 +918,10 @@ void inviscid_direction(const ostc_param *P, Z &Zn, int d) {
             const double kx = std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
             const double ky = std::sqrt(m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
             const double kz = std::sqrt(m[6] * m[6] + m[7] * m[7] + m[8] * m[8]);
-            delta[is] = P->entropy_fix_factor * (U + V + W + Zn.a(i, j, k) * (kx + ky + kz) / 3.0);
+            if (Zn.mz == 1)  // param->dim == 2 (Roe.cu:79-81)
+              delta[is] = P->entropy_fix_factor * (U + V + Zn.a(i, j, k) * 0.5 * (kx + ky));
+            else
+              delta[is] = P->entropy_fix_factor * (U + V + W + Zn.a(i, j, k) * (kx + ky + kz) / 3.0);
           }
         }
         // face fluxes for s = -1 .. n-1 (face between s and s+1), stored at s+1
@@ -2325,6 +2328,24 @@ int oracle_data_communication(const ostc_param *P, ostc_zone *zones, int n_zones
   return 0;
 }
 
+// eliminate_k_gradient (FieldOperation.cuh:372-400) on a 2-D block (mz == 1):
+// the k ghost planes of bv, sv (and cv) copy the plane k = 0 over the whole
+// ghosted (i, j) range
+int oracle_eliminate_k_gradient(const ostc_param *P, ostc_zone *z, int with_cv) {
+  Z Zn(z);
+  if (Zn.mz != 1) return 0;
+  const int g = Zn.ngg;
+  for (int j = -g; j < Zn.my + g; ++j)
+    for (int i = -g; i < Zn.mx + g; ++i)
+      for (int k = 1; k <= g; ++k) {
+        for (int l = 0; l < 6; ++l) Zn.bv(i, j, k, l) = Zn.bv(i, j, -k, l) = Zn.bv(i, j, 0, l);
+        for (int l = 0; l < P->n_scalar; ++l) Zn.sv(i, j, k, l) = Zn.sv(i, j, -k, l) = Zn.sv(i, j, 0, l);
+        if (with_cv)
+          for (int l = 0; l < P->n_var; ++l) Zn.cv(i, j, k, l) = Zn.cv(i, j, -k, l) = Zn.cv(i, j, 0, l);
+      }
+  return 0;
+}
+
 int oracle_update_physical_properties(const ostc_param *P, ostc_zone *z) {
   Z Zn(z);
 #pragma omp parallel for collapse(2) schedule(static)
@@ -2337,8 +2358,10 @@ int oracle_update_physical_properties(const ostc_param *P, ostc_zone *z) {
 int oracle_initialize(const ostc_config *c, const ostc_param *P, ostc_zone *zones, int n_zones,
                       const ostc_bc_face *f, int n_faces) {
   (void)c;
-  // Driver::initialize_computation (Driver.cu:39-98): BCs without cv, velocity
-  // everywhere, interfaces, properties; then RK3_bv pre-loop (RK.cuh:40-49).
+  // Driver::initialize_computation (Driver.cu:39-98): on 2-D blocks the k
+  // ghost planes first, BCs without cv, velocity everywhere, interfaces,
+  // properties; then RK3_bv pre-loop (RK.cuh:40-49).
+  for (int b = 0; b < n_zones; ++b) oracle_eliminate_k_gradient(P, &zones[b], 0);
   int st = oracle_apply_boundary_conditions(P, zones, n_zones, f, n_faces, 0);
   if (st) return st;
   for (int b = 0; b < n_zones; ++b) {
@@ -2399,6 +2422,7 @@ int oracle_rk3_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zones
       int st = oracle_apply_boundary_conditions(P, zones, n_zones, f, n_faces, 1);
       if (st) return st;
       oracle_data_communication(P, zones, n_zones, 1);
+      for (int b = 0; b < n_zones; ++b) oracle_eliminate_k_gradient(P, &zones[b], 1);  // 2-D (RK.cuh:147-153)
       for (int b = 0; b < n_zones; ++b) oracle_update_physical_properties(P, &zones[b]);
     }
     if (c->chem_mode == 1) {
@@ -2438,6 +2462,7 @@ int oracle_rk3_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zones
       int st = oracle_apply_boundary_conditions(P, zones, n_zones, f, n_faces, 1);
       if (st) return st;
       oracle_data_communication(P, zones, n_zones, 1);
+      for (int b = 0; b < n_zones; ++b) oracle_eliminate_k_gradient(P, &zones[b], 1);  // 2-D (RK.cuh:147-153)
       for (int b = 0; b < n_zones; ++b) oracle_update_physical_properties(P, &zones[b]);
     }
     if (dt_hist) dt_hist[step] = dt;
@@ -2515,6 +2540,7 @@ int oracle_steady_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zo
     int st = oracle_apply_boundary_conditions(P, zones, n_zones, f, n_faces, 0);
     if (st) return st;
     oracle_data_communication(P, zones, n_zones, 0);
+    for (int b = 0; b < n_zones; ++b) oracle_eliminate_k_gradient(P, &zones[b], 0);  // 2-D (SteadySim.cuh:101-107)
     for (int b = 0; b < n_zones; ++b) oracle_update_physical_properties(P, &zones[b]);
     if (res_hist) {
       double res[4] = {0, 0, 0, 0};

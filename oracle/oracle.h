@@ -40,6 +40,8 @@ int oracle_apply_boundary_conditions(const ostc_param *p, ostc_zone *zones, int 
                                      const ostc_bc_face *f, int n_faces, int with_cv);
 /* update_physical_properties over [-1, m] (src/FieldOperation.cuh:112-146) */
 int oracle_update_physical_properties(const ostc_param *p, ostc_zone *z);
+/* 2-D blocks: the k ghost planes copy k = 0 (no-op when mz > 1) */
+int oracle_eliminate_k_gradient(const ostc_param *p, ostc_zone *z, int with_cv);
 /* Driver::initialize_computation + RK3_bv pre-loop */
 int oracle_initialize(const ostc_config *c, const ostc_param *p, ostc_zone *zones, int n_zones,
                       const ostc_bc_face *f, int n_faces);

@@ -90,9 +90,26 @@ void fill_matrix(M &m, const T *src, int r, int c) {
 
 size_t plane(int mx, int my, int mz, int g) { return (size_t)(mx + 2 * g) * (my + 2 * g) * (mz + 2 * g); }
 
+// the reference's per-cell launch shape: {8, 8, 4}, or {16, 16, 1} for 2-D
+// problems (RK.cuh:25-30, SteadySim.cuh:27-31)
+dim3 tpb_for(int mz) { return mz == 1 ? dim3{16, 16, 1} : dim3{8, 8, 4}; }
+
+// eliminate_k_gradient on every block of a 2-D problem (RK.cuh:147-153,
+// SteadySim.cuh:101-107, Driver.cu:54-60)
+template <bool with_cv>
+void eliminate_k(RefMulti &m) {
+  if (m.blk.empty() || m.blk[0]->mz != 1) return;
+  const dim3 tpb = tpb_for(1);
+  for (RefCtx *c : m.blk) {
+    const int ng_1 = 2 * c->ngg - 1;
+    dim3 BPG{(unsigned)((c->mx + ng_1) / tpb.x + 1), (unsigned)((c->my + ng_1) / tpb.y + 1), 1};
+    eliminate_k_gradient<with_cv><<<BPG, tpb>>>(c->d_zone, c->d_param);
+  }
+}
+
 void build_param(RefCtx &c, const ostc_param *p) {
   DParameter &d = c.h_param;
-  d.dim = 3;
+  d.dim = c.mz == 1 ? 2 : 3;  // DParameter.cu:9 from the mesh dimension (Mesh.cpp:612-614)
   d.n_var = p->n_var;
   d.n_scalar = p->n_scalar;
   d.n_scalar_transported = p->n_scalar;
@@ -281,7 +298,8 @@ void communicate(RefMulti &m) {
 template <MixtureModel mix, class Turb>
 void initialize(RefMulti &m) {
   // Driver::initialize_computation (Driver.cu:39-98) + RK3_bv pre-loop (RK.cuh:40-49)
-  dim3 tpb{8, 8, 4};
+  const dim3 tpb = tpb_for(m.blk[0]->mz);
+  eliminate_k<false>(m);
   for (RefCtx *c : m.blk) apply_bcs<mix, Turb, false>(*c);
   for (RefCtx *c : m.blk) {
     const int ng_1 = 2 * c->ngg - 1;
@@ -314,7 +332,7 @@ void initialize(RefMulti &m) {
 
 template <MixtureModel mix, class Turb>
 void rhs(RefCtx &c) {
-  dim3 tpb{8, 8, 4};
+  const dim3 tpb = tpb_for(c.mz);
   dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
   cudaMemset(c.h.dq.data(), 0, c.h.dq.size() * c.n_var * sizeof(real));
   compute_source<mix, Turb><<<bpg, tpb>>>(c.d_zone, c.d_param);
@@ -338,7 +356,7 @@ double block_dt(RefCtx &c) {  // one block of global_time_step (TimeAdvanceFunc.
 
 // one block of compute_residual (Residual.cuh:57-111): the summed squares
 void block_residual(RefCtx &c, double *r) {
-  dim3 tpb{8, 8, 4};
+  const dim3 tpb = tpb_for(c.mz);
   dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
   compute_square_of_dbv<<<bpg, tpb>>>(c.d_zone);
   constexpr integer TPB{128};
@@ -355,7 +373,7 @@ void block_residual(RefCtx &c, double *r) {
 template <MixtureModel mix, class Turb>
 int steps(RefMulti &m, int n, double *res_hist, double *dt_hist) {
   // the body of RK3_bv's while loop (RK.cuh:89-170), all blocks
-  dim3 tpb{8, 8, 4};
+  const dim3 tpb = tpb_for(m.blk[0]->mz);
   auto bpg = [&](RefCtx *c, int e) {
     return dim3{(unsigned)((c->mx + e) / tpb.x + 1), (unsigned)((c->my + e) / tpb.y + 1),
                 (unsigned)((c->mz + e) / tpb.z + 1)};
@@ -380,6 +398,7 @@ int steps(RefMulti &m, int n, double *res_hist, double *dt_hist) {
         apply_bcs<mix, Turb, true>(*c);
       }
       communicate<mix, Turb, true>(m);
+      eliminate_k<true>(m);
       for (RefCtx *c : m.blk) update_physical_properties<mix><<<bpg(c, 1), tpb>>>(c->d_zone, c->d_param);
     }
     if (res_hist) {
@@ -403,7 +422,7 @@ int steps(RefMulti &m, int n, double *res_hist, double *dt_hist) {
 // this block's wall faces
 template <MixtureModel mix, class Turb>
 void implicit_treatment_block(RefMulti &m, RefCtx &c) {
-  dim3 tpb{8, 8, 4};
+  const dim3 tpb = tpb_for(c.mz);
   dim3 bpg{(unsigned)((c.mx - 1) / tpb.x + 1), (unsigned)((c.my - 1) / tpb.y + 1), (unsigned)((c.mz - 1) / tpb.z + 1)};
   if (m.cfg.implicit_method == 0) {
     if constexpr (mix == MixtureModel::FR) {
@@ -438,7 +457,7 @@ void implicit_treatment_block(RefMulti &m, RefCtx &c) {
 template <MixtureModel mix, class Turb>
 int steady_steps(RefMulti &m, int n, double *res_hist) {
   // the loop body of steady_simulation (SteadySim.cuh:51-126), all blocks
-  dim3 tpb{8, 8, 4};
+  const dim3 tpb = tpb_for(m.blk[0]->mz);
   auto bpg = [&](RefCtx *c, int e) {
     return dim3{(unsigned)((c->mx + e) / tpb.x + 1), (unsigned)((c->my + e) / tpb.y + 1),
                 (unsigned)((c->mz + e) / tpb.z + 1)};
@@ -456,6 +475,7 @@ int steady_steps(RefMulti &m, int n, double *res_hist) {
       apply_bcs<mix, Turb, false>(*c);
     }
     communicate<mix, Turb, false>(m);
+    eliminate_k<false>(m);
     for (RefCtx *c : m.blk) update_physical_properties<mix><<<bpg(c, 1), tpb>>>(c->d_zone, c->d_param);
     if (res_hist) {
       double acc[4] = {0, 0, 0, 0};
