@@ -173,7 +173,9 @@ cudaError_t flux_launch(const ostc_ctx *ctx, const DevZone &z, int d, const Flux
                         cudaStream_t s) {
   const int inv = ctx->prm.inviscid_type;
   const int vis = ctx->prm.viscous_scheme != 0;
-  if (ctx->nt == 2) return launch_flux_nt<0, 2>(z, inv, d, ctx->tile[d], tab, accumulate, vis, part, s);
+  if (ctx->nt == 2)
+    return ctx->ns == 9 ? launch_flux_nt<9, 2>(z, inv, d, ctx->tile[d], tab, accumulate, vis, part, s)
+                        : launch_flux_nt<0, 2>(z, inv, d, ctx->tile[d], tab, accumulate, vis, part, s);
   return dispatch_ns(ctx->ns, [&](auto n) {
     return launch_flux_nt<decltype(n)::value, 0>(z, inv, d, ctx->tile[d], tab, accumulate, vis, part, s);
   });
@@ -261,16 +263,23 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
   if (!cfg || !p || !zones || n_zones <= 0 || (n_faces > 0 && !faces)) return OSTC_ERR_INVALID_ARG;
   const bool sst = p->turbulence != 0;
   if (sst) {
-    // k-omega SST (rans_model 2): air, RK3, primitive-variable reconstruction with AUSM+ or HLLC
+    // k-omega SST (rans_model 2): air or the 9-species mixtures (Driver<Air|Mixture|FR, SST>,
+    // main.cu:25-96), primitive-variable reconstruction with AUSM+ or HLLC (and AWENO for air)
     if (p->rans_model != 2) return OSTC_ERR_UNSUPPORTED;
-    if (p->mix_model != OSTC_MIX_AIR || cfg->chem_mode != 0) return OSTC_ERR_UNSUPPORTED;
+    if (cfg->chem_mode != 0) return OSTC_ERR_UNSUPPORTED;
+    if (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_MIXTURE && p->mix_model != OSTC_MIX_FR)
+      return OSTC_ERR_UNSUPPORTED;
+    if (p->mix_model != OSTC_MIX_AIR && p->n_spec != 9) return OSTC_ERR_UNSUPPORTED;
+    if (p->mix_model == OSTC_MIX_FR && (p->n_reac < 0 || p->n_reac > OSTC_MAX_REAC)) return OSTC_ERR_INVALID_ARG;
     if (p->turb_implicit != 0 && p->turb_implicit != 1) return OSTC_ERR_INVALID_ARG;
     // primitive-variable reconstruction with AUSM+ / HLLC, or AWENO (its Roe tag runs AUSM+, A1) with AUSM+ / HLLC
     const bool pv = p->inviscid_type == 0 && (p->inviscid_scheme == 3 || p->inviscid_scheme == 4);
     const bool aweno = p->inviscid_type == 1 && p->inviscid_scheme >= 2 && p->inviscid_scheme <= 4;
     if (!pv && !aweno) return OSTC_ERR_UNSUPPORTED;
     if (p->viscous_scheme == 0) return OSTC_ERR_UNSUPPORTED;
-    if (p->n_spec != 0 || p->n_scalar != 2 || p->n_var != 7 || p->i_turb_cv != 5) return OSTC_ERR_INVALID_ARG;
+    const int ns = p->mix_model == OSTC_MIX_AIR ? 0 : p->n_spec;
+    if (p->n_spec != ns || p->n_scalar != ns + 2 || p->n_var != 7 + ns || p->i_turb_cv != 5 + ns)
+      return OSTC_ERR_INVALID_ARG;
     if (p->compressibility_correction < 0 || p->compressibility_correction > 3) return OSTC_ERR_INVALID_ARG;
     if (!(p->Prt > 0)) return OSTC_ERR_INVALID_ARG;
   } else if (p->mix_model == OSTC_MIX_AIR) {

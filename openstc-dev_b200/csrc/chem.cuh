@@ -302,6 +302,45 @@ __device__ __forceinline__ void point_implicit_increment(double T, double p, con
   dT = t - T;
 }
 
+// compute_viscosity (Transport.cu:112-145): the mixture's Wilke viscosity at
+// temperature T for mass fractions Y, the transport kernel's formula below
+// with the viscosity alone (the SST wall and initial turbulent viscosity)
+template <int NS>
+__device__ __forceinline__ double mixture_viscosity(double T, const double *Y) {
+  double mw_inv = 0;
+#pragma unroll
+  for (int l = 0; l < NS; ++l) mw_inv += Y[l] * c_p.imw[l];
+  const double mw_total = 1.0 / mw_inv;
+  double X[NS], vis[NS], svis[NS], rsvis[NS];
+  const double sqT = sqrt(T);
+  const double Tm145 = exp(-0.145 * log(T));
+#pragma unroll
+  for (int l = 0; l < NS; ++l) {
+    X[l] = Y[l] * mw_total * c_p.imw[l];
+    const double t_dl = T * c_p.LJ_inv[l] + 0.5;
+    const double ci = 1.147 * (Tm145 * c_p.LJm145[l]) + 1.0 / (t_dl * t_dl);
+    vis[l] = c_p.vis_coeff[l] * sqT / ci;
+    svis[l] = sqrt(vis[l]);
+    rsvis[l] = 1.0 / svis[l];
+  }
+  double viscosity = 0;
+#pragma unroll
+  for (int m = 0; m < NS; ++m) {
+    double vt = 0;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      double pf = 1.0;
+      if (m != n) {
+        const double num = 1 + svis[m] * rsvis[n] * c_p.WjWi4[m][n];
+        pf = num * num * c_p.sqWW8[m][n];
+      }
+      vt += pf * X[n];
+    }
+    viscosity += vis[m] * X[m] / vt;
+  }
+  return viscosity;
+}
+
 // mixture transport at one state (Transport.cu:40-109)
 template <int NS>
 __device__ __forceinline__ void mixture_transport(double T, double mw_total, const double *Y, const double *cp,

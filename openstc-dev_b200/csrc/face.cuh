@@ -704,6 +704,7 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
       const double *ys = z.sv + l * z.isz;
       yk[l] = 0.5 * (ld(ys + g0) + ld(ys + g1));
       diff[l] = 0.5 * (ld(z.rhoD + l * z.isz + g0) + ld(z.rhoD + l * z.isz + g1));
+      if constexpr (NT > 0) diff[l] += mut / c_p.Sct;  // turbulent diffusivity (ViscousScheme.cuh:122-125)
       double dy[3];
       der(ys, dy);
       const double y_x = dy[0] * mm[0] + dy[1] * mm[3] + dy[2] * mm[6];

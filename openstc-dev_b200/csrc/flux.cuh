@@ -256,11 +256,13 @@ template <int NS, int NT>
 cudaError_t launch_flux_nt(const DevZone &z, int inv, int dir, const TileShape &t, const FluxTable *tab, int accumulate,
                            int viscous, int part, cudaStream_t s) {
   if constexpr (NT > 0) {
-    if (inv == 1) {  // AWENO with the scalars reconstructed component-wise
-      switch (dir) {
-        case 0: return launch_flux_t<NS, 1, 0, NT>(z, t, tab, accumulate, viscous, part, s);
-        case 1: return launch_flux_t<NS, 1, 1, NT>(z, t, tab, accumulate, viscous, part, s);
-        default: return launch_flux_t<NS, 1, 2, NT>(z, t, tab, accumulate, viscous, part, s);
+    if constexpr (NS == 0) {
+      if (inv == 1) {  // AWENO (air) with the scalars reconstructed component-wise
+        switch (dir) {
+          case 0: return launch_flux_t<NS, 1, 0, NT>(z, t, tab, accumulate, viscous, part, s);
+          case 1: return launch_flux_t<NS, 1, 1, NT>(z, t, tab, accumulate, viscous, part, s);
+          default: return launch_flux_t<NS, 1, 2, NT>(z, t, tab, accumulate, viscous, part, s);
+        }
       }
     }
     if (inv != 0) return cudaErrorInvalidValue;  // no Roe with turbulence scalars

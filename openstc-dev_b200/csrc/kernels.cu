@@ -1,5 +1,5 @@
 // kernels.cu — sm_100a kernels of the RHS / RK3 stage (the flux kernels,
-// flux_dir in flux.cuh, are built in flux0.cu, flux9.cu and flux0t.cu).
+// flux_dir in flux.cuh, are built in flux0.cu, flux9.cu, flux0t.cu and flux9t.cu).
 //
 //  source_kernel<NS>      finite-rate chemistry or SST source, starts dq (SourceTerm.cuh:11-37)
 //  update_rk_kernel<NS>   SSPRK3 stage update, cv -> bv/sv, T and p (RK.cuh:197-253)
@@ -43,21 +43,19 @@ __device__ __forceinline__ void source_cells(const DevZone &z, const int bx, con
   double *dq = z.dq + qidx(z, i, j, k);
 #pragma unroll
   for (int l = 0; l < 5; ++l) dq[l * z.qsz] = 0;
-  if constexpr (NS == 0) {
-    if (c_p.sst) {  // SST::compute_source_and_mut and the turbulent conductivity (SourceTerm.cuh:19-27)
-      double mut, sk, sw, jk, jw;
-      sst::source_point(z, g, mut, sk, sw, jk, jw);
-      z.mut[g] = mut;
-      if (c_p.turb_implicit == 1 && z.tsj) {  // SST.cu:243-246
-        const int n = nidx(z, i, j, k);
-        z.tsj[n] = jk;
-        z.tsj[z.nsz + n] = jw;
-      }
-      constexpr double cpa = gamma_air * R_u / mw_air / (gamma_air - 1);
-      z.ttc[g] = mut * cpa / c_p.Prt;
-      dq[5 * z.qsz] = sk;
-      dq[6 * z.qsz] = sw;
+  if (c_p.sst) {  // SST::compute_source_and_mut and the turbulent conductivity (SourceTerm.cuh:19-27)
+    double mut, sk, sw, jk, jw;
+    sst::source_point<NS>(z, g, mut, sk, sw, jk, jw);
+    z.mut[g] = mut;
+    if (c_p.turb_implicit == 1 && z.tsj) {  // SST.cu:243-246
+      const int n = nidx(z, i, j, k);
+      z.tsj[n] = jk;
+      z.tsj[z.nsz + n] = jw;
     }
+    constexpr double cpa = gamma_air * R_u / mw_air / (gamma_air - 1);
+    z.ttc[g] = mut * (NS > 0 ? z.cp[g] : cpa) / c_p.Prt;  // the mixture's cp (SourceTerm.cuh:21-23)
+    dq[(5 + NS) * z.qsz] = sk;
+    dq[(6 + NS) * z.qsz] = sw;
   }
   if constexpr (NS > 0) {
     double Y[NS], om[NS];
@@ -279,18 +277,31 @@ __global__ void __launch_bounds__(256) properties_kernel(DevZone z) {
 }
 
 // initialize_mut (FieldOperation.cuh:175-195) over [-1, m]: the SST turbulent
-// viscosity from the initial field, air (Sutherland viscosity)
+// viscosity from the initial field, with Sutherland's viscosity for air or
+// the mixture's Wilke viscosity (compute_viscosity)
+template <int NS>
 __device__ __forceinline__ void init_mut_cells(const DevZone &z, const int bx, const int by, const int bz) {
   const int i = bx * blockDim.x + threadIdx.x - 1;
   const int j = by * blockDim.y + threadIdx.y - 1;
   const int k = bz - 1;
   if (i > z.mx || j > z.my) return;
   const int g = gidx(z, i, j, k);
-  z.mut[g] = sst::mut_point(z, g, sutherland(z.bv[5 * z.sz + g]));
+  const double T = z.bv[5 * z.sz + g];
+  double mul;
+  if constexpr (NS > 0) {
+    double Y[NS];
+#pragma unroll
+    for (int l = 0; l < NS; ++l) Y[l] = z.sv[l * z.sz + g];
+    mul = mixture_viscosity<NS>(T, Y);
+  } else {
+    mul = sutherland(T);
+  }
+  z.mut[g] = sst::mut_point<NS>(z, g, mul);
 }
 
+template <int NS>
 __global__ void __launch_bounds__(256) init_mut_kernel(DevZone z) {
-  init_mut_cells(z, blockIdx.x, blockIdx.y, blockIdx.z);
+  init_mut_cells<NS>(z, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 template <int NS>
@@ -557,13 +568,20 @@ __global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
   z.bv[4 * z.sz + g] = p;
   z.bv[5 * z.sz + g] = t_wall;
   z.vel[g] = 0;
-  if constexpr (NS == 0) {
-    if (c_p.sst) {
-      const double mu_wall = sutherland(t_wall);
-      const double dy = z.wall[gin];
-      z.sv[g] = 0;
-      z.sv[z.sz + g] = dy > 1e-25 ? 60 * mu_wall / (rho_wall * sst::beta_1 * dy * dy) : z.sv[z.sz + gin];
+  if (c_p.sst) {  // BoundCond.cuh:471-485: mu at the wall temperature (the mixture's at the wall species)
+    double mu_wall;
+    if constexpr (NS > 0) {
+      double Y[NS];
+#pragma unroll
+      for (int l = 0; l < NS; ++l) Y[l] = z.sv[l * z.sz + g];
+      mu_wall = mixture_viscosity<NS>(t_wall, Y);
+    } else {
+      mu_wall = sutherland(t_wall);
     }
+    const double dy = z.wall[gin];
+    z.sv[NS * z.sz + g] = 0;
+    z.sv[(NS + 1) * z.sz + g] =
+        dy > 1e-25 ? 60 * mu_wall / (rho_wall * sst::beta_1 * dy * dy) : z.sv[(NS + 1) * z.sz + gin];
   }
   if (with_cv) cv_from_bv_point<NS>(z, g);
   for (int gg = 1; gg <= z.ngg; ++gg) {
@@ -590,12 +608,10 @@ __global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
     z.bv[3 * z.sz + go] = -w_i;
     z.bv[4 * z.sz + go] = p_i;
     z.bv[5 * z.sz + go] = t_g;
-    if constexpr (NS == 0) {
-      if (c_p.sst) {
-        z.sv[go] = 0;
-        z.sv[z.sz + go] = z.sv[z.sz + g];
-        z.mut[go] = 0;
-      }
+    if (c_p.sst) {
+      z.sv[NS * z.sz + go] = 0;
+      z.sv[(NS + 1) * z.sz + go] = z.sv[(NS + 1) * z.sz + g];
+      z.mut[go] = 0;
     }
     if (with_cv) cv_from_bv_point<NS>(z, go);
   }
@@ -690,8 +706,7 @@ __global__ void bc_farfield_kernel(DevZone z, BcFace b) {
         u = b.u + (Un - u_inf) * nx;
         v = b.v + (Un - u_inf) * ny;
         w = b.w + (Un - u_inf) * nz;
-#pragma unroll
-        for (int l = 0; l < NS; ++l) sv_b[l] = b.sv[l];
+        for (int l = 0; l < c_p.n_scalar && l < NS + 2; ++l) sv_b[l] = b.sv[l];  // species, k, omega
         mw = b.mw;
       } else {
         u = u_b + (Un - u_face) * nx;
@@ -934,8 +949,9 @@ struct DtOp {
 struct StoreLastOp {
   __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { store_last_cells(z, bx, by, bz); }
 };
+template <int NS>
 struct InitMutOp {
-  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { init_mut_cells(z, bx, by, bz); }
+  __device__ void operator()(const DevZone &z, int bx, int by, int bz) const { init_mut_cells<NS>(z, bx, by, bz); }
 };
 
 }  // namespace ostc
@@ -976,6 +992,7 @@ cudaError_t upload_zones(const DevZone *z, int n, cudaStream_t s) {
   if (e == cudaSuccess) e = upload_zones_flux0(z, n, s);
   if (e == cudaSuccess) e = upload_zones_flux9(z, n, s);
   if (e == cudaSuccess) e = upload_zones_flux0t(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_flux9t(z, n, s);
   return e;
 }
 
@@ -990,7 +1007,7 @@ cudaError_t launch_cells_table(CellOp op, const CellTable &tab, const CellArgs &
     case CellOp::Velocity: return launch_table(tab, VelocityOp{}, s);
     case CellOp::Dt: return launch_table(tab, DtOp<NS>{a.dt_bits}, s);
     case CellOp::StoreLast: return launch_table(tab, StoreLastOp{}, s);
-    case CellOp::InitMut: return launch_table(tab, InitMutOp{}, s);
+    case CellOp::InitMut: return launch_table(tab, InitMutOp<NS>{}, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1012,7 +1029,7 @@ cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStr
       properties_kernel<NS><<<plane_grid(z.mx + 2, z.my + 2, z.mz + 2, blk), blk, 0, s>>>(z);
       break;
     case CellOp::InitMut:
-      init_mut_kernel<<<plane_grid(z.mx + 2, z.my + 2, z.mz + 2, blk), blk, 0, s>>>(z);
+      init_mut_kernel<NS><<<plane_grid(z.mx + 2, z.my + 2, z.mz + 2, blk), blk, 0, s>>>(z);
       break;
     case CellOp::CvFromBv:
       cv_from_bv_kernel<NS>
@@ -1207,6 +1224,7 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   if (e == cudaSuccess) e = upload_param_flux0(p, s);
   if (e == cudaSuccess) e = upload_param_flux9(p, s);
   if (e == cudaSuccess) e = upload_param_flux0t(p, s);
+  if (e == cudaSuccess) e = upload_param_flux9t(p, s);
   return e;
 }
 

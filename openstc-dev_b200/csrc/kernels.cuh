@@ -90,7 +90,7 @@ struct SteadyArgs {
 // else tab[0] (shape t) and tab[1] (viscous shape) hold the tiles of every
 // zone of the uploaded table and z is not used
 // NT: turbulence scalars after the NS species (0, or 2 for SST with NS = 0);
-// built in flux0.cu (NS 0, NT 0), flux9.cu (9, 0) and flux0t.cu (0, 2)
+// built in flux0.cu (NS 0, NT 0), flux9.cu (9, 0), flux0t.cu (0, 2) and flux9t.cu (9, 2)
 template <int NS, int NT>
 cudaError_t launch_flux_nt(const DevZone &z, int inv, int dir, const TileShape &t, const FluxTable *tab,
                            int accumulate, int viscous, int part, cudaStream_t s);
@@ -108,6 +108,7 @@ cudaError_t upload_zones(const DevZone *z, int n, cudaStream_t s);
 cudaError_t upload_zones_flux0(const DevZone *z, int n, cudaStream_t s);   // flux0.cu
 cudaError_t upload_zones_flux9(const DevZone *z, int n, cudaStream_t s);   // flux9.cu
 cudaError_t upload_zones_flux0t(const DevZone *z, int n, cudaStream_t s);  // flux0t.cu
+cudaError_t upload_zones_flux9t(const DevZone *z, int n, cudaStream_t s);  // flux9t.cu
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s);
 template <int NS>
@@ -134,6 +135,7 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s);
 cudaError_t upload_param_flux0(const DevParam &p, cudaStream_t s);   // flux0.cu
 cudaError_t upload_param_flux9(const DevParam &p, cudaStream_t s);   // flux9.cu
 cudaError_t upload_param_flux0t(const DevParam &p, cudaStream_t s);  // flux0t.cu
+cudaError_t upload_param_flux9t(const DevParam &p, cudaStream_t s);  // flux9t.cu
 // whether a mechanism has the structure of the generated mech_h2air9.cuh
 bool mechanism_is_h2air9(const int *reac_type, const int *stoi_f, const int *stoi_b, const int *reac_order, int nr,
                          int ns);

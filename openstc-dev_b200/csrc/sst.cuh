@@ -2,8 +2,9 @@
 // omega source terms with the optional compressibility corrections
 // (SST.cu:8-247, SST.cuh:12-45), the turbulent parts of the viscous face
 // flux (ViscousScheme.cuh:82-95, 111-113, 200-251) and of the wall boundary
-// (BoundCond.cuh:471-484, 536-541). Air only (n_spec = 0): sv holds k and
-// omega in its planes 0 and 1, dq and cv in their planes 5 and 6.
+// (BoundCond.cuh:471-484, 536-541). NS species before them: sv holds k and
+// omega in its planes NS and NS + 1, dq and cv in their planes 5 + NS and
+// 6 + NS (i_turb_cv, DParameter.cu).
 #pragma once
 #include "common.cuh"
 
@@ -47,6 +48,7 @@ __device__ __forceinline__ Grad diffs(const DevZone &z, const double *base, int 
 }
 
 // SST::compute_mut (SST.cu:44-97): the initial turbulent viscosity of a point
+template <int NS>
 __device__ __forceinline__ double mut_point(const DevZone &z, int g, double mul) {
   double m[9];
 #pragma unroll
@@ -56,9 +58,9 @@ __device__ __forceinline__ double mut_point(const DevZone &z, int g, double mul)
   const double v_x = gv.c(m, 0), v_z = gv.c(m, 2);
   const double w_x = gw.c(m, 0), w_y = gw.c(m, 1);
   const double density = z.bv[g];
-  const double tke = z.sv[g];
+  const double tke = z.sv[NS * z.sz + g];
   const double rhoK = density * tke;
-  const double omega = z.sv[z.sz + g];
+  const double omega = z.sv[(NS + 1) * z.sz + g];
   const double vorticity = sqrt((v_x - u_y) * (v_x - u_y) + (w_x - u_z) * (w_x - u_z) + (w_y - v_z) * (w_y - v_z));
   double f2 = 1;
   const double dy = z.wall[g];
@@ -77,6 +79,7 @@ __device__ __forceinline__ double mut_point(const DevZone &z, int g, double mul)
 // SST::compute_source_and_mut (SST.cu:99-247) at interior point g: mut, the k
 // and omega sources (zero when mut <= 1e-25) and the diagonal source Jacobian
 // (-2 beta* omega, -2 beta omega) the steady path's implicit treatment uses
+template <int NS>
 __device__ __forceinline__ void source_point(const DevZone &z, int g, double &mut_out, double &src_k,
                                              double &src_w, double &jac_k, double &jac_w) {
   double m[9];
@@ -87,12 +90,12 @@ __device__ __forceinline__ void source_point(const DevZone &z, int g, double &mu
   const double v_x = gv.c(m, 0), v_y = gv.c(m, 1), v_z = gv.c(m, 2);
   const double w_x = gw.c(m, 0), w_y = gw.c(m, 1), w_z = gw.c(m, 2);
   const double density = z.bv[g];
-  const double omega = z.sv[z.sz + g];
-  const Grad gk = diffs(z, z.sv, g), go = diffs(z, z.sv + z.sz, g);
+  const double omega = z.sv[(NS + 1) * z.sz + g];
+  const Grad gk = diffs(z, z.sv + NS * z.sz, g), go = diffs(z, z.sv + (NS + 1) * z.sz, g);
   const double k_x = gk.c(m, 0), k_y = gk.c(m, 1), k_z = gk.c(m, 2);
   const double omega_x = go.c(m, 0), omega_y = go.c(m, 1), omega_z = go.c(m, 2);
   const double inter_var = 2 * density * sigma_omega2 / omega * (k_x * omega_x + k_y * omega_y + k_z * omega_z);
-  const double tke = z.sv[g];
+  const double tke = z.sv[NS * z.sz + g];
   const double rhoK = density * tke;
   const double vorticity = sqrt((v_x - u_y) * (v_x - u_y) + (w_x - u_z) * (w_x - u_z) + (w_y - v_z) * (w_y - v_z));
   double f1 = 1, f2 = 1;
@@ -114,13 +117,14 @@ __device__ __forceinline__ void source_point(const DevZone &z, int g, double &mu
   mut_out = mut;
   double beta = beta_2 + delta_beta * f1;
   double betaStar = beta_star;
-  if (c_p.comp_corr) {
-    const double Mt = sqrt(2 * tke / (gamma_air * z.bv[4 * z.sz + g] / density));
+  if (c_p.comp_corr) {  // the mixture's gamma when there are species (SST.cu:195-199)
+    const double gam = NS > 0 ? z.gam[g] : gamma_air;
+    const double Mt = sqrt(2 * tke / (gam * z.bv[4 * z.sz + g] / density));
     double corr;
     switch (c_p.comp_corr) {
       case 1: corr = wilcox(Mt); break;
       case 2: corr = beta_star * Mt * Mt; break;
-      default: corr = zeman(Mt, gamma_air + 1.0); break;
+      default: corr = zeman(Mt, gam + 1.0); break;
     }
     betaStar += corr;
     beta -= corr;

@@ -144,11 +144,11 @@ __global__ void __launch_bounds__(256) update_bv_kernel(DevZone z) {
 // ---------------------------------------------------------------------------
 // DPLUR
 // ---------------------------------------------------------------------------
-// NVX: the largest variable count of the build (air may carry the two SST
-// scalars); the variables beyond c_p.n_var are not touched
+// NVX: the largest variable count of the build (the species may be followed
+// by the two SST scalars); the variables beyond c_p.n_var are not touched
 template <int NS>
 constexpr int nvx() {
-  return 5 + NS + (NS == 0 ? 2 : 0);
+  return 5 + NS + 2;
 }
 
 // SST::implicit_treat_for_SST under the explicit steady path (SST.cu:8-22)
@@ -160,8 +160,9 @@ __global__ void __launch_bounds__(256) turb_implicit_kernel(DevZone z) {
   const int n = nidx(z, i, j, k);
   double *dq = z.dq + qidx(z, i, j, k);
   const double dt = z.dt_local[n];
-  dq[5 * z.qsz] /= 1 - dt * z.tsj[n];
-  dq[6 * z.qsz] /= 1 - dt * z.tsj[z.nsz + n];
+  const int it = 5 + c_p.n_spec;  // i_turb_cv
+  dq[it * z.qsz] /= 1 - dt * z.tsj[n];
+  dq[(it + 1) * z.qsz] /= 1 - dt * z.tsj[z.nsz + n];
 }
 
 template <int NS>
@@ -218,18 +219,16 @@ __global__ void __launch_bounds__(128) dplur_dq0_kernel(DevZone z, SteadyArgs a)
       }
     } else {
 #pragma unroll
-      for (int l = 5; l < NV; ++l) d[l] /= diag;
+      for (int l = 5; l < 5 + NS; ++l) d[l] /= diag;
     }
   }
-  if constexpr (NS == 0) {
-    if (c_p.sst) {  // DPLUR.cuh:72-84 with SST::implicit_treat_for_dq0 (SST.cu:249-258)
-      if (c_p.turb_implicit == 1) {
-        d[5] /= diag - dt * z.tsj[n];
-        d[6] /= diag - dt * z.tsj[z.nsz + n];
-      } else {
-        d[5] /= diag;
-        d[6] /= diag;
-      }
+  if (c_p.sst) {  // DPLUR.cuh:72-84 with SST::implicit_treat_for_dq0 (SST.cu:249-258), rows i_turb_cv, +1
+    if (c_p.turb_implicit == 1) {
+      d[5 + NS] /= diag - dt * z.tsj[n];
+      d[6 + NS] /= diag - dt * z.tsj[z.nsz + n];
+    } else {
+      d[5 + NS] /= diag;
+      d[6 + NS] /= diag;
     }
   }
 #pragma unroll
@@ -361,16 +360,15 @@ __global__ void __launch_bounds__(128) dplur_sweep_kernel(DevZone z, SteadyArgs 
         out[5 + l] = a.dq0[q + (5 + l) * z.qsz] + dt * tot[5 + l] / a.da[(long long)l * N + n];
     } else {
 #pragma unroll
-      for (int l = 5; l < NV; ++l) out[l] = a.dq0[q + l * z.qsz] + dt * tot[l] / diag;
+      for (int l = 5; l < 5 + NS; ++l) out[l] = a.dq0[q + l * z.qsz] + dt * tot[l] / diag;
     }
   }
-  if constexpr (NS == 0) {
-    if (c_p.sst) {  // DPLUR.cuh:262-276 with SST::implicit_treat_for_dqk (SST.cu:260-273)
-      const double d5 = c_p.turb_implicit == 1 ? diag - dt * z.tsj[n] : diag;
-      const double d6 = c_p.turb_implicit == 1 ? diag - dt * z.tsj[N + n] : diag;
-      out[5] = a.dq0[q + 5 * z.qsz] + dt * tot[5] / d5;
-      out[6] = a.dq0[q + 6 * z.qsz] + dt * tot[6] / d6;
-    }
+  if (c_p.sst) {  // DPLUR.cuh:262-276 with SST::implicit_treat_for_dqk (SST.cu:260-273), rows i_turb_cv, +1
+    constexpr int T0 = 5 + NS, T1 = 6 + NS;
+    const double d5 = c_p.turb_implicit == 1 ? diag - dt * z.tsj[n] : diag;
+    const double d6 = c_p.turb_implicit == 1 ? diag - dt * z.tsj[N + n] : diag;
+    out[T0] = a.dq0[q + T0 * z.qsz] + dt * tot[T0] / d5;
+    out[T1] = a.dq0[q + T1 * z.qsz] + dt * tot[T1] / d6;
   }
   if (a.final_div) {
 #pragma unroll

@@ -1199,7 +1199,7 @@ def mixture_state(mech: Mechanism, Y, T, p, mach):
 
 
 def case_mixing_layer(mx=256, my=256, mz=256, dx=1e-4, seed=2024, steps=200, full_host=False, mech=None,
-                      cfl=0.4) -> Case:
+                      cfl=0.4, rans_model=0, wall=False, compressibility_correction=0) -> Case:
     """The reacting mixing layer: upper stream (y > 0) air (O2/N2 mass
     0.233/0.767) at 1500 K, Mach 2; lower stream H2/N2 (mole 0.3/0.7) at
     300 K, Mach 1.2; p = 1 atm; profiles blended by 0.5(1 + tanh(y / 8dy));
@@ -1208,15 +1208,19 @@ def case_mixing_layer(mx=256, my=256, mz=256, dx=1e-4, seed=2024, steps=200, ful
     19-reaction H2-air mechanism, MUSCL (minmod) + AUSM+, laminar viscous
     flux, point-implicit chemistry tag (explicit under RK3, quirk A8), RK3 at
     CFL 0.4. Uniform Cartesian grid dx = dy = dz. Extrapolation (outflow)
-    faces in x and y, periodic in z."""
+    faces in x and y, periodic in z. rans_model=2: k-omega SST (Driver<FR,
+    SST>) with k = 1.5 (0.01 U)^2 and omega = rho k / (10 * 1.8e-5) from
+    the local stream speed U and density, the wall distance to the j = 0
+    plane; wall=True makes j = 0 an isothermal 300 K wall (the fuel side)."""
     import chemdata
 
     mech = mech or chemdata.h2_air_9sp()
     s = Scheme(mix_model=MIX_FR, inviscid_scheme=3, reconstruction=2, limiter=0, viscous_order=2, chemSrcMethod=1,
-               cfl=cfl)
+               cfl=cfl, rans_model=rans_model, compressibility_correction=compressibility_correction)
     ng = s.ngg
     ns = mech.n_spec
-    b = HostBlock.allocate(mx, my, mz, ng, 5 + ns, ns, full=full_host)
+    nt = 2 if rans_model == 2 else 0
+    b = HostBlock.allocate(mx, my, mz, ng, 5 + ns + nt, ns, full=full_host, n_turb=nt)
     x, y, z = grid_coordinates(mx, my, mz, ng + 1, dx, warp=0.0)
     fill_metric(b, x, y, z)
     names = mech.names
@@ -1249,12 +1253,19 @@ def case_mixing_layer(mx=256, my=256, mz=256, dx=1e-4, seed=2024, steps=200, ful
     bv[3] = 0.01 * U * rng.uniform(-1, 1, P) if mz > 1 else 0.0  # a 2-D layer (mz == 1) has no w
     bv[4] = p0
     bv[5] = T
+    if nt:
+        tke = 1.5 * (0.01 * U) ** 2
+        sv[ns] = tke
+        sv[ns + 1] = bv[0] * tke / (10 * 1.8e-5)
+        xs, ys, zs = x[1:-1, 1:-1, 1:-1], y[1:-1, 1:-1, 1:-1], z[1:-1, 1:-1, 1:-1]
+        b.arrays["wall_distance"][...] = wall_distance_j0(None, xs, ys, zs, 0, 0, 0, mx, my, mz, ng)
     ext = (mx, my, mz)
     faces = [bc_face(0, BC_OUTFLOW, 0, -1, ext, ng), bc_face(0, BC_OUTFLOW, 0, 1, ext, ng),
+             bc_face(0, BC_WALL, 1, -1, ext, ng, dict(wall_isothermal=1, wall_temperature=300.0)) if wall else
              bc_face(0, BC_OUTFLOW, 1, -1, ext, ng), bc_face(0, BC_OUTFLOW, 1, 1, ext, ng)]
     if mz > 1:
         faces += [bc_face(0, BC_PERIODIC, 2, -1, ext, ng), bc_face(0, BC_PERIODIC, 2, 1, ext, ng)]
-    return Case("mixing_layer_h2air_%dx%dx%d" % (mx, my, mz), s, mech, [b], faces, steps)
+    return Case("mixing_layer_h2air%s_%dx%dx%d" % ("_sst" if nt else "", mx, my, mz), s, mech, [b], faces, steps)
 
 
 def case_premixed_box(mx=16, my=14, mz=8, dx=2e-3, T0=1400.0, seed=7, mech=None, chem_src_method=1,

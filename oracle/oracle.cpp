@@ -186,6 +186,37 @@ double omega_d(double t_red) {  // Transport.cu:142-145
   return 1.0 / std::pow(t_red, 0.145) + 1.0 / ((t_red + 0.5) * (t_red + 0.5));
 }
 
+// compute_viscosity (Transport.cu:112-145): the Wilke viscosity of a mixture
+// at temperature T (the SST wall and the initial turbulent viscosity)
+double mixture_viscosity(const ostc_param *P, double temperature, const double *Y) {
+  const int ns = P->n_spec;
+  const double *mw = P->mw;
+  double mw_total = 0;
+  for (int l = 0; l < ns; ++l) mw_total += Y[l] / mw[l];
+  mw_total = 1 / mw_total;
+  double X[MAXS], vis[MAXS];
+  for (int l = 0; l < ns; ++l) {
+    X[l] = Y[l] * mw_total / mw[l];
+    const double t_dl = temperature * P->LJ_potent_inv[l];
+    const double ci = 1.147 * std::pow(t_dl, -0.145) + std::pow(t_dl + 0.5, -2);
+    vis[l] = P->vis_coeff[l] * std::sqrt(temperature) / ci;
+  }
+  double viscosity = 0;
+  for (int m = 0; m < ns; ++m) {
+    double vis_temp = 0;
+    for (int n = 0; n < ns; ++n) {
+      double pf = 1.0;
+      if (m != n) {
+        const double num = 1 + std::sqrt(vis[m] / vis[n]) * P->WjDivWi_to_One4th[m * ns + n];
+        pf = num * num * P->sqrt_WiDivWjPl1Mul8[m * ns + n];
+      }
+      vis_temp += pf * X[n];
+    }
+    viscosity += vis[m] * X[m] / vis_temp;
+  }
+  return viscosity;
+}
+
 // compute_transport_property (Transport.cu:40-109): mu, kappa, rho*D_k
 void transport(const ostc_param *P, double temperature, double mw_total, const double *Y,
                const double *cp, double rho, double pressure, double *mu_out, double *kappa_out,
@@ -1004,12 +1035,13 @@ double grad(const Z &Zn, const View &V, int l, const double *m, int c, int i, in
                 m[6 + c] * (V(i, j, k + 1, l) - V(i, j, k - 1, l)));
 }
 
-double compute_mut(const Z &Zn, int i, int j, int k, double mul) {  // SST.cu:44-97
+// it: the plane of k in sv (n_spec; omega follows)
+double compute_mut(const Z &Zn, int it, int i, int j, int k, double mul) {  // SST.cu:44-97
   const double *m = Zn.metric.at(i, j, k);
   const double u_y = grad(Zn, Zn.bv, 1, m, 1, i, j, k), u_z = grad(Zn, Zn.bv, 1, m, 2, i, j, k);
   const double v_x = grad(Zn, Zn.bv, 2, m, 0, i, j, k), v_z = grad(Zn, Zn.bv, 2, m, 2, i, j, k);
   const double w_x = grad(Zn, Zn.bv, 3, m, 0, i, j, k), w_y = grad(Zn, Zn.bv, 3, m, 1, i, j, k);
-  const double density = Zn.bv(i, j, k, 0), tke = Zn.sv(i, j, k, 0), omega = Zn.sv(i, j, k, 1);
+  const double density = Zn.bv(i, j, k, 0), tke = Zn.sv(i, j, k, it), omega = Zn.sv(i, j, k, it + 1);
   const double rhoK = density * tke;
   const double vorticity =
       std::sqrt((v_x - u_y) * (v_x - u_y) + (w_x - u_z) * (w_x - u_z) + (w_y - v_z) * (w_y - v_z));
@@ -1043,6 +1075,7 @@ double zeman(double Mt, double gammaP1) {  // SST.cu:33-42
 
 // compute_source_and_mut (SST.cu:99-247) + the turbulent conductivity (SourceTerm.cuh:19-27)
 void source_and_mut(const ostc_param *P, Z &Zn, int i, int j, int k) {
+  const int it = P->n_spec;  // k, omega planes it, it + 1; dq rows 5 + it, 6 + it (i_turb_cv)
   const double *m = Zn.metric.at(i, j, k);
   const View &bv = Zn.bv, &sv = Zn.sv;
   const double u_x = grad(Zn, bv, 1, m, 0, i, j, k), u_y = grad(Zn, bv, 1, m, 1, i, j, k);
@@ -1052,13 +1085,13 @@ void source_and_mut(const ostc_param *P, Z &Zn, int i, int j, int k) {
   const double w_x = grad(Zn, bv, 3, m, 0, i, j, k), w_y = grad(Zn, bv, 3, m, 1, i, j, k);
   const double w_z = grad(Zn, bv, 3, m, 2, i, j, k);
   const double density = bv(i, j, k, 0);
-  const double omega = sv(i, j, k, 1);
-  const double k_x = grad(Zn, sv, 0, m, 0, i, j, k), k_y = grad(Zn, sv, 0, m, 1, i, j, k);
-  const double k_z = grad(Zn, sv, 0, m, 2, i, j, k);
-  const double omega_x = grad(Zn, sv, 1, m, 0, i, j, k), omega_y = grad(Zn, sv, 1, m, 1, i, j, k);
-  const double omega_z = grad(Zn, sv, 1, m, 2, i, j, k);
+  const double omega = sv(i, j, k, it + 1);
+  const double k_x = grad(Zn, sv, it, m, 0, i, j, k), k_y = grad(Zn, sv, it, m, 1, i, j, k);
+  const double k_z = grad(Zn, sv, it, m, 2, i, j, k);
+  const double omega_x = grad(Zn, sv, it + 1, m, 0, i, j, k), omega_y = grad(Zn, sv, it + 1, m, 1, i, j, k);
+  const double omega_z = grad(Zn, sv, it + 1, m, 2, i, j, k);
   const double inter_var = 2 * density * sigma_omega2 / omega * (k_x * omega_x + k_y * omega_y + k_z * omega_z);
-  const double tke = sv(i, j, k, 0);
+  const double tke = sv(i, j, k, it);
   const double rhoK = density * tke;
   const double vorticity =
       std::sqrt((v_x - u_y) * (v_x - u_y) + (w_x - u_z) * (w_x - u_z) + (w_y - v_z) * (w_y - v_z));
@@ -1082,12 +1115,13 @@ void source_and_mut(const ostc_param *P, Z &Zn, int i, int j, int k) {
   double beta = beta_2 + delta_beta * f1;
   double betaStar = beta_star;
   if (const int correction = P->compressibility_correction) {
-    const double Mt = std::sqrt(2 * tke / (gamma_air * bv(i, j, k, 4) / density));
+    const double gam = it > 0 ? Zn.gam(i, j, k) : gamma_air;  // SST.cu:195-199
+    const double Mt = std::sqrt(2 * tke / (gam * bv(i, j, k, 4) / density));
     double c;
     switch (correction) {
       case 1: c = wilcox(Mt); break;
       case 2: c = beta_star * Mt * Mt; break;
-      default: c = zeman(Mt, gamma_air + 1.0); break;
+      default: c = zeman(Mt, gam + 1.0); break;
     }
     betaStar += c;
     beta -= c;
@@ -1102,18 +1136,18 @@ void source_and_mut(const ostc_param *P, Z &Zn, int i, int j, int k) {
     if (prod_k > 10 * prod_k2) prod_k = prod_k2;
     const double diss_k = betaStar * rhoK * omega;
     const double jac = Zn.jac(i, j, k);
-    Zn.dq(i, j, k, 5) += jac * (prod_k - diss_k);
+    Zn.dq(i, j, k, 5 + it) += jac * (prod_k - diss_k);
     const double gamma = gamma2 + delta_gamma * f1;
     const double prod_omega = gamma * density / mut * prod_k + (1 - f1) * inter_var;
     const double diss_omega = beta * density * omega * omega;
-    Zn.dq(i, j, k, 6) += jac * (prod_omega - diss_omega);
+    Zn.dq(i, j, k, 6 + it) += jac * (prod_omega - diss_omega);
   }
   if (P->turb_implicit == 1 && Zn.tsj.p) {  // SST.cu:243-246
     Zn.tsj(i, j, k, 0) = -2 * betaStar * omega;
     Zn.tsj(i, j, k, 1) = -2 * beta * omega;
   }
-  constexpr double cp = gamma_air * R_u / mw_air / (gamma_air - 1);
-  Zn.ttc(i, j, k) = Zn.mut(i, j, k) * cp / P->Prt;
+  constexpr double cpa = gamma_air * R_u / mw_air / (gamma_air - 1);
+  Zn.ttc(i, j, k) = Zn.mut(i, j, k) * (it > 0 ? Zn.cp(i, j, k) : cpa) / P->Prt;
 }
 }  // namespace sst
 
@@ -1163,7 +1197,8 @@ void viscous_face(const ostc_param *P, const Z &Zn, int d, int i, int j, int k, 
     constexpr double delta_d = 1e-3;
     const double dy_div_delta = std::min(0.5 * (Zn.wall(i, j, k) + Zn.wall(i1, j1, k1)) / delta_d, 1.0);
     const double twoThirdrhoKm =
-        -2.0 / 3 * 0.5 * (Zn.bv(i, j, k, 0) * Zn.sv(i, j, k, 0) + Zn.bv(i1, j1, k1, 0) * Zn.sv(i1, j1, k1, 0)) *
+        -2.0 / 3 * 0.5 *
+        (Zn.bv(i, j, k, 0) * Zn.sv(i, j, k, P->n_spec) + Zn.bv(i1, j1, k1, 0) * Zn.sv(i1, j1, k1, P->n_spec)) *
         dy_div_delta;
     tau_xx += twoThirdrhoKm;
     tau_yy += twoThirdrhoKm;
@@ -1195,6 +1230,7 @@ void viscous_face(const ostc_param *P, const Z &Zn, int d, int i, int j, int k, 
     for (int l = 0; l < ns; ++l) {
       yk[l] = 0.5 * (Zn.sv(i, j, k, l) + Zn.sv(i1, j1, k1, l));
       diff[l] = 0.5 * (Zn.rhoD(i, j, k, l) + Zn.rhoD(i1, j1, k1, l));
+      if (turb) diff[l] += mut / P->Sct;  // turbulent diffusivity (ViscousScheme.cuh:122-125)
       double dy[3];
       der(Zn.sv, l, dy);
       const double y_x = dy[0] * xi_x + dy[1] * eta_x + dy[2] * zeta_x;
@@ -1231,9 +1267,10 @@ void viscous_face(const ostc_param *P, const Z &Zn, int d, int i, int j, int k, 
     }
   }
   if (turb) {  // k and omega diffusion, ViscousScheme.cuh:200-251
+    const int it = P->n_spec;
     double dk[3], dw[3];
-    der(Zn.sv, 0, dk);
-    der(Zn.sv, 1, dw);
+    der(Zn.sv, it, dk);
+    der(Zn.sv, it + 1, dw);
     const double k_x = dk[0] * xi_x + dk[1] * eta_x + dk[2] * zeta_x;
     const double k_y = dk[0] * xi_y + dk[1] * eta_y + dk[2] * zeta_y;
     const double k_z = dk[0] * xi_z + dk[1] * eta_z + dk[2] * zeta_z;
@@ -1243,8 +1280,8 @@ void viscous_face(const ostc_param *P, const Z &Zn, int d, int i, int j, int k, 
     const double wall_dist = 0.5 * (Zn.wall(i, j, k) + Zn.wall(i1, j1, k1));
     double f1 = 1;
     if (wall_dist > 1e-25) {
-      const double km = 0.5 * (Zn.sv(i, j, k, 0) + Zn.sv(i1, j1, k1, 0));
-      const double omegam = 0.5 * (Zn.sv(i, j, k, 1) + Zn.sv(i1, j1, k1, 1));
+      const double km = 0.5 * (Zn.sv(i, j, k, it) + Zn.sv(i1, j1, k1, it));
+      const double omegam = 0.5 * (Zn.sv(i, j, k, it + 1) + Zn.sv(i1, j1, k1, it + 1));
       const double param1 = std::sqrt(km) / (0.09 * omegam * wall_dist);
       const double rhom = 0.5 * (Zn.bv(i, j, k, 0) + Zn.bv(i1, j1, k1, 0));
       const double d2 = wall_dist * wall_dist;
@@ -1257,8 +1294,8 @@ void viscous_face(const ostc_param *P, const Z &Zn, int d, int i, int j, int k, 
     }
     const double sigma_k = sst::sigma_k2 + sst::delta_sigma_k * f1;
     const double sigma_omega = sst::sigma_omega2 + sst::delta_sigma_omega * f1;
-    fv[5] = (mul + mut * sigma_k) * (kxj * k_x + kyj * k_y + kzj * k_z);
-    fv[6] = (mul + mut * sigma_omega) * (kxj * omega_x + kyj * omega_y + kzj * omega_z);
+    fv[5 + it] = (mul + mut * sigma_k) * (kxj * k_x + kyj * k_y + kzj * k_z);
+    fv[6 + it] = (mul + mut * sigma_omega) * (kxj * omega_x + kyj * omega_y + kzj * omega_z);
   }
 }
 
@@ -1499,11 +1536,14 @@ void bc_wall(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
         Zn.bv(i, j, k, 4) = p;
         Zn.bv(i, j, k, 5) = t_wall;
         Zn.vel(i, j, k) = 0;
-        if (is_sst(P)) {  // BoundCond.cuh:471-484
-          const double mu_wall = sutherland(t_wall);
+        if (is_sst(P)) {  // BoundCond.cuh:471-484; the mixture's viscosity at the wall species
+          double Yw[MAXS];
+          for (int l = 0; l < ns; ++l) Yw[l] = Zn.sv(i, j, k, l);
+          const double mu_wall = ns > 0 ? mixture_viscosity(P, t_wall, Yw) : sutherland(t_wall);
           const double dy = Zn.wall(ii, ij, ik);
-          Zn.sv(i, j, k, 0) = 0;
-          Zn.sv(i, j, k, 1) = dy > 1e-25 ? 60 * mu_wall / (rho_wall * sst::beta_1 * dy * dy) : Zn.sv(ii, ij, ik, 1);
+          Zn.sv(i, j, k, ns) = 0;
+          Zn.sv(i, j, k, ns + 1) =
+              dy > 1e-25 ? 60 * mu_wall / (rho_wall * sst::beta_1 * dy * dy) : Zn.sv(ii, ij, ik, ns + 1);
         }
         if (with_cv) cv_from_bv_point(P, Zn, i, j, k);
         for (int g = 1; g <= Zn.ngg; ++g) {
@@ -1531,8 +1571,8 @@ void bc_wall(const ostc_param *P, Z &Zn, const ostc_bc_face &b, int with_cv) {
           Zn.bv(gi, gj, gk, 4) = p_i;
           Zn.bv(gi, gj, gk, 5) = t_g;
           if (is_sst(P)) {  // BoundCond.cuh:536-541
-            Zn.sv(gi, gj, gk, 0) = 0;
-            Zn.sv(gi, gj, gk, 1) = Zn.sv(i, j, k, 1);
+            Zn.sv(gi, gj, gk, ns) = 0;
+            Zn.sv(gi, gj, gk, ns + 1) = Zn.sv(i, j, k, ns + 1);
             Zn.mut(gi, gj, gk) = 0;
           }
           if (with_cv) cv_from_bv_point(P, Zn, gi, gj, gk);
@@ -2073,12 +2113,12 @@ void dplur_zone(const ostc_config *c, const ostc_param *P, Z &Zn, const std::vec
               Zn.dq(i, j, k, 5 + l) /= diag - dt * jd;
             }
           } else {
-            for (int l = 5; l < nv; ++l) Zn.dq(i, j, k, l) /= diag;
+            for (int l = 5; l < 5 + ns; ++l) Zn.dq(i, j, k, l) /= diag;
           }
         }
-        if (is_sst(P)) {  // DPLUR.cuh:72-84, SST.cu:249-258
+        if (is_sst(P)) {  // DPLUR.cuh:72-84, SST.cu:249-258 (rows i_turb_cv, +1)
           for (int t = 0; t < 2; ++t)
-            Zn.dq(i, j, k, 5 + t) /= P->turb_implicit == 1 ? diag - dt * Zn.tsj(i, j, k, t) : diag;
+            Zn.dq(i, j, k, 5 + ns + t) /= P->turb_implicit == 1 ? diag - dt * Zn.tsj(i, j, k, t) : diag;
         }
         for (int l = 0; l < nv; ++l) dq0(i, j, k, l) = Zn.dq(i, j, k, l);
       }
@@ -2140,13 +2180,14 @@ void dplur_zone(const ostc_config *c, const ostc_param *P, Z &Zn, const std::vec
                 dqk(i, j, k, 5 + l) = dq0(i, j, k, 5 + l) + dt * tot[5 + l] / (diag - dt * jd);
               }
             } else {
-              for (int l = 5; l < nv; ++l) dqk(i, j, k, l) = dq0(i, j, k, l) + dt * tot[l] / diag;
+              for (int l = 5; l < 5 + ns; ++l) dqk(i, j, k, l) = dq0(i, j, k, l) + dt * tot[l] / diag;
             }
           }
-          if (is_sst(P)) {  // DPLUR.cuh:262-276, SST.cu:260-273
+          if (is_sst(P)) {  // DPLUR.cuh:262-276, SST.cu:260-273 (rows i_turb_cv, +1)
             for (int t = 0; t < 2; ++t)
-              dqk(i, j, k, 5 + t) = dq0(i, j, k, 5 + t) +
-                                    dt * tot[5 + t] / (P->turb_implicit == 1 ? diag - dt * Zn.tsj(i, j, k, t) : diag);
+              dqk(i, j, k, 5 + ns + t) =
+                  dq0(i, j, k, 5 + ns + t) +
+                  dt * tot[5 + ns + t] / (P->turb_implicit == 1 ? diag - dt * Zn.tsj(i, j, k, t) : diag);
           }
         }
     // dq <- dqk over the interior (the ghost layer of dq is never read)
@@ -2375,8 +2416,14 @@ int oracle_initialize(const ostc_config *c, const ostc_param *P, ostc_zone *zone
     if (is_sst(P))  // initialize_mut over [-1, m] (FieldOperation.cuh:175-195)
       for (int k = -1; k <= Zn.mz; ++k)
         for (int j = -1; j <= Zn.my; ++j)
-          for (int i = -1; i <= Zn.mx; ++i)
-            Zn.mut(i, j, k) = sst::compute_mut(Zn, i, j, k, sutherland(Zn.bv(i, j, k, 5)));
+          for (int i = -1; i <= Zn.mx; ++i) {
+            // Sutherland's viscosity for air, the mixture's (compute_viscosity) with species
+            double Y[MAXS];
+            for (int l = 0; l < P->n_spec; ++l) Y[l] = Zn.sv(i, j, k, l);
+            const double T = Zn.bv(i, j, k, 5);
+            const double mul = P->n_spec > 0 ? mixture_viscosity(P, T, Y) : sutherland(T);
+            Zn.mut(i, j, k) = sst::compute_mut(Zn, P->n_spec, i, j, k, mul);
+          }
   }
   oracle_data_communication(P, zones, n_zones, 0);
   for (int b = 0; b < n_zones; ++b) oracle_update_physical_properties(P, &zones[b]);
@@ -2530,8 +2577,8 @@ int oracle_steady_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zo
             for (int j = 0; j < Zn.my; ++j)
               for (int i = 0; i < Zn.mx; ++i) {
                 const double dt = Zn.dt_local(i, j, k);
-                Zn.dq(i, j, k, 5) /= 1 - dt * Zn.tsj(i, j, k, 0);
-                Zn.dq(i, j, k, 6) /= 1 - dt * Zn.tsj(i, j, k, 1);
+                Zn.dq(i, j, k, P->i_turb_cv) /= 1 - dt * Zn.tsj(i, j, k, 0);
+                Zn.dq(i, j, k, P->i_turb_cv + 1) /= 1 - dt * Zn.tsj(i, j, k, 1);
               }
         }
       }

@@ -70,7 +70,7 @@ struct RefCtx {  // one block
 struct RefMulti {  // all blocks of a run
   ostc_config cfg{};
   int mix = 0;
-  int sst = 0;  // k-omega SST (air)
+  int sst = 0;  // k-omega SST (Driver<Air, SST> or Driver<FR, SST>)
   std::vector<RefCtx *> blk;
 };
 
@@ -636,7 +636,7 @@ int ref_create_multi(const ostc_config *cfg, const ostc_param *p, const ostc_zon
                      int nf, const ostc_interface *ifc, int nif, void **out) {
   if (!cfg || !p || !z || !out || nz < 1) return 1;
   if (p->mix_model != OSTC_MIX_AIR && p->mix_model != OSTC_MIX_FR) return 5;
-  if (p->turbulence && (p->rans_model != 2 || p->mix_model != OSTC_MIX_AIR)) return 5;
+  if (p->turbulence && p->rans_model != 2) return 5;
   for (int q = 0; q < nf; ++q)
     if (f[q].block < 0 || f[q].block >= nz) return 1;
   for (int q = 0; q < nif; ++q)
@@ -675,7 +675,9 @@ int ref_create(const ostc_config *cfg, const ostc_param *p, const ostc_zone *z, 
 
 int ref_initialize(void *h) {
   auto *m = (RefMulti *)h;
-  if (m->sst)
+  if (m->sst && m->mix != OSTC_MIX_AIR)
+    initialize<MixtureModel::FR, SST>(*m);
+  else if (m->sst)
     initialize<MixtureModel::Air, SST>(*m);
   else if (m->mix == OSTC_MIX_AIR)
     initialize<MixtureModel::Air, Laminar>(*m);
@@ -687,7 +689,9 @@ int ref_initialize(void *h) {
 int ref_rhs(void *h) {
   auto *m = (RefMulti *)h;
   for (RefCtx *c : m->blk) {
-    if (m->sst)
+    if (m->sst && m->mix != OSTC_MIX_AIR)
+      rhs<MixtureModel::FR, SST>(*c);
+    else if (m->sst)
       rhs<MixtureModel::Air, SST>(*c);
     else if (m->mix == OSTC_MIX_AIR)
       rhs<MixtureModel::Air, Laminar>(*c);
@@ -699,6 +703,7 @@ int ref_rhs(void *h) {
 
 int ref_steps(void *h, int n, double *res_hist, double *dt_hist) {
   auto *m = (RefMulti *)h;
+  if (m->sst && m->mix != OSTC_MIX_AIR) return steps<MixtureModel::FR, SST>(*m, n, res_hist, dt_hist);
   if (m->sst) return steps<MixtureModel::Air, SST>(*m, n, res_hist, dt_hist);
   return m->mix == OSTC_MIX_AIR ? steps<MixtureModel::Air, Laminar>(*m, n, res_hist, dt_hist)
                                 : steps<MixtureModel::FR, Laminar>(*m, n, res_hist, dt_hist);
@@ -707,6 +712,7 @@ int ref_steps(void *h, int n, double *res_hist, double *dt_hist) {
 int ref_steady_steps(void *h, int n, double *res_hist) {
   auto *m = (RefMulti *)h;
   if (!m->cfg.steady) return 1;
+  if (m->sst && m->mix != OSTC_MIX_AIR) return steady_steps<MixtureModel::FR, SST>(*m, n, res_hist);
   if (m->sst) return steady_steps<MixtureModel::Air, SST>(*m, n, res_hist);
   return m->mix == OSTC_MIX_AIR ? steady_steps<MixtureModel::Air, Laminar>(*m, n, res_hist)
                                 : steady_steps<MixtureModel::FR, Laminar>(*m, n, res_hist);
