@@ -200,6 +200,26 @@ static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, const Flu
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
+  if (smem > 0) {
+    // carve out only the shared memory of the CTAs the register budget lets an SM hold
+    // (plus the 1 KB the driver reserves per CTA): the rest of the 256 KB stays L1, which
+    // serves the stencil's re-reads (the default sizes the carveout for the shared-memory
+    // limit alone)
+    int per_sm = 0;
+    cudaError_t e = tab ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                              &per_sm, flux_dir_table<NS, INV, DIR, MINB, PART, NT>, 32 * R, smem)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flux_dir<NS, INV, DIR, MINB, PART, NT>,
+                                                                        32 * R, smem);
+    if (e != cudaSuccess) return e;
+    const size_t need = (size_t)per_sm * (smem + 1024);
+    int pct = (int)((need * 100 + 228 * 1024 - 1) / (228 * 1024));
+    pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+    e = tab ? cudaFuncSetAttribute(flux_dir_table<NS, INV, DIR, MINB, PART, NT>,
+                                   cudaFuncAttributePreferredSharedMemoryCarveout, pct)
+            : cudaFuncSetAttribute(flux_dir<NS, INV, DIR, MINB, PART, NT>,
+                                   cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    if (e != cudaSuccess) return e;
+  }
   if (!tab) {
     flux_dir<NS, INV, DIR, MINB, PART, NT><<<flux_grid(z.mx, z.my, z.mz, DIR, R, C), blk, smem, s>>>(z, C, accumulate,
                                                                                                  viscous);
