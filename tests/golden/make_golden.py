@@ -10,7 +10,7 @@ Needs a GPU and the reference build; writes one compressed .npz per case:
 Each file holds, per block b: the SHA-256 of the block's inputs (bv, sv,
 jac, metric as built by the case builder, to detect builder drift), the
 interior RHS dq after initialisation (`dq_b`), and after the case's steps
-the interior bv / sv (`bv_b`, `sv_b`) plus the residual history `res` and,
+the interior bv / sv (species and SST k, omega: `bv_b`, `sv_b`) plus the residual history `res` and,
 for RK3, the dt history `dt`; `reduction_ok` says whether the reference's
 block reductions are well defined at these sizes (they are for every case
 here)."""
@@ -45,6 +45,21 @@ def _vortex(recon, inv):
     return ostc.case_vortex(16, 12, 6, k_bc="symmetry", reconstruction=recon, inviscid_scheme=inv)
 
 
+def _sst_air():
+    """one walled SST block (case_uneven_blocks); the far field becomes outflow because the
+    reference's air + SST far field reads unset boundary scalars (quirk A20)"""
+    c = ostc.case_uneven_blocks(layout=[((0, 0, 0), (18, 14, 6))], rans_model=2)
+    for f in c.faces:
+        if f.type_label == ostc.BC_FARFIELD:
+            f.type_label = ostc.BC_OUTFLOW
+    return c
+
+
+def _sst_h2air():
+    """the reacting mixing layer with SST and an isothermal wall at j = 0 (Driver<FR, SST>)"""
+    return _no_periodic(ostc.case_mixing_layer(12, 11, 6, full_host=True, rans_model=2, wall=True))
+
+
 # name -> (builder, mode, steps); mode "rk3" or "steady"
 CASES = {
     "vortex_aweno": (lambda: _vortex(4, 2), "rk3", 5),
@@ -60,6 +75,12 @@ CASES = {
     "premixed_dplur_epi": (lambda: ostc.make_steady(ostc.case_premixed_box(12, 10, 6), 1, 1), "steady", 4),
     "premixed_dplur_da": (lambda: ostc.make_steady(ostc.case_premixed_box(12, 10, 6), 1, 2), "steady", 4),
     "wall_dplur": (lambda: ostc.make_steady(ostc.case_bc_box("wall_farfield", 20, 16, 6), 1), "steady", 4),
+    "sst_air_hllc": (_sst_air, "rk3", 4),
+    "sst_air_dplur": (lambda: ostc.make_steady(_sst_air(), 1), "steady", 4),
+    "sst_h2air_wall": (_sst_h2air, "rk3", 3),
+    "sst_h2air_dplur_epi": (lambda: ostc.make_steady(_sst_h2air(), 1, 1), "steady", 3),
+    "planar_roe_muscl": (lambda: ostc.case_vortex(25, 21, 1, reconstruction=2, inviscid_scheme=2), "rk3", 5),
+    "planar_wall_dplur": (lambda: ostc.make_steady(ostc.case_bc_box("wall_farfield", 25, 21, 1), 1), "steady", 4),
 }
 
 
@@ -115,7 +136,7 @@ def main():
         data["res"] = res
         for b, blk in enumerate(case.blocks):
             data["bv_%d" % b] = interior(r2.download("bv", b), blk.ngg)
-            if blk.n_spec:
+            if blk.n_spec + blk.n_turb:
                 data["sv_%d" % b] = interior(r2.download("sv", b), blk.ngg)
         np.savez_compressed(out / ("%s.npz" % name), **data)
         print("wrote", name, sum(v.nbytes for v in data.values()))
