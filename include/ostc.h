@@ -329,7 +329,7 @@ ostc_status ostc_steady_steps(ostc_ctx *ctx, int n_steps, double *res_hist, void
  * Y' = Y + d(rho Y)/rho, and T' from e(T', Y') = e(T, Y) by the Newton
  * iteration of compute_temperature_and_pressure (src/FieldOperation.cu:
  * 3-39) run to a relative 1e-13. The reference has no single function for
- * this composition; it is the labeller, fallback and judge of the chemistry
+ * this composition; it is the labeller, fallback and arbiter of the chemistry
  * surrogate. All pointers are DEVICE arrays: T, p, dt, dT of n doubles, Y
  * and dY of n_spec x n (species-major). dT is NaN where the Newton solve did
  * not converge. Needs a context with a finite-rate mechanism.              */

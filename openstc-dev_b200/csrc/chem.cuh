@@ -250,7 +250,7 @@ __device__ __forceinline__ void lu_solve(double *A, double *b) {
 //   d(rho Y) = (I - dt J)^-1 dt omega; Y' = Y + d(rho Y) / rho;
 //   T' solves e(T', Y') = e(T, Y), e = sum Y h(T) - R_u T sum(Y/W), by Newton
 //   to |1 - T1/T| <= 1e-13 (at most 100 iterations; the reference's 1e-3
-//   tolerance would leave kelvin-sized errors in an integrator used as judge).
+//   tolerance would leave kelvin-sized errors in an integrator that arbitrates the surrogate).
 // Returns dY (NS) and dT; `iters` is the Newton count (0 if it failed).
 template <int NS>
 __device__ __forceinline__ void point_implicit_increment(double T, double p, const double *Y, double dt, double *dY,

@@ -2433,7 +2433,7 @@ int oracle_initialize(const ostc_config *c, const ostc_param *P, ostc_zone *zone
 
 int oracle_rk3_steps(const ostc_config *c, const ostc_param *P, ostc_zone *zones, int n_zones,
                      const ostc_bc_face *f, int n_faces, int n_steps, double *res_hist, double *dt_hist) {
-  if (c->chem_mode == 2) return OSTC_ERR_UNSUPPORTED;  // the oracle judges the surrogate through chem_mode 1
+  if (c->chem_mode == 2) return OSTC_ERR_UNSUPPORTED;  // the oracle checks the surrogate through chem_mode 1
   struct SkipGuard {
     explicit SkipGuard(bool on) { g_skip_source = on; }
     ~SkipGuard() { g_skip_source = false; }

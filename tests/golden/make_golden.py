@@ -112,7 +112,7 @@ def main():
     import ref_bind
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=str(REPO / "gpurun_out" / "golden"))
+    ap.add_argument("--out", default=str(REPO / "tests" / "golden"))
     a = ap.parse_args()
     out = Path(a.out)
     out.mkdir(parents=True, exist_ok=True)
