@@ -1089,9 +1089,7 @@ cudaError_t launch_eliminate_k(const DevZone &z, int with_cv, cudaStream_t s) {
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s) {
   const int n0 = b.re[0] - b.rs[0] + 1, n1 = b.re[1] - b.rs[1] + 1, n2 = b.re[2] - b.rs[2] + 1;
-  // every boundary point is one thread writing its own ghost line, so the shape is free: 256
-  // threads where the range allows (an i face runs its threads along j)
-  const dim3 blk(n0 >= 32 ? 32 : (n0 >= 8 ? 8 : 1), n0 >= 32 ? (n1 >= 8 ? 8 : 1) : (n1 >= 64 ? 64 : (n1 >= 8 ? 8 : 1)));
+  const dim3 blk(n0 >= 32 ? 32 : (n0 >= 8 ? 8 : 1), n1 >= 8 ? 8 : 1);
   const dim3 grid((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, n2);
   switch (b.type) {
     case OSTC_BC_OUTFLOW: bc_outflow_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
