@@ -764,6 +764,25 @@ int ref_download_block(void *h, int b, const char *name, double *dst) {
 
 int ref_download(void *h, const char *name, double *dst) { return ref_download_block(h, 0, name, dst); }
 
+// Block::compute_jac_metric (Mesh.cpp:259-521), the reference's own host code,
+// on caller coordinates with ngg+1 ghost layers (x, y, z in the ghosted
+// layout of gxl::Array3D): fills jac (ngg ghosts) and the 80-byte metric
+// records (ngg ghosts). Host only; the grid must have positive Jacobians (the
+// reference logs and copies a neighbour otherwise).
+int ref_metric(int mx, int my, int mz, int ngg, const double *x, const double *y, const double *z, double *jac_out,
+               void *metric_out) {
+  if (mx < 1 || my < 1 || mz < 1 || ngg < 1 || !x || !y || !z || !jac_out || !metric_out) return 1;
+  Block b(mx, my, mz, ngg, 0);
+  const size_t nc = plane(mx, my, mz, ngg + 1), np = plane(mx, my, mz, ngg);
+  std::memcpy(b.x.data(), x, nc * sizeof(double));
+  std::memcpy(b.y.data(), y, nc * sizeof(double));
+  std::memcpy(b.z.data(), z, nc * sizeof(double));
+  b.compute_jac_metric(0);
+  std::memcpy(jac_out, b.jacobian.data(), np * sizeof(double));
+  std::memcpy(metric_out, b.metric.data(), np * sizeof(gxl::Matrix<real, 3, 3, 1>));
+  return 0;
+}
+
 // bytes of device memory the reference arrays of this run hold
 double ref_device_bytes(void *h) {
   auto *m = (RefMulti *)h;

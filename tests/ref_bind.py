@@ -44,6 +44,8 @@ def ref():
         L.ref_time_steps.restype = C.c_double
         L.ref_download.argtypes = [vp, C.c_char_p, d]
         L.ref_download.restype = C.c_int
+        L.ref_metric.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, d, d, d, d, vp]
+        L.ref_metric.restype = C.c_int
         _r = L
     return _r
 
@@ -100,3 +102,18 @@ class RefCudaRun:
         out = np.zeros(shapes[name])
         assert ref().ref_download_block(self.h, block, name.encode(), out.ctypes.data_as(C.POINTER(C.c_double))) == 0
         return out
+
+
+def metric(mx, my, mz, ngg, x, y, z):
+    """the reference's Block::compute_jac_metric on coordinates with ngg+1
+    ghost layers: (jac, metric) as ghosted arrays (metric in ostc.METRIC_DTYPE)"""
+    shape = ostc.plane_shape(mx, my, mz, ngg)
+    jac = np.zeros(shape)
+    met = np.zeros(shape, dtype=ostc.METRIC_DTYPE)
+    d = C.POINTER(C.c_double)
+    xs, ys, zs = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+    st = ref().ref_metric(mx, my, mz, ngg, xs.ctypes.data_as(d), ys.ctypes.data_as(d), zs.ctypes.data_as(d),
+                          jac.ctypes.data_as(d), met.ctypes.data)
+    if st != 0:
+        raise RuntimeError("ref_metric -> %d" % st)
+    return jac, met
