@@ -182,6 +182,27 @@ def algorithmic_bytes(name, case):
 
 
 # ---------------------------------------------------------------------------
+# replicas (one independent copy of the workload per rank; no collective on
+# the data path): the job ends with its slowest rank
+# ---------------------------------------------------------------------------
+def replica_ms(ms, world, device):
+    """the device-timed ms of this rank -> the max over all ranks"""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(cells, steps, world, ms):
+    """whole-job Mcell-updates/s: every rank advanced its own cells"""
+    return cells * steps * world / (ms * 1e-3) / 1e6
+
+
+# ---------------------------------------------------------------------------
 # the timed run
 # ---------------------------------------------------------------------------
 def run_ours(a):
@@ -224,14 +245,10 @@ def run_ours(a):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
     ck = clocks.stop()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replica_ms(e0.elapsed_time(e1), world, "cuda")
     cells = case.cells
-    value = cells * a.steps * world / (ms * 1e-3) / 1e6
+    value = replica_value(cells, a.steps, world, ms)
 
     # several blocks: the same steps with one launch per block instead of the
     # tile-table launches (same tiles, same start state)
