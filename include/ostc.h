@@ -254,6 +254,40 @@ ostc_status ostc_data_communication(ostc_ctx *ctx, int with_cv, void *stream);
 /* update_physical_properties<mix> over [-1, m] (src/FieldOperation.cuh:112-146). */
 ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream);
 
+/* ----------------------------------------------------------------------- */
+/* per-step epilogues of the RK3 loop (src/RK.cuh:164-180)                  */
+/* ----------------------------------------------------------------------- */
+/* Every step of ostc_rk3_steps ends with physical_time += dt of its last
+ * stage and step += 1 (both reset by ostc_initialize); this returns them
+ * (synchronises the device; either pointer may be NULL).                   */
+ostc_status ostc_physical_time(ostc_ctx *ctx, double *time, int *step);
+
+/* Monitor points (Monitor.cu:196-251, record_monitor_data): after every step
+ * the bv planes bv_label[0..n_bv) (0 rho, 1 u, 2 v, 3 w, 4 p, 5 T) and the sv
+ * planes sv_label[0..n_sv) (species, then k, omega) at the interior points
+ * (block[p], i[p], j[p], k[p]), followed by the physical time, go to a device
+ * ring of `capacity` steps. n_points = 0 removes the monitor. Resets the
+ * cached step graphs.                                                       */
+ostc_status ostc_set_monitor(ostc_ctx *ctx, int n_points, const int *block, const int *i, const int *j,
+                             const int *k, int n_bv, const int *bv_label, int n_sv, const int *sv_label,
+                             int capacity);
+/* Copies the ring to the HOST array out[(p * capacity + s) * (n_bv + n_sv + 1)
+ * + v] and restarts it (Monitor::output_data); *n_recorded = the steps
+ * recorded since the last call (at most capacity; ring slot s = step index
+ * modulo capacity). Synchronises the device.                               */
+ostc_status ostc_get_monitor(ostc_ctx *ctx, double *out, int *n_recorded);
+
+/* Statistics (StatisticsCollector.cu:14-52): on = 1 starts per-cell sums over
+ * the interior of every block, for each step after start_step (and after this
+ * call): rho, u, v, w, p, T and their squares (sum12, 12 planes), cubes and
+ * fourth powers (sum34, 12 planes), uv, uw, vw (3 planes) and the mass
+ * fractions (n_spec planes). on = 0 frees them. Resets the cached graphs.   */
+ostc_status ostc_set_statistics(ostc_ctx *ctx, int on, int start_step);
+/* The sums of one block to HOST arrays (each may be NULL; interior layout,
+ * g = 0) and the number of steps summed. Synchronises the device.          */
+ostc_status ostc_get_statistics(ostc_ctx *ctx, int block, double *sum12, double *sum34, double *sum_rs,
+                                double *sum_yk, int *n_collected);
+
 /* eliminate_k_gradient<with_cv> (src/FieldOperation.cuh:372-400): on 2-D
  * blocks (mz == 1) every k ghost plane of bv, sv (and cv when with_cv) takes
  * the values of the plane k = 0 over the whole ghosted (i, j) range, so

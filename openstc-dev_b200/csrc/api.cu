@@ -54,6 +54,13 @@ struct ostc_ctx {
   int hist_cap = 0;
   double n_total = 0;
   std::map<int, GraphEntry> graphs;  // key: with_residual (+2 for the steady step)
+  // per-step epilogues of the RK3 loop: step count and physical time (one int, one
+  // double), monitor points, statistics sums (per zone)
+  int *ep_step = nullptr;
+  double *ep_time = nullptr;
+  MonitorSet mon;
+  int stat_on = 0, stat_start = 0;
+  std::vector<StatSums> stats;
   // steady path: spectral radii (3 interior planes), DPLUR buffers (dq layout),
   // DPLUR point-implicit chemistry (LU factors + pivots, or DA divisors)
   std::vector<double *> isr, dq0, dqk, lu, da;
@@ -611,6 +618,10 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
   c->n_part_per_zone = 148 * 2;
   CK(cudaMalloc(&c->res_partial, sizeof(double) * 4 * c->n_part_per_zone * n_zones));
   CK(cudaMalloc(&c->hist_counter, sizeof(int)));
+  CK(cudaMalloc(&c->ep_step, sizeof(int)));
+  CK(cudaMalloc(&c->ep_time, sizeof(double)));
+  CK(cudaMemset(c->ep_step, 0, sizeof(int)));
+  CK(cudaMemset(c->ep_time, 0, sizeof(double)));
   CK(cudaDeviceSynchronize());
   default_tiles(ctx);
   // several blocks: one tile-table launch per kernel over all of them
@@ -637,6 +648,13 @@ ostc_status ostc_destroy(ostc_ctx *ctx) {
   cudaFree(ctx->hist_counter);
   cudaFree(ctx->hist_res);
   cudaFree(ctx->hist_dt);
+  cudaFree(ctx->ep_step);
+  cudaFree(ctx->ep_time);
+  cudaFree(ctx->mon.pts);
+  cudaFree(ctx->mon.labels);
+  cudaFree(ctx->mon.data);
+  cudaFree(ctx->mon.counter);
+  for (auto &st : ctx->stats) cudaFree(st.s12);
   if (g_uploaded == ctx) g_uploaded = nullptr;
   delete ctx;
   return OSTC_OK;
@@ -818,6 +836,9 @@ ostc_status ostc_initialize(ostc_ctx *ctx, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;
   ostc_status st;
   if ((st = repack_metrics(ctx, S(stream)))) return st;
+  // a fresh run: step 0 at physical time 0
+  CK(cudaMemsetAsync(ctx->ep_step, 0, sizeof(int), S(stream)));
+  CK(cudaMemsetAsync(ctx->ep_time, 0, sizeof(double), S(stream)));
   // 2-D: the k ghost planes copy the plane k = 0 first (Driver.cu:54-60)
   if ((st = ostc_eliminate_k_gradient(ctx, 0, stream))) return st;
   if ((st = ostc_apply_boundary_conditions(ctx, 0, stream))) return st;
@@ -899,6 +920,17 @@ static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
                                      ctx->hist_res, ctx->hist_dt, ctx->hist_counter, ctx->hist_cap);
     CK(cudaGetLastError());
   }
+  // epilogues (RK.cuh:164-180): physical_time += dt of the last stage, then the
+  // monitor points and the statistics sums of the step
+  CK(launch_step_clock(ctx->ep_step, ctx->ep_time,
+                       ctx->cfg.fixed_time_step ? nullptr : (const double *)ctx->dt_bits, ctx->cfg.dt, s));
+  if (ctx->mon.n > 0) {
+    for (size_t b = 0; b < ctx->dz.size(); ++b) CK(launch_monitor(ctx->dz[b], (int)b, ctx->mon, s));
+    CK(launch_monitor_advance(ctx->mon.counter, s));
+  }
+  if (ctx->stat_on)
+    for (size_t b = 0; b < ctx->dz.size(); ++b)
+      CK(launch_statistics(ctx->dz[b], ctx->ep_step, ctx->stat_start, ctx->stats[b], ctx->prm.n_spec, s));
   return OSTC_OK;
 }
 
@@ -1201,6 +1233,130 @@ ostc_status ostc_step_kernel_count(ostc_ctx *ctx, int with_hist, int *count) {
     if (t == cudaGraphNodeTypeKernel) ++k;
   }
   *count = k;
+  return OSTC_OK;
+}
+
+static void drop_graphs(ostc_ctx *ctx) {
+  for (auto &kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  ctx->graphs.clear();
+}
+
+ostc_status ostc_set_monitor(ostc_ctx *ctx, int n_points, const int *block, const int *i, const int *j, const int *k,
+                             int n_bv, const int *bv_label, int n_sv, const int *sv_label, int capacity) {
+  if (!ctx || n_points < 0) return OSTC_ERR_INVALID_ARG;
+  MonitorSet m;
+  if (n_points > 0) {
+    if (!block || !i || !j || !k || n_bv < 0 || n_sv < 0 || n_bv + n_sv < 1 || capacity < 1 ||
+        (n_bv > 0 && !bv_label) || (n_sv > 0 && !sv_label))
+      return OSTC_ERR_INVALID_ARG;
+    std::vector<int4> pts(n_points);
+    for (int p = 0; p < n_points; ++p) {
+      if (block[p] < 0 || block[p] >= (int)ctx->dz.size()) return OSTC_ERR_INVALID_ARG;
+      const DevZone &z = ctx->dz[block[p]];
+      if (i[p] < 0 || i[p] >= z.mx || j[p] < 0 || j[p] >= z.my || k[p] < 0 || k[p] >= z.mz) return OSTC_ERR_INVALID_ARG;
+      pts[p] = make_int4(block[p], i[p], j[p], k[p]);
+    }
+    std::vector<int> labels;
+    for (int l = 0; l < n_bv; ++l) {
+      if (bv_label[l] < 0 || bv_label[l] > 5) return OSTC_ERR_INVALID_ARG;
+      labels.push_back(bv_label[l]);
+    }
+    for (int l = 0; l < n_sv; ++l) {
+      if (sv_label[l] < 0 || sv_label[l] >= ctx->prm.n_scalar) return OSTC_ERR_INVALID_ARG;
+      labels.push_back(sv_label[l]);
+    }
+    m.n = n_points, m.nbv = n_bv, m.nsv = n_sv, m.cap = capacity;
+    const size_t nd = (size_t)n_points * capacity * (n_bv + n_sv + 1);
+    CK(cudaMalloc(&m.pts, sizeof(int4) * n_points));
+    CK(cudaMalloc(&m.labels, sizeof(int) * labels.size()));
+    CK(cudaMalloc(&m.data, sizeof(double) * nd));
+    CK(cudaMalloc(&m.counter, sizeof(int)));
+    CK(cudaMemcpy(m.pts, pts.data(), sizeof(int4) * n_points, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m.labels, labels.data(), sizeof(int) * labels.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemset(m.data, 0, sizeof(double) * nd));
+    CK(cudaMemset(m.counter, 0, sizeof(int)));
+    m.time = ctx->ep_time;
+  }
+  CK(cudaDeviceSynchronize());
+  cudaFree(ctx->mon.pts);
+  cudaFree(ctx->mon.labels);
+  cudaFree(ctx->mon.data);
+  cudaFree(ctx->mon.counter);
+  ctx->mon = m;
+  drop_graphs(ctx);
+  return OSTC_OK;
+}
+
+ostc_status ostc_get_monitor(ostc_ctx *ctx, double *out, int *n_recorded) {
+  if (!ctx || !n_recorded || (ctx->mon.n > 0 && !out)) return OSTC_ERR_INVALID_ARG;
+  *n_recorded = 0;
+  if (ctx->mon.n == 0) return OSTC_OK;
+  CK(cudaDeviceSynchronize());
+  int c = 0;
+  CK(cudaMemcpy(&c, ctx->mon.counter, sizeof(int), cudaMemcpyDeviceToHost));
+  const size_t nd = (size_t)ctx->mon.n * ctx->mon.cap * (ctx->mon.nbv + ctx->mon.nsv + 1);
+  CK(cudaMemcpy(out, ctx->mon.data, sizeof(double) * nd, cudaMemcpyDeviceToHost));
+  CK(cudaMemset(ctx->mon.counter, 0, sizeof(int)));  // Monitor::output_data restarts the ring
+  *n_recorded = c < ctx->mon.cap ? c : ctx->mon.cap;
+  return OSTC_OK;
+}
+
+ostc_status ostc_physical_time(ostc_ctx *ctx, double *time, int *step) {
+  if (!ctx) return OSTC_ERR_INVALID_ARG;
+  CK(cudaDeviceSynchronize());
+  if (time) CK(cudaMemcpy(time, ctx->ep_time, sizeof(double), cudaMemcpyDeviceToHost));
+  if (step) CK(cudaMemcpy(step, ctx->ep_step, sizeof(int), cudaMemcpyDeviceToHost));
+  return OSTC_OK;
+}
+
+ostc_status ostc_set_statistics(ostc_ctx *ctx, int on, int start_step) {
+  if (!ctx || (on != 0 && on != 1) || start_step < 0) return OSTC_ERR_INVALID_ARG;
+  CK(cudaDeviceSynchronize());
+  for (auto &st : ctx->stats) cudaFree(st.s12);
+  ctx->stats.clear();
+  ctx->stat_on = 0;
+  if (on) {
+    const int ns = ctx->prm.n_spec;
+    for (auto &z : ctx->dz) {
+      StatSums st;
+      const size_t n = (size_t)z.nsz, planes = 27 + ns;
+      CK(cudaMalloc(&st.s12, sizeof(double) * planes * n));
+      CK(cudaMemset(st.s12, 0, sizeof(double) * planes * n));
+      st.s34 = st.s12 + 12 * n;
+      st.srs = st.s34 + 12 * n;
+      st.syk = st.srs + 3 * n;
+      ctx->stats.push_back(st);
+    }
+    // sums from the step after start_step (StatisticsCollector: step > start), and never for
+    // steps taken before this call
+    int cur = 0;
+    CK(cudaMemcpy(&cur, ctx->ep_step, sizeof(int), cudaMemcpyDeviceToHost));
+    ctx->stat_on = 1;
+    ctx->stat_start = start_step > cur ? start_step : cur;
+  }
+  drop_graphs(ctx);
+  return OSTC_OK;
+}
+
+ostc_status ostc_get_statistics(ostc_ctx *ctx, int block, double *sum12, double *sum34, double *sum_rs,
+                                double *sum_yk, int *n_collected) {
+  if (!ctx || !ctx->stat_on || block < 0 || block >= (int)ctx->dz.size()) return OSTC_ERR_INVALID_ARG;
+  CK(cudaDeviceSynchronize());
+  const size_t n = (size_t)ctx->dz[block].nsz;
+  const StatSums &st = ctx->stats[block];
+  if (sum12) CK(cudaMemcpy(sum12, st.s12, sizeof(double) * 12 * n, cudaMemcpyDeviceToHost));
+  if (sum34) CK(cudaMemcpy(sum34, st.s34, sizeof(double) * 12 * n, cudaMemcpyDeviceToHost));
+  if (sum_rs) CK(cudaMemcpy(sum_rs, st.srs, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+  if (sum_yk && ctx->prm.n_spec > 0)
+    CK(cudaMemcpy(sum_yk, st.syk, sizeof(double) * ctx->prm.n_spec * n, cudaMemcpyDeviceToHost));
+  if (n_collected) {
+    int step = 0;
+    CK(cudaMemcpy(&step, ctx->ep_step, sizeof(int), cudaMemcpyDeviceToHost));
+    *n_collected = step > ctx->stat_start ? step - ctx->stat_start : 0;
+  }
   return OSTC_OK;
 }
 

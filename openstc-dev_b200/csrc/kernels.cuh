@@ -129,6 +129,25 @@ cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, do
                               long long *stats, const int *count, cudaStream_t s);
 cudaError_t prepare_chem_surrogate();
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s);
+
+// per-step epilogues (epilogue.cu): step count and physical time, monitor
+// points, statistics sums
+struct MonitorSet {
+  int n = 0, nbv = 0, nsv = 0, cap = 0;
+  int4 *pts = nullptr;       // {block, i, j, k} per point
+  int *labels = nullptr;     // nbv bv planes, then nsv sv planes
+  double *data = nullptr;    // [n][cap][nbv + nsv + 1]
+  int *counter = nullptr;    // records since the last read (ring position = counter % cap)
+  const double *time = nullptr;
+};
+struct StatSums {
+  double *s12 = nullptr, *s34 = nullptr, *srs = nullptr, *syk = nullptr;  // 12, 12, 3, n_spec interior planes
+};
+cudaError_t launch_step_clock(int *step, double *time, const double *dt_dev, double dt_fixed, cudaStream_t s);
+cudaError_t launch_monitor(const DevZone &z, int blk, const MonitorSet &m, cudaStream_t s);
+cudaError_t launch_monitor_advance(int *counter, cudaStream_t s);
+cudaError_t launch_statistics(const DevZone &z, const int *step, int start, const StatSums &st, int ns,
+                              cudaStream_t s);
 // 2-D blocks: copy the plane k = 0 into every k ghost plane (no-op when mz > 1)
 cudaError_t launch_eliminate_k(const DevZone &z, int with_cv, cudaStream_t s);
 cudaError_t upload_param(const DevParam &p, cudaStream_t s);

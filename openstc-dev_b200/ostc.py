@@ -107,6 +107,7 @@ def lib():
             raise RuntimeError("libostc.so is missing at %s: run __graft_entry__.build() (no CPU fallback)" % LIB_PATH)
         L = C.CDLL(str(LIB_PATH))
         vp, i, d = C.c_void_p, C.c_int, C.c_double
+        dp, ip = C.POINTER(d), C.POINTER(i)
         sig = {
             "ostc_create": [C.POINTER(Config), C.POINTER(Param), C.POINTER(Zone), i, C.POINTER(BcFaceC), i,
                             C.POINTER(vp)],
@@ -119,6 +120,11 @@ def lib():
             "ostc_data_communication": [vp, i, vp],
             "ostc_update_physical_properties": [vp, vp],
             "ostc_eliminate_k_gradient": [vp, i, vp],
+            "ostc_physical_time": [vp, dp, ip],
+            "ostc_set_monitor": [vp, i, ip, ip, ip, ip, i, ip, i, ip, i],
+            "ostc_get_monitor": [vp, dp, ip],
+            "ostc_set_statistics": [vp, i, i],
+            "ostc_get_statistics": [vp, i, dp, dp, dp, dp, ip],
             "ostc_initialize": [vp, vp],
             "ostc_rk3_stage": [vp, i, vp],
             "ostc_rk3_steps": [vp, i, C.POINTER(d), C.POINTER(d), vp],
@@ -540,6 +546,53 @@ class Solver:
     def eliminate_k_gradient(self, with_cv: bool):
         """2-D blocks: the k ghost planes take the plane k = 0 (a no-op in 3-D)"""
         check(lib().ostc_eliminate_k_gradient(self.ctx, int(with_cv), self._s()), "ostc_eliminate_k_gradient")
+
+    def physical_time(self):
+        """(physical time, step count) of the RK3 loop since initialize"""
+        t, n = C.c_double(), C.c_int()
+        check(lib().ostc_physical_time(self.ctx, C.byref(t), C.byref(n)), "ostc_physical_time")
+        return t.value, n.value
+
+    def set_monitor(self, points, bv_labels=(0, 1, 2, 3, 4, 5), sv_labels=(), capacity=64):
+        """monitor points [(block, i, j, k), ...]; [] removes the monitor"""
+        n = len(points)
+        cols = [np.ascontiguousarray([p[c] for p in points], dtype=np.int32) for c in range(4)] if n else [
+            np.zeros(1, np.int32)] * 4
+        bl = np.ascontiguousarray(bv_labels, dtype=np.int32)
+        sl = np.ascontiguousarray(sv_labels, dtype=np.int32)
+        ip = C.POINTER(C.c_int)
+        check(lib().ostc_set_monitor(self.ctx, n, *[c.ctypes.data_as(ip) for c in cols], len(bl),
+                                     bl.ctypes.data_as(ip) if len(bl) else None, len(sl),
+                                     sl.ctypes.data_as(ip) if len(sl) else None, capacity), "ostc_set_monitor")
+        self._monitor = (n, len(bl) + len(sl) + 1, capacity)
+
+    def get_monitor(self):
+        """records since the last read: array [point][step][bv labels, sv labels, time]"""
+        n, nv, cap = getattr(self, "_monitor", (0, 0, 0))
+        out = np.zeros((max(n, 1), cap, nv))
+        rec = C.c_int()
+        check(lib().ostc_get_monitor(self.ctx, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(rec)),
+              "ostc_get_monitor")
+        return out[:n, :rec.value]
+
+    def set_statistics(self, on=True, start_step=0):
+        check(lib().ostc_set_statistics(self.ctx, int(bool(on)), start_step), "ostc_set_statistics")
+
+    def get_statistics(self, block=0):
+        """per-cell sums of one block (interior): sum12 [12], sum34 [12], sum_rs [3], sum_yk [n_spec], count"""
+        b = self.blocks[block]
+        shape = (b.mz, b.my, b.mx)
+        ns = self.param.n_spec
+        out = {"sum12": np.zeros((12,) + shape), "sum34": np.zeros((12,) + shape), "sum_rs": np.zeros((3,) + shape),
+               "sum_yk": np.zeros((max(ns, 1),) + shape)}
+        dp = C.POINTER(C.c_double)
+        cnt = C.c_int()
+        check(lib().ostc_get_statistics(self.ctx, block, *[out[k].ctypes.data_as(dp) for k in
+                                                           ("sum12", "sum34", "sum_rs", "sum_yk")], C.byref(cnt)),
+              "ostc_get_statistics")
+        out["sum_yk"] = out["sum_yk"][:ns]
+        out["count"] = cnt.value
+        return out
 
     def rk3_stage(self, rk: int):
         check(lib().ostc_rk3_stage(self.ctx, rk, self._s()), "ostc_rk3_stage")
