@@ -261,6 +261,12 @@ ostc_status ostc_update_physical_properties(ostc_ctx *ctx, void *stream);
  * stage and step += 1 (both reset by ostc_initialize); this returns them
  * (synchronises the device; either pointer may be NULL).                   */
 ostc_status ostc_physical_time(ostc_ctx *ctx, double *time, int *step);
+/* Resuming a run from a checkpoint (the reference's restart: solution_time of
+ * the flow-field file, read_flowfield, Initialize.cuh:64-243, and the step of
+ * step.txt): after restoring bv / sv in the caller's arrays and calling
+ * ostc_initialize, sets the physical time and step count the following steps
+ * continue from.                                                           */
+ostc_status ostc_set_physical_time(ostc_ctx *ctx, double time, int step);
 
 /* Monitor points (Monitor.cu:196-251, record_monitor_data): after every step
  * the bv planes bv_label[0..n_bv) (0 rho, 1 u, 2 v, 3 w, 4 p, 5 T) and the sv

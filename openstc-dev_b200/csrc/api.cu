@@ -1312,6 +1312,14 @@ ostc_status ostc_physical_time(ostc_ctx *ctx, double *time, int *step) {
   return OSTC_OK;
 }
 
+ostc_status ostc_set_physical_time(ostc_ctx *ctx, double time, int step) {
+  if (!ctx || step < 0 || !(time >= 0)) return OSTC_ERR_INVALID_ARG;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(ctx->ep_time, &time, sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->ep_step, &step, sizeof(int), cudaMemcpyHostToDevice));
+  return OSTC_OK;
+}
+
 ostc_status ostc_set_statistics(ostc_ctx *ctx, int on, int start_step) {
   if (!ctx || (on != 0 && on != 1) || start_step < 0) return OSTC_ERR_INVALID_ARG;
   CK(cudaDeviceSynchronize());

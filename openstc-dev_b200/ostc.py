@@ -121,6 +121,7 @@ def lib():
             "ostc_update_physical_properties": [vp, vp],
             "ostc_eliminate_k_gradient": [vp, i, vp],
             "ostc_physical_time": [vp, dp, ip],
+            "ostc_set_physical_time": [vp, d, i],
             "ostc_set_monitor": [vp, i, ip, ip, ip, ip, i, ip, i, ip, i],
             "ostc_get_monitor": [vp, dp, ip],
             "ostc_set_statistics": [vp, i, i],
@@ -552,6 +553,10 @@ class Solver:
         t, n = C.c_double(), C.c_int()
         check(lib().ostc_physical_time(self.ctx, C.byref(t), C.byref(n)), "ostc_physical_time")
         return t.value, n.value
+
+    def set_physical_time(self, time: float, step: int):
+        """continue a restarted run from (time, step) (call after initialize)"""
+        check(lib().ostc_set_physical_time(self.ctx, float(time), int(step)), "ostc_set_physical_time")
 
     def set_monitor(self, points, bv_labels=(0, 1, 2, 3, 4, 5), sv_labels=(), capacity=64):
         """monitor points [(block, i, j, k), ...]; [] removes the monitor"""
