@@ -38,6 +38,7 @@ def planar_cases():
         "subsonic": lambda: ostc.case_bc_box("subsonic", 25, 21, 1),
         "mixing_h2air": lambda: ostc.case_mixing_layer(25, 21, 1, full_host=True),
         "sst_wall": lambda: planar_sst(),
+        "sst_h2air_wall": lambda: ostc.case_mixing_layer(25, 21, 1, full_host=True, rans_model=2, wall=True),
     }
 
 

@@ -16,8 +16,8 @@ from planar_cases import extrude, k_plane, planar_cases, with_fixed_dt
 pytestmark = pytest.mark.gpu
 
 NAMES = list(planar_cases())
-EQUIVALENT = [n for n in NAMES if n not in ("vortex_muscl_roe", "vortex_aweno", "sst_wall")]
-DT = {"mixing_h2air": 5e-9, "sst_wall": 1e-8}
+EQUIVALENT = [n for n in NAMES if n not in ("vortex_muscl_roe", "vortex_aweno", "sst_wall", "sst_h2air_wall")]
+DT = {"mixing_h2air": 5e-9, "sst_wall": 1e-8, "sst_h2air_wall": 5e-9}
 
 
 def _errors(got, ref):
@@ -180,7 +180,7 @@ def test_planar_matches_reference_build(name):
 
 
 @pytest.mark.parametrize("name,implicit_method", [("wall_farfield", 0), ("wall_farfield", 1), ("sst_wall", 0),
-                                                  ("sst_wall", 1), ("mixing_h2air", 1)])
+                                                  ("sst_wall", 1), ("mixing_h2air", 1), ("sst_h2air_wall", 1)])
 def test_planar_steady(name, implicit_method):
     """the steady path on 2-D blocks (SteadySim.cuh:51-126 with its
     eliminate_k_gradient, DPLUR without k neighbours): 4 iterations against
