@@ -40,8 +40,10 @@ def _args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mixing256", choices=["mixing256", "vortex128", "mixing96", "blocks37"],
-                    help="mixing96: the 96^3 mixing layer the kernel profiles are captured on")
+    ap.add_argument("--workload", default="mixing256",
+                    choices=["mixing256", "vortex128", "mixing96", "blocks37", "mixing512"],
+                    help="mixing96: the 96^3 mixing layer the kernel profiles are captured on; "
+                         "mixing512: the 512x256x256 layer of the learned-chemistry configuration")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-refcuda", action="store_true")
@@ -66,6 +68,8 @@ def _make_case(name, full_host=False):
 
     if name == "mixing256":
         return ostc.case_mixing_layer(256, 256, 256, full_host=full_host)
+    if name == "mixing512":
+        return ostc.case_mixing_layer(512, 256, 256, full_host=full_host)
     if name == "mixing96":
         return ostc.case_mixing_layer(96, 96, 96, full_host=full_host)
     if name == "blocks37":
@@ -605,6 +609,7 @@ def run_reference(a):
 
 def _make_case_name(w):
     return {"mixing256": "mixing_layer_h2air_256x256x256", "mixing96": "mixing_layer_h2air_96x96x96",
+            "mixing512": "mixing_layer_h2air_512x256x256",
             "blocks37": "uneven_blocks_37_air_sst_10453312cells"}.get(w, "vortex_air_128x128x8")
 
 
