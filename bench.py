@@ -77,9 +77,7 @@ def _make_case(name, full_host=False):
     return ostc.case_vortex(128, 128, 8)
 
 
-def _scheme_text(case):
-    import ostc
-
+def _scheme_text(case, n_blocks=None):
     sc = case.scheme
     rec = {1: "first order", 2: "MUSCL(minmod)", 3: "NND2", 4: "AWENO5"}[sc.reconstruction]
     inv = {1: "L-F", 2: "Roe", 3: "AUSM+", 4: "HLLC"}[sc.inviscid_scheme]
@@ -87,7 +85,8 @@ def _scheme_text(case):
         inv = "AUSM+"  # quirk A1
     vis = ("k-omega SST" if sc.rans_model == 2 else "laminar") if sc.viscous_order else "inviscid"
     chem = ", finite-rate chemistry" if case.mech is not None else ""
-    blocks = ", %d blocks" % len(case.blocks) if len(case.blocks) > 1 else ""
+    nb = len(case.blocks) if n_blocks is None else n_blocks
+    blocks = ", %d blocks" % nb if nb > 1 else ""
     return "%s+%s, %s%s, SSPRK3 CFL %.1f%s" % (rec, inv, vis, chem, sc.cfl, blocks)
 
 
@@ -352,14 +351,7 @@ def run_ours(a):
                 "unit": "Mcell-updates/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
                 "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": case.name, "cells_per_gpu": cells,
-                           "n_spec": case.mech.n_spec if case.mech else 0,
-                           "n_reac": case.mech.n_reac if case.mech else 0,
-                           "scheme": _scheme_text(case),
-                           "parallelism": "replicas" if world > 1 else "single",
-                           "l2": ("state %.2f GB below 2x L2: L2 flushed (%d MB written) before each step, steps "
-                                  "timed one by one" % (state_bytes(case) / 1e9, 2 * L2_BYTES >> 20)) if small else
-                                 "inputs larger than L2 (%.1f GB state), no flush" % (state_bytes(case) / 1e9)},
+                "config": workload_config(a, world, case),
                 "gpu_launches": launches_per_step * a.steps, "launches_per_step": launches_per_step,
                 "tiles": tiles,
                 "clocks": ck, "roofline": roofline, "step_roofline": step_roofline, "kernels_ms": {k: round(v["ms"], 4) for k, v in ktab.items()},
@@ -459,10 +451,14 @@ def step_bytes_per_cell(case):
 
 
 def state_bytes(case):
+    return state_bytes_dims(case, [(b.mx, b.my, b.mz) for b in case.blocks], case.blocks[0].ngg)
+
+
+def state_bytes_dims(case, dims, ngg):
     ns = case.mech.n_spec if case.mech else 0
     nt = 2 if case.scheme.rans_model == 2 else 0
-    return sum(8.0 * (6 + ns + nt + 10 + 2 * (5 + ns + nt)) * (b.mx + 2 * b.ngg) * (b.my + 2 * b.ngg) *
-               (b.mz + 2 * b.ngg) for b in case.blocks)
+    return sum(8.0 * (6 + ns + nt + 10 + 2 * (5 + ns + nt)) * (x + 2 * ngg) * (y + 2 * ngg) * (z + 2 * ngg)
+               for x, y, z in dims)
 
 
 def run_e2e(a, case, tiles=None):
@@ -507,47 +503,49 @@ def run_e2e(a, case, tiles=None):
 
 
 # ---------------------------------------------------------------------------
-# CPU legs (oracle port / reference host build)
+# CPU legs (the oracle port on the host cores) and the reference's CUDA build
 # ---------------------------------------------------------------------------
-def _cpu_engine():
-    sys.path.insert(0, str(REPO / "tests"))
-    ref = REPO / "oracle" / "_ref" / "libostc_ref.so"
-    if ref.exists():
-        import ref_bind
-
-        return "reference", ref_bind.RefRun
-    from oracle_bind import OracleRun
-
-    return "port", OracleRun
-
-
-def cpu_sample(a, budget_s=15.0):
-    """Time the CPU implementation on a bounded sample of the workload: the
-    same case at 64^3 (or the full air case), stepping until ~budget_s."""
+def _cpu_case(w):
+    """The bounded CPU sample of workload w and its description. The mixing
+    layers are sampled by a 256 x 256 x 8 slab of the same layer (same x-y
+    extent, tanh profiles, stream states and noise distribution; z periodic
+    as in the full case), so the per-cell work is the full case's."""
     import ostc
 
-    kind, Run = _cpu_engine()
-    if a.workload == "mixing256":
-        case = ostc.case_mixing_layer(64, 64, 64, full_host=True)
-    elif a.workload == "blocks37":
+    if w in ("mixing256", "mixing512", "mixing96"):
+        nx = {"mixing256": 256, "mixing512": 512, "mixing96": 96}[w]
+        ny = 96 if w == "mixing96" else 256
+        case = ostc.case_mixing_layer(nx, ny, 8, full_host=True)
+        return case, "%dx%dx8 slab of the layer (%d cells)" % (nx, ny, case.cells)
+    if w == "blocks37":
         case = ostc.case_uneven_blocks(layout=ostc.block_layout(5, dims=(80, 64, 64), ranges=((16, 40), (16, 28),
                                                                                               (16, 20)),
                                                                 anchors=False), rans_model=2)
-    else:
-        case = ostc.case_vortex(128, 128, 8)
-    r = Run(case)
+        return case, "5 uneven SST blocks (%d cells) of the same scheme" % case.cells
+    case = ostc.case_vortex(128, 128, 8)
+    return case, "the whole 128x128x8 case"
+
+
+def cpu_sample(a, budget_s=15.0, max_steps=50):
+    """Time the oracle port (the CPU restatement of the reference's path,
+    OpenMP over all host cores) on the bounded sample of the workload,
+    stepping RK3 until ~budget_s."""
+    sys.path.insert(0, str(REPO / "tests"))
+    from oracle_bind import OracleRun
+
+    case, what = _cpu_case(a.workload)
+    r = OracleRun(case)
     r.initialize()
-    threads = r.threads() if hasattr(r, "threads") else 1
     steps, t0 = 0, time.perf_counter()
     while True:
         r.rk3_steps(1)
         steps += 1
         el = time.perf_counter() - t0
-        if el >= budget_s or steps >= 50:
+        if el >= budget_s or steps >= max_steps:
             break
     value = case.cells * steps / el / 1e6
-    return {"value": round(value, 4), "unit": "Mcell-updates/s", "cores": threads, "kind": kind,
-            "sample": "%s, %d RK3 steps, %.1f s" % (case.name, steps, el)}
+    return {"value": round(value, 4), "unit": "Mcell-updates/s", "cores": r.threads(), "kind": "port",
+            "sample": "%s, %d RK3 steps, %.1f s" % (what, steps, el)}
 
 
 def cpu_baseline(a):
@@ -557,8 +555,9 @@ def cpu_baseline(a):
 def reference_cuda_build(a, ours_value):
     """The reference's own kernels (sources compiled for sm_100a, driven by
     oracle/ref_cuda_harness.cu through RK3_bv's per-step sequence) on the same
-    workload, timed with CUDA events; periodic faces become extrapolation
-    faces since the reference has no periodic boundary."""
+    workload, timed with CUDA events: 10 warm-up steps, then the median of 3
+    runs of 5 steps. Periodic faces become extrapolation faces since the
+    reference has no periodic boundary."""
     sys.path.insert(0, str(REPO / "tests"))
     import ref_bind
 
@@ -574,35 +573,93 @@ def reference_cuda_build(a, ours_value):
             f.type_label = ostc.BC_OUTFLOW
     r = ref_bind.RefCudaRun(case)
     r.initialize()
-    r.time_steps(1)
-    n = 3
-    ms = r.time_steps(n)
-    v = case.cells * n / (ms * 1e-3) / 1e6
-    return {"value": round(v, 2), "unit": "Mcell-updates/s", "steps": n, "ms_per_step": round(ms / n, 3),
+    r.time_steps(10)
+    n, runs = 5, []
+    for _ in range(3):
+        runs.append(r.time_steps(n) / n)
+    ms = sorted(runs)[1]
+    v = case.cells / (ms * 1e-3) / 1e6
+    return {"value": round(v, 2), "unit": "Mcell-updates/s", "ms_per_step": round(ms, 3),
+            "protocol": "10 warm-up steps, median of 3 runs of 5 steps (CUDA events)",
+            "runs_ms_per_step": [round(x, 3) for x in runs],
             "speedup_ours_over_reference_build": round(ours_value / v, 2),
             "note": "reference sources compiled for sm_100a, same workload, extrapolation faces instead of periodic"
                     " (and of the SST far field)"}
 
 
+def workload_config(a, world, case=None, sample=None):
+    """The `config` object of a bench line: the same for both arms (the
+    reference arm describes the workload from its bounded sample without
+    building it at full size)."""
+    if case is None:
+        small = sample if sample is not None else _cpu_case(a.workload)[0]
+        if a.workload == "blocks37":
+            small = _make_case(a.workload)
+        dims = {"mixing256": [(256, 256, 256)], "mixing512": [(512, 256, 256)], "mixing96": [(96, 96, 96)],
+                "vortex128": [(128, 128, 8)]}.get(a.workload, [(b.mx, b.my, b.mz) for b in small.blocks])
+        ng = small.blocks[0].ngg
+        info = dict(name=_make_case_name(a.workload), mech=small.mech, scheme_case=small,
+                    cells=sum(x * y * z for x, y, z in dims), dims=dims, ngg=ng)
+    else:
+        info = dict(name=case.name, mech=case.mech, scheme_case=case, cells=case.cells,
+                    dims=[(b.mx, b.my, b.mz) for b in case.blocks], ngg=case.blocks[0].ngg)
+    sb = state_bytes_dims(info["scheme_case"], info["dims"], info["ngg"])
+    small_state = sb < 2 * L2_BYTES
+    return {"workload": info["name"], "cells_per_gpu": info["cells"],
+            "n_spec": info["mech"].n_spec if info["mech"] else 0,
+            "n_reac": info["mech"].n_reac if info["mech"] else 0,
+            "scheme": _scheme_text(info["scheme_case"], n_blocks=len(info["dims"])),
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": ("state %.2f GB below 2x L2: L2 flushed (%d MB written) before each step, steps timed one by "
+                   "one" % (sb / 1e9, 2 * L2_BYTES >> 20)) if small_state else
+                  "inputs larger than L2 (%.1f GB state), no flush" % (sb / 1e9)}
+
+
+def _libostc_mapped():
+    try:
+        return any("libostc.so" in ln for ln in open("/proc/self/maps"))
+    except OSError:
+        return False
+
+
 def run_reference(a):
+    """The reference arm: the CPU implementation of the path (the oracle
+    port, a cited FP64 restatement of the reference's kernels; the reference
+    itself has no CPU code) on all host cores. Each timed step is one RK3
+    step of the bounded sample of the workload. The product library is never
+    loaded: the workloads' geometry comes from the numpy restatement of the
+    reference's metric (oracle/metric_oracle.py)."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    samples = []
-    vals = []
-    for _ in range(max(1, min(a.steps, 3))):
-        c = cpu_sample(a, budget_s=20.0)
-        vals.append(c["value"])
-        samples.append(c)
-    value = sorted(vals)[len(vals) // 2]
-    c = samples[0]
+    sys.path.insert(0, str(REPO / "oracle"))
+    sys.path.insert(0, str(REPO / "tests"))
+    import metric_oracle
+    import ostc
+    from oracle_bind import OracleRun
+
+    ostc.set_metric_provider(metric_oracle.metric)
+    case, what = _cpu_case(a.workload)
+    r = OracleRun(case)
+    r.initialize()
+    for _ in range(a.warmup):
+        r.rk3_steps(1)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        r.rk3_steps(1)
+    el = time.perf_counter() - t0
+    value = round(case.cells * a.steps / el / 1e6, 4)
+    sample = "%s, %d timed RK3 steps after %d warm-up, %.1f s" % (what, a.steps, a.warmup, el)
+    assert not _libostc_mapped(), "the reference arm must not load the product library"
     line = {"impl": "reference", "metric": "Mcell-updates/s per RK3 step (plain FP64 chemistry)", "value": value,
-            "unit": "Mcell-updates/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": a.steps,
-            "warmup": a.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": _make_case_name(a.workload), "sample": c["sample"]},
-            "cpu_baseline": {"value": value, "unit": c["unit"], "cores": c["cores"], "kind": c["kind"],
-                             "sample": c["sample"]},
+            "unit": "Mcell-updates/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(el * 1e3 / a.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(a, world, sample=case),
+            "sample": sample,
+            "cpu_baseline": {"value": value, "unit": "Mcell-updates/s", "cores": r.threads(), "kind": "port",
+                             "sample": sample},
             "e2e": {"value": value, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 

@@ -290,7 +290,9 @@ ostc_status ostc_get_monitor(ostc_ctx *ctx, double *out, int *n_recorded);
  * fractions (n_spec planes). on = 0 frees them. Resets the cached graphs.   */
 ostc_status ostc_set_statistics(ostc_ctx *ctx, int on, int start_step);
 /* The sums of one block to HOST arrays (each may be NULL; interior layout,
- * g = 0) and the number of steps summed. Synchronises the device.          */
+ * g = 0) and the number of samples summed into them (counted on the device,
+ * so it stays exact when ostc_set_physical_time moves the step count after
+ * statistics were switched on). Synchronises the device.                  */
 ostc_status ostc_get_statistics(ostc_ctx *ctx, int block, double *sum12, double *sum34, double *sum_rs,
                                 double *sum_yk, int *n_collected);
 
@@ -325,7 +327,13 @@ ostc_status ostc_rk3_stage(ostc_ctx *ctx, int rk, void *stream);
  * src/RK.cuh:89-170), captured once as a CUDA graph and replayed.
  * If res_hist is non-NULL it receives 4 doubles per step (the RMS change of
  * rho, |V|, p, T, src/Residual.cuh:57-161, unnormalised) and dt_hist one dt
- * per step; both synchronise the stream at the end.                        */
+ * per step; both synchronise the stream at the end. With either history the
+ * residual epilogue also checks the state of every interior cell after each
+ * step (the reference stops on a NaN residual, src/Residual.cuh:153-158):
+ * a non-positive or NaN density or pressure, or a NaN residual term, makes
+ * the call return OSTC_ERR_NONPHYSICAL after all n_steps, and ostc_get_error
+ * reports the first such cell (earliest step, then lowest block, then lowest
+ * k, j, i). The histories are still written.                              */
 ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist,
                            double *dt_hist, void *stream);
 
@@ -356,7 +364,8 @@ ostc_status ostc_update_bv(ostc_ctx *ctx, void *stream);
 /* n_steps steady iterations (the loop body of steady_simulation,
  * src/SteadySim.cuh:51-126: RHS, local dt, implicit treatment, update_bv,
  * BCs and interfaces without cv, properties), captured as a CUDA graph.
- * res_hist as for ostc_rk3_steps; the caller tests convergence on it.      */
+ * res_hist and the state check as for ostc_rk3_steps; the caller tests
+ * convergence on res_hist.                                                 */
 ostc_status ostc_steady_steps(ostc_ctx *ctx, int n_steps, double *res_hist, void *stream);
 
 /* ---- FP64 point-implicit chemistry integrator -------------------------- */
@@ -441,6 +450,17 @@ ostc_status ostc_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur, int n, const
                                 const double *Y, const double *dt, double *dY, double *dT, int *n_fallback,
                                 void *stream);
 
+/* Diagnostic of the timeout path, for callers that test their error
+ * handling: with on = 1 the tensor-core kernels launched afterwards for s
+ * (ostc_surrogate_forward_tc, ostc_chem_surrogate) withhold the completion
+ * signal of their first matrix product, so their bounded wait for it runs
+ * out after about one second and the call returns OSTC_ERR_TIMEOUT. The
+ * kernels still drain their in-flight work and free their tensor memory, so
+ * the device stays usable; on = 0 restores normal operation. Steps captured
+ * in graphs before the call keep the setting they were captured with.
+ * No reference counterpart.                                                */
+ostc_status ostc_surrogate_inject_timeout(ostc_surrogate *s, int on);
+
 /* The surrogate used by chem_mode 2 (the context keeps the pointer; the
  * surrogate must outlive it). Resets the cached step graphs.               */
 ostc_status ostc_set_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur);
@@ -524,9 +544,12 @@ ostc_status ostc_step_kernel_count(ostc_ctx *ctx, int with_hist, int *count);
  * library's own device memory (OSTC_NOALLOC_MAX_PARTIALS x 4 doubles =
  * 512 KiB, held on every GPU that loads the library until exit); blocks of
  * more than OSTC_NOALLOC_MAX_CELLS cells are rejected with
- * OSTC_ERR_INVALID_ARG. The first call on a device looks up the array's
- * address, so make that first call before any stream capture. All calls
- * share the array: calls that overlap on the GPU race.                     */
+ * OSTC_ERR_INVALID_ARG. Every call made outside a stream capture looks up the
+ * array's address on the current device; a call made while its stream is
+ * being captured uses the address found by the last such call and returns
+ * OSTC_ERR_INVALID_ARG when there was none, so make a first call on each
+ * device before any capture. All calls share the array: calls that overlap
+ * on the GPU race.                                                         */
 #define OSTC_NOALLOC_MAX_PARTIALS 16384
 #define OSTC_NOALLOC_MAX_CELLS (OSTC_NOALLOC_MAX_PARTIALS * 2048LL)
 ostc_status ostc_compute_residual_noalloc(const ostc_zone *zone, double *res_out, void *stream);

@@ -52,6 +52,9 @@ struct ostc_ctx {
   double *hist_res = nullptr, *hist_dt = nullptr;  // device history buffers
   int *hist_counter = nullptr;
   int hist_cap = 0;
+  // state check of the residual epilogue: key of the first non-physical cell
+  // (step of the call << 44 | zone << 34 | interior cell index), all ones when none
+  unsigned long long *bad_key = nullptr;
   double n_total = 0;
   std::map<int, GraphEntry> graphs;  // key: with_residual (+2 for the steady step)
   // per-step epilogues of the RK3 loop: step count and physical time (one int, one
@@ -73,7 +76,7 @@ struct ostc_ctx {
   long long max_cells = 0;
   ostc_status last = OSTC_OK;
   int last_cuda = 0;
-  int err_block = -1, err_i = 0, err_j = 0, err_k = 0;
+  int err_block = -1, err_i = 0, err_j = 0, err_k = 0, err_step = -1;
 };
 
 namespace {
@@ -618,6 +621,7 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
   c->n_part_per_zone = 148 * 2;
   CK(cudaMalloc(&c->res_partial, sizeof(double) * 4 * c->n_part_per_zone * n_zones));
   CK(cudaMalloc(&c->hist_counter, sizeof(int)));
+  CK(cudaMalloc(&c->bad_key, sizeof(unsigned long long)));
   CK(cudaMalloc(&c->ep_step, sizeof(int)));
   CK(cudaMalloc(&c->ep_time, sizeof(double)));
   CK(cudaMemset(c->ep_step, 0, sizeof(int)));
@@ -646,6 +650,7 @@ ostc_status ostc_destroy(ostc_ctx *ctx) {
   cudaFree(ctx->tab_dev);
   cudaFree(ctx->res_partial);
   cudaFree(ctx->hist_counter);
+  cudaFree(ctx->bad_key);
   cudaFree(ctx->hist_res);
   cudaFree(ctx->hist_dt);
   cudaFree(ctx->ep_step);
@@ -654,7 +659,10 @@ ostc_status ostc_destroy(ostc_ctx *ctx) {
   cudaFree(ctx->mon.labels);
   cudaFree(ctx->mon.data);
   cudaFree(ctx->mon.counter);
-  for (auto &st : ctx->stats) cudaFree(st.s12);
+  for (auto &st : ctx->stats) {
+    cudaFree(st.s12);
+    cudaFree(st.count);
+  }
   if (g_uploaded == ctx) g_uploaded = nullptr;
   delete ctx;
   return OSTC_OK;
@@ -911,8 +919,11 @@ static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
   if (with_hist) {
     CellArgs a;
     a.n_part = ctx->n_part_per_zone;
+    a.bad = ctx->bad_key;
+    a.step = ctx->hist_counter;
     for (size_t b = 0; b < ctx->dz.size(); ++b) {
       a.partial = ctx->res_partial + 4 * ctx->n_part_per_zone * b;
+      a.block = (int)b;
       CK(launch_cells<0>(CellOp::ResidualPartial, ctx->dz[b], a, s));
     }
     step_end_kernel<<<1, 32, 0, s>>>(ctx->res_partial, ctx->n_part_per_zone * (int)ctx->dz.size(), ctx->n_total,
@@ -964,13 +975,37 @@ static ostc_status ensure_graph(ostc_ctx *ctx, bool hist, GraphEntry **out, bool
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);
-    if (st) return st;
-    CK(e);
-    CK(cudaGraphInstantiate(&ge.exec, g, 0));
+    if (st != OSTC_OK || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return st != OSTC_OK ? st : fail(ctx, OSTC_ERR_CUDA, e);
+    }
+    e = cudaGraphInstantiate(&ge.exec, g, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      ge.exec = nullptr;
+      return fail(ctx, OSTC_ERR_CUDA, e);
+    }
     ge.graph = g;
   }
   *out = &ge;
   return OSTC_OK;
+}
+
+// after a synchronised call with histories: the first non-physical cell found by
+// the residual epilogue, if any, becomes OSTC_ERR_NONPHYSICAL with its zone and
+// cell (ostc_get_error) and the step of the call it was found in (err_step)
+static ostc_status check_state(ostc_ctx *ctx, unsigned long long key) {
+  if (key == ~0ull) return OSTC_OK;
+  const long long q = (long long)(key & ((1ull << 34) - 1));
+  const int b = (int)((key >> 34) & 1023);
+  if (b >= (int)ctx->dz.size()) return fail(ctx, OSTC_ERR_NONPHYSICAL);
+  const DevZone &z = ctx->dz[b];
+  ctx->err_block = b;
+  ctx->err_i = (int)(q % z.mx);
+  ctx->err_j = (int)((q / z.mx) % z.my);
+  ctx->err_k = (int)(q / ((long long)z.mx * z.my));
+  ctx->err_step = (int)(key >> 44);
+  return fail(ctx, OSTC_ERR_NONPHYSICAL);
 }
 
 ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist, double *dt_hist, void *stream) {
@@ -982,13 +1017,17 @@ ostc_status ostc_rk3_steps(ostc_ctx *ctx, int n_steps, double *res_hist, double 
   if (hist && (st = ensure_hist(ctx, n_steps))) return st;
   if (ensure_param(ctx, s)) return ctx->last;
   if (hist) CK(cudaMemsetAsync(ctx->hist_counter, 0, sizeof(int), s));
+  if (hist) CK(cudaMemsetAsync(ctx->bad_key, 0xff, sizeof(unsigned long long), s));
   GraphEntry *ge = nullptr;
   if ((st = ensure_graph(ctx, hist, &ge))) return st;
   for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(ge->exec, s));
   if (hist) {
+    unsigned long long key = ~0ull;
     if (res_hist) CK(cudaMemcpyAsync(res_hist, ctx->hist_res, sizeof(double) * 4 * n_steps, cudaMemcpyDeviceToHost, s));
     if (dt_hist) CK(cudaMemcpyAsync(dt_hist, ctx->hist_dt, sizeof(double) * n_steps, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&key, ctx->bad_key, sizeof(key), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    return check_state(ctx, key);
   }
   return OSTC_OK;
 }
@@ -1077,8 +1116,11 @@ static ostc_status enqueue_steady_step(ostc_ctx *ctx, bool with_hist, cudaStream
   if (with_hist) {
     CellArgs a;
     a.n_part = ctx->n_part_per_zone;
+    a.bad = ctx->bad_key;
+    a.step = ctx->hist_counter;
     for (size_t b = 0; b < ctx->dz.size(); ++b) {
       a.partial = ctx->res_partial + 4 * ctx->n_part_per_zone * b;
+      a.block = (int)b;
       CK(launch_cells<0>(CellOp::ResidualPartial, ctx->dz[b], a, s));
     }
     step_end_kernel<<<1, 32, 0, s>>>(ctx->res_partial, ctx->n_part_per_zone * (int)ctx->dz.size(), ctx->n_total,
@@ -1096,12 +1138,16 @@ ostc_status ostc_steady_steps(ostc_ctx *ctx, int n_steps, double *res_hist, void
   if (hist && (st = ensure_hist(ctx, n_steps))) return st;
   if (ensure_param(ctx, s)) return ctx->last;
   if (hist) CK(cudaMemsetAsync(ctx->hist_counter, 0, sizeof(int), s));
+  if (hist) CK(cudaMemsetAsync(ctx->bad_key, 0xff, sizeof(unsigned long long), s));
   GraphEntry *ge = nullptr;
   if ((st = ensure_graph(ctx, hist, &ge, true))) return st;
   for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(ge->exec, s));
   if (hist) {
+    unsigned long long key = ~0ull;
     CK(cudaMemcpyAsync(res_hist, ctx->hist_res, sizeof(double) * 4 * n_steps, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&key, ctx->bad_key, sizeof(key), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    return check_state(ctx, key);
   }
   return OSTC_OK;
 }
@@ -1323,7 +1369,10 @@ ostc_status ostc_set_physical_time(ostc_ctx *ctx, double time, int step) {
 ostc_status ostc_set_statistics(ostc_ctx *ctx, int on, int start_step) {
   if (!ctx || (on != 0 && on != 1) || start_step < 0) return OSTC_ERR_INVALID_ARG;
   CK(cudaDeviceSynchronize());
-  for (auto &st : ctx->stats) cudaFree(st.s12);
+  for (auto &st : ctx->stats) {
+    cudaFree(st.s12);
+    cudaFree(st.count);
+  }
   ctx->stats.clear();
   ctx->stat_on = 0;
   if (on) {
@@ -1333,6 +1382,8 @@ ostc_status ostc_set_statistics(ostc_ctx *ctx, int on, int start_step) {
       const size_t n = (size_t)z.nsz, planes = 27 + ns;
       CK(cudaMalloc(&st.s12, sizeof(double) * planes * n));
       CK(cudaMemset(st.s12, 0, sizeof(double) * planes * n));
+      CK(cudaMalloc(&st.count, sizeof(int)));
+      CK(cudaMemset(st.count, 0, sizeof(int)));
       st.s34 = st.s12 + 12 * n;
       st.srs = st.s34 + 12 * n;
       st.syk = st.srs + 3 * n;
@@ -1360,11 +1411,7 @@ ostc_status ostc_get_statistics(ostc_ctx *ctx, int block, double *sum12, double 
   if (sum_rs) CK(cudaMemcpy(sum_rs, st.srs, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
   if (sum_yk && ctx->prm.n_spec > 0)
     CK(cudaMemcpy(sum_yk, st.syk, sizeof(double) * ctx->prm.n_spec * n, cudaMemcpyDeviceToHost));
-  if (n_collected) {
-    int step = 0;
-    CK(cudaMemcpy(&step, ctx->ep_step, sizeof(int), cudaMemcpyDeviceToHost));
-    *n_collected = step > ctx->stat_start ? step - ctx->stat_start : 0;
-  }
+  if (n_collected) CK(cudaMemcpy(n_collected, st.count, sizeof(int), cudaMemcpyDeviceToHost));
   return OSTC_OK;
 }
 

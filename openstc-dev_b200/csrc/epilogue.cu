@@ -35,13 +35,16 @@ __global__ void counter_inc_kernel(int *c) { *c += 1; }
 
 // collect_basic_variable_statistics + collect_species_statistics over the
 // interior, once the step count has passed `start`: sums of bv, bv^2 (s12),
-// bv^3, bv^4 (s34), uv, uw, vw (srs) and Y_k (syk), interior planes
+// bv^3, bv^4 (s34), uv, uw, vw (srs) and Y_k (syk), interior planes; count
+// is the number of samples summed (the step count alone cannot tell it once
+// the clock was set back or forward by a restart)
 __global__ void __launch_bounds__(256) statistics_kernel(DevZone z, const int *step, int start, double *s12,
-                                                         double *s34, double *srs, double *syk, int ns) {
+                                                         double *s34, double *srs, double *syk, int ns, int *count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
   if (i >= z.mx || j >= z.my || *step <= start) return;
+  if (i == 0 && j == 0 && k == 0) *count += 1;
   const int g = gidx(z, i, j, k);
   const long long n = nidx(z, i, j, k), N = z.nsz;
 #pragma unroll
@@ -79,7 +82,7 @@ cudaError_t launch_monitor_advance(int *counter, cudaStream_t s) {
 cudaError_t launch_statistics(const DevZone &z, const int *step, int start, const StatSums &st, int ns,
                               cudaStream_t s) {
   const dim3 blk(32, 8), grid((z.mx + 31) / 32, (z.my + 7) / 8, z.mz);
-  statistics_kernel<<<grid, blk, 0, s>>>(z, step, start, st.s12, st.s34, st.srs, st.syk, ns);
+  statistics_kernel<<<grid, blk, 0, s>>>(z, step, start, st.s12, st.s34, st.srs, st.syk, ns, st.count);
   return cudaGetLastError();
 }
 

@@ -864,7 +864,14 @@ __global__ void store_last_kernel(DevZone z) {
 }
 
 // one partial sum of the 4 squared changes per CTA (256 threads, grid-stride)
-__global__ void __launch_bounds__(256) residual_partial_kernel(DevZone z, double *partial) {
+// bad (optional): the state check of the residual epilogue. The reference
+// stops when its residual is NaN (Residual.cuh:153-158); here every cell whose
+// density or pressure is not positive, or whose residual terms are NaN, offers
+// the key (step << 44 | block << 34 | interior cell index; the step of the
+// call, at most 2^20 - 1, and a block below 1024) to an atomic minimum, so the
+// host learns the first failing cell of the earliest step.
+__global__ void __launch_bounds__(256) residual_partial_kernel(DevZone z, double *partial, unsigned long long *bad,
+                                                               const int *step, int block) {
   const long long n = (long long)z.mx * z.my * z.mz;
   double s[4] = {0, 0, 0, 0};
   for (long long q = blockIdx.x * 256ll + threadIdx.x; q < n; q += 256ll * gridDim.x) {
@@ -876,6 +883,10 @@ __global__ void __launch_bounds__(256) residual_partial_kernel(DevZone z, double
     const double d1 = z.vel[g] - z.bv_last[z.nsz + q];
     const double d2 = z.bv[4 * z.sz + g] - z.bv_last[2 * z.nsz + q];
     const double d3 = z.bv[5 * z.sz + g] - z.bv_last[3 * z.nsz + q];
+    if (bad && !(z.bv[g] > 0 && z.bv[4 * z.sz + g] > 0 && d0 == d0 && d1 == d1 && d2 == d2 && d3 == d3)) {
+      const unsigned long long st = step ? (unsigned long long)min(*step, (1 << 20) - 1) : 0ull;
+      atomicMin(bad, (st << 44) | ((unsigned long long)(block & 1023) << 34) | (unsigned long long)q);
+    }
     s[0] += d0 * d0;
     s[1] += d1 * d1;
     s[2] += d2 * d2;
@@ -1048,7 +1059,7 @@ cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStr
       store_last_kernel<<<plane_grid(z.mx, z.my, z.mz, blk), blk, 0, s>>>(z);
       break;
     case CellOp::ResidualPartial:
-      residual_partial_kernel<<<a.n_part, 256, 0, s>>>(z, a.partial);
+      residual_partial_kernel<<<a.n_part, 256, 0, s>>>(z, a.partial, a.bad, a.step, a.block);
       break;
   }
   return cudaGetLastError();

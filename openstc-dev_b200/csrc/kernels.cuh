@@ -70,6 +70,9 @@ struct CellArgs {
   unsigned long long *dt_bits = nullptr;
   double *partial = nullptr;
   int n_part = 0;
+  unsigned long long *bad = nullptr;  // ResidualPartial: first non-physical cell (key, atomic minimum)
+  const int *step = nullptr;          // ResidualPartial: device step counter of the key
+  int block = 0;                      // ResidualPartial: zone index of the key
   int spec = 0;  // Source: use the mechanism-specialised chemistry
 };
 
@@ -142,6 +145,7 @@ struct MonitorSet {
 };
 struct StatSums {
   double *s12 = nullptr, *s34 = nullptr, *srs = nullptr, *syk = nullptr;  // 12, 12, 3, n_spec interior planes
+  int *count = nullptr;  // samples summed (device)
 };
 cudaError_t launch_step_clock(int *step, double *time, const double *dt_dev, double dt_fixed, cudaStream_t s);
 cudaError_t launch_monitor(const DevZone &z, int blk, const MonitorSet &m, cudaStream_t s);

@@ -534,6 +534,12 @@ ostc_status ostc_surrogate_set_checks(ostc_surrogate *s, int n_elem, int n_spec,
   return OSTC_OK;
 }
 
+ostc_status ostc_surrogate_inject_timeout(ostc_surrogate *s, int on) {
+  if (!s || (on != 0 && on != 1)) return OSTC_ERR_INVALID_ARG;
+  s->net.withhold_commit = on;
+  return OSTC_OK;
+}
+
 ostc_status ostc_surrogate_get_params(const ostc_surrogate *s, float *host_out) {
   if (!s || !host_out) return OSTC_ERR_INVALID_ARG;
   std::vector<float> pad(NPAR);

@@ -53,6 +53,7 @@ struct Net {
   __nv_bfloat16 *wb = nullptr;  // BF16 copy of every parameter (padded layout)
   float *wf = nullptr;          // FP32 master parameters (padded layout; biases are read from here)
   double *scale = nullptr;      // SCALE_COUNT doubles
+  int withhold_commit = 0;      // diagnostic (ostc_surrogate_inject_timeout): tensor-core waits run out
   __device__ __host__ const __nv_bfloat16 *w1() const { return wb + OFF_W1; }
   __device__ __host__ const __nv_bfloat16 *w2() const { return wb + OFF_W2; }
   __device__ __host__ const __nv_bfloat16 *w3() const { return wb + OFF_W3; }

@@ -14,6 +14,8 @@
 // the GPU (other streams, other host threads) race on it. Every slot a call
 // reads is written earlier in that same call, so no slot has to start at
 // zero and stale contents of a previous call are never read.
+#include <atomic>
+
 #include <cuda_runtime.h>
 
 #include "../../include/ostc.h"
@@ -26,8 +28,10 @@ constexpr int kCellsPerCta = kThreads * 8;  // each thread sums 8 cells
 // 16384 partials x 4 doubles = 512 KiB: room for 16384 * 2048 = 33,554,432 cells
 __device__ __align__(256) double g_residual_scratch[OSTC_NOALLOC_MAX_PARTIALS * 4];
 
-// device address of g_residual_scratch per device, looked up once per device
-double *g_scratch_addr[64] = {nullptr};
+// device address of g_residual_scratch per device: looked up again on every
+// call made outside a stream capture (so a context that was torn down and
+// re-created gets the new address), remembered for calls made during one
+std::atomic<double *> g_scratch_addr[64];
 
 struct Planes {
   const double *bv, *vel, *bv_last;
@@ -95,12 +99,19 @@ extern "C" ostc_status ostc_compute_residual_noalloc(const ostc_zone *zone, doub
   if (n_part > OSTC_NOALLOC_MAX_PARTIALS) return OSTC_ERR_INVALID_ARG;  // more than OSTC_NOALLOC_MAX_CELLS cells
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return OSTC_ERR_CUDA;
-  if (!g_scratch_addr[dev]) {
-    // first call on this device: look up the array's device address (host
-    // code may not use the symbol itself as a device pointer)
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) return OSTC_ERR_CUDA;
+  double *scratch = g_scratch_addr[dev].load();
+  if (cap == cudaStreamCaptureStatusNone) {
+    // look up the array's device address (host code may not use the symbol
+    // itself as a device pointer)
     double *ptr = nullptr;
     if (cudaGetSymbolAddress((void **)&ptr, g_residual_scratch) != cudaSuccess || !ptr) return OSTC_ERR_CUDA;
-    g_scratch_addr[dev] = ptr;
+    g_scratch_addr[dev].store(ptr);
+    scratch = ptr;
+  } else if (!scratch) {
+    return OSTC_ERR_INVALID_ARG;  // no call outside a capture on this device yet
   }
   Planes p;
   p.bv = zone->bv;
@@ -115,8 +126,7 @@ extern "C" ostc_status ostc_compute_residual_noalloc(const ostc_zone *zone, doub
   p.dt_ = (p.d1 + p.d2 + 1) * g;
   p.sz = (long long)(zone->mx + 2 * g) * (zone->my + 2 * g) * (zone->mz + 2 * g);
   p.nsz = n;
-  cudaStream_t s = (cudaStream_t)stream;
-  residual_partials<<<(unsigned)n_part, kThreads, 0, s>>>(p, g_scratch_addr[dev]);
-  residual_finish<<<1, kThreads, 0, s>>>(g_scratch_addr[dev], (int)n_part, (double)n, res_out);
+  residual_partials<<<(unsigned)n_part, kThreads, 0, s>>>(p, scratch);
+  residual_finish<<<1, kThreads, 0, s>>>(scratch, (int)n_part, (double)n, res_out);
   return cudaGetLastError() == cudaSuccess ? OSTC_OK : OSTC_ERR_CUDA;
 }

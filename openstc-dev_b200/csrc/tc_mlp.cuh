@@ -12,8 +12,11 @@
 // with the bias + SiLU + BF16 epilogues read from tensor memory by all 8
 // warps (warp w reads lanes 32 (w % 4).., columns 128 (w / 4)..). One
 // thread issues the MMAs and commits them to an mbarrier that every thread
-// waits on with an iteration limit; a wait that runs out sets the error
-// word, and the CTA still waits (bounded) before freeing its tensor memory.
+// waits on for at most WAIT_NS of the global timer. When a wait runs out
+// anywhere in the CTA, the whole CTA stops walking tiles: it sets the error
+// word, commits once more so that the barrier tracks every MMA it issued,
+// waits for that (bounded again) and for its own asynchronous copies, and
+// frees its tensor memory before it returns.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -41,7 +44,7 @@ constexpr unsigned SM_BAR = SM_IO + IO_BYTES;  // mbarrier (8 B)
 constexpr unsigned SM_TMEM = SM_BAR + 8;             // allocated tensor-memory base (4 B)
 constexpr unsigned SM_BYTES = SM_TMEM + 8;
 constexpr unsigned TMEM_COLS = 512;
-constexpr unsigned WAIT_LIMIT = 1u << 20;  // mbarrier polls before giving up
+constexpr unsigned long long WAIT_NS = 1000000000ull;  // 1 s of the global timer per mbarrier wait
 
 // byte offset of element (r, k) of an R x K operand in the canonical K-major
 // no-swizzle layout: 8 x 16-byte core matrices, K-adjacent cores 128 B apart
@@ -81,9 +84,16 @@ __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::be
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// bounded wait for the mbarrier phase `parity`; false when the limit ran out
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait for the mbarrier phase `parity`; false when WAIT_NS ran out
 __device__ __forceinline__ bool bar_wait(unsigned bar, unsigned parity) {
-  for (unsigned it = 0; it < WAIT_LIMIT; ++it) {
+  const unsigned long long t0 = global_ns();
+  for (unsigned it = 0;; ++it) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred P;\n\t"
@@ -93,8 +103,8 @@ __device__ __forceinline__ bool bar_wait(unsigned bar, unsigned parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((it & 31) == 31 && global_ns() - t0 > WAIT_NS) return false;
   }
-  return false;
 }
 
 // 32 consecutive FP32 columns of this thread's lane
@@ -186,7 +196,7 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
   const unsigned tmem = *tmem_slot;
   const unsigned tmem_d4 = tmem + NH;  // columns 256..271
   unsigned parity = 0;
-  bool ok = true;
+  bool timed_out = false;  // CTA-uniform: a bounded wait ran out somewhere in the CTA
   const int row = (warp & 3) * 32 + lane;   // the TMEM lane this thread reads
   const int col0 = (warp >> 2) * (NH / 2);  // first of its 128 columns
   const unsigned lane_addr = (unsigned)((warp & 3) * 32) << 16;
@@ -214,10 +224,15 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
     if (tid == 0) {
       mma_issue(tmem, smem_desc(smem_u32(smem + SM_X0), 128, 2 * 128), smem_desc(smem_u32(smem + SM_W1), 128, 2 * 128),
                 idesc_bf16(NH), 0);
-      mma_commit(bar);
+      // net.withhold_commit (a diagnostic of the timeout path): no completion
+      // signal for this product, so the wait below runs out
+      if (!net.withhold_commit) mma_commit(bar);
     }
     for (int layer = 0; layer < 3; ++layer) {
-      ok = bar_wait(bar, parity) && ok;
+      if (__syncthreads_or(!bar_wait(bar, parity))) {
+        timed_out = true;
+        break;
+      }
       parity ^= 1;
       fence_after();
       if (layer == 1) load_weights(smem, SM_W, net.w3(), NH, NH);  // W2 is no longer read
@@ -253,7 +268,10 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
         mma_commit(bar);
       }
     }
-    ok = bar_wait(bar, parity) && ok;
+    if (timed_out || __syncthreads_or(!bar_wait(bar, parity))) {
+      timed_out = true;
+      break;
+    }
     parity ^= 1;
     fence_after();
     if (warp < 4) {
@@ -267,7 +285,16 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
     __syncthreads();
     fence_after();
   }
-  if (!ok && err) atomicExch(err, 1);
+  if (timed_out) {
+    // drain: one more commit tracks every MMA this CTA issued; wait for it
+    // (bounded) and for the CTA's own weight copies before the memory goes
+    if (tid == 0) {
+      mma_commit(bar);
+      if (err) atomicExch(err, 1);
+    }
+    bar_wait(bar, parity);
+    cp_async_wait_all();
+  }
   fence_before();
   __syncthreads();
   fence_after();

@@ -153,6 +153,7 @@ def lib():
             "ostc_surrogate_gradients": [vp, vp, vp, i, vp, vp, vp],
             "ostc_surrogate_forward_tc": [vp, vp, i, vp, vp],
             "ostc_surrogate_set_checks": [vp, i, i, C.POINTER(d), C.POINTER(d), d, d],
+            "ostc_surrogate_inject_timeout": [vp, i],
             "ostc_chem_surrogate": [vp, vp, i, vp, vp, vp, vp, vp, vp, C.POINTER(i), vp],
             "ostc_set_chem_surrogate": [vp, vp],
             "ostc_use_generated_chemistry": [vp, i],
@@ -580,6 +581,13 @@ class Solver:
               "ostc_get_monitor")
         return out[:n, :rec.value]
 
+    def get_error(self):
+        """the context's last status and, for OSTC_ERR_NONPHYSICAL, the first
+        failing cell: (status, cuda_error, block, i, j, k)"""
+        v = [C.c_int() for _ in range(5)]
+        st = lib().ostc_get_error(self.ctx, *[C.byref(x) for x in v])
+        return (st,) + tuple(x.value for x in v)
+
     def set_statistics(self, on=True, start_step=0):
         check(lib().ostc_set_statistics(self.ctx, int(bool(on)), start_step), "ostc_set_statistics")
 
@@ -798,7 +806,24 @@ def grid_coordinates(mx, my, mz, ng, dx, warp=0.02, periodic_k=True):
     return x, y, z
 
 
+_metric_provider = None
+
+
+def set_metric_provider(fn):
+    """Route the synthetic workloads' geometry through fn(mx, my, mz, ngg, x,
+    y, z) -> (jac, metric) instead of ostc_metric_from_grid (None restores
+    the library's helper). For callers that build the same workloads without
+    loading the library, such as a CPU baseline."""
+    global _metric_provider
+    _metric_provider = fn
+
+
 def fill_metric(block: HostBlock, x, y, z):
+    if _metric_provider is not None:
+        jac, met = _metric_provider(block.mx, block.my, block.mz, block.ngg, x, y, z)
+        block.arrays["jac"][...] = jac
+        block.arrays["metric"][...] = met.view(block.arrays["metric"].dtype)
+        return
     check(lib().ostc_metric_from_grid(block.mx, block.my, block.mz, block.ngg, x.ctypes.data, y.ctypes.data,
                                       z.ctypes.data, block.arrays["jac"].ctypes.data,
                                       block.arrays["metric"].ctypes.data), "ostc_metric_from_grid")
@@ -1490,6 +1515,11 @@ class Surrogate:
         check(lib().ostc_surrogate_forward(self.h, xs.data_ptr(), xs.shape[0], ys.data_ptr(), self._s()),
               "ostc_surrogate_forward")
         return ys
+
+    def inject_timeout(self, on: bool):
+        """diagnostic: make the tensor-core kernels' bounded waits run out
+        (their calls then return OSTC_ERR_TIMEOUT)"""
+        check(lib().ostc_surrogate_inject_timeout(self.h, 1 if on else 0), "ostc_surrogate_inject_timeout")
 
     def forward_tc(self, xs):
         """the same network on the tcgen05 inference kernel"""

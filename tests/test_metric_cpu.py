@@ -43,3 +43,4 @@ def test_metric_bit_identical_to_reference(dims, ngg, kind):
     assert np.all(jac_r > 0)
     assert np.array_equal(jac_o.view(np.uint64), jac_r.view(np.uint64))
     assert np.array_equal(met_o["m"].view(np.uint64), met_r["m"].view(np.uint64))
+
