@@ -49,6 +49,8 @@ def _args():
     ap.add_argument("--no-refcuda", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the operator-split comparison (FP64 point-implicit vs learned chemistry)")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the other configurations' legs (small air vortex, 37-block SST RK3 and DPLUR)")
     return ap.parse_args()
 
 
@@ -333,10 +335,20 @@ def run_ours(a):
     if not a.no_e2e:
         e2e = run_e2e(a, case, tiles)
 
+    legs = None
+    if rank == 0 and world == 1 and not a.no_legs and a.workload == "mixing256":
+        legs = {}
+        for key, w, st in (("C1_vortex_128x128x8", "vortex128", False), ("C3_blocks37_sst_rk3", "blocks37", False),
+                           ("C3_blocks37_sst_dplur", "blocks37", True)):
+            try:
+                legs[key] = run_config_leg(a, w, steady=st)
+            except Exception as exc:  # reported, not fatal for the headline line
+                legs[key] = {"error": repr(exc)[:300]}
     surr = None
     if rank == 0 and world == 1 and not a.no_surrogate and case.mech is not None:
         try:
-            surr = run_surrogate_compare(a, tiles)
+            # the learned-chemistry configuration: the layer at 512 x 256 x 256
+            surr = run_surrogate_compare(a, tiles, "mixing512" if a.workload == "mixing256" else None)
         except Exception as exc:  # reported, not fatal for the headline line
             surr = {"error": repr(exc)[:300]}
     cpu = None
@@ -355,7 +367,8 @@ def run_ours(a):
                 "gpu_launches": launches_per_step * a.steps, "launches_per_step": launches_per_step,
                 "tiles": tiles,
                 "clocks": ck, "roofline": roofline, "step_roofline": step_roofline, "kernels_ms": {k: round(v["ms"], 4) for k, v in ktab.items()},
-                "e2e": e2e, "cpu_baseline": cpu, "reference_cuda_build": refcuda, "surrogate_chem": surr}
+                "e2e": e2e, "cpu_baseline": cpu, "reference_cuda_build": refcuda, "surrogate_chem": surr,
+                "other_configs": legs}
         if per_block is not None:
             line["per_block_launches"] = per_block
         print(json.dumps(line))
@@ -363,38 +376,113 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
-def run_surrogate_compare(a, tiles):
+def _timed_steps(solver, steps, small, steady=False):
+    """device ms of `steps` steps: each step timed alone after a 2x L2 write
+    when the state is smaller than 2x L2, else all steps back to back"""
+    import torch
+
+    go = (lambda n: solver.steady_steps(n)) if steady else (lambda n: solver.rk3_steps(n))
+    if small:
+        flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+        ms = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            go(1)
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    go(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_config_leg(a, workload, steady=False):
+    """One more configuration on the same GPU, through the same API: its own
+    workload, autotuned tiles, W warm-up and K timed steps (RK3 steps, or
+    DPLUR steady iterations with 3 inner sweeps), with its step roofline."""
+    import torch
+
+    import ostc
+
+    case = _make_case(workload)
+    if steady:
+        case = ostc.make_steady(case, implicit_method=1, dplur_inner_step=3)
+    blocks = [ostc.DeviceBlock(b) for b in case.blocks]
+    solver = ostc.Solver(case.scheme, case.mech, blocks, case.faces, interfaces=case.interfaces)
+    solver.initialize()
+    if not steady:
+        solver.autotune(warmup=1, reps=2)
+        solver.initialize()
+    torch.cuda.synchronize()
+    (solver.steady_steps if steady else solver.rk3_steps)(max(a.warmup, 3))
+    torch.cuda.synchronize()
+    small = state_bytes(case) < 2 * L2_BYTES
+    steps = min(a.steps, 20)
+    ms = _timed_steps(solver, steps, small, steady)
+    hbm, src = _peaks()
+    value = case.cells * steps / (ms * 1e-3) / 1e6
+    out = {"workload": case.name, "cells": case.cells, "scheme": _scheme_text(case), "steps": steps,
+           "value": round(value, 2), "unit": "Mcell-updates/s", "ms_per_step": round(ms / steps, 4),
+           "launches_per_step": solver.step_kernel_count(False),
+           "l2": "flushed before each step" if small else "inputs larger than L2"}
+    if steady:
+        out["iterations_per_s"] = round(steps / (ms * 1e-3), 2)
+        out["method"] = "DPLUR, 3 inner sweeps, local time stepping"
+    else:
+        b_alg = step_bytes_per_cell(case)
+        out["step_roofline"] = {"bytes_per_cell_update": b_alg, "achieved": round(value * 1e6 * b_alg / 1e9, 1),
+                                "peak": hbm, "unit": "GB/s", "frac": round(value * 1e6 * b_alg / 1e9 / hbm, 4),
+                                "peak_source": src}
+        ktab = kernel_table(solver, case)
+        out["kernels_ms"] = {k: round(v["ms"], 4) for k, v in ktab.items()}
+        fl = [k for k in ktab if k.startswith("flux_")]
+        alg = sum(algorithmic_bytes(k, case) for k in fl) / len(fl)
+        lm = sum(ktab[k]["ms"] for k in fl) / len(fl)
+        out["flux_roofline"] = {"achieved": round(alg / (lm * 1e-3) / 1e9, 1), "peak": hbm, "unit": "GB/s",
+                                "frac": round(alg / (lm * 1e-3) / 1e9 / hbm, 4), "launch_ms": round(lm, 4)}
+    solver.close()
+    del blocks
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_surrogate_compare(a, tiles, workload=None):
     """Plain vs learned chemistry on the same workload, both operator-split
     (the flow's three RK3 stages, then each cell's chemistry over the step's
     dt): chem_mode 1 runs the FP64 point-implicit integrator, chem_mode 2 the
     tcgen05 surrogate with FP64 fallback. The surrogate is first trained
-    (timed separately) on 4M labelled states: 3M from the synthetic sampler
-    over the training envelope plus 1M cells of this workload's initial
-    field with log-uniform dt. Both runs start from the same state; the
-    final fields are compared after warm-up + timed steps."""
+    (timed separately) on 4M labelled states: 2M sampled from snapshots of
+    FP64 operator-split runs of 64 x 256 x 64 slabs of the layer (its full y
+    extent) with other noise seeds
+    (surrogate.trajectory_states) and 2M from the synthetic sampler over the
+    training envelope, so the evaluated workload is held out. Both runs
+    start from the same state; the final fields are compared after warm-up
+    + timed steps. The chemistry operator alone (the learned step with its
+    fallback against the FP64 integrator, on the cells of the final field
+    at the step's dt) is timed as well."""
     import numpy as np
     import torch
 
     import ostc
     import surrogate as S
 
+    workload = workload or a.workload
     lab_case = ostc.case_premixed_box(8, 8, 4)
     lab_solver, _ = lab_case.solver()
-    case = _make_case(a.workload)
-    mech = case.mech
-    b = case.blocks[0]
-    g = b.ngg
-    rng = np.random.default_rng(17)
-    bv = b.arrays["bv"][:, g:-g, g:-g, g:-g].reshape(6, -1)
-    sv = b.arrays["sv"][:, g:-g, g:-g, g:-g].reshape(b.n_spec, -1)
-    n_field = min(1_000_000, bv.shape[1])
-    pick = rng.choice(bv.shape[1], n_field, replace=False)
-    field_states = (bv[5, pick].copy(), bv[4, pick].copy(), np.ascontiguousarray(sv[:, pick]),
-                    10 ** rng.uniform(-9, -7, pick.size))
+    mech = lab_case.mech
     torch.cuda.synchronize()
     t0 = time.time()
-    sur, sc, log = S.build(lab_solver, mech, n_train=4_000_000 - n_field, epochs=20, seed=1,
-                           extra_states=field_states)
+    # slabs of the layer with its full 256-cell y extent, so the pure streams
+    # (no fuel on the air side, no oxygen on the fuel side) are in the data
+    traj = S.trajectory_states(2_000_000, size=(64, 256, 64), seeds=(5, 6), steps=40, every=10, seed=17)
+    sur, sc, log = S.build(lab_solver, mech, n_train=2_000_000, epochs=20, seed=1, extra_states=traj)
     torch.cuda.synchronize()
     train_s = time.time() - t0
     n_samples = log.steps * 65536
@@ -405,7 +493,7 @@ def run_surrogate_compare(a, tiles):
                      "final_loss": log.loss[-1]}}
     finals, rates = {}, {}
     for mode in (1, 2):
-        c = _make_case(a.workload)
+        c = _make_case(workload)
         c.scheme.chem_mode = mode
         s, blocks = c.solver()
         s.set_tiles(tiles)
@@ -425,12 +513,43 @@ def run_surrogate_compare(a, tiles):
         rates[mode] = {"value": round(c.cells * a.steps / (ms * 1e-3) / 1e6, 2), "ms_per_step": round(ms / a.steps, 3),
                        "fallback_fraction": round((f1 - f0) / max(1, n1 - n0), 5)}
         finals[mode] = (blocks[0].t["bv"][5].clone(), blocks[0].t["sv"].clone())
+        if mode == 2:
+            # the chemistry operator alone on the cells of the final field at the last dt
+            g = c.blocks[0].ngg
+            bvt, svt = blocks[0].t["bv"], blocks[0].t["sv"]
+            st = [bvt[5, g:-g, g:-g, g:-g].reshape(-1).contiguous(), bvt[4, g:-g, g:-g, g:-g].reshape(-1).contiguous(),
+                  svt[:, g:-g, g:-g, g:-g].reshape(svt.shape[0], -1).contiguous()]
+            _, dts = s.rk3_steps(1, history=True)
+            st.append(torch.full_like(st[0], float(dts[-1])))
+            lab_solver.chem_surrogate(sur, *st)
+            lab_solver.chem_point_implicit(*st)
+            t_ops = {}
+            for nm, fn in (("surrogate", lambda: lab_solver.chem_surrogate(sur, *st)),
+                           ("fp64_integrator", lambda: lab_solver.chem_point_implicit(*st))):
+                torch.cuda.synchronize()
+                q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                q0.record()
+                for _ in range(3):
+                    r = fn()
+                q1.record()
+                torch.cuda.synchronize()
+                t_ops[nm] = q0.elapsed_time(q1) / 3
+            nfb = lab_solver.chem_surrogate(sur, *st)[2]
+            chem_op = {"states": st[0].numel(), "ms_surrogate": round(t_ops["surrogate"], 3),
+                       "ms_fp64_integrator": round(t_ops["fp64_integrator"], 3),
+                       "ns_per_state_surrogate": round(t_ops["surrogate"] * 1e6 / st[0].numel(), 3),
+                       "ns_per_state_integrator": round(t_ops["fp64_integrator"] * 1e6 / st[0].numel(), 3),
+                       "speedup": round(t_ops["fp64_integrator"] / t_ops["surrogate"], 3),
+                       "fallback_fraction": round(nfb / st[0].numel(), 5),
+                       "tensor_tflops": round(273408 * st[0].numel() / (t_ops["surrogate"] * 1e-3) / 1e12, 1)}
+            del st
         s.close()
         del blocks
         torch.cuda.empty_cache()
     dT = (finals[2][0] - finals[1][0]).abs()
     dY = (finals[2][1] - finals[1][1]).abs()
-    out.update({"unit": "Mcell-updates/s", "plain_split_fp64": rates[1], "surrogate_split": rates[2],
+    out.update({"workload": _make_case_name(workload), "chemistry_operator": chem_op,
+                "unit": "Mcell-updates/s", "plain_split_fp64": rates[1], "surrogate_split": rates[2],
                 "speedup_surrogate_over_plain_split": round(rates[2]["value"] / rates[1]["value"], 3),
                 "final_field_vs_plain": {"steps": max(a.warmup, 3) + a.steps, "max_abs_dT_K": float(dT.max()),
                                          "mean_abs_dT_K": float(dT.mean()), "max_abs_dY": float(dY.max()),

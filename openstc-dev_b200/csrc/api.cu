@@ -900,9 +900,10 @@ static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
           return launch_chem_integrator<decltype(m)::value>((int)n, T, p, Y, dt, dY, dT, s);
         }));
       } else {
-        int *list = nullptr, *err = nullptr;
-        CK(surrogate_scratch(ctx->sur, (int)n, &list, &count, &err));
-        CK(launch_chem_surrogate<NS>(*surrogate_net(ctx->sur), (int)n, T, p, Y, dt, dY, dT, list, count, err, s));
+        ChemScratch w;
+        CK(surrogate_scratch(ctx->sur, (int)n, &w));
+        count = w.count;
+        CK(launch_chem_surrogate<NS>(*surrogate_net(ctx->sur), (int)n, T, p, Y, dt, dY, dT, w, s));
       }
       CK(dispatch_ns(ctx->ns, [&](auto m) {
         return launch_chem_split<decltype(m)::value>(2, z, nullptr, 0, nullptr, ctx->chem_stats, count, s);
@@ -1180,11 +1181,11 @@ ostc_status ostc_set_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur) {
   if (!ctx->has_source || ctx->ns != mlp::NIN - 3) return OSTC_ERR_INVALID_ARG;
   // everything a captured step needs is set up here, outside any capture
   CK(prepare_chem_surrogate());
-  int *list = nullptr, *count = nullptr, *err = nullptr;
+  ChemScratch w;
   long long cells = 1;
   for (auto &z : ctx->dz) cells = std::max(cells, (long long)z.nsz);
   if (cells > 2147483647ll) return OSTC_ERR_INVALID_ARG;
-  CK(surrogate_scratch(sur, (int)cells, &list, &count, &err));
+  CK(surrogate_scratch(sur, (int)cells, &w));
   ctx->sur = sur;
   for (auto &kv : ctx->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -1213,14 +1214,14 @@ ostc_status ostc_chem_surrogate(ostc_ctx *ctx, ostc_surrogate *sur, int n, const
   if (!ctx->has_source || ctx->ns != mlp::NIN - 3) return OSTC_ERR_INVALID_ARG;
   if (ensure_param(ctx, S(stream))) return ctx->last;
   CK(prepare_chem_surrogate());
-  int *list = nullptr, *count = nullptr, *err = nullptr;
-  CK(surrogate_scratch(sur, n > 0 ? n : 1, &list, &count, &err));
-  CK(cudaMemsetAsync(err, 0, sizeof(int), S(stream)));
-  CK(launch_chem_surrogate<mlp::NIN - 3>(*surrogate_net(sur), n, T, p, Y, dt, dY, dT, list, count, err, S(stream)));
+  ChemScratch w;
+  CK(surrogate_scratch(sur, n > 0 ? n : 1, &w));
+  CK(cudaMemsetAsync(w.err, 0, sizeof(int), S(stream)));
+  CK(launch_chem_surrogate<mlp::NIN - 3>(*surrogate_net(sur), n, T, p, Y, dt, dY, dT, w, S(stream)));
   if (n_fallback) {
     int h[2] = {0, 0};
-    CK(cudaMemcpyAsync(&h[0], count, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
-    CK(cudaMemcpyAsync(&h[1], err, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+    CK(cudaMemcpyAsync(&h[0], w.count, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+    CK(cudaMemcpyAsync(&h[1], w.err, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
     CK(cudaStreamSynchronize(S(stream)));
     *n_fallback = h[0];
     if (h[1]) return fail(ctx, OSTC_ERR_TIMEOUT);

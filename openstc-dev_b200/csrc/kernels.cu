@@ -1170,26 +1170,28 @@ cudaError_t launch_chem_integrator(int n, const double *T, const double *p, cons
 
 template <int NS>
 cudaError_t launch_chem_surrogate(const mlp::Net &net, int n, const double *T, const double *p, const double *Y,
-                                  const double *dt, double *dY, double *dT, int *list, int *count, int *err,
-                                  cudaStream_t s) {
+                                  const double *dt, double *dY, double *dT, const ChemScratch &w, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   if constexpr (NS != mlp::NIN - 3) {
     return cudaErrorInvalidValue;
   } else {
-    // the kernel's shared-memory attribute is set by prepare_chem_surrogate
+    // the network kernel's shared-memory attribute is set by prepare_chem_surrogate
     int dev = 0, sms = 148;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(count, 0, sizeof(int), s)) != cudaSuccess) return e;
-    ChemIo<NS> io{};
-    io.T = T, io.p = p, io.Y = Y, io.dt = dt, io.dY = dY, io.dT = dT, io.n = n;
-    io.scale = net.scale, io.ck = net.checks, io.list = list, io.count = count;
+    if ((e = cudaMemsetAsync(w.count, 0, sizeof(int), s)) != cudaSuccess) return e;
+    const int cb = (n + 255) / 256, cells_grid = cb < 16 * sms ? cb : 16 * sms;
+    chem_features_kernel<NS><<<cells_grid, 256, 0, s>>>(n, T, p, Y, dt, net.scale, net.checks, w.x, w.env);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int tiles = (n + tc::ROWS - 1) / tc::ROWS;
-    surrogate_chem_kernel<NS><<<tiles < sms ? tiles : sms, tc::THREADS, tc::SM_BYTES, s>>>(net, io, err);
+    surrogate_chem_kernel<<<tiles < sms ? tiles : sms, tc::THREADS, tc::SM_BYTES, s>>>(net, w.x, w.y, n, w.err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    chem_checks_kernel<NS><<<cells_grid, 256, 0, s>>>(n, T, Y, dt, w.y, w.env, net.scale, net.checks, dY, dT, w.list,
+                                                      w.count);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int fb = (n + 127) / 128;
-    chem_fallback_kernel<NS><<<fb < 8 * sms ? fb : 8 * sms, 128, 0, s>>>(list, count, n, T, p, Y, dt, dY, dT);
+    chem_fallback_kernel<NS><<<fb < 8 * sms ? fb : 8 * sms, 128, 0, s>>>(w.list, w.count, n, T, p, Y, dt, dY, dT);
     return cudaGetLastError();
   }
 }
@@ -1212,8 +1214,7 @@ cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, do
 }
 
 cudaError_t prepare_chem_surrogate() {
-  return cudaFuncSetAttribute(surrogate_chem_kernel<mlp::NIN - 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              tc::SM_BYTES);
+  return cudaFuncSetAttribute(surrogate_chem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SM_BYTES);
 }
 
 bool mechanism_is_h2air9(const int *reac_type, const int *stoi_f, const int *stoi_b, const int *reac_order, int nr,
@@ -1248,7 +1249,7 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   template cudaError_t launch_chem_integrator<NS>(int, const double *, const double *, const double *, const double *, \
                                                   double *, double *, cudaStream_t);                                  \
   template cudaError_t launch_chem_surrogate<NS>(const mlp::Net &, int, const double *, const double *, const double *, \
-                                                 const double *, double *, double *, int *, int *, int *, cudaStream_t); \
+                                                 const double *, double *, double *, const ChemScratch &, cudaStream_t); \
   template cudaError_t launch_chem_split<NS>(int, const DevZone &, const double *, double, double *, long long *,        \
                                              const int *, cudaStream_t);
 

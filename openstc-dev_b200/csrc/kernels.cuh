@@ -123,8 +123,7 @@ cudaError_t launch_chem_integrator(int n, const double *T, const double *p, cons
                                    double *dY, double *dT, cudaStream_t s);
 template <int NS>
 cudaError_t launch_chem_surrogate(const mlp::Net &net, int n, const double *T, const double *p, const double *Y,
-                                  const double *dt, double *dY, double *dT, int *list, int *count, int *err,
-                                  cudaStream_t s);
+                                  const double *dt, double *dY, double *dT, const ChemScratch &w, cudaStream_t s);
 // split chemistry of a block: op 0 gathers the interior states into buf,
 // 1 scatters the increments back, 2 adds the block's counts to stats
 template <int NS>

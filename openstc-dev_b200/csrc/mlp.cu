@@ -262,6 +262,7 @@ unsigned blocks(long long n) { return (unsigned)((n + 255) / 256); }
 
 // the tensor-core forward on standardised rows (x [n][12] -> y [n][10])
 struct RawIo {
+  static constexpr bool kPacked = false;
   const float *x;
   float *y;
   int n;
@@ -311,6 +312,10 @@ struct ostc_surrogate {
   Checks *checks = nullptr;  // device copy of the acceptance tests
   int *list = nullptr, *count = nullptr;
   int list_cap = 0;
+  // the learned chemistry step's per-state buffers (list_cap states)
+  __nv_bfloat16 *cx = nullptr;
+  float *cy = nullptr;
+  unsigned char *cenv = nullptr;
   std::vector<void *> owned;
 };
 
@@ -632,23 +637,36 @@ ostc_status ostc_surrogate_train_step(ostc_surrogate *s, const float *xs, const 
 namespace ostc {
 const Net *surrogate_net(const ostc_surrogate *s) { return s ? &s->net : nullptr; }
 
-cudaError_t surrogate_scratch(ostc_surrogate *s, int n, int **list, int **count, int **err) {
+cudaError_t surrogate_scratch(ostc_surrogate *s, int n, ChemScratch *out) {
   if (n > s->list_cap) {
-    if (s->list) {
-      cudaFree(s->list);
+    for (void *q : {(void *)s->list, (void *)s->cx, (void *)s->cy, (void *)s->cenv}) {
+      if (!q) continue;
+      cudaFree(q);
       for (auto &p : s->owned)
-        if (p == s->list) p = nullptr;
+        if (p == q) p = nullptr;
     }
     s->list = nullptr;
+    s->cx = nullptr;
+    s->cy = nullptr;
+    s->cenv = nullptr;
     s->list_cap = 0;
     cudaError_t e = cudaMalloc(&s->list, sizeof(int) * (size_t)n);
+    if (e == cudaSuccess) s->owned.push_back(s->list);
+    if (e == cudaSuccess) e = cudaMalloc(&s->cx, sizeof(__nv_bfloat16) * mlp::KIN * (size_t)n);
+    if (e == cudaSuccess) s->owned.push_back(s->cx);
+    if (e == cudaSuccess) e = cudaMalloc(&s->cy, sizeof(float) * mlp::NOUT * (size_t)n);
+    if (e == cudaSuccess) s->owned.push_back(s->cy);
+    if (e == cudaSuccess) e = cudaMalloc(&s->cenv, (size_t)n);
+    if (e == cudaSuccess) s->owned.push_back(s->cenv);
     if (e != cudaSuccess) return e;
-    s->owned.push_back(s->list);
     s->list_cap = n;
   }
-  *list = s->list;
-  *count = s->count;
-  *err = s->err;
+  out->list = s->list;
+  out->count = s->count;
+  out->err = s->err;
+  out->x = s->cx;
+  out->y = s->cy;
+  out->env = s->cenv;
   return cudaSuccess;
 }
 }  // namespace ostc

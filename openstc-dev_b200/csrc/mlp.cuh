@@ -68,8 +68,16 @@ struct Net {
 
 // the device parameters of a surrogate (mlp.cu), for the inference path
 const mlp::Net *surrogate_net(const ostc_surrogate *s);
-// per-call scratch of the surrogate chemistry step: a fallback list of at
-// least n entries (grown on demand), its counter and the error word
-cudaError_t surrogate_scratch(ostc_surrogate *s, int n, int **list, int **count, int **err);
+// per-call scratch of the surrogate chemistry step, for at least n states
+// (grown on demand): the fallback list and its counter, the error word, the
+// standardised BF16 feature rows [n][16], the network's outputs [n][10] and
+// the training-envelope flags [n]
+struct ChemScratch {
+  int *list = nullptr, *count = nullptr, *err = nullptr;
+  __nv_bfloat16 *x = nullptr;
+  float *y = nullptr;
+  unsigned char *env = nullptr;
+};
+cudaError_t surrogate_scratch(ostc_surrogate *s, int n, ChemScratch *out);
 
 }  // namespace ostc

@@ -2,15 +2,15 @@
 // tensor cores (tcgen05): 128-row tiles, operands in shared memory in the
 // canonical no-swizzle K-major layout, FP32 accumulators in tensor memory.
 //
-// One CTA of 256 threads owns one SM (217 KB of shared memory) and walks
+// One CTA of 512 threads owns one SM (217 KB of shared memory) and walks
 // tiles of 128 rows. Per tile:
 //   features (FP64 -> standardised BF16, rows 0..127 by threads 0..127)
 //   L1  D[128x256]  = X0[128x16]  W1^T      1 MMA  (W1 resident)
 //   L2  D           = A1[128x256] W2^T     16 MMAs (W2 streamed from L2)
 //   L3  D           = A2          W3^T     16 MMAs (W3 streamed from L2)
 //   L4  D4[128x16]  = A3          W4^T     16 MMAs (W4 resident)
-// with the bias + SiLU + BF16 epilogues read from tensor memory by all 8
-// warps (warp w reads lanes 32 (w % 4).., columns 128 (w / 4)..). One
+// with the bias + SiLU + BF16 epilogues read from tensor memory by all 16
+// warps (warp w reads lanes 32 (w % 4).., columns 64 (w / 4)..). One
 // thread issues the MMAs and commits them to an mbarrier that every thread
 // waits on for at most WAIT_NS of the global timer. When a wait runs out
 // anywhere in the CTA, the whole CTA stops walking tiles: it sets the error
@@ -30,7 +30,7 @@ using mlp::NH;
 using mlp::NOUTP;
 
 constexpr int ROWS = 128;
-constexpr int THREADS = 256;
+constexpr int THREADS = 512;
 // shared memory map (bytes)
 constexpr unsigned SM_ACT = 0;                       // 128 x 256 bf16
 constexpr unsigned SM_W = SM_ACT + ROWS * NH * 2;    // 256 x 256 bf16 (W2 or W3)
@@ -107,6 +107,19 @@ __device__ __forceinline__ bool bar_wait(unsigned bar, unsigned parity) {
   }
 }
 
+// 32 consecutive FP32 columns of this thread's lane (no wait: tmem_wait_ld)
+__device__ __forceinline__ void tmem_ld32_async(unsigned taddr, unsigned *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 // 32 consecutive FP32 columns of this thread's lane
 __device__ __forceinline__ void tmem_ld32(unsigned taddr, float *v) {
   unsigned r[32];
@@ -144,11 +157,17 @@ __device__ __forceinline__ void cp_async16(unsigned dst, const void *src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prior1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-// copy a row-major global N x K bf16 matrix into the canonical layout
+// copy a row-major global N x K bf16 matrix into the canonical layout; each
+// CTA starts at its own offset, so the SMs that stream the same weights at
+// the same time spread over the L2 slices instead of queueing on one line
 __device__ __forceinline__ void load_weights(unsigned char *smem, unsigned off, const __nv_bfloat16 *w, int N, int K) {
   const int chunks = N * K / 8;
-  for (int c = threadIdx.x; c < chunks; c += THREADS) {
+  const int rot = (int)((blockIdx.x * 613u) % (unsigned)chunks);
+  for (int i = threadIdx.x; i < chunks; i += THREADS) {
+    const int c = i + rot < chunks ? i + rot : i + rot - chunks;
     const int n = c / (K / 8), kc = c % (K / 8);
     cp_async16(smem_u32(smem + off + core_off(n, kc * 8, K)), w + (long long)n * K + kc * 8);
   }
@@ -157,9 +176,14 @@ __device__ __forceinline__ void load_weights(unsigned char *smem, unsigned off, 
 // The network core. `Io` supplies
 //   void setup(unsigned char *tables)          fills IO_BYTES of shared memory
 //                                              (all threads, once per CTA)
-// and, per tile,
+// and, per tile, with Io::kPacked false
 //   bool load(int tile, int row, float *x12)   standardised features of a row
 //                                              (threads 0..127); false: no row
+// or with Io::kPacked true
+//   void stage(int tile, unsigned char *x0)    all threads: the tile's rows,
+//                                              already standardised BF16, into
+//                                              the operand layout (cp.async)
+// and
 //   void store(int tile, int row, const float *y10)   standardised outputs
 // Returns nothing; errors go to *err (1 = a wait ran out).
 template <typename Io>
@@ -198,10 +222,18 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
   unsigned parity = 0;
   bool timed_out = false;  // CTA-uniform: a bounded wait ran out somewhere in the CTA
   const int row = (warp & 3) * 32 + lane;   // the TMEM lane this thread reads
-  const int col0 = (warp >> 2) * (NH / 2);  // first of its 128 columns
+  const int col0 = (warp >> 2) * (NH / 4);  // first of its 64 columns
   const unsigned lane_addr = (unsigned)((warp & 3) * 32) << 16;
 
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    if constexpr (Io::kPacked) {
+      // the tile's feature rows first, then W2, which streams during layer 1
+      io.stage(tile, smem + SM_X0);
+      cp_async_commit();
+      load_weights(smem, SM_W, net.w2(), NH, NH);
+      cp_async_commit();
+      cp_async_wait_prior1();
+    } else {
     // stream W2 while the features and layer 1 run
     load_weights(smem, SM_W, net.w2(), NH, NH);
     if (tid < ROWS) {
@@ -216,6 +248,7 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
           pack_bf16(xs[0], xs[1]), pack_bf16(xs[2], xs[3]), pack_bf16(xs[4], xs[5]), pack_bf16(xs[6], xs[7]));
       *(uint4 *)(smem + SM_X0 + core_off(tid, 8, KIN)) = make_uint4(
           pack_bf16(xs[8], xs[9]), pack_bf16(xs[10], xs[11]), pack_bf16(xs[12], xs[13]), pack_bf16(xs[14], xs[15]));
+    }
     }
     fence_async_smem();
     fence_before();
@@ -238,20 +271,22 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
       if (layer == 1) load_weights(smem, SM_W, net.w3(), NH, NH);  // W2 is no longer read
       // epilogue: bias + SiLU -> BF16 activations (the next layer's A operand)
       const float *b = sbias + layer * NH;
-#pragma unroll 1
-      for (int ch = 0; ch < NH / 2; ch += 32) {
-        float v[32];
-        tmem_ld32(tmem + lane_addr + col0 + ch, v);
+      // both 32-column loads in flight before the one wait
+      unsigned acc[NH / 4];
+      tmem_ld32_async(tmem + lane_addr + col0, acc);
+      tmem_ld32_async(tmem + lane_addr + col0 + 32, acc + 32);
+      tmem_wait_ld();
 #pragma unroll
-        for (int q = 0; q < 32; q += 8) {
-          unsigned w4[4];
+      for (int q = 0; q < NH / 4; q += 8) {
+        const float4 b0 = *(const float4 *)(b + col0 + q), b1 = *(const float4 *)(b + col0 + q + 4);
+        const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        unsigned w4[4];
 #pragma unroll
-          for (int e = 0; e < 8; e += 2) {
-            const float z0 = v[q + e] + b[col0 + ch + q + e], z1 = v[q + e + 1] + b[col0 + ch + q + e + 1];
-            w4[e / 2] = pack_bf16(__fdividef(z0, 1.0f + __expf(-z0)), __fdividef(z1, 1.0f + __expf(-z1)));
-          }
-          *(uint4 *)(smem + SM_ACT + core_off(row, col0 + ch + q, NH)) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        for (int e = 0; e < 8; e += 2) {
+          const float z0 = __uint_as_float(acc[q + e]) + bb[e], z1 = __uint_as_float(acc[q + e + 1]) + bb[e + 1];
+          w4[e / 2] = pack_bf16(__fdividef(z0, 1.0f + __expf(-z0)), __fdividef(z1, 1.0f + __expf(-z1)));
         }
+        *(uint4 *)(smem + SM_ACT + core_off(row, col0 + q, NH)) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
       }
       cp_async_wait_all();
       fence_async_smem();
@@ -300,6 +335,34 @@ __device__ void mlp_tiles(const mlp::Net &net, int n_tiles, Io &io, int *err) {
   fence_after();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
+
+// rows of 16 standardised BF16 features (12 and 4 zeros, 32 bytes, the
+// operand's K) in; rows of 10 FP32 outputs out
+struct PackedIo {
+  static constexpr bool kPacked = true;
+  const __nv_bfloat16 *x;
+  float *y;
+  int n;
+  __device__ void setup(unsigned char *) {}
+  __device__ void stage(int tile, unsigned char *x0) const {
+    for (int c = threadIdx.x; c < 2 * ROWS; c += THREADS) {
+      const int row = c >> 1, half = c & 1;
+      const long long q = (long long)tile * ROWS + row;
+      unsigned char *dst = x0 + core_off(row, half * 8, KIN);
+      if (q < n)
+        cp_async16(smem_u32(dst), x + q * KIN + half * 8);
+      else
+        *(uint4 *)dst = make_uint4(0, 0, 0, 0);
+    }
+  }
+  __device__ void store(int tile, int row, const float *o) const {
+    const long long q = (long long)tile * ROWS + row;
+    if (q >= n) return;
+    float2 *d = (float2 *)(y + q * mlp::NOUT);
+#pragma unroll
+    for (int i = 0; i < mlp::NOUT / 2; ++i) d[i] = make_float2(o[2 * i], o[2 * i + 1]);
+  }
+};
 
 }  // namespace tc
 }  // namespace ostc

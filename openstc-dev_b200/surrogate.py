@@ -10,9 +10,16 @@ thousandth of the rate's standard deviation: small rates keep relative
 precision (a radical's formation enthalpy turns a 1e-6 error in its mass
 fraction into a kelvin of temperature), large ones are compressed
 logarithmically. Features and z are standardised with the training set's mean and standard deviation; the
-envelope (per-feature min / max of the training inputs) bounds where the
-network is trusted. The formula of the features is the one of
-csrc/surrogate.cuh: surrogate_features.
+envelope (per-feature min / max of the training inputs, widened on each side
+by ENVELOPE_MARGIN of the feature's range) bounds where the network is
+trusted. The formula of the features is the one of csrc/surrogate.cuh:
+surrogate_features.
+
+Training states (the chemistry-surrogate configuration: "states sampled from
+runs of" the reacting mixing layer) come from trajectory_states: snapshots of
+FP64 operator-split runs of the layer (chem_mode 1), next to the seeded
+synthetic states of ostc.sample_chem_states that cover the wider envelope
+(T 300-3000 K, p 0.5-3 atm, dt 1e-9..1e-7 s).
 """
 from __future__ import annotations
 
@@ -86,6 +93,11 @@ class Scaling:
 
 
 R0_FRACTION = 1e-3
+# the trusted envelope reaches this fraction of each feature's training range
+# beyond its training minimum and maximum: a flow step moves states a little
+# past the extremes of the data (the cold stream cools below its 300 K inflow
+# by expansion), where the network is still accurate
+ENVELOPE_MARGIN = 0.02
 
 
 def _transform(G, r0):
@@ -103,8 +115,10 @@ def fit_scaling(d: Dataset) -> Scaling:
     Z = _transform(G, r0)
     fm, fs = F.mean(0), F.std(0).clamp_min(1e-12)
     gm, gs = Z.mean(0), Z.std(0).clamp_min(1e-12)
+    lo, hi = F.min(0).values, F.max(0).values
+    pad = ENVELOPE_MARGIN * (hi - lo)
     return Scaling(fm.cpu().numpy(), fs.cpu().numpy(), gm.cpu().numpy(), gs.cpu().numpy(),
-                   F.min(0).values.cpu().numpy(), F.max(0).values.cpu().numpy(), r0.cpu().numpy())
+                   (lo - pad).cpu().numpy(), (hi + pad).cpu().numpy(), r0.cpu().numpy())
 
 
 def standardise(d: Dataset, sc: Scaling):
@@ -154,6 +168,39 @@ def train(sur: "ostc.Surrogate", X, Yt, epochs: int = 20, batch: int = 65536, lr
     log.steps = step
     log.seconds = time.time() - t0
     return log
+
+
+def trajectory_states(n: int, size=(64, 256, 64), seeds=(5, 6), steps: int = 40, every: int = 10, seed: int = 0,
+                      dt_range=(1e-9, 1e-7)):
+    """n cell states (T, p, Y [n_spec][n], dt as numpy arrays) sampled from
+    snapshots of FP64 operator-split runs of the reacting mixing layer
+    (chem_mode 1, one run per noise seed, a snapshot every `every` of
+    `steps` RK3 steps); dt log-uniform in dt_range, as the labeller's
+    increments are learned over that span."""
+    import torch
+
+    snaps = []
+    for sd in seeds:
+        c = ostc.case_mixing_layer(*size, seed=sd)
+        c.scheme.chem_mode = 1
+        s, blocks = c.solver()
+        s.initialize()
+        g = c.blocks[0].ngg
+        for _ in range(0, steps, every):
+            s.rk3_steps(every)
+            bv, sv = blocks[0].t["bv"], blocks[0].t["sv"]
+            snaps.append((bv[5, g:-g, g:-g, g:-g].reshape(-1), bv[4, g:-g, g:-g, g:-g].reshape(-1),
+                          sv[:, g:-g, g:-g, g:-g].reshape(sv.shape[0], -1)))
+        torch.cuda.synchronize()
+        s.close()
+        del blocks
+    T = torch.cat([x[0] for x in snaps])
+    p = torch.cat([x[1] for x in snaps])
+    Y = torch.cat([x[2] for x in snaps], dim=1)
+    rng = np.random.default_rng(seed)
+    pick = torch.from_numpy(rng.choice(T.numel(), min(n, T.numel()), replace=False)).to(T.device)
+    dt = 10 ** rng.uniform(np.log10(dt_range[0]), np.log10(dt_range[1]), pick.numel())
+    return (T[pick].cpu().numpy(), p[pick].cpu().numpy(), np.ascontiguousarray(Y[:, pick].cpu().numpy()), dt)
 
 
 def set_checks(sur: "ostc.Surrogate", mech: "ostc.Mechanism", tol_elem: float = 1e-4, tol_T: float = 1.0):
