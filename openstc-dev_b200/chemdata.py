@@ -384,3 +384,70 @@ def h2_air_9sp():
     """The 9-species, 19-reaction H2-air mechanism of the reacting workload
     (tables generated by data/make_mechanism.py from the CHEMKIN inputs)."""
     return load_json(DATA / "h2_air_9sp.json")
+
+
+def h2_mixing_4sp():
+    """The reference's non-reacting 4-species set (H2, H2O, O2, N2 in the
+    order of input_files/chemistry/H2_mech_mixing.inp, with therm.dat and
+    tran.dat; the reference reads no reactions for it, reaction = 0)."""
+    return load_json(DATA / "h2_mixing_4sp.json")
+
+
+_SPECIES_TABS = ("t_low", "t_mid", "t_high", "high_temp_coeff", "low_temp_coeff", "mw", "LJ_potent_inv", "vis_coeff")
+_PAIR_TABS = ("WjDivWi_to_One4th", "sqrt_WiDivWjPl1Mul8", "binary_diffusivity_coeff", "kb_over_eps_jk")
+_REAC_SPECIES_TABS = ("stoi_f", "stoi_b", "third_body_coeff")
+
+
+def with_inert_copies(mech, name: str, k: int):
+    """The mechanism with k more species that are inert copies of `name`
+    (same thermodynamic and transport data, pair data of the copied pairs,
+    never reacting, third-body efficiency of the original), appended after
+    the others as name_1 .. name_k: mechanisms of any species count up to
+    OSTC_MAX_SPEC for the tests of the per-count builds."""
+    import numpy as np
+
+    src = mech.names.index(name)
+    ix = list(range(mech.n_spec)) + [src] * k
+    tab = {}
+    for key, v in mech.tables.items():
+        if key in _SPECIES_TABS:
+            tab[key] = np.ascontiguousarray(v[ix])
+        elif key in _PAIR_TABS:
+            tab[key] = np.ascontiguousarray(v[np.ix_(ix, ix)])
+        elif key in ("stoi_f", "stoi_b"):
+            tab[key] = np.ascontiguousarray(np.concatenate([v, np.zeros((v.shape[0], k), v.dtype)], axis=1))
+        elif key == "third_body_coeff":
+            tab[key] = np.ascontiguousarray(v[:, ix])
+        else:
+            tab[key] = v.copy()
+    return type(mech)(mech.names + ["%s_%d" % (name, q + 1) for q in range(k)], tab, mech.n_reac)
+
+
+def subset(mech, keep: List[str], reactions: bool = True):
+    """The mechanism restricted to the species `keep` (in that order) and,
+    with reactions, to the reactions whose reactants and products are all
+    kept (third-body efficiencies of dropped species are dropped with them).
+    Species and pair tables are the same numbers, re-indexed: what the
+    reference's parser builds for a mechanism file listing those species."""
+    import numpy as np
+
+    ix = [mech.names.index(n) for n in keep]
+    tab = {}
+    for k in _SPECIES_TABS:
+        tab[k] = np.ascontiguousarray(mech.tables[k][ix])
+    for k in _PAIR_TABS:
+        tab[k] = np.ascontiguousarray(mech.tables[k][np.ix_(ix, ix)])
+    nr = 0
+    if reactions and mech.n_reac:
+        drop = [i for i in range(mech.n_spec) if i not in ix]
+        sf, sb = mech.tables["stoi_f"], mech.tables["stoi_b"]
+        rows = [r for r in range(mech.n_reac) if not any(sf[r, d] or sb[r, d] for d in drop)]
+        for k, v in mech.tables.items():
+            if k in _SPECIES_TABS or k in _PAIR_TABS:
+                continue
+            v = v[rows]
+            if k in _REAC_SPECIES_TABS:
+                v = v[:, ix]
+            tab[k] = np.ascontiguousarray(v)
+        nr = len(rows)
+    return type(mech)(list(keep), tab, nr)

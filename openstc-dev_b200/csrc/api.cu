@@ -171,9 +171,31 @@ ostc_status cells_all(ostc_ctx *ctx, CellOp op, int table, const CellArgs &a, cu
 
 template <typename F>
 cudaError_t dispatch_ns(int ns, F &&f) {
+  // every species count has a build: 0 and 9 in kernels.cu / flux0.cu / flux9.cu, the others in
+  // kernels_ns_*.cu / flux_ns_*.cu
+  static_assert(OSTC_MAX_SPEC == 20, "one case per species count");
   switch (ns) {
     case 0: return f(std::integral_constant<int, 0>{});
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    case 7: return f(std::integral_constant<int, 7>{});
+    case 8: return f(std::integral_constant<int, 8>{});
     case 9: return f(std::integral_constant<int, 9>{});
+    case 10: return f(std::integral_constant<int, 10>{});
+    case 11: return f(std::integral_constant<int, 11>{});
+    case 12: return f(std::integral_constant<int, 12>{});
+    case 13: return f(std::integral_constant<int, 13>{});
+    case 14: return f(std::integral_constant<int, 14>{});
+    case 15: return f(std::integral_constant<int, 15>{});
+    case 16: return f(std::integral_constant<int, 16>{});
+    case 17: return f(std::integral_constant<int, 17>{});
+    case 18: return f(std::integral_constant<int, 18>{});
+    case 19: return f(std::integral_constant<int, 19>{});
+    case 20: return f(std::integral_constant<int, 20>{});
     default: return cudaErrorInvalidValue;
   }
 }
@@ -295,7 +317,8 @@ ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zon
   } else if (p->mix_model == OSTC_MIX_AIR) {
     if (p->n_spec != 0 || p->n_var != 5 || p->n_scalar != 0) return OSTC_ERR_INVALID_ARG;
   } else if (p->mix_model == OSTC_MIX_MIXTURE || p->mix_model == OSTC_MIX_FR) {
-    if (p->n_spec != 9) return OSTC_ERR_UNSUPPORTED;
+    // any mechanism up to MAX_SPEC_NUMBER species (CMakeLists.txt:13-19)
+    if (p->n_spec < 1 || p->n_spec > OSTC_MAX_SPEC) return OSTC_ERR_INVALID_ARG;
     if (p->n_var != 5 + p->n_spec || p->n_scalar != p->n_spec) return OSTC_ERR_INVALID_ARG;
     if (p->mix_model == OSTC_MIX_FR && (p->n_reac < 0 || p->n_reac > OSTC_MAX_REAC)) return OSTC_ERR_INVALID_ARG;
   } else {
@@ -887,10 +910,12 @@ static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
     // operator-split chemistry over the step's dt (the last stage's dt, quirk A12)
     if (ctx->cfg.chem_mode == 2 && !ctx->sur) return fail(ctx, OSTC_ERR_INVALID_ARG);
     const double *dt_dev = ctx->cfg.fixed_time_step ? nullptr : (const double *)ctx->dt_bits;
-    constexpr int NS = mlp::NIN - 3;
+    constexpr int NS_SUR = mlp::NIN - 3;  // the surrogate's species count
+    const int ns = ctx->prm.n_spec;
     for (auto &z : ctx->dz) {
+      // the staging layout of launch_chem_split: T, p, Y [ns][n], dt, dY [ns][n], dT
       const long long n = z.nsz;
-      double *T = ctx->chem_buf, *p = T + n, *Y = p + n, *dt = Y + NS * n, *dY = dt + n, *dT = dY + NS * n;
+      double *T = ctx->chem_buf, *p = T + n, *Y = p + n, *dt = Y + ns * n, *dY = dt + n, *dT = dY + ns * n;
       int *count = nullptr;
       CK(dispatch_ns(ctx->ns, [&](auto m) {
         return launch_chem_split<decltype(m)::value>(0, z, dt_dev, ctx->cfg.dt, ctx->chem_buf, nullptr, nullptr, s);
@@ -903,7 +928,7 @@ static ostc_status enqueue_step(ostc_ctx *ctx, bool with_hist, cudaStream_t s) {
         ChemScratch w;
         CK(surrogate_scratch(ctx->sur, (int)n, &w));
         count = w.count;
-        CK(launch_chem_surrogate<NS>(*surrogate_net(ctx->sur), (int)n, T, p, Y, dt, dY, dT, w, s));
+        CK(launch_chem_surrogate<NS_SUR>(*surrogate_net(ctx->sur), (int)n, T, p, Y, dt, dY, dT, w, s));
       }
       CK(dispatch_ns(ctx->ns, [&](auto m) {
         return launch_chem_split<decltype(m)::value>(2, z, nullptr, 0, nullptr, ctx->chem_stats, count, s);

@@ -1,7 +1,8 @@
 // flux.cuh — the per-direction flux kernel family flux_dir<NS,INV,DIR,MINB,PART>
-// and its launchers. Included by one translation unit per species count
-// (flux0.cu, flux9.cu) so the builds compile in parallel; each unit holds its
-// own copy of the __constant__ parameters (uploaded by upload_param).
+// and its launchers. Included by one translation unit per species count or
+// group of counts (flux0.cu, flux9.cu, flux0t.cu, flux9t.cu, flux_ns_*.cu) so
+// the builds compile in parallel; each unit holds its own copy of the
+// __constant__ parameters (uploaded by upload_param).
 //
 // Flux kernels march along the sweep direction: a CTA owns a segment of
 // S = R*C - 1 cells of 32 (or R) lines, computes the R*C faces that bound
@@ -243,6 +244,10 @@ static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, const Flu
 template <int NS, int INV, int DIR, int PART, int NT>
 static cudaError_t launch_flux_p(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
                                  int viscous, cudaStream_t s) {
+#ifdef OSTC_FLUX_REDUCED
+  // the units of further species counts build the 128-register budget only
+  return launch_flux_m<NS, INV, DIR, 2, PART, NT>(z, t, tab, accumulate, viscous, s);
+#else
   switch (t.minb) {
     case 5: return launch_flux_m<NS, INV, DIR, 5, PART, NT>(z, t, tab, accumulate, viscous, s);
     case 4: return launch_flux_m<NS, INV, DIR, 4, PART, NT>(z, t, tab, accumulate, viscous, s);
@@ -250,6 +255,7 @@ static cudaError_t launch_flux_p(const DevZone &z, const TileShape &t, const Flu
     case 2: return launch_flux_m<NS, INV, DIR, 2, PART, NT>(z, t, tab, accumulate, viscous, s);
     default: return launch_flux_m<NS, INV, DIR, 1, PART, NT>(z, t, tab, accumulate, viscous, s);
   }
+#endif
 }
 
 // part 0: the face flux of the flow — the fused kernel, or (viscous flow with

@@ -13,7 +13,8 @@
 #include "common.cuh"
 
 namespace ostc {
-__constant__ DevParam c_p;
+// this unit's copy of the run parameters (written by upload_param)
+static __constant__ DevParam c_p;
 }
 
 #include "chem.cuh"
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(256) chem_scatter_kernel(DevZone z, const doub
   }
 }
 
-__global__ void chem_stats_kernel(long long *stats, long long n, const int *count) {
+static __global__ void chem_stats_kernel(long long *stats, long long n, const int *count) {
   stats[0] += n;
   if (count) stats[1] += *count;
 }
@@ -358,7 +359,7 @@ __device__ __forceinline__ void velocity_cells(const DevZone &z, const int bx, c
   z.vel[g] = sqrt(u * u + v * v + w * w);
 }
 
-__global__ void __launch_bounds__(256) velocity_kernel(DevZone z) {
+static __global__ void __launch_bounds__(256) velocity_kernel(DevZone z) {
   velocity_cells(z, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -423,7 +424,7 @@ __global__ void __launch_bounds__(256) dt_kernel(DevZone z, unsigned long long *
   dt_cells<NS>(z, blockIdx.x, blockIdx.y, blockIdx.z, dt_bits);
 }
 
-__global__ void dt_reset_kernel(unsigned long long *dt_bits) {
+static __global__ void dt_reset_kernel(unsigned long long *dt_bits) {
   *dt_bits = (unsigned long long)__double_as_longlong(1e6);
 }
 
@@ -473,7 +474,7 @@ __global__ void bc_inflow_kernel(DevZone z, BcFace b, int with_cv) {  // BoundCo
   }
 }
 
-__global__ void bc_symmetry_kernel(DevZone z, BcFace b) {  // BoundCond.cuh:52-118
+static __global__ void bc_symmetry_kernel(DevZone z, BcFace b) {  // BoundCond.cuh:52-118
   const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = b.rs[2] + blockIdx.z;
@@ -517,7 +518,7 @@ __global__ void bc_symmetry_kernel(DevZone z, BcFace b) {  // BoundCond.cuh:52-1
 
 // periodic wrap (no reference counterpart): ghost layer gg of this face takes
 // the point n cells back along the face normal
-__global__ void bc_periodic_kernel(DevZone z, BcFace b, int with_cv) {
+static __global__ void bc_periodic_kernel(DevZone z, BcFace b, int with_cv) {
   const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = b.rs[2] + blockIdx.z;
@@ -754,7 +755,7 @@ __global__ void bc_back_pressure_kernel(DevZone z, BcFace b, int with_cv) {
 }
 
 // subsonic inflow from total conditions, air (BoundCond.cuh:528-634)
-__global__ void bc_subsonic_inflow_kernel(DevZone z, BcFace b, int with_cv) {
+static __global__ void bc_subsonic_inflow_kernel(DevZone z, BcFace b, int with_cv) {
   const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = b.rs[2] + blockIdx.z;
@@ -859,7 +860,7 @@ __device__ __forceinline__ void store_last_cells(const DevZone &z, const int bx,
   z.bv_last[3 * z.nsz + n] = z.bv[5 * z.sz + g];
 }
 
-__global__ void store_last_kernel(DevZone z) {
+static __global__ void store_last_kernel(DevZone z) {
   store_last_cells(z, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -870,7 +871,7 @@ __global__ void store_last_kernel(DevZone z) {
 // the key (step << 44 | block << 34 | interior cell index; the step of the
 // call, at most 2^20 - 1, and a block below 1024) to an atomic minimum, so the
 // host learns the first failing cell of the earliest step.
-__global__ void __launch_bounds__(256) residual_partial_kernel(DevZone z, double *partial, unsigned long long *bad,
+static __global__ void __launch_bounds__(256) residual_partial_kernel(DevZone z, double *partial, unsigned long long *bad,
                                                                const int *step, int block) {
   const long long n = (long long)z.mx * z.my * z.mz;
   double s[4] = {0, 0, 0, 0};
@@ -908,7 +909,7 @@ __global__ void __launch_bounds__(256) residual_partial_kernel(DevZone z, double
 }
 
 // sums n_part partials (fixed order) of every zone and writes sqrt(sum / n_total)
-__global__ void residual_final_kernel(const double *partial, int n_part, double n_total, double *out) {
+static __global__ void residual_final_kernel(const double *partial, int n_part, double n_total, double *out) {
   const int l = threadIdx.x;
   if (l >= 4) return;
   double s = 0;
@@ -996,6 +997,7 @@ cudaError_t launch_table(const CellTable &tab, const Op &op, cudaStream_t s) {
 }
 }  // namespace
 
+#ifndef OSTC_NS_UNIT
 cudaError_t upload_zones(const DevZone *z, int n, cudaStream_t s) {
   if (n < 0 || n > kMaxTableZones) return cudaErrorInvalidValue;
   cudaError_t e = n ? cudaMemcpyToSymbolAsync(c_zones, z, sizeof(DevZone) * n, 0, cudaMemcpyHostToDevice, s)
@@ -1004,8 +1006,17 @@ cudaError_t upload_zones(const DevZone *z, int n, cudaStream_t s) {
   if (e == cudaSuccess) e = upload_zones_flux9(z, n, s);
   if (e == cudaSuccess) e = upload_zones_flux0t(z, n, s);
   if (e == cudaSuccess) e = upload_zones_flux9t(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_ns_a(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_flux_ns_a(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_ns_b(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_flux_ns_b(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_ns_c(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_flux_ns_c(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_ns_d(z, n, s);
+  if (e == cudaSuccess) e = upload_zones_flux_ns_d(z, n, s);
   return e;
 }
+#endif  // OSTC_NS_UNIT
 
 template <int NS>
 cudaError_t launch_cells_table(CellOp op, const CellTable &tab, const CellArgs &a, cudaStream_t s) {
@@ -1065,16 +1076,18 @@ cudaError_t launch_cells(CellOp op, const DevZone &z, const CellArgs &a, cudaStr
   return cudaGetLastError();
 }
 
+#ifndef OSTC_NS_UNIT
 cudaError_t launch_residual_final(const double *partial, int n_part, double n_total, double *out, cudaStream_t s) {
   residual_final_kernel<<<1, 32, 0, s>>>(partial, n_part, n_total, out);
   return cudaGetLastError();
 }
+#endif  // OSTC_NS_UNIT
 
 // 2-D blocks (mz == 1): eliminate_k_gradient (FieldOperation.cuh:372-400).
 // Every ghost plane k = +-1 .. +-ngg of bv, sv (and cv) becomes a copy of the
 // plane k = 0, over the whole ghosted (i, j) range, so every difference
 // across k vanishes.
-__global__ void eliminate_k_kernel(DevZone z, int with_cv) {
+static __global__ void eliminate_k_kernel(DevZone z, int with_cv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x - z.ngg;
   const int j = blockIdx.y * blockDim.y + threadIdx.y - z.ngg;
   if (i >= z.mx + z.ngg || j >= z.my + z.ngg) return;
@@ -1089,6 +1102,7 @@ __global__ void eliminate_k_kernel(DevZone z, int with_cv) {
   }
 }
 
+#ifndef OSTC_NS_UNIT
 cudaError_t launch_eliminate_k(const DevZone &z, int with_cv, cudaStream_t s) {
   if (z.mz != 1) return cudaSuccess;
   const dim3 blk(32, 8);
@@ -1096,6 +1110,7 @@ cudaError_t launch_eliminate_k(const DevZone &z, int with_cv, cudaStream_t s) {
   eliminate_k_kernel<<<grid, blk, 0, s>>>(z, with_cv);
   return cudaGetLastError();
 }
+#endif  // OSTC_NS_UNIT
 
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s) {
@@ -1213,6 +1228,7 @@ cudaError_t launch_chem_split(int op, const DevZone &z, const double *dt_dev, do
   return cudaGetLastError();
 }
 
+#ifndef OSTC_NS_UNIT
 cudaError_t prepare_chem_surrogate() {
   return cudaFuncSetAttribute(surrogate_chem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SM_BYTES);
 }
@@ -1237,8 +1253,17 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   if (e == cudaSuccess) e = upload_param_flux9(p, s);
   if (e == cudaSuccess) e = upload_param_flux0t(p, s);
   if (e == cudaSuccess) e = upload_param_flux9t(p, s);
+  if (e == cudaSuccess) e = upload_param_ns_a(p, s);
+  if (e == cudaSuccess) e = upload_param_flux_ns_a(p, s);
+  if (e == cudaSuccess) e = upload_param_ns_b(p, s);
+  if (e == cudaSuccess) e = upload_param_flux_ns_b(p, s);
+  if (e == cudaSuccess) e = upload_param_ns_c(p, s);
+  if (e == cudaSuccess) e = upload_param_flux_ns_c(p, s);
+  if (e == cudaSuccess) e = upload_param_ns_d(p, s);
+  if (e == cudaSuccess) e = upload_param_flux_ns_d(p, s);
   return e;
 }
+#endif  // OSTC_NS_UNIT
 
 #define OSTC_INSTANTIATE(NS)                                                                                  \
   template cudaError_t launch_cells<NS>(CellOp, const DevZone &, const CellArgs &, cudaStream_t);            \
@@ -1253,7 +1278,23 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   template cudaError_t launch_chem_split<NS>(int, const DevZone &, const double *, double, double *, long long *,        \
                                              const int *, cudaStream_t);
 
+#ifndef OSTC_NS_UNIT
 OSTC_INSTANTIATE(0)
 OSTC_INSTANTIATE(9)
+#else
+// a unit of further species counts (kernels_ns*.cu): OSTC_NS_LIST(X) names
+// them, OSTC_NS_UNIT the unit; its own parameter and zone copies are written
+// through upload_param_<unit> / upload_zones_<unit>
+OSTC_NS_LIST(OSTC_INSTANTIATE)
+#define OSTC_CAT2(a, b) a##b
+#define OSTC_CAT(a, b) OSTC_CAT2(a, b)
+cudaError_t OSTC_CAT(upload_param_, OSTC_NS_UNIT)(const DevParam &p, cudaStream_t s) {
+  return cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
+}
+cudaError_t OSTC_CAT(upload_zones_, OSTC_NS_UNIT)(const DevZone *z, int n, cudaStream_t s) {
+  if (n < 0 || n > kMaxTableZones) return cudaErrorInvalidValue;
+  return n ? cudaMemcpyToSymbolAsync(c_zones, z, sizeof(DevZone) * n, 0, cudaMemcpyHostToDevice, s) : cudaSuccess;
+}
+#endif
 
 }  // namespace ostc

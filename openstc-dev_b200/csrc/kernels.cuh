@@ -158,6 +158,25 @@ cudaError_t upload_param_flux0(const DevParam &p, cudaStream_t s);   // flux0.cu
 cudaError_t upload_param_flux9(const DevParam &p, cudaStream_t s);   // flux9.cu
 cudaError_t upload_param_flux0t(const DevParam &p, cudaStream_t s);  // flux0t.cu
 cudaError_t upload_param_flux9t(const DevParam &p, cudaStream_t s);  // flux9t.cu
+// the units of the other species counts, 1..OSTC_MAX_SPEC
+cudaError_t upload_param_ns_a(const DevParam &p, cudaStream_t s);       // kernels_ns_a.cu
+cudaError_t upload_zones_ns_a(const DevZone *z, int n, cudaStream_t s);
+cudaError_t upload_param_flux_ns_a(const DevParam &p, cudaStream_t s);  // flux_ns_a.cu
+cudaError_t upload_zones_flux_ns_a(const DevZone *z, int n, cudaStream_t s);
+cudaError_t upload_param_ns_b(const DevParam &p, cudaStream_t s);       // kernels_ns_b.cu
+cudaError_t upload_zones_ns_b(const DevZone *z, int n, cudaStream_t s);
+cudaError_t upload_param_flux_ns_b(const DevParam &p, cudaStream_t s);  // flux_ns_b.cu
+cudaError_t upload_zones_flux_ns_b(const DevZone *z, int n, cudaStream_t s);
+cudaError_t upload_param_ns_c(const DevParam &p, cudaStream_t s);       // kernels_ns_c.cu
+cudaError_t upload_zones_ns_c(const DevZone *z, int n, cudaStream_t s);
+cudaError_t upload_param_flux_ns_c(const DevParam &p, cudaStream_t s);  // flux_ns_c.cu
+cudaError_t upload_zones_flux_ns_c(const DevZone *z, int n, cudaStream_t s);
+cudaError_t upload_param_ns_d(const DevParam &p, cudaStream_t s);       // kernels_ns_d.cu
+cudaError_t upload_zones_ns_d(const DevZone *z, int n, cudaStream_t s);
+cudaError_t upload_param_flux_ns_d(const DevParam &p, cudaStream_t s);  // flux_ns_d.cu
+cudaError_t upload_zones_flux_ns_d(const DevZone *z, int n, cudaStream_t s);
+// every species count with a build: 0 (air), 1..OSTC_MAX_SPEC
+constexpr int kMaxBuiltSpecies = OSTC_MAX_SPEC;
 // whether a mechanism has the structure of the generated mech_h2air9.cuh
 bool mechanism_is_h2air9(const int *reac_type, const int *stoi_f, const int *stoi_b, const int *reac_order, int nr,
                          int ns);

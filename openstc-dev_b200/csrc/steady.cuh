@@ -152,7 +152,7 @@ constexpr int nvx() {
 }
 
 // SST::implicit_treat_for_SST under the explicit steady path (SST.cu:8-22)
-__global__ void __launch_bounds__(256) turb_implicit_kernel(DevZone z) {
+static __global__ void __launch_bounds__(256) turb_implicit_kernel(DevZone z) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(256) dplur_finish_kernel(DevZone z, const doub
 
 // zero dq on a wall face range; points outside dq's allocation are skipped
 template <int NS>
-__global__ void wall_dq_zero_kernel(DevZone z, BcFace b, double *dqv) {
+static __global__ void wall_dq_zero_kernel(DevZone z, BcFace b, double *dqv) {
   const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = b.rs[2] + blockIdx.z;

@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(256) chem_features_kernel(int n, const double 
 }
 
 // the network on the tensor cores over the staged rows (tc_mlp.cuh)
-__global__ void __launch_bounds__(tc::THREADS, 1) surrogate_chem_kernel(mlp::Net net, const __nv_bfloat16 *x,
+static __global__ void __launch_bounds__(tc::THREADS, 1) surrogate_chem_kernel(mlp::Net net, const __nv_bfloat16 *x,
                                                                          float *y, int n, int *err) {
   tc::PackedIo io{x, y, n};
   tc::mlp_tiles(net, (n + tc::ROWS - 1) / tc::ROWS, io, err);

@@ -1282,7 +1282,7 @@ def mixture_state(mech: Mechanism, Y, T, p, mach):
 
 
 def case_mixing_layer(mx=256, my=256, mz=256, dx=1e-4, seed=2024, steps=200, full_host=False, mech=None,
-                      cfl=0.4, rans_model=0, wall=False, compressibility_correction=0) -> Case:
+                      cfl=0.4, rans_model=0, wall=False, compressibility_correction=0, mix_model=None) -> Case:
     """The reacting mixing layer: upper stream (y > 0) air (O2/N2 mass
     0.233/0.767) at 1500 K, Mach 2; lower stream H2/N2 (mole 0.3/0.7) at
     300 K, Mach 1.2; p = 1 atm; profiles blended by 0.5(1 + tanh(y / 8dy));
@@ -1294,11 +1294,16 @@ def case_mixing_layer(mx=256, my=256, mz=256, dx=1e-4, seed=2024, steps=200, ful
     faces in x and y, periodic in z. rans_model=2: k-omega SST (Driver<FR,
     SST>) with k = 1.5 (0.01 U)^2 and omega = rho k / (10 * 1.8e-5) from
     the local stream speed U and density, the wall distance to the j = 0
-    plane; wall=True makes j = 0 an isothermal 300 K wall (the fuel side)."""
+    plane; wall=True makes j = 0 an isothermal 300 K wall (the fuel side).
+    mech: any mechanism holding O2, N2 and H2 (species up to OSTC_MAX_SPEC);
+    mix_model defaults to finite-rate chemistry when the mechanism has
+    reactions and to the non-reacting mixture (MIX_MIXTURE) when it has none."""
     import chemdata
 
     mech = mech or chemdata.h2_air_9sp()
-    s = Scheme(mix_model=MIX_FR, inviscid_scheme=3, reconstruction=2, limiter=0, viscous_order=2, chemSrcMethod=1,
+    if mix_model is None:
+        mix_model = MIX_FR if mech.n_reac > 0 else MIX_MIXTURE
+    s = Scheme(mix_model=mix_model, inviscid_scheme=3, reconstruction=2, limiter=0, viscous_order=2, chemSrcMethod=1,
                cfl=cfl, rans_model=rans_model, compressibility_correction=compressibility_correction)
     ng = s.ngg
     ns = mech.n_spec
