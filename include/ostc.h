@@ -45,7 +45,8 @@ typedef enum ostc_status {
   OSTC_ERR_TIMEOUT = 3,       /* a bounded device wait gave up              */
   OSTC_ERR_NONPHYSICAL = 4,   /* NaN / non-positive density or pressure     */
   OSTC_ERR_UNSUPPORTED = 5,   /* scheme combination not built               */
-  OSTC_ERR_NO_DEVICE = 6      /* no CUDA device visible                     */
+  OSTC_ERR_NO_DEVICE = 6,     /* no CUDA device visible                     */
+  OSTC_ERR_IO = 7             /* a file could not be opened, read or written */
 } ostc_status;
 
 /* Mixture model, same meaning as cfd::MixtureModel (src/Define.h:19-25).  */
@@ -295,6 +296,36 @@ ostc_status ostc_set_statistics(ostc_ctx *ctx, int on, int start_step);
  * statistics were switched on). Synchronises the device.                  */
 ostc_status ostc_get_statistics(ostc_ctx *ctx, int block, double *sum12, double *sum34, double *sum_rs,
                                 double *sum_yk, int *n_collected);
+
+/* ---- restart and output: the reference's flow-field file --------------- */
+/* Writes the context's flow field to `path` in the layout of
+ * FieldIO::print_field (src/FieldIO.h:44-560), the file the reference
+ * restarts from (output/field/flowfield.plt): Tecplot binary V112, one
+ * ordered zone "zone b" per block with the solution time, nodal FP64 values
+ * over [-ngg_out, m + ngg_out) per axis of x, y, z, density, u, v, w,
+ * pressure, temperature, mach, the species (named by species_names, n_spec
+ * HOST strings), and tke, omega, mut with SST, each with its min / max in the
+ * zone header. x, y, z: HOST arrays per block with the block's ngg ghost
+ * layers (the reference's Block::x); the flow data are copied from the
+ * blocks' device arrays (mach as the properties last computed it).
+ * Synchronises the device; OSTC_ERR_IO when the file cannot be written.    */
+ostc_status ostc_write_flowfield(ostc_ctx *ctx, const char *path, const double *const *x,
+                                 const double *const *y, const double *const *z,
+                                 const char *const *species_names, int ngg_out, double solution_time);
+/* Reads such a file into the blocks' bv and sv device arrays as
+ * read_flowfield (src/Initialize.cuh:64-243): variables are matched by name,
+ * case-insensitive, as identify_variable_labels (src/Initialize.cuh:
+ * 246-310) does: DENSITY / ROE / RHO, U, V, W, P / PRESSURE, T / TEMPERATURE,
+ * the species names, and K / TKE, OMEGA with SST; others are skipped. A zone
+ * may hold fewer ghost layers than its block ((file extent - m) / 2); the
+ * values it does not cover keep theirs. *found (optional) gets bit 0 when
+ * species were in the file and bit 1 when k and omega were (the reference
+ * then initialises what is missing from the inflow, src/Initialize.cuh:
+ * 195-214; here the caller does), *solution_time (optional) the zones' time
+ * (for ostc_set_physical_time). Call ostc_initialize afterwards.
+ * Synchronises the device.                                                 */
+ostc_status ostc_read_flowfield(ostc_ctx *ctx, const char *path, const char *const *species_names,
+                                double *solution_time, int *found);
 
 /* eliminate_k_gradient<with_cv> (src/FieldOperation.cuh:372-400): on 2-D
  * blocks (mz == 1) every k ghost plane of bv, sv (and cv when with_cv) takes

@@ -9,6 +9,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "../host/flowfield.h"
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -1438,6 +1439,89 @@ ostc_status ostc_get_statistics(ostc_ctx *ctx, int block, double *sum12, double 
   if (sum_yk && ctx->prm.n_spec > 0)
     CK(cudaMemcpy(sum_yk, st.syk, sizeof(double) * ctx->prm.n_spec * n, cudaMemcpyDeviceToHost));
   if (n_collected) CK(cudaMemcpy(n_collected, st.count, sizeof(int), cudaMemcpyDeviceToHost));
+  return OSTC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// restart / output files (FieldIO::print_field, read_flowfield)
+// ---------------------------------------------------------------------------
+static std::vector<std::string> species_list(const ostc_ctx *ctx, const char *const *names) {
+  std::vector<std::string> v;
+  for (int l = 0; l < ctx->prm.n_spec; ++l) v.emplace_back(names[l] ? names[l] : "");
+  return v;
+}
+
+ostc_status ostc_write_flowfield(ostc_ctx *ctx, const char *path, const double *const *x, const double *const *y,
+                                 const double *const *z, const char *const *species_names, int ngg_out,
+                                 double solution_time) {
+  if (!ctx || !path || !x || !y || !z || ngg_out < 0) return OSTC_ERR_INVALID_ARG;
+  const int ns = ctx->prm.n_spec, nsc = ctx->prm.n_scalar;
+  const bool sst = ctx->nt > 0;
+  if (ns > 0 && !species_names) return OSTC_ERR_INVALID_ARG;
+  const size_t nb = ctx->zones.size();
+  for (size_t b = 0; b < nb; ++b)
+    if (!x[b] || !y[b] || !z[b] || ngg_out > ctx->zones[b].ngg || !ctx->zones[b].mach) return OSTC_ERR_INVALID_ARG;
+  CK(cudaDeviceSynchronize());
+  std::vector<std::vector<double>> hbv(nb), hsv(nb), hmach(nb), hmut(nb);
+  std::vector<ostc_io::PltBlock> blocks(nb);
+  for (size_t b = 0; b < nb; ++b) {
+    const ostc_zone &z0 = ctx->zones[b];
+    const size_t sz = (size_t)(z0.mx + 2 * z0.ngg) * (z0.my + 2 * z0.ngg) * (z0.mz + 2 * z0.ngg);
+    hbv[b].resize(6 * sz);
+    hmach[b].resize(sz);
+    CK(cudaMemcpy(hbv[b].data(), z0.bv, 6 * sz * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(hmach[b].data(), z0.mach, sz * sizeof(double), cudaMemcpyDeviceToHost));
+    if (nsc > 0) {
+      hsv[b].resize(nsc * sz);
+      CK(cudaMemcpy(hsv[b].data(), z0.sv, nsc * sz * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    if (sst) {
+      hmut[b].resize(sz);
+      CK(cudaMemcpy(hmut[b].data(), z0.mut, sz * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    ostc_io::PltBlock &B = blocks[b];
+    B.mx = z0.mx, B.my = z0.my, B.mz = z0.mz, B.ngg = z0.ngg;
+    B.x = x[b], B.y = y[b], B.z = z[b];
+    B.bv = hbv[b].data(), B.mach = hmach[b].data();
+    B.sv = nsc > 0 ? hsv[b].data() : nullptr;
+    B.mut = sst ? hmut[b].data() : nullptr;
+  }
+  const int r = ostc_io::write_plt(path, blocks, species_list(ctx, species_names), sst, ngg_out, solution_time);
+  return r == 0 ? OSTC_OK : fail(ctx, OSTC_ERR_IO);
+}
+
+ostc_status ostc_read_flowfield(ostc_ctx *ctx, const char *path, const char *const *species_names,
+                                double *solution_time, int *found) {
+  if (!ctx || !path) return OSTC_ERR_INVALID_ARG;
+  const int ns = ctx->prm.n_spec, nsc = ctx->prm.n_scalar;
+  if (ns > 0 && !species_names) return OSTC_ERR_INVALID_ARG;
+  const size_t nb = ctx->zones.size();
+  CK(cudaDeviceSynchronize());
+  // the variables the file does not hold keep their values
+  std::vector<std::vector<double>> hbv(nb), hsv(nb);
+  std::vector<ostc_io::PltBlock> blocks(nb);
+  for (size_t b = 0; b < nb; ++b) {
+    const ostc_zone &z0 = ctx->zones[b];
+    const size_t sz = (size_t)(z0.mx + 2 * z0.ngg) * (z0.my + 2 * z0.ngg) * (z0.mz + 2 * z0.ngg);
+    hbv[b].resize(6 * sz);
+    CK(cudaMemcpy(hbv[b].data(), z0.bv, 6 * sz * sizeof(double), cudaMemcpyDeviceToHost));
+    if (nsc > 0) {
+      hsv[b].resize(nsc * sz);
+      CK(cudaMemcpy(hsv[b].data(), z0.sv, nsc * sz * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    ostc_io::PltBlock &B = blocks[b];
+    B.mx = z0.mx, B.my = z0.my, B.mz = z0.mz, B.ngg = z0.ngg;
+    B.bv_out = hbv[b].data();
+    B.sv_out = nsc > 0 ? hsv[b].data() : nullptr;
+  }
+  const int r = ostc_io::read_plt(path, blocks, species_list(ctx, species_names), ctx->nt > 0, solution_time, found);
+  if (r == 3) return fail(ctx, OSTC_ERR_INVALID_ARG);
+  if (r != 0) return fail(ctx, OSTC_ERR_IO);
+  for (size_t b = 0; b < nb; ++b) {
+    const ostc_zone &z0 = ctx->zones[b];
+    CK(cudaMemcpy(z0.bv, hbv[b].data(), hbv[b].size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (nsc > 0) CK(cudaMemcpy(z0.sv, hsv[b].data(), hsv[b].size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   return OSTC_OK;
 }
 

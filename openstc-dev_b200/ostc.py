@@ -24,9 +24,9 @@ MAX_SPEC = 20
 MAX_REAC = 50
 
 # status codes (include/ostc.h)
-OK, ERR_INVALID_ARG, ERR_CUDA, ERR_TIMEOUT, ERR_NONPHYSICAL, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(7)
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_TIMEOUT, ERR_NONPHYSICAL, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_IO = range(8)
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "CUDA", 3: "TIMEOUT", 4: "NONPHYSICAL", 5: "UNSUPPORTED",
-                6: "NO_DEVICE"}
+                6: "NO_DEVICE", 7: "IO"}
 MIX_AIR, MIX_MIXTURE, MIX_FR = 0, 1, 2
 BC_WALL, BC_SYMMETRY, BC_FARFIELD, BC_INFLOW, BC_OUTFLOW = 2, 3, 4, 5, 6
 BC_SUBSONIC_INFLOW, BC_BACK_PRESSURE, BC_PERIODIC = 7, 9, 100
@@ -154,6 +154,8 @@ def lib():
             "ostc_surrogate_forward_tc": [vp, vp, i, vp, vp],
             "ostc_surrogate_set_checks": [vp, i, i, C.POINTER(d), C.POINTER(d), d, d],
             "ostc_surrogate_inject_timeout": [vp, i],
+            "ostc_write_flowfield": [vp, C.c_char_p, vp, vp, vp, vp, i, d],
+            "ostc_read_flowfield": [vp, C.c_char_p, vp, C.POINTER(d), C.POINTER(i)],
             "ostc_chem_surrogate": [vp, vp, i, vp, vp, vp, vp, vp, vp, C.POINTER(i), vp],
             "ostc_set_chem_surrogate": [vp, vp],
             "ostc_use_generated_chemistry": [vp, i],
@@ -489,6 +491,7 @@ class Solver:
         import torch
 
         self.scheme = scheme
+        self.mech = mech
         self.blocks = blocks
         self.param, self._keep = make_param(scheme, mech)
         self.config = make_config(scheme, output_screen)
@@ -580,6 +583,27 @@ class Solver:
         check(lib().ostc_get_monitor(self.ctx, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(rec)),
               "ostc_get_monitor")
         return out[:n, :rec.value]
+
+    def _names(self):
+        names = list(self.mech.names) if (self.mech is not None and self.param.n_spec > 0) else []
+        arr = (C.c_char_p * max(1, len(names)))(*[n.encode() for n in names])
+        return arr if names else None
+
+    def write_flowfield(self, path, coords, ngg_out=0, solution_time=0.0):
+        """the reference's restart / output file (ostc_write_flowfield);
+        coords: per block (x, y, z) host arrays with the block's ghost layers"""
+        keep = [np.ascontiguousarray(a, dtype=np.float64) for xyz in coords for a in xyz]
+        ptrs = [(C.c_void_p * len(coords))(*[keep[3 * b + c].ctypes.data for b in range(len(coords))])
+                for c in range(3)]
+        check(lib().ostc_write_flowfield(self.ctx, str(path).encode(), *ptrs, self._names(), ngg_out,
+                                         float(solution_time)), "ostc_write_flowfield")
+
+    def read_flowfield(self, path):
+        """fills bv / sv from such a file; returns (solution_time, found bits)"""
+        t, f = C.c_double(), C.c_int()
+        check(lib().ostc_read_flowfield(self.ctx, str(path).encode(), self._names(), C.byref(t), C.byref(f)),
+              "ostc_read_flowfield")
+        return t.value, f.value
 
     def get_error(self):
         """the context's last status and, for OSTC_ERR_NONPHYSICAL, the first
