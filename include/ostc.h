@@ -297,6 +297,39 @@ ostc_status ostc_set_statistics(ostc_ctx *ctx, int on, int start_step);
 ostc_status ostc_get_statistics(ostc_ctx *ctx, int block, double *sum12, double *sum34, double *sum_rs,
                                 double *sum_yk, int *n_collected);
 
+/* ---- grid pre-processing: the reference's grid and boundary files ------- */
+/* A mesh read on the host as cfd::Mesh reads it (src/Mesh.cpp:550-588) from
+ * the text grid file (input_files/grid/grid N.grd: block count, mx my mz per
+ * block, then x, y, z of each block with i fastest), the boundary file
+ * (boundary N.txt: per block a face count, then i1 i2 j1 j2 k1 k2 label) and
+ * the inner-face file (inner N.txt; NULL: no interfaces): faces and 1-to-1
+ * interfaces registered as Boundary / InnerFace::register_boundary
+ * (src/Mesh.cpp:14-178), coordinates scaled by grid_scale, ghost grid
+ * extrapolated, copied across interfaces and completed at edges and corners
+ * (init_ghost_grid, src/Mesh.cpp:789-987), and the Jacobian and metrics of
+ * ostc_metric_from_grid. Host only; one process (no parallel-interface
+ * file). OSTC_ERR_IO: a file is missing or malformed.                      */
+typedef struct ostc_mesh ostc_mesh;
+ostc_status ostc_mesh_read(const char *grid_file, const char *boundary_file, const char *inner_file, int ngg,
+                           double grid_scale, ostc_mesh **out);
+ostc_status ostc_mesh_destroy(ostc_mesh *m);
+/* counts: blocks, dimension (2 when the first block has mz == 1), boundary
+ * faces and interfaces over all blocks (each may be NULL)                   */
+ostc_status ostc_mesh_sizes(const ostc_mesh *m, int *n_blocks, int *dimension, int *n_faces, int *n_interfaces);
+/* one block: its extents and, where non-NULL, HOST arrays with ngg ghost
+ * layers (the ostc_zone layout) of x, y, z, the Jacobian and the 80-byte
+ * metric records                                                            */
+ostc_status ostc_mesh_block(const ostc_mesh *m, int b, int *mx, int *my, int *mz, double *x, double *y, double *z,
+                            double *jac, void *metric);
+/* the registered boundary faces of all blocks, block by block in file order:
+ * block, type_label (the file's label), face, direction and ranges; the
+ * condition's state is left zero, and wall faces are not yet trimmed (the
+ * boundary-condition set-up does both, src/BoundCond.cu:167-416)           */
+ostc_status ostc_mesh_faces(const ostc_mesh *m, ostc_bc_face *faces);
+/* the registered interfaces of all blocks, block by block in file order,
+ * ready for ostc_set_interfaces                                             */
+ostc_status ostc_mesh_interfaces(const ostc_mesh *m, ostc_interface *faces);
+
 /* ---- restart and output: the reference's flow-field file --------------- */
 /* Writes the context's flow field to `path` in the layout of
  * FieldIO::print_field (src/FieldIO.h:44-560), the file the reference

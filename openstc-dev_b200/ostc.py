@@ -155,6 +155,12 @@ def lib():
             "ostc_surrogate_set_checks": [vp, i, i, C.POINTER(d), C.POINTER(d), d, d],
             "ostc_surrogate_inject_timeout": [vp, i],
             "ostc_write_flowfield": [vp, C.c_char_p, vp, vp, vp, vp, i, d],
+            "ostc_mesh_read": [C.c_char_p, C.c_char_p, C.c_char_p, i, d, C.POINTER(vp)],
+            "ostc_mesh_destroy": [vp],
+            "ostc_mesh_sizes": [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(i)],
+            "ostc_mesh_block": [vp, i, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp, vp, vp, vp, vp],
+            "ostc_mesh_faces": [vp, vp],
+            "ostc_mesh_interfaces": [vp, vp],
             "ostc_read_flowfield": [vp, C.c_char_p, vp, C.POINTER(d), C.POINTER(i)],
             "ostc_chem_surrogate": [vp, vp, i, vp, vp, vp, vp, vp, vp, C.POINTER(i), vp],
             "ostc_set_chem_surrogate": [vp, vp],
@@ -1570,3 +1576,231 @@ class Surrogate:
         check(lib().ostc_surrogate_train_step(self.h, xs.data_ptr(), ys.data_ptr(), xs.shape[0], float(lr),
                                               loss_dev.data_ptr() if loss_dev is not None else None, self._s()),
               "ostc_surrogate_train_step")
+
+
+# ---------------------------------------------------------------------------
+# the reference's input files: grid, boundary and inner-face files, setup files
+# ---------------------------------------------------------------------------
+@dataclass
+class Mesh:
+    """A mesh read by ostc_mesh_read: per block the extents and the host
+    arrays x, y, z, jac, metric (ngg ghost layers), the registered boundary
+    faces (file labels, no state yet) and interfaces."""
+    dimension: int
+    ngg: int
+    dims: List[tuple]
+    coords: List[tuple]
+    jac: List[np.ndarray]
+    metric: List[np.ndarray]
+    faces: List[BcFaceC]
+    interfaces: List[IfaceC]
+
+
+def read_mesh(grid_file, boundary_file, inner_file=None, ngg=2, grid_scale=1.0) -> Mesh:
+    """cfd::Mesh's pre-processing (src/Mesh.cpp:550-588) through ostc_mesh_read"""
+    h = C.c_void_p()
+    check(lib().ostc_mesh_read(str(grid_file).encode(), str(boundary_file).encode(),
+                               str(inner_file).encode() if inner_file else None, ngg, float(grid_scale), C.byref(h)),
+          "ostc_mesh_read")
+    try:
+        nb, dim, nf, ni = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().ostc_mesh_sizes(h, C.byref(nb), C.byref(dim), C.byref(nf), C.byref(ni)), "ostc_mesh_sizes")
+        dims, coords, jacs, mets = [], [], [], []
+        for b in range(nb.value):
+            mx, my, mz = C.c_int(), C.c_int(), C.c_int()
+            check(lib().ostc_mesh_block(h, b, C.byref(mx), C.byref(my), C.byref(mz), None, None, None, None, None),
+                  "ostc_mesh_block")
+            shape = plane_shape(mx.value, my.value, mz.value, ngg)
+            x, y, z, jac = (np.zeros(shape) for _ in range(4))
+            met = np.zeros(shape, dtype=METRIC_DTYPE)
+            check(lib().ostc_mesh_block(h, b, C.byref(mx), C.byref(my), C.byref(mz), x.ctypes.data, y.ctypes.data,
+                                        z.ctypes.data, jac.ctypes.data, met.ctypes.data), "ostc_mesh_block")
+            dims.append((mx.value, my.value, mz.value))
+            coords.append((x, y, z))
+            jacs.append(jac)
+            mets.append(met)
+        faces = (BcFaceC * max(1, nf.value))()
+        ifaces = (IfaceC * max(1, ni.value))()
+        check(lib().ostc_mesh_faces(h, faces), "ostc_mesh_faces")
+        if ni.value:
+            check(lib().ostc_mesh_interfaces(h, ifaces), "ostc_mesh_interfaces")
+        return Mesh(dim.value, ngg, dims, coords, jacs, mets, list(faces)[:nf.value], list(ifaces)[:ni.value])
+    finally:
+        lib().ostc_mesh_destroy(h)
+
+
+def read_setup(path) -> dict:
+    """One of the reference's setup files, as Parameter::read_one_file parses
+    it (src/Parameter.cpp:53-163): lines `type key = value` with type int,
+    real, bool or string; `array <type> name { ... }` over one or more lines;
+    `struct name { type key = value ... }`; // and ! start comments. Returns
+    {key: value}, arrays as lists, structs as dicts."""
+    conv = {"int": int, "real": float, "bool": lambda v: bool(int(v)), "string": str}
+    out = {}
+    lines = iter(Path(path).read_text().splitlines())
+    for raw in lines:
+        line = raw.split("//")[0].strip()
+        if not line or raw.lstrip().startswith("!"):
+            continue
+        tok = line.split()
+        if tok[0] in conv and len(tok) >= 4:
+            out[tok[1]] = conv[tok[0]](tok[3])
+        elif tok[0] == "array" and len(tok) >= 3:
+            typ, name = tok[1], tok[2]
+            body = line.split("{", 1)[1] if "{" in line else ""
+            while "}" not in body:
+                body += " " + next(lines).split("//")[0]
+            body = body.split("}", 1)[0]
+            out[name] = [conv[typ](v) for v in body.split()]
+        elif tok[0] == "struct" and len(tok) >= 2:
+            name, st = tok[1], {}
+            for r in lines:
+                r = r.split("//")[0].strip()
+                if r.startswith("}"):
+                    break
+                t = r.split()
+                if len(t) >= 4 and t[0] in conv:
+                    st[t[1]] = conv[t[0]](t[3])
+            out[name] = st
+    return out
+
+
+# default condition types of the labels no named condition claims (src/BoundCond.cu:228-252)
+_LABEL_TYPES = {2: "wall", 3: "symmetry", 4: "farfield", 5: "inflow", 6: "outflow", 7: "subsonic_inflow",
+                9: "back_pressure"}
+_TYPE_LABELS = {"wall": BC_WALL, "symmetry": BC_SYMMETRY, "farfield": BC_FARFIELD, "inflow": BC_INFLOW,
+                "outflow": BC_OUTFLOW, "subsonic_inflow": BC_SUBSONIC_INFLOW, "back_pressure": BC_BACK_PRESSURE}
+
+
+def _nasa_cp(mech, l, T):
+    """cp_k (J/kg/K) of the NASA-7 polynomials (src/Thermo.cu:47-61)"""
+    t = mech.tables
+    tt, c = T, t["high_temp_coeff"][l]
+    if T < t["t_low"][l]:
+        tt, c = t["t_low"][l], t["low_temp_coeff"][l]
+    elif T < t["t_mid"][l]:
+        c = t["low_temp_coeff"][l]
+    return (c[0] + c[1] * tt + c[2] * tt ** 2 + c[3] * tt ** 3 + c[4] * tt ** 4) * R_U / t["mw"][l]
+
+
+def inflow_state(info: dict, mech: Optional[Mechanism] = None) -> dict:
+    """cfd::Inflow from its setup struct (src/BoundCond.cpp:7-90): (mach,
+    pressure, temperature) or (density, velocity, pressure); u, v, w are the
+    direction; species by name (mass fractions, or mole fractions when
+    mole_or_mass = 0); the mixture's cp / cv ratio at the temperature"""
+    ns = mech.n_spec if mech is not None else 0
+    sv = np.zeros(ns)
+    mw = MW_AIR
+    if ns:
+        for n, val in info.items():
+            if n in mech.names:
+                sv[mech.names.index(n)] = val
+        W = mech.tables["mw"]
+        if int(info.get("mole_or_mass", 1)) == 0:
+            sv = sv * W / np.sum(sv * W)
+        mw = 1.0 / np.sum(sv / W)
+    T, p = info.get("temperature", -1.0), info.get("pressure", -1.0)
+    rho = info.get("density", -1.0)
+    if T < 0:
+        T = p * mw / (rho * R_U)
+    gamma = GAMMA_AIR
+    if ns:
+        cp = cv = 0.0
+        for l in range(ns):
+            c = _nasa_cp(mech, l, T)
+            cp += sv[l] * c
+            cv += sv[l] * (c - R_U / W[l])
+        gamma = cp / cv
+    c = math.sqrt(gamma * R_U / mw * T)
+    mach = info.get("mach", -1.0)
+    vel = info.get("velocity", 0.0)
+    if mach < 0:
+        mach = vel / c
+    else:
+        vel = mach * c
+    if rho < 0:
+        rho = p * mw / (R_U * T)
+    return dict(density=rho, u=info.get("u", 1.0) * vel, v=info.get("v", 0.0) * vel, w=info.get("w", 0.0) * vel,
+                pressure=p, temperature=T, velocity=vel, mut=0.0, sv=list(sv))
+
+
+def boundary_setup(setup: dict, faces: List[BcFaceC], ngg: int, mech: Optional[Mechanism] = None) -> List[BcFaceC]:
+    """DBoundCond::initialize_bc_on_GPU (src/BoundCond.cu:167-416) for faces
+    read by read_mesh: each label takes the type of the named condition of
+    `boundary_conditions` that claims it, else the default type of its number;
+    inflow states from their structs (inflow_state), walls isothermal at the
+    struct's temperature or adiabatic; wall faces trimmed by ngg on their
+    tangential axes (src/BoundCond.cu:369-387). Returns new faces whose
+    type_label is the condition type."""
+    named = {}
+    for name in setup.get("boundary_conditions", []):
+        st = setup.get(name)
+        if isinstance(st, dict) and "label" in st:
+            named.setdefault(int(st["label"]), st)
+    out = []
+    for f in faces:
+        st = named.get(f.type_label)
+        typ = st.get("type") if st else _LABEL_TYPES.get(f.type_label)
+        if typ not in _TYPE_LABELS:
+            raise ValueError("boundary label %d: no condition type" % f.type_label)
+        g = BcFaceC()
+        C.pointer(g)[0] = f
+        g.type_label = _TYPE_LABELS[typ]
+        if typ == "inflow" and st:
+            s = inflow_state(st, mech)
+            for k in ("density", "u", "v", "w", "pressure", "temperature", "velocity", "mut"):
+                setattr(g, k, float(s[k]))
+            for l, y in enumerate(s["sv"]):
+                g.sv[l] = float(y)
+        if typ == "wall":
+            if st and st.get("thermal_type", "isothermal") == "isothermal":
+                g.wall_isothermal, g.wall_temperature = 1, float(st.get("temperature", 300.0))
+            for a in range(3):
+                if a != g.face:
+                    g.range_start[a] += ngg
+                    g.range_end[a] -= ngg
+        out.append(g)
+    return out
+
+
+def write_reference_mesh(directory, dims, coords, boundaries, inner=None, n_file=0):
+    """Writes a mesh in the reference's input-file formats under
+    directory/input_files: grid/grid{n:>4}.grd (block count, extents, then x,
+    y, z per block, i fastest), boundary_condition/boundary{n:>4}.txt (per
+    block a count and rows i1 i2 j1 j2 k1 k2 label) and, with inner faces,
+    boundary_condition/inner{n:>4}.txt (count line, faces per block, a title,
+    then per face the source row with its 1-based block and the target row
+    with the target's). coords: per block (x, y, z) arrays of the interior
+    nodes, numpy layout [k][j][i]. Returns the three paths."""
+    root = Path(directory) / "input_files"
+    (root / "grid").mkdir(parents=True, exist_ok=True)
+    (root / "boundary_condition").mkdir(parents=True, exist_ok=True)
+    tag = "%4d" % n_file
+    g = root / "grid" / ("grid%s.grd" % tag)
+    with open(g, "w") as f:
+        f.write("%12d\n" % len(dims))
+        for d in dims:
+            f.write("%12d%12d%12d\n" % tuple(d))
+        for xyz in coords:
+            for a in xyz:
+                vals = np.asarray(a, dtype=np.float64).ravel()
+                for q in range(0, vals.size, 3):
+                    f.write("".join("%24.15f" % v for v in vals[q:q + 3]) + "\n")
+    b = root / "boundary_condition" / ("boundary%s.txt" % tag)
+    with open(b, "w") as f:
+        for rows in boundaries:
+            f.write("%12d\n" % len(rows))
+            for r in rows:
+                f.write("".join("%6d" % v for v in r) + "\n")
+    i = None
+    if inner is not None:
+        i = root / "boundary_condition" / ("inner%s.txt" % tag)
+        with open(i, "w") as f:
+            f.write("%12d\n" % len(dims))
+            f.write("".join("%12d" % len(rows) for rows in inner) + "\n")
+            f.write(" imin  imax  jmin  jmax  kmin  kmax   id\n")
+            for rows in inner:
+                for src, tar in rows:
+                    f.write("".join("%10d" % v for v in src) + "\n")
+                    f.write("".join("%10d" % v for v in tar) + "\n")
+    return g, b, i

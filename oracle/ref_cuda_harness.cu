@@ -18,6 +18,8 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <string>
+#include <unistd.h>
 #include <vector>
 
 // include order of the reference's own translation units (RK.cuh needs the
@@ -780,6 +782,96 @@ int ref_metric(int mx, int my, int mz, int ngg, const double *x, const double *y
   b.compute_jac_metric(0);
   std::memcpy(jac_out, b.jacobian.data(), np * sizeof(double));
   std::memcpy(metric_out, b.metric.data(), np * sizeof(gxl::Matrix<real, 3, 3, 1>));
+  return 0;
+}
+
+// the reference's own Mesh (src/Mesh.cpp:550-588): its grid, boundary and
+// inner-face files read from dir/input_files (grid   0.grd, boundary   0.txt,
+// inner   0.txt), faces registered, ghost grid, metrics. Host only.
+struct RefMesh {
+  Parameter *parameter = nullptr;
+  Mesh *mesh = nullptr;
+};
+
+int ref_mesh_read(const char *dir, int ngg, double grid_scale, void **out) {
+  if (!dir || !out || ngg < 1) return 1;
+  char old[4096];
+  if (!getcwd(old, sizeof(old))) return 2;
+  // the Parameter keys Mesh reads, in the reference's setup-file syntax
+  const std::string pfile = "/tmp/ostc_ref_mesh_param_" + std::to_string((long)getpid()) + ".txt";
+  {
+    FILE *f = std::fopen(pfile.c_str(), "w");
+    if (!f) return 2;
+    std::fprintf(f, "int ngg = %d\nint n_proc = 1\nint myid = 0\nbool parallel = 0\nreal gridScale = %.17g\n", ngg,
+                 grid_scale);
+    std::fclose(f);
+  }
+  if (chdir(dir) != 0) return 2;
+  auto *m = new RefMesh;
+  m->parameter = new Parameter(pfile);
+  m->mesh = new Mesh(*m->parameter);
+  if (chdir(old) != 0) return 2;
+  std::remove(pfile.c_str());
+  *out = m;
+  return 0;
+}
+
+int ref_mesh_counts(void *h, int *n_block, int *dimension) {
+  auto *m = (RefMesh *)h;
+  *n_block = m->mesh->n_block;
+  *dimension = m->mesh->dimension;
+  return 0;
+}
+
+// extents, and x, y, z / jac / metric with ngg ghost layers (any pointer may be NULL)
+int ref_mesh_block(void *h, int b, int *dims, double *x, double *y, double *z, double *jac, void *metric) {
+  auto *m = (RefMesh *)h;
+  if (b < 0 || b >= m->mesh->n_block) return 1;
+  Block &B = (*m->mesh)[b];
+  dims[0] = B.mx, dims[1] = B.my, dims[2] = B.mz;
+  const int g = B.ngg;
+  const size_t np = plane(B.mx, B.my, B.mz, g);
+  if (x) std::memcpy(x, B.x.data(), np * sizeof(double));
+  if (y) std::memcpy(y, B.y.data(), np * sizeof(double));
+  if (z) std::memcpy(z, B.z.data(), np * sizeof(double));
+  if (jac) std::memcpy(jac, B.jacobian.data(), np * sizeof(double));
+  if (metric) std::memcpy(metric, B.metric.data(), np * sizeof(gxl::Matrix<real, 3, 3, 1>));
+  return 0;
+}
+
+// the registered boundary faces of block b: 9 ints each (range_start[3],
+// range_end[3], face, direction, type_label); *n the count (out may be NULL)
+int ref_mesh_boundaries(void *h, int b, int *n, int *out) {
+  auto *m = (RefMesh *)h;
+  Block &B = (*m->mesh)[b];
+  *n = (int)B.boundary.size();
+  if (out)
+    for (size_t q = 0; q < B.boundary.size(); ++q) {
+      const Boundary &f = B.boundary[q];
+      int *o = out + 9 * q;
+      for (int a = 0; a < 3; ++a) o[a] = f.range_start[a], o[3 + a] = f.range_end[a];
+      o[6] = f.face, o[7] = f.direction, o[8] = f.type_label;
+    }
+  return 0;
+}
+
+// the registered inner faces of block b: 25 ints each (range_start[3],
+// range_end[3], target_start[3], loop_dir[3], target_loop_dir[3], src_tar[3],
+// n_point[3], face, direction, target_block, target_face)
+int ref_mesh_inner(void *h, int b, int *n, int *out) {
+  auto *m = (RefMesh *)h;
+  Block &B = (*m->mesh)[b];
+  *n = (int)B.inner_face.size();
+  if (out)
+    for (size_t q = 0; q < B.inner_face.size(); ++q) {
+      const InnerFace &f = B.inner_face[q];
+      int *o = out + 25 * q;
+      for (int a = 0; a < 3; ++a) {
+        o[a] = f.range_start[a], o[3 + a] = f.range_end[a], o[6 + a] = f.target_start[a];
+        o[9 + a] = f.loop_dir[a], o[12 + a] = f.target_loop_dir[a], o[15 + a] = f.src_tar[a], o[18 + a] = f.n_point[a];
+      }
+      o[21] = f.face, o[22] = f.direction, o[23] = f.target_block, o[24] = f.target_face;
+    }
   return 0;
 }
 

@@ -46,6 +46,17 @@ def ref():
         L.ref_download.restype = C.c_int
         L.ref_metric.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, d, d, d, d, vp]
         L.ref_metric.restype = C.c_int
+        ip = C.POINTER(C.c_int)
+        L.ref_mesh_read.argtypes = [C.c_char_p, C.c_int, C.c_double, C.POINTER(vp)]
+        L.ref_mesh_read.restype = C.c_int
+        L.ref_mesh_counts.argtypes = [vp, ip, ip]
+        L.ref_mesh_counts.restype = C.c_int
+        L.ref_mesh_block.argtypes = [vp, C.c_int, ip, d, d, d, d, vp]
+        L.ref_mesh_block.restype = C.c_int
+        L.ref_mesh_boundaries.argtypes = [vp, C.c_int, ip, ip]
+        L.ref_mesh_boundaries.restype = C.c_int
+        L.ref_mesh_inner.argtypes = [vp, C.c_int, ip, ip]
+        L.ref_mesh_inner.restype = C.c_int
         _r = L
     return _r
 
@@ -117,3 +128,40 @@ def metric(mx, my, mz, ngg, x, y, z):
     if st != 0:
         raise RuntimeError("ref_metric -> %d" % st)
     return jac, met
+
+
+def mesh(directory, ngg, grid_scale):
+    """the reference's own cfd::Mesh (src/Mesh.cpp:550-588) from the files
+    under directory/input_files: per block a dict of extents, x, y, z, jac,
+    metric (ngg ghost layers), the registered boundary faces (rows of
+    range_start, range_end, face, direction, label) and inner faces (rows of
+    range_start, range_end, target_start, loop_dir, target_loop_dir, src_tar,
+    n_point, face, direction, target_block, target_face); and the dimension"""
+    h = C.c_void_p()
+    st = ref().ref_mesh_read(str(directory).encode(), ngg, grid_scale, C.byref(h))
+    if st != 0:
+        raise RuntimeError("ref_mesh_read -> %d" % st)
+    nb, dim = C.c_int(), C.c_int()
+    ref().ref_mesh_counts(h, C.byref(nb), C.byref(dim))
+    out = []
+    d = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    for b in range(nb.value):
+        dims = (C.c_int * 3)()
+        ref().ref_mesh_block(h, b, dims, None, None, None, None, None)
+        mx, my, mz = list(dims)
+        shape = ostc.plane_shape(mx, my, mz, ngg)
+        x, y, z, jac = (np.zeros(shape) for _ in range(4))
+        met = np.zeros(shape, dtype=ostc.METRIC_DTYPE)
+        ref().ref_mesh_block(h, b, dims, x.ctypes.data_as(d), y.ctypes.data_as(d), z.ctypes.data_as(d),
+                             jac.ctypes.data_as(d), met.ctypes.data)
+        n = C.c_int()
+        ref().ref_mesh_boundaries(h, b, C.byref(n), None)
+        bnd = np.zeros((n.value, 9), dtype=np.int32)
+        ref().ref_mesh_boundaries(h, b, C.byref(n), bnd.ctypes.data_as(ip))
+        ref().ref_mesh_inner(h, b, C.byref(n), None)
+        inner = np.zeros((n.value, 25), dtype=np.int32)
+        ref().ref_mesh_inner(h, b, C.byref(n), inner.ctypes.data_as(ip))
+        out.append({"dims": (mx, my, mz), "x": x, "y": y, "z": z, "jac": jac, "metric": met, "boundaries": bnd,
+                    "inner": inner})
+    return out, dim.value
