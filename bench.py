@@ -11,10 +11,13 @@ Multi-GPU runs (torchrun) are independent replicas, one per rank: the
 single-GPU path has no exchange step of its own (replicas only); value is
 the sum of cell updates over all ranks divided by the max time over ranks.
 
---impl reference times the reference's own physics as FP64 host code
-(oracle/_ref, the reference sources compiled by oracle/build_ref.sh) with
-OpenMP on all host cores, or the oracle port when that library is absent,
-on a bounded sample of the same workload.
+--impl reference times the CPU implementation of the path: the oracle port
+(the reference's kernels restated as FP64 host code, each function citing
+the reference file:line it follows; the reference itself runs the path only
+as CUDA kernels) with OpenMP on all host cores, on a bounded sample of the
+same workload, without loading the product library. The reference's own
+CUDA kernels, compiled for sm_100a into oracle/_ref, are timed on the same
+workload inside our own line (`reference_cuda_build`).
 """
 from __future__ import annotations
 
@@ -89,7 +92,12 @@ def _scheme_text(case, n_blocks=None):
     chem = ", finite-rate chemistry" if case.mech is not None else ""
     nb = len(case.blocks) if n_blocks is None else n_blocks
     blocks = ", %d blocks" % nb if nb > 1 else ""
-    return "%s+%s, %s%s, SSPRK3 CFL %.1f%s" % (rec, inv, vis, chem, sc.cfl, blocks)
+    if sc.steady:
+        adv = ("DPLUR (%d sweeps)" % sc.dplur_inner_step if sc.implicit_method == 1 else "explicit") + \
+              ", local time stepping CFL %.1f" % sc.cfl
+    else:
+        adv = "SSPRK3 CFL %.1f" % sc.cfl
+    return "%s+%s, %s%s, %s%s" % (rec, inv, vis, chem, adv, blocks)
 
 
 # ---------------------------------------------------------------------------

@@ -593,8 +593,9 @@ enum { OSTC_OP_FLUX = 0, OSTC_OP_SOURCE = 1, OSTC_OP_PROPERTIES = 2, OSTC_OP_UPD
        OSTC_OP_BC = 5 };
 ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream);
 
-/* Number of kernel nodes in the CUDA graph of one RK3 step (with or without
- * the residual epilogue); captures the graph if it does not exist yet.     */
+/* Number of kernel nodes in the CUDA graph of one RK3 step, or of one steady
+ * iteration for a steady context (with or without the residual epilogue);
+ * captures the graph if it does not exist yet.                             */
 ostc_status ostc_step_kernel_count(ostc_ctx *ctx, int with_hist, int *count);
 
 /* Residual of one block without any device allocation. No counterpart in

@@ -1288,13 +1288,14 @@ ostc_status ostc_launch_op(ostc_ctx *ctx, int op, int arg, void *stream) {
   }
 }
 
-// kernel launches in one captured step (captures the graph if needed)
+// kernel launches in one captured step: an RK3 step, or a steady iteration for
+// a steady context (captures the graph if needed)
 ostc_status ostc_step_kernel_count(ostc_ctx *ctx, int with_hist, int *count) {
   if (!ctx || !count) return OSTC_ERR_INVALID_ARG;
   ostc_status st;
   if (with_hist && (st = ensure_hist(ctx, 1))) return st;
   GraphEntry *ge = nullptr;
-  if ((st = ensure_graph(ctx, with_hist != 0, &ge))) return st;
+  if ((st = ensure_graph(ctx, with_hist != 0, &ge, ctx->cfg.steady != 0))) return st;
   size_t n = 0;
   CK(cudaGraphGetNodes(ge->graph, nullptr, &n));
   std::vector<cudaGraphNode_t> nodes(n);
