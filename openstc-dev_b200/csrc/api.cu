@@ -1529,20 +1529,23 @@ ostc_status ostc_read_flowfield(ostc_ctx *ctx, const char *path, const char *con
 // tile-shape control for the autotuner: dir 0..2
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
   if (!ctx || dir < 0 || dir > 5) return OSTC_ERR_INVALID_ARG;
-  // rows may carry the register budget in its upper bits: rows | (minb << 8)
+  // rows may carry the register budget and the staged kernels in its upper
+  // bits: rows | (minb << 8) | (staged << 16), staged 1 or 2 = tile buffers
   const int minb = (rows >> 8) & 0xff;
+  const int staged = (rows >> 16) & 0xff;
   rows &= 0xff;
   TileShape &t = ctx->tile[dir % 3];
   if (dir > 2 && rows == 0) {  // back to the fused kernel
     t.vrows = 0;
   } else {
-    if (chunks < 1 || chunks > 4096 || minb < 0 || minb > 5) return OSTC_ERR_INVALID_ARG;
+    if (chunks < 1 || chunks > 4096 || minb < 0 || minb > 5 || staged > 2) return OSTC_ERR_INVALID_ARG;
+    if (staged && minb > 2) return OSTC_ERR_INVALID_ARG;  // the staged kernels are built for 128 registers
     if (!(rows == 1 || rows == 2 || rows == 4 || rows == 8)) return OSTC_ERR_INVALID_ARG;
     if (minb >= 4 && rows > 4) return OSTC_ERR_INVALID_ARG;  // the 168- and 96-register builds take <= 128 threads
     if (dir > 2) {
-      t.vrows = rows, t.vchunks = chunks, t.vminb = minb < 1 ? 1 : minb;
+      t.vrows = rows, t.vchunks = chunks, t.vminb = staged ? 2 : (minb < 1 ? 1 : minb), t.vstaged = staged;
     } else {
-      t.rows = rows, t.chunks = chunks, t.minb = minb < 1 ? 1 : minb;
+      t.rows = rows, t.chunks = chunks, t.minb = staged ? 2 : (minb < 1 ? 1 : minb), t.staged = staged;
     }
   }
   for (auto &kv : ctx->graphs) {
@@ -1577,11 +1580,11 @@ ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks) 
   if (!ctx || dir < 0 || dir > 5 || !rows || !chunks) return OSTC_ERR_INVALID_ARG;
   const TileShape &t = ctx->tile[dir % 3];
   if (dir > 2) {
-    *rows = t.vrows == 0 ? 0 : (t.vrows | (t.vminb > 1 ? (t.vminb << 8) : 0));
+    *rows = t.vrows == 0 ? 0 : (t.vrows | (t.vminb > 1 ? (t.vminb << 8) : 0) | (t.vstaged << 16));
     *chunks = t.vrows == 0 ? 0 : t.vchunks;
     return OSTC_OK;
   }
-  *rows = t.rows | (t.minb > 1 ? (t.minb << 8) : 0);
+  *rows = t.rows | (t.minb > 1 ? (t.minb << 8) : 0) | (t.staged << 16);
   *chunks = t.chunks;
   return OSTC_OK;
 }

@@ -2,9 +2,13 @@
 // central correction, as device functions of one thread.
 //
 // A face of direction DIR lies between the cell at ghosted index gi and the
-// cell at gi + sd (sd = the stride along DIR). All inputs are read straight
-// from the ColMajor planes through the read-only path; threads of a warp
-// always differ in i, so every load is a coalesced 32-wide row.
+// cell at gi + sd (sd = the stride along DIR). The primitive and scalar values
+// of the face's stencil come through a cell accessor: PlaneCells reads the
+// ColMajor planes through the read-only path (threads of a warp always differ
+// in i, so every load is a coalesced 32-wide row); TileCells reads the cells
+// of the CTA's sweep plane from its shared-memory tile and only the cells
+// across that plane from HBM. Metrics and transport properties are read from
+// the planes in both cases.
 #pragma once
 #include "common.cuh"
 #include "sst.cuh"
@@ -21,6 +25,53 @@ __device__ __forceinline__ double bvl(const DevZone &z, int g, int l) { return l
 __device__ __forceinline__ double svl(const DevZone &z, int g, int l) { return ld(z.sv + l * z.isz + g); }
 __device__ __forceinline__ double cvl(const DevZone &z, int g, int l) { return ld(z.cv + l * z.isz + g); }
 __device__ __forceinline__ double met(const DevZone &z, int g, int c) { return ld(z.met + c * z.isz + g); }
+
+// Cell accessors of one face: bv(l, n, a, b) / sv(l, n, a, b) is plane l at
+// n steps along the face normal (n = 0: the cell before the face, 1: the cell
+// after it) and a, b steps along the face's two tangential directions (TA,
+// TB of viscous_face: for the x sweep a = j, b = k; for y, a = i, b = k; for
+// z, a = i, b = j). Every call site passes literal steps, so the tile
+// accessor's choice between shared memory and HBM is resolved at compile time.
+struct PlaneCells {
+  const double *bvp, *svp;
+  int isz, g0, sn, sa, sb;
+  // the cell's index: the face's first cell, then the step along the normal,
+  // then the tangential step
+  __device__ __forceinline__ double at(const double *plane, int n, int a, int b) const {
+    const double *q = plane + (g0 + n * sn);
+    return ld(a != 0 ? q + a * sa : (b != 0 ? q + b * sb : q));
+  }
+  __device__ __forceinline__ double bv(int l, int n, int a = 0, int b = 0) const {
+    return at(bvp + l * isz, n, a, b);
+  }
+  __device__ __forceinline__ double sv(int l, int n, int a = 0, int b = 0) const {
+    return at(svp + l * isz, n, a, b);
+  }
+};
+
+template <int DIR>
+__device__ __forceinline__ PlaneCells plane_cells(const DevZone &z, int g0) {
+  // tangential strides: TA = j for the x sweep, else i; TB = j for the z sweep, else k
+  const int sa = DIR == 0 ? z.d2 : 1;
+  const int sb = DIR == 2 ? z.d2 : z.d1;
+  return PlaneCells{z.bv, z.sv, z.isz, g0, dir_stride<DIR>(z), sa, sb};
+}
+
+// the tile holds, for the CTA's sweep plane (b = 0), bv planes 0..5 then the sv
+// planes, each as a [row][column] array: t points at the thread's own cell of
+// plane 0, tn / ta are the tile strides of one step along n / a, tv the tile
+// stride of one plane; cells across the plane (b != 0) come from HBM
+struct TileCells {
+  PlaneCells p;
+  const double *t;
+  int tn, ta, tv;
+  __device__ __forceinline__ double bv(int l, int n, int a = 0, int b = 0) const {
+    return b != 0 ? p.bv(l, n, a, b) : t[l * tv + n * tn + a * ta];
+  }
+  __device__ __forceinline__ double sv(int l, int n, int a = 0, int b = 0) const {
+    return b != 0 ? p.sv(l, n, a, b) : t[(6 + l) * tv + n * tn + a * ta];
+  }
+};
 
 // 0.5 * (sgn(a) + sgn(b)) * min(|a|, |b|) with sgn(x) = (x < 0 ? -1 : 1)
 // (Limiter.cuh:13-16), written without the integer sum and its conversion:
@@ -196,17 +247,17 @@ __device__ __forceinline__ void riemann(const double *pl, const double *pr, cons
 // Reconstruction.cu:5-46 + Reconstruction.cuh:20-72)
 // ---------------------------------------------------------------------------
 // NT: turbulence scalars (k, omega) after the NS species, reconstructed alike
-template <int NS, int DIR, int NT = 0>
-__device__ __forceinline__ void reconstruct_pv(const DevZone &z, int g0, double *pl, double *pr) {
+template <int NS, int NT, class Cells>
+__device__ __forceinline__ void reconstruct_pv_c(const Cells &c, double *pl, double *pr) {
   constexpr int NV = 5 + NS + NT;
-  const int sd = dir_stride<DIR>(z);
   const int rec = c_p.reconstruction;
+  // variable l of the reconstruction: bv 0..4 (rho, u, v, w, p), then the scalars
+  auto val = [&](int l, int n) { return l < 5 ? c.bv(l, n) : c.sv(l - 5, n); };
 #pragma unroll
   for (int l = 0; l < NV; ++l) {
-    const double *base = l < 5 ? z.bv + l * z.isz : z.sv + (l - 5) * z.isz;
-    const double v0 = ld(base + g0), v1 = ld(base + g0 + sd);
+    const double v0 = val(l, 0), v1 = val(l, 1);
     if (rec == 2 || rec == 3) {
-      const double vm = ld(base + g0 - sd), v2 = ld(base + g0 + 2 * sd);
+      const double vm = val(l, -1), v2 = val(l, 2);
       const double di = v0 - vm, di1 = v1 - v0, di2 = v2 - v1;
       if (rec == 2) {
         constexpr double kappa = 1.0 / 3.0;
@@ -266,10 +317,15 @@ __device__ __forceinline__ void reconstruct_pv(const DevZone &z, int g0, double 
 }
 
 template <int NS, int DIR, int NT = 0>
-__device__ __forceinline__ void inviscid_face_pv(const DevZone &z, int g0, double *F) {
+__device__ __forceinline__ void reconstruct_pv(const DevZone &z, int g0, double *pl, double *pr) {
+  reconstruct_pv_c<NS, NT>(plane_cells<DIR>(z, g0), pl, pr);
+}
+
+template <int NS, int DIR, int NT, class Cells>
+__device__ __forceinline__ void inviscid_face_pv(const DevZone &z, const Cells &c, int g0, double *F) {
   constexpr int NV = 5 + NS + NT;
   double pl[NV + 2], pr[NV + 2];
-  reconstruct_pv<NS, DIR, NT>(z, g0, pl, pr);
+  reconstruct_pv_c<NS, NT>(c, pl, pr);
   riemann<NV, NS>(pl, pr, z, g0, g0 + dir_stride<DIR>(z), DIR, F);
 }
 
@@ -628,32 +684,32 @@ __device__ __forceinline__ void cds_correction(const DevZone &z, int g, double *
 // NT = 2: the SST terms (turbulent viscosity and conductivity, the -2/3 rho k
 // normal stresses, k and omega diffusion with the F1 blend)
 // ---------------------------------------------------------------------------
-template <int NS, int DIR, int NT = 0>
-__device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F) {
+template <int NS, int DIR, int NT, class Cells>
+__device__ __forceinline__ void viscous_face(const DevZone &z, const Cells &cc, int g0, double *F) {
   constexpr int NV = 5 + NS + NT;
   const int sd = dir_stride<DIR>(z);
   const int g1 = g0 + sd;
-  // tangential strides
+  // tangential directions
   constexpr int TA = DIR == 0 ? 1 : 0, TB = DIR == 2 ? 1 : 2;
-  const int sa = TA == 0 ? 1 : (TA == 1 ? z.d2 : z.d1);
-  const int sb = TB == 1 ? z.d2 : z.d1;
   double mm[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) mm[c] = 0.5 * (met(z, g0, c) + met(z, g1, c));
-  // derivative along (normal, ta, tb) ordered as (xi, eta, zeta)
-  auto der = [&](const double *base, double out[3]) {
-    const double dn = ld(base + g1) - ld(base + g0);
-    const double da = 0.25 * (ld(base + g0 + sa) - ld(base + g0 - sa) + ld(base + g1 + sa) - ld(base + g1 - sa));
-    const double db = 0.25 * (ld(base + g0 + sb) - ld(base + g0 - sb) + ld(base + g1 + sb) - ld(base + g1 - sb));
+  // derivative along (normal, ta, tb) ordered as (xi, eta, zeta); v(n, a, b) is the variable's cell value
+  auto der = [&](auto v, double out[3]) {
+    const double dn = v(1, 0, 0) - v(0, 0, 0);
+    const double da = 0.25 * (v(0, 1, 0) - v(0, -1, 0) + v(1, 1, 0) - v(1, -1, 0));
+    const double db = 0.25 * (v(0, 0, 1) - v(0, 0, -1) + v(1, 0, 1) - v(1, 0, -1));
     out[DIR] = dn;
     out[TA] = da;
     out[TB] = db;
   };
+  auto bvv = [&](int l) { return [&cc, l](int n, int a, int b) { return cc.bv(l, n, a, b); }; };
+  auto svv = [&](int l) { return [&cc, l](int n, int a, int b) { return cc.sv(l, n, a, b); }; };
   double du[3], dv[3], dw[3], dt[3];
-  der(z.bv + 1 * z.isz, du);
-  der(z.bv + 2 * z.isz, dv);
-  der(z.bv + 3 * z.isz, dw);
-  der(z.bv + 5 * z.isz, dt);
+  der(bvv(1), du);
+  der(bvv(2), dv);
+  der(bvv(3), dw);
+  der(bvv(5), dt);
   const double u_x = du[0] * mm[0] + du[1] * mm[3] + du[2] * mm[6];
   const double u_y = du[0] * mm[1] + du[1] * mm[4] + du[2] * mm[7];
   const double u_z = du[0] * mm[2] + du[1] * mm[5] + du[2] * mm[8];
@@ -674,7 +730,7 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
     constexpr double delta_d = 1e-3;
     const double dy_div_delta = fmin(0.5 * (ld(z.wall + g0) + ld(z.wall + g1)) / delta_d, 1.0);
     const double twoThirdrhoKm =
-        -2.0 / 3 * 0.5 * (bvl(z, g0, 0) * svl(z, g0, NS) + bvl(z, g1, 0) * svl(z, g1, NS)) * dy_div_delta;
+        -2.0 / 3 * 0.5 * (cc.bv(0, 0) * cc.sv(NS, 0) + cc.bv(0, 1) * cc.sv(NS, 1)) * dy_div_delta;
     txx += twoThirdrhoKm;
     tyy += twoThirdrhoKm;
     tzz += twoThirdrhoKm;
@@ -687,9 +743,9 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
   F[1] = kxj * txx + kyj * txy + kzj * txz;
   F[2] = kxj * txy + kyj * tyy + kzj * tyz;
   F[3] = kxj * txz + kyj * tyz + kzj * tzz;
-  const double um = 0.5 * (bvl(z, g0, 1) + bvl(z, g1, 1));
-  const double vm = 0.5 * (bvl(z, g0, 2) + bvl(z, g1, 2));
-  const double wm = 0.5 * (bvl(z, g0, 3) + bvl(z, g1, 3));
+  const double um = 0.5 * (cc.bv(1, 0) + cc.bv(1, 1));
+  const double vm = 0.5 * (cc.bv(2, 0) + cc.bv(2, 1));
+  const double wm = 0.5 * (cc.bv(3, 0) + cc.bv(3, 1));
   const double t_x = dt[0] * mm[0] + dt[1] * mm[3] + dt[2] * mm[6];
   const double t_y = dt[0] * mm[1] + dt[1] * mm[4] + dt[2] * mm[7];
   const double t_z = dt[0] * mm[2] + dt[1] * mm[5] + dt[2] * mm[8];
@@ -701,12 +757,11 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
     double sgw = 0, srdy = 0, corr = 0, mwt = 0;
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
-      const double *ys = z.sv + l * z.isz;
-      yk[l] = 0.5 * (ld(ys + g0) + ld(ys + g1));
+      yk[l] = 0.5 * (cc.sv(l, 0) + cc.sv(l, 1));
       diff[l] = 0.5 * (ld(z.rhoD + l * z.isz + g0) + ld(z.rhoD + l * z.isz + g1));
       if constexpr (NT > 0) diff[l] += mut / c_p.Sct;  // turbulent diffusivity (ViscousScheme.cuh:122-125)
       double dy[3];
-      der(ys, dy);
+      der(svv(l), dy);
       const double y_x = dy[0] * mm[0] + dy[1] * mm[3] + dy[2] * mm[6];
       const double y_y = dy[0] * mm[1] + dy[1] * mm[4] + dy[2] * mm[7];
       const double y_z = dy[0] * mm[2] + dy[1] * mm[5] + dy[2] * mm[8];
@@ -721,11 +776,11 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
     corr -= mwt * srdy * sgw;
     if (c_p.gradP) {
       double dp[3];
-      der(z.bv + 4 * z.isz, dp);
+      der(bvv(4), dp);
       const double p_x = dp[0] * mm[0] + dp[1] * mm[3] + dp[2] * mm[6];
       const double p_y = dp[0] * mm[1] + dp[1] * mm[4] + dp[2] * mm[7];
       const double p_z = dp[0] * mm[2] + dp[1] * mm[5] + dp[2] * mm[8];
-      const double gp = (kxj * p_x + kyj * p_y + kzj * p_z) / (0.5 * (bvl(z, g1, 4) + bvl(z, g0, 4)));
+      const double gp = (kxj * p_x + kyj * p_y + kzj * p_z) / (0.5 * (cc.bv(4, 1) + cc.bv(4, 0)));
 #pragma unroll
       for (int l = 0; l < NS; ++l) {
         ddf[l] += (mwt * c_p.imw[l] - 1) * yk[l] * gp;
@@ -733,7 +788,7 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
       }
     }
     double h[NS];
-    enthalpy<NS>(0.5 * (bvl(z, g0, 5) + bvl(z, g1, 5)), h);
+    enthalpy<NS>(0.5 * (cc.bv(5, 0) + cc.bv(5, 1)), h);
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
       const double flux = diff[l] * (ddf[l] - mwt * yk[l] * sgw) - yk[l] * corr;
@@ -743,8 +798,8 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
   }
   if constexpr (NT > 0) {  // k and omega diffusion (ViscousScheme.cuh:200-251)
     double dk[3], dw[3];
-    der(z.sv + NS * z.isz, dk);
-    der(z.sv + (NS + 1) * z.isz, dw);
+    der(svv(NS), dk);
+    der(svv(NS + 1), dw);
     const double k_x = dk[0] * mm[0] + dk[1] * mm[3] + dk[2] * mm[6];
     const double k_y = dk[0] * mm[1] + dk[1] * mm[4] + dk[2] * mm[7];
     const double k_z = dk[0] * mm[2] + dk[1] * mm[5] + dk[2] * mm[8];
@@ -754,10 +809,10 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, int g0, double *F
     const double wall_dist = 0.5 * (ld(z.wall + g0) + ld(z.wall + g1));
     double f1 = 1;
     if (wall_dist > 1e-25) {
-      const double km = 0.5 * (svl(z, g0, NS) + svl(z, g1, NS));
-      const double omegam = 0.5 * (svl(z, g0, NS + 1) + svl(z, g1, NS + 1));
+      const double km = 0.5 * (cc.sv(NS, 0) + cc.sv(NS, 1));
+      const double omegam = 0.5 * (cc.sv(NS + 1, 0) + cc.sv(NS + 1, 1));
       const double param1 = sqrt(km) / (0.09 * omegam * wall_dist);
-      const double rhom = 0.5 * (bvl(z, g0, 0) + bvl(z, g1, 0));
+      const double rhom = 0.5 * (cc.bv(0, 0) + cc.bv(0, 1));
       const double d2 = wall_dist * wall_dist;
       const double param2 = 500 * mul / (rhom * d2 * omegam);
       const double CDkomega =

@@ -18,6 +18,10 @@ struct TileShape {
   int vrows = 0;
   int vchunks = 1;
   int vminb = 1;
+  // 1 or 2: the staged kernels (flux_dir_staged: the sweep plane's cells in a
+  // shared-memory tile, one buffer or two), 0: cells read from the planes
+  int staged = 0;
+  int vstaged = 0;
 };
 
 // tile-table launches: all zones of a context in one persistent launch per

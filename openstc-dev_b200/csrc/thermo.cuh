@@ -49,27 +49,30 @@ __device__ __forceinline__ void enthalpy_cp(double t, double *h, double *cp) {
   }
 }
 
+// enthalpy of species i (Thermo.cu:5-23) at t with its powers t2..t5
+__device__ __forceinline__ double enthalpy_one(int i, double t, double t2, double t3, double t4, double t5) {
+  double tt = t, tt2 = t2, tt3 = t3, tt4 = t4, tt5 = t5;
+  const bool below = t < c_p.t_low[i];
+  if (below) {
+    tt = c_p.t_low[i];
+    tt2 = tt * tt; tt3 = tt2 * tt; tt4 = tt3 * tt; tt5 = tt4 * tt;
+  }
+  double c[6];
+  nasa_coeffs<6>(i, below || t < c_p.t_mid[i], c);
+  double hi = c[0] * tt + 0.5 * c[1] * tt2 + c[2] * tt3 * (1.0 / 3) + 0.25 * c[3] * tt4 + 0.2 * c[4] * tt5 + c[5];
+  if (below) {
+    const double cpi = c[0] + c[1] * tt + c[2] * tt2 + c[3] * tt3 + c[4] * tt4;
+    hi += cpi * (t - tt);
+  }
+  return hi * c_p.Rmw[i];
+}
+
 // enthalpy only (Thermo.cu:5-23)
 template <int NS>
 __device__ __forceinline__ void enthalpy(double t, double *h) {
   const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
 #pragma unroll
-  for (int i = 0; i < NS; ++i) {
-    double tt = t, tt2 = t2, tt3 = t3, tt4 = t4, tt5 = t5;
-    const bool below = t < c_p.t_low[i];
-    if (below) {
-      tt = c_p.t_low[i];
-      tt2 = tt * tt; tt3 = tt2 * tt; tt4 = tt3 * tt; tt5 = tt4 * tt;
-    }
-    double c[6];
-    nasa_coeffs<6>(i, below || t < c_p.t_mid[i], c);
-    double hi = c[0] * tt + 0.5 * c[1] * tt2 + c[2] * tt3 * (1.0 / 3) + 0.25 * c[3] * tt4 + 0.2 * c[4] * tt5 + c[5];
-    if (below) {
-      const double cpi = c[0] + c[1] * tt + c[2] * tt2 + c[3] * tt3 + c[4] * tt4;
-      hi += cpi * (t - tt);
-    }
-    h[i] = hi * c_p.Rmw[i];
-  }
+  for (int i = 0; i < NS; ++i) h[i] = enthalpy_one(i, t, t2, t3, t4, t5);
 }
 
 // cp only (Thermo.cu:47-61)

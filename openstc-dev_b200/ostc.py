@@ -743,8 +743,15 @@ class Solver:
             self.set_tile(d, r, c)
 
     def _time_flux(self, arg, warmup, reps):
+        """device ms of one flux launch (op argument arg), or None when the
+        tile setting cannot run for this scheme (a staged kernel for AWENO,
+        or a tile larger than a CTA's shared memory)"""
         import torch
 
+        try:
+            self.launch_op(self.OP_FLUX, arg)
+        except OstcError:
+            return None
         for _ in range(warmup):
             self.launch_op(self.OP_FLUX, arg)
         torch.cuda.synchronize()
@@ -765,6 +772,10 @@ class Solver:
         blk = self.blocks[0]
         ext = (blk.mx, blk.my, blk.mz)
         viscous = self.scheme.viscous_order != 0
+        # the staged kernels (one or two shared-memory tile buffers, 128
+        # registers) compete with the plane kernels of every register budget;
+        # AWENO has no staged build
+        staged = (0,) if self.scheme.reconstruction == 4 else (0, 1, 2)
         best = {}
         for d in range(3):
             n = ext[d]
@@ -780,28 +791,35 @@ class Solver:
                             if minb >= 4 and R > 4:
                                 continue
                             out.append((R | (minb << 8 if minb > 1 else 0), min(c, cmax)))
+                        for nb in staged[1:]:
+                            out.append((R | (2 << 8) | (nb << 16), min(c, cmax)))
                         if c >= cmax:
                             break
                         c *= 2
                 return sorted(set(out))
 
+            def timed(arg, R, Cc, sets):
+                for q in sets:
+                    self.set_tile(q, R, Cc)
+                t = self._time_flux(arg, warmup, reps)
+                return None if t is None else (t, R, Cc)
+
             self.set_tile(d + 3, 0, 0)
-            fused = []
-            for R, Cc in cands((1, 2, 3, 4, 5)):
-                self.set_tile(d, R, Cc)
-                fused.append((self._time_flux(d, warmup, reps), R, Cc))
+            fused = [x for x in (timed(d, R, Cc, (d,)) for R, Cc in cands((1, 2, 3, 4, 5))) if x]
             fused.sort()
             choice = (fused[0][0], fused[0][1:], (0, 0))
             if viscous:
                 inv, vis = [], []
                 for R, Cc in cands((2, 3, 4, 5)):
-                    self.set_tile(d, R, Cc)
-                    inv.append((self._time_flux(d + 3, warmup, reps), R, Cc))
-                    self.set_tile(d + 3, R, Cc)
-                    vis.append((self._time_flux(d + 6, warmup, reps), R, Cc))
+                    x = timed(d + 3, R, Cc, (d,))
+                    if x:
+                        inv.append(x)
+                    x = timed(d + 6, R, Cc, (d + 3,))
+                    if x:
+                        vis.append(x)
                 inv.sort()
                 vis.sort()
-                if inv[0][0] + vis[0][0] < choice[0]:
+                if inv and vis and inv[0][0] + vis[0][0] < choice[0]:
                     choice = (inv[0][0] + vis[0][0], inv[0][1:], vis[0][1:])
             self.set_tile(d, *choice[1])
             self.set_tile(d + 3, *choice[2])
