@@ -558,12 +558,14 @@ ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg,
  * OR-ed with (2 << 8) or (3 << 8) to select the builds limited to 128 or 80
  * registers (two or three 256-thread CTAs per SM), or with (4 << 8) / (5 << 8)
  * for the builds limited to 168 / 96 registers (three / five CTAs of at most
- * 4 rows per SM). OR-ing (1 << 16) or (2 << 16) selects the staged kernels
- * (128 registers; the cells of the CTA's sweep plane copied into a
- * shared-memory tile before its faces are computed, with one tile buffer or
- * two so that the next chunk's copy overlaps this one's faces); they are
- * built for the primitive-variable and Roe faces, not AWENO (launches then
- * fail with OSTC_ERR_CUDA). Results are bit-identical to the plane kernels.
+ * 4 rows per SM). OR-ing (1 << 16) selects the staged kernels (rows = 8
+ * only, 128 registers): before its faces are computed a CTA copies with
+ * cp.async into shared memory the primitive and scalar values of the cells of
+ * its sweep plane that they read (with the reconstruction halo along the
+ * sweep) and the metric, Jacobian and transport properties of the faces' own
+ * cells; only the cells across the plane are read from HBM by the faces. Built
+ * for the primitive-variable and Roe faces, not AWENO (launches then fail with
+ * OSTC_ERR_CUDA). Results are bit-identical to the plane kernels.
  * dir 3, 4, 5: a tile for a separate viscous-flux kernel of direction
  * dir - 3; with one set, a viscous flow runs the inviscid flux (tile of dir
  * - 3) and the viscous flux as two kernels instead of the fused one. rows = 0

@@ -1530,7 +1530,7 @@ ostc_status ostc_read_flowfield(ostc_ctx *ctx, const char *path, const char *con
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
   if (!ctx || dir < 0 || dir > 5) return OSTC_ERR_INVALID_ARG;
   // rows may carry the register budget and the staged kernels in its upper
-  // bits: rows | (minb << 8) | (staged << 16), staged 1 or 2 = tile buffers
+  // bits: rows | (minb << 8) | (staged << 16), staged 1 = the staged kernels
   const int minb = (rows >> 8) & 0xff;
   const int staged = (rows >> 16) & 0xff;
   rows &= 0xff;
@@ -1538,8 +1538,9 @@ ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
   if (dir > 2 && rows == 0) {  // back to the fused kernel
     t.vrows = 0;
   } else {
-    if (chunks < 1 || chunks > 4096 || minb < 0 || minb > 5 || staged > 2) return OSTC_ERR_INVALID_ARG;
-    if (staged && minb > 2) return OSTC_ERR_INVALID_ARG;  // the staged kernels are built for 128 registers
+    if (chunks < 1 || chunks > 4096 || minb < 0 || minb > 5 || staged > 1) return OSTC_ERR_INVALID_ARG;
+    // the staged kernels are built for 128 registers and CTAs of 8 rows
+    if (staged && (minb > 2 || rows != 8)) return OSTC_ERR_INVALID_ARG;
     if (!(rows == 1 || rows == 2 || rows == 4 || rows == 8)) return OSTC_ERR_INVALID_ARG;
     if (minb >= 4 && rows > 4) return OSTC_ERR_INVALID_ARG;  // the 168- and 96-register builds take <= 128 threads
     if (dir > 2) {

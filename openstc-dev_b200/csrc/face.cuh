@@ -33,7 +33,7 @@ __device__ __forceinline__ double met(const DevZone &z, int g, int c) { return l
 // z, a = i, b = j). Every call site passes literal steps, so the tile
 // accessor's choice between shared memory and HBM is resolved at compile time.
 struct PlaneCells {
-  const double *bvp, *svp;
+  const double *bvp, *svp, *metp, *jacp, *mulp, *kappap, *rhodp, *mutp, *ttcp, *wallp;
   int isz, g0, sn, sa, sb;
   // the cell's index: the face's first cell, then the step along the normal,
   // then the tangential step
@@ -47,6 +47,15 @@ struct PlaneCells {
   __device__ __forceinline__ double sv(int l, int n, int a = 0, int b = 0) const {
     return at(svp + l * isz, n, a, b);
   }
+  // metric, Jacobian and transport properties of the face's cells n = 0, 1
+  __device__ __forceinline__ double met(int c, int n) const { return ld(metp + c * isz + (g0 + n * sn)); }
+  __device__ __forceinline__ double jac(int n) const { return ld(jacp + (g0 + n * sn)); }
+  __device__ __forceinline__ double mul(int n) const { return ld(mulp + (g0 + n * sn)); }
+  __device__ __forceinline__ double kappa(int n) const { return ld(kappap + (g0 + n * sn)); }
+  __device__ __forceinline__ double rhod(int l, int n) const { return ld(rhodp + l * isz + (g0 + n * sn)); }
+  __device__ __forceinline__ double mut(int n) const { return ld(mutp + (g0 + n * sn)); }
+  __device__ __forceinline__ double ttc(int n) const { return ld(ttcp + (g0 + n * sn)); }
+  __device__ __forceinline__ double wall(int n) const { return ld(wallp + (g0 + n * sn)); }
 };
 
 template <int DIR>
@@ -54,23 +63,40 @@ __device__ __forceinline__ PlaneCells plane_cells(const DevZone &z, int g0) {
   // tangential strides: TA = j for the x sweep, else i; TB = j for the z sweep, else k
   const int sa = DIR == 0 ? z.d2 : 1;
   const int sb = DIR == 2 ? z.d2 : z.d1;
-  return PlaneCells{z.bv, z.sv, z.isz, g0, dir_stride<DIR>(z), sa, sb};
+  return PlaneCells{z.bv,   z.sv,  z.met, z.jac, z.mul, z.kappa, z.rhoD, z.mut, z.ttc, z.wall,
+                    z.isz, g0,    dir_stride<DIR>(z),  sa,    sb};
 }
 
-// the tile holds, for the CTA's sweep plane (b = 0), bv planes 0..5 then the sv
-// planes, each as a [row][column] array: t points at the thread's own cell of
-// plane 0, tn / ta are the tile strides of one step along n / a, tv the tile
-// stride of one plane; cells across the plane (b != 0) come from HBM
+// The state tile holds, for the CTA's sweep plane (b = 0), bv planes 0..5 then
+// the sv planes, each as a [row][column] array: t points at the thread's own
+// cell of plane 0, TN / TA are the tile strides of one step along n / a, TV
+// the tile stride of one plane (compile-time, so every tile read is one
+// shared-memory load at a constant offset from t); cells across the plane
+// (b != 0) come from HBM. The cell tile holds the metric, Jacobian and
+// transport planes of the faces' own cells (QN: stride of one step along n,
+// QV: stride of one plane), in the order of StagedPlanes.
+enum StagedPlanes { Q_MET = 0, Q_JAC = 9, Q_MUL = 10, Q_KAPPA = 11, Q_MUT = 12, Q_TTC = 13, Q_WALL = 14 };
+template <int NT>
+constexpr int q_rhod() { return NT > 0 ? 15 : 12; }  // first rhoD plane
+
+template <int TN, int TA, int TV, int QN, int QV, int RD>
 struct TileCells {
   PlaneCells p;
-  const double *t;
-  int tn, ta, tv;
+  const double *t, *q;
   __device__ __forceinline__ double bv(int l, int n, int a = 0, int b = 0) const {
-    return b != 0 ? p.bv(l, n, a, b) : t[l * tv + n * tn + a * ta];
+    return b != 0 ? p.bv(l, n, a, b) : t[l * TV + n * TN + a * TA];
   }
   __device__ __forceinline__ double sv(int l, int n, int a = 0, int b = 0) const {
-    return b != 0 ? p.sv(l, n, a, b) : t[(6 + l) * tv + n * tn + a * ta];
+    return b != 0 ? p.sv(l, n, a, b) : t[(6 + l) * TV + n * TN + a * TA];
   }
+  __device__ __forceinline__ double met(int c, int n) const { return q[(Q_MET + c) * QV + n * QN]; }
+  __device__ __forceinline__ double jac(int n) const { return q[Q_JAC * QV + n * QN]; }
+  __device__ __forceinline__ double mul(int n) const { return q[Q_MUL * QV + n * QN]; }
+  __device__ __forceinline__ double kappa(int n) const { return q[Q_KAPPA * QV + n * QN]; }
+  __device__ __forceinline__ double rhod(int l, int n) const { return q[(RD + l) * QV + n * QN]; }
+  __device__ __forceinline__ double mut(int n) const { return q[Q_MUT * QV + n * QN]; }
+  __device__ __forceinline__ double ttc(int n) const { return q[Q_TTC * QV + n * QN]; }
+  __device__ __forceinline__ double wall(int n) const { return q[Q_WALL * QV + n * QN]; }
 };
 
 // 0.5 * (sgn(a) + sgn(b)) * min(|a|, |b|) with sgn(x) = (x < 0 ? -1 : 1)
@@ -225,12 +251,11 @@ __device__ __forceinline__ void lax_friedrichs(const double *pl, const double *p
 }
 
 // dispatch on the inviscid_scheme tag (InviscidScheme.cu:137-150; Roe -> AUSM+, quirk A1)
-template <int NV, int NS>
-__device__ __forceinline__ void riemann(const double *pl, const double *pr, const DevZone &z, int g0, int g1,
-                                        int DIR, double *F) {
-  const double j0 = ld(z.jac + g0), j1 = ld(z.jac + g1);
-  const double m0x = met(z, g0, 3 * DIR), m0y = met(z, g0, 3 * DIR + 1), m0z = met(z, g0, 3 * DIR + 2);
-  const double m1x = met(z, g1, 3 * DIR), m1y = met(z, g1, 3 * DIR + 1), m1z = met(z, g1, 3 * DIR + 2);
+template <int NV, int NS, class Cells>
+__device__ __forceinline__ void riemann(const double *pl, const double *pr, const Cells &c, int DIR, double *F) {
+  const double j0 = c.jac(0), j1 = c.jac(1);
+  const double m0x = c.met(3 * DIR, 0), m0y = c.met(3 * DIR + 1, 0), m0z = c.met(3 * DIR + 2, 0);
+  const double m1x = c.met(3 * DIR, 1), m1y = c.met(3 * DIR + 1, 1), m1z = c.met(3 * DIR + 2, 1);
   const int sch = c_p.inviscid_scheme;
   if (sch == 4) {
     hllc<NV, NS>(pl, pr, 0.5 * (m0x + m1x), 0.5 * (m0y + m1y), 0.5 * (m0z + m1z), 0.5 * (j0 + j1), F);
@@ -322,11 +347,11 @@ __device__ __forceinline__ void reconstruct_pv(const DevZone &z, int g0, double 
 }
 
 template <int NS, int DIR, int NT, class Cells>
-__device__ __forceinline__ void inviscid_face_pv(const DevZone &z, const Cells &c, int g0, double *F) {
+__device__ __forceinline__ void inviscid_face_pv(const Cells &c, double *F) {
   constexpr int NV = 5 + NS + NT;
   double pl[NV + 2], pr[NV + 2];
   reconstruct_pv_c<NS, NT>(c, pl, pr);
-  riemann<NV, NS>(pl, pr, z, g0, g0 + dir_stride<DIR>(z), DIR, F);
+  riemann<NV, NS>(pl, pr, c, DIR, F);
 }
 
 // Harten entropy-fix width at one point (compute_entropy_fix_delta, Roe.cu:61-85): the 3-D
@@ -636,7 +661,7 @@ __device__ __forceinline__ void inviscid_face_aweno(const DevZone &z, int g0, do
     pl[5 + t] = vmn / ql[0];
     pr[5 + t] = vpl / qr[0];
   }
-  riemann<NV, 0>(pl, pr, z, g0, g1, DIR, F);
+  riemann<NV, 0>(pl, pr, plane_cells<DIR>(z, g0), DIR, F);
 }
 
 // physical flux of the AWENO central correction at one point (AWENO.cu:236-249);
@@ -685,15 +710,13 @@ __device__ __forceinline__ void cds_correction(const DevZone &z, int g, double *
 // normal stresses, k and omega diffusion with the F1 blend)
 // ---------------------------------------------------------------------------
 template <int NS, int DIR, int NT, class Cells>
-__device__ __forceinline__ void viscous_face(const DevZone &z, const Cells &cc, int g0, double *F) {
+__device__ __forceinline__ void viscous_face(const Cells &cc, double *F) {
   constexpr int NV = 5 + NS + NT;
-  const int sd = dir_stride<DIR>(z);
-  const int g1 = g0 + sd;
   // tangential directions
   constexpr int TA = DIR == 0 ? 1 : 0, TB = DIR == 2 ? 1 : 2;
   double mm[9];
 #pragma unroll
-  for (int c = 0; c < 9; ++c) mm[c] = 0.5 * (met(z, g0, c) + met(z, g1, c));
+  for (int c = 0; c < 9; ++c) mm[c] = 0.5 * (cc.met(c, 0) + cc.met(c, 1));
   // derivative along (normal, ta, tb) ordered as (xi, eta, zeta); v(n, a, b) is the variable's cell value
   auto der = [&](auto v, double out[3]) {
     const double dn = v(1, 0, 0) - v(0, 0, 0);
@@ -719,8 +742,8 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, const Cells &cc, 
   const double w_x = dw[0] * mm[0] + dw[1] * mm[3] + dw[2] * mm[6];
   const double w_y = dw[0] * mm[1] + dw[1] * mm[4] + dw[2] * mm[7];
   const double w_z = dw[0] * mm[2] + dw[1] * mm[5] + dw[2] * mm[8];
-  const double mul = 0.5 * (ld(z.mul + g0) + ld(z.mul + g1));
-  const double mut = NT > 0 ? 0.5 * (ld(z.mut + g0) + ld(z.mut + g1)) : 0.0;
+  const double mul = 0.5 * (cc.mul(0) + cc.mul(1));
+  const double mut = NT > 0 ? 0.5 * (cc.mut(0) + cc.mut(1)) : 0.0;
   const double mu = NT > 0 ? mul + mut : mul;
   double txx = mu * (4 * u_x - 2 * v_y - 2 * w_z) * (1.0 / 3);
   double tyy = mu * (4 * v_y - 2 * u_x - 2 * w_z) * (1.0 / 3);
@@ -728,17 +751,17 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, const Cells &cc, 
   const double txy = mu * (u_y + v_x), txz = mu * (u_z + w_x), tyz = mu * (v_z + w_y);
   if constexpr (NT > 0) {  // ViscousScheme.cuh:82-95
     constexpr double delta_d = 1e-3;
-    const double dy_div_delta = fmin(0.5 * (ld(z.wall + g0) + ld(z.wall + g1)) / delta_d, 1.0);
+    const double dy_div_delta = fmin(0.5 * (cc.wall(0) + cc.wall(1)) / delta_d, 1.0);
     const double twoThirdrhoKm =
         -2.0 / 3 * 0.5 * (cc.bv(0, 0) * cc.sv(NS, 0) + cc.bv(0, 1) * cc.sv(NS, 1)) * dy_div_delta;
     txx += twoThirdrhoKm;
     tyy += twoThirdrhoKm;
     tzz += twoThirdrhoKm;
   }
-  const double j0 = ld(z.jac + g0), j1 = ld(z.jac + g1);
-  const double kxj = 0.5 * (met(z, g0, 3 * DIR) * j0 + met(z, g1, 3 * DIR) * j1);
-  const double kyj = 0.5 * (met(z, g0, 3 * DIR + 1) * j0 + met(z, g1, 3 * DIR + 1) * j1);
-  const double kzj = 0.5 * (met(z, g0, 3 * DIR + 2) * j0 + met(z, g1, 3 * DIR + 2) * j1);
+  const double j0 = cc.jac(0), j1 = cc.jac(1);
+  const double kxj = 0.5 * (cc.met(3 * DIR, 0) * j0 + cc.met(3 * DIR, 1) * j1);
+  const double kyj = 0.5 * (cc.met(3 * DIR + 1, 0) * j0 + cc.met(3 * DIR + 1, 1) * j1);
+  const double kzj = 0.5 * (cc.met(3 * DIR + 2, 0) * j0 + cc.met(3 * DIR + 2, 1) * j1);
   F[0] = 0;
   F[1] = kxj * txx + kyj * txy + kzj * txz;
   F[2] = kxj * txy + kyj * tyy + kzj * tyz;
@@ -749,8 +772,8 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, const Cells &cc, 
   const double t_x = dt[0] * mm[0] + dt[1] * mm[3] + dt[2] * mm[6];
   const double t_y = dt[0] * mm[1] + dt[1] * mm[4] + dt[2] * mm[7];
   const double t_z = dt[0] * mm[2] + dt[1] * mm[5] + dt[2] * mm[8];
-  double cond = 0.5 * (ld(z.kappa + g0) + ld(z.kappa + g1));
-  if constexpr (NT > 0) cond += 0.5 * (ld(z.ttc + g0) + ld(z.ttc + g1));
+  double cond = 0.5 * (cc.kappa(0) + cc.kappa(1));
+  if constexpr (NT > 0) cond += 0.5 * (cc.ttc(0) + cc.ttc(1));
   F[4] = um * F[1] + vm * F[2] + wm * F[3] + cond * (kxj * t_x + kyj * t_y + kzj * t_z);
   if constexpr (NS > 0) {
     double yk[NS], diff[NS], ddf[NS];
@@ -758,7 +781,7 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, const Cells &cc, 
 #pragma unroll
     for (int l = 0; l < NS; ++l) {
       yk[l] = 0.5 * (cc.sv(l, 0) + cc.sv(l, 1));
-      diff[l] = 0.5 * (ld(z.rhoD + l * z.isz + g0) + ld(z.rhoD + l * z.isz + g1));
+      diff[l] = 0.5 * (cc.rhod(l, 0) + cc.rhod(l, 1));
       if constexpr (NT > 0) diff[l] += mut / c_p.Sct;  // turbulent diffusivity (ViscousScheme.cuh:122-125)
       double dy[3];
       der(svv(l), dy);
@@ -806,7 +829,7 @@ __device__ __forceinline__ void viscous_face(const DevZone &z, const Cells &cc, 
     const double omega_x = dw[0] * mm[0] + dw[1] * mm[3] + dw[2] * mm[6];
     const double omega_y = dw[0] * mm[1] + dw[1] * mm[4] + dw[2] * mm[7];
     const double omega_z = dw[0] * mm[2] + dw[1] * mm[5] + dw[2] * mm[8];
-    const double wall_dist = 0.5 * (ld(z.wall + g0) + ld(z.wall + g1));
+    const double wall_dist = 0.5 * (cc.wall(0) + cc.wall(1));
     double f1 = 1;
     if (wall_dist > 1e-25) {
       const double km = 0.5 * (cc.sv(NS, 0) + cc.sv(NS, 1));

@@ -29,7 +29,7 @@ __device__ __forceinline__ void face_total(const DevZone &z, const Cells &c, int
   constexpr int NV = 5 + NS + NT;
   static_assert(NT == 0 || INV != 2, "turbulence scalars: primitive-variable or AWENO reconstruction");
   if constexpr (PART == 2) {
-    viscous_face<NS, DIR, NT>(z, c, g0, G);
+    viscous_face<NS, DIR, NT>(c, G);
     return;
   }
   double Fi[NV];
@@ -38,10 +38,10 @@ __device__ __forceinline__ void face_total(const DevZone &z, const Cells &c, int
   else if constexpr (INV == 2)
     inviscid_face_roe<NS, DIR>(z, g0, Fi);
   else
-    inviscid_face_pv<NS, DIR, NT>(z, c, g0, Fi);
+    inviscid_face_pv<NS, DIR, NT>(c, Fi);
   if (PART == 0 && viscous) {
     double Fv[NV];
-    viscous_face<NS, DIR, NT>(z, c, g0, Fv);
+    viscous_face<NS, DIR, NT>(c, Fv);
 #pragma unroll
     for (int l = 0; l < NV; ++l) G[l] = Fv[l] - Fi[l];
   } else {
@@ -180,20 +180,39 @@ __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const 
 // the cells across the plane, the metrics and the transport properties from
 // HBM. Same arithmetic as the plane kernels, so the results are bit-identical.
 //
-// Tile of one chunk, per variable (bv 0..5, then sv 0..NS+NT-1):
+// Tile of one chunk, per variable (bv 0..5, then sv 0..NS+NT-1), for CTAs of
+// R = 8 rows:
 //   x sweep: [R + 2 rows j0-1 .. j0+R][35 cells F-1 .. F+33 along i]
 //   y / z sweep: [R + 3 rows F-1 .. F+R+1 along j / k][34 cells i0-1 .. i0+32]
 // with F the chunk's first face (face f lies between cells f and f+1).
 // ---------------------------------------------------------------------------
+// Tile geometry of a staged CTA of SR = 8 rows of 32 threads (compile-time, so
+// that every tile read is a shared-memory load at a constant offset and the
+// copy loops divide by constants)
+constexpr int SR = 8;
 template <int DIR>
 struct StageGeom {
-  static constexpr int W = DIR == 0 ? 35 : 34;
-  __host__ __device__ static constexpr int rows(int R) { return DIR == 0 ? R + 2 : R + 3; }
+  static constexpr int W = DIR == 0 ? 35 : 34;           // state tile: cells per row
+  static constexpr int TR = DIR == 0 ? SR + 2 : SR + 3;  // state tile: rows per variable
+  static constexpr int TV = TR * W;                      // state tile: stride of one variable
+  static constexpr int QW = DIR == 0 ? 33 : 32;          // cell tile: cells per row
+  static constexpr int QR = DIR == 0 ? SR : SR + 1;      // cell tile: rows per plane
+  static constexpr int QV = QR * QW;                     // cell tile: stride of one plane
 };
 
+// planes of the cell tile: the metric and Jacobian, and for viscous faces the
+// transport properties (with the SST planes when NT > 0)
+template <int NS, int NT>
+__host__ __device__ constexpr int stage_q_planes(bool viscous) {
+  return viscous ? q_rhod<NT>() + NS : Q_JAC + 1;
+}
+
+// doubles of dynamic shared memory: state tile, cell tile and (y / z sweeps)
+// the carried face flux; the y / z face-flux exchange reuses the state tile
 template <int NS, int NT, int DIR>
-__host__ __device__ constexpr size_t stage_tile_doubles(int R) {
-  return (size_t)(6 + NS + NT) * StageGeom<DIR>::rows(R) * StageGeom<DIR>::W;
+__host__ __device__ constexpr size_t stage_smem_doubles(bool viscous) {
+  return (size_t)(6 + NS + NT) * StageGeom<DIR>::TV + (size_t)stage_q_planes<NS, NT>(viscous) * StageGeom<DIR>::QV +
+         (DIR == 0 ? 0 : (size_t)(5 + NS + NT) * 32);
 }
 
 __device__ __forceinline__ void stage_cp8(double *dst, const double *src) {
@@ -201,34 +220,65 @@ __device__ __forceinline__ void stage_cp8(double *dst, const double *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void stage_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void stage_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+__device__ __forceinline__ void stage_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// base pointer of plane p of the cell tile (StagedPlanes order)
+template <int NT>
+__device__ __forceinline__ const double *stage_q_plane(const DevZone &z, int p) {
+  if (p < Q_JAC) return z.met + p * z.isz;
+  if (p == Q_JAC) return z.jac;
+  if (p == Q_MUL) return z.mul;
+  if (p == Q_KAPPA) return z.kappa;
+  if (NT > 0 && p == Q_MUT) return z.mut;
+  if (NT > 0 && p == Q_TTC) return z.ttc;
+  if (NT > 0 && p == Q_WALL) return z.wall;
+  return z.rhoD + (p - q_rhod<NT>()) * z.isz;
 }
 
-// issue the copies of one chunk's tile: warp w copies tile rows w, w + R, ...
-// o1, o2: the CTA's fixed coordinates (x sweep: j0 = first row, k; y sweep:
-// i0 = first column, k; z sweep: i0, j)
-// (one row = W consecutive cells of one variable); cells outside the block's
-// ghosted extent are not copied (no face that is computed reads them)
+// issue the copies of one chunk's tiles (warp w copies tile rows w, w + SR, ...;
+// one row = consecutive cells of one plane): the state tile (bv, sv of the
+// chunk's cells with the reconstruction halo along the sweep and one cell on
+// each side in-plane) and the cell tile (metric, Jacobian, properties of the
+// faces' own cells). Cells outside the block's ghosted extent are not copied
+// (no face that is computed reads them). o1, o2: the CTA's fixed coordinates
+// (x sweep: j0 = first row, k; y sweep: i0 = first column, k; z sweep: i0, j)
 template <int NS, int NT, int DIR>
-__device__ __forceinline__ void stage_issue(const DevZone &z, double *tile, int F, int o1, int o2) {
-  constexpr int NVAR = 6 + NS + NT, W = StageGeom<DIR>::W;
-  const int R = blockDim.y, TR = StageGeom<DIR>::rows(R);
+__device__ __forceinline__ void stage_issue(const DevZone &z, double *tile, double *qtile, int nq, int F, int o1,
+                                            int o2) {
+  using G = StageGeom<DIR>;
+  constexpr int NVAR = 6 + NS + NT;
   const int lane = threadIdx.x;
   const int g = z.ngg;
-  for (int rr = threadIdx.y; rr < NVAR * TR; rr += R) {
-    const int var = rr / TR, r = rr - var * TR;
-    // first cell of the tile row: x sweep (F-1, j0-1+r, k); y (i0-1, F-1+r, k); z (i0-1, j, F-1+r)
+  auto in_i = [&](int i) { return i >= -g && i < z.mx + g; };
+  auto rows_ok = [&](int j, int k) { return j >= -g && j < z.my + g && k >= -g && k < z.mz + g; };
+  {  // state tile: first cell of row r is x (F-1, j0-1+r, k); y (i0-1, F-1+r, k); z (i0-1, j, F-1+r)
     const int i0 = DIR == 0 ? F - 1 : o1 - 1;
-    const int j = DIR == 0 ? o1 - 1 + r : (DIR == 1 ? F - 1 + r : o2);
-    const int k = DIR == 2 ? F - 1 + r : o2;
-    if (j < -g || j >= z.my + g || k < -g || k >= z.mz + g) continue;
-    const double *src = (var < 6 ? z.bv + var * z.isz : z.sv + (var - 6) * z.isz) + gidx(z, i0, j, k);
-    double *dst = tile + rr * W;
-    for (int c = lane; c < W; c += 32) {
-      const int i = i0 + c;
-      if (i >= -g && i < z.mx + g) stage_cp8(dst + c, src + c);
+    const bool c0_ok = in_i(i0 + lane), c1_ok = lane + 32 < G::W && in_i(i0 + lane + 32);
+#pragma unroll 2
+    for (int rr = threadIdx.y; rr < NVAR * G::TR; rr += SR) {
+      const int var = rr / G::TR, r = rr - var * G::TR;
+      const int j = DIR == 0 ? o1 - 1 + r : (DIR == 1 ? F - 1 + r : o2);
+      const int k = DIR == 2 ? F - 1 + r : o2;
+      if (!rows_ok(j, k)) continue;
+      const double *src = (var < 6 ? z.bv + var * z.isz : z.sv + (var - 6) * z.isz) + gidx(z, i0, j, k);
+      double *dst = tile + rr * G::W;
+      if (c0_ok) stage_cp8(dst + lane, src + lane);
+      if (c1_ok) stage_cp8(dst + lane + 32, src + lane + 32);
+    }
+  }
+  {  // cell tile: first cell of row r is x (F, j0+r, k); y (i0, F+r, k); z (i0, j, F+r)
+    const int i0 = DIR == 0 ? F : o1;
+    const bool c0_ok = in_i(i0 + lane), c1_ok = lane + 32 < G::QW && in_i(i0 + lane + 32);
+#pragma unroll 2
+    for (int rr = threadIdx.y; rr < nq * G::QR; rr += SR) {
+      const int p = rr / G::QR, r = rr - p * G::QR;
+      const int j = DIR == 0 ? o1 + r : (DIR == 1 ? F + r : o2);
+      const int k = DIR == 2 ? F + r : o2;
+      if (!rows_ok(j, k)) continue;
+      const double *src = stage_q_plane<NT>(z, p) + gidx(z, i0, j, k);
+      double *dst = qtile + rr * G::QW;
+      if (c0_ok) stage_cp8(dst + lane, src + lane);
+      if (c1_ok) stage_cp8(dst + lane + 32, src + lane + 32);
     }
   }
   stage_commit();
@@ -236,42 +286,30 @@ __device__ __forceinline__ void stage_issue(const DevZone &z, double *tile, int 
 
 template <int NS, int INV, int DIR, int PART, int NT>
 __device__ __forceinline__ void flux_tile_staged(const DevZone &z, const int bx, const int by, const int bz,
-                                                 int nchunk, int accumulate, int viscous, int nbuf, double *smem) {
-  constexpr int NV = 5 + NS + NT;
-  constexpr int W = StageGeom<DIR>::W;
+                                                 int nchunk, int accumulate, int viscous, double *smem) {
+  using Geo = StageGeom<DIR>;
+  constexpr int NV = 5 + NS + NT, NVAR = 6 + NS + NT, R = SR;
   static_assert(INV != 1, "AWENO reads its cells (and the central correction's) from the planes");
-  const int lane = threadIdx.x, row = threadIdx.y, R = blockDim.y;
+  const int lane = threadIdx.x, row = threadIdx.y;
   const int n = DIR == 0 ? z.mx : (DIR == 1 ? z.my : z.mz);
-  const int TR = StageGeom<DIR>::rows(R);
-  const int tv = TR * W;                          // tile stride of one variable
-  const size_t tsz = stage_tile_doubles<NS, NT, DIR>(R);
   const bool vis = viscous != 0;
+  const int nq = stage_q_planes<NS, NT>(PART == 2 || (PART == 0 && vis));
+  double *tile = smem;                                  // state tile; y / z: then the chunk's face fluxes
+  double *qtile = smem + (size_t)NVAR * Geo::TV;        // cell tile
+  double *cG = qtile + (size_t)nq * Geo::QV;            // y / z: [NV][32] last face flux of the previous chunk
   // segment geometry, as in flux_tile
   const int S = DIR == 0 ? 32 * nchunk - 1 : R * nchunk - 1;
   const int c0 = (DIR == 0 ? bx : (DIR == 1 ? by : bz)) * S;
-  const int span = DIR == 0 ? 32 : R;
-  // tile origin arguments of stage_issue: x (j0, k); y (i0, k); z (i0, j)
+  constexpr int span = DIR == 0 ? 32 : R;
   const int o1 = DIR == 0 ? by * R : bx * 32, o2 = DIR == 0 ? bz : (DIR == 1 ? bz : by);
-  __shared__ double carry[8][NV];  // x sweep: the last face flux of the previous chunk of each row
-  double *sG = smem + (size_t)nbuf * tsz;  // y / z sweep: [R+1][NV][32] face fluxes of the chunk
+  __shared__ double carry[R][NV];  // x sweep: the last face flux of the previous chunk of each row
   if (DIR == 0 && lane == 31)
 #pragma unroll
     for (int l = 0; l < NV; ++l) carry[row][l] = 0;
-  if (nbuf == 2) stage_issue<NS, NT, DIR>(z, smem, c0 - 1, o1, o2);
   for (int ch = 0; ch < nchunk; ++ch) {
     const int F = c0 - 1 + span * ch;
-    double *tile = smem + (nbuf == 2 ? (size_t)(ch & 1) * tsz : 0);
-    if (nbuf == 2) {
-      if (ch + 1 < nchunk) {
-        stage_issue<NS, NT, DIR>(z, smem + (size_t)((ch + 1) & 1) * tsz, F + span, o1, o2);
-        stage_wait<1>();
-      } else {
-        stage_wait<0>();
-      }
-    } else {
-      stage_issue<NS, NT, DIR>(z, tile, F, o1, o2);
-      stage_wait<0>();
-    }
+    stage_issue<NS, NT, DIR>(z, tile, qtile, nq, F, o1, o2);
+    stage_wait_all();
     __syncthreads();
     // this thread's face and cell
     const int f = F + (DIR == 0 ? lane : row);
@@ -282,8 +320,9 @@ __device__ __forceinline__ void flux_tile_staged(const DevZone &z, const int bx,
     double G[NV];
     if (active) {
       const int g = gidx(z, i, j, k);
-      const TileCells tc{plane_cells<DIR>(z, g), tile + (row + 1) * W + lane + 1, DIR == 0 ? 1 : W, DIR == 0 ? W : 1,
-                         tv};
+      const TileCells<DIR == 0 ? 1 : Geo::W, DIR == 0 ? Geo::W : 1, Geo::TV, DIR == 0 ? 1 : Geo::QW, Geo::QV,
+                      q_rhod<NT>()>
+          tc{plane_cells<DIR>(z, g), tile + (row + 1) * Geo::W + lane + 1, qtile + row * Geo::QW + lane};
       face_total<NS, INV, DIR, PART, NT>(z, tc, g, vis, G);
     } else {
 #pragma unroll
@@ -312,47 +351,48 @@ __device__ __forceinline__ void flux_tile_staged(const DevZone &z, const int bx,
             dq[l * z.iqsz] = d;
         }
       }
-      __syncthreads();  // every face of the chunk has read the tile before it is refilled
+      __syncthreads();  // every face of the chunk has read the tiles before they are refilled
     } else {
+      __syncthreads();  // every face has read the tiles: the state tile now takes the face fluxes
+      double *sG = tile;  // [R][NV][32]
 #pragma unroll
-      for (int l = 0; l < NV; ++l) sG[((row + 1) * NV + l) * 32 + lane] = G[l];
+      for (int l = 0; l < NV; ++l) sG[(row * NV + l) * 32 + lane] = G[l];
       __syncthreads();
       if (active && f >= c0 && f >= 0 && !(ch == 0 && row == 0)) {
         double *dq = z.dq + qidx(z, i, j, k);
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
-          const double d = G[l] - sG[(row * NV + l) * 32 + lane];
+          const double gm = row == 0 ? cG[l * 32 + lane] : sG[((row - 1) * NV + l) * 32 + lane];
+          const double d = G[l] - gm;
           if (accumulate)
             dq[l * z.iqsz] += d;
           else
             dq[l * z.iqsz] = d;
         }
       }
-      __syncthreads();
-      if (row == 0) {
+      __syncthreads();  // the previous chunk's carried flux and the exchange are read
+      if (row == R - 1)
 #pragma unroll
-        for (int l = 0; l < NV; ++l) sG[l * 32 + lane] = sG[(R * NV + l) * 32 + lane];
-      }
-      __syncthreads();
+        for (int l = 0; l < NV; ++l) cG[l * 32 + lane] = G[l];
     }
   }
+  if constexpr (DIR != 0) __syncthreads();  // the carried flux of this tile is written before a next tile starts
 }
 
 template <int NS, int INV, int DIR, int MINB, int PART, int NT>
 __global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::blocks)
-    flux_dir_staged(DevZone z, int nchunk, int accumulate, int viscous, int nbuf) {
+    flux_dir_staged(DevZone z, int nchunk, int accumulate, int viscous) {
   extern __shared__ double smem[];
-  flux_tile_staged<NS, INV, DIR, PART, NT>(z, blockIdx.x, blockIdx.y, blockIdx.z, nchunk, accumulate, viscous, nbuf,
-                                           smem);
+  flux_tile_staged<NS, INV, DIR, PART, NT>(z, blockIdx.x, blockIdx.y, blockIdx.z, nchunk, accumulate, viscous, smem);
 }
 
 template <int NS, int INV, int DIR, int MINB, int PART, int NT>
 __global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::blocks)
-    flux_dir_staged_table(const int4 *tiles, int n_tiles, int nchunk, int accumulate, int viscous, int nbuf) {
+    flux_dir_staged_table(const int4 *tiles, int n_tiles, int nchunk, int accumulate, int viscous) {
   extern __shared__ double smem[];
   for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
     const int4 c = tiles[t];
-    flux_tile_staged<NS, INV, DIR, PART, NT>(c_zones[c.x], c.y, c.z, c.w, nchunk, accumulate, viscous, nbuf, smem);
+    flux_tile_staged<NS, INV, DIR, PART, NT>(c_zones[c.x], c.y, c.z, c.w, nchunk, accumulate, viscous, smem);
   }
 }
 
@@ -431,17 +471,18 @@ static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, const Flu
   return cudaGetLastError();
 }
 
-// the staged kernels (128-register budget): dynamic shared memory = nbuf
-// tiles (+ the y / z sweep's face-flux exchange), checked against the 227 KB a
-// CTA may use; the carveout is sized for the CTAs that fit
+// the staged kernels (CTAs of 8 rows, 128-register budget): dynamic shared
+// memory = state tile + cell tile (+ the y / z sweep's carried face flux),
+// checked against the 227 KB a CTA may use; the carveout is sized for the CTAs
+// that fit
 template <int NS, int INV, int DIR, int PART, int NT>
-static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, int nbuf, const FluxTable *tab,
-                                 int accumulate, int viscous, cudaStream_t s) {
-  constexpr int NV = 5 + NS + NT, MINB = 2;
-  const int R = t.rows, C = t.chunks;
-  if (32 * R > FluxBounds<MINB>::threads || R > 8 || (nbuf != 1 && nbuf != 2)) return cudaErrorInvalidConfiguration;
-  const size_t smem = sizeof(double) * ((size_t)nbuf * stage_tile_doubles<NS, NT, DIR>(R) +
-                                        (DIR == 0 ? 0 : (size_t)(R + 1) * NV * 32));
+static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
+                                 int viscous, cudaStream_t s) {
+  constexpr int NV = 5 + NS + NT, MINB = 2, R = SR;
+  const int C = t.chunks;
+  if (t.rows != SR) return cudaErrorInvalidConfiguration;
+  const bool vis_planes = PART == 2 || (PART == 0 && viscous);
+  const size_t smem = sizeof(double) * stage_smem_doubles<NS, NT, DIR>(vis_planes);
   if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
   const void *fn = tab ? (const void *)flux_dir_staged_table<NS, INV, DIR, MINB, PART, NT>
                        : (const void *)flux_dir_staged<NS, INV, DIR, MINB, PART, NT>;
@@ -452,7 +493,7 @@ static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, int nbuf,
   if (e != cudaSuccess) return e;
   if (per_sm <= 0) return cudaErrorInvalidConfiguration;
   {
-    const size_t need = (size_t)per_sm * (smem + 8 * NV * 8 + 1024);
+    const size_t need = (size_t)per_sm * (smem + SR * NV * 8 + 1024);
     int pct = (int)((need * 100 + 228 * 1024 - 1) / (228 * 1024));
     pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
     e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
@@ -461,7 +502,7 @@ static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, int nbuf,
   const dim3 blk(32, R);
   if (!tab) {
     flux_dir_staged<NS, INV, DIR, MINB, PART, NT><<<flux_grid(z.mx, z.my, z.mz, DIR, R, C), blk, smem, s>>>(
-        z, C, accumulate, viscous, nbuf);
+        z, C, accumulate, viscous);
     return cudaGetLastError();
   }
   if (tab->n <= 0) return cudaSuccess;
@@ -472,7 +513,7 @@ static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, int nbuf,
   const int slots = per_sm * sms;
   const int grid = tab->n < slots ? tab->n : slots;
   flux_dir_staged_table<NS, INV, DIR, MINB, PART, NT><<<grid, blk, smem, s>>>(tab->tiles, tab->n, C, accumulate,
-                                                                              viscous, nbuf);
+                                                                              viscous);
   return cudaGetLastError();
 }
 
@@ -483,7 +524,7 @@ static cudaError_t launch_flux_p(const DevZone &z, const TileShape &t, const Flu
     if constexpr (INV == 1) {
       return cudaErrorInvalidConfiguration;  // AWENO reads its cells from the planes
     } else {
-      return launch_flux_s<NS, INV, DIR, PART, NT>(z, t, t.staged, tab, accumulate, viscous, s);
+      return launch_flux_s<NS, INV, DIR, PART, NT>(z, t, tab, accumulate, viscous, s);
     }
   }
 #ifdef OSTC_FLUX_REDUCED

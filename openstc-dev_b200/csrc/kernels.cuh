@@ -18,8 +18,8 @@ struct TileShape {
   int vrows = 0;
   int vchunks = 1;
   int vminb = 1;
-  // 1 or 2: the staged kernels (flux_dir_staged: the sweep plane's cells in a
-  // shared-memory tile, one buffer or two), 0: cells read from the planes
+  // 1: the staged kernels (flux_dir_staged: the cells a CTA's faces read
+  // copied into shared-memory tiles first), 0: cells read from the planes
   int staged = 0;
   int vstaged = 0;
 };

@@ -772,10 +772,10 @@ class Solver:
         blk = self.blocks[0]
         ext = (blk.mx, blk.my, blk.mz)
         viscous = self.scheme.viscous_order != 0
-        # the staged kernels (one or two shared-memory tile buffers, 128
-        # registers) compete with the plane kernels of every register budget;
-        # AWENO has no staged build
-        staged = (0,) if self.scheme.reconstruction == 4 else (0, 1, 2)
+        # the staged kernels (shared-memory tiles, 8 rows, 128 registers)
+        # compete with the plane kernels of every register budget; AWENO has
+        # no staged build
+        staged = (0,) if self.scheme.reconstruction == 4 else (0, 1)
         best = {}
         for d in range(3):
             n = ext[d]
@@ -791,7 +791,7 @@ class Solver:
                             if minb >= 4 and R > 4:
                                 continue
                             out.append((R | (minb << 8 if minb > 1 else 0), min(c, cmax)))
-                        for nb in staged[1:]:
+                        for nb in (staged[1:] if R == 8 else ()):
                             out.append((R | (2 << 8) | (nb << 16), min(c, cmax)))
                         if c >= cmax:
                             break
