@@ -153,10 +153,13 @@ ostc_status build_tables(ostc_ctx *ctx) {
     ctx->tab_cap = all.size();
   }
   if (!all.empty()) CK(cudaMemcpy(ctx->tab_dev, all.data(), sizeof(int4) * all.size(), cudaMemcpyHostToDevice));
+  bool all_bulk = true;
+  for (const DevZone &z : ctx->dz) all_bulk = all_bulk && (z.flags & kZoneBulk) != 0;
   auto table = [&](size_t q) {
     FluxTable t;
     t.tiles = ctx->tab_dev + spans[q].first;
     t.n = (int)(spans[q].second - spans[q].first);
+    t.bulk = all_bulk;
     return t;
   };
   for (int c = 0; c < 3; ++c) ctx->cell_tab[c] = table(c);
@@ -289,6 +292,15 @@ void fill_devzone(const ostc_zone &z, DevZone &d) {
   d.isr = nullptr;
   d.tsj = z.turb_src_jac;
   d.jac = z.jac;
+}
+
+// kZoneBulk when the ghosted row length (and so the plane size) is even and the
+// planes the staged flux kernels copy start on 16-byte boundaries
+static int zone_flags(const DevZone &d) {
+  auto a16 = [](const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  const bool ok = d.d2 % 2 == 0 && d.isz % 2 == 0 && a16(d.bv) && a16(d.sv) && a16(d.met) && a16(d.jac) &&
+                  a16(d.mul) && a16(d.kappa) && a16(d.rhoD) && a16(d.mut) && a16(d.ttc) && a16(d.wall);
+  return ok ? kZoneBulk : 0;
 }
 
 ostc_status validate(const ostc_config *cfg, const ostc_param *p, const ostc_zone *zones, int n_zones,
@@ -552,6 +564,7 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
     CK(cudaMalloc(&soa, sizeof(double) * 9 * c->dz[b].sz));
     c->met_soa.push_back(soa);
     c->dz[b].met = soa;
+    c->dz[b].flags = zone_flags(c->dz[b]);
     c->n_total += (double)zones[b].mx * zones[b].my * zones[b].mz;
   }
   for (int q = 0; q < n_faces; ++q) {
@@ -1022,6 +1035,11 @@ static ostc_status ensure_graph(ostc_ctx *ctx, bool hist, GraphEntry **out, bool
 // the residual epilogue, if any, becomes OSTC_ERR_NONPHYSICAL with its zone and
 // cell (ostc_get_error) and the step of the call it was found in (err_step)
 static ostc_status check_state(ostc_ctx *ctx, unsigned long long key) {
+  // a staged flux kernel that gave up waiting for its tile (bounded wait) left
+  // its faces uncomputed: the steps are not valid
+  int late = 0;
+  CK(stage_timeouts(&late));
+  if (late) return fail(ctx, OSTC_ERR_TIMEOUT);
   if (key == ~0ull) return OSTC_OK;
   const long long q = (long long)(key & ((1ull << 34) - 1));
   const int b = (int)((key >> 34) & 1023);

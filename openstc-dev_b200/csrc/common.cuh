@@ -70,8 +70,13 @@ struct DevZone {
   // sz and qsz as 32-bit ints for the flux kernels' index arithmetic (every
   // plane offset of a block is below 2^31: checked at ostc_create)
   int isz, iqsz;
-  int pad_;
+  // bit 0 (kZoneBulk): the ghosted row length is even and every plane the
+  // staged flux kernels copy starts on a 16-byte boundary, so that their tile
+  // rows can move as 16-byte-aligned bulk copies
+  int flags;
 };
+
+constexpr int kZoneBulk = 1;
 
 __device__ __forceinline__ int gidx(const DevZone &z, int i, int j, int k) {
   return k * z.d1 + j * z.d2 + i + z.dt_;

@@ -188,16 +188,22 @@ __device__ __forceinline__ void flux_tile(const DevZone &z, const int bx, const 
 // ---------------------------------------------------------------------------
 // Tile geometry of a staged CTA of SR = 8 rows of 32 threads (compile-time, so
 // that every tile read is a shared-memory load at a constant offset and the
-// copy loops divide by constants)
+// copy loops divide by constants). A tile row holds W (state) or QW (cell)
+// cells starting at column `shift` of a slot of WS / QWS doubles: slots are
+// 16-byte multiples, so that a row copied in bulk from a 16-byte boundary of
+// HBM (shift = 1 when the row's first cell is not on one) lands aligned.
 constexpr int SR = 8;
 template <int DIR>
 struct StageGeom {
   static constexpr int W = DIR == 0 ? 35 : 34;           // state tile: cells per row
+  static constexpr int WS = 36;                          // state tile: row slot
   static constexpr int TR = DIR == 0 ? SR + 2 : SR + 3;  // state tile: rows per variable
-  static constexpr int TV = TR * W;                      // state tile: stride of one variable
+  static constexpr int TV = TR * WS;                     // state tile: stride of one variable
   static constexpr int QW = DIR == 0 ? 33 : 32;          // cell tile: cells per row
+  static constexpr int QWS = 34;                         // cell tile: row slot
   static constexpr int QR = DIR == 0 ? SR : SR + 1;      // cell tile: rows per plane
-  static constexpr int QV = QR * QW;                     // cell tile: stride of one plane
+  static constexpr int QV = QR * QWS;                    // cell tile: stride of one plane
+  static_assert(W + 1 <= WS && QW + 1 <= QWS && WS % 2 == 0 && QWS % 2 == 0, "row slots hold a shifted row");
 };
 
 // planes of the cell tile: the metric and Jacobian, and for viscous faces the
@@ -222,6 +228,65 @@ __device__ __forceinline__ void stage_cp8(double *dst, const double *src) {
 __device__ __forceinline__ void stage_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void stage_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// the CTA's tile mbarrier (bulk copies signal their bytes on it; one arrival
+// per chunk by thread 0 after every copying thread has announced its bytes)
+__device__ __forceinline__ void stage_bar_init(unsigned bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void stage_expect(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void stage_arrive(unsigned bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// one row: `bytes` (a multiple of 16) from a 16-byte-aligned global address to
+// a 16-byte-aligned shared address, completion counted on the mbarrier
+__device__ __forceinline__ void stage_bulk(double *dst, const double *src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+constexpr unsigned long long kStageWaitNs = 1000000000ull;  // 1 s of the global timer per tile wait
+// bounded wait for the mbarrier phase `parity`; false when the time ran out
+__device__ __forceinline__ bool stage_bar_wait(unsigned bar, unsigned parity) {
+  unsigned long long t0;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t0));
+  for (unsigned it = 0;; ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((it & 31) == 31) {
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+      if (t - t0 > kStageWaitNs) return false;
+    }
+  }
+}
+
+// set when a staged flux CTA gave up waiting for its tile (read and cleared
+// by the unit's host accessor, stage_timeout_read)
+static __device__ int g_stage_timeout;
+
+// host side: this unit's timeout flag, cleared after the read
+static cudaError_t stage_timeout_read(int *flag) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_stage_timeout, sizeof(int));
+  if (e == cudaSuccess && v) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_stage_timeout, &zero, sizeof(int));
+  }
+  *flag = v;
+  return e;
+}
+
 // base pointer of plane p of the cell tile (StagedPlanes order)
 template <int NT>
 __device__ __forceinline__ const double *stage_q_plane(const DevZone &z, int p) {
@@ -235,58 +300,115 @@ __device__ __forceinline__ const double *stage_q_plane(const DevZone &z, int p) 
   return z.rhoD + (p - q_rhod<NT>()) * z.isz;
 }
 
-// issue the copies of one chunk's tiles (warp w copies tile rows w, w + SR, ...;
-// one row = consecutive cells of one plane): the state tile (bv, sv of the
-// chunk's cells with the reconstruction halo along the sweep and one cell on
-// each side in-plane) and the cell tile (metric, Jacobian, properties of the
-// faces' own cells). Cells outside the block's ghosted extent are not copied
-// (no face that is computed reads them). o1, o2: the CTA's fixed coordinates
-// (x sweep: j0 = first row, k; y sweep: i0 = first column, k; z sweep: i0, j)
-template <int NS, int NT, int DIR>
+// copy one tile row of `w` cells starting at ghosted index gi of `plane` into
+// its slot `dst` (the row's first cell at dst[shift]). Bulk: one thread copies
+// `slot` cells from gi - shift, 16-byte aligned at both ends and inside the
+// plane, else the row falls back to 8-byte cp.async by the same thread.
+// Returns the bytes announced on the mbarrier.
+__device__ __forceinline__ unsigned stage_row_bulk(const double *plane, int isz, int gi, int w, int slot, int shift,
+                                                   double *dst, unsigned bar, int i0, int lo, int hi) {
+  const int start = gi - shift;
+  const double *src = plane + start;
+  if (start >= 0 && start + slot <= isz && (reinterpret_cast<uintptr_t>(src) & 15) == 0 &&
+      (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+    const unsigned bytes = (unsigned)slot * 8u;
+    stage_expect(bar, bytes);
+    stage_bulk(dst, src, bytes, bar);
+    return bytes;
+  }
+  for (int c = 0; c < w; ++c)
+    if (i0 + c >= lo && i0 + c < hi) stage_cp8(dst + shift + c, plane + gi + c);
+  return 0;
+}
+
+// issue the copies of one chunk's tiles: the state tile (bv, sv of the chunk's
+// cells with the reconstruction halo along the sweep and one cell on each side
+// in-plane) and the cell tile (metric, Jacobian, properties of the faces' own
+// cells). Rows outside the block's ghosted extent are not copied, nor (8-byte
+// path) cells outside it: no face that is computed reads them. o1, o2: the
+// CTA's fixed coordinates (x sweep: j0 = first row, k; y sweep: i0 = first
+// column, k; z sweep: i0, j). Bulk path (zone flag kZoneBulk): thread t copies
+// rows t, t + 256, ... of both tiles, one bulk copy each; 8-byte path: warp w
+// copies rows w, w + 8, ..., one cp.async per cell and lane. sshift / qshift:
+// the tile column of a state / cell row's first cell.
+template <int NS, int NT, int DIR, bool BULK>
 __device__ __forceinline__ void stage_issue(const DevZone &z, double *tile, double *qtile, int nq, int F, int o1,
-                                            int o2) {
+                                            int o2, int sshift, int qshift, unsigned bar) {
   using G = StageGeom<DIR>;
-  constexpr int NVAR = 6 + NS + NT;
+  constexpr int NVAR = 6 + NS + NT, NT_S = NVAR * G::TR;
   const int lane = threadIdx.x;
   const int g = z.ngg;
   auto in_i = [&](int i) { return i >= -g && i < z.mx + g; };
   auto rows_ok = [&](int j, int k) { return j >= -g && j < z.my + g && k >= -g && k < z.mz + g; };
-  {  // state tile: first cell of row r is x (F-1, j0-1+r, k); y (i0-1, F-1+r, k); z (i0-1, j, F-1+r)
-    const int i0 = DIR == 0 ? F - 1 : o1 - 1;
-    const bool c0_ok = in_i(i0 + lane), c1_ok = lane + 32 < G::W && in_i(i0 + lane + 32);
-#pragma unroll 2
-    for (int rr = threadIdx.y; rr < NVAR * G::TR; rr += SR) {
-      const int var = rr / G::TR, r = rr - var * G::TR;
-      const int j = DIR == 0 ? o1 - 1 + r : (DIR == 1 ? F - 1 + r : o2);
-      const int k = DIR == 2 ? F - 1 + r : o2;
-      if (!rows_ok(j, k)) continue;
-      const double *src = (var < 6 ? z.bv + var * z.isz : z.sv + (var - 6) * z.isz) + gidx(z, i0, j, k);
-      double *dst = tile + rr * G::W;
-      if (c0_ok) stage_cp8(dst + lane, src + lane);
-      if (c1_ok) stage_cp8(dst + lane + 32, src + lane + 32);
+  // state row r of variable var: first cell x (F-1, j0-1+r, k); y (i0-1, F-1+r, k); z (i0-1, j, F-1+r)
+  const int si0 = DIR == 0 ? F - 1 : o1 - 1;
+  auto srow = [&](int rr, const double *&plane, int &gi) {
+    const int var = rr / G::TR, r = rr - var * G::TR;
+    const int j = DIR == 0 ? o1 - 1 + r : (DIR == 1 ? F - 1 + r : o2);
+    const int k = DIR == 2 ? F - 1 + r : o2;
+    if (!rows_ok(j, k)) return false;
+    plane = var < 6 ? z.bv + var * z.isz : z.sv + (var - 6) * z.isz;
+    gi = gidx(z, si0, j, k);
+    return true;
+  };
+  // cell row r of plane p: first cell x (F, j0+r, k); y (i0, F+r, k); z (i0, j, F+r)
+  const int qi0 = DIR == 0 ? F : o1;
+  auto qrow = [&](int rr, const double *&plane, int &gi) {
+    const int p = rr / G::QR, r = rr - p * G::QR;
+    const int j = DIR == 0 ? o1 + r : (DIR == 1 ? F + r : o2);
+    const int k = DIR == 2 ? F + r : o2;
+    if (!rows_ok(j, k)) return false;
+    plane = stage_q_plane<NT>(z, p);
+    gi = gidx(z, qi0, j, k);
+    return true;
+  };
+  if constexpr (BULK) {
+    const int tid = threadIdx.y * 32 + lane;
+    for (int rr = tid; rr < NT_S + nq * G::QR; rr += 32 * SR) {
+      const double *plane;
+      int gi;
+      if (rr < NT_S) {
+        if (srow(rr, plane, gi))
+          stage_row_bulk(plane, z.isz, gi, G::W, G::WS, sshift, tile + rr * G::WS, bar, si0, -g, z.mx + g);
+      } else {
+        const int q = rr - NT_S;
+        if (qrow(q, plane, gi))
+          stage_row_bulk(plane, z.isz, gi, G::QW, G::QWS, qshift, qtile + q * G::QWS, bar, qi0, -g, z.mx + g);
+      }
     }
-  }
-  {  // cell tile: first cell of row r is x (F, j0+r, k); y (i0, F+r, k); z (i0, j, F+r)
-    const int i0 = DIR == 0 ? F : o1;
-    const bool c0_ok = in_i(i0 + lane), c1_ok = lane + 32 < G::QW && in_i(i0 + lane + 32);
+  } else {
+    const bool s0 = in_i(si0 + lane), s1 = lane + 32 < G::W && in_i(si0 + lane + 32);
+#pragma unroll 2
+    for (int rr = threadIdx.y; rr < NT_S; rr += SR) {
+      const double *plane;
+      int gi;
+      if (!srow(rr, plane, gi)) continue;
+      double *dst = tile + rr * G::WS + sshift;
+      if (s0) stage_cp8(dst + lane, plane + gi + lane);
+      if (s1) stage_cp8(dst + lane + 32, plane + gi + lane + 32);
+    }
+    const bool q0 = in_i(qi0 + lane), q1 = lane + 32 < G::QW && in_i(qi0 + lane + 32);
 #pragma unroll 2
     for (int rr = threadIdx.y; rr < nq * G::QR; rr += SR) {
-      const int p = rr / G::QR, r = rr - p * G::QR;
-      const int j = DIR == 0 ? o1 + r : (DIR == 1 ? F + r : o2);
-      const int k = DIR == 2 ? F + r : o2;
-      if (!rows_ok(j, k)) continue;
-      const double *src = stage_q_plane<NT>(z, p) + gidx(z, i0, j, k);
-      double *dst = qtile + rr * G::QW;
-      if (c0_ok) stage_cp8(dst + lane, src + lane);
-      if (c1_ok) stage_cp8(dst + lane + 32, src + lane + 32);
+      const double *plane;
+      int gi;
+      if (!qrow(rr, plane, gi)) continue;
+      double *dst = qtile + rr * G::QWS + qshift;
+      if (q0) stage_cp8(dst + lane, plane + gi + lane);
+      if (q1) stage_cp8(dst + lane + 32, plane + gi + lane + 32);
     }
   }
   stage_commit();
 }
 
-template <int NS, int INV, int DIR, int PART, int NT>
-__device__ __forceinline__ void flux_tile_staged(const DevZone &z, const int bx, const int by, const int bz,
-                                                 int nchunk, int accumulate, int viscous, double *smem) {
+// one segment (bx, by, bz) of zone z; BULK: the tiles move as bulk copies (the
+// zone has kZoneBulk), else as 8-byte cp.async; bar: the CTA's initialised tile
+// mbarrier, phase: its current phase parity (advanced per bulk chunk). Returns
+// false when a tile wait ran out (CTA-uniform; the kernel then stops).
+template <int NS, int INV, int DIR, int PART, int NT, bool BULK>
+__device__ __forceinline__ bool flux_tile_staged(const DevZone &z, const int bx, const int by, const int bz,
+                                                 int nchunk, int accumulate, int viscous, double *smem, unsigned bar,
+                                                 unsigned &phase) {
   using Geo = StageGeom<DIR>;
   constexpr int NV = 5 + NS + NT, NVAR = 6 + NS + NT, R = SR;
   static_assert(INV != 1, "AWENO reads its cells (and the central correction's) from the planes");
@@ -308,9 +430,27 @@ __device__ __forceinline__ void flux_tile_staged(const DevZone &z, const int bx,
     for (int l = 0; l < NV; ++l) carry[row][l] = 0;
   for (int ch = 0; ch < nchunk; ++ch) {
     const int F = c0 - 1 + span * ch;
-    stage_issue<NS, NT, DIR>(z, tile, qtile, nq, F, o1, o2);
+    // tile columns of the rows' first cells: with bulk copies each row starts on
+    // a 16-byte boundary, which (even row and plane lengths) the parity of the
+    // first cell's index decides alike for every row of a tile
+    const int si0 = DIR == 0 ? F - 1 : o1 - 1;
+    const int sshift = BULK ? (si0 + z.dt_) & 1 : 0, qshift = BULK ? (si0 + 1 + z.dt_) & 1 : 0;
+    stage_issue<NS, NT, DIR, BULK>(z, tile, qtile, nq, F, o1, o2, sshift, qshift, bar);
     stage_wait_all();
-    __syncthreads();
+    if constexpr (BULK) {
+      __syncthreads();  // every copying thread has announced its bytes
+      if (threadIdx.x == 0 && threadIdx.y == 0) stage_arrive(bar);
+      const bool late = !stage_bar_wait(bar, phase);
+      if (__syncthreads_or(late)) {
+        // give up: record it, let the copies in flight land (bounded) and stop
+        if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(&g_stage_timeout, 1);
+        stage_bar_wait(bar, phase);
+        return false;
+      }
+      phase ^= 1u;
+    } else {
+      __syncthreads();
+    }
     // this thread's face and cell
     const int f = F + (DIR == 0 ? lane : row);
     const int i = DIR == 0 ? f : bx * 32 + lane;
@@ -320,9 +460,10 @@ __device__ __forceinline__ void flux_tile_staged(const DevZone &z, const int bx,
     double G[NV];
     if (active) {
       const int g = gidx(z, i, j, k);
-      const TileCells<DIR == 0 ? 1 : Geo::W, DIR == 0 ? Geo::W : 1, Geo::TV, DIR == 0 ? 1 : Geo::QW, Geo::QV,
+      const TileCells<DIR == 0 ? 1 : Geo::WS, DIR == 0 ? Geo::WS : 1, Geo::TV, DIR == 0 ? 1 : Geo::QWS, Geo::QV,
                       q_rhod<NT>()>
-          tc{plane_cells<DIR>(z, g), tile + (row + 1) * Geo::W + lane + 1, qtile + row * Geo::QW + lane};
+          tc{plane_cells<DIR>(z, g), tile + (row + 1) * Geo::WS + lane + 1 + sshift,
+             qtile + row * Geo::QWS + lane + qshift};
       face_total<NS, INV, DIR, PART, NT>(z, tc, g, vis, G);
     } else {
 #pragma unroll
@@ -351,7 +492,10 @@ __device__ __forceinline__ void flux_tile_staged(const DevZone &z, const int bx,
             dq[l * z.iqsz] = d;
         }
       }
-      __syncthreads();  // every face of the chunk has read the tiles before they are refilled
+      // every face of the chunk has read the tiles (ordered before the next
+      // chunk's asynchronous copies into them) before they are refilled
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
     } else {
       __syncthreads();  // every face has read the tiles: the state tile now takes the face fluxes
       double *sG = tile;  // [R][NV][32]
@@ -370,6 +514,7 @@ __device__ __forceinline__ void flux_tile_staged(const DevZone &z, const int bx,
             dq[l * z.iqsz] = d;
         }
       }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();  // the previous chunk's carried flux and the exchange are read
       if (row == R - 1)
 #pragma unroll
@@ -377,22 +522,41 @@ __device__ __forceinline__ void flux_tile_staged(const DevZone &z, const int bx,
     }
   }
   if constexpr (DIR != 0) __syncthreads();  // the carried flux of this tile is written before a next tile starts
+  return true;
 }
 
-template <int NS, int INV, int DIR, int MINB, int PART, int NT>
+// the CTA's tile mbarrier, initialised once per launch
+__device__ __forceinline__ unsigned stage_bar_setup(unsigned long long *bar_mem) {
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(bar_mem);
+  if (threadIdx.x == 0 && threadIdx.y == 0) stage_bar_init(bar);
+  __syncthreads();
+  return bar;
+}
+
+// BULK: every zone the launch walks has kZoneBulk (the launcher checks)
+template <int NS, int INV, int DIR, int MINB, int PART, int NT, bool BULK>
 __global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::blocks)
     flux_dir_staged(DevZone z, int nchunk, int accumulate, int viscous) {
-  extern __shared__ double smem[];
-  flux_tile_staged<NS, INV, DIR, PART, NT>(z, blockIdx.x, blockIdx.y, blockIdx.z, nchunk, accumulate, viscous, smem);
+  extern __shared__ __align__(16) double smem[];
+  __shared__ unsigned long long bar_mem;
+  const unsigned bar = stage_bar_setup(&bar_mem);
+  unsigned phase = 0;
+  flux_tile_staged<NS, INV, DIR, PART, NT, BULK>(z, blockIdx.x, blockIdx.y, blockIdx.z, nchunk, accumulate, viscous,
+                                                 smem, bar, phase);
 }
 
-template <int NS, int INV, int DIR, int MINB, int PART, int NT>
+template <int NS, int INV, int DIR, int MINB, int PART, int NT, bool BULK>
 __global__ void __launch_bounds__(FluxBounds<MINB>::threads, FluxBounds<MINB>::blocks)
     flux_dir_staged_table(const int4 *tiles, int n_tiles, int nchunk, int accumulate, int viscous) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
+  __shared__ unsigned long long bar_mem;
+  const unsigned bar = stage_bar_setup(&bar_mem);
+  unsigned phase = 0;
   for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
     const int4 c = tiles[t];
-    flux_tile_staged<NS, INV, DIR, PART, NT>(c_zones[c.x], c.y, c.z, c.w, nchunk, accumulate, viscous, smem);
+    if (!flux_tile_staged<NS, INV, DIR, PART, NT, BULK>(c_zones[c.x], c.y, c.z, c.w, nchunk, accumulate, viscous,
+                                                        smem, bar, phase))
+      return;
   }
 }
 
@@ -475,17 +639,17 @@ static cudaError_t launch_flux_m(const DevZone &z, const TileShape &t, const Flu
 // memory = state tile + cell tile (+ the y / z sweep's carried face flux),
 // checked against the 227 KB a CTA may use; the carveout is sized for the CTAs
 // that fit
-template <int NS, int INV, int DIR, int PART, int NT>
-static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
-                                 int viscous, cudaStream_t s) {
+template <int NS, int INV, int DIR, int PART, int NT, bool BULK>
+static cudaError_t launch_flux_sb(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
+                                  int viscous, cudaStream_t s) {
   constexpr int NV = 5 + NS + NT, MINB = 2, R = SR;
   const int C = t.chunks;
   if (t.rows != SR) return cudaErrorInvalidConfiguration;
   const bool vis_planes = PART == 2 || (PART == 0 && viscous);
   const size_t smem = sizeof(double) * stage_smem_doubles<NS, NT, DIR>(vis_planes);
   if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
-  const void *fn = tab ? (const void *)flux_dir_staged_table<NS, INV, DIR, MINB, PART, NT>
-                       : (const void *)flux_dir_staged<NS, INV, DIR, MINB, PART, NT>;
+  const void *fn = tab ? (const void *)flux_dir_staged_table<NS, INV, DIR, MINB, PART, NT, BULK>
+                       : (const void *)flux_dir_staged<NS, INV, DIR, MINB, PART, NT, BULK>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -501,7 +665,7 @@ static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, const Flu
   }
   const dim3 blk(32, R);
   if (!tab) {
-    flux_dir_staged<NS, INV, DIR, MINB, PART, NT><<<flux_grid(z.mx, z.my, z.mz, DIR, R, C), blk, smem, s>>>(
+    flux_dir_staged<NS, INV, DIR, MINB, PART, NT, BULK><<<flux_grid(z.mx, z.my, z.mz, DIR, R, C), blk, smem, s>>>(
         z, C, accumulate, viscous);
     return cudaGetLastError();
   }
@@ -512,9 +676,19 @@ static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, const Flu
   if (e != cudaSuccess) return e;
   const int slots = per_sm * sms;
   const int grid = tab->n < slots ? tab->n : slots;
-  flux_dir_staged_table<NS, INV, DIR, MINB, PART, NT><<<grid, blk, smem, s>>>(tab->tiles, tab->n, C, accumulate,
+  flux_dir_staged_table<NS, INV, DIR, MINB, PART, NT, BULK><<<grid, blk, smem, s>>>(tab->tiles, tab->n, C, accumulate,
                                                                               viscous);
   return cudaGetLastError();
+}
+
+// the bulk-copy build when every zone of the launch has kZoneBulk (tab_bulk:
+// the context's verdict over the zones a tile table walks)
+template <int NS, int INV, int DIR, int PART, int NT>
+static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
+                                 int viscous, cudaStream_t s) {
+  const bool bulk = tab ? tab->bulk : (z.flags & kZoneBulk) != 0;
+  return bulk ? launch_flux_sb<NS, INV, DIR, PART, NT, true>(z, t, tab, accumulate, viscous, s)
+              : launch_flux_sb<NS, INV, DIR, PART, NT, false>(z, t, tab, accumulate, viscous, s);
 }
 
 template <int NS, int INV, int DIR, int PART, int NT>

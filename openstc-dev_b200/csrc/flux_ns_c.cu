@@ -35,6 +35,9 @@ cudaError_t upload_param_flux_ns_c(const DevParam &p, cudaStream_t s) {
   return cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);
 }
 
+// this unit's staged-kernel timeout flag (read and cleared)
+cudaError_t stage_timeout_flux_ns_c(int *flag) { return stage_timeout_read(flag); }
+
 cudaError_t upload_zones_flux_ns_c(const DevZone *z, int n, cudaStream_t s) {
   if (n < 0 || n > kMaxTableZones) return cudaErrorInvalidValue;
   return n ? cudaMemcpyToSymbolAsync(c_zones, z, sizeof(DevZone) * n, 0, cudaMemcpyHostToDevice, s) : cudaSuccess;

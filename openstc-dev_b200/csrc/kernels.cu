@@ -1246,6 +1246,21 @@ bool mechanism_is_h2air9(const int *reac_type, const int *stoi_f, const int *sto
   return true;
 }
 
+// any staged-flux tile wait that ran out, over all flux units (flags cleared)
+cudaError_t stage_timeouts(int *any) {
+  cudaError_t (*const fns[])(int *) = {stage_timeout_flux0,     stage_timeout_flux9,     stage_timeout_flux0t,
+                                        stage_timeout_flux9t,    stage_timeout_flux_ns_a, stage_timeout_flux_ns_b,
+                                        stage_timeout_flux_ns_c, stage_timeout_flux_ns_d};
+  *any = 0;
+  for (auto fn : fns) {
+    int f = 0;
+    const cudaError_t e = fn(&f);
+    if (e != cudaSuccess) return e;
+    *any |= f;
+  }
+  return cudaSuccess;
+}
+
 // this unit's parameters and those of the flux units (flux0.cu, flux9.cu)
 cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   cudaError_t e = cudaMemcpyToSymbolAsync(c_p, &p, sizeof(DevParam), 0, cudaMemcpyHostToDevice, s);

@@ -32,6 +32,7 @@ constexpr int kMaxTableZones = 64;
 struct FluxTable {
   const int4 *tiles = nullptr;
   int n = 0;
+  bool bulk = false;  // every zone of the table has kZoneBulk
 };
 using CellTable = FluxTable;
 
@@ -116,6 +117,17 @@ cudaError_t upload_zones_flux0(const DevZone *z, int n, cudaStream_t s);   // fl
 cudaError_t upload_zones_flux9(const DevZone *z, int n, cudaStream_t s);   // flux9.cu
 cudaError_t upload_zones_flux0t(const DevZone *z, int n, cudaStream_t s);  // flux0t.cu
 cudaError_t upload_zones_flux9t(const DevZone *z, int n, cudaStream_t s);  // flux9t.cu
+// staged flux kernels: whether a tile wait ran out since the last read (the
+// flag is cleared), per flux unit and over all of them (kernels.cu)
+cudaError_t stage_timeout_flux0(int *flag);
+cudaError_t stage_timeout_flux9(int *flag);
+cudaError_t stage_timeout_flux0t(int *flag);
+cudaError_t stage_timeout_flux9t(int *flag);
+cudaError_t stage_timeout_flux_ns_a(int *flag);
+cudaError_t stage_timeout_flux_ns_b(int *flag);
+cudaError_t stage_timeout_flux_ns_c(int *flag);
+cudaError_t stage_timeout_flux_ns_d(int *flag);
+cudaError_t stage_timeouts(int *any);
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s);
 template <int NS>

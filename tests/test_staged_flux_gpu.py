@@ -5,7 +5,10 @@ the same RHS bit for bit and the same steps, for every face they are built
 for (primitive-variable reconstruction of first order, MUSCL and NND2 with
 AUSM+, HLLC and Roe; the mixture; k-omega SST; several blocks walked by the
 tile table; 2-D blocks), with tile shapes whose last tiles are partial at the
-block edges. The split inviscid and viscous kernels are staged alike.
+block edges. Blocks whose ghosted rows have an even length move their tiles
+as 16-byte bulk copies, the others as 8-byte cp.async: both are covered (the
+"_even" cases and their odd twins). The split inviscid and viscous kernels
+are staged alike.
 """
 import numpy as np
 import pytest
@@ -22,8 +25,8 @@ def staged(chunks=(2, 3, 2)):
     return [(8 | 2 << 8 | 1 << 16, chunks[d]) for d in range(3)]
 
 
-def _mixing(**kw):
-    return ostc.case_mixing_layer(37, 29, 19, dx=1e-3, full_host=True, **kw)
+def _mixing(mx=37, **kw):
+    return ostc.case_mixing_layer(mx, 29, 19, dx=1e-3, full_host=True, **kw)
 
 
 def _scheme(case, reconstruction=None, inviscid_scheme=None):
@@ -47,7 +50,21 @@ CASES = {
         rans_model=2),
     "planar_sst": lambda: planar_sst(),
     "planar_mixing": lambda: ostc.case_mixing_layer(41, 23, 1, full_host=True),
+    "mixing_muscl_ausm_even": lambda: _mixing(38),
+    "mixing_muscl_roe_even": lambda: _scheme(_mixing(38), inviscid_scheme=2),
+    "mixing_sst_wall_even": lambda: _mixing(38, rans_model=2, wall=True),
+    "vortex_muscl_hllc_even": lambda: ostc.case_vortex(46, 38, 11, reconstruction=2, inviscid_scheme=4),
+    "planar_mixing_even": lambda: ostc.case_mixing_layer(42, 23, 1, full_host=True),
+    "even_blocks": lambda: ostc.case_uneven_blocks(
+        layout=[((0, 0, 0), (20, 14, 10)), ((19, 0, 0), (40, 14, 10))], rans_model=2),
 }
+
+
+def test_even_rows_take_the_bulk_copies():
+    """the zone flag that selects bulk copies: even ghosted rows and aligned planes"""
+    for name, even in (("mixing_muscl_ausm", False), ("mixing_muscl_ausm_even", True)):
+        b = CASES[name]().blocks[0]
+        assert ((b.mx + 2 * b.ngg) % 2 == 0) == even
 
 
 def _run(case, tiles, split=False, steps=0):
@@ -88,8 +105,9 @@ def test_staged_split_kernels():
         assert np.max(np.abs(a - b) / np.where(scale > 0, scale, 1)) < 1e-12
 
 
-def test_staged_steps_are_the_plane_steps():
-    case = CASES["mixing_muscl_ausm"]
+@pytest.mark.parametrize("name", ["mixing_muscl_ausm", "mixing_muscl_ausm_even"])
+def test_staged_steps_are_the_plane_steps(name):
+    case = CASES[name]
     _, (h_ref, bv_ref) = _run(case(), PLANE, steps=4)
     _, (h_got, bv_got) = _run(case(), staged(), steps=4)
     assert np.array_equal(h_got[0], h_ref[0]) and np.array_equal(h_got[1], h_ref[1])
