@@ -112,6 +112,7 @@ ostc_status ensure_param(ostc_ctx *ctx, cudaStream_t s) {
 ostc_status build_tables(ostc_ctx *ctx) {
   std::vector<int4> all;
   std::vector<std::pair<size_t, size_t>> spans;  // [begin, end) of each table in `all`
+  std::vector<size_t> flux_bulk_tiles;           // per flux table: its leading tiles of kZoneBulk zones
   auto cells = [&](int ext_add_xy, bool ghosted) {
     const size_t b0 = all.size();
     for (size_t b = 0; b < ctx->dz.size(); ++b) {
@@ -133,16 +134,23 @@ ostc_status build_tables(ostc_ctx *ctx) {
       const size_t b0 = all.size();
       const TileShape &t = ctx->tile[d];
       const int R = v ? t.vrows : t.rows, C = v ? t.vchunks : t.chunks;
+      // the tiles of zones with kZoneBulk first, then the others: the staged
+      // kernels walk the two parts with their bulk-copy and 8-byte builds
+      size_t nb = 0;
       if (R > 0)
-        for (size_t b = 0; b < ctx->dz.size(); ++b) {
-          const DevZone &z = ctx->dz[b];
-          if (d == 2 && z.mz <= 1) continue;
-          const dim3 g = flux_grid(z.mx, z.my, z.mz, d, R, C);
-          for (unsigned bz = 0; bz < g.z; ++bz)
-            for (unsigned by = 0; by < g.y; ++by)
-              for (unsigned bx = 0; bx < g.x; ++bx) all.push_back(make_int4((int)b, bx, by, bz));
-        }
+        for (int pass = 0; pass < 2; ++pass)
+          for (size_t b = 0; b < ctx->dz.size(); ++b) {
+            const DevZone &z = ctx->dz[b];
+            if (d == 2 && z.mz <= 1) continue;
+            if (((z.flags & kZoneBulk) != 0) != (pass == 0)) continue;
+            const dim3 g = flux_grid(z.mx, z.my, z.mz, d, R, C);
+            for (unsigned bz = 0; bz < g.z; ++bz)
+              for (unsigned by = 0; by < g.y; ++by)
+                for (unsigned bx = 0; bx < g.x; ++bx) all.push_back(make_int4((int)b, bx, by, bz));
+            if (pass == 0) nb += (size_t)g.x * g.y * g.z;
+          }
       spans.push_back({b0, all.size()});
+      flux_bulk_tiles.push_back(nb);
     }
   if (all.size() > (size_t)INT32_MAX) return fail(ctx, OSTC_ERR_UNSUPPORTED);
   if (all.size() > ctx->tab_cap) {
@@ -153,18 +161,18 @@ ostc_status build_tables(ostc_ctx *ctx) {
     ctx->tab_cap = all.size();
   }
   if (!all.empty()) CK(cudaMemcpy(ctx->tab_dev, all.data(), sizeof(int4) * all.size(), cudaMemcpyHostToDevice));
-  bool all_bulk = true;
-  for (const DevZone &z : ctx->dz) all_bulk = all_bulk && (z.flags & kZoneBulk) != 0;
   auto table = [&](size_t q) {
     FluxTable t;
     t.tiles = ctx->tab_dev + spans[q].first;
     t.n = (int)(spans[q].second - spans[q].first);
-    t.bulk = all_bulk;
     return t;
   };
   for (int c = 0; c < 3; ++c) ctx->cell_tab[c] = table(c);
   for (int d = 0; d < 3; ++d)
-    for (int v = 0; v < 2; ++v) ctx->flux_tab[d][v] = table(3 + 2 * d + v);
+    for (int v = 0; v < 2; ++v) {
+      ctx->flux_tab[d][v] = table(3 + 2 * d + v);
+      ctx->flux_tab[d][v].n_bulk = (int)flux_bulk_tiles[2 * d + v];
+    }
   return OSTC_OK;
 }
 

@@ -681,14 +681,21 @@ static cudaError_t launch_flux_sb(const DevZone &z, const TileShape &t, const Fl
   return cudaGetLastError();
 }
 
-// the bulk-copy build when every zone of the launch has kZoneBulk (tab_bulk:
-// the context's verdict over the zones a tile table walks)
+// the bulk-copy build for zones with kZoneBulk, the 8-byte one for the others:
+// a tile table holds the tiles of the bulk zones first (n_bulk), so it is
+// walked by one launch of each build over its part (zones are independent)
 template <int NS, int INV, int DIR, int PART, int NT>
 static cudaError_t launch_flux_s(const DevZone &z, const TileShape &t, const FluxTable *tab, int accumulate,
                                  int viscous, cudaStream_t s) {
-  const bool bulk = tab ? tab->bulk : (z.flags & kZoneBulk) != 0;
-  return bulk ? launch_flux_sb<NS, INV, DIR, PART, NT, true>(z, t, tab, accumulate, viscous, s)
-              : launch_flux_sb<NS, INV, DIR, PART, NT, false>(z, t, tab, accumulate, viscous, s);
+  if (!tab) {
+    return (z.flags & kZoneBulk) ? launch_flux_sb<NS, INV, DIR, PART, NT, true>(z, t, nullptr, accumulate, viscous, s)
+                                 : launch_flux_sb<NS, INV, DIR, PART, NT, false>(z, t, nullptr, accumulate, viscous, s);
+  }
+  const FluxTable tb{tab->tiles, tab->n_bulk, tab->n_bulk}, tc{tab->tiles + tab->n_bulk, tab->n - tab->n_bulk, 0};
+  cudaError_t e = cudaSuccess;
+  if (tb.n > 0) e = launch_flux_sb<NS, INV, DIR, PART, NT, true>(z, t, &tb, accumulate, viscous, s);
+  if (e == cudaSuccess && tc.n > 0) e = launch_flux_sb<NS, INV, DIR, PART, NT, false>(z, t, &tc, accumulate, viscous, s);
+  return e;
 }
 
 template <int NS, int INV, int DIR, int PART, int NT>

@@ -1,0 +1,183 @@
+// gemm_tc.cuh — the training GEMM of the chemistry surrogate on the 5th-generation
+// tensor cores: C[M][N] (+)= A[M][K] B[N][K]^T with BF16 operands stored K-major
+// (row-major, K contiguous), FP32 accumulation in tensor memory.
+//
+// One CTA of 128 threads owns 128 rows of C (all N <= 256 columns) and a
+// slice of K. K moves through shared memory in chunks of 64 (two stages):
+// every thread copies its share of the chunk's A and B rows into the
+// canonical no-swizzle K-major layout with 16-byte cp.async (rows of A past M
+// are zero-filled), one thread issues the chunk's MMAs (tcgen05.mma kind::f16,
+// M = 128, N, K = 16 each) and commits them to the stage's mbarrier, which is
+// waited on (bounded by the global timer) before the stage is refilled two
+// chunks later, so the copies of one chunk overlap the MMAs of the previous
+// one. The epilogue reads the accumulators with tcgen05.ld (warp w: rows
+// 32w..32w+31) and either stores C (+ bias, with the BF16 SiLU activation) or
+// adds it atomically (split-K over blockIdx.y). A wait that runs out sets the
+// error word; the CTA then waits (bounded) for the MMAs it issued, frees its
+// tensor memory and returns.
+#pragma once
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "tc_mlp.cuh"
+
+namespace ostc {
+namespace mlp {
+
+struct TcGemmArgs {
+  const __nv_bfloat16 *a;  // [M][lda], K contiguous; rows 16-byte aligned
+  const __nv_bfloat16 *b;  // [N][ldb], K contiguous; rows 16-byte aligned
+  float *c;                // [M][ldc]
+  int lda, ldb, ldc;
+  int M, N, K;             // N % 16 == 0, 16 <= N <= 256, K % 16 == 0
+  int k_per_split;         // K of one blockIdx.y (a multiple of TC_BK)
+  const float *bias;       // per column, or null (stored results only)
+  __nv_bfloat16 *act;      // bf16 silu(C) [M][ldc], or null
+  int atomic;              // add into C (C pre-zeroed) instead of storing
+  int *err;                // set when a bounded wait ran out
+};
+
+constexpr int TC_BK = 64;                               // K of one chunk
+constexpr int TC_THREADS = 128;
+constexpr unsigned TC_A_BYTES = 128 * TC_BK * 2;        // 16 KB
+constexpr unsigned TC_B_BYTES = 256 * TC_BK * 2;        // 32 KB (N <= 256)
+constexpr unsigned TC_STAGE = TC_A_BYTES + TC_B_BYTES;  // 48 KB
+constexpr unsigned TC_SMEM = 2 * TC_STAGE + 32;         // two stages, two mbarriers, the TMEM slot
+
+__device__ __forceinline__ void cp_async16_zfill(unsigned dst, const void *src, unsigned src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
+__device__ __forceinline__ float silu_tc(float z) { return z / (1.0f + __expf(-z)); }
+
+__global__ void __launch_bounds__(TC_THREADS, 1) gemm_tc_kernel(TcGemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  using namespace tc;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned base = smem_u32(sm);
+  const unsigned bar[2] = {base + 2 * TC_STAGE, base + 2 * TC_STAGE + 8};
+  unsigned *tmem_slot = (unsigned *)(sm + 2 * TC_STAGE + 16);
+  const unsigned ncols = g.N <= 32 ? 32u : (g.N <= 64 ? 64u : (g.N <= 128 ? 128u : 256u));
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar[0]));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar[1]));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const unsigned tmem = *tmem_slot;
+  const int m0 = blockIdx.x * 128;
+  const int kb = blockIdx.y * g.k_per_split;
+  const int ke = min(g.K, kb + g.k_per_split);
+  const int nchunks = ke > kb ? (ke - kb + TC_BK - 1) / TC_BK : 0;
+  const unsigned idesc = idesc_bf16(g.N);
+  unsigned phase[2] = {0u, 0u};
+  bool pending[2] = {false, false};
+  bool late = false;
+  for (int c = 0; c < nchunks; ++c) {
+    const int s = c & 1;
+    const int k0 = kb + c * TC_BK, kc = min(TC_BK, ke - k0);
+    if (pending[s]) {  // the MMAs of chunk c - 2 read this stage
+      if (bar_wait(bar[s], phase[s])) {
+        phase[s] ^= 1u;
+        pending[s] = false;
+      } else {
+        late = true;
+      }
+      if (__syncthreads_or(late)) break;
+    }
+    const unsigned sa = base + s * TC_STAGE, sb = sa + TC_A_BYTES;
+    const int q = kc / 8;  // 16-byte pieces per row
+    for (int i = tid; i < 128 * q; i += TC_THREADS) {
+      const int r = i / q, kq = i - r * q;
+      const bool ok = m0 + r < g.M;
+      const __nv_bfloat16 *src = g.a + (long long)(ok ? m0 + r : 0) * g.lda + k0 + kq * 8;
+      cp_async16_zfill(sa + core_off(r, kq * 8, TC_BK), src, ok ? 16u : 0u);
+    }
+    for (int i = tid; i < g.N * q; i += TC_THREADS) {
+      const int n = i / q, kq = i - n * q;
+      cp_async16(sb + core_off(n, kq * 8, TC_BK), g.b + (long long)n * g.ldb + k0 + kq * 8);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    fence_async_smem();  // the copies (generic proxy) before the MMAs' reads (async proxy)
+    __syncthreads();
+    if (tid == 0) {
+      fence_after();
+      for (int ks = 0; ks < kc / 16; ++ks) {
+        // K-adjacent core matrices 128 B apart, 8-row groups TC_BK / 8 * 128 B apart
+        const unsigned long long ad = smem_desc(sa + ks * 256, 128, (TC_BK / 8) * 128);
+        const unsigned long long bd = smem_desc(sb + ks * 256, 128, (TC_BK / 8) * 128);
+        mma_issue(tmem, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+      }
+      mma_commit(bar[s]);
+    }
+    pending[s] = true;
+  }
+  // the MMAs still in flight (bounded again after a timeout)
+  for (int s = 0; s < 2; ++s)
+    if (pending[s]) {
+      if (bar_wait(bar[s], phase[s]))
+        phase[s] ^= 1u;
+      else
+        late = true;
+    }
+  late = __syncthreads_or(late);
+  fence_after();
+  if (late) {
+    if (tid == 0) atomicExch(g.err, 1);
+  } else if (nchunks > 0) {
+    const int row = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < g.N; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
+      if (row >= g.M) continue;
+      float *crow = g.c + (long long)row * g.ldc + c0;
+      if (g.atomic) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) atomicAdd(crow + j, v[j]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          float x = v[j];
+          if (g.bias) x += g.bias[c0 + j];
+          crow[j] = x;
+          if (g.act) g.act[(long long)row * g.ldc + c0 + j] = __float2bfloat16_rn(silu_tc(x));
+        }
+      }
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+// host launcher: grid (ceil(M / 128), splits); shapes and alignment checked here
+inline cudaError_t gemm_tc(const TcGemmArgs &a0, int splits, cudaStream_t s) {
+  TcGemmArgs a = a0;
+  if (a.N % 16 || a.N < 16 || a.N > 256 || a.K % 16 || a.K <= 0 || a.M <= 0 || a.lda % 8 || a.ldb % 8 ||
+      (reinterpret_cast<uintptr_t>(a.a) & 15) || (reinterpret_cast<uintptr_t>(a.b) & 15) || !a.err)
+    return cudaErrorInvalidValue;
+  splits = splits < 1 ? 1 : splits;
+  a.k_per_split = ((a.K + splits - 1) / splits + TC_BK - 1) / TC_BK * TC_BK;
+  const int z = (a.K + a.k_per_split - 1) / a.k_per_split;
+  a.atomic = z > 1 ? 1 : a.atomic;
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  gemm_tc_kernel<<<dim3((a.M + 127) / 128, z), TC_THREADS, TC_SMEM, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace mlp
+}  // namespace ostc

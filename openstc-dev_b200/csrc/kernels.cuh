@@ -32,7 +32,7 @@ constexpr int kMaxTableZones = 64;
 struct FluxTable {
   const int4 *tiles = nullptr;
   int n = 0;
-  bool bulk = false;  // every zone of the table has kZoneBulk
+  int n_bulk = 0;  // flux tables: the leading tiles, of zones with kZoneBulk
 };
 using CellTable = FluxTable;
 

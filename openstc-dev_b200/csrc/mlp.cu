@@ -8,24 +8,29 @@
 // FP32, and training keeps FP32 master weights with Adam.
 //
 // Training runs on hand-written kernels only:
-//   gemm_bf16_kernel     C = op(A) op(B)^T on the BF16 tensor cores
-//                        (mma.sync m16n8k16, FP32 accumulation) with
-//                        generic operand strides, so the same kernel gives
-//                        the forward products X W^T, the input gradients
-//                        dZ W and the weight gradients dZ^T X (split over
-//                        the batch with FP32 atomics), and a fused epilogue
-//                        (bias, SiLU, BF16 store);
-//   loss / SiLU-backward / column-sum / Adam kernels for the rest.
+//   gemm_tc_kernel       C = A B^T on the tcgen05 tensor cores (gemm_tc.cuh:
+//                        BF16 K-major operands, FP32 accumulators in tensor
+//                        memory): the forward products X W^T with a fused
+//                        bias + SiLU + BF16 epilogue, the input gradients
+//                        dZ W (against the transposed weights) and the weight
+//                        gradients dZ^T X (against the transposed gradients
+//                        and activations, split over the batch with FP32
+//                        atomics);
+//   transpose / loss / SiLU-backward / column-sum / Adam kernels for the rest.
+// gemm_bf16_kernel (mma.sync m16n8k16, generic strides) serves the
+// reference forward of ostc_surrogate_forward.
 // The fused inference kernel of the hot path (tcgen05, TMEM accumulators)
 // lives in surrogate.cuh and reads the BF16 weights kept here.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "../../include/ostc.h"
+#include "gemm_tc.cuh"
 #include "mlp.cuh"
 #include "tc_mlp.cuh"
 
@@ -218,6 +223,23 @@ __global__ void silu_backward_kernel(const float *da, const float *z, long long 
   dzb[e] = __float2bfloat16_rn(d);
 }
 
+// out[c][b] = in[b][c] for b < rows, 0 for rows <= b < ldo (a K-major operand
+// with its K padded to a multiple of 16); 32 x 32 tiles through shared memory
+__global__ void transpose_bf16_kernel(const __nv_bfloat16 *in, int rows, int cols, int ldi, __nv_bfloat16 *out,
+                                      int ldo) {
+  __shared__ __nv_bfloat16 t[32][33];
+  const int b0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int b = b0 + r, c = c0 + threadIdx.x;
+    t[r][threadIdx.x] = (b < rows && c < cols) ? in[(long long)b * ldi + c] : __float2bfloat16_rn(0.f);
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int c = c0 + r, b = b0 + threadIdx.x;
+    if (c < cols && b < ldo) out[(long long)c * ldo + b] = t[threadIdx.x][r];
+  }
+}
+
 // db[c] = sum_r dz[r][c] over n rows (one CTA per column block of 32)
 __global__ void colsum_kernel(const float *dz, int n, int ncol, float *db) {
   const int c = blockIdx.x * 32 + (threadIdx.x & 31);
@@ -308,6 +330,9 @@ struct ostc_surrogate {
   __nv_bfloat16 *x0 = nullptr, *a[3] = {nullptr, nullptr, nullptr}, *dzb[4] = {nullptr, nullptr, nullptr, nullptr};
   float *z[4] = {nullptr, nullptr, nullptr, nullptr}, *dz[4] = {nullptr, nullptr, nullptr, nullptr};
   float *da = nullptr, *loss = nullptr;
+  // K-major operands of the backward GEMMs: transposed gradients and
+  // activations ([256][batch padded to 16]) and transposed weights of layers 2..4
+  __nv_bfloat16 *tg = nullptr, *ta = nullptr, *wt = nullptr;
   int *err = nullptr;  // set by a tensor-core kernel whose bounded wait ran out
   Checks *checks = nullptr;  // device copy of the acceptance tests
   int *list = nullptr, *count = nullptr;
@@ -358,8 +383,25 @@ ostc_status refresh_bf16(ostc_surrogate *s, cudaStream_t st) {
   return OSTC_OK;
 }
 
-// forward of n standardised rows (x0 packed): z[0..3], a[0..2]
+// forward of n standardised rows (x0 packed): z[0..3], a[0..2] (tcgen05)
 ostc_status forward(ostc_surrogate *s, int n, cudaStream_t st) {
+  const Net &w = s->net;
+  const __nv_bfloat16 *in[4] = {s->x0, s->a[0], s->a[1], s->a[2]};
+  const __nv_bfloat16 *wl[4] = {w.w1(), w.w2(), w.w3(), w.w4()};
+  const float *bl[4] = {w.b1(), w.b2(), w.b3(), w.b4()};
+  for (int l = 0; l < 4; ++l) {
+    TcGemmArgs g{};
+    const int k = l == 0 ? KIN : NH, nn = l == 3 ? NOUTP : NH;
+    g.a = in[l], g.lda = k, g.b = wl[l], g.ldb = k;
+    g.c = s->z[l], g.ldc = nn, g.M = n, g.N = nn, g.K = k, g.bias = bl[l], g.act = l < 3 ? s->a[l] : nullptr;
+    g.err = s->err;
+    SK(gemm_tc(g, 1, st));
+  }
+  return OSTC_OK;
+}
+
+// the generic mma.sync forward (the reference of the tensor-core paths' tests)
+ostc_status forward_reference(ostc_surrogate *s, int n, cudaStream_t st) {
   const Net &w = s->net;
   GemmArgs g{};
   // layer 1: Z1 = X0 W1^T + b1
@@ -387,27 +429,41 @@ ostc_status backward(ostc_surrogate *s, const float *y, int n, cudaStream_t st) 
   SK(cudaMemsetAsync(s->grad, 0, sizeof(float) * NPAR, st));
   loss_grad_kernel<<<blocks((long long)n * NOUTP), 256, 0, st>>>(s->z[3], y, n, s->dz[3], s->dzb[3], s->loss);
   SK(cudaGetLastError());
-  const int splits = n >= 4096 ? n / 1024 : 1;
+  const int np = (n + 15) / 16 * 16;  // the batch as a K, padded with zero columns
   const __nv_bfloat16 *acts[4] = {s->x0, s->a[0], s->a[1], s->a[2]};
   const int kin[4] = {KIN, NH, NH, NH}, nout[4] = {NH, NH, NH, NOUTP};
   const long long offw[4] = {OFF_W1, OFF_W2, OFF_W3, OFF_W4}, offb[4] = {OFF_B1, OFF_B2, OFF_B3, OFF_B4};
   const __nv_bfloat16 *wl[4] = {w.w1(), w.w2(), w.w3(), w.w4()};
+  const dim3 tb(32, 8);
   for (int l = 3; l >= 0; --l) {
-    // weight gradient dW[n_out][k_in] = sum_b dZ[b][n_out] A[b][k_in] (split over the batch)
-    GemmArgs g{};
-    g.a = s->dzb[l], g.a_sm = 1, g.a_sk = nout[l];
-    g.b = acts[l], g.b_sn = 1, g.b_sk = kin[l];
-    g.c = s->grad + offw[l], g.ldc = kin[l], g.M = nout[l], g.N = kin[l], g.K = n;
-    SK(gemm(g, splits, st));
+    // weight gradient dW[n_out][k_in] = sum_b dZ[b][n_out] A[b][k_in]: dZ^T and A^T
+    // as K-major operands, split over the batch so that about two CTAs per SM run
+    transpose_bf16_kernel<<<dim3((np + 31) / 32, (nout[l] + 31) / 32), tb, 0, st>>>(s->dzb[l], n, nout[l], nout[l],
+                                                                                   s->tg, np);
+    SK(cudaGetLastError());
+    transpose_bf16_kernel<<<dim3((np + 31) / 32, (kin[l] + 31) / 32), tb, 0, st>>>(acts[l], n, kin[l], kin[l], s->ta,
+                                                                                  np);
+    SK(cudaGetLastError());
+    TcGemmArgs g{};
+    g.a = s->tg, g.lda = np, g.b = s->ta, g.ldb = np;
+    g.c = s->grad + offw[l], g.ldc = kin[l], g.M = nout[l], g.N = kin[l], g.K = np, g.atomic = 1;
+    g.err = s->err;
+    const int mt = (nout[l] + 127) / 128;
+    const int splits = std::max(1, std::min(np / 1024, 296 / mt));
+    SK(gemm_tc(g, splits, st));
     colsum_kernel<<<(nout[l] + 31) / 32, 256, 0, st>>>(s->dz[l], n, nout[l], s->grad + offb[l]);
     SK(cudaGetLastError());
     if (l == 0) break;
-    // input gradient dA[b][k] = sum_n dZ[b][n] W[n][k]
-    GemmArgs h{};
-    h.a = s->dzb[l], h.a_sm = nout[l], h.a_sk = 1;
-    h.b = wl[l], h.b_sn = 1, h.b_sk = kin[l];
+    // input gradient dA[b][k] = sum_n dZ[b][n] W[n][k], against W^T [k_in][n_out]
+    __nv_bfloat16 *wt = s->wt + (long long)(l - 1) * NH * NH;
+    transpose_bf16_kernel<<<dim3((nout[l] + 31) / 32, (kin[l] + 31) / 32), tb, 0, st>>>(wl[l], nout[l], kin[l],
+                                                                                       kin[l], wt, nout[l]);
+    SK(cudaGetLastError());
+    TcGemmArgs h{};
+    h.a = s->dzb[l], h.lda = nout[l], h.b = wt, h.ldb = nout[l];
     h.c = s->da, h.ldc = NH, h.M = n, h.N = kin[l], h.K = nout[l];
-    SK(gemm(h, 1, st));
+    h.err = s->err;
+    SK(gemm_tc(h, 1, st));
     silu_backward_kernel<<<blocks((long long)n * NH), 256, 0, st>>>(s->da, s->z[l - 1], (long long)n * NH,
                                                                      s->dz[l - 1], s->dzb[l - 1]);
     SK(cudaGetLastError());
@@ -440,6 +496,9 @@ ostc_status ostc_surrogate_create(int max_batch, unsigned long long seed, ostc_s
             dalloc(s, (void **)&s->net.scale, sizeof(double) * SCALE_COUNT) == cudaSuccess &&
             dalloc(s, (void **)&s->x0, sizeof(__nv_bfloat16) * B * KIN) == cudaSuccess &&
             dalloc(s, (void **)&s->da, sizeof(float) * B * NH) == cudaSuccess &&
+            dalloc(s, (void **)&s->tg, sizeof(__nv_bfloat16) * NH * ((B + 15) / 16 * 16)) == cudaSuccess &&
+            dalloc(s, (void **)&s->ta, sizeof(__nv_bfloat16) * NH * ((B + 15) / 16 * 16)) == cudaSuccess &&
+            dalloc(s, (void **)&s->wt, sizeof(__nv_bfloat16) * 3 * NH * NH) == cudaSuccess &&
             dalloc(s, (void **)&s->loss, sizeof(float)) == cudaSuccess &&
             dalloc(s, (void **)&s->err, sizeof(int)) == cudaSuccess &&
             dalloc(s, (void **)&s->count, sizeof(int)) == cudaSuccess &&
@@ -571,7 +630,7 @@ ostc_status ostc_surrogate_forward(ostc_surrogate *s, const float *xs, int n, fl
   if (n == 0) return OSTC_OK;
   cudaStream_t st = (cudaStream_t)stream;
   ostc_status r;
-  if ((r = pack(s, xs, n, st)) || (r = forward(s, n, st))) return r;
+  if ((r = pack(s, xs, n, st)) || (r = forward_reference(s, n, st))) return r;
   // the 10 outputs of the padded layer
   SK(cudaMemcpy2DAsync(ys, sizeof(float) * NOUT, s->z[3], sizeof(float) * NOUTP, sizeof(float) * NOUT, n,
                        cudaMemcpyDeviceToDevice, st));
@@ -611,7 +670,13 @@ ostc_status ostc_surrogate_gradients(ostc_surrogate *s, const float *xs, const f
   SK(cudaMemcpyAsync(pad.data(), s->grad, sizeof(float) * NPAR, cudaMemcpyDeviceToHost, st));
   float l = 0;
   SK(cudaMemcpyAsync(&l, s->loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+  int late = 0;
+  SK(cudaMemcpyAsync(&late, s->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   SK(cudaStreamSynchronize(st));
+  if (late) {
+    SK(cudaMemset(s->err, 0, sizeof(int)));
+    return OSTC_ERR_TIMEOUT;
+  }
   for_each_param([&](long long q, long long off) { grad_host[q] = pad[off]; });
   if (loss_host) *loss_host = l / ((float)n * NOUT);
   return OSTC_OK;
