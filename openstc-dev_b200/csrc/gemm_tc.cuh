@@ -11,8 +11,10 @@
 // waited on (bounded by the global timer) before the stage is refilled two
 // chunks later, so the copies of one chunk overlap the MMAs of the previous
 // one. The epilogue reads the accumulators with tcgen05.ld (warp w: rows
-// 32w..32w+31) and either stores C (+ bias, with the BF16 SiLU activation) or
-// adds it atomically (split-K over blockIdx.y). A wait that runs out sets the
+// 32w..32w+31, 32 columns at a time), turns each 32 x 32 block around in
+// shared memory so that a warp writes one row's 32 columns per instruction,
+// and either stores C (+ bias, with the BF16 SiLU activation) or adds it
+// atomically (split-K over blockIdx.y). A wait that runs out sets the
 // error word; the CTA then waits (bounded) for the MMAs it issued, frees its
 // tensor memory and returns.
 #pragma once
@@ -134,24 +136,36 @@ __global__ void __launch_bounds__(TC_THREADS, 1) gemm_tc_kernel(TcGemmArgs g) {
   if (late) {
     if (tid == 0) atomicExch(g.err, 1);
   } else if (nchunks > 0) {
-    const int row = m0 + warp * 32 + lane;
-    for (int c0 = 0; c0 < g.N; c0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
-      if (row >= g.M) continue;
-      float *crow = g.c + (long long)row * g.ldc + c0;
-      if (g.atomic) {
+    // the stages are free (every MMA has completed): warp w turns its blocks
+    // around in a 32 x 33 float tile of its own
+    float *tile = reinterpret_cast<float *>(sm) + warp * 32 * 33;
+    const int r0 = m0 + warp * 32;
+    for (int c0 = 0; c0 < g.N; c0 += 32) {
+      const int w = min(32, g.N - c0);  // 16 for the last block of N = 16 .. 240 mod 32
+      float v[32];
+      if (w == 32)
+        tmem_ld32(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
+      else
+        tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) atomicAdd(crow + j, v[j]);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          float x = v[j];
-          if (g.bias) x += g.bias[c0 + j];
-          crow[j] = x;
-          if (g.act) g.act[(long long)row * g.ldc + c0 + j] = __float2bfloat16_rn(silu_tc(x));
+      for (int j = 0; j < 32; ++j)
+        if (j < w) tile[lane * 33 + j] = v[j];
+      __syncwarp();
+      if (lane < w) {
+        const float bias = (!g.atomic && g.bias) ? g.bias[c0 + lane] : 0.f;
+        for (int r = 0; r < 32 && r0 + r < g.M; ++r) {
+          const long long o = (long long)(r0 + r) * g.ldc + c0 + lane;
+          const float x = tile[r * 33 + lane];
+          if (g.atomic) {
+            atomicAdd(g.c + o, x);
+          } else {
+            const float y = x + bias;
+            g.c[o] = y;
+            if (g.act) g.act[o] = __float2bfloat16_rn(silu_tc(y));
+          }
         }
       }
+      __syncwarp();
     }
   }
   fence_before();

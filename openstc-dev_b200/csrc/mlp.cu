@@ -241,19 +241,22 @@ __global__ void transpose_bf16_kernel(const __nv_bfloat16 *in, int rows, int col
 }
 
 // db[c] = sum_r dz[r][c] over n rows (one CTA per column block of 32)
+// blockIdx.y takes rows y, y + gridDim.y * 8, ... in 8 streams; the CTA's
+// column sums are added into db (pre-zeroed)
 __global__ void colsum_kernel(const float *dz, int n, int ncol, float *db) {
   const int c = blockIdx.x * 32 + (threadIdx.x & 31);
   const int rs = threadIdx.x >> 5;  // 8 row streams
+  const int step = 8 * gridDim.y;
   float s = 0.f;
   if (c < ncol)
-    for (int r = rs; r < n; r += 8) s += dz[(long long)r * ncol + c];
+    for (int r = blockIdx.y * 8 + rs; r < n; r += step) s += dz[(long long)r * ncol + c];
   __shared__ float red[8][32];
   red[rs][threadIdx.x & 31] = s;
   __syncthreads();
   if (rs == 0 && c < ncol) {
     float t = 0.f;
     for (int q = 0; q < 8; ++q) t += red[q][threadIdx.x & 31];
-    db[c] = t;
+    atomicAdd(db + c, t);
   }
 }
 
@@ -451,7 +454,8 @@ ostc_status backward(ostc_surrogate *s, const float *y, int n, cudaStream_t st) 
     const int mt = (nout[l] + 127) / 128;
     const int splits = std::max(1, std::min(np / 1024, 296 / mt));
     SK(gemm_tc(g, splits, st));
-    colsum_kernel<<<(nout[l] + 31) / 32, 256, 0, st>>>(s->dz[l], n, nout[l], s->grad + offb[l]);
+    colsum_kernel<<<dim3((nout[l] + 31) / 32, std::max(1, std::min(n / 64, 256))), 256, 0, st>>>(
+        s->dz[l], n, nout[l], s->grad + offb[l]);
     SK(cudaGetLastError());
     if (l == 0) break;
     // input gradient dA[b][k] = sum_n dZ[b][n] W[n][k], against W^T [k_in][n_out]
