@@ -2,19 +2,20 @@
 // tensor cores: C[M][N] (+)= A[M][K] B[N][K]^T with BF16 operands stored K-major
 // (row-major, K contiguous), FP32 accumulation in tensor memory.
 //
-// One CTA of 128 threads owns 128 rows of C (all N <= 256 columns) and a
+// One CTA of 256 threads owns 128 rows of C (all N <= 256 columns) and a
 // slice of K. K moves through shared memory in chunks of 64 (two stages):
 // every thread copies its share of the chunk's A and B rows into the
 // canonical no-swizzle K-major layout with 16-byte cp.async (rows of A past M
 // are zero-filled), one thread issues the chunk's MMAs (tcgen05.mma kind::f16,
 // M = 128, N, K = 16 each) and commits them to the stage's mbarrier, which is
-// waited on (bounded by the global timer) before the stage is refilled two
-// chunks later, so the copies of one chunk overlap the MMAs of the previous
-// one. The epilogue reads the accumulators with tcgen05.ld (warp w: rows
-// 32w..32w+31, 32 columns at a time), turns each 32 x 32 block around in
-// shared memory so that a warp writes one row's 32 columns per instruction,
-// and either stores C (+ bias, with the BF16 SiLU activation) or adds it
-// atomically (split-K over blockIdx.y). A wait that runs out sets the
+// waited on (bounded by the global timer) before the stage is refilled. The
+// copies of chunk c + 1 are issued before chunk c's are waited for, so they
+// overlap that wait and chunk c's MMAs. The epilogue reads the accumulators
+// with tcgen05.ld (warp w: rows 32 (w % 4) .. + 31, half w / 4 of the
+// columns, 32 at a time), turns each 32 x 32 block around in shared memory so
+// that a warp writes one row's 32 columns per instruction, and either stores
+// C (+ bias, with the BF16 SiLU activation) or adds it atomically (split-K
+// over blockIdx.y). A wait that runs out sets the
 // error word; the CTA then waits (bounded) for the MMAs it issued, frees its
 // tensor memory and returns.
 #pragma once
@@ -41,7 +42,7 @@ struct TcGemmArgs {
 };
 
 constexpr int TC_BK = 64;                               // K of one chunk
-constexpr int TC_THREADS = 128;
+constexpr int TC_THREADS = 256;
 constexpr unsigned TC_A_BYTES = 128 * TC_BK * 2;        // 16 KB
 constexpr unsigned TC_B_BYTES = 256 * TC_BK * 2;        // 32 KB (N <= 256)
 constexpr unsigned TC_STAGE = TC_A_BYTES + TC_B_BYTES;  // 48 KB
@@ -83,18 +84,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) gemm_tc_kernel(TcGemmArgs g) {
   unsigned phase[2] = {0u, 0u};
   bool pending[2] = {false, false};
   bool late = false;
-  for (int c = 0; c < nchunks; ++c) {
+  // copies of chunk c into stage c & 1 (one cp.async group per chunk)
+  auto load = [&](int c) {
     const int s = c & 1;
     const int k0 = kb + c * TC_BK, kc = min(TC_BK, ke - k0);
-    if (pending[s]) {  // the MMAs of chunk c - 2 read this stage
-      if (bar_wait(bar[s], phase[s])) {
-        phase[s] ^= 1u;
-        pending[s] = false;
-      } else {
-        late = true;
-      }
-      if (__syncthreads_or(late)) break;
-    }
     const unsigned sa = base + s * TC_STAGE, sb = sa + TC_A_BYTES;
     const int q = kc / 8;  // 16-byte pieces per row
     for (int i = tid; i < 128 * q; i += TC_THREADS) {
@@ -108,11 +101,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1) gemm_tc_kernel(TcGemmArgs g) {
       cp_async16(sb + core_off(n, kq * 8, TC_BK), g.b + (long long)n * g.ldb + k0 + kq * 8);
     }
     cp_async_commit();
-    cp_async_wait_all();
+  };
+  if (nchunks > 0) load(0);
+  for (int c = 0; c < nchunks; ++c) {
+    const int s = c & 1, s1 = s ^ 1;
+    // the next chunk's copies go out before this chunk's are waited for; its
+    // stage is free once the MMAs of chunk c - 1 that read it have completed
+    if (c + 1 < nchunks) {
+      if (pending[s1]) {
+        if (bar_wait(bar[s1], phase[s1])) {
+          phase[s1] ^= 1u;
+          pending[s1] = false;
+        } else {
+          late = true;
+        }
+        if (__syncthreads_or(late)) break;
+      }
+      load(c + 1);
+      cp_async_wait_prior1();  // chunk c's group has landed
+    } else {
+      cp_async_wait_all();
+    }
     fence_async_smem();  // the copies (generic proxy) before the MMAs' reads (async proxy)
     __syncthreads();
     if (tid == 0) {
       fence_after();
+      const int kc = min(TC_BK, ke - (kb + c * TC_BK));
+      const unsigned sa = base + s * TC_STAGE, sb = sa + TC_A_BYTES;
       for (int ks = 0; ks < kc / 16; ++ks) {
         // K-adjacent core matrices 128 B apart, 8-row groups TC_BK / 8 * 128 B apart
         const unsigned long long ad = smem_desc(sa + ks * 256, 128, (TC_BK / 8) * 128);
@@ -123,6 +138,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) gemm_tc_kernel(TcGemmArgs g) {
     }
     pending[s] = true;
   }
+  cp_async_wait_all();  // no copy outlives the loop (a timed-out CTA leaves it early)
   // the MMAs still in flight (bounded again after a timeout)
   for (int s = 0; s < 2; ++s)
     if (pending[s]) {
@@ -138,15 +154,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) gemm_tc_kernel(TcGemmArgs g) {
   } else if (nchunks > 0) {
     // the stages are free (every MMA has completed): warp w turns its blocks
     // around in a 32 x 33 float tile of its own
+    // (warps w and w + 4 read the same 32 accumulator lanes, each half of the columns)
     float *tile = reinterpret_cast<float *>(sm) + warp * 32 * 33;
-    const int r0 = m0 + warp * 32;
-    for (int c0 = 0; c0 < g.N; c0 += 32) {
-      const int w = min(32, g.N - c0);  // 16 for the last block of N = 16 .. 240 mod 32
+    const int quarter = warp & 3, half = warp >> 2;
+    const int r0 = m0 + quarter * 32;
+    const int cb = g.N <= 32 ? (half ? g.N : 0) : half * ((g.N / 2 + 31) / 32 * 32);
+    const int ce = g.N <= 32 ? (half ? g.N : g.N) : min(g.N, cb + (g.N / 2 + 31) / 32 * 32);
+    for (int c0 = cb; c0 < ce; c0 += 32) {
+      const int w = min(32, g.N - c0);  // 16 for a last block of 16 columns
       float v[32];
       if (w == 32)
-        tmem_ld32(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
+        tmem_ld32(tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)c0, v);
       else
-        tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0, v);
+        tmem_ld16(tmem + ((unsigned)(quarter * 32) << 16) + (unsigned)c0, v);
 #pragma unroll
       for (int j = 0; j < 32; ++j)
         if (j < w) tile[lane * 33 + j] = v[j];
