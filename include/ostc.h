@@ -575,6 +575,18 @@ ostc_status ostc_metric_from_grid(int mx, int my, int mz, int ngg,
 ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks);
 ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks);
 
+/* The flux autotuner (no reference counterpart: the reference launches fixed
+ * block shapes, InviscidScheme.cu / ViscousScheme.cuh). For each direction it
+ * times, with CUDA events on `stream` (warmup + reps launches each), every
+ * tile of rows {2,4,8} (x) or {4,8} (y, z) x chunks 1, 2, 4, .. up to the
+ * first block's extent x register budgets 1..5, and the staged kernels (8
+ * rows; not for AWENO); for a viscous flow also the separate inviscid and
+ * viscous kernels, each tuned on its own, which replace the fused kernel when
+ * their sum is faster. Sets the winners (ostc_set_tile) and, if ms_out is not
+ * null, writes the chosen device ms per launch of each direction (3 floats).
+ * Only dq is written, so the flow state is left as it was. Synchronises.    */
+ostc_status ostc_autotune(ostc_ctx *ctx, int warmup, int reps, void *stream, float *ms_out);
+
 /* Batched multi-block launches. on = 1: every block of the context is
  * processed by one persistent launch per kernel (flux of each direction,
  * source, stage update, properties, time step, conservative variables): the

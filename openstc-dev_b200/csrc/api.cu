@@ -1603,6 +1603,99 @@ ostc_status ostc_get_batching(const ostc_ctx *ctx, int *on) {
   return OSTC_OK;
 }
 
+// the flux autotuner: device ms of one launch of flux op `arg` (0..8, as
+// ostc_launch_op) at the current tiles, or a negative value when this tile
+// setting cannot run for the scheme (a staged kernel for AWENO, a tile past a
+// CTA's shared memory); CUDA events on the stream, after `warmup` launches
+static float time_flux(ostc_ctx *ctx, int arg, int warmup, int reps, cudaStream_t s) {
+  if (ostc_launch_op(ctx, OSTC_OP_FLUX, arg, s) != OSTC_OK) {
+    cudaGetLastError();
+    return -1.f;
+  }
+  for (int i = 0; i < warmup; ++i)
+    if (ostc_launch_op(ctx, OSTC_OP_FLUX, arg, s) != OSTC_OK) return -1.f;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return -1.f;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return -1.f;
+  }
+  float ms = -1.f;
+  bool ok = cudaEventRecord(e0, s) == cudaSuccess;
+  for (int i = 0; ok && i < reps; ++i) ok = ostc_launch_op(ctx, OSTC_OP_FLUX, arg, s) == OSTC_OK;
+  if (ok && cudaEventRecord(e1, s) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+      cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+    ms /= reps;
+  else
+    ms = -1.f;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms;
+}
+
+ostc_status ostc_autotune(ostc_ctx *ctx, int warmup, int reps, void *stream, float *ms_out) {
+  if (!ctx || warmup < 0 || reps < 1) return OSTC_ERR_INVALID_ARG;
+  cudaStream_t s = S(stream);
+  if (ensure_param(ctx, s)) return ctx->last;
+  const DevZone &z0 = ctx->dz[0];
+  const int ext[3] = {z0.mx, z0.my, z0.mz};
+  const bool viscous = ctx->prm.viscous_scheme != 0;
+  const bool staged_ok = ctx->prm.reconstruction != 4;  // AWENO has no staged build
+  struct Cand {
+    int rows, chunks;
+  };
+  for (int d = 0; d < 3; ++d) {
+    // tile candidates: rows x chunks (doubling up to the direction's extent)
+    // x register budgets, and the staged kernels (8 rows, 128 registers)
+    auto cands = [&](int min_budget) {
+      std::vector<Cand> out;
+      const int rows_list[3] = {2, 4, 8};
+      for (int ri = d == 0 ? 0 : 1; ri < 3; ++ri) {
+        const int R = rows_list[ri], span = d == 0 ? 32 : R;
+        const int cmax = std::min(64, std::max(1, (ext[d] + 1 + span - 1) / span));
+        for (int c = 1;; c *= 2) {
+          const int cc = std::min(c, cmax);
+          for (int b = min_budget; b <= 5; ++b) {
+            if (b >= 4 && R > 4) continue;
+            out.push_back({R | (b > 1 ? b << 8 : 0), cc});
+          }
+          if (staged_ok && R == 8) out.push_back({R | (2 << 8) | (1 << 16), cc});
+          if (c >= cmax) break;
+        }
+      }
+      return out;
+    };
+    if (ostc_set_tile(ctx, d + 3, 0, 0) != OSTC_OK) return ctx->last;
+    float best = -1.f;
+    Cand bf{}, bi{}, bv{};
+    for (const Cand &c : cands(1)) {
+      if (ostc_set_tile(ctx, d, c.rows, c.chunks) != OSTC_OK) continue;
+      const float t = time_flux(ctx, d, warmup, reps, s);
+      if (t >= 0 && (best < 0 || t < best)) best = t, bf = c;
+    }
+    if (best < 0) return fail(ctx, OSTC_ERR_CUDA);
+    bool split = false;
+    if (viscous) {
+      // the separate inviscid and viscous kernels, each tuned on its own
+      float ti = -1.f, tv = -1.f;
+      for (const Cand &c : cands(2)) {
+        if (ostc_set_tile(ctx, d, c.rows, c.chunks) != OSTC_OK) continue;
+        const float a = time_flux(ctx, d + 3, warmup, reps, s);
+        if (a >= 0 && (ti < 0 || a < ti)) ti = a, bi = c;
+        if (ostc_set_tile(ctx, d + 3, c.rows, c.chunks) != OSTC_OK) continue;
+        const float b = time_flux(ctx, d + 6, warmup, reps, s);
+        if (b >= 0 && (tv < 0 || b < tv)) tv = b, bv = c;
+      }
+      if (ti >= 0 && tv >= 0 && ti + tv < best) best = ti + tv, split = true;
+    }
+    ostc_status st = split ? ostc_set_tile(ctx, d, bi.rows, bi.chunks) : ostc_set_tile(ctx, d, bf.rows, bf.chunks);
+    if (st == OSTC_OK) st = split ? ostc_set_tile(ctx, d + 3, bv.rows, bv.chunks) : ostc_set_tile(ctx, d + 3, 0, 0);
+    if (st != OSTC_OK) return st;
+    if (ms_out) ms_out[d] = best;
+  }
+  return OSTC_OK;
+}
+
 ostc_status ostc_get_tile(const ostc_ctx *ctx, int dir, int *rows, int *chunks) {
   if (!ctx || dir < 0 || dir > 5 || !rows || !chunks) return OSTC_ERR_INVALID_ARG;
   const TileShape &t = ctx->tile[dir % 3];

@@ -136,6 +136,7 @@ def lib():
             "ostc_set_batching": [vp, i],
             "ostc_get_batching": [vp, C.POINTER(i)],
             "ostc_launch_op": [vp, i, i, vp],
+            "ostc_autotune": [vp, i, i, vp, C.POINTER(C.c_float)],
             "ostc_set_interfaces": [vp, C.POINTER(IfaceC), i],
             "ostc_step_kernel_count": [vp, i, C.POINTER(i)],
             "ostc_local_time_step": [vp, vp],
@@ -764,68 +765,18 @@ class Solver:
         return e0.elapsed_time(e1) / reps
 
     def autotune(self, warmup: int = 1, reps: int = 3, verbose: bool = False):
-        """Pick per-direction flux tile shapes (rows, chunks, register budget)
-        by timing each flux kernel with CUDA events on the launching stream.
-        For a viscous flow the fused kernel competes with the pair of
-        separate inviscid and viscous kernels, each tuned on its own. Only
-        dq is written, so the state is left as it was."""
-        blk = self.blocks[0]
-        ext = (blk.mx, blk.my, blk.mz)
-        viscous = self.scheme.viscous_order != 0
-        # the staged kernels (shared-memory tiles, 8 rows, 128 registers)
-        # compete with the plane kernels of every register budget; AWENO has
-        # no staged build
-        staged = (0,) if self.scheme.reconstruction == 4 else (0, 1)
-        best = {}
-        for d in range(3):
-            n = ext[d]
-
-            def cands(budgets):
-                out = []
-                for R in ((2, 4, 8) if d == 0 else (4, 8)):
-                    span = 32 if d == 0 else R
-                    cmax = min(64, max(1, (n + 1 + span - 1) // span))
-                    c = 1
-                    while True:
-                        for minb in budgets:
-                            if minb >= 4 and R > 4:
-                                continue
-                            out.append((R | (minb << 8 if minb > 1 else 0), min(c, cmax)))
-                        for nb in (staged[1:] if R == 8 else ()):
-                            out.append((R | (2 << 8) | (nb << 16), min(c, cmax)))
-                        if c >= cmax:
-                            break
-                        c *= 2
-                return sorted(set(out))
-
-            def timed(arg, R, Cc, sets):
-                for q in sets:
-                    self.set_tile(q, R, Cc)
-                t = self._time_flux(arg, warmup, reps)
-                return None if t is None else (t, R, Cc)
-
-            self.set_tile(d + 3, 0, 0)
-            fused = [x for x in (timed(d, R, Cc, (d,)) for R, Cc in cands((1, 2, 3, 4, 5))) if x]
-            fused.sort()
-            choice = (fused[0][0], fused[0][1:], (0, 0))
-            if viscous:
-                inv, vis = [], []
-                for R, Cc in cands((2, 3, 4, 5)):
-                    x = timed(d + 3, R, Cc, (d,))
-                    if x:
-                        inv.append(x)
-                    x = timed(d + 6, R, Cc, (d + 3,))
-                    if x:
-                        vis.append(x)
-                inv.sort()
-                vis.sort()
-                if inv and vis and inv[0][0] + vis[0][0] < choice[0]:
-                    choice = (inv[0][0] + vis[0][0], inv[0][1:], vis[0][1:])
-            self.set_tile(d, *choice[1])
-            self.set_tile(d + 3, *choice[2])
-            best[d] = (choice[0], choice[1], choice[2])
-            if verbose:
-                print("dir", d, "fused", fused[0], "chosen", best[d])
+        """Pick per-direction flux tile shapes (rows, chunks, register budget,
+        staged or not) with the library's autotuner (ostc_autotune), which
+        times each flux kernel with CUDA events on the launching stream; for a
+        viscous flow the fused kernel competes with the pair of separate
+        inviscid and viscous kernels. Only dq is written, so the state is left
+        as it was. Returns {direction: (ms, tile, viscous tile)}."""
+        ms = (C.c_float * 3)()
+        check(lib().ostc_autotune(self.ctx, warmup, reps, self._s(), ms), "ostc_autotune")
+        best = {d: (float(ms[d]), self.get_tile(d), self.get_tile(d + 3)) for d in range(3)}
+        if verbose:
+            for d in range(3):
+                print("dir", d, "chosen", best[d])
         return best
 
 
