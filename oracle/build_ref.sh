@@ -18,7 +18,8 @@ OBJ="$OUT/obj"
 LIB="$OUT/libostc_ref_cuda.so"
 if [ ! -d "$SRC" ]; then echo "reference sources not found at $SRC; skipping"; exit 0; fi
 if [ -f "$LIB" ] && [ "$LIB" -nt "$HERE/ref_cuda_harness.cu" ] && [ "$LIB" -nt "$HERE/build_ref.sh" ] \
-   && [ "$LIB" -nt "$HERE/ref_shim/mpi.h" ]; then exit 0; fi
+   && [ "$LIB" -nt "$HERE/ref_shim/mpi.h" ] && [ "$LIB" -nt "$HERE/../include/ostc_reference_shim.h" ] \
+   && [ "$LIB" -nt "$HERE/../include/ostc.h" ]; then exit 0; fi
 mkdir -p "$OBJ"
 NVCC="${NVCC:-nvcc}"
 FLAGS=(-gencode arch=compute_100a,code=sm_100a -rdc=true -std=c++20 -O3 -Xcompiler -fPIC

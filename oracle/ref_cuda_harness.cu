@@ -41,6 +41,7 @@
 #include "SchemeSelector.cuh"
 #include "SourceTerm.cuh"
 #include "../include/ostc.h"
+#include "../include/ostc_reference_shim.h"
 
 using namespace cfd;
 
@@ -765,6 +766,16 @@ int ref_download_block(void *h, int b, const char *name, double *dst) {
 }
 
 int ref_download(void *h, const char *name, double *dst) { return ref_download_block(h, 0, name, dst); }
+
+// block b's device arrays as an ostc_zone, through the maintainer's shim
+// (include/ostc_reference_shim.h) compiled against the reference's Field.h
+int ref_zone_view(void *h, int b, ostc_zone *out) {
+  auto *m = (RefMulti *)h;
+  if (!out || b < 0 || b >= (int)m->blk.size()) return 1;
+  RefCtx *c = m->blk[b];
+  *out = ostc_from_reference::to_ostc(c->h, c->cfg.steady && c->cfg.implicit_method == 1 ? 1 : 0);
+  return 0;
+}
 
 // Block::compute_jac_metric (Mesh.cpp:259-521), the reference's own host code,
 // on caller coordinates with ngg+1 ghost layers (x, y, z in the ghosted

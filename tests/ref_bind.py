@@ -44,6 +44,8 @@ def ref():
         L.ref_time_steps.restype = C.c_double
         L.ref_download.argtypes = [vp, C.c_char_p, d]
         L.ref_download.restype = C.c_int
+        L.ref_zone_view.argtypes = [vp, C.c_int, C.POINTER(ostc.Zone)]
+        L.ref_zone_view.restype = C.c_int
         L.ref_metric.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, d, d, d, d, vp]
         L.ref_metric.restype = C.c_int
         ip = C.POINTER(C.c_int)
@@ -101,6 +103,13 @@ class RefCudaRun:
 
     def time_steps(self, n):
         return ref().ref_time_steps(self.h, n)
+
+    def zone_view(self, block=0):
+        """block's device arrays in the reference build as an ostc_zone
+        (include/ostc_reference_shim.h): this library can run on them"""
+        z = ostc.Zone()
+        assert ref().ref_zone_view(self.h, block, C.byref(z)) == 0
+        return z
 
     def download(self, name, block=0):
         b = self.blocks[block]
