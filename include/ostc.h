@@ -594,9 +594,11 @@ ostc_status ostc_autotune(ostc_ctx *ctx, int warmup, int reps, void *stream, flo
  * of {block, tile} entries built from the blocks' extents and the flux tile
  * shapes. Results are identical to the per-block launches (on = 0): every
  * cell sees the same operations in the same order. Default: on for 2 to 64
- * blocks, off for one. Boundary
- * faces and interfaces keep their per-face launches (their order matters,
- * DataCommunication.cuh:30-49, BoundCond.cuh:673-822). At most 64 blocks:
+ * blocks, off for one. Boundary faces go in one launch per wave of each
+ * priority level (BoundCond.cuh:673-822; faces of a level and block whose
+ * footprints meet keep their order, in separate waves); periodic faces and
+ * interfaces keep their per-face launches (the interfaces' order matters,
+ * DataCommunication.cuh:30-49). At most 64 blocks:
  * OSTC_ERR_UNSUPPORTED beyond. No reference counterpart: the reference
  * launches every kernel per block (RK.cuh:107-161).                       */
 ostc_status ostc_set_batching(ostc_ctx *ctx, int on);

@@ -45,6 +45,11 @@ struct ostc_ctx {
   int batched = 0;
   int4 *tab_dev = nullptr;
   size_t tab_cap = 0;
+  // batched boundary conditions: the face records on the device and, in
+  // launch order, the waves of each priority level (type, tiles)
+  BcFace *faces_dev = nullptr;
+  std::vector<CellTable> bc_waves;
+  std::vector<int> bc_wave_type;
   CellTable cell_tab[3];
   FluxTable flux_tab[3][2];
   unsigned long long *dt_bits = nullptr;  // device dt (as bits)
@@ -152,6 +157,70 @@ ostc_status build_tables(ostc_ctx *ctx) {
       spans.push_back({b0, all.size()});
       flux_bulk_tiles.push_back(nb);
     }
+  // boundary faces by priority level (BoundCond.cuh:673-822; periodic faces
+  // keep their own launches), each level split into waves: a face goes one
+  // wave after the last earlier face of its level and zone that writes a
+  // cell it reads or writes, or reads a cell it writes, so every such pair
+  // keeps the per-face order and the faces of a wave touch disjoint cells.
+  // Footprints along the normal: writes from the boundary layer (types that
+  // set it) or the first ghost layer out to ngg ghosts; reads from the
+  // boundary layer ngg layers inward; tangentially the face's ranges.
+  std::vector<std::pair<size_t, size_t>> bc_spans;
+  std::vector<int> bc_types;
+  {
+    struct Box {
+      int lo[3], hi[3];
+    };
+    auto boxes = [&](const BcFace &b, Box &W, Box &R) {
+      const int f = b.face, d = b.direction, g = ctx->dz[b.zone].ngg, bi = b.rs[f];
+      for (int a = 0; a < 3; ++a) W.lo[a] = R.lo[a] = b.rs[a], W.hi[a] = R.hi[a] = b.re[a];
+      const bool sets_boundary = b.type == OSTC_BC_INFLOW || b.type == OSTC_BC_SYMMETRY || b.type == OSTC_BC_WALL ||
+                                 b.type == OSTC_BC_FARFIELD;
+      const int wa = sets_boundary ? bi : bi + d, wb = bi + d * g, ra = bi, rb = bi - d * g;
+      W.lo[f] = std::min(wa, wb), W.hi[f] = std::max(wa, wb);
+      R.lo[f] = std::min(ra, rb), R.hi[f] = std::max(ra, rb);
+    };
+    auto meet = [](const Box &x, const Box &y) {
+      for (int a = 0; a < 3; ++a)
+        if (x.hi[a] < y.lo[a] || y.hi[a] < x.lo[a]) return false;
+      return true;
+    };
+    static const int order[] = {OSTC_BC_FARFIELD,        OSTC_BC_OUTFLOW,  OSTC_BC_BACK_PRESSURE, OSTC_BC_INFLOW,
+                                OSTC_BC_SUBSONIC_INFLOW, OSTC_BC_SYMMETRY, OSTC_BC_WALL};
+    for (int t : order) {
+      std::vector<int> qs, wave;
+      std::vector<Box> W, R;
+      for (size_t q = 0; q < ctx->faces.size(); ++q) {
+        if (ctx->faces[q].type != t) continue;
+        Box w, r;
+        boxes(ctx->faces[q], w, r);
+        int wv = 0;
+        for (size_t p = 0; p < qs.size(); ++p) {
+          if (ctx->faces[qs[p]].zone != ctx->faces[q].zone) continue;
+          if (meet(w, W[p]) || meet(w, R[p]) || meet(W[p], r)) wv = std::max(wv, wave[p] + 1);
+        }
+        qs.push_back((int)q), wave.push_back(wv), W.push_back(w), R.push_back(r);
+      }
+      const int n_waves = qs.empty() ? 0 : *std::max_element(wave.begin(), wave.end()) + 1;
+      for (int wv = 0; wv < n_waves; ++wv) {
+        const size_t b0 = all.size();
+        for (size_t p = 0; p < qs.size(); ++p) {
+          if (wave[p] != wv) continue;
+          const BcFace &b = ctx->faces[qs[p]];
+          const int n0 = b.re[0] - b.rs[0] + 1, n1 = b.re[1] - b.rs[1] + 1, n2 = b.re[2] - b.rs[2] + 1;
+          for (int bz = 0; bz < n2; ++bz)
+            for (int by = 0; by < (n1 + 7) / 8; ++by)
+              for (int bx = 0; bx < (n0 + 31) / 32; ++bx) all.push_back(make_int4(qs[p], bx, by, bz));
+        }
+        bc_spans.push_back({b0, all.size()});
+        bc_types.push_back(t);
+      }
+    }
+  }
+  if (!ctx->faces.empty() && !ctx->faces_dev) {
+    CK(cudaMalloc(&ctx->faces_dev, sizeof(BcFace) * ctx->faces.size()));
+    CK(cudaMemcpy(ctx->faces_dev, ctx->faces.data(), sizeof(BcFace) * ctx->faces.size(), cudaMemcpyHostToDevice));
+  }
   if (all.size() > (size_t)INT32_MAX) return fail(ctx, OSTC_ERR_UNSUPPORTED);
   if (all.size() > ctx->tab_cap) {
     cudaFree(ctx->tab_dev);
@@ -173,6 +242,14 @@ ostc_status build_tables(ostc_ctx *ctx) {
       ctx->flux_tab[d][v] = table(3 + 2 * d + v);
       ctx->flux_tab[d][v].n_bulk = (int)flux_bulk_tiles[2 * d + v];
     }
+  ctx->bc_waves.clear();
+  for (const auto &sp : bc_spans) {
+    CellTable t;
+    t.tiles = ctx->tab_dev + sp.first;
+    t.n = (int)(sp.second - sp.first);
+    ctx->bc_waves.push_back(t);
+  }
+  ctx->bc_wave_type = bc_types;
   return OSTC_OK;
 }
 
@@ -607,6 +684,7 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
     b.mw = f.mw;
     b.total_pressure = f.total_pressure;
     b.total_temperature = f.total_temperature;
+    b.zone = f.block;
     c->faces.push_back(b);
     c->face_zone.push_back(f.block);
   }
@@ -693,6 +771,7 @@ ostc_status ostc_destroy(ostc_ctx *ctx) {
   for (void *p : ctx->owned) cudaFree(p);
   cudaFree(ctx->dt_bits);
   cudaFree(ctx->tab_dev);
+  cudaFree(ctx->faces_dev);
   cudaFree(ctx->res_partial);
   cudaFree(ctx->hist_counter);
   cudaFree(ctx->bad_key);
@@ -795,6 +874,20 @@ ostc_status ostc_apply_boundary_conditions(ostc_ctx *ctx, int with_cv, void *str
   // priority order of BoundCond.cuh:673-822; periodic wraps after all others
   static const int order[] = {OSTC_BC_FARFIELD, OSTC_BC_OUTFLOW, OSTC_BC_BACK_PRESSURE, OSTC_BC_INFLOW,
                               OSTC_BC_SUBSONIC_INFLOW, OSTC_BC_SYMMETRY, OSTC_BC_WALL, OSTC_BC_PERIODIC};
+  if (ctx->batched) {
+    // every priority level's waves in one launch each over all zones
+    // (tables of build_tables, same order), then the periodic faces
+    for (size_t w = 0; w < ctx->bc_waves.size(); ++w)
+      CK(dispatch_ns(ctx->ns, [&](auto n) {
+        return launch_bc_table<decltype(n)::value>(ctx->faces_dev, ctx->bc_waves[w], with_cv, S(stream));
+      }));
+    for (size_t q = 0; q < ctx->faces.size(); ++q) {
+      if (ctx->faces[q].type != OSTC_BC_PERIODIC) continue;
+      const DevZone &z = ctx->dz[ctx->face_zone[q]];
+      CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_bc<decltype(n)::value>(z, ctx->faces[q], with_cv, S(stream)); }));
+    }
+    return OSTC_OK;
+  }
   for (int t : order) {
     for (size_t q = 0; q < ctx->faces.size(); ++q) {
       if (ctx->faces[q].type != t) continue;

@@ -432,11 +432,7 @@ static __global__ void dt_reset_kernel(unsigned long long *dt_bits) {
 // boundary conditions. One thread per boundary point of the face range.
 // ---------------------------------------------------------------------------
 template <int NS>
-__global__ void bc_outflow_kernel(DevZone z, BcFace b, int with_cv) {  // BoundCond.cuh:120-150
-  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = b.rs[2] + blockIdx.z;
-  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+__device__ __forceinline__ void bc_outflow_point(const DevZone &z, const BcFace &b, int with_cv, int i, int j, int k) {  // BoundCond.cuh:120-150
   const int g = gidx(z, i, j, k);
   const int step = b.dir_stride;
   for (int gg = 1; gg <= z.ngg; ++gg) {
@@ -449,11 +445,7 @@ __global__ void bc_outflow_kernel(DevZone z, BcFace b, int with_cv) {  // BoundC
 }
 
 template <int NS>
-__global__ void bc_inflow_kernel(DevZone z, BcFace b, int with_cv) {  // BoundCond.cuh:152-210
-  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = b.rs[2] + blockIdx.z;
-  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+__device__ __forceinline__ void bc_inflow_point(const DevZone &z, const BcFace &b, int with_cv, int i, int j, int k) {  // BoundCond.cuh:152-210
   const int g = gidx(z, i, j, k);
   const int step = b.dir_stride;
   for (int gg = 0; gg <= z.ngg; ++gg) {
@@ -474,11 +466,7 @@ __global__ void bc_inflow_kernel(DevZone z, BcFace b, int with_cv) {  // BoundCo
   }
 }
 
-static __global__ void bc_symmetry_kernel(DevZone z, BcFace b) {  // BoundCond.cuh:52-118
-  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = b.rs[2] + blockIdx.z;
-  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+static __device__ __forceinline__ void bc_symmetry_point(const DevZone &z, const BcFace &b, int, int i, int j, int k) {  // BoundCond.cuh:52-118
   const int g = gidx(z, i, j, k);
   const int step = b.dir_stride;
   const int gin = g - step;
@@ -518,11 +506,7 @@ static __global__ void bc_symmetry_kernel(DevZone z, BcFace b) {  // BoundCond.c
 
 // periodic wrap (no reference counterpart): ghost layer gg of this face takes
 // the point n cells back along the face normal
-static __global__ void bc_periodic_kernel(DevZone z, BcFace b, int with_cv) {
-  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = b.rs[2] + blockIdx.z;
-  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+static __device__ __forceinline__ void bc_periodic_point(const DevZone &z, const BcFace &b, int with_cv, int i, int j, int k) {
   const int g = gidx(z, i, j, k);
   for (int gg = 1; gg <= z.ngg; ++gg) {
     const int go = g + gg * b.dir_stride;
@@ -540,11 +524,7 @@ static __global__ void bc_periodic_kernel(DevZone z, BcFace b, int with_cv) {
 // on the wall and in the ghosts, omega = 60 mu_w / (rho_w beta_1 d^2) from the
 // wall distance d of the first interior point, mut = 0 in the ghosts
 template <int NS>
-__global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
-  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = b.rs[2] + blockIdx.z;
-  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+__device__ __forceinline__ void bc_wall_point(const DevZone &z, const BcFace &b, int with_cv, int i, int j, int k) {
   const int g = gidx(z, i, j, k);
   const int step = b.dir_stride;
   const int gin = g - step;
@@ -622,11 +602,7 @@ __global__ void bc_wall_kernel(DevZone z, BcFace b, int with_cv) {
 // never recomputes cv. The mixture's gamma iteration, unbounded in the
 // reference, stops after 100 sweeps here.
 template <int NS>
-__global__ void bc_farfield_kernel(DevZone z, BcFace b) {
-  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = b.rs[2] + blockIdx.z;
-  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+__device__ __forceinline__ void bc_farfield_point(const DevZone &z, const BcFace &b, int, int i, int j, int k) {
   const int g = gidx(z, i, j, k);
   const int step = b.dir_stride;
   double nx = z.met[(3 * b.face) * z.sz + g], ny = z.met[(3 * b.face + 1) * z.sz + g];
@@ -737,11 +713,7 @@ __global__ void bc_farfield_kernel(DevZone z, BcFace b) {
 
 // back pressure: extrapolate all but p (BoundCond.cuh:636-671)
 template <int NS>
-__global__ void bc_back_pressure_kernel(DevZone z, BcFace b, int with_cv) {
-  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = b.rs[2] + blockIdx.z;
-  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+__device__ __forceinline__ void bc_back_pressure_point(const DevZone &z, const BcFace &b, int with_cv, int i, int j, int k) {
   const int g = gidx(z, i, j, k);
   for (int gg = 1; gg <= z.ngg; ++gg) {
     const int go = g + gg * b.dir_stride;
@@ -755,11 +727,7 @@ __global__ void bc_back_pressure_kernel(DevZone z, BcFace b, int with_cv) {
 }
 
 // subsonic inflow from total conditions, air (BoundCond.cuh:528-634)
-static __global__ void bc_subsonic_inflow_kernel(DevZone z, BcFace b, int with_cv) {
-  const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = b.rs[2] + blockIdx.z;
-  if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;
+static __device__ __forceinline__ void bc_subsonic_inflow_point(const DevZone &z, const BcFace &b, int with_cv, int i, int j, int k) {
   const int g = gidx(z, i, j, k);
   double nx = z.met[(3 * b.face) * z.sz + g], ny = z.met[(3 * b.face + 1) * z.sz + g];
   double nz = z.met[(3 * b.face + 2) * z.sz + g];
@@ -799,6 +767,56 @@ static __global__ void bc_subsonic_inflow_kernel(DevZone z, BcFace b, int with_c
     for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + go] = u_bar > 0 ? z.sv[l * z.sz + g] : b.sv[l];
     if (c_p.sst) z.mut[go] = z.mut[g];
     if (with_cv) cv_from_bv_point<0>(z, go);
+  }
+}
+
+// per-face kernels: the launch of one face's points (launch_bc)
+#define OSTC_BC_KERNEL(name, point)                                      \
+  __global__ void name(DevZone z, BcFace b, int with_cv) {               \
+    const int i = b.rs[0] + blockIdx.x * blockDim.x + threadIdx.x;       \
+    const int j = b.rs[1] + blockIdx.y * blockDim.y + threadIdx.y;       \
+    const int k = b.rs[2] + blockIdx.z;                                  \
+    if (i > b.re[0] || j > b.re[1] || k > b.re[2]) return;               \
+    point(z, b, with_cv, i, j, k);                                       \
+  }
+template <int NS>
+OSTC_BC_KERNEL(bc_outflow_kernel, bc_outflow_point<NS>)
+template <int NS>
+OSTC_BC_KERNEL(bc_inflow_kernel, bc_inflow_point<NS>)
+static OSTC_BC_KERNEL(bc_symmetry_kernel, bc_symmetry_point)
+static OSTC_BC_KERNEL(bc_periodic_kernel, bc_periodic_point)
+template <int NS>
+OSTC_BC_KERNEL(bc_wall_kernel, bc_wall_point<NS>)
+template <int NS>
+OSTC_BC_KERNEL(bc_farfield_kernel, bc_farfield_point<NS>)
+template <int NS>
+OSTC_BC_KERNEL(bc_back_pressure_kernel, bc_back_pressure_point<NS>)
+static OSTC_BC_KERNEL(bc_subsonic_inflow_kernel, bc_subsonic_inflow_point)
+#undef OSTC_BC_KERNEL
+
+// the faces of one wave of a priority level over every zone in one launch:
+// a persistent grid walks tiles {face, bx, by, bz} of 32 x 8 points of the
+// faces' ranges (faces in device memory, zones in c_zones); the faces of a
+// wave write no cell that another face of the wave reads or writes
+template <int NS>
+__global__ void __launch_bounds__(256) bc_table_kernel(const BcFace *faces, const int4 *tiles, int n_tiles,
+                                                       int with_cv) {
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const int4 c = tiles[t];
+    const BcFace &b = faces[c.x];
+    const int i = b.rs[0] + c.y * 32 + threadIdx.x, j = b.rs[1] + c.z * 8 + threadIdx.y, k = b.rs[2] + c.w;
+    if (i > b.re[0] || j > b.re[1] || k > b.re[2]) continue;
+    const DevZone &z = c_zones[b.zone];
+    switch (b.type) {
+      case OSTC_BC_OUTFLOW: bc_outflow_point<NS>(z, b, with_cv, i, j, k); break;
+      case OSTC_BC_INFLOW: bc_inflow_point<NS>(z, b, with_cv, i, j, k); break;
+      case OSTC_BC_SYMMETRY: bc_symmetry_point(z, b, with_cv, i, j, k); break;
+      case OSTC_BC_WALL: bc_wall_point<NS>(z, b, with_cv, i, j, k); break;
+      case OSTC_BC_FARFIELD: bc_farfield_point<NS>(z, b, with_cv, i, j, k); break;
+      case OSTC_BC_BACK_PRESSURE: bc_back_pressure_point<NS>(z, b, with_cv, i, j, k); break;
+      case OSTC_BC_SUBSONIC_INFLOW: bc_subsonic_inflow_point(z, b, with_cv, i, j, k); break;
+      default: break;  // periodic faces are launched one by one
+    }
   }
 }
 
@@ -1120,14 +1138,29 @@ cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream
   switch (b.type) {
     case OSTC_BC_OUTFLOW: bc_outflow_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
     case OSTC_BC_INFLOW: bc_inflow_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
-    case OSTC_BC_SYMMETRY: bc_symmetry_kernel<<<grid, blk, 0, s>>>(z, b); break;
+    case OSTC_BC_SYMMETRY: bc_symmetry_kernel<<<grid, blk, 0, s>>>(z, b, with_cv); break;
     case OSTC_BC_PERIODIC: bc_periodic_kernel<<<grid, blk, 0, s>>>(z, b, with_cv); break;
     case OSTC_BC_WALL: bc_wall_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
-    case OSTC_BC_FARFIELD: bc_farfield_kernel<NS><<<grid, blk, 0, s>>>(z, b); break;
+    case OSTC_BC_FARFIELD: bc_farfield_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
     case OSTC_BC_BACK_PRESSURE: bc_back_pressure_kernel<NS><<<grid, blk, 0, s>>>(z, b, with_cv); break;
     case OSTC_BC_SUBSONIC_INFLOW: bc_subsonic_inflow_kernel<<<grid, blk, 0, s>>>(z, b, with_cv); break;
     default: return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+// one wave of boundary faces over every zone (bc_table_kernel): every
+// resident CTA slot, at most one per tile
+template <int NS>
+cudaError_t launch_bc_table(const BcFace *faces, const CellTable &tab, int with_cv, cudaStream_t s) {
+  if (tab.n <= 0) return cudaSuccess;
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bc_table_kernel<NS>, 256, 0);
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const int slots = per_sm * sms > 0 ? per_sm * sms : 1;
+  bc_table_kernel<NS><<<tab.n < slots ? tab.n : slots, dim3(32, 8), 0, s>>>(faces, tab.tiles, tab.n, with_cv);
   return cudaGetLastError();
 }
 
@@ -1284,6 +1317,7 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   template cudaError_t launch_cells<NS>(CellOp, const DevZone &, const CellArgs &, cudaStream_t);            \
   template cudaError_t launch_cells_table<NS>(CellOp, const CellTable &, const CellArgs &, cudaStream_t);    \
   template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);                    \
+  template cudaError_t launch_bc_table<NS>(const BcFace *, const CellTable &, int, cudaStream_t);             \
   template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t); \
   template cudaError_t launch_steady<NS>(SteadyOp, const DevZone &, const SteadyArgs &, const BcFace *, cudaStream_t); \
   template cudaError_t launch_chem_integrator<NS>(int, const double *, const double *, const double *, const double *, \

@@ -50,6 +50,7 @@ inline dim3 flux_grid(int mx, int my, int mz, int dir, int R, int C) {
 // one boundary face as the kernels see it
 struct BcFace {
   int type, face, direction;
+  int zone;  // index of the face's zone in the context (tile-table launches)
   int rs[3], re[3];
   int dir_stride;     // ghosted-index stride of one step along the outward normal
   int period_stride;  // periodic: ghosted-index stride of n cells along the normal
@@ -130,6 +131,9 @@ cudaError_t stage_timeout_flux_ns_d(int *flag);
 cudaError_t stage_timeouts(int *any);
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s);
+// one wave of faces (device records, zones in the tile-table zone table)
+template <int NS>
+cudaError_t launch_bc_table(const BcFace *faces, const CellTable &tab, int with_cv, cudaStream_t s);
 template <int NS>
 cudaError_t launch_interface(const DevZone &self, const DevZone &tar, const Iface &f, int with_cv, cudaStream_t s);
 template <int NS>

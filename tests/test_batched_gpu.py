@@ -85,3 +85,38 @@ def test_batching_toggle_on_one_context():
         for b, r in zip(blocks, ref):
             assert np.array_equal(b.download("dq"), r)
     s.close()
+
+
+# boundary faces in batched launches: each priority level's faces over all
+# blocks in waves of faces with disjoint footprints; the per-face order of the
+# reference stays wherever two faces of a block touch the same cells
+BC_CASES = {
+    "wall_farfield": lambda: ostc.case_bc_box("wall_farfield", 34, 27, 9),
+    "subsonic": lambda: ostc.case_bc_box("subsonic", 34, 27, 9),
+    "planar_wall_farfield": lambda: ostc.case_bc_box("wall_farfield", 34, 27, 1),
+    "mixing_layer": lambda: ostc.case_mixing_layer(33, 26, 9, dx=1e-3, full_host=True),
+    "uneven_sst": lambda: ostc.case_uneven_blocks(
+        layout=ostc.block_layout(5, dims=(40, 30, 32), ranges=((8, 20), (8, 14), (8, 10)), anchors=False),
+        rans_model=2),
+}
+
+
+@pytest.mark.parametrize("name", list(BC_CASES))
+def test_batched_boundary_faces_equal_per_face(name):
+    case = BC_CASES[name]
+    _equal(_run(case(), True, steps=4), _run(case(), False, steps=4))
+
+
+def test_boundary_waves_batch_the_faces_that_do_not_meet():
+    """the wall-farfield box: its two far-field faces share an edge and both
+    set their boundary layer (two waves), its two symmetry faces do not meet
+    (one wave), so a batched stage has fewer launches than a per-face one"""
+    case = ostc.case_bc_box("wall_farfield", 34, 27, 9)
+    s, _ = case.solver()
+    s.set_batching(True)
+    s.initialize()
+    n_batched = s.step_kernel_count(False)
+    s.set_batching(False)
+    n_face = s.step_kernel_count(False)
+    s.close()
+    assert n_batched < n_face, (n_batched, n_face)
