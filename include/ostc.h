@@ -596,9 +596,10 @@ ostc_status ostc_autotune(ostc_ctx *ctx, int warmup, int reps, void *stream, flo
  * cell sees the same operations in the same order. Default: on for 2 to 64
  * blocks, off for one. Boundary faces go in one launch per wave of each
  * priority level (BoundCond.cuh:673-822; faces of a level and block whose
- * footprints meet keep their order, in separate waves); periodic faces and
- * interfaces keep their per-face launches (the interfaces' order matters,
- * DataCommunication.cuh:30-49). At most 64 blocks:
+ * footprints meet keep their order, in separate waves), the interfaces in
+ * waves of faces whose footprints (own range and plane, partner's range and
+ * plane) do not meet, in their order (DataCommunication.cuh:30-49); periodic
+ * faces keep their per-face launches. At most 64 blocks:
  * OSTC_ERR_UNSUPPORTED beyond. No reference counterpart: the reference
  * launches every kernel per block (RK.cuh:107-161).                       */
 ostc_status ostc_set_batching(ostc_ctx *ctx, int on);

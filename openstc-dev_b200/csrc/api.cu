@@ -50,6 +50,10 @@ struct ostc_ctx {
   BcFace *faces_dev = nullptr;
   std::vector<CellTable> bc_waves;
   std::vector<int> bc_wave_type;
+  // batched interfaces: their records on the device and the waves in order
+  Iface *ifaces_dev = nullptr;
+  size_t ifaces_cap = 0;
+  std::vector<CellTable> if_waves;
   CellTable cell_tab[3];
   FluxTable flux_tab[3][2];
   unsigned long long *dt_bits = nullptr;  // device dt (as bits)
@@ -217,6 +221,91 @@ ostc_status build_tables(ostc_ctx *ctx) {
       }
     }
   }
+  // interfaces in the order of data_communication (block by block, each
+  // block's faces in order; DataCommunication.cuh:30-49), split into waves
+  // the same way: a face goes one wave after the last earlier face that writes
+  // a cell it reads or writes, or reads a cell it writes. A face writes its
+  // own range in its zone and the coincident plane in its partner's, and
+  // reads the partner's range and its own plane.
+  std::vector<std::pair<size_t, size_t>> if_spans;
+  {
+    struct ZBox {
+      int zone, lo[3], hi[3];
+    };
+    auto meet = [](const ZBox &x, const ZBox &y) {
+      if (x.zone != y.zone) return false;
+      for (int a = 0; a < 3; ++a)
+        if (x.hi[a] < y.lo[a] || y.hi[a] < x.lo[a]) return false;
+      return true;
+    };
+    struct Foot {
+      ZBox w[2], r[2];
+    };
+    auto foot = [&](const Iface &f) {
+      Foot o;
+      ZBox self{f.zone, {}, {}}, tar{f.target, {}, {}};
+      for (int d = 0; d < 3; ++d) {
+        const int a = f.rs[d], b = f.rs[d] + f.ld[d] * (f.np[d] - 1);
+        self.lo[d] = std::min(a, b), self.hi[d] = std::max(a, b);
+        const int span = f.np[f.st[d]] - 1;
+        const int ta = f.ts[d], tb = f.ts[d] + f.tld[d] * f.ld[f.st[d]] * span;
+        tar.lo[d] = std::min(ta, tb), tar.hi[d] = std::max(ta, tb);
+      }
+      // the coincident plane: n[face] fixed where idx[face] == plane
+      const int plane = f.direction > 0 ? f.rs[f.face] : f.rs[f.face] + f.ld[f.face] * (f.np[f.face] - 1);
+      const int nf = (plane - f.rs[f.face]) / f.ld[f.face];
+      ZBox sp = self, tp = tar;
+      sp.lo[f.face] = sp.hi[f.face] = plane;
+      for (int d = 0; d < 3; ++d)
+        if (f.st[d] == f.face) tp.lo[d] = tp.hi[d] = f.ts[d] + f.tld[d] * f.ld[f.face] * nf;
+      o.w[0] = self, o.w[1] = tp, o.r[0] = tar, o.r[1] = sp;
+      return o;
+    };
+    auto conflict = [&](const Foot &x, const Foot &y) {
+      for (const ZBox &a : x.w) {
+        for (const ZBox &b : y.w)
+          if (meet(a, b)) return true;
+        for (const ZBox &b : y.r)
+          if (meet(a, b)) return true;
+      }
+      for (const ZBox &a : y.w)
+        for (const ZBox &b : x.r)
+          if (meet(a, b)) return true;
+      return false;
+    };
+    std::vector<int> qs, wave;
+    std::vector<Foot> fs;
+    for (size_t b = 0; b < ctx->dz.size(); ++b)
+      for (size_t q = 0; q < ctx->ifaces.size(); ++q) {
+        if (ctx->iface_zone[q] != (int)b) continue;
+        const Foot f = foot(ctx->ifaces[q]);
+        int wv = 0;
+        for (size_t p = 0; p < qs.size(); ++p)
+          if (conflict(f, fs[p])) wv = std::max(wv, wave[p] + 1);
+        qs.push_back((int)q), wave.push_back(wv), fs.push_back(f);
+      }
+    const int n_waves = qs.empty() ? 0 : *std::max_element(wave.begin(), wave.end()) + 1;
+    for (int wv = 0; wv < n_waves; ++wv) {
+      const size_t b0 = all.size();
+      for (size_t p = 0; p < qs.size(); ++p) {
+        if (wave[p] != wv) continue;
+        const Iface &f = ctx->ifaces[qs[p]];
+        for (int n2 = 0; n2 < f.np[2]; ++n2)
+          for (int b1 = 0; b1 < (f.np[1] + 7) / 8; ++b1)
+            for (int b0_ = 0; b0_ < (f.np[0] + 31) / 32; ++b0_) all.push_back(make_int4(qs[p], b0_, b1, n2));
+      }
+      if_spans.push_back({b0, all.size()});
+    }
+    if (ctx->ifaces.size() > ctx->ifaces_cap) {
+      cudaFree(ctx->ifaces_dev);
+      ctx->ifaces_dev = nullptr;
+      ctx->ifaces_cap = 0;
+      CK(cudaMalloc(&ctx->ifaces_dev, sizeof(Iface) * ctx->ifaces.size()));
+      ctx->ifaces_cap = ctx->ifaces.size();
+    }
+    if (!ctx->ifaces.empty())
+      CK(cudaMemcpy(ctx->ifaces_dev, ctx->ifaces.data(), sizeof(Iface) * ctx->ifaces.size(), cudaMemcpyHostToDevice));
+  }
   if (!ctx->faces.empty() && !ctx->faces_dev) {
     CK(cudaMalloc(&ctx->faces_dev, sizeof(BcFace) * ctx->faces.size()));
     CK(cudaMemcpy(ctx->faces_dev, ctx->faces.data(), sizeof(BcFace) * ctx->faces.size(), cudaMemcpyHostToDevice));
@@ -250,6 +339,13 @@ ostc_status build_tables(ostc_ctx *ctx) {
     ctx->bc_waves.push_back(t);
   }
   ctx->bc_wave_type = bc_types;
+  ctx->if_waves.clear();
+  for (const auto &sp : if_spans) {
+    CellTable t;
+    t.tiles = ctx->tab_dev + sp.first;
+    t.n = (int)(sp.second - sp.first);
+    ctx->if_waves.push_back(t);
+  }
   return OSTC_OK;
 }
 
@@ -772,6 +868,7 @@ ostc_status ostc_destroy(ostc_ctx *ctx) {
   cudaFree(ctx->dt_bits);
   cudaFree(ctx->tab_dev);
   cudaFree(ctx->faces_dev);
+  cudaFree(ctx->ifaces_dev);
   cudaFree(ctx->res_partial);
   cudaFree(ctx->hist_counter);
   cudaFree(ctx->bad_key);
@@ -902,6 +999,13 @@ ostc_status ostc_data_communication(ostc_ctx *ctx, int with_cv, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;
   if (ctx->ifaces.empty()) return OSTC_OK;
   if (ensure_param(ctx, S(stream))) return ctx->last;
+  if (ctx->batched) {  // the waves of build_tables, one launch each over all zones
+    for (const CellTable &w : ctx->if_waves)
+      CK(dispatch_ns(ctx->ns, [&](auto n) {
+        return launch_interface_table<decltype(n)::value>(ctx->ifaces_dev, w, with_cv, S(stream));
+      }));
+    return OSTC_OK;
+  }
   // per block, per face, in order (DataCommunication.cuh:30-49)
   for (size_t b = 0; b < ctx->dz.size(); ++b)
     for (size_t q = 0; q < ctx->ifaces.size(); ++q) {
@@ -950,6 +1054,8 @@ ostc_status ostc_set_interfaces(ostc_ctx *ctx, const ostc_interface *f, int n) {
       const int thi = std::max(g.ts[d], g.ts[d] + g.tld[d] * g.ld[g.st[d]] * span);
       if (tlo < -t.ngg || thi > et[d] - 1 + t.ngg) return OSTC_ERR_INVALID_ARG;
     }
+    g.zone = a.block;
+    g.target = a.target;
     v.push_back(g);
     zb.push_back(a.block);
     tb.push_back(a.target);
@@ -962,6 +1068,7 @@ ostc_status ostc_set_interfaces(ostc_ctx *ctx, const ostc_interface *f, int n) {
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
   ctx->graphs.clear();
+  if (ctx->batched) return build_tables(ctx);  // the interface waves
   return OSTC_OK;
 }
 

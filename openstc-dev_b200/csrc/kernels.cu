@@ -823,11 +823,8 @@ __global__ void __launch_bounds__(256) bc_table_kernel(const BcFace *faces, cons
 // 1-to-1 interface (inner_communication, DataCommunication.cuh:58-110): ghosts
 // take the partner's values, the coincident plane the average of both blocks
 template <int NS>
-__global__ void interface_kernel(DevZone z, DevZone t, Iface f, int with_cv) {
-  const int n0 = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n1 = blockIdx.y * blockDim.y + threadIdx.y;
-  const int n2 = blockIdx.z;
-  if (n0 >= f.np[0] || n1 >= f.np[1] || n2 >= f.np[2]) return;
+__device__ __forceinline__ void interface_point(const DevZone &z, const DevZone &t, const Iface &f, int with_cv,
+                                                int n0, int n1, int n2) {
   const int n[3] = {n0, n1, n2};
   int idx[3], d[3], it[3];
 #pragma unroll
@@ -860,6 +857,30 @@ __global__ void interface_kernel(DevZone z, DevZone t, Iface f, int with_cv) {
     for (int l = 0; l < c_p.n_scalar; ++l) z.sv[l * z.sz + g] = t.sv[l * t.sz + gt];
   }
   if (with_cv) cv_from_bv_point<NS>(z, g);
+}
+
+template <int NS>
+__global__ void interface_kernel(DevZone z, DevZone t, Iface f, int with_cv) {
+  const int n0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n1 = blockIdx.y * blockDim.y + threadIdx.y;
+  const int n2 = blockIdx.z;
+  if (n0 >= f.np[0] || n1 >= f.np[1] || n2 >= f.np[2]) return;
+  interface_point<NS>(z, t, f, with_cv, n0, n1, n2);
+}
+
+// the interfaces of one wave over every zone in one launch: tiles {face, b0,
+// b1, n2} of 32 x 8 points of the faces' ranges; the faces of a wave touch
+// disjoint cells (in their own zones and their partners')
+template <int NS>
+__global__ void __launch_bounds__(256) interface_table_kernel(const Iface *faces, const int4 *tiles, int n_tiles,
+                                                              int with_cv) {
+  for (int q = blockIdx.x; q < n_tiles; q += gridDim.x) {
+    const int4 c = tiles[q];
+    const Iface &f = faces[c.x];
+    const int n0 = c.y * 32 + threadIdx.x, n1 = c.z * 8 + threadIdx.y, n2 = c.w;
+    if (n0 >= f.np[0] || n1 >= f.np[1]) continue;
+    interface_point<NS>(c_zones[f.zone], c_zones[f.target], f, with_cv, n0, n1, n2);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1165,6 +1186,19 @@ cudaError_t launch_bc_table(const BcFace *faces, const CellTable &tab, int with_
 }
 
 template <int NS>
+cudaError_t launch_interface_table(const Iface *faces, const CellTable &tab, int with_cv, cudaStream_t s) {
+  if (tab.n <= 0) return cudaSuccess;
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, interface_table_kernel<NS>, 256, 0);
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const int slots = per_sm * sms > 0 ? per_sm * sms : 1;
+  interface_table_kernel<NS><<<tab.n < slots ? tab.n : slots, dim3(32, 8), 0, s>>>(faces, tab.tiles, tab.n, with_cv);
+  return cudaGetLastError();
+}
+
+template <int NS>
 cudaError_t launch_interface(const DevZone &self, const DevZone &tar, const Iface &f, int with_cv, cudaStream_t s) {
   // launch shape of data_communication (DataCommunication.cuh:36-45)
   const dim3 blk(f.np[0] <= 2 * self.ngg + 1 ? 1 : 16, f.np[1] <= 2 * self.ngg + 1 ? 1 : 16);
@@ -1318,6 +1352,7 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   template cudaError_t launch_cells_table<NS>(CellOp, const CellTable &, const CellArgs &, cudaStream_t);    \
   template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);                    \
   template cudaError_t launch_bc_table<NS>(const BcFace *, const CellTable &, int, cudaStream_t);             \
+  template cudaError_t launch_interface_table<NS>(const Iface *, const CellTable &, int, cudaStream_t);       \
   template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t); \
   template cudaError_t launch_steady<NS>(SteadyOp, const DevZone &, const SteadyArgs &, const BcFace *, cudaStream_t); \
   template cudaError_t launch_chem_integrator<NS>(int, const double *, const double *, const double *, const double *, \

@@ -65,6 +65,7 @@ struct BcFace {
 struct Iface {
   int face, direction;
   int rs[3], ts[3], ld[3], tld[3], st[3], np[3];
+  int zone, target;  // the face's zone and its partner's in the context (tile-table launches)
 };
 
 enum class CellOp { Source, UpdateRK, Properties, CvFromBv, Velocity, Dt, DtReset, StoreLast, ResidualPartial, InitMut };
@@ -134,6 +135,8 @@ cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream
 // one wave of faces (device records, zones in the tile-table zone table)
 template <int NS>
 cudaError_t launch_bc_table(const BcFace *faces, const CellTable &tab, int with_cv, cudaStream_t s);
+template <int NS>
+cudaError_t launch_interface_table(const Iface *faces, const CellTable &tab, int with_cv, cudaStream_t s);
 template <int NS>
 cudaError_t launch_interface(const DevZone &self, const DevZone &tar, const Iface &f, int with_cv, cudaStream_t s);
 template <int NS>
