@@ -23,7 +23,11 @@
  *
  * Every entry point returns an ostc_status; none aborts. Work is enqueued on
  * the stream passed in; no entry point below synchronises the host unless
- * its comment says so.
+ * its comment says so. The library keeps the run parameters and the zone
+ * table of the context used last in constant memory and uploads them when
+ * a call on another context comes first; an operator called into a caller's
+ * stream capture at that moment returns OSTC_ERR_INVALID_ARG (a captured
+ * upload would take effect only when the graph runs).
  */
 #ifndef OSTC_H
 #define OSTC_H
@@ -594,16 +598,29 @@ ostc_status ostc_autotune(ostc_ctx *ctx, int warmup, int reps, void *stream, flo
  * of {block, tile} entries built from the blocks' extents and the flux tile
  * shapes. Results are identical to the per-block launches (on = 0): every
  * cell sees the same operations in the same order. Default: on for 2 to 64
- * blocks, off for one. Boundary faces go in one launch per wave of each
- * priority level (BoundCond.cuh:673-822; faces of a level and block whose
- * footprints meet keep their order, in separate waves), the interfaces in
- * waves of faces whose footprints (own range and plane, partner's range and
- * plane) do not meet, in their order (DataCommunication.cuh:30-49); periodic
- * faces keep their per-face launches. At most 64 blocks:
+ * blocks, off for one. Batched, ostc_apply_boundary_conditions is one
+ * cooperative launch over
+ * every face in the per-face order (priority levels of BoundCond.cuh:673-822,
+ * then the periodic wraps), ostc_data_communication one over every interface
+ * in their order (DataCommunication.cuh:30-49). Each splits its faces into
+ * waves of faces whose footprints do not meet (a face goes one wave after
+ * the last earlier face whose footprint meets its own: for interfaces own
+ * range and plane, partner's range and plane), with a grid barrier between
+ * waves, so the results are the per-face ones bit for bit. A barrier wait is
+ * bounded (about one second); one that runs out makes the next check of a
+ * call with histories return OSTC_ERR_TIMEOUT. At most 64 blocks:
  * OSTC_ERR_UNSUPPORTED beyond. No reference counterpart: the reference
- * launches every kernel per block (RK.cuh:107-161).                       */
+ * launches every kernel per block and face (RK.cuh:107-161).              */
 ostc_status ostc_set_batching(ostc_ctx *ctx, int on);
 ostc_status ostc_get_batching(const ostc_ctx *ctx, int *on);
+/* Diagnostic for failure handling: with on = 1 the grid barriers of the
+ * batched boundary-face and interface launches withhold their release, so
+ * each launch with more than one wave waits about one second, stops, and
+ * the next ostc_rk3_steps / ostc_steady_steps with histories returns
+ * OSTC_ERR_TIMEOUT (the waves after the first were not computed); on = 0
+ * restores normal operation. Synchronises the device. No reference
+ * counterpart.                                                              */
+ostc_status ostc_inject_wave_timeout(ostc_ctx *ctx, int on);
 
 /* Launch one kernel family on every block (timing and autotuning aid):
  * OSTC_OP_FLUX (arg = direction, accumulates into dq; arg + 3: the inviscid

@@ -45,15 +45,19 @@ struct ostc_ctx {
   int batched = 0;
   int4 *tab_dev = nullptr;
   size_t tab_cap = 0;
-  // batched boundary conditions: the face records on the device and, in
-  // launch order, the waves of each priority level (type, tiles)
+  // boundary faces and interfaces in waves (one cooperative launch per call
+  // over every zone): on by default for up to kMaxTableZones zones, one block
+  // included; ostc_set_batching switches it with the tile tables. The face
+  // and interface records on the device, the two wave plans (their tiles in
+  // tab_dev, their ends in wave_ends_dev) and the grid barriers (two WaveSync)
+  int face_batched = 0;
   BcFace *faces_dev = nullptr;
-  std::vector<CellTable> bc_waves;
-  std::vector<int> bc_wave_type;
-  // batched interfaces: their records on the device and the waves in order
   Iface *ifaces_dev = nullptr;
   size_t ifaces_cap = 0;
-  std::vector<CellTable> if_waves;
+  WavePlan bc_plan, if_plan;
+  int *wave_ends_dev = nullptr;
+  size_t wave_ends_cap = 0;
+  WaveSync *wave_sync = nullptr;
   CellTable cell_tab[3];
   FluxTable flux_tab[3][2];
   unsigned long long *dt_bits = nullptr;  // device dt (as bits)
@@ -107,10 +111,18 @@ ostc_status fail(ostc_ctx *c, ostc_status s, cudaError_t e = cudaSuccess) {
     if (e_ != cudaSuccess) return fail(ctx, OSTC_ERR_CUDA, e_); \
   } while (0)
 
+// the run parameters and zone table of ctx in every kernel unit's constant
+// memory, uploaded when another context (or none) was the last one uploaded.
+// Not inside a stream capture: an upload captured into a graph would happen
+// only when the graph runs, while later calls took it as done (ensure_graph
+// uploads before it captures).
 ostc_status ensure_param(ostc_ctx *ctx, cudaStream_t s) {
   if (g_uploaded != ctx) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return fail(ctx, OSTC_ERR_INVALID_ARG);
     CK(upload_param(ctx->dp, s));
-    if (ctx->batched) CK(upload_zones(ctx->dz.data(), (int)ctx->dz.size(), s));
+    if (ctx->batched || ctx->face_batched) CK(upload_zones(ctx->dz.data(), (int)ctx->dz.size(), s));
     g_uploaded = ctx;
   }
   return OSTC_OK;
@@ -161,16 +173,26 @@ ostc_status build_tables(ostc_ctx *ctx) {
       spans.push_back({b0, all.size()});
       flux_bulk_tiles.push_back(nb);
     }
-  // boundary faces by priority level (BoundCond.cuh:673-822; periodic faces
-  // keep their own launches), each level split into waves: a face goes one
-  // wave after the last earlier face of its level and zone that writes a
-  // cell it reads or writes, or reads a cell it writes, so every such pair
-  // keeps the per-face order and the faces of a wave touch disjoint cells.
-  // Footprints along the normal: writes from the boundary layer (types that
-  // set it) or the first ghost layer out to ngg ghosts; reads from the
-  // boundary layer ngg layers inward; tangentially the face's ranges.
+  // the tiles of a face of n[0] x n[1] x n[2] points with normal axis f in a
+  // wave: 32 points along its first tangential axis, 8 along the second, one
+  // layer along the normal (waves_kernel maps them back)
+  auto wave_tiles = [&](int rec, int f, const int n[3]) {
+    const int a = f == 0 ? 1 : 0, b = f == 2 ? 1 : 2;
+    for (int tc = 0; tc < n[f]; ++tc)
+      for (int tb = 0; tb < (n[b] + 7) / 8; ++tb)
+        for (int ta = 0; ta < (n[a] + 31) / 32; ++ta) all.push_back(make_int4(rec, ta, tb, tc));
+  };
+  // boundary faces in the per-face order of apply_boundary_conditions
+  // (priority levels of BoundCond.cuh:673-822, each level's faces in order,
+  // then the periodic wraps), split into waves: a face goes one wave after
+  // the last earlier face of its zone that writes a cell it reads or writes,
+  // or reads a cell it writes, so every such pair keeps the per-face order and
+  // the faces of a wave touch disjoint cells. Footprints along the normal:
+  // writes from the boundary layer (types that set it) or the first ghost
+  // layer out to ngg ghosts; reads from the boundary layer ngg layers inward
+  // (periodic: the layers one period back from its ghosts); tangentially the
+  // face's ranges.
   std::vector<std::pair<size_t, size_t>> bc_spans;
-  std::vector<int> bc_types;
   {
     struct Box {
       int lo[3], hi[3];
@@ -180,7 +202,12 @@ ostc_status build_tables(ostc_ctx *ctx) {
       for (int a = 0; a < 3; ++a) W.lo[a] = R.lo[a] = b.rs[a], W.hi[a] = R.hi[a] = b.re[a];
       const bool sets_boundary = b.type == OSTC_BC_INFLOW || b.type == OSTC_BC_SYMMETRY || b.type == OSTC_BC_WALL ||
                                  b.type == OSTC_BC_FARFIELD;
-      const int wa = sets_boundary ? bi : bi + d, wb = bi + d * g, ra = bi, rb = bi - d * g;
+      const int wa = sets_boundary ? bi : bi + d, wb = bi + d * g;
+      int ra = bi, rb = bi - d * g;
+      if (b.type == OSTC_BC_PERIODIC) {  // go = g + gg * dir_stride reads go - period_stride
+        const int ext[3] = {ctx->dz[b.zone].mx, ctx->dz[b.zone].my, ctx->dz[b.zone].mz};
+        ra = bi + d - d * ext[f], rb = bi + d * g - d * ext[f];
+      }
       W.lo[f] = std::min(wa, wb), W.hi[f] = std::max(wa, wb);
       R.lo[f] = std::min(ra, rb), R.hi[f] = std::max(ra, rb);
     };
@@ -190,10 +217,10 @@ ostc_status build_tables(ostc_ctx *ctx) {
       return true;
     };
     static const int order[] = {OSTC_BC_FARFIELD,        OSTC_BC_OUTFLOW,  OSTC_BC_BACK_PRESSURE, OSTC_BC_INFLOW,
-                                OSTC_BC_SUBSONIC_INFLOW, OSTC_BC_SYMMETRY, OSTC_BC_WALL};
-    for (int t : order) {
-      std::vector<int> qs, wave;
-      std::vector<Box> W, R;
+                                OSTC_BC_SUBSONIC_INFLOW, OSTC_BC_SYMMETRY, OSTC_BC_WALL,          OSTC_BC_PERIODIC};
+    std::vector<int> qs, wave;
+    std::vector<Box> W, R;
+    for (int t : order)
       for (size_t q = 0; q < ctx->faces.size(); ++q) {
         if (ctx->faces[q].type != t) continue;
         Box w, r;
@@ -205,20 +232,16 @@ ostc_status build_tables(ostc_ctx *ctx) {
         }
         qs.push_back((int)q), wave.push_back(wv), W.push_back(w), R.push_back(r);
       }
-      const int n_waves = qs.empty() ? 0 : *std::max_element(wave.begin(), wave.end()) + 1;
-      for (int wv = 0; wv < n_waves; ++wv) {
-        const size_t b0 = all.size();
-        for (size_t p = 0; p < qs.size(); ++p) {
-          if (wave[p] != wv) continue;
-          const BcFace &b = ctx->faces[qs[p]];
-          const int n0 = b.re[0] - b.rs[0] + 1, n1 = b.re[1] - b.rs[1] + 1, n2 = b.re[2] - b.rs[2] + 1;
-          for (int bz = 0; bz < n2; ++bz)
-            for (int by = 0; by < (n1 + 7) / 8; ++by)
-              for (int bx = 0; bx < (n0 + 31) / 32; ++bx) all.push_back(make_int4(qs[p], bx, by, bz));
-        }
-        bc_spans.push_back({b0, all.size()});
-        bc_types.push_back(t);
+    const int n_waves = qs.empty() ? 0 : *std::max_element(wave.begin(), wave.end()) + 1;
+    for (int wv = 0; wv < n_waves; ++wv) {
+      const size_t b0 = all.size();
+      for (size_t p = 0; p < qs.size(); ++p) {
+        if (wave[p] != wv) continue;
+        const BcFace &b = ctx->faces[qs[p]];
+        const int n[3] = {b.re[0] - b.rs[0] + 1, b.re[1] - b.rs[1] + 1, b.re[2] - b.rs[2] + 1};
+        wave_tiles(qs[p], b.face, n);
       }
+      bc_spans.push_back({b0, all.size()});
     }
   }
   // interfaces in the order of data_communication (block by block, each
@@ -290,9 +313,13 @@ ostc_status build_tables(ostc_ctx *ctx) {
       for (size_t p = 0; p < qs.size(); ++p) {
         if (wave[p] != wv) continue;
         const Iface &f = ctx->ifaces[qs[p]];
-        for (int n2 = 0; n2 < f.np[2]; ++n2)
-          for (int b1 = 0; b1 < (f.np[1] + 7) / 8; ++b1)
-            for (int b0_ = 0; b0_ < (f.np[0] + 31) / 32; ++b0_) all.push_back(make_int4(qs[p], b0_, b1, n2));
+        if (f.face == 0) {  // tiles of 4 layers x 8 (j) x 8 (k) points
+          for (int tc = 0; tc < (f.np[0] + 3) / 4; ++tc)
+            for (int tb = 0; tb < (f.np[2] + 7) / 8; ++tb)
+              for (int ta = 0; ta < (f.np[1] + 7) / 8; ++ta) all.push_back(make_int4(qs[p], ta, tb, tc));
+        } else {
+          wave_tiles(qs[p], f.face, f.np);
+        }
       }
       if_spans.push_back({b0, all.size()});
     }
@@ -331,20 +358,35 @@ ostc_status build_tables(ostc_ctx *ctx) {
       ctx->flux_tab[d][v] = table(3 + 2 * d + v);
       ctx->flux_tab[d][v].n_bulk = (int)flux_bulk_tiles[2 * d + v];
     }
-  ctx->bc_waves.clear();
-  for (const auto &sp : bc_spans) {
-    CellTable t;
-    t.tiles = ctx->tab_dev + sp.first;
-    t.n = (int)(sp.second - sp.first);
-    ctx->bc_waves.push_back(t);
+  // the wave plans: tiles from the first wave's on, ends relative to it; the
+  // boundary plan's ends first in wave_ends_dev, then the interfaces'
+  std::vector<int> ends;
+  auto plan = [&](const std::vector<std::pair<size_t, size_t>> &sp, WavePlan &p) {
+    p = WavePlan{};
+    if (sp.empty()) return;
+    p.tiles = ctx->tab_dev + sp.front().first;
+    p.n_waves = (int)sp.size();
+    for (const auto &w : sp) {
+      ends.push_back((int)(w.second - sp.front().first));
+      p.max_tiles = std::max(p.max_tiles, (int)(w.second - w.first));
+    }
+  };
+  plan(bc_spans, ctx->bc_plan);
+  plan(if_spans, ctx->if_plan);
+  if (ends.size() > ctx->wave_ends_cap) {
+    cudaFree(ctx->wave_ends_dev);
+    ctx->wave_ends_dev = nullptr;
+    ctx->wave_ends_cap = 0;
+    CK(cudaMalloc(&ctx->wave_ends_dev, sizeof(int) * ends.size()));
+    ctx->wave_ends_cap = ends.size();
   }
-  ctx->bc_wave_type = bc_types;
-  ctx->if_waves.clear();
-  for (const auto &sp : if_spans) {
-    CellTable t;
-    t.tiles = ctx->tab_dev + sp.first;
-    t.n = (int)(sp.second - sp.first);
-    ctx->if_waves.push_back(t);
+  if (!ends.empty())
+    CK(cudaMemcpy(ctx->wave_ends_dev, ends.data(), sizeof(int) * ends.size(), cudaMemcpyHostToDevice));
+  if (ctx->bc_plan.n_waves) ctx->bc_plan.ends = ctx->wave_ends_dev;
+  if (ctx->if_plan.n_waves) ctx->if_plan.ends = ctx->wave_ends_dev + ctx->bc_plan.n_waves;
+  if (!ctx->wave_sync) {
+    CK(cudaMalloc(&ctx->wave_sync, 2 * sizeof(WaveSync)));
+    CK(cudaMemset(ctx->wave_sync, 0, 2 * sizeof(WaveSync)));
   }
   return OSTC_OK;
 }
@@ -847,9 +889,11 @@ ostc_status ostc_create(const ostc_config *cfg, const ostc_param *param, const o
   CK(cudaMemset(c->ep_time, 0, sizeof(double)));
   CK(cudaDeviceSynchronize());
   default_tiles(ctx);
-  // several blocks: one tile-table launch per kernel over all of them
+  // several blocks: one tile-table launch per kernel over all of them, the
+  // boundary faces and interfaces in waves
   if (n_zones > 1 && n_zones <= kMaxTableZones) {
     c->batched = 1;
+    c->face_batched = 1;
     if ((st = build_tables(ctx))) return st;
   }
   *out = c.release();
@@ -869,6 +913,8 @@ ostc_status ostc_destroy(ostc_ctx *ctx) {
   cudaFree(ctx->tab_dev);
   cudaFree(ctx->faces_dev);
   cudaFree(ctx->ifaces_dev);
+  cudaFree(ctx->wave_ends_dev);
+  cudaFree(ctx->wave_sync);
   cudaFree(ctx->res_partial);
   cudaFree(ctx->hist_counter);
   cudaFree(ctx->bad_key);
@@ -971,18 +1017,11 @@ ostc_status ostc_apply_boundary_conditions(ostc_ctx *ctx, int with_cv, void *str
   // priority order of BoundCond.cuh:673-822; periodic wraps after all others
   static const int order[] = {OSTC_BC_FARFIELD, OSTC_BC_OUTFLOW, OSTC_BC_BACK_PRESSURE, OSTC_BC_INFLOW,
                               OSTC_BC_SUBSONIC_INFLOW, OSTC_BC_SYMMETRY, OSTC_BC_WALL, OSTC_BC_PERIODIC};
-  if (ctx->batched) {
-    // every priority level's waves in one launch each over all zones
-    // (tables of build_tables, same order), then the periodic faces
-    for (size_t w = 0; w < ctx->bc_waves.size(); ++w)
-      CK(dispatch_ns(ctx->ns, [&](auto n) {
-        return launch_bc_table<decltype(n)::value>(ctx->faces_dev, ctx->bc_waves[w], with_cv, S(stream));
-      }));
-    for (size_t q = 0; q < ctx->faces.size(); ++q) {
-      if (ctx->faces[q].type != OSTC_BC_PERIODIC) continue;
-      const DevZone &z = ctx->dz[ctx->face_zone[q]];
-      CK(dispatch_ns(ctx->ns, [&](auto n) { return launch_bc<decltype(n)::value>(z, ctx->faces[q], with_cv, S(stream)); }));
-    }
+  if (ctx->face_batched) {
+    // every face in the per-face order's waves, one cooperative launch (build_tables)
+    CK(dispatch_ns(ctx->ns, [&](auto n) {
+      return launch_bc_waves<decltype(n)::value>(ctx->faces_dev, ctx->bc_plan, with_cv, ctx->wave_sync, S(stream));
+    }));
     return OSTC_OK;
   }
   for (int t : order) {
@@ -999,11 +1038,11 @@ ostc_status ostc_data_communication(ostc_ctx *ctx, int with_cv, void *stream) {
   if (!ctx) return OSTC_ERR_INVALID_ARG;
   if (ctx->ifaces.empty()) return OSTC_OK;
   if (ensure_param(ctx, S(stream))) return ctx->last;
-  if (ctx->batched) {  // the waves of build_tables, one launch each over all zones
-    for (const CellTable &w : ctx->if_waves)
-      CK(dispatch_ns(ctx->ns, [&](auto n) {
-        return launch_interface_table<decltype(n)::value>(ctx->ifaces_dev, w, with_cv, S(stream));
-      }));
+  if (ctx->face_batched) {  // the waves of build_tables, one cooperative launch over all zones
+    CK(dispatch_ns(ctx->ns, [&](auto n) {
+      return launch_interface_waves<decltype(n)::value>(ctx->ifaces_dev, ctx->if_plan, with_cv, ctx->wave_sync + 1,
+                                                        S(stream));
+    }));
     return OSTC_OK;
   }
   // per block, per face, in order (DataCommunication.cuh:30-49)
@@ -1068,7 +1107,7 @@ ostc_status ostc_set_interfaces(ostc_ctx *ctx, const ostc_interface *f, int n) {
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
   ctx->graphs.clear();
-  if (ctx->batched) return build_tables(ctx);  // the interface waves
+  if (ctx->batched || ctx->face_batched) return build_tables(ctx);  // the interface waves
   return OSTC_OK;
 }
 
@@ -1215,6 +1254,12 @@ static ostc_status enqueue_steady_step(ostc_ctx *ctx, bool with_hist, cudaStream
 static ostc_status ensure_graph(ostc_ctx *ctx, bool hist, GraphEntry **out, bool steady = false) {
   GraphEntry &ge = ctx->graphs[(hist ? 1 : 0) + (steady ? 2 : 0)];
   if (!ge.exec) {
+    // parameters and zones uploaded now, so that the capture holds no upload
+    // (every launch of the graph is preceded by ensure_param on its stream)
+    if (g_uploaded != ctx) {
+      if (ensure_param(ctx, nullptr)) return ctx->last;
+      CK(cudaStreamSynchronize(nullptr));
+    }
     // a legacy default stream cannot be captured: capture on a private stream
     cudaStream_t cs;
     CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
@@ -1247,6 +1292,18 @@ static ostc_status check_state(ostc_ctx *ctx, unsigned long long key) {
   // its faces uncomputed: the steps are not valid
   int late = 0;
   CK(stage_timeouts(&late));
+  // likewise a wave launch whose grid barrier ran out (the waves after it
+  // were not computed); the flags are cleared for the next steps
+  if (ctx->wave_sync) {
+    WaveSync ws[2];
+    CK(cudaMemcpy(ws, ctx->wave_sync, sizeof(ws), cudaMemcpyDeviceToHost));
+    if (ws[0].timed_out || ws[1].timed_out) {
+      const int zero = 0;
+      for (int k = 0; k < 2; ++k)
+        CK(cudaMemcpy(&ctx->wave_sync[k].timed_out, &zero, sizeof(int), cudaMemcpyHostToDevice));
+      late = 1;
+    }
+  }
   if (late) return fail(ctx, OSTC_ERR_TIMEOUT);
   if (key == ~0ull) return OSTC_OK;
   const long long q = (long long)(key & ((1ull << 34) - 1));
@@ -1780,7 +1837,7 @@ ostc_status ostc_set_tile(ostc_ctx *ctx, int dir, int rows, int chunks) {
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
   ctx->graphs.clear();
-  if (ctx->batched) return build_tables(ctx);
+  if (ctx->batched || ctx->face_batched) return build_tables(ctx);
   return OSTC_OK;
 }
 
@@ -1788,6 +1845,7 @@ ostc_status ostc_set_batching(ostc_ctx *ctx, int on) {
   if (!ctx || (on != 0 && on != 1)) return OSTC_ERR_INVALID_ARG;
   if (on && ctx->dz.size() > (size_t)kMaxTableZones) return OSTC_ERR_UNSUPPORTED;
   ctx->batched = on;
+  ctx->face_batched = on;
   for (auto &kv : ctx->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
@@ -1795,6 +1853,14 @@ ostc_status ostc_set_batching(ostc_ctx *ctx, int on) {
   ctx->graphs.clear();
   g_uploaded = nullptr;  // the next launch uploads this context's zone table
   return on ? build_tables(ctx) : OSTC_OK;
+}
+
+ostc_status ostc_inject_wave_timeout(ostc_ctx *ctx, int on) {
+  if (!ctx || (on != 0 && on != 1)) return OSTC_ERR_INVALID_ARG;
+  if (!ctx->wave_sync) return OSTC_ERR_INVALID_ARG;  // no batched faces on this context
+  CK(cudaDeviceSynchronize());
+  for (int k = 0; k < 2; ++k) CK(cudaMemcpy(&ctx->wave_sync[k].hold, &on, sizeof(int), cudaMemcpyHostToDevice));
+  return OSTC_OK;
 }
 
 ostc_status ostc_get_batching(const ostc_ctx *ctx, int *on) {

@@ -7,6 +7,8 @@
 //  cv_from_bv_kernel<NS>  conservative from primitive, ghosts included (FieldOperation.cuh:43-79)
 //  dt_kernel<NS>          local time step + block min + atomic min (TimeAdvanceFunc.cuh:50-100, .cu:155-201)
 //  bc_*_kernel            boundary conditions (BoundCond.cuh:52-210) and periodic wrap
+//  waves_kernel<NS,KIND>  every boundary face (KIND 0) or interface (KIND 1) of a call in
+//                         one cooperative launch, waves apart by a bounded grid barrier
 //  residual kernels       store_last_step / square of d(bv) / deterministic sums (Residual.cuh:57-161)
 #include <cstdio>
 
@@ -794,29 +796,20 @@ OSTC_BC_KERNEL(bc_back_pressure_kernel, bc_back_pressure_point<NS>)
 static OSTC_BC_KERNEL(bc_subsonic_inflow_kernel, bc_subsonic_inflow_point)
 #undef OSTC_BC_KERNEL
 
-// the faces of one wave of a priority level over every zone in one launch:
-// a persistent grid walks tiles {face, bx, by, bz} of 32 x 8 points of the
-// faces' ranges (faces in device memory, zones in c_zones); the faces of a
-// wave write no cell that another face of the wave reads or writes
+// one point of a boundary face of any type (the face records of the wave
+// launches carry the type)
 template <int NS>
-__global__ void __launch_bounds__(256) bc_table_kernel(const BcFace *faces, const int4 *tiles, int n_tiles,
-                                                       int with_cv) {
-  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-    const int4 c = tiles[t];
-    const BcFace &b = faces[c.x];
-    const int i = b.rs[0] + c.y * 32 + threadIdx.x, j = b.rs[1] + c.z * 8 + threadIdx.y, k = b.rs[2] + c.w;
-    if (i > b.re[0] || j > b.re[1] || k > b.re[2]) continue;
-    const DevZone &z = c_zones[b.zone];
-    switch (b.type) {
-      case OSTC_BC_OUTFLOW: bc_outflow_point<NS>(z, b, with_cv, i, j, k); break;
-      case OSTC_BC_INFLOW: bc_inflow_point<NS>(z, b, with_cv, i, j, k); break;
-      case OSTC_BC_SYMMETRY: bc_symmetry_point(z, b, with_cv, i, j, k); break;
-      case OSTC_BC_WALL: bc_wall_point<NS>(z, b, with_cv, i, j, k); break;
-      case OSTC_BC_FARFIELD: bc_farfield_point<NS>(z, b, with_cv, i, j, k); break;
-      case OSTC_BC_BACK_PRESSURE: bc_back_pressure_point<NS>(z, b, with_cv, i, j, k); break;
-      case OSTC_BC_SUBSONIC_INFLOW: bc_subsonic_inflow_point(z, b, with_cv, i, j, k); break;
-      default: break;  // periodic faces are launched one by one
-    }
+__device__ __forceinline__ void bc_point(const DevZone &z, const BcFace &b, int with_cv, int i, int j, int k) {
+  switch (b.type) {
+    case OSTC_BC_OUTFLOW: bc_outflow_point<NS>(z, b, with_cv, i, j, k); break;
+    case OSTC_BC_INFLOW: bc_inflow_point<NS>(z, b, with_cv, i, j, k); break;
+    case OSTC_BC_SYMMETRY: bc_symmetry_point(z, b, with_cv, i, j, k); break;
+    case OSTC_BC_WALL: bc_wall_point<NS>(z, b, with_cv, i, j, k); break;
+    case OSTC_BC_FARFIELD: bc_farfield_point<NS>(z, b, with_cv, i, j, k); break;
+    case OSTC_BC_BACK_PRESSURE: bc_back_pressure_point<NS>(z, b, with_cv, i, j, k); break;
+    case OSTC_BC_SUBSONIC_INFLOW: bc_subsonic_inflow_point(z, b, with_cv, i, j, k); break;
+    case OSTC_BC_PERIODIC: bc_periodic_point(z, b, with_cv, i, j, k); break;
+    default: break;
   }
 }
 
@@ -868,18 +861,104 @@ __global__ void interface_kernel(DevZone z, DevZone t, Iface f, int with_cv) {
   interface_point<NS>(z, t, f, with_cv, n0, n1, n2);
 }
 
-// the interfaces of one wave over every zone in one launch: tiles {face, b0,
-// b1, n2} of 32 x 8 points of the faces' ranges; the faces of a wave touch
-// disjoint cells (in their own zones and their partners')
-template <int NS>
-__global__ void __launch_bounds__(256) interface_table_kernel(const Iface *faces, const int4 *tiles, int n_tiles,
-                                                              int with_cv) {
-  for (int q = blockIdx.x; q < n_tiles; q += gridDim.x) {
-    const int4 c = tiles[q];
-    const Iface &f = faces[c.x];
-    const int n0 = c.y * 32 + threadIdx.x, n1 = c.z * 8 + threadIdx.y, n2 = c.w;
-    if (n0 >= f.np[0] || n1 >= f.np[1]) continue;
-    interface_point<NS>(c_zones[f.zone], c_zones[f.target], f, with_cv, n0, n1, n2);
+// ---------------------------------------------------------------------------
+// the waves of one call in one cooperative launch: boundary faces (KIND 0,
+// every priority level's faces, then the periodic ones) or interfaces (KIND
+// 1, in the order of data_communication). The faces of a wave touch disjoint
+// cells; every CTA walks wave w's tiles and then waits at a grid barrier until
+// all CTAs have finished wave w, so wave w + 1 reads what wave w wrote. The
+// barrier counts arrivals in the context's WaveSync. Each wait is bounded by
+// the global timer: a CTA whose wait runs out sets abort (every other wait
+// then ends at once) and timed_out, which the host reads after the step; the
+// waves after it are not computed. The last CTA to leave resets the counters
+// for the next launch on the stream.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kWaveWaitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ unsigned long long wave_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// thread (0, 0) of a CTA: arrive, then wait until `target` arrivals in all
+__device__ __forceinline__ bool wave_barrier(WaveSync *s, unsigned target) {
+  __threadfence();  // this CTA's writes of the wave before its arrival
+  atomicAdd(&s->arrive, 1u);
+  const bool held = *(volatile int *)&s->hold != 0;
+  const unsigned long long t0 = wave_clock();
+  for (unsigned it = 0;; ++it) {
+    unsigned a;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(a) : "l"(&s->arrive) : "memory");
+    if (a >= target && !held) {
+      __threadfence();
+      return true;
+    }
+    if (*(volatile int *)&s->abort) return false;
+    if ((it & 15) == 15 && wave_clock() - t0 > kWaveWaitNs) {
+      atomicExch(&s->timed_out, 1);
+      atomicExch(&s->abort, 1);
+      return false;
+    }
+    if (it >= 4) __nanosleep(64);  // fewer polls of the one counter every CTA waits on
+  }
+}
+
+template <int NS, int KIND>
+__global__ void __launch_bounds__(256) waves_kernel(const void *records, const int4 *tiles, const int *ends,
+                                                    int n_waves, int with_cv, WaveSync *sync) {
+  __shared__ int go_on;
+  const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+  int begin = 0;
+  for (int w = 0; w < n_waves; ++w) {
+    const int end = ends[w];
+    for (int q = begin + blockIdx.x; q < end; q += gridDim.x) {
+      const int4 c = tiles[q];
+      // a tile spans the face's two tangential axes (32 along the first, 8
+      // along the second) at one layer along its normal (wave_axes)
+      const int u = c.y * 32 + threadIdx.x, v = c.z * 8 + threadIdx.y, w = c.w;
+      if constexpr (KIND == 0) {
+        const BcFace &b = static_cast<const BcFace *>(records)[c.x];
+        const int f = b.face;
+        const int i = b.rs[0] + (f == 0 ? w : u);
+        const int j = b.rs[1] + (f == 1 ? w : (f == 0 ? u : v));
+        const int k = b.rs[2] + (f == 2 ? w : v);
+        if (i <= b.re[0] && j <= b.re[1] && k <= b.re[2]) bc_point<NS>(c_zones[b.zone], b, with_cv, i, j, k);
+      } else {
+        // an interface normal to i (a few layers along i, the fastest index):
+        // each warp covers 4 layers x 8 points along j, so that the layers of
+        // a row share their sectors; the other faces as the boundary faces
+        const Iface &f = static_cast<const Iface *>(records)[c.x];
+        const int nf = f.face;
+        int n0, n1, n2;
+        if (nf == 0) {
+          n0 = c.w * 4 + (threadIdx.x & 3);
+          n1 = c.y * 8 + (threadIdx.x >> 2);
+          n2 = c.z * 8 + threadIdx.y;
+        } else {
+          n0 = u, n1 = nf == 1 ? w : v, n2 = nf == 2 ? w : v;
+        }
+        if (n0 < f.np[0] && n1 < f.np[1] && n2 < f.np[2])
+          interface_point<NS>(c_zones[f.zone], c_zones[f.target], f, with_cv, n0, n1, n2);
+      }
+    }
+    begin = end;
+    if (w + 1 < n_waves) {
+      __syncthreads();
+      if (lead) go_on = wave_barrier(sync, (unsigned)(w + 1) * gridDim.x) ? 1 : 0;
+      __syncthreads();
+      if (!go_on) break;
+    }
+  }
+  if (lead) {
+    __threadfence();
+    if (atomicAdd(&sync->done, 1u) == gridDim.x - 1) {
+      // every CTA has left its last wait: reset for the next launch
+      sync->arrive = 0;
+      sync->abort = 0;
+      __threadfence();
+      sync->done = 0;
+    }
   }
 }
 
@@ -1170,32 +1249,45 @@ cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream
   return cudaGetLastError();
 }
 
-// one wave of boundary faces over every zone (bc_table_kernel): every
-// resident CTA slot, at most one per tile
-template <int NS>
-cudaError_t launch_bc_table(const BcFace *faces, const CellTable &tab, int with_cv, cudaStream_t s) {
-  if (tab.n <= 0) return cudaSuccess;
-  int per_sm = 0, dev = 0, sms = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bc_table_kernel<NS>, 256, 0);
+// the waves of one call (waves_kernel): one cooperative launch of at most
+// every resident CTA slot and at most the largest wave's tiles (the barrier
+// needs every CTA resident at once, which a cooperative launch guarantees)
+template <int NS, int KIND>
+static cudaError_t launch_waves(const void *records, const WavePlan &p, int with_cv, WaveSync *sync, cudaStream_t s) {
+  if (p.n_waves <= 0 || p.max_tiles <= 0) return cudaSuccess;
+  if (!records || !p.tiles || !p.ends || !sync) return cudaErrorInvalidValue;
+  int per_sm = 0, dev = 0, sms = 0, coop = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, waves_kernel<NS, KIND>, 256, 0);
   if (e == cudaSuccess) e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
   if (e != cudaSuccess) return e;
-  const int slots = per_sm * sms > 0 ? per_sm * sms : 1;
-  bc_table_kernel<NS><<<tab.n < slots ? tab.n : slots, dim3(32, 8), 0, s>>>(faces, tab.tiles, tab.n, with_cv);
-  return cudaGetLastError();
+  const int slots = per_sm * sms;
+  if (slots < 1) return cudaErrorInvalidConfiguration;
+  const int grid = p.max_tiles < slots ? p.max_tiles : slots;
+  if (!coop) return cudaErrorNotSupported;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(32, 8);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  e = cudaLaunchKernelEx(&cfg, waves_kernel<NS, KIND>, records, p.tiles, p.ends, p.n_waves, with_cv, sync);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <int NS>
-cudaError_t launch_interface_table(const Iface *faces, const CellTable &tab, int with_cv, cudaStream_t s) {
-  if (tab.n <= 0) return cudaSuccess;
-  int per_sm = 0, dev = 0, sms = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, interface_table_kernel<NS>, 256, 0);
-  if (e == cudaSuccess) e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e != cudaSuccess) return e;
-  const int slots = per_sm * sms > 0 ? per_sm * sms : 1;
-  interface_table_kernel<NS><<<tab.n < slots ? tab.n : slots, dim3(32, 8), 0, s>>>(faces, tab.tiles, tab.n, with_cv);
-  return cudaGetLastError();
+cudaError_t launch_bc_waves(const BcFace *faces, const WavePlan &p, int with_cv, WaveSync *sync, cudaStream_t s) {
+  return launch_waves<NS, 0>(faces, p, with_cv, sync, s);
+}
+
+template <int NS>
+cudaError_t launch_interface_waves(const Iface *faces, const WavePlan &p, int with_cv, WaveSync *sync, cudaStream_t s) {
+  return launch_waves<NS, 1>(faces, p, with_cv, sync, s);
 }
 
 template <int NS>
@@ -1351,8 +1443,8 @@ cudaError_t upload_param(const DevParam &p, cudaStream_t s) {
   template cudaError_t launch_cells<NS>(CellOp, const DevZone &, const CellArgs &, cudaStream_t);            \
   template cudaError_t launch_cells_table<NS>(CellOp, const CellTable &, const CellArgs &, cudaStream_t);    \
   template cudaError_t launch_bc<NS>(const DevZone &, const BcFace &, int, cudaStream_t);                    \
-  template cudaError_t launch_bc_table<NS>(const BcFace *, const CellTable &, int, cudaStream_t);             \
-  template cudaError_t launch_interface_table<NS>(const Iface *, const CellTable &, int, cudaStream_t);       \
+  template cudaError_t launch_bc_waves<NS>(const BcFace *, const WavePlan &, int, WaveSync *, cudaStream_t);   \
+  template cudaError_t launch_interface_waves<NS>(const Iface *, const WavePlan &, int, WaveSync *, cudaStream_t); \
   template cudaError_t launch_interface<NS>(const DevZone &, const DevZone &, const Iface &, int, cudaStream_t); \
   template cudaError_t launch_steady<NS>(SteadyOp, const DevZone &, const SteadyArgs &, const BcFace *, cudaStream_t); \
   template cudaError_t launch_chem_integrator<NS>(int, const double *, const double *, const double *, const double *, \

@@ -132,11 +132,31 @@ cudaError_t stage_timeout_flux_ns_d(int *flag);
 cudaError_t stage_timeouts(int *any);
 template <int NS>
 cudaError_t launch_bc(const DevZone &z, const BcFace &b, int with_cv, cudaStream_t s);
-// one wave of faces (device records, zones in the tile-table zone table)
+// The waves of one call (boundary faces or interfaces over every zone; device
+// records, zones in the tile-table zone table): tiles {record, a, b, c} of a
+// face's points (32 along its first tangential axis and 8 along the second at
+// one layer along its normal; interfaces normal to i: 4 layers x 8 x 8), wave
+// after wave; ends[w] is the end of wave w in tiles. One cooperative launch
+// walks all waves with a grid barrier between them.
+struct WavePlan {
+  const int4 *tiles = nullptr;
+  const int *ends = nullptr;  // device, n_waves entries
+  int n_waves = 0;
+  int max_tiles = 0;          // tiles of the largest wave (grid bound)
+};
+// the grid barrier of a wave launch (device memory of the context, zeroed
+// once): arrivals, CTAs that have left, the abort flag of a wait that ran
+// out, timed_out, which stays set until the host reads and clears it, and
+// hold, a diagnostic the host sets to withhold every barrier's release (its
+// waits then run out: ostc_inject_wave_timeout)
+struct WaveSync {
+  unsigned arrive, done;
+  int abort, timed_out, hold, pad;
+};
 template <int NS>
-cudaError_t launch_bc_table(const BcFace *faces, const CellTable &tab, int with_cv, cudaStream_t s);
+cudaError_t launch_bc_waves(const BcFace *faces, const WavePlan &p, int with_cv, WaveSync *sync, cudaStream_t s);
 template <int NS>
-cudaError_t launch_interface_table(const Iface *faces, const CellTable &tab, int with_cv, cudaStream_t s);
+cudaError_t launch_interface_waves(const Iface *faces, const WavePlan &p, int with_cv, WaveSync *sync, cudaStream_t s);
 template <int NS>
 cudaError_t launch_interface(const DevZone &self, const DevZone &tar, const Iface &f, int with_cv, cudaStream_t s);
 template <int NS>

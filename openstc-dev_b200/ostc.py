@@ -135,6 +135,7 @@ def lib():
             "ostc_get_tile": [vp, i, C.POINTER(i), C.POINTER(i)],
             "ostc_set_batching": [vp, i],
             "ostc_get_batching": [vp, C.POINTER(i)],
+            "ostc_inject_wave_timeout": [vp, i],
             "ostc_launch_op": [vp, i, i, vp],
             "ostc_autotune": [vp, i, i, vp, C.POINTER(C.c_float)],
             "ostc_set_interfaces": [vp, C.POINTER(IfaceC), i],
@@ -717,9 +718,16 @@ class Solver:
         return n.value
 
     def set_batching(self, on: bool):
-        """one persistent tile-table launch per kernel over all blocks (True)
-        or one launch per block (False)"""
+        """one persistent tile-table launch per kernel over all blocks, and
+        one launch per call for the boundary faces and for the interfaces
+        (True), or one launch per block and face (False)"""
         check(lib().ostc_set_batching(self.ctx, int(bool(on))), "ostc_set_batching")
+
+    def inject_wave_timeout(self, on: bool):
+        """diagnostic: make the grid barriers of the batched boundary-face and
+        interface launches run out (calls with histories then return
+        OSTC_ERR_TIMEOUT)"""
+        check(lib().ostc_inject_wave_timeout(self.ctx, 1 if on else 0), "ostc_inject_wave_timeout")
 
     def batching(self) -> bool:
         v = C.c_int()

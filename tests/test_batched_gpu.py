@@ -87,9 +87,10 @@ def test_batching_toggle_on_one_context():
     s.close()
 
 
-# boundary faces in batched launches: each priority level's faces over all
-# blocks in waves of faces with disjoint footprints; the per-face order of the
-# reference stays wherever two faces of a block touch the same cells
+# boundary faces in batched launches: every face of every block (priority
+# levels, then the periodic wraps) in one cooperative launch, in waves of faces
+# with disjoint footprints; the per-face order of the reference stays wherever
+# two faces of a block touch the same cells
 BC_CASES = {
     "wall_farfield": lambda: ostc.case_bc_box("wall_farfield", 34, 27, 9),
     "subsonic": lambda: ostc.case_bc_box("subsonic", 34, 27, 9),
@@ -120,3 +121,53 @@ def test_boundary_waves_batch_the_faces_that_do_not_meet():
     n_face = s.step_kernel_count(False)
     s.close()
     assert n_batched < n_face, (n_batched, n_face)
+
+
+def _stage_count(case, batched):
+    s, _ = case.solver()
+    s.set_batching(batched)
+    n = s.step_kernel_count(False)
+    s.close()
+    return n
+
+
+def test_faces_and_interfaces_are_one_launch_per_call():
+    """batched, a step's launches do not depend on how many faces and
+    interfaces the blocks have: a layout of 9 blocks and one of 37 blocks of
+    the same flow give the same count (default tiles, one flux launch per
+    sweep), and fewer than the per-face launches"""
+    few = ostc.case_uneven_blocks(
+        layout=ostc.block_layout(5, n_layers=2, n_cols=2, rows=(2, 2), extra_row=(0, 0), dims=(40, 30, 24),
+                                 ranges=((8, 24), (8, 16), (8, 14)), anchors=False),
+        rans_model=2)
+    many = ostc.case_uneven_blocks(
+        layout=ostc.block_layout(5, dims=(40, 30, 32), ranges=((8, 20), (8, 14), (8, 10)), anchors=False),
+        rans_model=2)
+    assert len(few.blocks) < len(many.blocks) and len(few.interfaces) < len(many.interfaces)
+    n_few, n_many = _stage_count(few, True), _stage_count(many, True)
+    assert n_few == n_many, (n_few, n_many)
+    assert n_few < _stage_count(few, False)
+
+
+def test_one_block_launches_per_face_by_default():
+    """one block: per-face launches by default (batching off), batched faces
+    on request; the step count is taken first, before any other call on the
+    context (its graph capture must not hold the parameter upload), and the
+    steps that follow equal those of a per-face context bit for bit"""
+    case = lambda: ostc.case_mixing_layer(33, 26, 9, dx=1e-3, full_host=True)
+    s, blocks = case().solver()
+    assert not s.batching()
+    n_default = s.step_kernel_count(False)
+    s.initialize()
+    res, dts = s.rk3_steps(4, history=True)
+    got = {"res": res, "dt": dts, "bv": [b.download("bv") for b in blocks]}
+    s.close()
+    ref = _run(case(), False, steps=4)
+    for k in ("res", "dt", "bv"):
+        if isinstance(got[k], list):
+            for x, y in zip(got[k], ref[k]):
+                assert np.array_equal(x, y), k
+        else:
+            assert np.array_equal(got[k], ref[k]), k
+    assert n_default == _stage_count(case(), False)
+    assert _stage_count(case(), True) < n_default

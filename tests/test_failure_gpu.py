@@ -7,7 +7,11 @@
   restores a valid state;
 * a bounded tensor-core wait that runs out (its completion signal withheld
   on request, a flag that nothing sets) is reported as OSTC_ERR_TIMEOUT after
-  about a second, and the next call gives the normal result.
+  about a second, and the next call gives the normal result;
+* likewise the bounded grid barrier between the waves of the batched
+  boundary-face and interface launches (its release withheld on request):
+  the steps with histories return OSTC_ERR_TIMEOUT and, with the release
+  restored, the same context steps as a fresh one.
 """
 import time
 
@@ -86,3 +90,35 @@ def test_bounded_tensor_core_wait_runs_out_and_recovers():
     torch.cuda.synchronize()
     assert torch.equal(y, y_ref)
     sur.close()
+
+
+def test_bounded_wave_barrier_runs_out_and_recovers():
+    def make():
+        return ostc.case_uneven_blocks(
+            layout=ostc.block_layout(5, dims=(40, 30, 32), ranges=((8, 20), (8, 14), (8, 10)), anchors=False),
+            rans_model=2)
+
+    ref_case = make()
+    s_ref, _ = ref_case.solver()
+    s_ref.initialize()
+    res_ref, dt_ref = s_ref.rk3_steps(2, history=True)
+    s_ref.close()
+
+    s, blocks = make().solver()
+    assert s.batching()
+    s.initialize()
+    s.inject_wave_timeout(True)
+    t0 = time.perf_counter()
+    with pytest.raises(ostc.OstcError) as e:
+        s.rk3_steps(1, history=True)
+    waited = time.perf_counter() - t0
+    assert e.value.status == ostc.ERR_TIMEOUT
+    assert 0.5 < waited < 60.0, waited
+    s.inject_wave_timeout(False)
+    # the state after the withheld waves is not valid: start again from the inputs
+    for b, h in zip(blocks, make().blocks):
+        b.upload_inputs(h)
+    s.initialize()
+    res, dts = s.rk3_steps(2, history=True)
+    assert np.array_equal(res, res_ref) and np.array_equal(dts, dt_ref)
+    s.close()
