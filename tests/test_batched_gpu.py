@@ -149,11 +149,12 @@ def test_faces_and_interfaces_are_one_launch_per_call():
     assert n_few < _stage_count(few, False)
 
 
-def test_one_block_launches_per_face_by_default():
-    """one block: per-face launches by default (batching off), batched faces
-    on request; the step count is taken first, before any other call on the
+def test_one_block_with_small_faces_batches_them_by_default():
+    """one block: tile tables off by default; its faces (outflow and periodic,
+    a few thousand points) in one wave launch, which launch-bound small faces
+    favour. The step count is taken first, before any other call on the
     context (its graph capture must not hold the parameter upload), and the
-    steps that follow equal those of a per-face context bit for bit"""
+    steps that follow equal those of per-face launches bit for bit"""
     case = lambda: ostc.case_mixing_layer(33, 26, 9, dx=1e-3, full_host=True)
     s, blocks = case().solver()
     assert not s.batching()
@@ -169,5 +170,4 @@ def test_one_block_launches_per_face_by_default():
                 assert np.array_equal(x, y), k
         else:
             assert np.array_equal(got[k], ref[k]), k
-    assert n_default == _stage_count(case(), False)
-    assert _stage_count(case(), True) < n_default
+    assert n_default < _stage_count(case(), False)
