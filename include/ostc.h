@@ -598,7 +598,9 @@ ostc_status ostc_autotune(ostc_ctx *ctx, int warmup, int reps, void *stream, flo
  * of {block, tile} entries built from the blocks' extents and the flux tile
  * shapes. Results are identical to the per-block launches (on = 0): every
  * cell sees the same operations in the same order. Default: on for 2 to 64
- * blocks, off for one. Batched, ostc_apply_boundary_conditions is one
+ * blocks, off for one (a single block whose boundary faces hold at most
+ * 2^17 points still takes the one-launch boundary faces below, which small,
+ * launch-bound faces favour). Batched, ostc_apply_boundary_conditions is one
  * cooperative launch over
  * every face in the per-face order (priority levels of BoundCond.cuh:673-822,
  * then the periodic wraps), ostc_data_communication one over every interface
